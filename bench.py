@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Closest-hit throughput benchmark (Mrays/s) on one or more B200s.
+
+Workload (one step = one closest-hit launch over one ray batch):
+  scene  : 512 instanced icospheres (subdivision 3, radius log-uniform
+           [0.02, 0.2], centres U[-1,1]^3) + a tessellated floor quad =
+           655,872 FP32 triangles, seeded (the plain path-tracing scene).
+  rays   : 512x512 pixels x 64 spp jittered camera rays, plus the first
+           cosine-distributed diffuse bounce of every camera ray that hits
+           (the extension rays of the first two wavefront stages). The batch
+           is larger than L2 (no flush needed between steps).
+Multi-GPU: one process per GPU, each tracing its own batch (weak scaling, no
+collective on the data path); time = max over ranks of the device time.
+
+Arms: default = this framework (CUDA, sm_100a). `--impl reference` = the
+reference's CPU path (its BVH build + its GLSL traversal and intersector
+compiled as C++, oracle/_ref) on the host cores, on a bounded sample of the
+same rays.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s closest-hit"
+UNIT = "Mrays/s"
+WORKLOAD = ("icosphere scene, 655,872 tris (512 icospheres subdiv 3 + floor); 512x512 px x 64 spp jittered camera "
+            "rays + first diffuse bounce of each hit")
+NODE_BYTES, TRI_BYTES, RAY_BYTES, HIT_BYTES = 80, 48, 32, 16
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--spp", type=int, default=64)
+    p.add_argument("--res", type=int, default=512)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=None)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------- workload --
+def camera_rays_torch(res: int, spp: int, seed: int, device):
+    """Jittered pinhole rays of the icosphere scene's camera, float32 [res*res*spp, 8]."""
+    import torch
+
+    g = torch.Generator(device=device).manual_seed(seed)
+    eye = torch.tensor([0.0, 1.0, -4.5], dtype=torch.float64, device=device)
+    tgt = torch.tensor([0.0, -0.3, 0.0], dtype=torch.float64, device=device)
+    fwd = (tgt - eye) / torch.linalg.norm(tgt - eye)
+    right = torch.linalg.cross(fwd, torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64, device=device))
+    right = right / torch.linalg.norm(right)
+    up = torch.linalg.cross(right, fwd)
+    tan_half = float(np.tan(np.radians(50.0) / 2))
+    n = res * res * spp
+    pix = torch.arange(res * res, device=device, dtype=torch.float64).repeat(spp)
+    px = (pix % res) + torch.rand(n, generator=g, device=device, dtype=torch.float64)
+    py = torch.div(pix, res, rounding_mode="floor") + torch.rand(n, generator=g, device=device, dtype=torch.float64)
+    sx = (2.0 * px / res - 1.0) * tan_half
+    sy = (1.0 - 2.0 * py / res) * tan_half
+    d = fwd[None] + sx[:, None] * right[None] + sy[:, None] * up[None]
+    d = d / torch.linalg.norm(d, dim=1, keepdim=True)
+    rays = torch.empty((n, 8), dtype=torch.float32, device=device)
+    rays[:, 0:3] = eye.float()
+    rays[:, 3] = 0.0
+    rays[:, 4:7] = d.float()
+    rays[:, 7] = float("inf")
+    return rays
+
+
+def world_triangles(scene) -> np.ndarray:
+    """World-space triangles [T, 9] in prim order (drawables in order)."""
+    idx = scene["indices"].astype(np.int64)
+    v = scene["vertices"].astype(np.float64)
+    out = []
+    for d in scene["drawables"]:
+        m = np.array(d.transformation[:], np.float64).reshape(4, 4).T
+        sel = idx[d.indices_base_index: d.indices_base_index + d.index_count] + d.points_base_index
+        p = v[sel] @ m[:3, :3].T + m[:3, 3]
+        out.append(p.reshape(-1, 9))
+    return np.concatenate(out).astype(np.float32)
+
+
+def bounce_rays_torch(rays, hits, tris9, seed: int):
+    """First diffuse bounce (cosine-weighted about the face normal) of each hit ray."""
+    import torch
+
+    hit = hits[:, 0].view(torch.int32)
+    ok = hit >= 0
+    r = rays[ok]
+    h = hits[ok]
+    prim = hit[ok].long()
+    tri = tris9[prim].view(-1, 3, 3)
+    n = torch.linalg.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
+    n = n / torch.linalg.norm(n, dim=1, keepdim=True).clamp_min(1e-30)
+    d = r[:, 4:7]
+    n = torch.where(((n * d).sum(1, keepdim=True) > 0), -n, n)
+    p = r[:, 0:3] + h[:, 1:2] * d
+    g = torch.Generator(device=rays.device).manual_seed(seed)
+    u1 = torch.rand(r.shape[0], generator=g, device=rays.device)
+    u2 = torch.rand(r.shape[0], generator=g, device=rays.device)
+    a = torch.where(n[:, 0:1].abs() > 0.9, torch.tensor([0.0, 1.0, 0.0], device=rays.device),
+                    torch.tensor([1.0, 0.0, 0.0], device=rays.device))
+    t = torch.linalg.cross(n, a)
+    t = t / torch.linalg.norm(t, dim=1, keepdim=True)
+    b = torch.linalg.cross(n, t)
+    rad = u1.sqrt()
+    phi = 2.0 * np.pi * u2
+    local = torch.stack([rad * phi.cos(), rad * phi.sin(), (1.0 - u1).clamp_min(0).sqrt()], 1)
+    wd = local[:, 0:1] * t + local[:, 1:2] * b + local[:, 2:3] * n
+    out = torch.empty((r.shape[0], 8), dtype=torch.float32, device=rays.device)
+    out[:, 0:3] = p + 1e-4 * n
+    out[:, 3] = 0.0
+    out[:, 4:7] = wd / torch.linalg.norm(wd, dim=1, keepdim=True)
+    out[:, 7] = float("inf")
+    return out
+
+
+def make_batch(ctx, scene, res, spp, seed, device):
+    import torch
+
+    prim_rays = camera_rays_torch(res, spp, seed, device)
+    hits = torch.empty((prim_rays.shape[0], 4), dtype=torch.float32, device=device)
+    s = torch.cuda.current_stream(device).cuda_stream
+    ctx.trace_closest_device(prim_rays, hits, stream=s)
+    ctx.sync()
+    tris9 = torch.from_numpy(world_triangles(scene)).to(device)
+    sec = bounce_rays_torch(prim_rays, hits, tris9, seed + 1)
+    del hits
+    rays = torch.cat([prim_rays, sec], 0).contiguous()
+    return rays, int(prim_rays.shape[0]), int(sec.shape[0])
+
+
+# ---------------------------------------------------------------- helpers --
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": FALLBACK_HBM_GBS}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        time.sleep(0.25)
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.proc or not self.path or not os.path.exists(self.path):
+            return None
+        rows = [ln.split(",") for ln in open(self.path).read().strip().splitlines() if ln.count(",") >= 8]
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_reference_rate(scene, rays_np: np.ndarray, target_seconds: float = 12.0):
+    """The reference's CPU path on a bounded sample: oracle/_ref when built
+    (reference BVH build with dont_split + its GLSL traversal compiled as C++),
+    else the oracle's restatement. Returns (Mrays/s, cores, kind, sample)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    tris9 = world_triangles(scene)
+    idx = np.arange(tris9.shape[0] * 3, dtype=np.uint32)
+    pts = tris9.reshape(-1, 3)
+    cores = po.nthreads()
+    if po.ref_available():
+        kind = "reference"
+        h = po.ref_bvh(idx, pts, split=False)
+        nodes, bi = po.ref_bvh_arrays(h)
+        po.ref().ref_bvh_free(h)
+
+        def run(r):
+            return po.ref_glsl_traverse(nodes, bi, idx, pts, r, threads=cores)
+    else:
+        kind = "port"
+        nodes, bi = po.refbvh_build(idx, pts)
+
+        def run(r):
+            return po.refbvh_traverse(nodes, bi, idx, pts, r, canonical=False)
+    rng = np.random.default_rng(0)
+    probe = rays_np[rng.choice(rays_np.shape[0], 32768, replace=False)]
+    t0 = time.perf_counter()
+    run(probe)
+    rate = probe.shape[0] / (time.perf_counter() - t0)
+    n = int(min(rays_np.shape[0], max(65536, rate * target_seconds)))
+    sample = rays_np[rng.choice(rays_np.shape[0], n, replace=False)]
+    t0 = time.perf_counter()
+    run(sample)
+    dt = time.perf_counter() - t0
+    desc = (f"{n} rays drawn uniformly from the step's batch; reference BVH (bvh.cpp, dont_split) over the baked "
+            f"world triangles + bvh.impl.glsl/intersect.glsl traversal, {cores} threads")
+    return n / dt / 1e6, cores, kind, desc, dt
+
+
+# ------------------------------------------------------------------- arms --
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from myrt_b200.scenes import icosphere_camera_rays, icosphere_field
+
+    scene = icosphere_field()
+    rays = icosphere_camera_rays(args.res, args.res, spp=1)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    tris9 = world_triangles(scene)
+    idx = np.arange(tris9.shape[0] * 3, dtype=np.uint32)
+    pts = tris9.reshape(-1, 3)
+    cores = po.nthreads()
+    kind = "reference" if po.ref_available() else "port"
+    if kind == "reference":
+        h = po.ref_bvh(idx, pts, split=False)
+        nodes, bi = po.ref_bvh_arrays(h)
+        po.ref().ref_bvh_free(h)
+    else:
+        nodes, bi = po.refbvh_build(idx, pts)
+    per_step = 131072
+    rng = np.random.default_rng(1)
+
+    def step():
+        r = rays[rng.choice(rays.shape[0], per_step, replace=False)]
+        if kind == "reference":
+            po.ref_glsl_traverse(nodes, bi, idx, pts, r, threads=cores)
+        else:
+            po.refbvh_traverse(nodes, bi, idx, pts, r, canonical=False)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = time.perf_counter() - t0
+    value = per_step * args.steps / dt / 1e6
+    sample = (f"{per_step} camera rays per step drawn from the 512x512 view; reference BVH (bvh.cpp, dont_split) "
+              f"+ its GLSL traversal compiled as C++, {cores} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "triangles": int(tris9.shape[0]), "rays_per_step": per_step},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+
+    import myrt_b200 as mb
+    from myrt_b200.scenes import icosphere_field
+
+    scene = icosphere_field()
+    ctx = mb.Context(local)
+    info = ctx.upload_scene(**scene)
+    rays, n_primary, n_secondary = make_batch(ctx, scene, args.res, args.spp, seed=1000 + rank, device=device)
+    n = rays.shape[0]
+    hits = torch.empty((n, 4), dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+    s = stream.cuda_stream
+
+    # algorithmic bytes of one launch, from the exact per-ray counters
+    cn = torch.empty(n, dtype=torch.int32, device=device)
+    ct = torch.empty(n, dtype=torch.int32, device=device)
+    ctx.trace_closest_stats_device(rays, hits, cn, ct, stream=s)
+    ctx.sync()
+    nodes_total = int(cn.sum(dtype=torch.int64))
+    tris_total = int(ct.sum(dtype=torch.int64))
+    del cn, ct
+    alg_bytes = NODE_BYTES * nodes_total + TRI_BYTES * tris_total + (RAY_BYTES + HIT_BYTES) * n
+
+    for _ in range(args.warmup):
+        ctx.trace_closest_device(rays, hits, stream=s)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        start.record(stream)
+        for _ in range(args.steps):
+            ctx.trace_closest_device(rays, hits, stream=s)
+        end.record(stream)
+        torch.cuda.synchronize()
+    ctx.sync()
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = n * world * args.steps / (ms / 1e3) / 1e6
+
+    # end to end through the host-memory C-ABI call (pinned buffers, copies inside)
+    e2e_steps = args.e2e_steps or max(3, min(args.steps, 10))
+    h_rays = torch.empty((n, 8), dtype=torch.float32, pin_memory=True)
+    h_rays.copy_(rays)
+    h_hits = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+    rays_np = h_rays.numpy()
+    hits_np = h_hits.numpy().view(mb.HIT_DTYPE).reshape(-1)
+    ctx.trace_closest(rays_np, out=hits_np)  # warm (allocates staging)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.trace_closest(rays_np, out=hits_np)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = n * world * e2e_steps / e2e_s / 1e6
+    chunks = (n + (1 << 20) - 1) >> 20
+
+    peaks, peak_kind = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "triangles": int(info["triangles"]), "rays_per_step": n,
+                   "camera_rays": n_primary, "bounce_rays": n_secondary, "res": args.res, "spp": args.spp,
+                   "intersector": "reference (Moller-Trumbore, bit-exact)",
+                   "l2": f"inputs larger than L2: {n * (RAY_BYTES + HIT_BYTES) / 1e6:.0f} MB of rays+hits per step",
+                   "bvh": {"wide_nodes": int(info["wide_nodes"]), "wide_depth": int(info["wide_depth"]),
+                           "node_bytes": int(info["node_bytes"]), "triangle_bytes": int(info["triangle_bytes"]),
+                           "build_s": round(float(info["build_seconds"]), 3)},
+                   "parallelism": f"dp{world} (independent ray batches)"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": f"hbm_gbs of {peak_kind}", "traffic": None,
+                     "bytes_per_ray": alg_bytes / n, "nodes_per_ray": nodes_total / n, "tris_per_ray": tris_total / n,
+                     "note": "algorithmic bytes = 80 B/node + 48 B/triangle + 48 B ray+hit; the 37 MB BVH is "
+                             "L2-resident, so most node bytes are served by L2"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * RAY_BYTES,
+                "d2h_bytes_per_step": n * HIT_BYTES, "steps": e2e_steps,
+                "api": "myrt_trace_closest (host pinned buffers, chunked copy/compute overlap)"},
+        "clocks": clocks.summary(),
+        "gpu_launches": args.steps,
+        "gpu_launches_e2e": e2e_steps * chunks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, kind, sample, dt = cpu_reference_rate(scene, rays_np)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+                                "seconds": round(dt, 2)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,189 @@
+/*
+ * myrt_cuda.h -- C ABI of the B200 wavefront path-tracing core.
+ *
+ * Plain C: pointers, sizes and POD structs only. Every function returns an
+ * int status (MYRT_OK = 0, negative on error; see myrt_status) and never
+ * throws. A context owns one CUDA device, one stream and all device memory;
+ * it is not thread-safe (synchronise externally), different contexts may be
+ * used from different threads. Host arrays passed in are read during the call
+ * only.
+ *
+ * Each entry point names the reference interface it replaces
+ * (johannes-braun/myrt, paths relative to that project).
+ */
+#ifndef MYRT_CUDA_H
+#define MYRT_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MYRT_ABI_VERSION 1
+
+typedef enum myrt_status {
+  MYRT_OK = 0,
+  MYRT_ERR_INVALID_ARGUMENT = -1,
+  MYRT_ERR_CUDA = -2,
+  MYRT_ERR_OUT_OF_MEMORY = -3,
+  MYRT_ERR_NO_SCENE = -4,
+  MYRT_ERR_UNSUPPORTED = -5,
+  MYRT_ERR_DEVICE_ABORT = -6, /* a kernel hit an iteration or stack limit and stopped */
+  MYRT_ERR_INTERNAL = -7
+} myrt_status;
+
+typedef struct myrt_ctx myrt_ctx;
+
+typedef struct myrt_device_opts {
+  int device;            /* CUDA ordinal */
+  uint32_t flags;        /* reserved, 0 */
+} myrt_device_opts;
+
+/* 32-byte ray: origin, tmin, direction, tmax. Direction need not be unit. */
+typedef struct myrt_ray {
+  float o[3];
+  float tmin;
+  float d[3];
+  float tmax;
+} myrt_ray;
+
+/* 16-byte hit: prim = triangle index in the uploaded index buffer order
+ * (index_count / 3 numbering), -1 on miss; t and barycentrics u (weight of
+ * the triangle's second vertex) and v (third vertex) as in
+ * src/pt/intersect.glsl:3-28. On a miss t = ray tmax, u = v = 0. */
+typedef struct myrt_hit {
+  int32_t prim;
+  float t;
+  float u;
+  float v;
+} myrt_hit;
+
+/* Instance record, byte-compatible with scene::drawable_geometry_t
+ * (src/pathtracer/scene.hpp:97-104): 160 bytes. */
+typedef struct myrt_drawable {
+  float transformation[16];         /* column-major mat4 */
+  float inverse_transformation[16]; /* column-major mat4 */
+  uint32_t bvh_node_base_index;     /* ignored: the core builds its own BVH */
+  uint32_t bvh_index_base_index;    /* ignored */
+  uint32_t indices_base_index;
+  uint32_t points_base_index;
+  uint32_t index_count;
+  int32_t material_index;
+  int32_t geometry_index;
+  int32_t pad;
+} myrt_drawable;
+
+/* scene::material_reference_t (src/pathtracer/scene.hpp:111-114). */
+typedef struct myrt_material_ref {
+  int32_t id;     /* material type id; 0 = the app's PBR type (7 floats) */
+  int32_t offset; /* float offset into material_data */
+} myrt_material_ref;
+
+/* Host view of the scene arrays scene::prepare uploads
+ * (src/pathtracer/scene.hpp:216-224, scene.cpp:330-409). vertices and
+ * normals use the reference's 16-byte aligned_point_t stride (xyz + pad). If
+ * drawable_count == 0 the whole index buffer is one drawable with an identity
+ * transform and material 0. */
+typedef struct myrt_scene_view {
+  const uint32_t* indices;
+  size_t index_count;
+  const float* vertices; /* 4 floats per vertex */
+  size_t vertex_count;
+  const float* normals;  /* 4 floats per vertex, may be NULL */
+  const float* uvs;      /* 2 floats per vertex, may be NULL */
+  const myrt_drawable* drawables;
+  size_t drawable_count;
+  const myrt_material_ref* materials;
+  size_t material_count;
+  const float* material_data;
+  size_t material_data_count;
+} myrt_scene_view;
+
+/* Build statistics of the uploaded scene's BVH. */
+typedef struct myrt_bvh_info {
+  uint64_t triangles;
+  uint64_t binary_nodes;
+  uint64_t wide_nodes;
+  uint64_t leaf_slots;
+  int32_t binary_depth;
+  int32_t wide_depth;
+  int32_t max_leaf_size;
+  int32_t pad;
+  double build_seconds;
+  uint64_t node_bytes;
+  uint64_t triangle_bytes;
+} myrt_bvh_info;
+
+/* Intersector selection. MYRT_ISECT_REFERENCE is Moller-Trumbore exactly as
+ * src/pt/intersect.glsl:3-28 (det epsilon 1e-23, border slack 1e-6);
+ * MYRT_ISECT_WATERTIGHT is Woop, Benthin and Wald (JCGT 2013). Both report
+ * the closest hit with ties in t broken towards the smaller prim index. */
+typedef enum myrt_intersector {
+  MYRT_ISECT_REFERENCE = 0,
+  MYRT_ISECT_WATERTIGHT = 1
+} myrt_intersector;
+
+/* ---- host-only BVH (no device needed) -------------------------------------- */
+
+typedef struct myrt_bvh8_host myrt_bvh8_host;
+/* Builds the 8-wide BVH on the host from world-space triangles (9 floats each:
+ * v0, v1, v2). Replaces bvh::bvh + bvh::nodes() / reordered_indices()
+ * (src/pathtracer/bvh.hpp:157-176) for callers that inspect the tree. */
+int myrt_bvh8_build(const float* positions, size_t n_tris, myrt_bvh8_host** out);
+int myrt_bvh8_get_info(const myrt_bvh8_host* bvh, myrt_bvh_info* info);
+/* Copies the nodes (80 bytes each) and leaf-ordered triangles (48 bytes each). */
+int myrt_bvh8_copy(const myrt_bvh8_host* bvh, void* nodes, void* triangles);
+int myrt_bvh8_free(myrt_bvh8_host* bvh);
+
+/* ---- context ------------------------------------------------------------ */
+
+/* Replaces the GL context + sequential_pathtracer construction
+ * (src/main.cpp:228-231, src/pathtracer/sequential_pathtracer.hpp:22-59). */
+int myrt_ctx_create(const myrt_device_opts* opts, myrt_ctx** out);
+int myrt_ctx_destroy(myrt_ctx* ctx);
+/* Copies the last error message (NUL-terminated, truncated to size). */
+int myrt_get_last_error(myrt_ctx* ctx, char* buf, size_t size);
+/* The context's CUDA stream (cudaStream_t) for callers that enqueue work. */
+int myrt_get_stream(myrt_ctx* ctx, void** stream);
+
+/* ---- scene ---------------------------------------------------------------- */
+
+/* Replaces scene::prepare's buffer uploads (src/pathtracer/scene.cpp:330-409)
+ * and the per-geometry bvh build (scene.cpp:43-71): builds the 8-wide BVH on
+ * the host over all drawables (baked to world space) and uploads it. */
+int myrt_scene_upload(myrt_ctx* ctx, const myrt_scene_view* scene);
+int myrt_scene_bvh_info(myrt_ctx* ctx, myrt_bvh_info* info);
+
+/* ---- ray queries ---------------------------------------------------------- */
+
+/* Closest hit for n rays in HOST memory (pinned or pageable); results to host.
+ * Replaces nearest_hit (src/pt/pt_trace.comp:331-386) for meshes and the CPU
+ * pick path scene::pick (src/pathtracer/scene.cpp:273-314). Copies overlap the
+ * kernels in chunks. */
+int myrt_trace_closest(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, myrt_hit* hits, int intersector);
+/* Same with DEVICE pointers, enqueued on `stream` (NULL = the ctx stream);
+ * asynchronous: call myrt_sync to wait and collect device error status. */
+int myrt_trace_closest_device(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, myrt_hit* hits, int intersector,
+    void* stream);
+/* Any hit (occlusion) for n host rays: occluded[i] = 1 if a triangle is hit
+ * with tmin <= t < tmax. Replaces any_hit (src/pt/pt_trace.comp:311-329). */
+int myrt_trace_any(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, uint8_t* occluded, int intersector);
+int myrt_trace_any_device(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, uint8_t* occluded, int intersector,
+    void* stream);
+/* Per-ray traversal counters for the closest-hit kernel (device pointers):
+ * nodes[i] = wide nodes fetched, tris[i] = triangles tested. Used to count the
+ * algorithmic bytes per ray (80 B per node, 48 B per triangle). */
+int myrt_trace_closest_stats_device(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, myrt_hit* hits,
+    uint32_t* nodes, uint32_t* tris, int intersector, void* stream);
+
+/* Waits for the context's work and returns MYRT_ERR_DEVICE_ABORT if a kernel
+ * stopped at a limit since the last call (the error word is then cleared). */
+int myrt_sync(myrt_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MYRT_CUDA_H */

@@ -1,0 +1,167 @@
+"""myrt_b200: B200-native wavefront path-tracing core behind myrt's interfaces.
+
+Python front end over the C ABI (include/myrt_cuda.h). The compute path is the
+in-tree CUDA library libmyrt_b200.so; importing this package without it
+raises (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import ISECT_REFERENCE, ISECT_WATERTIGHT, MYRT_ERR_DEVICE_ABORT, MYRT_OK  # noqa: F401
+
+_abi.lib()  # fail loudly at import if the native library is absent
+
+HIT_DTYPE = np.dtype([("prim", np.int32), ("t", np.float32), ("u", np.float32), ("v", np.float32)])
+
+
+class MyrtError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"myrt error {code}: {message}")
+        self.code = code
+
+
+def _ptr(a) -> int | None:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return int(a.data_ptr())  # torch tensor
+
+
+def bvh_info_dict(info: _abi.myrt_bvh_info) -> dict:
+    return {f: getattr(info, f) for f, _ in _abi.myrt_bvh_info._fields_ if f != "pad"}
+
+
+def build_bvh8(positions: np.ndarray):
+    """Host-only BVH build. positions: float32 [T, 3, 3] (or [T, 9]).
+    Returns (nodes uint32 [N, 20], triangles float32 [M, 12], info dict)."""
+    pos = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 9)
+    L = _abi.lib()
+    h = C.c_void_p()
+    rc = L.myrt_bvh8_build(pos.ctypes.data, pos.shape[0], C.byref(h))
+    if rc != MYRT_OK:
+        raise MyrtError(rc, "myrt_bvh8_build failed")
+    try:
+        info = _abi.myrt_bvh_info()
+        L.myrt_bvh8_get_info(h, C.byref(info))
+        nodes = np.zeros((info.wide_nodes, 20), np.uint32)
+        tris = np.zeros((info.triangles, 12), np.float32)
+        L.myrt_bvh8_copy(h, nodes.ctypes.data, tris.ctypes.data)
+        return nodes, tris, bvh_info_dict(info)
+    finally:
+        L.myrt_bvh8_free(h)
+
+
+class Context:
+    """One CUDA device, one stream, one resident scene (myrt_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._L = _abi.lib()
+        self._h = C.c_void_p()
+        opts = _abi.myrt_device_opts(device, 0)
+        rc = self._L.myrt_ctx_create(C.byref(opts), C.byref(self._h))
+        if rc != MYRT_OK:
+            raise MyrtError(rc, "myrt_ctx_create failed")
+        self._keep = []
+
+    # -- lifecycle --
+    def close(self):
+        if self._h:
+            self._L.myrt_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str):
+        if rc != MYRT_OK:
+            buf = C.create_string_buffer(512)
+            self._L.myrt_get_last_error(self._h, buf, 512)
+            raise MyrtError(rc, f"{what}: {buf.value.decode(errors='replace')}")
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        self._check(self._L.myrt_get_stream(self._h, C.byref(s)), "myrt_get_stream")
+        return s.value or 0
+
+    # -- scene --
+    def upload_scene(self, indices: np.ndarray, vertices: np.ndarray, normals: np.ndarray | None = None,
+                     uvs: np.ndarray | None = None, drawables: np.ndarray | None = None,
+                     materials: np.ndarray | None = None, material_data: np.ndarray | None = None) -> dict:
+        """Mirror of scene::prepare's uploads. vertices/normals: float32 [V, 3|4]."""
+        idx = np.ascontiguousarray(indices, dtype=np.uint32).ravel()
+
+        def pad4(a):
+            a = np.asarray(a, np.float32)
+            if a.shape[1] == 4:
+                return np.ascontiguousarray(a)
+            out = np.zeros((a.shape[0], 4), np.float32)
+            out[:, :3] = a
+            return out
+
+        verts = pad4(vertices)
+        nrm = pad4(normals) if normals is not None else None
+        uv = np.ascontiguousarray(uvs, np.float32) if uvs is not None else None
+        mats = np.ascontiguousarray(materials, np.int32).reshape(-1, 2) if materials is not None else None
+        mdata = np.ascontiguousarray(material_data, np.float32).ravel() if material_data is not None else None
+        view = _abi.myrt_scene_view(
+            idx.ctypes.data, idx.size, verts.ctypes.data, verts.shape[0], _ptr(nrm), _ptr(uv),
+            _ptr(drawables), 0 if drawables is None else len(drawables), _ptr(mats),
+            0 if mats is None else mats.shape[0], _ptr(mdata), 0 if mdata is None else mdata.size)
+        self._check(self._L.myrt_scene_upload(self._h, C.byref(view)), "myrt_scene_upload")
+        return self.bvh_info()
+
+    def bvh_info(self) -> dict:
+        info = _abi.myrt_bvh_info()
+        self._check(self._L.myrt_scene_bvh_info(self._h, C.byref(info)), "myrt_scene_bvh_info")
+        return bvh_info_dict(info)
+
+    # -- host-memory queries (copies inside the call) --
+    def trace_closest(self, rays: np.ndarray, intersector: int = ISECT_REFERENCE, out: np.ndarray | None = None):
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        hits = out if out is not None else np.empty(r.shape[0], HIT_DTYPE)
+        self._check(self._L.myrt_trace_closest(self._h, r.ctypes.data, r.shape[0], hits.ctypes.data, intersector),
+                    "myrt_trace_closest")
+        return hits
+
+    def trace_any(self, rays: np.ndarray, intersector: int = ISECT_REFERENCE):
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        occ = np.empty(r.shape[0], np.uint8)
+        self._check(self._L.myrt_trace_any(self._h, r.ctypes.data, r.shape[0], occ.ctypes.data, intersector),
+                    "myrt_trace_any")
+        return occ
+
+    # -- device-memory queries (torch tensors; asynchronous on `stream`) --
+    def trace_closest_device(self, rays, hits, intersector: int = ISECT_REFERENCE, stream: int | None = None):
+        n = rays.numel() // 8
+        self._check(self._L.myrt_trace_closest_device(self._h, _ptr(rays), n, _ptr(hits), intersector, stream),
+                    "myrt_trace_closest_device")
+
+    def trace_any_device(self, rays, occluded, intersector: int = ISECT_REFERENCE, stream: int | None = None):
+        n = rays.numel() // 8
+        self._check(self._L.myrt_trace_any_device(self._h, _ptr(rays), n, _ptr(occluded), intersector, stream),
+                    "myrt_trace_any_device")
+
+    def trace_closest_stats_device(self, rays, hits, nodes, tris, intersector: int = ISECT_REFERENCE,
+                                   stream: int | None = None):
+        n = rays.numel() // 8
+        self._check(self._L.myrt_trace_closest_stats_device(self._h, _ptr(rays), n, _ptr(hits), _ptr(nodes),
+                                                            _ptr(tris), intersector, stream),
+                    "myrt_trace_closest_stats_device")
+
+    def sync(self):
+        self._check(self._L.myrt_sync(self._h), "myrt_sync")

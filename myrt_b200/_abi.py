@@ -1,0 +1,97 @@
+"""ctypes declarations of the C ABI in include/myrt_cuda.h.
+
+The shared library is built in-tree (myrt_b200/build.py) and loaded from the
+package directory. There is no fallback: if the library is missing, importing
+the package raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libmyrt_b200.so"
+
+MYRT_OK = 0
+MYRT_ERR_INVALID_ARGUMENT = -1
+MYRT_ERR_CUDA = -2
+MYRT_ERR_OUT_OF_MEMORY = -3
+MYRT_ERR_NO_SCENE = -4
+MYRT_ERR_UNSUPPORTED = -5
+MYRT_ERR_DEVICE_ABORT = -6
+MYRT_ERR_INTERNAL = -7
+
+ISECT_REFERENCE = 0
+ISECT_WATERTIGHT = 1
+
+
+class myrt_device_opts(C.Structure):
+    _fields_ = [("device", C.c_int), ("flags", C.c_uint32)]
+
+
+class myrt_drawable(C.Structure):
+    _fields_ = [("transformation", C.c_float * 16), ("inverse_transformation", C.c_float * 16),
+                ("bvh_node_base_index", C.c_uint32), ("bvh_index_base_index", C.c_uint32),
+                ("indices_base_index", C.c_uint32), ("points_base_index", C.c_uint32), ("index_count", C.c_uint32),
+                ("material_index", C.c_int32), ("geometry_index", C.c_int32), ("pad", C.c_int32)]
+
+
+class myrt_material_ref(C.Structure):
+    _fields_ = [("id", C.c_int32), ("offset", C.c_int32)]
+
+
+class myrt_scene_view(C.Structure):
+    _fields_ = [("indices", C.c_void_p), ("index_count", C.c_size_t), ("vertices", C.c_void_p),
+                ("vertex_count", C.c_size_t), ("normals", C.c_void_p), ("uvs", C.c_void_p),
+                ("drawables", C.c_void_p), ("drawable_count", C.c_size_t), ("materials", C.c_void_p),
+                ("material_count", C.c_size_t), ("material_data", C.c_void_p), ("material_data_count", C.c_size_t)]
+
+
+class myrt_bvh_info(C.Structure):
+    _fields_ = [("triangles", C.c_uint64), ("binary_nodes", C.c_uint64), ("wide_nodes", C.c_uint64),
+                ("leaf_slots", C.c_uint64), ("binary_depth", C.c_int32), ("wide_depth", C.c_int32),
+                ("max_leaf_size", C.c_int32), ("pad", C.c_int32), ("build_seconds", C.c_double),
+                ("node_bytes", C.c_uint64), ("triangle_bytes", C.c_uint64)]
+
+
+P = C.c_void_p
+SZ = C.c_size_t
+U32 = C.c_uint32
+I = C.c_int
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "myrt_bvh8_build": (I, [P, SZ, C.POINTER(P)]),
+    "myrt_bvh8_get_info": (I, [P, C.POINTER(myrt_bvh_info)]),
+    "myrt_bvh8_copy": (I, [P, P, P]),
+    "myrt_bvh8_free": (I, [P]),
+    "myrt_ctx_create": (I, [C.POINTER(myrt_device_opts), C.POINTER(P)]),
+    "myrt_ctx_destroy": (I, [P]),
+    "myrt_get_last_error": (I, [P, C.c_char_p, SZ]),
+    "myrt_get_stream": (I, [P, C.POINTER(P)]),
+    "myrt_scene_upload": (I, [P, C.POINTER(myrt_scene_view)]),
+    "myrt_scene_bvh_info": (I, [P, C.POINTER(myrt_bvh_info)]),
+    "myrt_trace_closest": (I, [P, P, U32, P, I]),
+    "myrt_trace_closest_device": (I, [P, P, U32, P, I, P]),
+    "myrt_trace_any": (I, [P, P, U32, P, I]),
+    "myrt_trace_any_device": (I, [P, P, U32, P, I, P]),
+    "myrt_trace_closest_stats_device": (I, [P, P, U32, P, P, P, I, P]),
+    "myrt_sync": (I, [P]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libmyrt_b200.so (once). Raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m myrt_b200.build` "
+                               "(or __graft_entry__.build()); there is no CPU fallback")
+        h = C.CDLL(str(LIB_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(h, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = h
+    return _lib

@@ -1,0 +1,426 @@
+// C ABI: context, scene upload and ray queries (include/myrt_cuda.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/myrt_cuda.h"
+#include "bvh8.hpp"
+#include "ctx.hpp"
+#include "trace.cuh"
+
+namespace myrt_b200 {
+
+int set_error(myrt_ctx* ctx, int code, std::string msg) {
+  if (ctx) ctx->last_error = std::move(msg);
+  return code;
+}
+
+int check_cuda(myrt_ctx* ctx, cudaError_t e, char const* what) {
+  if (e == cudaSuccess) return MYRT_OK;
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  return set_error(ctx, e == cudaErrorMemoryAllocation ? MYRT_ERR_OUT_OF_MEMORY : MYRT_ERR_CUDA, m);
+}
+
+namespace {
+
+void free_scene(device_scene& s) {
+  cudaFree(s.nodes);
+  cudaFree(s.tris);
+  cudaFree(s.tri_normals);
+  cudaFree(s.tri_uvs);
+  cudaFree(s.tri_material);
+  cudaFree(s.materials);
+  cudaFree(s.material_data);
+  s = device_scene{};
+}
+
+bool is_identity(float const* m) {
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r)
+      if (m[c * 4 + r] != (c == r ? 1.f : 0.f)) return false;
+  return true;
+}
+
+// column-major mat4 * (x, y, z, w), left-to-right sums
+void xform(float const* m, float const* v, float w, float* out) {
+  for (int r = 0; r < 3; ++r) out[r] = ((m[r] * v[0] + m[4 + r] * v[1]) + m[8 + r] * v[2]) + m[12 + r] * w;
+}
+
+template <typename T> int upload(myrt_ctx* ctx, T** dst, T const* src, size_t count, char const* what) {
+  if (count == 0) return MYRT_OK;
+  int rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(dst), count * sizeof(T)), what);
+  if (rc) return rc;
+  return check_cuda(ctx, cudaMemcpyAsync(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice, ctx->stream), what);
+}
+
+int ensure_stage(myrt_ctx* ctx, size_t bytes) {
+  if (ctx->stage_bytes >= bytes) return MYRT_OK;
+  for (auto& p : ctx->stage) {
+    cudaFree(p);
+    p = nullptr;
+  }
+  ctx->stage_bytes = 0;
+  for (auto& p : ctx->stage) {
+    int rc = check_cuda(ctx, cudaMalloc(&p, bytes), "staging buffer");
+    if (rc) return rc;
+  }
+  ctx->stage_bytes = bytes;
+  return MYRT_OK;
+}
+
+constexpr uint32_t kChunkRays = 1u << 20;
+
+int launch_trace(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s) {
+  if (a.n == 0) return MYRT_OK;
+  dim3 const block(128);
+  dim3 const grid((a.n + 127) / 128);
+  if (intersector == MYRT_ISECT_REFERENCE) {
+    if (any) k_trace<0, true, false><<<grid, block, 0, s>>>(a);
+    else if (stats) k_trace<0, false, true><<<grid, block, 0, s>>>(a);
+    else k_trace<0, false, false><<<grid, block, 0, s>>>(a);
+  } else {
+    if (any) k_trace<1, true, false><<<grid, block, 0, s>>>(a);
+    else if (stats) k_trace<1, false, true><<<grid, block, 0, s>>>(a);
+    else k_trace<1, false, false><<<grid, block, 0, s>>>(a);
+  }
+  return check_cuda(ctx, cudaGetLastError(), "trace launch");
+}
+
+int validate_query(myrt_ctx* ctx, void const* rays, void const* out, int intersector) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!ctx->scene.valid) return set_error(ctx, MYRT_ERR_NO_SCENE, "no scene uploaded");
+  if (!rays || !out) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "null ray or output pointer");
+  if (intersector != MYRT_ISECT_REFERENCE && intersector != MYRT_ISECT_WATERTIGHT)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "unknown intersector");
+  return MYRT_OK;
+}
+
+trace_args base_args(myrt_ctx* ctx) {
+  trace_args a{};
+  a.nodes = ctx->scene.nodes;
+  a.tris = ctx->scene.tris;
+  a.err = ctx->d_err;
+  return a;
+}
+
+// Host-memory query: chunks alternate between two streams so the copy of one
+// chunk overlaps the traversal of the other.
+int host_query(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, void* out, size_t out_stride, int intersector,
+    bool any) {
+  size_t const chunk_bytes = size_t(kChunkRays) * (sizeof(myrt_ray) + sizeof(myrt_hit));
+  int rc = ensure_stage(ctx, chunk_bytes);
+  if (rc) return rc;
+  cudaStream_t lanes[2] = {ctx->stream, ctx->aux_stream};
+  for (uint32_t c0 = 0, k = 0; c0 < n; c0 += kChunkRays, ++k) {
+    uint32_t const cn = std::min(kChunkRays, n - c0);
+    cudaStream_t const s = lanes[k & 1];
+    char* base = static_cast<char*>(ctx->stage[k & 1]);
+    auto* d_rays = reinterpret_cast<float4*>(base);
+    char* d_out = base + size_t(kChunkRays) * sizeof(myrt_ray);
+    rc = check_cuda(ctx, cudaMemcpyAsync(d_rays, rays + c0, size_t(cn) * sizeof(myrt_ray), cudaMemcpyHostToDevice, s),
+        "ray upload");
+    if (rc) return rc;
+    trace_args a = base_args(ctx);
+    a.rays = d_rays;
+    a.n = cn;
+    if (any) a.occluded = reinterpret_cast<uint8_t*>(d_out);
+    else a.hits = reinterpret_cast<float4*>(d_out);
+    rc = launch_trace(ctx, a, intersector, any, false, s);
+    if (rc) return rc;
+    rc = check_cuda(ctx,
+        cudaMemcpyAsync(static_cast<char*>(out) + size_t(c0) * out_stride, d_out, size_t(cn) * out_stride,
+            cudaMemcpyDeviceToHost, s),
+        "result download");
+    if (rc) return rc;
+  }
+  rc = check_cuda(ctx, cudaStreamSynchronize(ctx->aux_stream), "sync");
+  if (rc) return rc;
+  return myrt_sync(ctx);
+}
+
+}  // namespace
+}  // namespace myrt_b200
+
+using namespace myrt_b200;
+
+struct myrt_bvh8_host {
+  myrt_b200::bvh8 tree;
+};
+
+namespace {
+void fill_info(myrt_b200::bvh8_stats const& st, size_t n_nodes, size_t n_tris, myrt_bvh_info* info) {
+  *info = myrt_bvh_info{};
+  info->triangles = st.triangles;
+  info->binary_nodes = st.binary_nodes;
+  info->wide_nodes = st.wide_nodes;
+  info->leaf_slots = st.leaf_slots;
+  info->binary_depth = st.binary_depth;
+  info->wide_depth = st.wide_depth;
+  info->max_leaf_size = st.max_leaf_size;
+  info->build_seconds = st.build_seconds;
+  info->node_bytes = n_nodes * sizeof(myrt_b200::bvh8_node);
+  info->triangle_bytes = n_tris * sizeof(myrt_b200::bvh8_triangle);
+}
+}  // namespace
+
+extern "C" {
+
+int myrt_bvh8_build(float const* positions, size_t n_tris, myrt_bvh8_host** out) {
+  if (!out || (!positions && n_tris)) return MYRT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  auto* h = new (std::nothrow) myrt_bvh8_host;
+  if (!h) return MYRT_ERR_OUT_OF_MEMORY;
+  try {
+    h->tree = build_bvh8(positions, n_tris, nullptr, bvh8_build_options{});
+  } catch (...) {
+    delete h;
+    return MYRT_ERR_INVALID_ARGUMENT;
+  }
+  *out = h;
+  return MYRT_OK;
+}
+
+int myrt_bvh8_get_info(myrt_bvh8_host const* h, myrt_bvh_info* info) {
+  if (!h || !info) return MYRT_ERR_INVALID_ARGUMENT;
+  fill_info(h->tree.stats, h->tree.nodes.size(), h->tree.triangles.size(), info);
+  return MYRT_OK;
+}
+
+int myrt_bvh8_copy(myrt_bvh8_host const* h, void* nodes, void* triangles) {
+  if (!h) return MYRT_ERR_INVALID_ARGUMENT;
+  if (nodes) std::memcpy(nodes, h->tree.nodes.data(), h->tree.nodes.size() * sizeof(bvh8_node));
+  if (triangles) std::memcpy(triangles, h->tree.triangles.data(), h->tree.triangles.size() * sizeof(bvh8_triangle));
+  return MYRT_OK;
+}
+
+int myrt_bvh8_free(myrt_bvh8_host* h) {
+  delete h;
+  return MYRT_OK;
+}
+
+int myrt_ctx_create(myrt_device_opts const* opts, myrt_ctx** out) {
+  if (!out) return MYRT_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  auto* ctx = new (std::nothrow) myrt_ctx;
+  if (!ctx) return MYRT_ERR_OUT_OF_MEMORY;
+  ctx->device = opts ? opts->device : 0;
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (!rc) rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
+  if (!rc) rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking), "stream");
+  if (!rc) rc = check_cuda(ctx, cudaMalloc(&ctx->d_err, sizeof(uint32_t)), "error word");
+  if (!rc) rc = check_cuda(ctx, cudaMemset(ctx->d_err, 0, sizeof(uint32_t)), "error word");
+  if (rc) {
+    myrt_ctx_destroy(ctx);
+    return rc;
+  }
+  *out = ctx;
+  return MYRT_OK;
+}
+
+int myrt_ctx_destroy(myrt_ctx* ctx) {
+  if (!ctx) return MYRT_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->aux_stream) cudaStreamSynchronize(ctx->aux_stream);
+  free_scene(ctx->scene);
+  for (auto& p : ctx->stage) cudaFree(p);
+  cudaFree(ctx->d_err);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
+  delete ctx;
+  return MYRT_OK;
+}
+
+int myrt_get_last_error(myrt_ctx* ctx, char* buf, size_t size) {
+  if (!ctx || !buf || size == 0) return MYRT_ERR_INVALID_ARGUMENT;
+  std::snprintf(buf, size, "%s", ctx->last_error.c_str());
+  return MYRT_OK;
+}
+
+int myrt_get_stream(myrt_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return MYRT_ERR_INVALID_ARGUMENT;
+  *stream = ctx->stream;
+  return MYRT_OK;
+}
+
+int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
+  if (!ctx || !v) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!v->indices || !v->vertices || v->index_count == 0 || v->vertex_count == 0 || v->index_count % 3 != 0)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "scene needs a non-empty index buffer (multiple of 3) and vertices");
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc) return rc;
+  cudaStreamSynchronize(ctx->stream);
+  free_scene(ctx->scene);
+
+  std::vector<myrt_drawable> drawables;
+  if (v->drawable_count == 0) {
+    myrt_drawable d{};
+    for (int k = 0; k < 4; ++k) d.transformation[k * 5] = d.inverse_transformation[k * 5] = 1.f;
+    d.index_count = uint32_t(v->index_count);
+    drawables.push_back(d);
+  } else {
+    if (!v->drawables) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "drawable_count > 0 but drawables is null");
+    drawables.assign(v->drawables, v->drawables + v->drawable_count);
+  }
+  size_t n_prims = 0;
+  for (auto const& d : drawables) {
+    if (d.index_count % 3 != 0 || size_t(d.indices_base_index) + d.index_count > v->index_count)
+      return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "drawable index range outside the index buffer");
+    n_prims += d.index_count / 3;
+  }
+  if (n_prims >= (size_t(1) << 31)) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "too many triangles");
+
+  std::vector<float> pos(9 * n_prims);
+  std::vector<float4> nrm(v->normals ? 3 * n_prims : 0);
+  std::vector<float2> uvs(v->uvs ? 3 * n_prims : 0);
+  std::vector<int32_t> mat(n_prims);
+  size_t p = 0;
+  for (auto const& d : drawables) {
+    bool const ident = is_identity(d.transformation);
+    // normal matrix = mat3(transpose(inverse_transformation)) (pt_trace.comp:372)
+    float nm[9];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) nm[c * 3 + r] = d.inverse_transformation[r * 4 + c];
+    for (uint32_t t = 0; t < d.index_count / 3; ++t, ++p) {
+      mat[p] = d.material_index;
+      for (int k = 0; k < 3; ++k) {
+        size_t const vi = size_t(d.points_base_index) + v->indices[d.indices_base_index + 3 * t + k];
+        if (vi >= v->vertex_count) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "vertex index out of range");
+        float const* src = v->vertices + 4 * vi;
+        float* dst = &pos[9 * p + 3 * k];
+        if (ident) std::memcpy(dst, src, 12);
+        else xform(d.transformation, src, 1.f, dst);
+        if (v->normals) {
+          float const* ns = v->normals + 4 * vi;
+          float n3[3];
+          if (ident) std::memcpy(n3, ns, 12);
+          else
+            for (int r = 0; r < 3; ++r) n3[r] = (nm[r] * ns[0] + nm[3 + r] * ns[1]) + nm[6 + r] * ns[2];
+          nrm[3 * p + k] = make_float4(n3[0], n3[1], n3[2], 0.f);
+        }
+        if (v->uvs) uvs[3 * p + k] = make_float2(v->uvs[2 * vi], v->uvs[2 * vi + 1]);
+      }
+    }
+  }
+
+  bvh8 tree;
+  try {
+    tree = build_bvh8(pos.data(), n_prims, nullptr, bvh8_build_options{});
+  } catch (std::exception const& e) {
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, std::string("bvh build: ") + e.what());
+  }
+  if (tree.stats.wide_depth > MYRT_STACK_MAX)
+    return set_error(ctx, MYRT_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
+
+  device_scene& s = ctx->scene;
+  s.stats = tree.stats;
+  s.n_nodes = tree.nodes.size();
+  s.n_tris = tree.triangles.size();
+  s.n_prims = n_prims;
+  rc = upload(ctx, reinterpret_cast<bvh8_node**>(&s.nodes), tree.nodes.data(), tree.nodes.size(), "node upload");
+  if (!rc)
+    rc = upload(ctx, reinterpret_cast<bvh8_triangle**>(&s.tris), tree.triangles.data(), tree.triangles.size(),
+        "triangle upload");
+  if (!rc && !nrm.empty()) rc = upload(ctx, &s.tri_normals, nrm.data(), nrm.size(), "normal upload");
+  if (!rc && !uvs.empty()) rc = upload(ctx, &s.tri_uvs, uvs.data(), uvs.size(), "uv upload");
+  if (!rc) rc = upload(ctx, &s.tri_material, mat.data(), mat.size(), "material index upload");
+  if (!rc && v->material_count) {
+    if (!v->materials) rc = set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "material_count > 0 but materials is null");
+    else rc = upload(ctx, &s.materials, v->materials, v->material_count, "material upload");
+    s.n_materials = v->material_count;
+  }
+  if (!rc && v->material_data_count) {
+    if (!v->material_data) rc = set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "material_data is null");
+    else rc = upload(ctx, &s.material_data, v->material_data, v->material_data_count, "material data upload");
+    s.n_material_data = v->material_data_count;
+  }
+  if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "scene upload");
+  if (rc) {
+    free_scene(s);
+    return rc;
+  }
+  s.valid = true;
+  return MYRT_OK;
+}
+
+int myrt_scene_bvh_info(myrt_ctx* ctx, myrt_bvh_info* info) {
+  if (!ctx || !info) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!ctx->scene.valid) return set_error(ctx, MYRT_ERR_NO_SCENE, "no scene uploaded");
+  fill_info(ctx->scene.stats, ctx->scene.n_nodes, ctx->scene.n_tris, info);
+  return MYRT_OK;
+}
+
+int myrt_trace_closest(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, myrt_hit* hits, int intersector) {
+  int rc = validate_query(ctx, rays, hits, intersector);
+  if (rc) return rc;
+  return host_query(ctx, rays, n, hits, sizeof(myrt_hit), intersector, false);
+}
+
+int myrt_trace_any(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, uint8_t* occluded, int intersector) {
+  int rc = validate_query(ctx, rays, occluded, intersector);
+  if (rc) return rc;
+  return host_query(ctx, rays, n, occluded, sizeof(uint8_t), intersector, true);
+}
+
+int myrt_trace_closest_device(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, myrt_hit* hits, int intersector,
+    void* stream) {
+  int rc = validate_query(ctx, rays, hits, intersector);
+  if (rc) return rc;
+  trace_args a = base_args(ctx);
+  a.rays = reinterpret_cast<float4 const*>(rays);
+  a.n = n;
+  a.hits = reinterpret_cast<float4*>(hits);
+  return launch_trace(ctx, a, intersector, false, false, stream ? static_cast<cudaStream_t>(stream) : ctx->stream);
+}
+
+int myrt_trace_any_device(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, uint8_t* occluded, int intersector,
+    void* stream) {
+  int rc = validate_query(ctx, rays, occluded, intersector);
+  if (rc) return rc;
+  trace_args a = base_args(ctx);
+  a.rays = reinterpret_cast<float4 const*>(rays);
+  a.n = n;
+  a.occluded = occluded;
+  return launch_trace(ctx, a, intersector, true, false, stream ? static_cast<cudaStream_t>(stream) : ctx->stream);
+}
+
+int myrt_trace_closest_stats_device(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, myrt_hit* hits, uint32_t* nodes,
+    uint32_t* tris, int intersector, void* stream) {
+  int rc = validate_query(ctx, rays, hits, intersector);
+  if (rc) return rc;
+  if (!nodes || !tris) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "null counter pointer");
+  trace_args a = base_args(ctx);
+  a.rays = reinterpret_cast<float4 const*>(rays);
+  a.n = n;
+  a.hits = reinterpret_cast<float4*>(hits);
+  a.stat_nodes = nodes;
+  a.stat_tris = tris;
+  return launch_trace(ctx, a, intersector, false, true, stream ? static_cast<cudaStream_t>(stream) : ctx->stream);
+}
+
+int myrt_sync(myrt_ctx* ctx) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  int rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "stream sync");
+  if (rc) return rc;
+  rc = check_cuda(ctx, cudaDeviceSynchronize(), "device sync");
+  if (rc) return rc;
+  uint32_t err = 0;
+  rc = check_cuda(ctx, cudaMemcpy(&err, ctx->d_err, sizeof(err), cudaMemcpyDeviceToHost), "error word");
+  if (rc) return rc;
+  if (err) {
+    cudaMemset(ctx->d_err, 0, sizeof(uint32_t));
+    char buf[96];
+    std::snprintf(buf, sizeof buf, "device abort, error bits 0x%08x", err);
+    return set_error(ctx, MYRT_ERR_DEVICE_ABORT, buf);
+  }
+  return MYRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,362 @@
+// Host BVH build: binned SAH -> 8-wide quantised tree. See bvh8.hpp.
+#include "bvh8.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <limits>
+#include <stdexcept>
+#include <thread>
+
+namespace myrt_b200 {
+namespace {
+
+struct box3 {
+  float lo[3] = {std::numeric_limits<float>::max(), std::numeric_limits<float>::max(),
+      std::numeric_limits<float>::max()};
+  float hi[3] = {std::numeric_limits<float>::lowest(), std::numeric_limits<float>::lowest(),
+      std::numeric_limits<float>::lowest()};
+  void grow(box3 const& b) {
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], b.lo[a]);
+      hi[a] = std::max(hi[a], b.hi[a]);
+    }
+  }
+  void grow(float const* p) {
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], p[a]);
+      hi[a] = std::max(hi[a], p[a]);
+    }
+  }
+  bool valid() const { return lo[0] <= hi[0] && lo[1] <= hi[1] && lo[2] <= hi[2]; }
+  // Same expression as aabb_t::surface_area (bvh.hpp:44-47).
+  float area() const {
+    if (!valid()) return 0.f;
+    float const dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return ((dx + dy) * dz + dx * dy) * 2.f;
+  }
+};
+
+struct bnode {
+  box3 box;
+  std::int32_t left = -1;   // child pair: left, left + 1 (internal) ; -1 for leaves
+  std::uint32_t begin = 0;  // leaf: prim range in `order`
+  std::uint32_t count = 0;
+};
+
+struct builder {
+  bvh8_build_options opt;
+  std::vector<box3> prim_box;
+  std::vector<float> prim_c;  // 3 per prim
+  std::vector<std::uint32_t> order;
+  std::vector<bnode> nodes;
+  std::atomic<std::uint32_t> node_count{1};
+  std::atomic<int> max_depth{0};
+  std::atomic<int> max_leaf{0};
+
+  void make_leaf(std::uint32_t ni, std::uint32_t b, std::uint32_t e, int depth) {
+    nodes[ni].left = -1;
+    nodes[ni].begin = b;
+    nodes[ni].count = e - b;
+    int d = max_depth.load();
+    while (depth > d && !max_depth.compare_exchange_weak(d, depth)) {
+    }
+    int m = max_leaf.load();
+    int const c = int(e - b);
+    while (c > m && !max_leaf.compare_exchange_weak(m, c)) {
+    }
+  }
+
+  // Builds the subtree for order[b, e) into node ni (its box already set).
+  void build(std::uint32_t ni, std::uint32_t b, std::uint32_t e, int depth) {
+    std::uint32_t const n = e - b;
+    if (n <= 1) return make_leaf(ni, b, e, depth);
+
+    box3 cb;
+    for (std::uint32_t i = b; i < e; ++i) cb.grow(&prim_c[3 * order[i]]);
+
+    int const bins = opt.bins;
+    float best_cost = std::numeric_limits<float>::max();
+    int best_axis = -1, best_bin = -1;
+    float const parent_area = nodes[ni].box.area();
+    std::vector<box3> bin_box(std::size_t(bins) * 3);
+    std::vector<std::uint32_t> bin_cnt(std::size_t(bins) * 3, 0);
+    float scale[3];
+    for (int a = 0; a < 3; ++a) {
+      float const ext = cb.hi[a] - cb.lo[a];
+      scale[a] = ext > 0.f ? float(bins) / ext : 0.f;
+    }
+    for (std::uint32_t i = b; i < e; ++i) {
+      std::uint32_t const p = order[i];
+      for (int a = 0; a < 3; ++a) {
+        if (scale[a] == 0.f) continue;
+        int k = int((prim_c[3 * p + a] - cb.lo[a]) * scale[a]);
+        k = std::clamp(k, 0, bins - 1);
+        bin_box[std::size_t(a) * bins + k].grow(prim_box[p]);
+        bin_cnt[std::size_t(a) * bins + k]++;
+      }
+    }
+    std::vector<float> right_area(bins);
+    std::vector<std::uint32_t> right_cnt(bins);
+    for (int a = 0; a < 3; ++a) {
+      if (scale[a] == 0.f) continue;
+      box3 acc;
+      std::uint32_t cnt = 0;
+      for (int k = bins - 1; k > 0; --k) {
+        acc.grow(bin_box[std::size_t(a) * bins + k]);
+        cnt += bin_cnt[std::size_t(a) * bins + k];
+        right_area[k] = acc.area();
+        right_cnt[k] = cnt;
+      }
+      box3 lacc;
+      std::uint32_t lcnt = 0;
+      for (int k = 0; k < bins - 1; ++k) {
+        lacc.grow(bin_box[std::size_t(a) * bins + k]);
+        lcnt += bin_cnt[std::size_t(a) * bins + k];
+        std::uint32_t const rcnt = right_cnt[k + 1];
+        if (lcnt == 0 || rcnt == 0) continue;
+        float const cost = opt.cost_traverse +
+            opt.cost_intersect * (float(lcnt) * lacc.area() + float(rcnt) * right_area[k + 1]) /
+                std::max(parent_area, 1e-30f);
+        if (cost < best_cost) {
+          best_cost = cost;
+          best_axis = a;
+          best_bin = k;
+        }
+      }
+    }
+    float const leaf_cost = opt.cost_intersect * float(n);
+    if (n <= std::uint32_t(opt.max_leaf) && (best_axis < 0 || best_cost >= leaf_cost))
+      return make_leaf(ni, b, e, depth);
+
+    std::uint32_t mid;
+    if (best_axis < 0) {
+      mid = b + n / 2;  // all centroids coincide: split the range in half
+    } else {
+      float const lo = cb.lo[best_axis], sc = scale[best_axis];
+      auto it = std::partition(order.begin() + b, order.begin() + e, [&](std::uint32_t p) {
+        int k = std::clamp(int((prim_c[3 * p + best_axis] - lo) * sc), 0, bins - 1);
+        return k <= best_bin;
+      });
+      mid = std::uint32_t(it - order.begin());
+      if (mid == b || mid == e) mid = b + n / 2;
+    }
+
+    std::uint32_t const l = node_count.fetch_add(2);
+    nodes[ni].left = std::int32_t(l);
+    nodes[ni].count = 0;
+    box3 lb, rb;
+    for (std::uint32_t i = b; i < mid; ++i) lb.grow(prim_box[order[i]]);
+    for (std::uint32_t i = mid; i < e; ++i) rb.grow(prim_box[order[i]]);
+    nodes[l].box = lb;
+    nodes[l + 1].box = rb;
+    if (n > 65536 && depth < 6) {
+      auto fut = std::async(std::launch::async, [&] { build(l, b, mid, depth + 1); });
+      build(l + 1, mid, e, depth + 1);
+      fut.get();
+    } else {
+      build(l, b, mid, depth + 1);
+      build(l + 1, mid, e, depth + 1);
+    }
+  }
+};
+
+std::uint8_t biased_exponent_for(float extent) {
+  // Smallest e with extent / 2^e <= 255.
+  if (!(extent > 0.f)) return std::uint8_t(127 - 100);
+  int e = int(std::ceil(std::log2(double(extent) / 255.0)));
+  while (std::ldexp(255.0, e) < double(extent)) ++e;
+  e = std::clamp(e, -126, 127);
+  return std::uint8_t(e + 127);
+}
+
+}  // namespace
+
+bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const* prim_ids,
+    bvh8_build_options const& opt) {
+  auto const t0 = std::chrono::steady_clock::now();
+  bvh8 out;
+  if (n_tris == 0) return out;
+  if (n_tris >= (std::size_t(1) << 31)) throw std::runtime_error("too many triangles for one BVH");
+  if (opt.max_leaf < 1 || opt.max_leaf > 4) throw std::runtime_error("max_leaf must be in [1, 4]");
+
+  builder bld;
+  bld.opt = opt;
+  bld.prim_box.resize(n_tris);
+  bld.prim_c.resize(3 * n_tris);
+  bld.order.resize(n_tris);
+  box3 scene;
+  for (std::size_t i = 0; i < n_tris; ++i) {
+    float const* v = positions + 9 * i;
+    box3& bx = bld.prim_box[i];
+    bx.grow(v);
+    bx.grow(v + 3);
+    bx.grow(v + 6);
+    for (int a = 0; a < 3; ++a) {
+      bx.lo[a] -= opt.box_padding;
+      bx.hi[a] += opt.box_padding;
+      bld.prim_c[3 * i + a] = (v[a] + v[3 + a] + v[6 + a]) / 3.0f;
+    }
+    scene.grow(bx);
+    bld.order[i] = std::uint32_t(i);
+  }
+  bld.nodes.resize(2 * n_tris);
+  bld.nodes[0].box = scene;
+  bld.build(0, 0, std::uint32_t(n_tris), 0);
+  std::uint32_t const nb = bld.node_count.load();
+  for (int a = 0; a < 3; ++a) {
+    out.scene_lo[a] = scene.lo[a];
+    out.scene_hi[a] = scene.hi[a];
+  }
+
+  // ---- collapse to the 8-wide layout, breadth first ----
+  auto const& bn = bld.nodes;
+  struct item {
+    std::uint32_t bnode;
+    int depth;
+  };
+  std::vector<item> queue;
+  queue.push_back({0, 1});
+  out.nodes.resize(1);
+  out.triangles.reserve(n_tris);
+  int wide_depth = 0;
+  std::size_t leaf_slots = 0;
+  for (std::size_t qi = 0; qi < queue.size(); ++qi) {
+    item const it = queue[qi];
+    wide_depth = std::max(wide_depth, it.depth);
+    std::uint32_t kids[8];
+    int nk = 0;
+    if (bn[it.bnode].left < 0) {
+      kids[nk++] = it.bnode;  // a lone leaf (tiny scenes): one leaf slot
+    } else {
+      kids[nk++] = std::uint32_t(bn[it.bnode].left);
+      kids[nk++] = std::uint32_t(bn[it.bnode].left + 1);
+      while (nk < 8) {
+        int pick = -1;
+        float best = -1.f;
+        for (int k = 0; k < nk; ++k) {
+          if (bn[kids[k]].left < 0) continue;
+          float const a = bn[kids[k]].box.area();
+          if (a > best) {
+            best = a;
+            pick = k;
+          }
+        }
+        if (pick < 0) break;
+        std::uint32_t const c = kids[pick];
+        kids[pick] = std::uint32_t(bn[c].left);
+        kids[nk++] = std::uint32_t(bn[c].left + 1);
+      }
+    }
+
+    box3 nbox;
+    for (int k = 0; k < nk; ++k) nbox.grow(bn[kids[k]].box);
+    float const cx = 0.5f * (nbox.lo[0] + nbox.hi[0]), cy = 0.5f * (nbox.lo[1] + nbox.hi[1]),
+                cz = 0.5f * (nbox.lo[2] + nbox.hi[2]);
+
+    // Octant slot assignment: slot s faces direction (+-1,+-1,+-1) with bit a of
+    // s set meaning +; the child lying furthest that way takes the slot.
+    int slot_of[8];
+    {
+      bool kid_done[8] = {}, slot_done[8] = {};
+      float cost[8][8];
+      for (int k = 0; k < nk; ++k) {
+        float const dx = 0.5f * (bn[kids[k]].box.lo[0] + bn[kids[k]].box.hi[0]) - cx;
+        float const dy = 0.5f * (bn[kids[k]].box.lo[1] + bn[kids[k]].box.hi[1]) - cy;
+        float const dz = 0.5f * (bn[kids[k]].box.lo[2] + bn[kids[k]].box.hi[2]) - cz;
+        for (int s = 0; s < 8; ++s)
+          cost[k][s] = ((s & 1) ? dx : -dx) + ((s & 2) ? dy : -dy) + ((s & 4) ? dz : -dz);
+      }
+      for (int r = 0; r < nk; ++r) {
+        int bk = -1, bs = -1;
+        float bc = -std::numeric_limits<float>::max();
+        for (int k = 0; k < nk; ++k) {
+          if (kid_done[k]) continue;
+          for (int s = 0; s < 8; ++s) {
+            if (slot_done[s]) continue;
+            if (cost[k][s] > bc) {
+              bc = cost[k][s];
+              bk = k;
+              bs = s;
+            }
+          }
+        }
+        kid_done[bk] = slot_done[bs] = true;
+        slot_of[bk] = bs;
+      }
+    }
+    std::int32_t slot_kid[8];
+    for (int s = 0; s < 8; ++s) slot_kid[s] = -1;
+    for (int k = 0; k < nk; ++k) slot_kid[slot_of[k]] = std::int32_t(kids[k]);
+
+    bvh8_node node{};
+    node.px = nbox.lo[0];
+    node.py = nbox.lo[1];
+    node.pz = nbox.lo[2];
+    double scale[3];
+    for (int a = 0; a < 3; ++a) {
+      node.e[a] = biased_exponent_for(nbox.hi[a] - nbox.lo[a]);
+      scale[a] = std::ldexp(1.0, int(node.e[a]) - 127);
+    }
+    float const p[3] = {node.px, node.py, node.pz};
+    node.child_base = std::uint32_t(out.nodes.size());
+    node.tri_base = std::uint32_t(out.triangles.size());
+    std::uint32_t tri_off = 0;
+    for (int s = 0; s < 8; ++s) {
+      if (slot_kid[s] < 0) {
+        for (int a = 0; a < 3; ++a) {
+          node.qlo[a][s] = 1;
+          node.qhi[a][s] = 0;
+        }
+        node.meta[s] = 0;
+        continue;
+      }
+      bnode const& c = bn[std::uint32_t(slot_kid[s])];
+      for (int a = 0; a < 3; ++a) {
+        double const lo = std::floor((double(c.box.lo[a]) - double(p[a])) / scale[a]);
+        double const hi = std::ceil((double(c.box.hi[a]) - double(p[a])) / scale[a]);
+        node.qlo[a][s] = std::uint8_t(std::clamp(lo, 0.0, 255.0));
+        node.qhi[a][s] = std::uint8_t(std::clamp(hi, 0.0, 255.0));
+      }
+      if (c.left >= 0) {
+        node.imask |= std::uint8_t(1u << s);
+        node.meta[s] = std::uint8_t(0x20u | unsigned(s));
+        out.nodes.emplace_back();
+        queue.push_back({std::uint32_t(slot_kid[s]), it.depth + 1});
+      } else {
+        node.meta[s] = std::uint8_t(tri_off | (c.count << 5));
+        for (std::uint32_t i = 0; i < c.count; ++i) {
+          std::uint32_t const prim = bld.order[c.begin + i];
+          float const* v = positions + 9 * std::size_t(prim);
+          bvh8_triangle t{};
+          std::memcpy(t.v0, v, 12);
+          std::memcpy(t.v1, v + 3, 12);
+          std::memcpy(t.v2, v + 6, 12);
+          t.prim = prim_ids ? prim_ids[prim] : prim;
+          out.triangles.push_back(t);
+        }
+        tri_off += c.count;
+        ++leaf_slots;
+      }
+    }
+    out.nodes[qi] = node;
+  }
+  // The queue index equals the wide-node index: children are appended in the
+  // same order as they are queued.
+
+  auto const t1 = std::chrono::steady_clock::now();
+  out.stats.binary_nodes = nb;
+  out.stats.wide_nodes = out.nodes.size();
+  out.stats.leaf_slots = leaf_slots;
+  out.stats.triangles = out.triangles.size();
+  out.stats.binary_depth = bld.max_depth.load();
+  out.stats.wide_depth = wide_depth;
+  out.stats.max_leaf_size = bld.max_leaf.load();
+  out.stats.build_seconds = std::chrono::duration<double>(t1 - t0).count();
+  return out;
+}
+
+}  // namespace myrt_b200

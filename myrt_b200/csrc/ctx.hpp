@@ -1,0 +1,47 @@
+// Context state shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/myrt_cuda.h"
+#include "bvh8.hpp"
+
+namespace myrt_b200 {
+
+// Device-resident scene: BVH, pre-gathered triangles and the shading buffers.
+struct device_scene {
+  uint4* nodes = nullptr;      // 5 uint4 per wide node
+  float4* tris = nullptr;      // 3 float4 per triangle reference (leaf order)
+  // Shading attributes per baked triangle (prim id order): world-space
+  // shading normals at the 3 corners, uvs, material index.
+  float4* tri_normals = nullptr;  // 3 float4 per prim
+  float2* tri_uvs = nullptr;      // 3 float2 per prim
+  int32_t* tri_material = nullptr;
+  myrt_material_ref* materials = nullptr;
+  float* material_data = nullptr;
+  size_t n_nodes = 0, n_tris = 0, n_prims = 0, n_materials = 0, n_material_data = 0;
+  bvh8_stats stats{};
+  bool valid = false;
+};
+
+}  // namespace myrt_b200
+
+struct myrt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t aux_stream = nullptr;  // second lane for copy/compute overlap
+  std::string last_error;
+  uint32_t* d_err = nullptr;          // device error word (atomicOr of ERR_* bits)
+  myrt_b200::device_scene scene;
+  // staging buffers of the host-memory entry points (two chunk slots)
+  void* stage[2] = {nullptr, nullptr};
+  size_t stage_bytes = 0;
+};
+
+namespace myrt_b200 {
+int set_error(myrt_ctx* ctx, int code, std::string msg);
+int check_cuda(myrt_ctx* ctx, cudaError_t e, char const* what);
+}  // namespace myrt_b200

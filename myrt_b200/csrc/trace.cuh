@@ -1,0 +1,281 @@
+// Closest-hit / any-hit traversal of the 8-wide quantised BVH (bvh8.hpp).
+//
+// One thread per ray. A node is five 16-byte words fetched with 128-bit
+// read-only loads; all eight child boxes are tested from registers; hit
+// internal children form a "node group" (child_base, hit bits << 24 | imask)
+// and hit leaf slots a "triangle group" (tri_base, 32-bit triangle mask).
+// The stack holds node groups only; at most one per tree level, so its depth
+// is bounded by the tree depth checked at upload (MYRT_STACK_MAX).
+//
+// Triangle tests are bit-exact restatements of the reference's
+// Moller-Trumbore (src/pt/intersect.glsl:3-28) using explicitly rounded
+// intrinsics (no FMA contraction, IEEE division), or the watertight test of
+// Woop, Benthin and Wald (JCGT 2013). Closest hit keeps the smallest t, ties
+// going to the smaller prim id, so the answer does not depend on the order in
+// which the tree is walked (the reference keeps the first visited,
+// src/pt/pt_trace.comp:267-269).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace myrt_b200 {
+
+constexpr int MYRT_STACK_MAX = 32;
+
+enum : uint32_t {
+  ERR_STACK_OVERFLOW = 1u << 0,
+};
+
+// ---- exact-rounding vector helpers (no contraction) ----------------------
+struct f3 {
+  float x, y, z;
+};
+__device__ __forceinline__ f3 sub3(f3 a, f3 b) { return {__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)}; }
+__device__ __forceinline__ float dot3(f3 a, f3 b) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ f3 cross3(f3 a, f3 b) {
+  return {__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+      __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x))};
+}
+
+// src/pt/intersect.glsl:3-28, operation for operation.
+__device__ __forceinline__ bool isect_reference(f3 o, f3 d, f3 v1, f3 v2, f3 v3, float& t, float& u, float& v) {
+  const float float_epsilon = 1e-23f;
+  const float border_epsilon = 1e-6f;
+  f3 const e1 = sub3(v2, v1);
+  f3 const e2 = sub3(v3, v1);
+  f3 const P = cross3(d, e2);
+  float const det = dot3(e1, P);
+  if (det > -float_epsilon && det < float_epsilon) return false;
+  float const inv_det = __fdiv_rn(1.0f, det);
+  f3 const T = sub3(o, v1);
+  u = __fmul_rn(dot3(T, P), inv_det);
+  if (u < -border_epsilon || u > __fadd_rn(1.0f, border_epsilon)) return false;
+  f3 const Q = cross3(T, e1);
+  v = __fmul_rn(dot3(d, Q), inv_det);
+  if (v < -border_epsilon || __fadd_rn(u, v) > __fadd_rn(1.0f, border_epsilon)) return false;
+  float const tt = __fmul_rn(dot3(e2, Q), inv_det);
+  if (tt > float_epsilon) {
+    t = tt;
+    return true;
+  }
+  return false;
+}
+
+// Watertight ray/triangle test (Woop, Benthin, Wald, JCGT 2(1), 2013),
+// precomputed per ray: kx, ky, kz and the shear Sx, Sy, Sz.
+struct wt_ray {
+  int kx, ky, kz;
+  float Sx, Sy, Sz;
+};
+__device__ __forceinline__ float comp(f3 a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
+__device__ __forceinline__ wt_ray wt_setup(f3 d) {
+  wt_ray w;
+  float const ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  w.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  w.kx = w.kz + 1 == 3 ? 0 : w.kz + 1;
+  w.ky = w.kx + 1 == 3 ? 0 : w.kx + 1;
+  if (comp(d, w.kz) < 0.0f) {
+    int const tmp = w.kx;
+    w.kx = w.ky;
+    w.ky = tmp;
+  }
+  float const dz = comp(d, w.kz);
+  w.Sx = __fdiv_rn(comp(d, w.kx), dz);
+  w.Sy = __fdiv_rn(comp(d, w.ky), dz);
+  w.Sz = __fdiv_rn(1.0f, dz);
+  return w;
+}
+__device__ __forceinline__ bool isect_watertight(
+    wt_ray const& w, f3 o, f3 v0, f3 v1, f3 v2, float tmin, float& t, float& u, float& v) {
+  f3 const A = sub3(v0, o), B = sub3(v1, o), C = sub3(v2, o);
+  float const Az0 = comp(A, w.kz), Bz0 = comp(B, w.kz), Cz0 = comp(C, w.kz);
+  float const Ax = __fsub_rn(comp(A, w.kx), __fmul_rn(w.Sx, Az0));
+  float const Ay = __fsub_rn(comp(A, w.ky), __fmul_rn(w.Sy, Az0));
+  float const Bx = __fsub_rn(comp(B, w.kx), __fmul_rn(w.Sx, Bz0));
+  float const By = __fsub_rn(comp(B, w.ky), __fmul_rn(w.Sy, Bz0));
+  float const Cx = __fsub_rn(comp(C, w.kx), __fmul_rn(w.Sx, Cz0));
+  float const Cy = __fsub_rn(comp(C, w.ky), __fmul_rn(w.Sy, Cz0));
+  float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+  float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+  float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    U = float(__dsub_rn(__dmul_rn(double(Cx), double(By)), __dmul_rn(double(Cy), double(Bx))));
+    V = float(__dsub_rn(__dmul_rn(double(Ax), double(Cy)), __dmul_rn(double(Ay), double(Cx))));
+    W = float(__dsub_rn(__dmul_rn(double(Bx), double(Ay)), __dmul_rn(double(By), double(Ax))));
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+  float const det = __fadd_rn(__fadd_rn(U, V), W);
+  if (det == 0.0f) return false;
+  float const Az = __fmul_rn(w.Sz, Az0), Bz = __fmul_rn(w.Sz, Bz0), Cz = __fmul_rn(w.Sz, Cz0);
+  float const T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+  float const rcp = __fdiv_rn(1.0f, det);
+  float const tt = __fmul_rn(T, rcp);
+  if (!(tt > 0.0f) || tt < tmin) return false;
+  t = tt;
+  u = __fmul_rn(V, rcp);
+  v = __fmul_rn(W, rcp);
+  return true;
+}
+
+// ---- traversal ------------------------------------------------------------
+struct trace_args {
+  const float4* rays;  // 2 float4 per ray: (o, tmin), (d, tmax)
+  uint32_t n;
+  const uint4* nodes;  // 5 uint4 per node
+  const float4* tris;  // 3 float4 per triangle
+  float4* hits;        // closest: (prim bits, t, u, v)
+  uint8_t* occluded;   // any-hit output
+  uint32_t* stat_nodes;
+  uint32_t* stat_tris;
+  uint32_t* err;
+};
+
+__device__ __forceinline__ float q8(uint32_t w, int s) { return float((w >> (8 * (s & 3))) & 0xffu); }
+
+template <int ISECT, bool ANY, bool STATS>
+__device__ __forceinline__ void trace_one(trace_args const& a, uint32_t i) {
+  float4 const r0 = __ldg(a.rays + 2 * size_t(i));
+  float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
+  f3 const o{r0.x, r0.y, r0.z};
+  f3 const d{r1.x, r1.y, r1.z};
+  float const tmin = r0.w;
+  float const tmax = r1.w;
+
+  // Box-test reciprocal: zero components are nudged so no 0 * inf appears.
+  float const idx = 1.0f / (fabsf(d.x) > 1e-20f ? d.x : copysignf(1e-20f, d.x));
+  float const idy = 1.0f / (fabsf(d.y) > 1e-20f ? d.y : copysignf(1e-20f, d.y));
+  float const idz = 1.0f / (fabsf(d.z) > 1e-20f ? d.z : copysignf(1e-20f, d.z));
+  uint32_t const oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+  uint32_t const octinv = oct ^ 7u;
+  wt_ray wt{};
+  if (ISECT == 1) wt = wt_setup(d);
+
+  float tbest = tmax;
+  int32_t best = -1;
+  float bu = 0.f, bv = 0.f;
+  uint32_t n_nodes = 0, n_tris = 0;
+  bool occluded = false;
+
+  uint2 stack[MYRT_STACK_MAX];
+  int sp = 0;
+  uint2 group = make_uint2(0u, 0x80000000u);  // root: bit of slot 7 ^ octinv, imask 0 -> node 0
+
+  while (true) {
+    uint2 tgroup = make_uint2(0u, 0u);
+    if (group.y & 0xff000000u) {
+      uint32_t const pos = 31u - __clz(group.y & 0xff000000u);
+      group.y &= ~(1u << pos);
+      uint32_t const slot = (pos - 24u) ^ octinv;
+      uint32_t const node_idx = group.x + __popc(group.y & 0xffu & ((1u << slot) - 1u));
+      if (group.y & 0xff000000u) {
+        if (sp >= MYRT_STACK_MAX) {
+          atomicOr(a.err, ERR_STACK_OVERFLOW);
+          break;
+        }
+        stack[sp++] = group;
+      }
+      uint4 const* np = a.nodes + 5 * size_t(node_idx);
+      uint4 const w0 = __ldg(np + 0);
+      uint4 const w1 = __ldg(np + 1);
+      uint4 const w2 = __ldg(np + 2);
+      uint4 const w3 = __ldg(np + 3);
+      uint4 const w4 = __ldg(np + 4);
+      if (STATS) ++n_nodes;
+      float const sx = __uint_as_float((w0.w & 0xffu) << 23) * idx;
+      float const sy = __uint_as_float(((w0.w >> 8) & 0xffu) << 23) * idy;
+      float const sz = __uint_as_float(((w0.w >> 16) & 0xffu) << 23) * idz;
+      float const ox = (__uint_as_float(w0.x) - o.x) * idx;
+      float const oy = (__uint_as_float(w0.y) - o.y) * idy;
+      float const oz = (__uint_as_float(w0.z) - o.z) * idz;
+      uint32_t const imask = w0.w >> 24;
+      // near/far quantised planes per axis, swapped for negative directions
+      uint32_t const nx0 = idx >= 0.f ? w2.x : w3.z, nx1 = idx >= 0.f ? w2.y : w3.w;
+      uint32_t const fx0 = idx >= 0.f ? w3.z : w2.x, fx1 = idx >= 0.f ? w3.w : w2.y;
+      uint32_t const ny0 = idy >= 0.f ? w2.z : w4.x, ny1 = idy >= 0.f ? w2.w : w4.y;
+      uint32_t const fy0 = idy >= 0.f ? w4.x : w2.z, fy1 = idy >= 0.f ? w4.y : w2.w;
+      uint32_t const nz0 = idz >= 0.f ? w3.x : w4.z, nz1 = idz >= 0.f ? w3.y : w4.w;
+      uint32_t const fz0 = idz >= 0.f ? w4.z : w3.x, fz1 = idz >= 0.f ? w4.w : w3.y;
+      uint32_t hit_internal = 0, hit_tris = 0;
+#pragma unroll
+      for (int s = 0; s < 8; ++s) {
+        uint32_t const nxw = s < 4 ? nx0 : nx1, fxw = s < 4 ? fx0 : fx1;
+        uint32_t const nyw = s < 4 ? ny0 : ny1, fyw = s < 4 ? fy0 : fy1;
+        uint32_t const nzw = s < 4 ? nz0 : nz1, fzw = s < 4 ? fz0 : fz1;
+        float const tnx = fmaf(q8(nxw, s), sx, ox), tfx = fmaf(q8(fxw, s), sx, ox);
+        float const tny = fmaf(q8(nyw, s), sy, oy), tfy = fmaf(q8(fyw, s), sy, oy);
+        float const tnz = fmaf(q8(nzw, s), sz, oz), tfz = fmaf(q8(fzw, s), sz, oz);
+        float const tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
+        float const tf = fminf(fminf(tfx, tfy), fminf(tfz, tbest));
+        uint32_t const meta = ((s < 4 ? w1.z : w1.w) >> (8 * (s & 3))) & 0xffu;
+        if (meta != 0u && tn <= tf * 1.00000024f) {
+          if (imask & (1u << s)) {
+            hit_internal |= 1u << ((s ^ octinv) + 24u);
+          } else {
+            uint32_t const cnt = meta >> 5, off = meta & 31u;
+            hit_tris |= ((1u << cnt) - 1u) << off;
+          }
+        }
+      }
+      group = make_uint2(w1.x, hit_internal | imask);
+      tgroup = make_uint2(w1.y, hit_tris);
+    } else {
+      group.y = 0;
+    }
+
+    while (tgroup.y) {
+      uint32_t const b = __ffs(tgroup.y) - 1u;
+      tgroup.y &= tgroup.y - 1u;
+      float4 const* tp = a.tris + 3 * size_t(tgroup.x + b);
+      float4 const p0 = __ldg(tp + 0);
+      float4 const p1 = __ldg(tp + 1);
+      float4 const p2 = __ldg(tp + 2);
+      if (STATS) ++n_tris;
+      float t, u, v;
+      bool h;
+      if (ISECT == 0)
+        h = isect_reference(o, d, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, t, u, v) &&
+            t >= tmin;
+      else
+        h = isect_watertight(wt, o, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, tmin, t, u, v);
+      if (!h) continue;
+      int32_t const prim = __float_as_int(p0.w);
+      if (ANY) {
+        if (t < tmax) {
+          occluded = true;
+          break;
+        }
+      } else if (t < tbest || (t == tbest && best >= 0 && prim < best)) {
+        tbest = t;
+        best = prim;
+        bu = u;
+        bv = v;
+      }
+    }
+    if (ANY && occluded) break;
+    if (!(group.y & 0xff000000u)) {
+      if (sp == 0) break;
+      group = stack[--sp];
+    }
+  }
+
+  if (ANY) {
+    a.occluded[i] = occluded ? 1 : 0;
+  } else {
+    a.hits[i] = make_float4(__int_as_float(best), best >= 0 ? tbest : tmax, best >= 0 ? bu : 0.f, best >= 0 ? bv : 0.f);
+  }
+  if (STATS) {
+    a.stat_nodes[i] = n_nodes;
+    a.stat_tris[i] = n_tris;
+  }
+}
+
+template <int ISECT, bool ANY, bool STATS>
+__global__ void __launch_bounds__(128) k_trace(trace_args a) {
+  uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n) return;
+  trace_one<ISECT, ANY, STATS>(a, i);
+}
+
+}  // namespace myrt_b200

@@ -1,0 +1,173 @@
+"""Seeded synthetic scenes and ray sets for the benchmark configurations.
+
+All inputs are synthetic: no dataset or asset is read. Geometry is float32,
+built in float64 and rounded once, so every machine produces identical bits.
+
+* ``heightfield``  -- N x N cell grid on [-1,1]^2 in xz, vertex y ~ U[0, amp),
+  two triangles per cell (the 128 x 128 / 32,768-triangle closest-hit case).
+* ``icosphere_field`` -- random icospheres plus a tessellated floor quad (the
+  655,872-triangle path-tracing case).
+* ``pinhole_rays`` -- one ray per pixel centre of a pinhole camera.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def heightfield(n: int = 128, amp: float = 0.1, seed: int = 1):
+    """Return (indices uint32[3T], points float32[V,3]) for an n x n cell grid."""
+    rng = np.random.default_rng(seed)
+    xs = np.linspace(-1.0, 1.0, n + 1)
+    gx, gz = np.meshgrid(xs, xs, indexing="xy")
+    gy = rng.uniform(0.0, amp, size=gx.shape)
+    pts = np.stack([gx.ravel(), gy.ravel(), gz.ravel()], axis=1).astype(np.float32)
+    i, j = np.meshgrid(np.arange(n), np.arange(n), indexing="xy")
+    v00 = (j * (n + 1) + i).ravel()
+    v10 = v00 + 1
+    v01 = v00 + (n + 1)
+    v11 = v01 + 1
+    tris = np.stack([np.stack([v00, v01, v10], 1), np.stack([v10, v01, v11], 1)], axis=1).reshape(-1, 3)
+    return tris.astype(np.uint32).ravel(), pts
+
+
+def pinhole_rays(width: int, height: int, eye=(0.0, 2.0, -3.0), target=(0.0, 0.0, 0.0), up=(0.0, 1.0, 0.0),
+                 vfov_deg: float = 60.0, jitter: np.ndarray | None = None) -> np.ndarray:
+    """Rays through pixel centres (row-major, y down), as float32[n, 8]:
+    origin xyz, tmin (0), direction xyz (unit), tmax (+inf)."""
+    eye = np.asarray(eye, np.float64)
+    fwd = np.asarray(target, np.float64) - eye
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, np.asarray(up, np.float64))
+    right /= np.linalg.norm(right)
+    upv = np.cross(right, fwd)
+    tan_half = np.tan(np.radians(vfov_deg) * 0.5)
+    aspect = width / height
+    px, py = np.meshgrid(np.arange(width, dtype=np.float64), np.arange(height, dtype=np.float64), indexing="xy")
+    px = px.ravel() + 0.5
+    py = py.ravel() + 0.5
+    if jitter is not None:
+        px = px + jitter[:, 0]
+        py = py + jitter[:, 1]
+    sx = (2.0 * px / width - 1.0) * tan_half * aspect
+    sy = (1.0 - 2.0 * py / height) * tan_half
+    d = fwd[None, :] + sx[:, None] * right[None, :] + sy[:, None] * upv[None, :]
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.empty((d.shape[0], 8), np.float32)
+    rays[:, 0:3] = eye
+    rays[:, 3] = 0.0
+    rays[:, 4:7] = d
+    rays[:, 7] = np.inf
+    return rays
+
+
+def icosphere(subdiv: int = 3):
+    """Unit icosphere: (indices uint32[3T], points float32[V,3]); 20 * 4**subdiv triangles."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    verts = [np.array(p, np.float64) / np.linalg.norm(p) for p in v]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    for _ in range(subdiv):
+        cache = {}
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.asarray(faces, np.uint32).ravel(), np.asarray(verts, np.float64).astype(np.float32)
+
+
+def pack_unorm4x8(rgba) -> np.uint32:
+    c = np.clip(np.asarray(rgba, np.float64), 0.0, 1.0)
+    b = np.rint(c * 255.0).astype(np.uint32)
+    return np.uint32(b[0] | (b[1] << 8) | (b[2] << 16) | (b[3] << 24))
+
+
+def pbr_material(albedo, ior=1.5, roughness=0.5, metallic=0.0, transmission=0.0) -> np.ndarray:
+    """The reference app's 7-float PBR record (src/main.cpp:447-464): albedo as
+    vec4unorm8 bits, ior, roughness, metallic, transmission, albedo texture (0, 0)."""
+    rec = np.zeros(7, np.float32)
+    rec[0] = pack_unorm4x8([*albedo, 1.0]).view(np.float32)
+    rec[1:5] = ior, roughness, metallic, transmission
+    return rec
+
+
+def _affine(scale: float, t) -> tuple[np.ndarray, np.ndarray]:
+    m = np.zeros(16, np.float32)
+    m[0] = m[5] = m[10] = scale
+    m[12:15] = t
+    m[15] = 1.0
+    inv = np.zeros(16, np.float32)
+    inv[0] = inv[5] = inv[10] = 1.0 / scale
+    inv[12:15] = -np.asarray(t, np.float64) / scale
+    inv[15] = 1.0
+    return m, inv
+
+
+def icosphere_field(n_spheres: int = 512, subdiv: int = 3, floor_cells: int = 16, seed: int = 2):
+    """Random icospheres (radius log-uniform [0.02, 0.2], centres U[-1,1]^3) plus
+    a floor quad at y = -1.2 tessellated into 2 * floor_cells^2 triangles, as
+    instanced drawables with one material each (GGX roughness U[0.05, 1],
+    albedo U[0.2, 0.9]^3, metallic Bernoulli(0.3)). Default: 512 * 1280 + 512
+    = 655,872 triangles. Returns a dict of Context.upload_scene arguments."""
+    from ._abi import myrt_drawable
+
+    rng = np.random.default_rng(seed)
+    si, sp = icosphere(subdiv)
+    # floor: unit grid on [-3,3]^2 at y = -1.2
+    g = np.linspace(-3.0, 3.0, floor_cells + 1)
+    gx, gz = np.meshgrid(g, g, indexing="xy")
+    fp = np.stack([gx.ravel(), np.full(gx.size, -1.2), gz.ravel()], 1).astype(np.float32)
+    i, j = np.meshgrid(np.arange(floor_cells), np.arange(floor_cells), indexing="xy")
+    v00 = (j * (floor_cells + 1) + i).ravel()
+    fi = np.stack([np.stack([v00, v00 + floor_cells + 1, v00 + 1], 1),
+                   np.stack([v00 + 1, v00 + floor_cells + 1, v00 + floor_cells + 2], 1)], 1).reshape(-1)
+    indices = np.concatenate([si, fi.astype(np.uint32)])
+    vertices = np.concatenate([sp, fp]).astype(np.float32)
+    normals = np.concatenate([sp, np.tile(np.array([[0.0, 1.0, 0.0]], np.float32), (fp.shape[0], 1))])
+    radius = np.exp(rng.uniform(np.log(0.02), np.log(0.2), n_spheres))
+    centre = rng.uniform(-1.0, 1.0, (n_spheres, 3))
+    rough = rng.uniform(0.05, 1.0, n_spheres)
+    albedo = rng.uniform(0.2, 0.9, (n_spheres, 3))
+    metal = (rng.uniform(0.0, 1.0, n_spheres) < 0.3).astype(np.float32)
+    drawables = (myrt_drawable * (n_spheres + 1))()
+    mat_data = [pbr_material([0.6, 0.6, 0.6], roughness=0.8)]
+    for k in range(n_spheres):
+        m, inv = _affine(float(radius[k]), centre[k])
+        d = drawables[k]
+        d.transformation[:] = m.tolist()
+        d.inverse_transformation[:] = inv.tolist()
+        d.indices_base_index, d.points_base_index, d.index_count = 0, 0, si.size
+        d.material_index = k + 1
+        mat_data.append(pbr_material(albedo[k], roughness=float(rough[k]), metallic=float(metal[k])))
+    fl = drawables[n_spheres]
+    fl.transformation[:] = _affine(1.0, (0, 0, 0))[0].tolist()
+    fl.inverse_transformation[:] = _affine(1.0, (0, 0, 0))[1].tolist()
+    fl.indices_base_index, fl.points_base_index, fl.index_count = si.size, sp.shape[0], fi.size
+    fl.material_index = 0
+    mat_data = np.stack(mat_data)
+    materials = np.stack([np.zeros(len(mat_data), np.int32), np.arange(len(mat_data), dtype=np.int32) * 7], 1)
+    return dict(indices=indices, vertices=vertices, normals=normals, drawables=drawables, materials=materials,
+                material_data=mat_data.ravel())
+
+
+def icosphere_camera_rays(width: int = 512, height: int = 512, spp: int = 1, seed: int = 5) -> np.ndarray:
+    """Camera rays of the icosphere scene; spp > 1 adds sub-pixel jitter."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(spp):
+        jit = None if spp == 1 else rng.uniform(-0.5, 0.5, (width * height, 2))
+        out.append(pinhole_rays(width, height, eye=(0.0, 1.0, -4.5), target=(0.0, -0.3, 0.0), vfov_deg=50.0,
+                                jitter=jit))
+    return np.concatenate(out, 0)

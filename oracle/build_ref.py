@@ -1,0 +1,111 @@
+"""Build recipe for oracle/_ref: the reference's own code, compiled here.
+
+TEST INFRASTRUCTURE ONLY. Nothing in the product imports this file or the
+library it builds; tests/, the smoke check and bench.py's CPU-baseline leg use
+the result as a checker / reference timing.
+
+What it compiles, from the sources where they lie under the reference tree
+(REF_ROOT, default /root/reference):
+
+* src/pathtracer/bvh.cpp and src/thread_pool.cpp with the two shims under
+  oracle/shim (rnu vector math, <experimental/generator>). bvh.cpp needs one
+  build-time edit: the explicit ``myrt::`` qualification on
+  ``generate_triangle_bounds`` at bvh.cpp:136 is an MSVC-ism that g++ rejects,
+  so a copy with that token removed is written to oracle/_ref/src/.
+* The shader helper files src/pt/{random,intersect,ggx,color,pbr,transform,
+  bvh,bvh.impl}.glsl and the traversal visitor of src/pt/pt_trace.comp
+  (lines 229-282: traversal_state_t, traversal_init, visit_triangle), compiled
+  as C++ through oracle/glsl_compat.hpp after these mechanical rewrites only:
+    - ``out T x`` / ``inout T x`` parameters -> ``T& x``; ``const in`` -> ``const``;
+    - float literals without a suffix get ``f`` (GLSL literals are float);
+    - per-invocation globals become ``thread_local``.
+  The rewritten copies go to oracle/_ref/glsl/.
+
+Output: oracle/_ref/libmyrt_ref.so (git-ignored; it travels with the tree).
+The reference tree is only needed at build time.
+"""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+REF_ROOT = Path(os.environ.get("MYRT_REFERENCE_ROOT", "/root/reference"))
+
+GLSL_FILES = ["random.glsl", "intersect.glsl", "ggx.glsl", "color.glsl", "pbr.glsl", "transform.glsl", "bvh.glsl",
+              "bvh.impl.glsl"]
+
+_FLOAT_LIT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][-+]?\d+)?|\d+[eE][-+]?\d+)(?![\w.])")
+_PARAM_REF = re.compile(r"\b(?:inout|out)\s+([A-Za-z_]\w*)\s+([A-Za-z_]\w*)")
+_GLOBAL_VAR = re.compile(r"^(int|bool|float|uint|random_state_t|material_state_t)(\s+\w+\s*(?:=[^;]*)?;)", re.M)
+
+
+def glsl_to_cpp(src: str) -> str:
+    src = re.sub(r"\bconst\s+in\s+", "const ", src)
+    src = _PARAM_REF.sub(r"\1& \2", src)
+    src = _FLOAT_LIT.sub(r"\1f", src)
+    src = _GLOBAL_VAR.sub(r"thread_local \1\2", src)
+    return src
+
+
+def extract_trace_visitor(src: str) -> str:
+    """pt_trace.comp:229-282 (traversal state, traversal_init, visit_triangle)."""
+    start = src.index("struct traversal_state_t")
+    end = src.index("bool visit_object_aabb")
+    seg = src[start:end]
+    seg, n = re.subn(r"\}\s*traversal\s*;", "};\nthread_local traversal_state_t traversal;", seg)
+    assert n == 1, "pt_trace.comp: traversal_state_t layout changed"
+    return glsl_to_cpp(seg)
+
+
+def material_codegen(src: str, type_name: str = "material") -> str:
+    """The text substitution material_registry::push_type applies (material.hpp:18-29)."""
+    for word in ("open", "evaluate", "bounce"):
+        src = src.replace(word, f"{type_name}_{word}_")
+    src = src.replace("this", f"{type_name}_instance_")
+    return f"thread_local {type_name} {type_name}_instance_;\n" + glsl_to_cpp(src)
+
+
+def write_sources() -> None:
+    (OUT / "src").mkdir(parents=True, exist_ok=True)
+    (OUT / "glsl").mkdir(parents=True, exist_ok=True)
+    bvh_src = (REF_ROOT / "src/pathtracer/bvh.cpp").read_text()
+    needle = "std::vector<aabb_t> myrt::generate_triangle_bounds("
+    assert bvh_src.count(needle) == 1, "bvh.cpp:136 no longer has the expected qualifier"
+    (OUT / "src/bvh.cpp").write_text(bvh_src.replace(needle, "std::vector<aabb_t> generate_triangle_bounds("))
+    for name in GLSL_FILES:
+        (OUT / "glsl" / name).write_text(glsl_to_cpp((REF_ROOT / "src/pt" / name).read_text()))
+    (OUT / "glsl/material_new.glsl").write_text(material_codegen((REF_ROOT / "src/pt/material_new.glsl").read_text()))
+    trace = (REF_ROOT / "src/pt/pt_trace.comp").read_text()
+    (OUT / "glsl/pt_trace_visitor.glsl").write_text(extract_trace_visitor(trace))
+
+
+def compile_ref() -> Path:
+    lib = OUT / "libmyrt_ref.so"
+    flags = ["-std=c++23", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fwrapv", "-fno-fast-math", "-pthread",
+             "-w"]
+    incs = ["-I", str(HERE / "shim"), "-I", str(REF_ROOT / "src/pathtracer"), "-I", str(REF_ROOT / "src"), "-I",
+            str(OUT / "glsl"), "-I", str(HERE)]
+    srcs = [str(OUT / "src/bvh.cpp"), str(REF_ROOT / "src/thread_pool.cpp"), str(HERE / "ref_harness_bvh.cpp"),
+            str(HERE / "ref_harness_glsl.cpp")]
+    cmd = ["g++", *flags, *incs, *srcs, "-o", str(lib)]
+    subprocess.run(cmd, check=True)
+    return lib
+
+
+def main() -> int:
+    if not (REF_ROOT / "src/pathtracer/bvh.cpp").exists():
+        print(f"reference tree not found at {REF_ROOT}; oracle/_ref not rebuilt", file=sys.stderr)
+        return 0
+    write_sources()
+    lib = compile_ref()
+    print(f"built {lib}")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

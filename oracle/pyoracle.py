@@ -1,0 +1,220 @@
+"""ctypes front end of the CPU oracle (liboracle.so) and, when built, of the
+reference's own code compiled here (_ref/libmyrt_ref.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and bench.py's
+CPU-baseline leg, as the checker. The product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libmyrt_ref.so"
+
+P = C.c_void_p
+SZ = C.c_size_t
+I = C.c_int
+
+_orc = None
+_ref = None
+
+
+def oracle() -> C.CDLL:
+    global _orc
+    if _orc is None:
+        if not ORACLE_LIB.exists():
+            raise RuntimeError(f"{ORACLE_LIB} is missing: run `python oracle/build.py`")
+        h = C.CDLL(str(ORACLE_LIB))
+        sig = {
+            "orc_isect_reference": (I, [P, P, P, P, P]),
+            "orc_refbvh_build": (P, [P, SZ, P]),
+            "orc_refbvh_free": (None, [P]),
+            "orc_refbvh_node_count": (SZ, [P]),
+            "orc_refbvh_nodes": (None, [P, P]),
+            "orc_refbvh_indices": (None, [P, P]),
+            "orc_refbvh_traverse": (None, [P, P, P, P, P, SZ, I, I, P, P, P, P, I]),
+            "orc_bvh8_traverse": (None, [P, P, P, SZ, I, I, P, P, P, P, P, P, P, I]),
+            "orc_brute_closest": (None, [P, SZ, P, SZ, I, P, P, P, P, I]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(h, k)
+            f.restype, f.argtypes = r, a
+        _orc = h
+    return _orc
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        h = C.CDLL(str(REF_LIB))
+        sig = {
+            "ref_bvh_build": (P, [P, SZ, P, SZ, I]),
+            "ref_bvh_free": (None, [P]),
+            "ref_bvh_node_count": (SZ, [P]),
+            "ref_bvh_index_count": (SZ, [P]),
+            "ref_bvh_nodes": (None, [P, P]),
+            "ref_bvh_indices": (None, [P, P]),
+            "ref_pick_closest": (None, [P, P, SZ, P, P, P, P, I]),
+            "ref_glsl_traverse": (None, [P, P, P, P, P, SZ, I, P, P, P, P, I]),
+            "ref_glsl_wang_hash": (C.c_uint32, [C.c_uint32]),
+            "ref_glsl_random_stream": (None, [P, I, I, I, I, I, P, P]),
+            "ref_glsl_random_values": (None, [C.c_uint32, P, I, P, P]),
+            "ref_glsl_intersect_triangle": (I, [P, P, P, P, P]),
+            "ref_glsl_intersect_sphere": (C.c_float, [P, P, P, C.c_float]),
+            "ref_glsl_transform_local_to_world": (None, [P, P, P]),
+            "ref_glsl_pack_unorm4x8": (C.c_uint32, [P]),
+            "ref_glsl_material_bounce_eval": (None, [P, P, P, P, P, P, P, P, P]),
+            "ref_glsl_material_eval": (None, [P, I, C.c_float, P, P, P, P, P]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(h, k)
+            f.restype, f.argtypes = r, a
+        _ref = h
+    return _ref
+
+
+def nthreads() -> int:
+    return os.cpu_count() or 1
+
+
+def _hits(n):
+    return np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.float32), np.empty(n, np.float32)
+
+
+def _pack(prim, t, u, v):
+    out = np.empty(prim.size, [("prim", np.int32), ("t", np.float32), ("u", np.float32), ("v", np.float32)])
+    out["prim"], out["t"], out["u"], out["v"] = prim, t, u, v
+    return out
+
+
+# ---- oracle restatement -----------------------------------------------------
+def refbvh_build(indices: np.ndarray, points: np.ndarray):
+    """Restated reference build (dont_split). Returns (nodes uint32[N,12], bvh_indices)."""
+    L = oracle()
+    idx = np.ascontiguousarray(indices, np.uint32)
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    h = L.orc_refbvh_build(idx.ctypes.data, idx.size, pts.ctypes.data)
+    try:
+        n = L.orc_refbvh_node_count(h)
+        nodes = np.zeros((n, 12), np.uint32)
+        L.orc_refbvh_nodes(h, nodes.ctypes.data)
+        bi = np.zeros(idx.size // 3, np.uint32)
+        L.orc_refbvh_indices(h, bi.ctypes.data)
+        return nodes, bi
+    finally:
+        L.orc_refbvh_free(h)
+
+
+def refbvh_traverse(nodes, bvh_indices, indices, points, rays, any_hit=False, canonical=True):
+    L = oracle()
+    p4 = np.zeros((points.shape[0], 4), np.float32)
+    p4[:, :3] = points
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    out = _hits(r.shape[0])
+    nodes = np.ascontiguousarray(nodes)
+    bvh_indices = np.ascontiguousarray(bvh_indices, np.uint32)
+    indices = np.ascontiguousarray(indices, np.uint32)
+    L.orc_refbvh_traverse(nodes.ctypes.data, bvh_indices.ctypes.data, indices.ctypes.data, p4.ctypes.data,
+                          r.ctypes.data, r.shape[0], int(any_hit), int(canonical), *[o.ctypes.data for o in out],
+                          nthreads())
+    return _pack(*out)
+
+
+def bvh8_traverse(nodes, tris, rays, isect=0, any_hit=False):
+    """The device algorithm on the CPU. Returns (hits, n_nodes, n_tris[, occluded])."""
+    L = oracle()
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = r.shape[0]
+    out = _hits(n)
+    cn = np.zeros(n, np.uint32)
+    ct = np.zeros(n, np.uint32)
+    occ = np.zeros(n, np.uint8)
+    nodes = np.ascontiguousarray(nodes, np.uint32)
+    tris = np.ascontiguousarray(tris, np.float32)
+    L.orc_bvh8_traverse(nodes.ctypes.data, tris.ctypes.data, r.ctypes.data, n, int(any_hit), int(isect),
+                        *[o.ctypes.data for o in out], cn.ctypes.data, ct.ctypes.data, occ.ctypes.data, nthreads())
+    if any_hit:
+        return occ, cn, ct
+    return _pack(*out), cn, ct
+
+
+def brute_closest(tris9: np.ndarray, rays: np.ndarray, isect=0):
+    L = oracle()
+    t9 = np.ascontiguousarray(tris9, np.float32).reshape(-1, 9)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    out = _hits(r.shape[0])
+    L.orc_brute_closest(t9.ctypes.data, t9.shape[0], r.ctypes.data, r.shape[0], int(isect),
+                        *[o.ctypes.data for o in out], nthreads())
+    return _pack(*out)
+
+
+# ---- the reference's own code (oracle/_ref) -----------------------------------
+def ref_bvh(indices, points, split: bool):
+    L = ref()
+    idx = np.ascontiguousarray(indices, np.uint32)
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    h = L.ref_bvh_build(idx.ctypes.data, idx.size, pts.ctypes.data, pts.shape[0], int(split))
+    return h
+
+
+def ref_bvh_arrays(h):
+    L = ref()
+    nodes = np.zeros((L.ref_bvh_node_count(h), 12), np.uint32)
+    L.ref_bvh_nodes(h, nodes.ctypes.data)
+    bi = np.zeros(L.ref_bvh_index_count(h), np.uint32)
+    L.ref_bvh_indices(h, bi.ctypes.data)
+    return nodes, bi
+
+
+def ref_pick_closest(h, rays, threads=None):
+    L = ref()
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    out = _hits(r.shape[0])
+    L.ref_pick_closest(h, r.ctypes.data, r.shape[0], *[o.ctypes.data for o in out], threads or nthreads())
+    return _pack(*out)
+
+
+def ref_glsl_traverse(nodes, bvh_indices, indices, points, rays, any_hit=False, threads=None):
+    L = ref()
+    p4 = np.zeros((points.shape[0], 4), np.float32)
+    p4[:, :3] = points
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    out = _hits(r.shape[0])
+    nodes = np.ascontiguousarray(nodes)
+    bvh_indices = np.ascontiguousarray(bvh_indices, np.uint32)
+    indices = np.ascontiguousarray(indices, np.uint32)
+    L.ref_glsl_traverse(nodes.ctypes.data, bvh_indices.ctypes.data, indices.ctypes.data, p4.ctypes.data,
+                        r.ctypes.data, r.shape[0], int(any_hit), *[o.ctypes.data for o in out], threads or nthreads())
+    return _pack(*out)
+
+
+# ---- scene baking (numpy, independent of the product's C++ bake) -----------
+def bake_world_triangles(indices, vertices, drawables=None) -> np.ndarray:
+    """World-space triangles float32[T, 9] in the product's prim numbering
+    (drawable by drawable, then index order); float32 arithmetic with the same
+    left-to-right sums as a column-major mat4 * vec4."""
+    idx = np.asarray(indices, np.uint32)
+    v = np.asarray(vertices, np.float32)[:, :3]
+    if drawables is None or len(drawables) == 0:
+        return v[idx.reshape(-1, 3)].reshape(-1, 9)
+    out = []
+    for d in drawables:
+        m = np.array(d.transformation[:], np.float32)
+        sel = idx[d.indices_base_index: d.indices_base_index + d.index_count].astype(np.int64) + d.points_base_index
+        p = v[sel]
+        ident = np.array_equal(m, np.eye(4, dtype=np.float32).ravel())
+        if not ident:
+            x, y, z = p[:, 0], p[:, 1], p[:, 2]
+            one = np.float32(1.0)
+            p = np.stack([((m[r] * x + m[4 + r] * y) + m[8 + r] * z) + m[12 + r] * one for r in range(3)], 1)
+        out.append(p.reshape(-1, 9).astype(np.float32))
+    return np.concatenate(out, 0)

@@ -1,0 +1,232 @@
+// C entry points around the reference's shader helper code, compiled as C++.
+//
+// TEST INFRASTRUCTURE ONLY. oracle/build_ref.py rewrites the reference's GLSL
+// helper files mechanically (see its docstring) into oracle/_ref/glsl/ and this
+// file includes them inside namespace glsl, on top of oracle/glsl_compat.hpp.
+// What runs here is therefore the reference's own source for:
+//   src/pt/random.glsl:14-85        (Wang hash, xorshift32, prime cycle)
+//   src/pt/intersect.glsl:3-39      (Moller-Trumbore, ray/sphere)
+//   src/pt/bvh.glsl:31-55           (slab test, node accessors)
+//   src/pt/bvh.impl.glsl:8-72       (stackless bit-trail traversal)
+//   src/pt/pt_trace.comp:229-282    (closest / any-hit triangle visitor)
+//   src/pt/ggx.glsl, pbr.glsl, color.glsl, transform.glsl
+//   src/pt/material_new.glsl        (after the same text substitution that
+//                                    material_registry::push_type applies,
+//                                    src/material.hpp:18-37)
+#include "glsl_compat.hpp"
+
+#include <cstdint>
+#include <thread>
+#include <vector>
+
+#undef INT_MAX
+
+namespace glsl {
+#include "transform.glsl"
+#include "random.glsl"
+#include "intersect.glsl"
+#include "pbr.glsl"
+
+// Material record of the reference app's PBR type (src/main.cpp:447-464):
+// albedo vec4unorm8 (1 float), ior, roughness, metallic, transmission, albedo
+// texture uvec2 (2 floats) = 7 floats. The loader mirrors what
+// generate_object_loaders emits for it (src/types.hpp:46-100; vec4unorm8 is
+// loaded as unpackUnorm4x8(floatBitsToUint(x)), types.hpp:66).
+struct color_t {
+  vec4 value;
+};
+struct material {
+  color_t albedo;
+  float ior;
+  float roughness;
+  float metallic;
+  float transmission;
+  uvec2 albedo_texture;
+};
+struct sampler2D {
+  explicit sampler2D(uvec2) {}
+};
+inline vec4 texture(sampler2D const&, vec2 const&) { return vec4(1.f); }
+
+#include "material_new.glsl"
+
+thread_local float const* g_material_data = nullptr;
+inline material material_load_(uint buf) {
+  material m;
+  m.albedo.value = unpackUnorm4x8(floatBitsToUint(g_material_data[buf + 0]));
+  m.ior = g_material_data[buf + 1];
+  m.roughness = g_material_data[buf + 2];
+  m.metallic = g_material_data[buf + 3];
+  m.transmission = g_material_data[buf + 4];
+  m.albedo_texture = uvec2(floatBitsToUint(g_material_data[buf + 5]), floatBitsToUint(g_material_data[buf + 6]));
+  return m;
+}
+// material.hpp:26-27: "void {0}_load_mat_(uint buf) { {0}_instance_ = {0}_load_(buf); {0}_open_(); }"
+inline void material_load_mat_(uint buf) {
+  material_instance_ = material_load_(buf);
+  material_open_();
+}
+
+// Mesh buffers of pt_trace.comp:82-90, bound per call (read-only, shared).
+#define MYRT_POINT_TYPE vec3
+#define MYRT_INDEX_TYPE uint
+#define MYRT_BVH_NODE_PADDING_BYTES 3
+#define MYRT_BVH_NODE_TYPE_SHIFT 31
+#define MYRT_BVH_NODE_STRUCT bvh_node_t
+#include "bvh.glsl"
+static_assert(sizeof(bvh_node_t) == 48, "std430 node layout");
+
+bvh_node_t const* bvh_nodes = nullptr;
+uint const* bvh_indices = nullptr;
+uint const* indices = nullptr;
+vec4 const* points = nullptr;
+
+#define MYRT_BVH_NODES_BUFFER bvh_nodes
+#define MYRT_BVH_INDICES_BUFFER bvh_indices
+#define MYRT_BVH_TRAVERSE bvh_traverse
+#define MYRT_BVH_VISIT_PRIMITIVE visit_triangle
+#include "bvh.impl.glsl"
+#include "pt_trace_visitor.glsl"
+}  // namespace glsl
+
+using namespace glsl;
+
+extern "C" {
+
+std::uint32_t ref_glsl_wang_hash(std::uint32_t a) { return random_wang_hash(a); }
+
+// random_init(tex, pixel, seed) followed by n random_next() draws.
+void ref_glsl_random_stream(float const* tex, int tex_size, int px, int py, int seed, int n, float* out,
+    std::uint32_t* state_after_init) {
+  sampler1D s{tex, tex_size};
+  random_init(s, ivec2(px, py), seed);
+  if (state_after_init) state_after_init[0] = random_state.rng_state;
+  for (int i = 0; i < n; ++i) out[i] = random_next();
+}
+
+// random_value(seed[i]) from a given xorshift state.
+void ref_glsl_random_values(std::uint32_t state, int const* seeds, int n, float* out, std::uint32_t* state_out) {
+  random_state.rng_state = state;
+  random_state.current_prime = 0;
+  for (int i = 0; i < n; ++i) out[i] = random_value(seeds[i]);
+  if (state_out) *state_out = random_state.rng_state;
+}
+
+int ref_glsl_intersect_triangle(float const* o, float const* d, float const* tri, float* t, float* bary) {
+  float tt = 0.f;
+  vec2 b(0.f, 0.f);
+  bool const h =
+      intersect_triangle(vec3(o[0], o[1], o[2]), vec3(d[0], d[1], d[2]), vec3(tri[0], tri[1], tri[2]),
+          vec3(tri[3], tri[4], tri[5]), vec3(tri[6], tri[7], tri[8]), tt, b);
+  *t = tt;
+  bary[0] = b.x;
+  bary[1] = b.y;
+  return h ? 1 : 0;
+}
+
+float ref_glsl_intersect_sphere(float const* r0, float const* rd, float const* s0, float sr) {
+  return intersect_sphere(vec3(r0[0], r0[1], r0[2]), vec3(rd[0], rd[1], rd[2]), vec3(s0[0], s0[1], s0[2]), sr);
+}
+
+void ref_glsl_transform_local_to_world(float const* v, float const* n, float* out) {
+  vec3 const r = transform_local_to_world(vec3(v[0], v[1], v[2]), vec3(n[0], n[1], n[2]));
+  out[0] = r.x;
+  out[1] = r.y;
+  out[2] = r.z;
+}
+
+std::uint32_t ref_glsl_pack_unorm4x8(float const* v) { return packUnorm4x8(vec4(v[0], v[1], v[2], v[3])); }
+
+// pt_color.comp:137-143 for one surface hit: open the material, draw the two
+// material randoms, bounce, evaluate. Runs from the given RNG state and
+// returns the state afterwards, so a caller can continue the stream.
+//   mat7   : the 7-float material record
+//   io_rng : [rng_state, current_prime] in/out
+//   out_gen: sampled direction; out_refl/out_pdf: evaluate() result;
+//   out_lobe: pbr_state (0 reflect, 1 transmit, 2 diffuse); out_resample.
+void ref_glsl_material_bounce_eval(float const* mat7, std::uint32_t* io_rng, float const* towards_viewer,
+    float const* normal, float* out_gen, float* out_refl, float* out_pdf, int* out_lobe, float* out_resample) {
+  random_state.rng_state = io_rng[0];
+  random_state.current_prime = int(io_rng[1]);
+  g_material_data = mat7;
+  material_load_mat_(0);
+  vec2 const material_randoms = vec2(random_next(), random_next());
+  vec3 const tv(towards_viewer[0], towards_viewer[1], towards_viewer[2]);
+  vec3 const n(normal[0], normal[1], normal[2]);
+  vec3 const generated = material_bounce_(material_randoms, tv, n);
+  vec3 refl;
+  float pdf = 0.f;
+  material_evaluate_(vec3(0.f), vec2(0.f, 0.f), n, generated, tv, refl, pdf);
+  out_gen[0] = generated.x;
+  out_gen[1] = generated.y;
+  out_gen[2] = generated.z;
+  out_refl[0] = refl.x;
+  out_refl[1] = refl.y;
+  out_refl[2] = refl.z;
+  *out_pdf = pdf;
+  *out_lobe = pbr_state;
+  *out_resample = resample_factor;
+  io_rng[0] = random_state.rng_state;
+  io_rng[1] = std::uint32_t(random_state.current_prime);
+}
+
+// evaluate() for a given direction with the lobe state a previous bounce left
+// behind (pt_color.comp:168-177 evaluates the NEE direction this way).
+void ref_glsl_material_eval(float const* mat7, int lobe, float resample, float const* towards_light,
+    float const* towards_viewer, float const* normal, float* out_refl, float* out_pdf) {
+  g_material_data = mat7;
+  material_load_mat_(0);
+  pbr_state = lobe;
+  resample_factor = resample;
+  after_sample = false;
+  vec3 refl;
+  float pdf = 0.f;
+  material_evaluate_(vec3(0.f), vec2(0.f, 0.f), vec3(normal[0], normal[1], normal[2]),
+      vec3(towards_light[0], towards_light[1], towards_light[2]),
+      vec3(towards_viewer[0], towards_viewer[1], towards_viewer[2]), refl, pdf);
+  out_refl[0] = refl.x;
+  out_refl[1] = refl.y;
+  out_refl[2] = refl.z;
+  *out_pdf = pdf;
+}
+
+// bvh.impl.glsl traversal with the pt_trace.comp visitor, for one drawable with
+// an identity transform (what visit_object_aabb, pt_trace.comp:284-309, does
+// for it). nodes: 48-byte reference records; any_hit selects any_hit()'s mode
+// (pt_trace.comp:311-329). Outputs prim (-1 = miss), t, u, v.
+void ref_glsl_traverse(void const* nodes, std::uint32_t const* node_indices, std::uint32_t const* tri_indices,
+    float const* points_xyzw, float const* rays, std::size_t n, int any_hit, std::int32_t* prim, float* t_out,
+    float* u_out, float* v_out, int nthreads) {
+  bvh_nodes = static_cast<bvh_node_t const*>(nodes);
+  bvh_indices = node_indices;
+  indices = tri_indices;
+  points = reinterpret_cast<vec4 const*>(points_xyzw);
+  auto work = [=](std::size_t begin, std::size_t end) {
+    for (std::size_t r = begin; r < end; ++r) {
+      float const* q = rays + 8 * r;
+      float const maxt = q[7];
+      traversal_init();
+      traversal.any_hit = any_hit != 0;
+      traversal.t = maxt;
+      traversal.global_t = maxt;
+      bool const h = bvh_traverse(0, 0, vec3(q[0], q[1], q[2]), vec3(q[4], q[5], q[6]), maxt);
+      prim[r] = h ? std::int32_t(traversal.hit_index) : -1;
+      t_out[r] = h ? traversal.t : maxt;
+      u_out[r] = h ? traversal.barycentric.x : 0.f;
+      v_out[r] = h ? traversal.barycentric.y : 0.f;
+    }
+  };
+  if (nthreads <= 1) {
+    work(0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  std::size_t const per = (n + std::size_t(nthreads) - 1) / std::size_t(nthreads);
+  for (int i = 0; i < nthreads; ++i) {
+    std::size_t const b = std::size_t(i) * per, e = std::min(n, b + per);
+    if (b < e) pool.emplace_back(work, b, e);
+  }
+  for (auto& th : pool) th.join();
+}
+
+}  // extern "C"

@@ -1,0 +1,154 @@
+"""GPU closest-hit / any-hit parity against the CPU oracle, through the C ABI.
+
+Bar: bit-exact prim ids, t, u and v (integer/index work and the same IEEE
+operations on both sides), for both intersectors, at the full sizes of the
+closest-hit configuration (1024^2 rays, 32,768 triangles) and of the
+path-tracing scene (655,872 triangles).
+"""
+import numpy as np
+import pytest
+
+import myrt_b200 as mb
+import pyoracle as po
+from myrt_b200.scenes import heightfield, icosphere_camera_rays, icosphere_field, pinhole_rays
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_rays(n, seed, lo=-1.3, hi=1.3):
+    rng = np.random.default_rng(seed)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = rng.uniform(lo, hi, (n, 3))
+    d = rng.normal(size=(n, 3))
+    r[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    r[:, 7] = np.inf
+    r[::11, 7] = rng.uniform(0.05, 1.0, r[::11].shape[0])
+    r[::13, 3] = rng.uniform(0.0, 0.2, r[::13].shape[0])
+    r[::17, 4:7] = np.array([0.0, -1.0, 0.0])  # axis-aligned: zero direction components
+    r[::19, 4:7] *= 3.5  # unnormalised direction
+    return r
+
+
+@pytest.fixture(scope="module")
+def hf128(ctx):
+    idx, pts = heightfield(128, seed=1)
+    info = ctx.upload_scene(idx, pts)
+    tris9 = pts[idx.reshape(-1, 3)].reshape(-1, 9)
+    nodes, tris, _ = mb.build_bvh8(tris9)
+    return dict(idx=idx, pts=pts, tris9=tris9, nodes=nodes, tris=tris, info=info)
+
+
+def test_golden_closest_hits_on_gpu(ctx, golden):
+    g = golden("closest_hf128.npz")
+    idx, pts, rays, glsl = g["indices"], g["points"], g["rays"], g["glsl"]
+    ctx.upload_scene(idx, pts)
+    hits = ctx.trace_closest(rays)
+    same = hits["prim"] == glsl["prim"]
+    assert same.mean() >= 0.999
+    # where ids differ, the reference's first-visited rule resolved an exact tie in t
+    assert np.array_equal(hits["t"], glsl["t"])
+    hit = glsl["prim"] >= 0
+    assert np.array_equal(hits["u"][hit & same], glsl["u"][hit & same])
+    occ = ctx.trace_any(g["shadow_rays"])
+    assert np.array_equal(occ.astype(bool), g["any_short_prim"] >= 0)
+
+
+@pytest.mark.parametrize("isect", [mb.ISECT_REFERENCE, mb.ISECT_WATERTIGHT])
+def test_closest_full_camera_bit_exact(ctx, hf128, isect):
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = pinhole_rays(1024, 1024)
+    hits = ctx.trace_closest(rays, intersector=isect)
+    ora, _, _ = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays, isect=isect)
+    assert np.array_equal(hits, ora)
+    sub = slice(None, None, 97)
+    bf = po.brute_closest(hf128["tris9"], rays[sub], isect=isect)
+    assert np.array_equal(hits[sub], bf)
+
+
+@pytest.mark.parametrize("isect", [mb.ISECT_REFERENCE, mb.ISECT_WATERTIGHT])
+def test_random_rays_closest_and_any(ctx, hf128, isect):
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = _rand_rays(300_000, seed=isect + 10)
+    hits = ctx.trace_closest(rays, intersector=isect)
+    ora, _, _ = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays, isect=isect)
+    assert np.array_equal(hits, ora)
+    occ = ctx.trace_any(rays, intersector=isect)
+    occ_o, _, _ = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays, isect=isect, any_hit=True)
+    assert np.array_equal(occ, occ_o)
+    assert np.array_equal(occ.astype(bool), ora["prim"] >= 0)
+
+
+def test_device_entry_points_and_counters(ctx, hf128):
+    import torch
+
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = _rand_rays(100_000, seed=5)
+    d_rays = torch.from_numpy(rays).cuda()
+    d_hits = torch.empty((rays.shape[0], 4), dtype=torch.float32, device="cuda")
+    d_n = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+    d_t = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    ctx.trace_closest_stats_device(d_rays, d_hits, d_n, d_t)
+    ctx.sync()
+    ora, cn, ct = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays)
+    got = d_hits.cpu().numpy().view(mb.HIT_DTYPE).ravel()
+    assert np.array_equal(got, ora)
+    # the counters behind the roofline's bytes per ray are exact
+    assert np.array_equal(d_n.cpu().numpy().astype(np.uint32), cn)
+    assert np.array_equal(d_t.cpu().numpy().astype(np.uint32), ct)
+    ctx.trace_closest_device(d_rays, d_hits)
+    ctx.sync()
+    assert np.array_equal(d_hits.cpu().numpy().view(mb.HIT_DTYPE).ravel(), ora)
+    d_occ = torch.empty(rays.shape[0], dtype=torch.uint8, device="cuda")
+    ctx.trace_any_device(d_rays, d_occ)
+    ctx.sync()
+    assert np.array_equal(d_occ.cpu().numpy().astype(bool), ora["prim"] >= 0)
+
+
+def test_instanced_sphere_scene_bit_exact(ctx):
+    s = icosphere_field()
+    info = ctx.upload_scene(**s)
+    assert info["triangles"] == 655_872
+    tris9 = po.bake_world_triangles(s["indices"], s["vertices"], s["drawables"])
+    rays = np.concatenate([icosphere_camera_rays(512, 512, spp=2), _rand_rays(200_000, seed=9, lo=-1.1, hi=1.1)])
+    hits = ctx.trace_closest(rays)
+    nodes, tris, _ = mb.build_bvh8(tris9)
+    ora, _, _ = po.bvh8_traverse(nodes, tris, rays)
+    assert np.array_equal(hits, ora)
+    sub = slice(None, None, 331)
+    assert np.array_equal(hits[sub], po.brute_closest(tris9, rays[sub]))
+    occ = ctx.trace_any(rays)
+    assert np.array_equal(occ.astype(bool), ora["prim"] >= 0)
+
+
+def test_edge_cases(ctx):
+    tri = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0]], np.float32)
+    idx = np.array([0, 1, 2, 1, 3, 2], np.uint32)  # two triangles sharing an edge
+    ctx.upload_scene(idx, tri)
+    rays = np.zeros((6, 8), np.float32)
+    rays[:, 6] = 1.0
+    rays[:, 2] = -1.0
+    rays[:, 7] = np.inf
+    rays[0, 0:2] = (0.25, 0.25)  # inside the first triangle
+    rays[1, 0:2] = (0.5, 0.5)    # on the shared edge: tie in t, smaller prim wins
+    rays[2, 0:2] = (2.0, 2.0)    # miss
+    rays[3, 0:2] = (0.25, 0.25)
+    rays[3, 7] = 0.5             # tmax before the surface
+    rays[4, 0:2] = (0.75, 0.75)
+    rays[5, 0:2] = (0.25, 0.25)
+    rays[5, 3] = 2.0             # tmin beyond the surface
+    hits = ctx.trace_closest(rays)
+    assert list(hits["prim"]) == [0, 0, -1, -1, 1, -1]
+    assert hits["t"][0] == 1.0 and hits["t"][3] == 0.5
+    assert np.array_equal(ctx.trace_any(rays), np.array([1, 1, 0, 0, 1, 0], np.uint8))
+    # an empty batch is a no-op
+    assert ctx.trace_closest(np.zeros((0, 8), np.float32)).size == 0
+
+
+def test_errors_are_reported(ctx):
+    with pytest.raises(mb.MyrtError):
+        ctx.upload_scene(np.array([0, 1], np.uint32), np.zeros((3, 3), np.float32))  # not a multiple of 3
+    with pytest.raises(mb.MyrtError):
+        ctx.upload_scene(np.array([0, 1, 7], np.uint32), np.zeros((3, 3), np.float32))  # index out of range
+    with pytest.raises(mb.MyrtError):
+        ctx.trace_closest(np.zeros((4, 8), np.float32), intersector=7)
