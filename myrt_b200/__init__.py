@@ -29,6 +29,8 @@ def _ptr(a) -> int | None:
         return None
     if isinstance(a, np.ndarray):
         return a.ctypes.data
+    if isinstance(a, C.Array):
+        return C.addressof(a)
     return int(a.data_ptr())  # torch tensor
 
 

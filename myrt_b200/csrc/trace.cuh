@@ -134,15 +134,18 @@ struct trace_args {
 
 __device__ __forceinline__ float q8(uint32_t w, int s) { return float((w >> (8 * (s & 3))) & 0xffu); }
 
-template <int ISECT, bool ANY, bool STATS>
-__device__ __forceinline__ void trace_one(trace_args const& a, uint32_t i) {
-  float4 const r0 = __ldg(a.rays + 2 * size_t(i));
-  float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
-  f3 const o{r0.x, r0.y, r0.z};
-  f3 const d{r1.x, r1.y, r1.z};
-  float const tmin = r0.w;
-  float const tmax = r1.w;
+struct hit_rec {
+  int32_t prim;  // -1 = none
+  float t, u, v;
+};
 
+// Walks the tree for one ray. Closest hit (ANY = false): fills h and returns
+// whether a triangle was hit. Any hit (ANY = true): returns true at the first
+// triangle with tmin <= t < tmax. n_nodes / n_tris count fetched nodes and
+// tested triangles when STATS.
+template <int ISECT, bool ANY, bool STATS>
+__device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris, f3 o, f3 d,
+    float tmin, float tmax, hit_rec& h, uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris) {
   // Box-test reciprocal: zero components are nudged so no 0 * inf appears.
   float const idx = 1.0f / (fabsf(d.x) > 1e-20f ? d.x : copysignf(1e-20f, d.x));
   float const idy = 1.0f / (fabsf(d.y) > 1e-20f ? d.y : copysignf(1e-20f, d.y));
@@ -155,7 +158,6 @@ __device__ __forceinline__ void trace_one(trace_args const& a, uint32_t i) {
   float tbest = tmax;
   int32_t best = -1;
   float bu = 0.f, bv = 0.f;
-  uint32_t n_nodes = 0, n_tris = 0;
   bool occluded = false;
 
   uint2 stack[MYRT_STACK_MAX];
@@ -171,12 +173,12 @@ __device__ __forceinline__ void trace_one(trace_args const& a, uint32_t i) {
       uint32_t const node_idx = group.x + __popc(group.y & 0xffu & ((1u << slot) - 1u));
       if (group.y & 0xff000000u) {
         if (sp >= MYRT_STACK_MAX) {
-          atomicOr(a.err, ERR_STACK_OVERFLOW);
+          atomicOr(err, ERR_STACK_OVERFLOW);
           break;
         }
         stack[sp++] = group;
       }
-      uint4 const* np = a.nodes + 5 * size_t(node_idx);
+      uint4 const* np = nodes + 5 * size_t(node_idx);
       uint4 const w0 = __ldg(np + 0);
       uint4 const w1 = __ldg(np + 1);
       uint4 const w2 = __ldg(np + 2);
@@ -227,19 +229,19 @@ __device__ __forceinline__ void trace_one(trace_args const& a, uint32_t i) {
     while (tgroup.y) {
       uint32_t const b = __ffs(tgroup.y) - 1u;
       tgroup.y &= tgroup.y - 1u;
-      float4 const* tp = a.tris + 3 * size_t(tgroup.x + b);
+      float4 const* tp = tris + 3 * size_t(tgroup.x + b);
       float4 const p0 = __ldg(tp + 0);
       float4 const p1 = __ldg(tp + 1);
       float4 const p2 = __ldg(tp + 2);
       if (STATS) ++n_tris;
       float t, u, v;
-      bool h;
+      bool hit;
       if (ISECT == 0)
-        h = isect_reference(o, d, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, t, u, v) &&
+        hit = isect_reference(o, d, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, t, u, v) &&
             t >= tmin;
       else
-        h = isect_watertight(wt, o, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, tmin, t, u, v);
-      if (!h) continue;
+        hit = isect_watertight(wt, o, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, tmin, t, u, v);
+      if (!hit) continue;
       int32_t const prim = __float_as_int(p0.w);
       if (ANY) {
         if (t < tmax) {
@@ -260,10 +262,26 @@ __device__ __forceinline__ void trace_one(trace_args const& a, uint32_t i) {
     }
   }
 
+  if (ANY) return occluded;
+  h.prim = best;
+  h.t = best >= 0 ? tbest : tmax;
+  h.u = best >= 0 ? bu : 0.f;
+  h.v = best >= 0 ? bv : 0.f;
+  return best >= 0;
+}
+
+template <int ISECT, bool ANY, bool STATS>
+__device__ __forceinline__ void trace_one(trace_args const& a, uint32_t i) {
+  float4 const r0 = __ldg(a.rays + 2 * size_t(i));
+  float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
+  hit_rec h;
+  uint32_t n_nodes = 0, n_tris = 0;
+  bool const r = traverse<ISECT, ANY, STATS>(a.nodes, a.tris, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w, r1.w,
+      h, a.err, n_nodes, n_tris);
   if (ANY) {
-    a.occluded[i] = occluded ? 1 : 0;
+    a.occluded[i] = r ? 1 : 0;
   } else {
-    a.hits[i] = make_float4(__int_as_float(best), best >= 0 ? tbest : tmax, best >= 0 ? bu : 0.f, best >= 0 ? bv : 0.f);
+    a.hits[i] = make_float4(__int_as_float(h.prim), h.t, h.u, h.v);
   }
   if (STATS) {
     a.stat_nodes[i] = n_nodes;
