@@ -178,6 +178,51 @@ int myrt_trace_any_device(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, uint8
 int myrt_trace_closest_stats_device(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, myrt_hit* hits,
     uint32_t* nodes, uint32_t* tris, int intersector, void* stream);
 
+/* ---- wavefront rendering ---------------------------------------------------- */
+
+/* The matrices sequential_pathtracer uploads to pt_generate.comp (column-major):
+ * ray direction = normalize((inverse_view * inverse_projection * (ndc, 1, 1)).xyz),
+ * origin = inverse_view column 3 (src/pt/pt_generate.comp:63-66). */
+typedef struct myrt_camera {
+  float inverse_view[16];
+  float inverse_projection[16];
+} myrt_camera;
+
+typedef enum myrt_shading {
+  /* The reference's passes and shading: 2 hard-coded sphere lights with NEE,
+   * the PBR material's bounce/evaluate, Russian roulette on the path pdf, sky
+   * gradient (src/pt/pt_trace.comp, pt_color.comp). */
+  MYRT_SHADE_REFERENCE = 0
+} myrt_shading;
+
+typedef struct myrt_render_params {
+  uint32_t width, height;
+  int32_t num_bounces; /* sequential_pathtracer::set_num_bounces (reference default 10) */
+  uint32_t frames;     /* frames (one sample per pixel each) to accumulate in this call */
+  int32_t shading;     /* myrt_shading */
+  uint32_t flags;      /* reserved, 0 */
+} myrt_render_params;
+
+/* Renders `frames` frames, each the reference's generate -> {trace, color,
+ * filter} x num_bounces -> trace, color sequence, accumulating into the
+ * context's images. Replaces sequential_pathtracer::run
+ * (src/pathtracer/sequential_pathtracer.cpp:10-69). A change of resolution or
+ * camera, or a scene upload, restarts accumulation (invalidate_counter). The
+ * host random stream is std::mt19937 (default seed 5489) drawn in the
+ * reference's order; myrt_set_seed reseeds it. Asynchronous on the ctx stream
+ * until myrt_read_accumulation or myrt_sync. */
+int myrt_render(myrt_ctx* ctx, const myrt_camera* camera, const myrt_render_params* params);
+/* Copies the accumulation image (debug_image: rgb sum, sample count in a) and
+ * the display image (output_image: clamp(sum / count, 0, 4)), W*H*4 floats
+ * each, row-major from pixel (0, 0); either pointer may be NULL. */
+int myrt_read_accumulation(myrt_ctx* ctx, float* rgba_sum, float* rgba_display);
+/* Device pointers of the two images (valid until the next resolution change). */
+int myrt_render_buffers(myrt_ctx* ctx, void** accum, void** display);
+/* sequential_pathtracer::invalidate_counter / sample_count / the m_rng seed. */
+int myrt_reset_accumulation(myrt_ctx* ctx);
+int myrt_sample_count(myrt_ctx* ctx, uint32_t* count);
+int myrt_set_seed(myrt_ctx* ctx, uint32_t seed);
+
 /* Waits for the context's work and returns MYRT_ERR_DEVICE_ABORT if a kernel
  * stopped at a limit since the last call (the error word is then cleared). */
 int myrt_sync(myrt_ctx* ctx);

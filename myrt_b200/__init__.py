@@ -167,3 +167,31 @@ class Context:
 
     def sync(self):
         self._check(self._L.myrt_sync(self._h), "myrt_sync")
+
+    # -- wavefront rendering (sequential_pathtracer::run) --
+    def render(self, inverse_view, inverse_projection, width: int, height: int, num_bounces: int = 10,
+               frames: int = 1, shading: int = _abi.SHADE_REFERENCE):
+        cam = _abi.myrt_camera()
+        cam.inverse_view[:] = np.asarray(inverse_view, np.float32).ravel().tolist()
+        cam.inverse_projection[:] = np.asarray(inverse_projection, np.float32).ravel().tolist()
+        p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0)
+        self._check(self._L.myrt_render(self._h, C.byref(cam), C.byref(p)), "myrt_render")
+
+    def read_accumulation(self, width: int, height: int):
+        """(rgb sum + count, display) images as float32 [H, W, 4]."""
+        acc = np.empty((height, width, 4), np.float32)
+        disp = np.empty((height, width, 4), np.float32)
+        self._check(self._L.myrt_read_accumulation(self._h, acc.ctypes.data, disp.ctypes.data),
+                    "myrt_read_accumulation")
+        return acc, disp
+
+    def reset_accumulation(self):
+        self._check(self._L.myrt_reset_accumulation(self._h), "myrt_reset_accumulation")
+
+    def sample_count(self) -> int:
+        c = C.c_uint32()
+        self._check(self._L.myrt_sample_count(self._h, C.byref(c)), "myrt_sample_count")
+        return c.value
+
+    def set_seed(self, seed: int):
+        self._check(self._L.myrt_set_seed(self._h, seed), "myrt_set_seed")

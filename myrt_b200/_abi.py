@@ -53,6 +53,17 @@ class myrt_bvh_info(C.Structure):
                 ("node_bytes", C.c_uint64), ("triangle_bytes", C.c_uint64)]
 
 
+class myrt_camera(C.Structure):
+    _fields_ = [("inverse_view", C.c_float * 16), ("inverse_projection", C.c_float * 16)]
+
+
+class myrt_render_params(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("num_bounces", C.c_int32), ("frames", C.c_uint32),
+                ("shading", C.c_int32), ("flags", C.c_uint32)]
+
+
+SHADE_REFERENCE = 0
+
 P = C.c_void_p
 SZ = C.c_size_t
 U32 = C.c_uint32
@@ -75,6 +86,12 @@ SIGNATURES = {
     "myrt_trace_any": (I, [P, P, U32, P, I]),
     "myrt_trace_any_device": (I, [P, P, U32, P, I, P]),
     "myrt_trace_closest_stats_device": (I, [P, P, U32, P, P, P, I, P]),
+    "myrt_render": (I, [P, C.POINTER(myrt_camera), C.POINTER(myrt_render_params)]),
+    "myrt_read_accumulation": (I, [P, P, P]),
+    "myrt_render_buffers": (I, [P, C.POINTER(P), C.POINTER(P)]),
+    "myrt_reset_accumulation": (I, [P]),
+    "myrt_sample_count": (I, [P, C.POINTER(C.c_uint32)]),
+    "myrt_set_seed": (I, [P, C.c_uint32]),
     "myrt_sync": (I, [P]),
 }
 

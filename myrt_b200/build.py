@@ -22,6 +22,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CUDA_FLAGS = ["-O3", "-lineinfo", "-std=c++20", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-Xptxas",
               "-warn-spills"]
 CXX_FLAGS = ["-O3", "-std=c++20", "-fPIC", "-pthread"]
+# Translation units whose arithmetic must round every + and * separately (the
+# shading restates GLSL expressions operation by operation).
+NO_FMA = {"wavefront.cu"}
 
 
 def sources() -> list[Path]:
@@ -44,7 +47,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     for src in sources():
         obj = BUILD / (src.name + ".o")
         if src.suffix == ".cu":
-            cmd = [NVCC, *ARCH, *CUDA_FLAGS, "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
+            extra = ["-fmad=false"] if src.name in NO_FMA else []
+            cmd = [NVCC, *ARCH, *CUDA_FLAGS, *extra, "-I", str(ROOT / "include"), "-c", str(src), "-o", str(obj)]
         else:
             cmd = ["g++", *CXX_FLAGS, "-I", str(ROOT / "include"), "-I", "/usr/local/cuda/include", "-c", str(src),
                    "-o", str(obj)]

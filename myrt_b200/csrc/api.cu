@@ -230,6 +230,7 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->aux_stream) cudaStreamSynchronize(ctx->aux_stream);
   free_scene(ctx->scene);
+  free_render(ctx->render);
   for (auto& p : ctx->stage) cudaFree(p);
   cudaFree(ctx->d_err);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -347,6 +348,7 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
     return rc;
   }
   s.valid = true;
+  ctx->render.sample_counter = 0;  // prepare() reported a change -> invalidate_counter
   return MYRT_OK;
 }
 
@@ -403,6 +405,65 @@ int myrt_trace_closest_stats_device(myrt_ctx* ctx, myrt_ray const* rays, uint32_
   a.stat_nodes = nodes;
   a.stat_tris = tris;
   return launch_trace(ctx, a, intersector, false, true, stream ? static_cast<cudaStream_t>(stream) : ctx->stream);
+}
+
+int myrt_render(myrt_ctx* ctx, myrt_camera const* camera, myrt_render_params const* p) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!camera || !p) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "null camera or params");
+  if (!ctx->scene.valid) return set_error(ctx, MYRT_ERR_NO_SCENE, "no scene uploaded");
+  if (p->width == 0 || p->height == 0 || uint64_t(p->width) * p->height > (uint64_t(1) << 30))
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "image size must be 1 .. 2^30 pixels");
+  if (p->num_bounces < 0 || p->num_bounces > 1024)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "num_bounces must be in [0, 1024]");
+  if (p->shading != MYRT_SHADE_REFERENCE) return set_error(ctx, MYRT_ERR_UNSUPPORTED, "unknown shading mode");
+  if (p->frames == 0) return MYRT_OK;
+  // set_view_matrix / set_projection_matrix: a changed camera restarts accumulation
+  render_state& R = ctx->render;
+  if (!R.have_camera || std::memcmp(R.last_camera, camera, sizeof(R.last_camera)) != 0) {
+    std::memcpy(R.last_camera, camera, sizeof(R.last_camera));
+    R.have_camera = true;
+    R.sample_counter = 0;
+  }
+  return render_reference_frames(ctx, camera, p);
+}
+
+int myrt_read_accumulation(myrt_ctx* ctx, float* rgba_sum, float* rgba_display) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  render_state const& R = ctx->render;
+  if (!R.accum) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "nothing rendered yet");
+  size_t const bytes = size_t(R.width) * R.height * 16;
+  int rc = MYRT_OK;
+  if (rgba_sum)
+    rc = check_cuda(ctx, cudaMemcpyAsync(rgba_sum, R.accum, bytes, cudaMemcpyDeviceToHost, ctx->stream), "read");
+  if (!rc && rgba_display)
+    rc = check_cuda(ctx, cudaMemcpyAsync(rgba_display, R.display, bytes, cudaMemcpyDeviceToHost, ctx->stream), "read");
+  if (rc) return rc;
+  return myrt_sync(ctx);
+}
+
+int myrt_render_buffers(myrt_ctx* ctx, void** accum, void** display) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  if (accum) *accum = ctx->render.accum;
+  if (display) *display = ctx->render.display;
+  return MYRT_OK;
+}
+
+int myrt_reset_accumulation(myrt_ctx* ctx) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  ctx->render.sample_counter = 0;
+  return MYRT_OK;
+}
+
+int myrt_sample_count(myrt_ctx* ctx, uint32_t* count) {
+  if (!ctx || !count) return MYRT_ERR_INVALID_ARGUMENT;
+  *count = ctx->render.sample_counter;
+  return MYRT_OK;
+}
+
+int myrt_set_seed(myrt_ctx* ctx, uint32_t seed) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  ctx->host_rng.seed(seed);
+  return MYRT_OK;
 }
 
 int myrt_sync(myrt_ctx* ctx) {

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -27,6 +28,22 @@ struct device_scene {
   bool valid = false;
 };
 
+// Wavefront render state (sequential_pathtracer's buffers and counters).
+struct render_state {
+  uint32_t width = 0, height = 0;
+  float4* gen[2] = {nullptr, nullptr};  // generate_output_t, 5 float4 per ray (ping-pong)
+  float4* trace = nullptr;              // trace_output_t, 4 float4 per ray
+  float4* accum = nullptr;              // debug_image: rgb sum, sample count in a
+  float4* display = nullptr;            // output_image: clamp(sum / count, 0, 4)
+  uint32_t* counts = nullptr;           // [2] active ray counts (ping-pong)
+  uint32_t* block_sums = nullptr;       // per-block survivor counts, then offsets
+  float* pass_tex = nullptr;            // frames * passes * 1024 random texture floats
+  size_t pass_tex_capacity = 0;         // in floats
+  uint32_t sample_counter = 0;          // frames accumulated since the last reset
+  float last_camera[32] = {};
+  bool have_camera = false;
+};
+
 }  // namespace myrt_b200
 
 struct myrt_ctx {
@@ -36,6 +53,8 @@ struct myrt_ctx {
   std::string last_error;
   uint32_t* d_err = nullptr;          // device error word (atomicOr of ERR_* bits)
   myrt_b200::device_scene scene;
+  myrt_b200::render_state render;
+  std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
   // staging buffers of the host-memory entry points (two chunk slots)
   void* stage[2] = {nullptr, nullptr};
   size_t stage_bytes = 0;
@@ -44,4 +63,6 @@ struct myrt_ctx {
 namespace myrt_b200 {
 int set_error(myrt_ctx* ctx, int code, std::string msg);
 int check_cuda(myrt_ctx* ctx, cudaError_t e, char const* what);
+void free_render(render_state& r);
+int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p);
 }  // namespace myrt_b200

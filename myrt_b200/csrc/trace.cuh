@@ -135,8 +135,9 @@ struct trace_args {
 __device__ __forceinline__ float q8(uint32_t w, int s) { return float((w >> (8 * (s & 3))) & 0xffu); }
 
 struct hit_rec {
-  int32_t prim;  // -1 = none
+  int32_t prim;   // -1 = none
   float t, u, v;
+  uint32_t leaf;  // index of the hit triangle in the leaf-ordered array
 };
 
 // Walks the tree for one ray. Closest hit (ANY = false): fills h and returns
@@ -158,6 +159,7 @@ __device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4
   float tbest = tmax;
   int32_t best = -1;
   float bu = 0.f, bv = 0.f;
+  uint32_t bleaf = 0;
   bool occluded = false;
 
   uint2 stack[MYRT_STACK_MAX];
@@ -253,6 +255,7 @@ __device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4
         best = prim;
         bu = u;
         bv = v;
+        bleaf = tgroup.x + b;
       }
     }
     if (ANY && occluded) break;
@@ -267,6 +270,7 @@ __device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4
   h.t = best >= 0 ? tbest : tmax;
   h.u = best >= 0 ? bu : 0.f;
   h.v = best >= 0 ? bv : 0.f;
+  h.leaf = bleaf;
   return best >= 0;
 }
 

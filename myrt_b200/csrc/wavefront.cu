@@ -1,0 +1,534 @@
+// Wavefront path tracing, "reference shading" mode: the reference's
+// generate -> {trace, color, filter} x bounces -> trace, color frame
+// (src/pathtracer/sequential_pathtracer.cpp:10-69, :282-498) as sm_100a kernels.
+//
+//   k_generate     pt_generate.comp:50-84
+//   k_trace_pass   pt_trace.comp:134-226, nearest_hit :331-386 (meshes), any_hit
+//                  :311-329 for the NEE shadow ray; both walk the 8-wide BVH
+//   k_color_pass   pt_color.comp:77-202 (sky gradient, no cubemap), plus a
+//                  per-block count of surviving rays for the compaction
+//   k_scan_blocks + k_scatter
+//                  pt_ray_filter.comp:49-64 as a STABLE compaction: survivors
+//                  keep their relative order, so slot ids (which feed the
+//                  random stream, pt_color.comp:134-135) are reproducible
+//
+// Ray state keeps the reference's record layouts: generate_output_t = 80 bytes
+// (five float4), trace_output_t = 64 bytes (four float4). The per-pass host
+// randomness (an int seed and a 1024-float texture per pass, drawn from
+// std::mt19937 in the reference's order) is generated for all frames of a
+// call up front and copied to the device once.
+//
+// Compiled with -fmad=false (see build.py): the shading arithmetic rounds every
+// operation as written, like the CPU oracle.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "../../include/myrt_cuda.h"
+#include "ctx.hpp"
+#include "refshade.cuh"
+#include "trace.cuh"
+
+namespace myrt_b200 {
+namespace {
+
+using rs::v2;
+using rs::v3;
+
+constexpr int kBlock = 256;
+constexpr int kTexSize = 1024;
+
+struct scene_dev {
+  uint4 const* nodes;
+  float4 const* tris;
+  float4 const* tri_normals;  // 3 per prim, may be null
+  float2 const* tri_uvs;      // 3 per prim, may be null
+  int32_t const* tri_material;
+  int2 const* mat_refs;  // (id, offset)
+  int n_mats;
+  float const* mat_data;
+  uint32_t* err;
+};
+
+struct camera_dev {
+  float vp[16];  // inverse_view * inverse_projection (column major), computed on the host
+  float eye[3];
+};
+
+struct light_t {
+  float px, py, pz, r, cx, cy, cz;
+};
+// pt_trace.comp:141-146 (float products, as the GLSL folds them)
+__constant__ light_t c_lights[2] = {
+    {2.f * 4.f, 2.f * 5.f, 2.f * 4.f, 1.5f, 6.f * 1.f, 6.f * 1.8f, 6.f * 3.f},
+    {2.f * -4.f, 2.f * 3.f, 2.f * 5.f, 1.5f, 8.f * 3.f, 8.f * 1.8f, 8.f * 1.f},
+};
+
+__device__ __forceinline__ v3 xyz(float4 a) { return {a.x, a.y, a.z}; }
+
+// intersect.glsl:30-39
+__device__ __forceinline__ float intersect_sphere(v3 r0, v3 rd, v3 s0, float sr) {
+  float const a = rs::dot(rd, rd);
+  v3 const s0_r0 = r0 - s0;
+  float const b = 2.f * rs::dot(rd, s0_r0);
+  float const c = rs::dot(s0_r0, s0_r0) - (sr * sr);
+  if (b * b - 4.f * a * c < 0.f) return -1.f;
+  return (-b - sqrtf((b * b) - 4.f * a * c)) / (2.f * a);
+}
+
+// ---- pt_generate.comp -----------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_generate(uint32_t W, uint32_t H, float const* __restrict__ tex, int seed,
+    camera_dev cam, float4* __restrict__ gen, uint32_t* __restrict__ count) {
+  uint32_t const id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id == 0) *count = W * H;
+  if (id >= W * H) return;
+  int const x = int(id % W), y = int(id / W);
+  rs::rng_t r;
+  rs::random_init(r, tex, x, y, seed);
+  // random_uniform_circle(0.7071067812) (random.glsl:77-85)
+  float const a = rs::random_next(r) * 2.f * 3.1415926535897f;
+  float const b = rs::random_next(r);
+  float const s = sqrtf(b) * 0.7071067812f;
+  v2 const off{s * sinf(a), s * cosf(a)};
+  float const nx = ((off.x + float(x)) / float(W)) * 2.f - 1.f;
+  float const ny = ((off.y + float(y)) / float(H)) * 2.f - 1.f;
+  float h[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    h[k] = ((cam.vp[0 * 4 + k] * nx + cam.vp[1 * 4 + k] * ny) + cam.vp[2 * 4 + k] * 1.f) + cam.vp[3 * 4 + k] * 1.f;
+  v3 const dir = rs::normalize(v3{h[0], h[1], h[2]});
+  float const rv = rs::random_next(r);
+  float4* g = gen + 5 * size_t(id);
+  g[0] = make_float4(cam.eye[0], cam.eye[1], cam.eye[2], rv);
+  g[1] = make_float4(dir.x, dir.y, dir.z, float(x));
+  g[2] = make_float4(1.f, 1.f, 1.f, float(y));
+  g[3] = make_float4(0.f, 0.f, 0.f, 0.f);
+  g[4] = make_float4(1.f, 1.f, 0.f, 0.f);
+}
+
+// ---- pt_trace.comp --------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, float const* __restrict__ tex, int seed,
+    float4 const* __restrict__ gen, float4* __restrict__ trace, uint32_t const* __restrict__ count) {
+  uint32_t const id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= *count) return;
+  float4 const g0 = gen[5 * size_t(id) + 0];
+  float4 const g1 = gen[5 * size_t(id) + 1];
+  float4 const g2 = gen[5 * size_t(id) + 2];
+  v3 const ro = xyz(g0), rd = xyz(g1);
+  rs::rng_t r;
+  rs::random_init(r, tex, rs::f2i(g1.w), rs::f2i(g2.w), seed);
+  int const li = min(max(rs::f2i(2.f * rs::random_next(r)), 0), 1);
+  float const rx = rs::random_next(r);
+  float const ry = rs::random_next(r);
+  float const rz = rs::random_next(r);
+  float const rq = rs::random_next(r);
+  light_t const L = c_lights[li];
+  v3 const p_on_light = v3{L.px, L.py, L.pz} + rs::normalize(v3{rx, ry, rz}) * L.r * sqrtf(rq);
+
+  hit_rec h;
+  uint32_t cn = 0, ct = 0;
+  bool hits = traverse<0, false, false>(s.nodes, s.tris, f3{ro.x, ro.y, ro.z}, f3{rd.x, rd.y, rd.z}, 0.f,
+      __int_as_float(0x7f800000), h, s.err, cn, ct);
+  float ht = h.t;
+  int hits_light = -1;
+  v3 position{0.f, 0.f, 0.f}, normal{0.f, 0.f, 0.f};
+  v2 uv{0.f, 0.f};
+  int material = 0;
+  if (hits) {
+    float4 const* tp = s.tris + 3 * size_t(h.leaf);
+    v3 const p0 = xyz(__ldg(tp)), p1 = xyz(__ldg(tp + 1)), p2 = xyz(__ldg(tp + 2));
+    float const bx = h.u, by = h.v;
+    float const w = (1.f - bx) - by;
+    position = (bx * p1 + by * p2) + w * p0;
+    uint32_t const prim = uint32_t(h.prim);
+    if (s.tri_normals) {
+      v3 const n0 = xyz(__ldg(s.tri_normals + 3 * size_t(prim))), n1 = xyz(__ldg(s.tri_normals + 3 * size_t(prim) + 1)),
+               n2 = xyz(__ldg(s.tri_normals + 3 * size_t(prim) + 2));
+      normal = rs::normalize((bx * n1 + by * n2) + w * n0);
+    } else {
+      normal = rs::normalize(rs::cross(rs::normalize(p1 - p0), rs::normalize(p2 - p0)));
+    }
+    if (s.tri_uvs) {
+      float2 const u0 = __ldg(s.tri_uvs + 3 * size_t(prim)), u1 = __ldg(s.tri_uvs + 3 * size_t(prim) + 1),
+                   u2 = __ldg(s.tri_uvs + 3 * size_t(prim) + 2);
+      uv = {(bx * u1.x + by * u2.x) + w * u0.x, (bx * u1.y + by * u2.y) + w * u0.y};
+    }
+    material = __ldg(s.tri_material + prim);
+  }
+#pragma unroll
+  for (int l = 0; l < 2; ++l) {
+    float const tl = intersect_sphere(ro, rd, v3{c_lights[l].px, c_lights[l].py, c_lights[l].pz}, c_lights[l].r);
+    if (tl > 0.f && (!hits || tl < ht)) {
+      hits = true;
+      ht = tl;
+      hits_light = l;
+    }
+  }
+  int intersects = 0;
+  uint32_t light_color = 0;
+  v3 light_dir{0.f, 0.f, 0.f};
+  float light_strength = 0.f;
+  if (hits) {
+    intersects = 1;
+    if (rs::inf3(normal) || rs::nan3(normal)) intersects = 0;
+    v3 const path = p_on_light - position;
+    v3 const dir_l = rs::normalize(path);
+    float const dist_l = rs::length(path);
+    v3 const lnorm = rs::faceforward(normal, rd, normal);
+    if (hits_light >= 0) {
+      intersects = 2;
+      v3 const col{c_lights[hits_light].cx, c_lights[hits_light].cy, c_lights[hits_light].cz};
+      light_strength = rs::length(col);
+      light_color = rs::pack_unorm4x8(col.x / light_strength, col.y / light_strength, col.z / light_strength,
+          0.f / light_strength);
+      light_dir = dir_l;
+    } else if (rs::dot(dir_l, lnorm) > 0.f) {
+      v3 const so = position + lnorm * 0.01f;
+      hit_rec hs;
+      bool const occluded = traverse<0, true, false>(s.nodes, s.tris, f3{so.x, so.y, so.z},
+          f3{dir_l.x, dir_l.y, dir_l.z}, 0.f, dist_l, hs, s.err, cn, ct);
+      if (!occluded) {
+        v3 const col{L.cx, L.cy, L.cz};
+        light_strength = rs::length(col);
+        light_color = rs::pack_unorm4x8(col.x / light_strength, col.y / light_strength, col.z / light_strength,
+            0.f / light_strength);
+        light_strength = light_strength * (2.f / dist_l);
+        light_dir = dir_l;
+      }
+    }
+  } else {
+    position = {0.f, 0.f, 0.f};
+    normal = {0.f, 0.f, 0.f};
+  }
+  float4* t = trace + 4 * size_t(id);
+  t[0] = make_float4(position.x, position.y, position.z, __int_as_float(intersects));
+  t[1] = make_float4(normal.x, normal.y, normal.z, __uint_as_float(id));
+  t[2] = make_float4(uv.x, uv.y, __int_as_float(material), __uint_as_float(light_color));
+  t[3] = make_float4(light_dir.x, light_dir.y, light_dir.z, light_strength);
+}
+
+// ---- pt_color.comp ----------------------------------------------------------------
+struct color_args {
+  int2 const* mat_refs;
+  int n_mats;
+  float const* mat_data;
+  float4* accum;
+  float4* display;
+  uint32_t W;
+  uint32_t sample_index;
+  int force;
+};
+
+__device__ __forceinline__ bool naninf4(float4 v) {
+  return isnan(v.x) || isnan(v.y) || isnan(v.z) || isnan(v.w) || isinf(v.x) || isinf(v.y) || isinf(v.z) ||
+      isinf(v.w);
+}
+
+// pt_color.comp:77-101
+__device__ __forceinline__ void accumulate(color_args const& a, float4 nc, int px, int py) {
+  size_t const pi = size_t(py) * a.W + size_t(px);
+  float4 last = a.accum[pi];
+  if (naninf4(nc)) nc = last;
+  float4 const actual_last = last;
+  if (a.sample_index == 0) last = make_float4(nc.x, nc.y, nc.z, 1.f);
+  else last = make_float4(last.x + nc.x, last.y + nc.y, last.z + nc.z, last.w + 1.f);
+  if (naninf4(last)) last = actual_last;
+  a.accum[pi] = last;
+  a.display[pi] = make_float4(rs::gclamp(last.x / last.w, 0.f, 4.f), rs::gclamp(last.y / last.w, 0.f, 4.f),
+      rs::gclamp(last.z / last.w, 0.f, 4.f), 1.f);
+}
+
+__global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, float const* __restrict__ tex, int seed,
+    float4* __restrict__ gen, float4* __restrict__ trace, uint32_t const* __restrict__ count,
+    uint32_t* __restrict__ block_sums) {
+  uint32_t const id = blockIdx.x * blockDim.x + threadIdx.x;
+  bool keep = false;
+  if (id < *count) {
+    float4* gp = gen + 5 * size_t(id);
+    float4* tp = trace + 4 * size_t(id);
+    float4 const t0 = tp[0], t1 = tp[1], t2 = tp[2], t3 = tp[3];
+    float4 g0 = gp[0], g1 = gp[1], g2 = gp[2], g3 = gp[3], g4 = gp[4];
+    int const intersects = __float_as_int(t0.w);
+    int const px = rs::f2i(g1.w), py = rs::f2i(g2.w);
+    v3 const refl0 = xyz(g2);
+    float const pdf0 = g4.x;
+    if (intersects != 0) {
+      if (intersects == 2) {
+        reinterpret_cast<int*>(tp)[3] = 0;
+        v3 const lc = rs::unpack_rgb(__float_as_uint(t2.w));
+        v3 const c = lc * t3.w * refl0 / pdf0;
+        accumulate(a, make_float4(c.x + g3.x, c.y + g3.y, c.z + g3.z, 1.f + g3.w), px, py);
+      } else {
+        v3 const normal = xyz(t1);
+        rs::rng_t r;
+        rs::random_init(r, tex, px, py, seed);
+        uint32_t const uid = id;
+        float const rvin = g0.w;
+        rs::random_value(r, int(uint32_t(rs::f2i(56128966.f * rvin)) + 20945293u * uid));
+        rs::random_value(r, int(uint32_t(rs::f2i(12233432.f * rvin)) + 74867839u * uid));
+        rs::material_ctx mc;
+        int const mi = __float_as_int(t2.z);
+        bool const valid = mi >= 0 && mi < a.n_mats;
+        int2 const ref = valid ? __ldg(a.mat_refs + mi) : make_int2(-1, 0);
+        rs::mat_open(mc, ref.x, a.mat_data, ref.y);
+        float const m0 = rs::random_next(r);
+        float const m1 = rs::random_next(r);
+        v3 const dir = xyz(g1);
+        v3 const generated = rs::mat_bounce(mc, r, v2{m0, m1}, -dir, normal);
+        v3 mrefl;
+        float mpdf;
+        rs::mat_evaluate(mc, normal, generated, -dir, mrefl, mpdf);
+        float const rnd = rs::random_next(r);
+        bool done = false;
+        if (rnd > pdf0 * 1.f) {
+          reinterpret_cast<int*>(tp)[3] = 0;
+          v3 const c = refl0 / pdf0;
+          accumulate(a, make_float4(g3.x + c.x, g3.y + c.y, g3.z + c.z, g3.w), px, py);
+          done = true;
+        } else if (a.force || pdf0 < 1e-5f || mpdf < 1e-6f || isnan(mpdf) || isinf(mpdf) || rs::nan3(mrefl) ||
+                   rs::inf3(mrefl) || rs::nan3(generated) || rs::inf3(generated)) {
+          reinterpret_cast<int*>(tp)[3] = 0;
+          if (rs::nan3(mrefl) || rs::inf3(mrefl) || isnan(pdf0) || isinf(pdf0) || pdf0 < 1e-5f) {
+            accumulate(a, g3, px, py);
+          } else {
+            v3 const c = refl0 / pdf0;
+            accumulate(a, make_float4(g3.x + c.x, g3.y + c.y, g3.z + c.z, g3.w), px, py);
+          }
+          done = true;
+        }
+        if (!done) {
+          if (t3.w > 0.f) {
+            v3 lrefl{1.f, 1.f, 1.f};
+            float lpdf = 1.f;
+            rs::mat_evaluate(mc, normal, xyz(t3), -dir, lrefl, lpdf);
+            if (!rs::inf3(lrefl)) {
+              v3 const lc = rs::unpack_rgb(__float_as_uint(t2.w));
+              v3 const c = lc * t3.w * rs::clamp3(lrefl, 0.f, 1.f);
+              g3 = make_float4(g3.x + c.x, g3.y + c.y, g3.z + c.z, g3.w);
+            }
+          }
+          v3 const origin = xyz(t0) + 1e-4f * rs::faceforward(normal, -generated, normal);
+          float const pdf1 = pdf0 * mpdf;
+          v3 const refl1 = refl0 * mrefl;
+          // the literal 2341335623 is an int with that bit pattern in GLSL: -1953631673
+          float const rv1 = rs::random_value(r, int(uint32_t(rs::f2i(-1953631673.f * rvin)) + 357883444u * uid));
+          gp[0] = make_float4(origin.x, origin.y, origin.z, rv1);
+          gp[1] = make_float4(generated.x, generated.y, generated.z, g1.w);
+          gp[2] = make_float4(refl1.x, refl1.y, refl1.z, g2.w);
+          gp[3] = g3;
+          gp[4] = make_float4(pdf1, g4.y, g4.z, g4.w);
+          keep = true;
+        }
+      }
+    } else {
+      v3 const dir = xyz(g1);
+      float const t = (dir.y + 1.f) / 2.f;
+      v3 const sky = rs::mix3(v3{0.3f, 0.4f, 0.5f}, v3{1.f, 0.98f, 0.96f}, t);
+      v3 const env = rs::clamp3(refl0 * sky / pdf0, 0.f, 16.f);
+      accumulate(a, make_float4(g3.x + env.x, g3.y + env.y, g3.z + env.z, g3.w), px, py);
+    }
+  }
+  int const c = __syncthreads_count(keep);
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = uint32_t(c);
+}
+
+// ---- pt_ray_filter.comp (stable) ---------------------------------------------------
+// Exclusive scan of the per-block survivor counts (one block), total -> *new_count.
+__global__ void __launch_bounds__(1024) k_scan_blocks(uint32_t* __restrict__ sums, uint32_t nblocks,
+    uint32_t* __restrict__ new_count) {
+  __shared__ uint32_t warp_tot[32];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  uint32_t const lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  for (uint32_t base = 0; base < nblocks; base += 1024) {
+    uint32_t const i = base + threadIdx.x;
+    uint32_t const v = i < nblocks ? sums[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t const y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= uint32_t(o)) x += y;
+    }
+    if (lane == 31) warp_tot[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t w = warp_tot[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t const y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= uint32_t(o)) w += y;
+      }
+      warp_tot[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    uint32_t const excl = carry + (warp ? warp_tot[warp - 1] : 0u) + x - v;
+    if (i < nblocks) sums[i] = excl;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += warp_tot[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *new_count = carry;
+}
+
+__global__ void __launch_bounds__(kBlock) k_scatter(float4 const* __restrict__ gen_in, float4 const* __restrict__ trace,
+    uint32_t const* __restrict__ count, uint32_t const* __restrict__ offsets, float4* __restrict__ gen_out) {
+  __shared__ uint32_t warp_cnt[kBlock / 32];
+  uint32_t const id = blockIdx.x * blockDim.x + threadIdx.x;
+  bool const keep = id < *count && __float_as_int(trace[4 * size_t(id)].w) == 1;
+  uint32_t const lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t const ballot = __ballot_sync(0xffffffffu, keep);
+  if (lane == 0) warp_cnt[warp] = __popc(ballot);
+  __syncthreads();
+  uint32_t before = 0;
+  for (uint32_t w = 0; w < warp; ++w) before += warp_cnt[w];
+  if (keep) {
+    uint32_t const dst = offsets[blockIdx.x] + before + __popc(ballot & ((1u << lane) - 1u));
+    uint32_t const src = __float_as_uint(trace[4 * size_t(id) + 1].w);  // generated_ray
+#pragma unroll
+    for (int k = 0; k < 5; ++k) gen_out[5 * size_t(dst) + k] = gen_in[5 * size_t(src) + k];
+  }
+}
+
+// ---- host side ----------------------------------------------------------------------
+int ensure_render_buffers(myrt_ctx* ctx, uint32_t W, uint32_t H) {
+  render_state& R = ctx->render;
+  if (R.width == W && R.height == H && R.accum) return MYRT_OK;
+  free_render(R);
+  size_t const n = size_t(W) * H;
+  size_t const nb = (n + kBlock - 1) / kBlock;
+  int rc = MYRT_OK;
+  auto alloc = [&](void** p, size_t bytes, char const* what) {
+    if (!rc) rc = check_cuda(ctx, cudaMalloc(p, bytes), what);
+  };
+  alloc(reinterpret_cast<void**>(&R.gen[0]), n * 80, "ray state");
+  alloc(reinterpret_cast<void**>(&R.gen[1]), n * 80, "ray state");
+  alloc(reinterpret_cast<void**>(&R.trace), n * 64, "trace state");
+  alloc(reinterpret_cast<void**>(&R.accum), n * 16, "accumulation image");
+  alloc(reinterpret_cast<void**>(&R.display), n * 16, "display image");
+  alloc(reinterpret_cast<void**>(&R.counts), 2 * sizeof(uint32_t), "ray counts");
+  alloc(reinterpret_cast<void**>(&R.block_sums), std::max<size_t>(nb, 1) * sizeof(uint32_t), "block sums");
+  if (!rc) rc = check_cuda(ctx, cudaMemsetAsync(R.accum, 0, n * 16, ctx->stream), "clear");
+  if (!rc) rc = check_cuda(ctx, cudaMemsetAsync(R.display, 0, n * 16, ctx->stream), "clear");
+  if (rc) {
+    free_render(R);
+    return rc;
+  }
+  R.width = W;
+  R.height = H;
+  R.sample_counter = 0;  // invalidate_texture -> invalidate_counter
+  return MYRT_OK;
+}
+
+void mat_mul4(float const* a, float const* b, float* out) {
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r)
+      out[c * 4 + r] = ((a[0 * 4 + r] * b[c * 4 + 0] + a[1 * 4 + r] * b[c * 4 + 1]) + a[2 * 4 + r] * b[c * 4 + 2]) +
+          a[3 * 4 + r] * b[c * 4 + 3];
+}
+
+}  // namespace
+
+void free_render(render_state& R) {
+  cudaFree(R.gen[0]);
+  cudaFree(R.gen[1]);
+  cudaFree(R.trace);
+  cudaFree(R.accum);
+  cudaFree(R.display);
+  cudaFree(R.counts);
+  cudaFree(R.block_sums);
+  cudaFree(R.pass_tex);
+  R = render_state{};
+}
+
+// Host random stream of sequential_pathtracer.cpp:282-498 for `frames` frames:
+// pass_generate draws its int seed then the 1024 texture floats, pass_trace
+// likewise, pass_color the floats first and then the int.
+void draw_host_randomness(std::mt19937& rng, int frames, int bounces, std::vector<int>& seeds, std::vector<float>& tex) {
+  int const passes = 2 * bounces + 3;
+  seeds.resize(size_t(frames) * passes);
+  tex.resize(size_t(frames) * passes * kTexSize);
+  for (int f = 0; f < frames; ++f) {
+    for (int p = 0; p < passes; ++p) {
+      std::uniform_int_distribution<> dist;
+      std::uniform_real_distribution<float> uni(0.f, 1.f);
+      bool const is_color = p >= 1 && ((p - 1) % 2 == 1);
+      int& s = seeds[size_t(f) * passes + p];
+      float* t = tex.data() + (size_t(f) * passes + p) * kTexSize;
+      if (!is_color) s = dist(rng);
+      for (int k = 0; k < kTexSize; ++k) t[k] = uni(rng);
+      if (is_color) s = dist(rng);
+    }
+  }
+}
+
+int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p) {
+  uint32_t const W = p->width, H = p->height;
+  int rc = ensure_render_buffers(ctx, W, H);
+  if (rc) return rc;
+  render_state& R = ctx->render;
+  device_scene const& S = ctx->scene;
+  int const B = p->num_bounces;
+  int const F = int(p->frames);
+  int const passes = 2 * B + 3;
+  std::vector<int> seeds;
+  std::vector<float> tex;
+  draw_host_randomness(ctx->host_rng, F, B, seeds, tex);
+  if (R.pass_tex_capacity < tex.size()) {
+    cudaFree(R.pass_tex);
+    R.pass_tex = nullptr;
+    R.pass_tex_capacity = 0;
+    rc = check_cuda(ctx, cudaMalloc(&R.pass_tex, tex.size() * sizeof(float)), "pass randomness");
+    if (rc) return rc;
+    R.pass_tex_capacity = tex.size();
+  }
+  rc = check_cuda(ctx,
+      cudaMemcpyAsync(R.pass_tex, tex.data(), tex.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->stream),
+      "pass randomness upload");
+  if (rc) return rc;
+
+  camera_dev cd{};
+  mat_mul4(cam->inverse_view, cam->inverse_projection, cd.vp);
+  cd.eye[0] = cam->inverse_view[12];
+  cd.eye[1] = cam->inverse_view[13];
+  cd.eye[2] = cam->inverse_view[14];
+  scene_dev sd{S.nodes, S.tris, S.tri_normals, S.tri_uvs, S.tri_material,
+      reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err};
+  color_args ca{reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, R.accum, R.display, W,
+      0, 0};
+  size_t const n = size_t(W) * H;
+  uint32_t const nb = uint32_t((n + kBlock - 1) / kBlock);
+  cudaStream_t const st = ctx->stream;
+  for (int f = 0; f < F; ++f) {
+    auto tex_of = [&](int pass) { return R.pass_tex + (size_t(f) * passes + pass) * kTexSize; };
+    auto seed_of = [&](int pass) { return seeds[size_t(f) * passes + pass]; };
+    int cur = 0;
+    ca.sample_index = R.sample_counter;
+    k_generate<<<nb, kBlock, 0, st>>>(W, H, tex_of(0), seed_of(0), cd, R.gen[cur], R.counts + cur);
+    int pass = 1;
+    for (int i = 0; i <= B; ++i) {
+      bool const last = i == B;
+      k_trace_pass<<<nb, kBlock, 0, st>>>(sd, tex_of(pass), seed_of(pass), R.gen[cur], R.trace, R.counts + cur);
+      ++pass;
+      ca.force = last ? 1 : 0;
+      k_color_pass<<<nb, kBlock, 0, st>>>(ca, tex_of(pass), seed_of(pass), R.gen[cur], R.trace, R.counts + cur,
+          R.block_sums);
+      ++pass;
+      if (!last) {
+        k_scan_blocks<<<1, 1024, 0, st>>>(R.block_sums, nb, R.counts + (1 - cur));
+        k_scatter<<<nb, kBlock, 0, st>>>(R.gen[cur], R.trace, R.counts + cur, R.block_sums, R.gen[1 - cur]);
+        cur = 1 - cur;
+      }
+    }
+    rc = check_cuda(ctx, cudaGetLastError(), "wavefront launch");
+    if (rc) return rc;
+    ++R.sample_counter;
+  }
+  return MYRT_OK;
+}
+
+}  // namespace myrt_b200

@@ -44,6 +44,34 @@ _PARAM_REF = re.compile(r"\b(?:inout|out)\s+([A-Za-z_]\w*)\s+([A-Za-z_]\w*)")
 _GLOBAL_VAR = re.compile(r"^(int|bool|float|uint|random_state_t|material_state_t)(\s+\w+\s*(?:=[^;]*)?;)", re.M)
 
 
+# GLSL evaluates function arguments left to right (GLSL 4.60, 6.1.1); C++ leaves
+# the order unspecified and g++ goes right to left. Where one argument list holds
+# several draws from the random stream, the draws are hoisted into temporaries in
+# source order. Each pattern must match exactly (count given), so a change in the
+# reference fails the build instead of silently reordering.
+ORDER_FIXES = {
+    "random.glsl": [
+        (r"int seed_base = int\(random_int\((pixel\.x \^ 0xba77fa)\) \* random_primes\[0\] \+ "
+         r"random_int\((pixel\.y \^ 0xcca6df)\) \* random_primes\[1\] \+ random_int\(start_seed\)\);",
+         r"int _r0 = random_int(\1); int _r1 = random_int(\2); int _r2 = random_int(start_seed); "
+         r"int seed_base = int(_r0 * random_primes[0] + _r1 * random_primes[1] + _r2);", 2),
+        (r"return vec2\(random_next\(\), random_next\(\)\);",
+         r"float _a = random_next(); float _b = random_next(); return vec2(_a, _b);", 1),
+        (r"return vec3\(random_next\(\), random_next\(\), random_next\(\)\);",
+         r"float _a = random_next(); float _b = random_next(); float _c = random_next(); return vec3(_a, _b, _c);", 1),
+        (r"vec2 rands = vec2\(\s*random_next\(\) \* 2 \* (3\.1415926535897f),\s*random_next\(\)\s*\);",
+         r"float _a = random_next() * 2 * \1; float _b = random_next(); vec2 rands = vec2(_a, _b);", 1),
+    ],
+}
+
+
+def fix_evaluation_order(name: str, src: str) -> str:
+    for pat, rep, count in ORDER_FIXES.get(name, []):
+        src, n = re.subn(pat, rep, src)
+        assert n == count, f"{name}: evaluation-order rewrite matched {n} times, expected {count}: {pat}"
+    return src
+
+
 def glsl_to_cpp(src: str) -> str:
     src = re.sub(r"\bconst\s+in\s+", "const ", src)
     src = _PARAM_REF.sub(r"\1& \2", src)
@@ -78,7 +106,8 @@ def write_sources() -> None:
     assert bvh_src.count(needle) == 1, "bvh.cpp:136 no longer has the expected qualifier"
     (OUT / "src/bvh.cpp").write_text(bvh_src.replace(needle, "std::vector<aabb_t> generate_triangle_bounds("))
     for name in GLSL_FILES:
-        (OUT / "glsl" / name).write_text(glsl_to_cpp((REF_ROOT / "src/pt" / name).read_text()))
+        src = glsl_to_cpp((REF_ROOT / "src/pt" / name).read_text())
+        (OUT / "glsl" / name).write_text(fix_evaluation_order(name, src))
     (OUT / "glsl/material_new.glsl").write_text(material_codegen((REF_ROOT / "src/pt/material_new.glsl").read_text()))
     trace = (REF_ROOT / "src/pt/pt_trace.comp").read_text()
     (OUT / "glsl/pt_trace_visitor.glsl").write_text(extract_trace_visitor(trace))

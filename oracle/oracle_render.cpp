@@ -1,0 +1,821 @@
+// CPU oracle, part 2: the reference's wavefront passes in "reference shading"
+// mode, restated from the GLSL and the C++ pass driver.
+//
+// TEST INFRASTRUCTURE ONLY (checker for the device wavefront). Built into
+// liboracle.so with -ffp-contract=off -fwrapv.
+//
+// Follows, function by function:
+//   random.glsl:14-85            rng_* (with the evaluation order GLSL defines:
+//                                arguments left to right)
+//   ggx.glsl:9-43, pbr.glsl:29-232, transform.glsl:3-15, color.glsl,
+//   material_new.glsl:14-49 and the dispatch material_registry::generate_code
+//   emits (material.hpp:39-65) for the single PBR type
+//   pt_generate.comp:50-84       pass_generate
+//   pt_trace.comp:134-226, :331-386 (meshes; no SDF drawables)  pass_trace
+//   pt_color.comp:77-202         pass_color (no cubemap: sky gradient)
+//   pt_ray_filter.comp:49-64     pass_filter, as a STABLE compaction (slot order
+//                                = serial order; the reference's atomicAdd order
+//                                is not reproducible)
+//   sequential_pathtracer.cpp:10-69, :282-498  frame driver and the host random
+//                                stream (std::mt19937 + std distributions, in the
+//                                order the passes draw them)
+// Scene: world-space triangles with per-corner normals / uvs, one material index
+// per triangle. Closest / any hit come from the restated reference BVH
+// (oracle.cpp) with canonical ties; see orc_refbvh_* there.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <random>
+#include <thread>
+#include <vector>
+
+namespace {
+
+struct v2 {
+  float x, y;
+};
+struct v3 {
+  float x, y, z;
+};
+struct v4 {
+  float x, y, z, w;
+};
+inline v3 operator+(v3 a, v3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline v3 operator-(v3 a, v3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline v3 operator-(v3 a) { return {-a.x, -a.y, -a.z}; }
+inline v3 operator*(v3 a, v3 b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+inline v3 operator*(v3 a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+inline v3 operator*(float s, v3 a) { return {s * a.x, s * a.y, s * a.z}; }
+inline v3 operator/(v3 a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+inline float dot(v3 a, v3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+inline v3 cross(v3 a, v3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline float length(v3 v) { return std::sqrt(dot(v, v)); }
+inline v3 normalize(v3 v) { return v * (1.f / length(v)); }
+// GLSL min/max/clamp (NaN goes to the first operand's side as the ternary does)
+inline float gmin(float a, float b) { return b < a ? b : a; }
+inline float gmax(float a, float b) { return a < b ? b : a; }
+inline float gclamp(float v, float lo, float hi) { return gmin(gmax(v, lo), hi); }
+inline v3 clamp3(v3 v, float lo, float hi) { return {gclamp(v.x, lo, hi), gclamp(v.y, lo, hi), gclamp(v.z, lo, hi)}; }
+inline float mixf(float a, float b, float t) { return a * (1.f - t) + b * t; }
+inline v3 mix3(v3 a, v3 b, float t) { return a * (1.f - t) + b * t; }
+inline bool nan3(v3 v) { return std::isnan(v.x) || std::isnan(v.y) || std::isnan(v.z); }
+inline bool inf3(v3 v) { return std::isinf(v.x) || std::isinf(v.y) || std::isinf(v.z); }
+inline bool naninf4(v4 v) {
+  return std::isnan(v.x) || std::isnan(v.y) || std::isnan(v.z) || std::isnan(v.w) || std::isinf(v.x) ||
+      std::isinf(v.y) || std::isinf(v.z) || std::isinf(v.w);
+}
+inline float signf(float v) { return v > 0.f ? 1.f : (v < 0.f ? -1.f : 0.f); }
+inline v3 faceforward(v3 n, v3 i, v3 nref) { return dot(nref, i) < 0.f ? n : -n; }
+inline v3 reflect(v3 i, v3 n) { return i - 2.f * dot(n, i) * n; }
+inline v3 refract(v3 i, v3 n, float eta) {
+  float const k = 1.f - eta * eta * (1.f - dot(n, i) * dot(n, i));
+  if (k < 0.f) return {0.f, 0.f, 0.f};
+  return eta * i - (eta * dot(n, i) + std::sqrt(k)) * n;
+}
+
+// float -> int with the x86 out-of-range result (INT_MIN), the behaviour the
+// reference build on x86 has for int(float) of values >= 2^31.
+inline int f2i(float f) {
+  if (!(f > -2147483648.0f && f < 2147483648.0f)) return std::numeric_limits<int>::min();
+  return int(f);
+}
+inline std::uint32_t f2u(float f) { return std::uint32_t(f2i(f)); }
+
+inline std::uint32_t pack_unorm4x8(v4 c) {
+  float const v[4] = {c.x, c.y, c.z, c.w};
+  std::uint32_t r = 0;
+  for (int i = 0; i < 4; ++i) r |= std::uint32_t(std::nearbyint(gclamp(v[i], 0.f, 1.f) * 255.f)) << (8 * i);
+  return r;
+}
+inline v4 unpack_unorm4x8(std::uint32_t p) {
+  return {float(p & 0xffu) / 255.f, float((p >> 8) & 0xffu) / 255.f, float((p >> 16) & 0xffu) / 255.f,
+      float((p >> 24) & 0xffu) / 255.f};
+}
+
+// ---- random.glsl -------------------------------------------------------------
+struct rng_t {
+  std::uint32_t state = 0;
+  int prime = 0;
+  float const* tex = nullptr;
+  int tex_size = 0;
+};
+constexpr int kPrimes[6] = {69019, 96013, 32159, 22783, 87011, 45263};
+inline std::uint32_t wang(std::uint32_t a) {
+  a = (a ^ 61u) ^ (a >> 16);
+  a = a + (a << 3);
+  a = a ^ (a >> 4);
+  a = a * 0x27d4eb2du;
+  a = a ^ (a >> 15);
+  return a;
+}
+inline std::uint32_t xorshift(rng_t& r) {
+  r.state ^= (r.state << 13);
+  r.state ^= (r.state >> 17);
+  r.state ^= (r.state << 5);
+  return r.state;
+}
+inline float random_value(rng_t& r, int seed) {
+  r.state += wang(std::uint32_t(seed));
+  return gclamp(float(xorshift(r)) * (1.f / float(0xFFFFFFFFu)), 0.f, 1.f);
+}
+inline int random_int(rng_t& r, int seed) { return f2i(random_value(r, seed) * float(0x7fffffff)); }
+inline float texel(rng_t const& r, int i) { return (i < 0 || i >= r.tex_size) ? 0.f : r.tex[i]; }
+inline void random_init(rng_t& r, float const* tex, int tex_size, int px, int py, int seed) {
+  r.state = std::uint32_t(seed);
+  r.prime = 0;
+  r.tex = tex;
+  r.tex_size = tex_size;
+  int const a = random_int(r, px ^ 0xba77fa);
+  int const b = random_int(r, py ^ 0xcca6df);
+  int const c = random_int(r, seed);
+  int const seed_base = int(std::uint32_t(a) * std::uint32_t(kPrimes[0]) + std::uint32_t(b) * std::uint32_t(kPrimes[1]) +
+      std::uint32_t(c));
+  random_value(r, int(std::uint32_t(seed_base) + std::uint32_t(f2i(float(0xffaf86) * texel(r, seed_base % tex_size)))));
+}
+inline float random_next(rng_t& r) {
+  r.prime = (r.prime + 1) % 6;
+  return random_value(r, r.prime);
+}
+inline v2 random_uniform_circle(rng_t& r, float radius) {
+  float const a = random_next(r) * 2.f * 3.1415926535897f;
+  float const b = random_next(r);
+  float const s = std::sqrt(b) * radius;
+  return {s * std::sin(a), s * std::cos(a)};
+}
+
+// ---- ggx.glsl / pbr.glsl / transform.glsl -------------------------------------
+constexpr float kPi = 3.1415926535897f;
+inline float ggx_distribution(v3 n, v3 h, float alpha) {
+  float const ndotm = dot(n, h);
+  float const a2 = alpha * alpha;
+  float const den = ndotm * ndotm * (a2 - 1.f) + 1.f;
+  return a2 / (kPi * den * den);
+}
+inline v2 ggx_importance_sample(v2 rs, float roughness) {
+  float const phi = rs.y * 2.f * kPi;
+  float const rough2 = roughness * roughness;
+  float const theta = std::atan(std::sqrt(rough2 * rs.x / (1.f - rs.x)));
+  return {phi, theta};
+}
+inline v3 sample_hemisphere(v2 is) {
+  float const c = std::cos(is.y), s = std::sin(is.y);
+  return {s * std::cos(is.x), s * std::sin(is.x), c};
+}
+inline v3 transform_local_to_world(v3 v, v3 n) {
+  v3 perp{1.f, 0.f, 0.f};
+  v3 u = normalize(cross(n, perp));
+  for (int i = 1; nan3(u) && i < 3; ++i) {
+    float* p = &perp.x;
+    p[i - 1] = 0.f;
+    p[i] = 1.f;
+    u = normalize(cross(n, perp));
+  }
+  v3 const c = cross(n, u);
+  v3 const r{(u.x * v.x + c.x * v.y) + n.x * v.z, (u.y * v.x + c.y * v.y) + n.y * v.z, (u.z * v.x + c.z * v.y) + n.z * v.z};
+  return normalize(r);
+}
+inline float fresnel(float cos_theta, float ior_in, float ior_out, float metallic) {
+  float f0 = std::fabs((ior_in - ior_out) / (ior_in + ior_out));
+  f0 = mixf(f0 * f0, 1.f, metallic);
+  return f0 + (1.f - f0) * std::pow(1.f - cos_theta, 5.f);
+}
+inline v3 nreflect(v3 tv, v3 n, v3 mn) {
+  v3 ray = reflect(-tv, mn);
+  float const d = dot(ray, n);
+  if (d < 0.f) ray = ray - 2.f * d * n;
+  return normalize(ray);
+}
+inline float schlick(float ndv, float k) { return 1.f / (ndv * (1.f - k) + k); }
+inline float smith(v3 N, v3 V, v3 L, float k) {
+  float const ndv = std::fabs(dot(N, V)), ndl = std::fabs(dot(N, L));
+  float const g1 = ndl * schlick(ndv, k);
+  float const g2 = schlick(ndl, k);
+  return g1 * g2;
+}
+struct matinfo {
+  v4 color;
+  float ior, roughness, metallic, transmission;
+};
+struct brdf {
+  v3 refl{0, 0, 0};
+  float pdf = 0.f;
+};
+struct pbr_state_t {
+  int state = -1;
+  bool after_sample = false;
+  float resample = 1.f;
+};
+inline void ggx_eval(pbr_state_t const& ps, matinfo m, v3 tv, v3 tl, v3 n, float i1, float i2, brdf& r) {
+  float const rough = m.roughness * m.roughness;
+  v3 const mn = normalize(tl + tv);
+  float const D = (ps.after_sample && rough < 0.01f) ? 1.f : ggx_distribution(n, mn, rough);
+  float const G = smith(n, tv, tl, rough);
+  float const F = fresnel(dot(tv, mn), i1, i2, m.metallic);
+  float const den = 4.f * std::fabs(dot(tv, n)) * std::fabs(dot(tl, n));
+  float const cos_theta = dot(mn, n);
+  v3 const col = mix3(v3{1.f, 1.f, 1.f}, v3{m.color.x, m.color.y, m.color.z}, std::sqrt(m.metallic));
+  float mden = G / den;
+  mden = std::isnan(mden) ? 1.f : mden;
+  r.pdf = F * D * cos_theta * mden;
+  r.refl = col * r.pdf;
+}
+inline void transmit_eval(pbr_state_t const& ps, matinfo m, v3 tv, v3 tl, v3 n, float i1, float i2, brdf& r) {
+  float const rough = m.roughness * m.roughness;
+  v3 mn = normalize(-(i1 * tv + i2 * tl));
+  mn = mn * signf(dot(mn, n));
+  float const D = (ps.after_sample && rough < 0.01f) ? 1.f : ggx_distribution(n, mn, rough);
+  float const G = smith(n, tv, tl, rough);
+  float const idoth = dot(tv, mn), odoth = dot(tl, mn);
+  float const aidn = std::fabs(dot(tv, n)), aodn = std::fabs(dot(tl, n));
+  float const prefac = (std::fabs(idoth) * std::fabs(odoth)) / (aidn * aodn);
+  float const den = i1 * idoth + i2 * odoth;
+  float const F = fresnel(dot(tv, mn), i1, i2, m.metallic);
+  float const i2d2 = i2 * i2 / (den * den);
+  float const ft = prefac * (1.f - F) * G * D * i2d2;
+  float const cos_theta = dot(mn, n);
+  r.pdf = cos_theta * ft;
+  r.refl = v3{m.color.x, m.color.y, m.color.z} * r.pdf;
+}
+inline v3 pbr_resample(rng_t& rng, pbr_state_t& ps, v2 rs, matinfo m, v3 tv, v3 n, float i1, float i2) {
+  float const frand = random_value(rng, int(std::uint32_t(f2i(19022.f * rs.x)) * 2909293u));
+  float const trand = random_value(rng, int(std::uint32_t(f2i(23452.f * rs.y)) * 8994355u));
+  v2 is = ggx_importance_sample(rs, m.roughness * m.roughness);
+  v3 hs = sample_hemisphere(is);
+  v3 mn = transform_local_to_world(hs, n);
+  float const F = fresnel(dot(tv, mn), i1, i2, m.metallic);
+  ps.after_sample = true;
+  v3 const refracted = refract(-tv, mn, i1 / i2);
+  bool const zero = refracted.x == 0.f && refracted.y == 0.f && refracted.z == 0.f;
+  if ((m.transmission > 0.f && zero) || F >= frand) {
+    ps.state = 0;
+    ps.resample = F;
+    return nreflect(tv, n, mn);
+  } else if (m.transmission >= trand) {
+    ps.resample = (1.f - F) * m.transmission;
+    ps.state = 1;
+    return refracted;
+  }
+  ps.resample = (1.f - F) * (1.f - m.transmission);
+  ps.state = 2;
+  is = ggx_importance_sample(rs, 1.f);
+  hs = sample_hemisphere(is);
+  mn = transform_local_to_world(hs, n);
+  return nreflect(tv, n, mn);
+}
+inline void pbr_eval(pbr_state_t& ps, matinfo m, v3 tv, v3 tl, v3 n, float i1, float i2, brdf& r) {
+  brdf tr, gl, di;
+  transmit_eval(ps, m, tv, tl, n, i1, i2, tr);
+  ggx_eval(ps, m, tv, tl, n, i1, i2, gl);
+  matinfo md = m;
+  md.roughness = 1.f;
+  md.metallic = 1.f;
+  ggx_eval(ps, md, tv, tl, n, i1, i2, di);
+  switch (ps.state) {
+    case 1: r = tr; break;
+    case 2: r = di; break;
+    case 0: r = gl; break;
+    default: break;
+  }
+  ps.after_sample = false;
+  r.pdf *= ps.resample;
+  r.refl = r.refl * ps.resample;
+}
+
+// material_new.glsl + generated dispatch (type 0 = PBR, 7 floats)
+struct material_ctx {
+  int type = -1;
+  matinfo mat{};
+  bool incoming = false;
+  float ior1 = 1.f, ior2 = 1.f;
+  pbr_state_t ps;
+};
+inline std::uint32_t fbits(float f) {
+  std::uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return u;
+}
+inline void mat_open(material_ctx& mc, int type, float const* data, int offset) {
+  mc.type = type;
+  if (type != 0) return;
+  float const* d = data + offset;
+  mc.mat.color = unpack_unorm4x8(fbits(d[0]));
+  mc.mat.ior = d[1];
+  mc.mat.roughness = d[2];
+  mc.mat.metallic = d[3];
+  mc.mat.transmission = d[4];
+}
+inline void mat_evaluate(material_ctx& mc, v3 n, v3 tl, v3 tv, v3& refl, float& pdf) {
+  refl = {0.f, 0.f, 0.f};
+  pdf = 1.f;
+  if (mc.type != 0) return;
+  mc.incoming = dot(n, -tv) < 0.f;
+  mc.ior1 = mc.incoming ? 1.f : mc.mat.ior;
+  mc.ior2 = mc.incoming ? mc.mat.ior : 1.f;
+  brdf ev;
+  pbr_eval(mc.ps, mc.mat, tv, tl, mc.incoming ? n : -n, mc.ior1, mc.ior2, ev);
+  refl = ev.refl;
+  pdf = ev.pdf;
+}
+inline v3 mat_bounce(material_ctx& mc, rng_t& rng, v2 rnd, v3 tv, v3 n) {
+  if (mc.type != 0) return {0.f, 0.f, 0.f};
+  mc.incoming = dot(n, -tv) < 0.f;
+  mc.ior1 = mc.incoming ? 1.f : mc.mat.ior;
+  mc.ior2 = mc.incoming ? mc.mat.ior : 1.f;
+  return pbr_resample(rng, mc.ps, rnd, mc.mat, tv, mc.incoming ? n : -n, mc.ior1, mc.ior2);
+}
+
+// ---- pass state (pt_*.comp structs) -------------------------------------------
+struct gen_t {  // generate_output_t, 80 bytes
+  v3 origin;
+  float random_value;
+  v3 direction;
+  float pixel_x;
+  v3 reflectance;
+  float pixel_y;
+  v4 color;
+  float pdf, weight, pad[2];
+};
+struct trace_t {  // trace_output_t, 64 bytes
+  v3 point;
+  int intersects;
+  v3 normal;
+  std::uint32_t generated_ray;
+  v2 uv;
+  int material_index;
+  std::uint32_t light_color;
+  v3 light_direction;
+  float light_strength;
+};
+static_assert(sizeof(gen_t) == 80 && sizeof(trace_t) == 64);
+
+struct light_t {
+  v3 position;
+  float radius;
+  v3 color;
+};
+// pt_trace.comp:141-146, products rounded in float as the GLSL computes them
+// (6 * 1.8f is 10.79999924, not the float nearest 10.8)
+constexpr light_t kLights[2] = {
+    {{2.f * 4.f, 2.f * 5.f, 2.f * 4.f}, 1.5f, {6.f * 1.f, 6.f * 1.8f, 6.f * 3.f}},
+    {{2.f * -4.f, 2.f * 3.f, 2.f * 5.f}, 1.5f, {8.f * 3.f, 8.f * 1.8f, 8.f * 1.f}},
+};
+
+// intersect.glsl:30-39
+inline float intersect_sphere(v3 r0, v3 rd, v3 s0, float sr) {
+  float const a = dot(rd, rd);
+  v3 const s0_r0 = r0 - s0;
+  float const b = 2.f * dot(rd, s0_r0);
+  float const c = dot(s0_r0, s0_r0) - (sr * sr);
+  if (b * b - 4.f * a * c < 0.f) return -1.f;
+  return (-b - std::sqrt((b * b) - 4.f * a * c)) / (2.f * a);
+}
+
+}  // namespace
+
+// ray queries provided by oracle.cpp
+extern "C" void orc_refbvh_traverse(void const* nodes_v, std::uint32_t const* bvh_idx, std::uint32_t const* indices,
+    float const* points_xyzw, float const* rays, std::size_t n, int any_hit, int canonical, std::int32_t* prim,
+    float* t_out, float* u_out, float* v_out, int nthreads);
+
+namespace {
+
+struct scene_t {
+  std::size_t n_tris;
+  float const* tris9;       // world positions
+  float const* normals9;    // world shading normals per corner (may be null)
+  float const* uvs6;        // uvs per corner (may be null)
+  std::int32_t const* tri_material;
+  std::int32_t const* mat_refs;  // (id, offset) pairs
+  std::size_t n_mats;
+  float const* mat_data;
+  void const* nodes;  // restated reference BVH over the world triangles
+  std::uint32_t const* bvh_idx;
+  std::vector<std::uint32_t> seq;  // 0..3T-1 (index buffer of the baked soup)
+  std::vector<float> pts4;         // points as xyzw
+};
+
+template <typename F> void par(std::size_t n, int nthreads, F&& f) {
+  if (nthreads <= 1 || n < 2048) {
+    f(std::size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> th;
+  std::size_t const per = (n + std::size_t(nthreads) - 1) / std::size_t(nthreads);
+  for (int i = 0; i < nthreads; ++i) {
+    std::size_t const b = std::size_t(i) * per, e = std::min(n, b + per);
+    if (b < e) th.emplace_back([&f, b, e] { f(b, e); });
+  }
+  for (auto& x : th) x.join();
+}
+
+struct pass_rng {
+  int seed;
+  std::vector<float> tex;
+};
+
+// mat4 (column major) helpers, GLSL operator order
+inline void mat_mul(float const* a, float const* b, float* out) {
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r)
+      out[c * 4 + r] = ((a[0 * 4 + r] * b[c * 4 + 0] + a[1 * 4 + r] * b[c * 4 + 1]) + a[2 * 4 + r] * b[c * 4 + 2]) +
+          a[3 * 4 + r] * b[c * 4 + 3];
+}
+inline v4 mat_vec(float const* m, v4 v) {
+  float const in[4] = {v.x, v.y, v.z, v.w};
+  float o[4];
+  for (int r = 0; r < 4; ++r)
+    o[r] = ((m[0 * 4 + r] * in[0] + m[1 * 4 + r] * in[1]) + m[2 * 4 + r] * in[2]) + m[3 * 4 + r] * in[3];
+  return {o[0], o[1], o[2], o[3]};
+}
+
+struct frame_ctx {
+  scene_t* sc;
+  int W, H;
+  float const* inv_view;
+  float const* inv_proj;
+  std::vector<v4>* accum;   // debug_image (sum, count)
+  std::vector<v4>* display; // output_image
+  std::uint32_t sample_index;
+  int nthreads;
+};
+
+// pt_generate.comp:50-84
+void pass_generate(frame_ctx& f, pass_rng const& pr, std::vector<gen_t>& gen) {
+  float vp[16];
+  mat_mul(f.inv_view, f.inv_proj, vp);
+  gen.resize(std::size_t(f.W) * f.H);
+  par(gen.size(), f.nthreads, [&](std::size_t b, std::size_t e) {
+    for (std::size_t id = b; id < e; ++id) {
+      int const x = int(id % std::size_t(f.W)), y = int(id / std::size_t(f.W));
+      rng_t r;
+      random_init(r, pr.tex.data(), int(pr.tex.size()), x, y, pr.seed);
+      v2 const off = random_uniform_circle(r, 0.7071067812f);
+      float const nx = ((off.x + float(x)) / float(f.W)) * 2.f - 1.f;
+      float const ny = ((off.y + float(y)) / float(f.H)) * 2.f - 1.f;
+      v4 const hom = mat_vec(vp, v4{nx, ny, 1.f, 1.f});
+      gen_t g{};
+      g.direction = normalize(v3{hom.x, hom.y, hom.z});
+      g.origin = v3{f.inv_view[12], f.inv_view[13], f.inv_view[14]};
+      g.random_value = random_next(r);
+      g.reflectance = {1.f, 1.f, 1.f};
+      g.color = {0.f, 0.f, 0.f, 0.f};
+      g.pixel_x = float(x);
+      g.pixel_y = float(y);
+      g.pdf = 1.f;
+      g.weight = 1.f;
+      gen[id] = g;
+    }
+  });
+}
+
+// pt_trace.comp:134-226 for meshes
+void pass_trace(frame_ctx& f, pass_rng const& pr, std::vector<gen_t> const& gen, std::vector<trace_t>& out) {
+  scene_t& sc = *f.sc;
+  std::size_t const n = gen.size();
+  out.assign(n, trace_t{});
+  // closest hits of all rays first (the order of queries does not matter)
+  std::vector<float> rays(8 * n);
+  for (std::size_t i = 0; i < n; ++i) {
+    float* q = &rays[8 * i];
+    q[0] = gen[i].origin.x, q[1] = gen[i].origin.y, q[2] = gen[i].origin.z, q[3] = 0.f;
+    q[4] = gen[i].direction.x, q[5] = gen[i].direction.y, q[6] = gen[i].direction.z;
+    q[7] = std::numeric_limits<float>::infinity();
+  }
+  std::vector<std::int32_t> prim(n);
+  std::vector<float> tt(n), uu(n), vv(n);
+  orc_refbvh_traverse(sc.nodes, sc.bvh_idx, sc.seq.data(), sc.pts4.data(), rays.data(), n, 0, 1, prim.data(), tt.data(),
+      uu.data(), vv.data(), f.nthreads);
+  // per ray: lights, attributes, shadow ray parameters
+  std::vector<float> shadow(8 * n, 0.f);
+  std::vector<std::uint8_t> wants_shadow(n, 0);
+  std::vector<int> light_index(n);
+  std::vector<v3> pol(n);
+  par(n, f.nthreads, [&](std::size_t b, std::size_t e) {
+    for (std::size_t id = b; id < e; ++id) {
+      gen_t const& base = gen[id];
+      rng_t r;
+      random_init(r, pr.tex.data(), int(pr.tex.size()), f2i(base.pixel_x), f2i(base.pixel_y), pr.seed);
+      trace_t res{};
+      res.uv = {0.f, 0.f};
+      res.material_index = 0;
+      res.generated_ray = std::uint32_t(id);
+      int const li = std::clamp(f2i(2.f * random_next(r)), 0, 1);
+      float const rx = random_next(r), ry = random_next(r), rz = random_next(r);
+      float const rs = random_next(r);
+      v3 const p_on_light = kLights[li].position + normalize(v3{rx, ry, rz}) * kLights[li].radius * std::sqrt(rs);
+      bool hits = prim[id] >= 0;
+      float ht = tt[id];
+      int hits_light = -1;
+      // nearest_hit attributes (pt_trace.comp:357-385) of the closest triangle
+      // (triangle 0 when nothing was hit, as the reference reads index 0)
+      std::size_t const tri = hits ? std::size_t(prim[id]) : 0;
+      float const bx = hits ? uu[id] : 0.f, by = hits ? vv[id] : 0.f;
+      float const* P = sc.tris9 + 9 * tri;
+      v3 const p0{P[0], P[1], P[2]}, p1{P[3], P[4], P[5]}, p2{P[6], P[7], P[8]};
+      float const w = (1.f - bx) - by;
+      v3 const position = (bx * p1 + by * p2) + w * p0;
+      v3 normal;
+      if (sc.normals9) {
+        float const* N = sc.normals9 + 9 * tri;
+        v3 const n0{N[0], N[1], N[2]}, n1{N[3], N[4], N[5]}, n2{N[6], N[7], N[8]};
+        normal = normalize((bx * n1 + by * n2) + w * n0);
+      } else {
+        normal = normalize(cross(normalize(p1 - p0), normalize(p2 - p0)));
+      }
+      v2 uv{0.f, 0.f};
+      if (sc.uvs6) {
+        float const* U = sc.uvs6 + 6 * tri;
+        uv = {(bx * U[2] + by * U[4]) + w * U[0], (bx * U[3] + by * U[5]) + w * U[1]};
+      }
+      for (int l = 0; l < 2; ++l) {
+        float const t_light = intersect_sphere(base.origin, base.direction, kLights[l].position, kLights[l].radius);
+        if (t_light > 0.f && (!hits || t_light < ht)) {
+          hits = true;
+          ht = t_light;
+          hits_light = l;
+        }
+      }
+      res.light_direction = {0.f, 0.f, 0.f};
+      res.light_color = 0;
+      res.light_strength = 0.f;
+      if (hits) {
+        res.intersects = 1;
+        res.point = position;
+        res.normal = normal;
+        res.uv = uv;
+        res.material_index = sc.tri_material[tri];
+        if (inf3(res.normal) || nan3(res.normal)) res.intersects = 0;
+        v3 const path = p_on_light - position;
+        v3 const dir_l = normalize(path);
+        float const dist_l = length(path);
+        v3 const lnorm = faceforward(normal, base.direction, normal);
+        if (hits_light >= 0) {
+          res.intersects = 2;
+          v3 const col = kLights[hits_light].color;
+          res.light_strength = length(col);
+          res.light_color = pack_unorm4x8(v4{col.x / res.light_strength, col.y / res.light_strength,
+              col.z / res.light_strength, 0.f / res.light_strength});
+          res.light_direction = dir_l;
+        } else if (dot(dir_l, lnorm) > 0.f) {
+          v3 const so = position + lnorm * 0.01f;
+          float* q = &shadow[8 * id];
+          q[0] = so.x, q[1] = so.y, q[2] = so.z, q[3] = 0.f, q[4] = dir_l.x, q[5] = dir_l.y, q[6] = dir_l.z;
+          q[7] = dist_l;
+          wants_shadow[id] = 1;
+          light_index[id] = li;
+        }
+        res.generated_ray = std::uint32_t(id);
+      } else {
+        res.intersects = 0;
+        res.point = {0.f, 0.f, 0.f};
+        res.normal = {0.f, 0.f, 0.f};
+      }
+      out[id] = res;
+    }
+  });
+  // shadow rays (any_hit, pt_trace.comp:311-329), then the NEE record
+  std::vector<std::int32_t> sp(n);
+  std::vector<float> st(n), su(n), sv(n);
+  orc_refbvh_traverse(sc.nodes, sc.bvh_idx, sc.seq.data(), sc.pts4.data(), shadow.data(), n, 1, 0, sp.data(), st.data(),
+      su.data(), sv.data(), f.nthreads);
+  for (std::size_t id = 0; id < n; ++id) {
+    if (!wants_shadow[id] || sp[id] >= 0) continue;
+    trace_t& res = out[id];
+    v3 const col = kLights[light_index[id]].color;
+    float const strength = length(col);
+    res.light_color = pack_unorm4x8(v4{col.x / strength, col.y / strength, col.z / strength, 0.f / strength});
+    float const dist_l = shadow[8 * id + 7];
+    res.light_strength = strength * (2.f / dist_l);
+    res.light_direction = {shadow[8 * id + 4], shadow[8 * id + 5], shadow[8 * id + 6]};
+  }
+}
+
+// pt_color.comp:77-101
+void accumulate(frame_ctx& f, v4 nc, int px, int py) {
+  std::size_t const pi = std::size_t(py) * std::size_t(f.W) + std::size_t(px);
+  v4& dbg = (*f.accum)[pi];
+  v4 last = dbg;
+  if (naninf4(nc)) nc = last;
+  v4 const actual_last = last;
+  if (f.sample_index == 0) last = {nc.x, nc.y, nc.z, 1.f};
+  else last = {last.x + nc.x, last.y + nc.y, last.z + nc.z, last.w + 1.f};
+  if (naninf4(last)) last = actual_last;
+  dbg = last;
+  (*f.display)[pi] = {gclamp(last.x / last.w, 0.f, 4.f), gclamp(last.y / last.w, 0.f, 4.f),
+      gclamp(last.z / last.w, 0.f, 4.f), 1.f};
+}
+
+// pt_color.comp:113-202
+void pass_color(frame_ctx& f, pass_rng const& pr, std::vector<gen_t>& gen, std::vector<trace_t>& tr, bool force) {
+  scene_t& sc = *f.sc;
+  par(gen.size(), f.nthreads, [&](std::size_t b, std::size_t e) {
+    for (std::size_t id = b; id < e; ++id) {
+      trace_t const trace = tr[id];
+      gen_t g = gen[id];
+      int const px = f2i(g.pixel_x), py = f2i(g.pixel_y);
+      auto acc = [&](v4 c) { accumulate(f, c, px, py); };
+      if (trace.intersects != 0) {
+        if (trace.intersects == 2) {
+          tr[id].intersects = 0;
+          v4 const lc = unpack_unorm4x8(trace.light_color);
+          v3 const c = v3{lc.x, lc.y, lc.z} * trace.light_strength * g.reflectance / g.pdf;
+          acc(v4{c.x + g.color.x, c.y + g.color.y, c.z + g.color.z, 1.f + g.color.w});
+          continue;
+        }
+        rng_t r;
+        random_init(r, pr.tex.data(), int(pr.tex.size()), px, py, pr.seed);
+        std::uint32_t const uid = std::uint32_t(id);
+        random_value(r, int(std::uint32_t(f2i(56128966.f * g.random_value)) + 20945293u * uid));
+        random_value(r, int(std::uint32_t(f2i(12233432.f * g.random_value)) + 74867839u * uid));
+        material_ctx mc;
+        int const mi = trace.material_index;
+        bool const valid_mat = mi >= 0 && std::size_t(mi) < sc.n_mats;
+        mat_open(mc, valid_mat ? sc.mat_refs[2 * mi] : -1, sc.mat_data, valid_mat ? sc.mat_refs[2 * mi + 1] : 0);
+        float const r0 = random_next(r);
+        float const r1 = random_next(r);
+        v3 const generated = mat_bounce(mc, r, v2{r0, r1}, -g.direction, trace.normal);
+        v3 mrefl;
+        float mpdf;
+        mat_evaluate(mc, trace.normal, generated, -g.direction, mrefl, mpdf);
+        {
+          float const p = g.pdf * 1.f;
+          float const rnd = random_next(r);
+          if (rnd > p) {
+            tr[id].intersects = 0;
+            v3 const c = g.reflectance / g.pdf;
+            acc(v4{g.color.x + c.x, g.color.y + c.y, g.color.z + c.z, g.color.w});
+            continue;
+          }
+        }
+        if (force || g.pdf < 1e-5f || mpdf < 1e-6f || std::isnan(mpdf) || std::isinf(mpdf) || nan3(mrefl) ||
+            inf3(mrefl) || nan3(generated) || inf3(generated)) {
+          tr[id].intersects = 0;
+          if (nan3(mrefl) || inf3(mrefl) || std::isnan(g.pdf) || std::isinf(g.pdf) || g.pdf < 1e-5f) {
+            acc(g.color);
+          } else {
+            v3 const c = g.reflectance / g.pdf;
+            acc(v4{g.color.x + c.x, g.color.y + c.y, g.color.z + c.z, g.color.w});
+          }
+          continue;
+        }
+        if (trace.light_strength > 0.f) {
+          v3 lrefl{1.f, 1.f, 1.f};
+          float lpdf = 1.f;
+          mat_evaluate(mc, trace.normal, trace.light_direction, -g.direction, lrefl, lpdf);
+          if (!inf3(lrefl)) {
+            v4 const lc = unpack_unorm4x8(trace.light_color);
+            v3 const c = v3{lc.x, lc.y, lc.z} * trace.light_strength * clamp3(lrefl, 0.f, 1.f);
+            g.color = {g.color.x + c.x, g.color.y + c.y, g.color.z + c.z, g.color.w};
+          }
+        }
+        g.direction = generated;
+        g.origin = trace.point + 1e-4f * faceforward(trace.normal, -g.direction, trace.normal);
+        g.pdf *= mpdf;
+        g.reflectance = g.reflectance * mrefl;
+        // The literal 2341335623 has no suffix: GLSL makes it an int with the same
+        // bit pattern (GLSL 4.60, 4.1.3), i.e. -1953631673.
+        g.random_value = random_value(r, int(std::uint32_t(f2i(-1953631673.f * g.random_value)) + 357883444u * uid));
+        gen[id] = g;
+      } else {
+        float const t = (g.direction.y + 1.f) / 2.f;
+        v3 const sky = mix3(v3{0.3f, 0.4f, 0.5f}, v3{1.f, 0.98f, 0.96f}, t);
+        v3 const env = clamp3(g.reflectance * sky / g.pdf, 0.f, 16.f);
+        acc(v4{g.color.x + env.x, g.color.y + env.y, g.color.z + env.z, g.color.w});
+      }
+    }
+  });
+}
+
+// pt_ray_filter.comp:49-64, stable
+void pass_filter(std::vector<gen_t>& gen, std::vector<trace_t> const& tr) {
+  std::vector<gen_t> out;
+  out.reserve(gen.size());
+  for (std::size_t id = 0; id < gen.size(); ++id)
+    if (tr[id].intersects == 1) out.push_back(gen[tr[id].generated_ray]);
+  gen.swap(out);
+}
+
+}  // namespace
+
+extern "C" {
+
+// Per-pass host randomness in the order sequential_pathtracer draws it for
+// `frames` frames of `bounces` bounces from std::mt19937(seed):
+//   generate: int then 1024 floats; trace: int then floats; color: floats then int.
+// out_seeds: frames * passes ints, out_tex: frames * passes * 1024 floats,
+// passes = 2 * bounces + 3 (generate, {trace, color} x (bounces + 1)).
+void orc_host_rng(std::uint32_t seed, int frames, int bounces, std::int32_t* out_seeds, float* out_tex) {
+  std::mt19937 rng(seed);
+  int const passes = 2 * bounces + 3;
+  for (int f = 0; f < frames; ++f) {
+    for (int p = 0; p < passes; ++p) {
+      std::uniform_int_distribution<> dist;
+      std::uniform_real_distribution<float> uni(0.f, 1.f);
+      std::int32_t& s = out_seeds[f * passes + p];
+      float* t = out_tex + (std::size_t(f) * passes + p) * 1024;
+      bool const is_color = p >= 1 && ((p - 1) % 2 == 1);
+      if (!is_color) s = dist(rng);
+      for (int k = 0; k < 1024; ++k) t[k] = uni(rng);
+      if (is_color) s = dist(rng);
+    }
+  }
+}
+
+// Renders `frames` frames in reference-shading mode; accum/display are W*H*4
+// floats, read and written (accumulation continues from sample_index0).
+void orc_render_reference(std::size_t n_tris, float const* tris9, float const* normals9, float const* uvs6,
+    std::int32_t const* tri_material, std::int32_t const* mat_refs, std::size_t n_mats, float const* mat_data,
+    void const* nodes, std::uint32_t const* bvh_idx, int W, int H, int bounces, int frames,
+    std::uint32_t sample_index0, float const* inv_view, float const* inv_proj, std::int32_t const* seeds,
+    float const* tex, float* accum, float* display, int nthreads) {
+  scene_t sc{n_tris, tris9, normals9, uvs6, tri_material, mat_refs, n_mats, mat_data, nodes, bvh_idx, {}, {}};
+  sc.seq.resize(3 * n_tris);
+  for (std::size_t i = 0; i < sc.seq.size(); ++i) sc.seq[i] = std::uint32_t(i);
+  sc.pts4.resize(4 * 3 * n_tris);
+  for (std::size_t i = 0; i < 3 * n_tris; ++i)
+    for (int k = 0; k < 3; ++k) sc.pts4[4 * i + k] = tris9[3 * i + k];
+  std::vector<v4> acc(std::size_t(W) * H), disp(std::size_t(W) * H);
+  std::memcpy(acc.data(), accum, acc.size() * sizeof(v4));
+  std::memcpy(disp.data(), display, disp.size() * sizeof(v4));
+  int const passes = 2 * bounces + 3;
+  for (int fr = 0; fr < frames; ++fr) {
+    auto pr = [&](int p) {
+      pass_rng r;
+      r.seed = seeds[fr * passes + p];
+      float const* t = tex + (std::size_t(fr) * passes + p) * 1024;
+      r.tex.assign(t, t + 1024);
+      return r;
+    };
+    frame_ctx f{&sc, W, H, inv_view, inv_proj, &acc, &disp, sample_index0 + std::uint32_t(fr), nthreads};
+    std::vector<gen_t> gen;
+    std::vector<trace_t> tr;
+    pass_generate(f, pr(0), gen);
+    int p = 1;
+    for (int i = 0; i < bounces; ++i) {
+      pass_trace(f, pr(p++), gen, tr);
+      pass_color(f, pr(p++), gen, tr, false);
+      pass_filter(gen, tr);
+    }
+    pass_trace(f, pr(p++), gen, tr);
+    pass_color(f, pr(p++), gen, tr, true);
+  }
+  std::memcpy(accum, acc.data(), acc.size() * sizeof(v4));
+  std::memcpy(display, disp.data(), disp.size() * sizeof(v4));
+}
+
+// Known-answer access to the restated shading functions (for the pins).
+void orc_random_stream(float const* tex, int tex_size, int px, int py, int seed, int n, float* out,
+    std::uint32_t* state_after_init) {
+  rng_t r;
+  random_init(r, tex, tex_size, px, py, seed);
+  if (state_after_init) *state_after_init = r.state;
+  for (int i = 0; i < n; ++i) out[i] = random_next(r);
+}
+std::uint32_t orc_wang_hash(std::uint32_t a) { return wang(a); }
+void orc_transform_local_to_world(float const* v, float const* n, float* out) {
+  v3 const r = transform_local_to_world({v[0], v[1], v[2]}, {n[0], n[1], n[2]});
+  out[0] = r.x, out[1] = r.y, out[2] = r.z;
+}
+std::uint32_t orc_pack_unorm4x8(float const* v) { return pack_unorm4x8({v[0], v[1], v[2], v[3]}); }
+float orc_intersect_sphere(float const* r0, float const* rd, float const* s0, float sr) {
+  return intersect_sphere({r0[0], r0[1], r0[2]}, {rd[0], rd[1], rd[2]}, {s0[0], s0[1], s0[2]}, sr);
+}
+void orc_material_bounce_eval(float const* mat7, std::uint32_t* io_rng, float const* tv, float const* n, float* out_gen,
+    float* out_refl, float* out_pdf, int* out_lobe, float* out_resample) {
+  rng_t r;
+  r.state = io_rng[0];
+  r.prime = int(io_rng[1]);
+  material_ctx mc;
+  mat_open(mc, 0, mat7, 0);
+  float const a = random_next(r);
+  float const b = random_next(r);
+  v3 const t{tv[0], tv[1], tv[2]}, nn{n[0], n[1], n[2]};
+  v3 const g = mat_bounce(mc, r, v2{a, b}, t, nn);
+  v3 refl;
+  float pdf;
+  mat_evaluate(mc, nn, g, t, refl, pdf);
+  out_gen[0] = g.x, out_gen[1] = g.y, out_gen[2] = g.z;
+  out_refl[0] = refl.x, out_refl[1] = refl.y, out_refl[2] = refl.z;
+  *out_pdf = pdf;
+  *out_lobe = mc.ps.state;
+  *out_resample = mc.ps.resample;
+  io_rng[0] = r.state;
+  io_rng[1] = std::uint32_t(r.prime);
+}
+void orc_material_eval(float const* mat7, int lobe, float resample, float const* tl, float const* tv, float const* n,
+    float* out_refl, float* out_pdf) {
+  material_ctx mc;
+  mat_open(mc, 0, mat7, 0);
+  mc.ps.state = lobe;
+  mc.ps.resample = resample;
+  mc.ps.after_sample = false;
+  v3 refl;
+  float pdf;
+  mat_evaluate(mc, {n[0], n[1], n[2]}, {tl[0], tl[1], tl[2]}, {tv[0], tv[1], tv[2]}, refl, pdf);
+  out_refl[0] = refl.x, out_refl[1] = refl.y, out_refl[2] = refl.z;
+  *out_pdf = pdf;
+}
+
+}  // extern "C"

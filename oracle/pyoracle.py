@@ -40,6 +40,16 @@ def oracle() -> C.CDLL:
             "orc_refbvh_traverse": (None, [P, P, P, P, P, SZ, I, I, P, P, P, P, I]),
             "orc_bvh8_traverse": (None, [P, P, P, SZ, I, I, P, P, P, P, P, P, P, I]),
             "orc_brute_closest": (None, [P, SZ, P, SZ, I, P, P, P, P, I]),
+            "orc_host_rng": (None, [C.c_uint32, I, I, P, P]),
+            "orc_render_reference": (None, [SZ, P, P, P, P, P, SZ, P, P, P, I, I, I, I, C.c_uint32, P, P, P, P, P,
+                                            P, I]),
+            "orc_random_stream": (None, [P, I, I, I, I, I, P, P]),
+            "orc_wang_hash": (C.c_uint32, [C.c_uint32]),
+            "orc_transform_local_to_world": (None, [P, P, P]),
+            "orc_pack_unorm4x8": (C.c_uint32, [P]),
+            "orc_intersect_sphere": (C.c_float, [P, P, P, C.c_float]),
+            "orc_material_bounce_eval": (None, [P, P, P, P, P, P, P, P, P]),
+            "orc_material_eval": (None, [P, I, C.c_float, P, P, P, P, P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(h, k)
@@ -218,3 +228,70 @@ def bake_world_triangles(indices, vertices, drawables=None) -> np.ndarray:
             p = np.stack([((m[r] * x + m[4 + r] * y) + m[8 + r] * z) + m[12 + r] * one for r in range(3)], 1)
         out.append(p.reshape(-1, 9).astype(np.float32))
     return np.concatenate(out, 0)
+
+
+def bake_world_attributes(indices, normals, uvs, drawables, n_vertices):
+    """Per-triangle corner normals [T, 9] (normal matrix = transpose of the
+    inverse's 3x3, left-to-right sums; not normalised) and uvs [T, 6], and the
+    per-triangle material index, in prim order."""
+    idx = np.asarray(indices, np.uint32)
+    if drawables is None or len(drawables) == 0:
+        class _D:  # one identity drawable over the whole buffer
+            transformation = np.eye(4, dtype=np.float32).ravel()
+            inverse_transformation = np.eye(4, dtype=np.float32).ravel()
+            indices_base_index, points_base_index, index_count, material_index = 0, 0, idx.size, 0
+        drawables = [_D()]
+    nrm, uv, mat = [], [], []
+    for d in drawables:
+        sel = idx[d.indices_base_index: d.indices_base_index + d.index_count].astype(np.int64) + d.points_base_index
+        m = np.array(d.transformation[:], np.float32)
+        inv = np.array(d.inverse_transformation[:], np.float32)
+        ident = np.array_equal(m, np.eye(4, dtype=np.float32).ravel())
+        if normals is not None:
+            n = np.asarray(normals, np.float32)[:, :3][sel]
+            if not ident:
+                nm = np.array([[inv[r * 4 + c] for r in range(3)] for c in range(3)], np.float32).ravel()  # nm[c*3+r]
+                x, y, z = n[:, 0], n[:, 1], n[:, 2]
+                n = np.stack([(nm[r] * x + nm[3 + r] * y) + nm[6 + r] * z for r in range(3)], 1)
+            nrm.append(n.reshape(-1, 9).astype(np.float32))
+        if uvs is not None:
+            uv.append(np.asarray(uvs, np.float32)[sel].reshape(-1, 6))
+        mat.append(np.full(d.index_count // 3, d.material_index, np.int32))
+    return (np.concatenate(nrm) if nrm else None, np.concatenate(uv) if uv else None, np.concatenate(mat))
+
+
+def host_rng(seed: int, frames: int, bounces: int):
+    """Per-pass (seed, 1024-float texture) in sequential_pathtracer's draw order."""
+    passes = 2 * bounces + 3
+    seeds = np.zeros(frames * passes, np.int32)
+    tex = np.zeros((frames * passes, 1024), np.float32)
+    oracle().orc_host_rng(seed, frames, bounces, seeds.ctypes.data, tex.ctypes.data)
+    return seeds, tex
+
+
+def render_reference(scene: dict, width: int, height: int, bounces: int, frames: int, inv_view, inv_proj,
+                     seed: int = 5489, accum=None, display=None, sample_index0: int = 0):
+    """Reference-shading render on the CPU (restated passes). scene: dict with
+    indices, vertices, normals, uvs, drawables, materials, material_data."""
+    L = oracle()
+    tris9 = bake_world_triangles(scene["indices"], scene["vertices"], scene.get("drawables"))
+    nrm, uvs, mat = bake_world_attributes(scene["indices"], scene.get("normals"), scene.get("uvs"),
+                                          scene.get("drawables"), len(scene["vertices"]))
+    idx = np.arange(tris9.shape[0] * 3, dtype=np.uint32)
+    nodes, bi = refbvh_build(idx, tris9.reshape(-1, 3))
+    refs = np.ascontiguousarray(scene.get("materials", np.zeros((1, 2), np.int32)), np.int32).reshape(-1, 2)
+    mdata = np.ascontiguousarray(scene.get("material_data", np.zeros(7, np.float32)), np.float32).ravel()
+    seeds, tex = host_rng(seed, frames, bounces)
+    if accum is None:
+        accum = np.zeros((height, width, 4), np.float32)
+    if display is None:
+        display = np.zeros((height, width, 4), np.float32)
+    iv = np.ascontiguousarray(inv_view, np.float32).ravel()
+    ip = np.ascontiguousarray(inv_proj, np.float32).ravel()
+    nrm_p = nrm.ctypes.data if nrm is not None else None
+    uv_p = uvs.ctypes.data if uvs is not None else None
+    L.orc_render_reference(tris9.shape[0], tris9.ctypes.data, nrm_p, uv_p, mat.ctypes.data, refs.ctypes.data,
+                           refs.shape[0], mdata.ctypes.data, nodes.ctypes.data, bi.ctypes.data, width, height, bounces,
+                           frames, sample_index0, iv.ctypes.data, ip.ctypes.data, seeds.ctypes.data, tex.ctypes.data,
+                           accum.ctypes.data, display.ctypes.data, nthreads())
+    return accum, display

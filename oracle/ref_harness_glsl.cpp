@@ -150,7 +150,10 @@ void ref_glsl_material_bounce_eval(float const* mat7, std::uint32_t* io_rng, flo
   random_state.current_prime = int(io_rng[1]);
   g_material_data = mat7;
   material_load_mat_(0);
-  vec2 const material_randoms = vec2(random_next(), random_next());
+  // pt_color.comp:139, drawn left to right as GLSL evaluates arguments
+  float const r0 = random_next();
+  float const r1 = random_next();
+  vec2 const material_randoms = vec2(r0, r1);
   vec3 const tv(towards_viewer[0], towards_viewer[1], towards_viewer[2]);
   vec3 const n(normal[0], normal[1], normal[2]);
   vec3 const generated = material_bounce_(material_randoms, tv, n);
