@@ -433,16 +433,18 @@ void mat_mul4(float const* a, float const* b, float* out) {
 
 }  // namespace
 
+// Releases the device buffers; the camera record and the sample counter stay.
 void free_render(render_state& R) {
-  cudaFree(R.gen[0]);
-  cudaFree(R.gen[1]);
-  cudaFree(R.trace);
-  cudaFree(R.accum);
-  cudaFree(R.display);
-  cudaFree(R.counts);
-  cudaFree(R.block_sums);
-  cudaFree(R.pass_tex);
-  R = render_state{};
+  for (void* p : {static_cast<void*>(R.gen[0]), static_cast<void*>(R.gen[1]), static_cast<void*>(R.trace),
+           static_cast<void*>(R.accum), static_cast<void*>(R.display), static_cast<void*>(R.counts),
+           static_cast<void*>(R.block_sums), static_cast<void*>(R.pass_tex)})
+    cudaFree(p);
+  R.gen[0] = R.gen[1] = nullptr;
+  R.trace = R.accum = R.display = nullptr;
+  R.counts = R.block_sums = nullptr;
+  R.pass_tex = nullptr;
+  R.pass_tex_capacity = 0;
+  R.width = R.height = 0;
 }
 
 // Host random stream of sequential_pathtracer.cpp:282-498 for `frames` frames:
