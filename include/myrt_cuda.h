@@ -223,6 +223,26 @@ int myrt_reset_accumulation(myrt_ctx* ctx);
 int myrt_sample_count(myrt_ctx* ctx, uint32_t* count);
 int myrt_set_seed(myrt_ctx* ctx, uint32_t seed);
 
+/* Render without any device allocation. No counterpart in the reference: it
+ * exists for callers that cannot call cudaMalloc -- hosts that give all device
+ * memory to their own allocator or fixed budgets up front, and frame loops that
+ * must not pay cudaMalloc's implicit device synchronisation. It runs the same
+ * frames as myrt_render (same kernels, same host random stream of the context)
+ * but keeps every scratch buffer in one static device array inside the library
+ * (15.7 MB, held by every device that loads the library until the process
+ * exits) and writes into CALLER-PROVIDED device images: accum_rgba (rgb sum,
+ * count in a; read as well as written when sample_index > 0) and display_rgba,
+ * width * height * 4 floats each. The caller tracks sample_index (0 starts a new
+ * accumulation); the context's own images and sample counter are not touched.
+ * Limits: width * height <= 65536 and frames * (2 * num_bounces + 3) <= 256,
+ * else MYRT_ERR_INVALID_ARGUMENT. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture. All calls share the array: calls that overlap on the GPU
+ * (other streams, other threads) race and must be serialised by the caller.
+ * Asynchronous on `stream` (NULL = the ctx stream). */
+int myrt_render_noalloc(myrt_ctx* ctx, const myrt_camera* camera, const myrt_render_params* params,
+    uint32_t sample_index, float* accum_rgba, float* display_rgba, void* stream);
+
 /* Waits for the context's work and returns MYRT_ERR_DEVICE_ABORT if a kernel
  * stopped at a limit since the last call (the error word is then cleared). */
 int myrt_sync(myrt_ctx* ctx);

@@ -177,6 +177,18 @@ class Context:
         p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0)
         self._check(self._L.myrt_render(self._h, C.byref(cam), C.byref(p)), "myrt_render")
 
+    def render_noalloc(self, inverse_view, inverse_projection, width: int, height: int, accum, display,
+                       sample_index: int = 0, num_bounces: int = 10, frames: int = 1,
+                       shading: int = _abi.SHADE_REFERENCE, stream: int | None = None):
+        """myrt_render_noalloc: renders into caller-owned device images (torch
+        tensors, float32 [H, W, 4]) with no device allocation by the library."""
+        cam = _abi.myrt_camera()
+        cam.inverse_view[:] = np.asarray(inverse_view, np.float32).ravel().tolist()
+        cam.inverse_projection[:] = np.asarray(inverse_projection, np.float32).ravel().tolist()
+        p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0)
+        self._check(self._L.myrt_render_noalloc(self._h, C.byref(cam), C.byref(p), sample_index, _ptr(accum),
+                                                _ptr(display), stream), "myrt_render_noalloc")
+
     def read_accumulation(self, width: int, height: int):
         """(rgb sum + count, display) images as float32 [H, W, 4]."""
         acc = np.empty((height, width, 4), np.float32)

@@ -92,6 +92,7 @@ SIGNATURES = {
     "myrt_reset_accumulation": (I, [P]),
     "myrt_sample_count": (I, [P, C.POINTER(C.c_uint32)]),
     "myrt_set_seed": (I, [P, C.c_uint32]),
+    "myrt_render_noalloc": (I, [P, C.POINTER(myrt_camera), C.POINTER(myrt_render_params), C.c_uint32, P, P, P]),
     "myrt_sync": (I, [P]),
 }
 

@@ -427,6 +427,21 @@ int myrt_render(myrt_ctx* ctx, myrt_camera const* camera, myrt_render_params con
   return render_reference_frames(ctx, camera, p);
 }
 
+int myrt_render_noalloc(myrt_ctx* ctx, myrt_camera const* camera, myrt_render_params const* p, uint32_t sample_index,
+    float* accum_rgba, float* display_rgba, void* stream) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!camera || !p || !accum_rgba || !display_rgba)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "null camera, params or image pointer");
+  if (!ctx->scene.valid) return set_error(ctx, MYRT_ERR_NO_SCENE, "no scene uploaded");
+  if (p->width == 0 || p->height == 0) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "empty image");
+  if (p->num_bounces < 0 || p->num_bounces > 1024)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "num_bounces must be in [0, 1024]");
+  if (p->shading != MYRT_SHADE_REFERENCE) return set_error(ctx, MYRT_ERR_UNSUPPORTED, "unknown shading mode");
+  if (p->frames == 0) return MYRT_OK;
+  return render_reference_frames_noalloc(ctx, camera, p, sample_index, reinterpret_cast<float4*>(accum_rgba),
+      reinterpret_cast<float4*>(display_rgba), stream ? static_cast<cudaStream_t>(stream) : ctx->stream);
+}
+
 int myrt_read_accumulation(myrt_ctx* ctx, float* rgba_sum, float* rgba_display) {
   if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
   render_state const& R = ctx->render;

@@ -65,4 +65,6 @@ int set_error(myrt_ctx* ctx, int code, std::string msg);
 int check_cuda(myrt_ctx* ctx, cudaError_t e, char const* what);
 void free_render(render_state& r);
 int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p);
+int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p,
+    uint32_t sample_index, float4* accum, float4* display, cudaStream_t st);
 }  // namespace myrt_b200

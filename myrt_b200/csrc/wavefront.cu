@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <vector>
 
@@ -529,6 +530,127 @@ int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_p
     rc = check_cuda(ctx, cudaGetLastError(), "wavefront launch");
     if (rc) return rc;
     ++R.sample_counter;
+  }
+  return MYRT_OK;
+}
+
+// ---- render without device allocation -------------------------------------------
+// Some callers cannot call cudaMalloc: hosts that hand all device memory to
+// their own allocator or fixed budgets up front, and frame loops that must not
+// pay cudaMalloc's implicit device synchronisation. For them the render can
+// run with every scratch buffer (ray states, trace records, counts, block sums,
+// the pass randomness) in one fixed array below; the caller passes the scene
+// (through the context) and the two output images.
+namespace {
+constexpr size_t kNoAllocMaxPixels = 65536;  // width * height
+constexpr size_t kNoAllocMaxPasses = 256;    // frames * (2 * num_bounces + 3)
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t kNaGen = align256(kNoAllocMaxPixels * 80);
+constexpr size_t kNaTrace = align256(kNoAllocMaxPixels * 64);
+constexpr size_t kNaCounts = 256;
+constexpr size_t kNaSums = align256((kNoAllocMaxPixels / kBlock) * sizeof(uint32_t));
+constexpr size_t kNaTex = align256(kNoAllocMaxPasses * kTexSize * sizeof(float));
+constexpr size_t kNaBytes = 2 * kNaGen + kNaTrace + kNaCounts + kNaSums + kNaTex;  // 15.7 MB
+}  // namespace
+
+// Held by every device that loads the library, until exit. Every call shares it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+namespace {
+// Device address of g_noalloc_scratch, resolved once per device with that device
+// current (in host code the symbol is only a host-side stand-in).
+int noalloc_scratch(myrt_ctx* ctx, unsigned char** out) {
+  static std::mutex m;
+  static void* addr[64] = {};
+  if (ctx->device < 0 || ctx->device >= 64) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "device ordinal >= 64");
+  std::lock_guard<std::mutex> lock(m);
+  if (!addr[ctx->device]) {
+    int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (rc) return rc;
+    void* p = nullptr;
+    rc = check_cuda(ctx, cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)");
+    if (rc) return rc;
+    addr[ctx->device] = p;
+  }
+  *out = static_cast<unsigned char*>(addr[ctx->device]);
+  return MYRT_OK;
+}
+}  // namespace
+
+int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p,
+    uint32_t sample_index, float4* accum, float4* display, cudaStream_t st) {
+  uint32_t const W = p->width, H = p->height;
+  int const B = p->num_bounces;
+  int const F = int(p->frames);
+  int const passes = 2 * B + 3;
+  if (size_t(W) * H > kNoAllocMaxPixels)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "myrt_render_noalloc: width * height exceeds 65536 pixels");
+  if (size_t(F) * size_t(passes) > kNoAllocMaxPasses)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT,
+        "myrt_render_noalloc: frames * (2 * num_bounces + 3) exceeds 256 passes");
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(ctx, &base);
+  if (rc) return rc;
+  float4* gen[2] = {reinterpret_cast<float4*>(base), reinterpret_cast<float4*>(base + kNaGen)};
+  float4* trace = reinterpret_cast<float4*>(base + 2 * kNaGen);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(base + 2 * kNaGen + kNaTrace);
+  uint32_t* sums = reinterpret_cast<uint32_t*>(base + 2 * kNaGen + kNaTrace + kNaCounts);
+  float* ptex = reinterpret_cast<float*>(base + 2 * kNaGen + kNaTrace + kNaCounts + kNaSums);
+
+  // Host randomness in draw_host_randomness's order, one pass at a time through
+  // a stack buffer (no heap, no device allocation).
+  int seeds[kNoAllocMaxPasses];
+  float tbuf[kTexSize];
+  for (int f = 0; f < F; ++f) {
+    for (int q = 0; q < passes; ++q) {
+      std::uniform_int_distribution<> dist;
+      std::uniform_real_distribution<float> uni(0.f, 1.f);
+      bool const is_color = q >= 1 && ((q - 1) % 2 == 1);
+      int& s = seeds[f * passes + q];
+      if (!is_color) s = dist(ctx->host_rng);
+      for (int k = 0; k < kTexSize; ++k) tbuf[k] = uni(ctx->host_rng);
+      if (is_color) s = dist(ctx->host_rng);
+      rc = check_cuda(ctx,
+          cudaMemcpyAsync(ptex + (size_t(f) * passes + q) * kTexSize, tbuf, sizeof(tbuf), cudaMemcpyHostToDevice, st),
+          "pass randomness upload");
+      if (rc) return rc;
+    }
+  }
+
+  device_scene const& S = ctx->scene;
+  camera_dev cd{};
+  mat_mul4(cam->inverse_view, cam->inverse_projection, cd.vp);
+  cd.eye[0] = cam->inverse_view[12];
+  cd.eye[1] = cam->inverse_view[13];
+  cd.eye[2] = cam->inverse_view[14];
+  scene_dev sd{S.nodes, S.tris, S.tri_normals, S.tri_uvs, S.tri_material,
+      reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err};
+  color_args ca{reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, accum, display, W,
+      sample_index, 0};
+  size_t const n = size_t(W) * H;
+  uint32_t const nb = uint32_t((n + kBlock - 1) / kBlock);
+  for (int f = 0; f < F; ++f) {
+    auto tex_of = [&](int pass) { return ptex + (size_t(f) * passes + pass) * kTexSize; };
+    auto seed_of = [&](int pass) { return seeds[f * passes + pass]; };
+    int cur = 0;
+    ca.sample_index = sample_index + uint32_t(f);
+    k_generate<<<nb, kBlock, 0, st>>>(W, H, tex_of(0), seed_of(0), cd, gen[cur], counts + cur);
+    int pass = 1;
+    for (int i = 0; i <= B; ++i) {
+      bool const last = i == B;
+      k_trace_pass<<<nb, kBlock, 0, st>>>(sd, tex_of(pass), seed_of(pass), gen[cur], trace, counts + cur);
+      ++pass;
+      ca.force = last ? 1 : 0;
+      k_color_pass<<<nb, kBlock, 0, st>>>(ca, tex_of(pass), seed_of(pass), gen[cur], trace, counts + cur, sums);
+      ++pass;
+      if (!last) {
+        k_scan_blocks<<<1, 1024, 0, st>>>(sums, nb, counts + (1 - cur));
+        k_scatter<<<nb, kBlock, 0, st>>>(gen[cur], trace, counts + cur, sums, gen[1 - cur]);
+        cur = 1 - cur;
+      }
+    }
+    rc = check_cuda(ctx, cudaGetLastError(), "wavefront launch");
+    if (rc) return rc;
   }
   return MYRT_OK;
 }
