@@ -137,6 +137,17 @@ int myrt_bvh8_get_info(const myrt_bvh8_host* bvh, myrt_bvh_info* info);
 int myrt_bvh8_copy(const myrt_bvh8_host* bvh, void* nodes, void* triangles);
 int myrt_bvh8_free(myrt_bvh8_host* bvh);
 
+/* Launch configuration of the traversal kernels (set by hand or by the
+ * autotuner, myrt_b200/autotune.py). */
+typedef struct myrt_tuning {
+  uint32_t trace_persistent; /* 0: one thread per ray; 1: persistent warps that refill finished lanes */
+  uint32_t refill;           /* persistent: refill once at least this many lanes of a warp are idle (1..32) */
+  uint32_t blocks_per_sm;    /* persistent: resident 128-thread blocks per SM (0 = occupancy maximum) */
+  uint32_t trace_min_blocks; /* one-thread-per-ray: register cap as blocks per SM: 0 or 8 (64 regs), 10, 12 */
+  uint32_t trace_unit_steps; /* one-thread-per-ray: 0 = a node and all its triangles per iteration,
+                                1 = one node, triangle or pop per iteration */
+} myrt_tuning;
+
 /* ---- context ------------------------------------------------------------ */
 
 /* Replaces the GL context + sequential_pathtracer construction
@@ -147,6 +158,10 @@ int myrt_ctx_destroy(myrt_ctx* ctx);
 int myrt_get_last_error(myrt_ctx* ctx, char* buf, size_t size);
 /* The context's CUDA stream (cudaStream_t) for callers that enqueue work. */
 int myrt_get_stream(myrt_ctx* ctx, void** stream);
+/* Traversal launch configuration (no counterpart in the reference, whose
+ * dispatch sizes are fixed at 64 per group). */
+int myrt_set_tuning(myrt_ctx* ctx, const myrt_tuning* tuning);
+int myrt_get_tuning(myrt_ctx* ctx, myrt_tuning* tuning);
 
 /* ---- scene ---------------------------------------------------------------- */
 

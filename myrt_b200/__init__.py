@@ -94,6 +94,16 @@ class Context:
             self._L.myrt_get_last_error(self._h, buf, 512)
             raise MyrtError(rc, f"{what}: {buf.value.decode(errors='replace')}")
 
+    def set_tuning(self, trace_persistent: int = 0, refill: int = 1, blocks_per_sm: int = 0,
+                   trace_min_blocks: int = 0, trace_unit_steps: int = 0):
+        t = _abi.myrt_tuning(trace_persistent, refill, blocks_per_sm, trace_min_blocks, trace_unit_steps)
+        self._check(self._L.myrt_set_tuning(self._h, C.byref(t)), "myrt_set_tuning")
+
+    def get_tuning(self) -> dict:
+        t = _abi.myrt_tuning()
+        self._check(self._L.myrt_get_tuning(self._h, C.byref(t)), "myrt_get_tuning")
+        return {f: getattr(t, f) for f, _ in _abi.myrt_tuning._fields_}
+
     @property
     def stream(self) -> int:
         s = C.c_void_p()

@@ -62,6 +62,11 @@ class myrt_render_params(C.Structure):
                 ("shading", C.c_int32), ("flags", C.c_uint32)]
 
 
+class myrt_tuning(C.Structure):
+    _fields_ = [("trace_persistent", C.c_uint32), ("refill", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("trace_min_blocks", C.c_uint32), ("trace_unit_steps", C.c_uint32)]
+
+
 SHADE_REFERENCE = 0
 
 P = C.c_void_p
@@ -79,6 +84,8 @@ SIGNATURES = {
     "myrt_ctx_destroy": (I, [P]),
     "myrt_get_last_error": (I, [P, C.c_char_p, SZ]),
     "myrt_get_stream": (I, [P, C.POINTER(P)]),
+    "myrt_set_tuning": (I, [P, C.POINTER(myrt_tuning)]),
+    "myrt_get_tuning": (I, [P, C.POINTER(myrt_tuning)]),
     "myrt_scene_upload": (I, [P, C.POINTER(myrt_scene_view)]),
     "myrt_scene_bvh_info": (I, [P, C.POINTER(myrt_bvh_info)]),
     "myrt_trace_closest": (I, [P, P, U32, P, I]),

@@ -77,19 +77,68 @@ int ensure_stage(myrt_ctx* ctx, size_t bytes) {
 
 constexpr uint32_t kChunkRays = 1u << 20;
 
+constexpr uint32_t kCounterRing = 64;
+
+template <int ISECT, bool ANY, bool STATS>
+int launch_persistent(myrt_ctx* ctx, trace_args const& a, cudaStream_t s) {
+  static int occ = 0;  // resident blocks per SM at 128 threads (per instantiation)
+  if (!occ) {
+    int rc = check_cuda(ctx,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace_persistent<ISECT, ANY, STATS>, 128, 0),
+        "occupancy query");
+    if (rc) return rc;
+    if (occ < 1) occ = 1;
+  }
+  uint32_t const bps = ctx->tuning.blocks_per_sm ? ctx->tuning.blocks_per_sm : uint32_t(occ);
+  uint32_t grid = uint32_t(ctx->sm_count) * bps;
+  grid = std::max(1u, std::min(grid, (a.n + 127) / 128));
+  uint32_t* counter = ctx->d_next + (ctx->next_slot++ % kCounterRing);
+  int rc = check_cuda(ctx, cudaMemsetAsync(counter, 0, sizeof(uint32_t), s), "ray counter");
+  if (rc) return rc;
+  uint32_t const refill = std::max(1u, std::min(32u, ctx->tuning.refill));
+  k_trace_persistent<ISECT, ANY, STATS><<<grid, 128, 0, s>>>(a, counter, refill);
+  return MYRT_OK;
+}
+
 int launch_trace(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s) {
   if (a.n == 0) return MYRT_OK;
   dim3 const block(128);
   dim3 const grid((a.n + 127) / 128);
-  if (intersector == MYRT_ISECT_REFERENCE) {
-    if (any) k_trace<0, true, false><<<grid, block, 0, s>>>(a);
-    else if (stats) k_trace<0, false, true><<<grid, block, 0, s>>>(a);
-    else k_trace<0, false, false><<<grid, block, 0, s>>>(a);
-  } else {
-    if (any) k_trace<1, true, false><<<grid, block, 0, s>>>(a);
-    else if (stats) k_trace<1, false, true><<<grid, block, 0, s>>>(a);
-    else k_trace<1, false, false><<<grid, block, 0, s>>>(a);
+  if (ctx->tuning.trace_persistent) {
+    int rc;
+    if (intersector == MYRT_ISECT_REFERENCE) {
+      if (any) rc = launch_persistent<0, true, false>(ctx, a, s);
+      else if (stats) rc = launch_persistent<0, false, true>(ctx, a, s);
+      else rc = launch_persistent<0, false, false>(ctx, a, s);
+    } else {
+      if (any) rc = launch_persistent<1, true, false>(ctx, a, s);
+      else if (stats) rc = launch_persistent<1, false, true>(ctx, a, s);
+      else rc = launch_persistent<1, false, false>(ctx, a, s);
+    }
+    if (rc) return rc;
+    return check_cuda(ctx, cudaGetLastError(), "trace launch");
   }
+  uint32_t const mb = ctx->tuning.trace_min_blocks;
+  bool const unit = ctx->tuning.trace_unit_steps != 0;
+  auto go = [&](auto isect_tag) {
+    constexpr int IS = decltype(isect_tag)::value;
+    if (unit) {
+      if (stats) k_trace<IS, false, true, 8, true><<<grid, block, 0, s>>>(a);
+      else if (any) k_trace<IS, true, false, 8, true><<<grid, block, 0, s>>>(a);
+      else k_trace<IS, false, false, 8, true><<<grid, block, 0, s>>>(a);
+    } else if (stats) k_trace<IS, false, true><<<grid, block, 0, s>>>(a);
+    else if (any) {
+      if (mb >= 12) k_trace<IS, true, false, 12><<<grid, block, 0, s>>>(a);
+      else if (mb >= 10) k_trace<IS, true, false, 10><<<grid, block, 0, s>>>(a);
+      else k_trace<IS, true, false><<<grid, block, 0, s>>>(a);
+    } else {
+      if (mb >= 12) k_trace<IS, false, false, 12><<<grid, block, 0, s>>>(a);
+      else if (mb >= 10) k_trace<IS, false, false, 10><<<grid, block, 0, s>>>(a);
+      else k_trace<IS, false, false><<<grid, block, 0, s>>>(a);
+    }
+  };
+  if (intersector == MYRT_ISECT_REFERENCE) go(std::integral_constant<int, 0>{});
+  else go(std::integral_constant<int, 1>{});
   return check_cuda(ctx, cudaGetLastError(), "trace launch");
 }
 
@@ -216,6 +265,10 @@ int myrt_ctx_create(myrt_device_opts const* opts, myrt_ctx** out) {
   if (!rc) rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking), "stream");
   if (!rc) rc = check_cuda(ctx, cudaMalloc(&ctx->d_err, sizeof(uint32_t)), "error word");
   if (!rc) rc = check_cuda(ctx, cudaMemset(ctx->d_err, 0, sizeof(uint32_t)), "error word");
+  if (!rc) rc = check_cuda(ctx, cudaMalloc(&ctx->d_next, kCounterRing * sizeof(uint32_t)), "ray counters");
+  if (!rc)
+    rc = check_cuda(ctx, cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, ctx->device),
+        "SM count");
   if (rc) {
     myrt_ctx_destroy(ctx);
     return rc;
@@ -233,6 +286,7 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   free_render(ctx->render);
   for (auto& p : ctx->stage) cudaFree(p);
   cudaFree(ctx->d_err);
+  cudaFree(ctx->d_next);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
   delete ctx;
@@ -242,6 +296,21 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
 int myrt_get_last_error(myrt_ctx* ctx, char* buf, size_t size) {
   if (!ctx || !buf || size == 0) return MYRT_ERR_INVALID_ARGUMENT;
   std::snprintf(buf, size, "%s", ctx->last_error.c_str());
+  return MYRT_OK;
+}
+
+int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
+  if (!ctx || !t) return MYRT_ERR_INVALID_ARGUMENT;
+  if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
+      t->trace_unit_steps > 1)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
+  ctx->tuning = *t;
+  return MYRT_OK;
+}
+
+int myrt_get_tuning(myrt_ctx* ctx, myrt_tuning* t) {
+  if (!ctx || !t) return MYRT_ERR_INVALID_ARGUMENT;
+  *t = ctx->tuning;
   return MYRT_OK;
 }
 

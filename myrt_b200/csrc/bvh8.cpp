@@ -212,8 +212,99 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
     out.scene_hi[a] = scene.hi[a];
   }
 
-  // ---- collapse to the 8-wide layout, breadth first ----
+  // ---- collapse to the 8-wide layout ----
+  // SAH-optimal collapse by dynamic programming over the binary tree (Ylitie,
+  // Karras, Laine, HPG 2017, sec. 3.1): cost[i-1] is the least SAH cost of
+  // representing binary subtree n with at most i slots of its parent: one leaf
+  // slot (subtrees of at most max_leaf triangles, merged), one internal slot
+  // (a new wide node whose 8 slots are split between n's two children), or the
+  // i slots split between the children directly.
   auto const& bn = bld.nodes;
+  constexpr float kNodeCost = 1.0f, kPrimCost = 0.3f, kInf = std::numeric_limits<float>::infinity();
+  struct dp_t {
+    float cost[8];
+    std::uint8_t dec[8];    // 0 leaf slot, 1 internal slot, 2 split between children, 3 use one slot fewer
+    std::uint8_t split[8];  // left share for dec == 2
+    std::uint8_t split8;    // left share of the 8 slots when n becomes a wide node
+  };
+  std::vector<dp_t> D(nb);
+  std::vector<std::uint32_t> ntri(nb);
+  for (std::int64_t i = std::int64_t(nb) - 1; i >= 0; --i) {
+    bnode const& b = bn[std::size_t(i)];
+    dp_t& d = D[std::size_t(i)];
+    float const area = b.box.area();
+    if (b.left < 0) {
+      ntri[std::size_t(i)] = b.count;
+      float const leaf = area * kPrimCost * float(b.count);
+      for (int j = 0; j < 8; ++j) {
+        d.cost[j] = leaf;
+        d.dec[j] = j == 0 ? 0 : 3;
+        d.split[j] = 0;
+      }
+      d.split8 = 0;
+      continue;
+    }
+    std::size_t const L = std::size_t(b.left), R = L + 1;
+    ntri[std::size_t(i)] = ntri[L] + ntri[R];
+    float dist[9];
+    std::uint8_t dsplit[9];
+    for (int j = 2; j <= 8; ++j) {
+      dist[j] = kInf;
+      dsplit[j] = 1;
+      for (int k = 1; k < j; ++k) {
+        float const c = D[L].cost[k - 1] + D[R].cost[j - k - 1];
+        if (c < dist[j]) {
+          dist[j] = c;
+          dsplit[j] = std::uint8_t(k);
+        }
+      }
+    }
+    float const leaf = ntri[std::size_t(i)] <= std::uint32_t(opt.max_leaf) ? area * kPrimCost * float(ntri[std::size_t(i)])
+                                                                           : kInf;
+    float const internal = area * kNodeCost + dist[8];
+    d.split8 = dsplit[8];
+    d.cost[0] = std::min(leaf, internal);
+    d.dec[0] = leaf <= internal ? 0 : 1;
+    d.split[0] = 0;
+    for (int j = 2; j <= 8; ++j) {
+      if (dist[j] < d.cost[j - 2]) {
+        d.cost[j - 1] = dist[j];
+        d.dec[j - 1] = 2;
+        d.split[j - 1] = dsplit[j];
+      } else {
+        d.cost[j - 1] = d.cost[j - 2];
+        d.dec[j - 1] = 3;
+        d.split[j - 1] = 0;
+      }
+    }
+  }
+  // slots of the wide node made from binary node n, as (binary node, is_internal)
+  struct slot_t {
+    std::uint32_t bnode;
+    bool internal;
+  };
+  auto gather = [&](auto&& self, std::uint32_t n, int i, std::vector<slot_t>& out_slots) -> void {
+    dp_t const& d = D[n];
+    switch (d.dec[i - 1]) {
+      case 3: self(self, n, i - 1, out_slots); break;
+      case 2:
+        self(self, std::uint32_t(bn[n].left), d.split[i - 1], out_slots);
+        self(self, std::uint32_t(bn[n].left + 1), i - d.split[i - 1], out_slots);
+        break;
+      case 0: out_slots.push_back({n, false}); break;
+      default: out_slots.push_back({n, true}); break;
+    }
+  };
+  // triangles of a leaf slot: every binary leaf under n, in order
+  auto collect = [&](auto&& self, std::uint32_t n, std::vector<std::uint32_t>& prims) -> void {
+    if (bn[n].left < 0) {
+      for (std::uint32_t k = 0; k < bn[n].count; ++k) prims.push_back(bld.order[bn[n].begin + k]);
+      return;
+    }
+    self(self, std::uint32_t(bn[n].left), prims);
+    self(self, std::uint32_t(bn[n].left + 1), prims);
+  };
+
   struct item {
     std::uint32_t bnode;
     int depth;
@@ -224,33 +315,21 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
   out.triangles.reserve(n_tris);
   int wide_depth = 0;
   std::size_t leaf_slots = 0;
+  std::vector<slot_t> slots;
+  std::vector<std::uint32_t> prims;
   for (std::size_t qi = 0; qi < queue.size(); ++qi) {
     item const it = queue[qi];
     wide_depth = std::max(wide_depth, it.depth);
-    std::uint32_t kids[8];
-    int nk = 0;
+    slots.clear();
     if (bn[it.bnode].left < 0) {
-      kids[nk++] = it.bnode;  // a lone leaf (tiny scenes): one leaf slot
+      slots.push_back({it.bnode, false});  // a lone leaf (tiny scenes): one leaf slot
     } else {
-      kids[nk++] = std::uint32_t(bn[it.bnode].left);
-      kids[nk++] = std::uint32_t(bn[it.bnode].left + 1);
-      while (nk < 8) {
-        int pick = -1;
-        float best = -1.f;
-        for (int k = 0; k < nk; ++k) {
-          if (bn[kids[k]].left < 0) continue;
-          float const a = bn[kids[k]].box.area();
-          if (a > best) {
-            best = a;
-            pick = k;
-          }
-        }
-        if (pick < 0) break;
-        std::uint32_t const c = kids[pick];
-        kids[pick] = std::uint32_t(bn[c].left);
-        kids[nk++] = std::uint32_t(bn[c].left + 1);
-      }
+      gather(gather, std::uint32_t(bn[it.bnode].left), D[it.bnode].split8, slots);
+      gather(gather, std::uint32_t(bn[it.bnode].left + 1), 8 - D[it.bnode].split8, slots);
     }
+    int const nk = int(slots.size());
+    std::uint32_t kids[8];
+    for (int k = 0; k < nk; ++k) kids[k] = slots[std::size_t(k)].bnode;
 
     box3 nbox;
     for (int k = 0; k < nk; ++k) nbox.grow(bn[kids[k]].box);
@@ -289,8 +368,15 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
       }
     }
     std::int32_t slot_kid[8];
-    for (int s = 0; s < 8; ++s) slot_kid[s] = -1;
-    for (int k = 0; k < nk; ++k) slot_kid[slot_of[k]] = std::int32_t(kids[k]);
+    bool slot_internal[8];
+    for (int s = 0; s < 8; ++s) {
+      slot_kid[s] = -1;
+      slot_internal[s] = false;
+    }
+    for (int k = 0; k < nk; ++k) {
+      slot_kid[slot_of[k]] = std::int32_t(kids[k]);
+      slot_internal[slot_of[k]] = slots[std::size_t(k)].internal;
+    }
 
     bvh8_node node{};
     node.px = nbox.lo[0];
@@ -321,15 +407,17 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
         node.qlo[a][s] = std::uint8_t(std::clamp(lo, 0.0, 255.0));
         node.qhi[a][s] = std::uint8_t(std::clamp(hi, 0.0, 255.0));
       }
-      if (c.left >= 0) {
+      if (slot_internal[s]) {
         node.imask |= std::uint8_t(1u << s);
         node.meta[s] = std::uint8_t(0x20u | unsigned(s));
         out.nodes.emplace_back();
         queue.push_back({std::uint32_t(slot_kid[s]), it.depth + 1});
       } else {
-        node.meta[s] = std::uint8_t(tri_off | (c.count << 5));
-        for (std::uint32_t i = 0; i < c.count; ++i) {
-          std::uint32_t const prim = bld.order[c.begin + i];
+        prims.clear();
+        collect(collect, std::uint32_t(slot_kid[s]), prims);
+        std::uint32_t const cnt = std::uint32_t(prims.size());
+        node.meta[s] = std::uint8_t(tri_off | (cnt << 5));
+        for (std::uint32_t prim : prims) {
           float const* v = positions + 9 * std::size_t(prim);
           bvh8_triangle t{};
           std::memcpy(t.v0, v, 12);
@@ -338,7 +426,7 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
           t.prim = prim_ids ? prim_ids[prim] : prim;
           out.triangles.push_back(t);
         }
-        tri_off += c.count;
+        tri_off += cnt;
         ++leaf_slots;
       }
     }

@@ -55,6 +55,10 @@ struct myrt_ctx {
   myrt_b200::device_scene scene;
   myrt_b200::render_state render;
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
+  myrt_tuning tuning{0u, 1u, 0u, 0u};
+  int sm_count = 0;
+  uint32_t* d_next = nullptr;    // ring of ray counters for the persistent traversal
+  uint32_t next_slot = 0;
   // staging buffers of the host-memory entry points (two chunk slots)
   void* stage[2] = {nullptr, nullptr};
   size_t stage_bytes = 0;

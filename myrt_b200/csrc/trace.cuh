@@ -132,7 +132,12 @@ struct trace_args {
   uint32_t* err;
 };
 
-__device__ __forceinline__ float q8(uint32_t w, int s) { return float((w >> (8 * (s & 3))) & 0xffu); }
+// Byte (s & 3) of w as an exact float: one byte permute places it in the low
+// mantissa bits of 2^23 (0x4B0000bb), one subtraction removes 2^23. This keeps
+// the 48 plane conversions per node off the quarter-rate conversion pipe.
+__device__ __forceinline__ float q8(uint32_t w, int s) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | uint32_t(s & 3))) - 8388608.0f;
+}
 
 struct hit_rec {
   int32_t prim;   // -1 = none
@@ -140,35 +145,55 @@ struct hit_rec {
   uint32_t leaf;  // index of the hit triangle in the leaf-ordered array
 };
 
-// Walks the tree for one ray. Closest hit (ANY = false): fills h and returns
-// whether a triangle was hit. Any hit (ANY = true): returns true at the first
-// triangle with tmin <= t < tmax. n_nodes / n_tris count fetched nodes and
-// tested triangles when STATS.
-template <int ISECT, bool ANY, bool STATS>
-__device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris, f3 o, f3 d,
-    float tmin, float tmax, hit_rec& h, uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris) {
-  // Box-test reciprocal: zero components are nudged so no 0 * inf appears.
-  float const idx = 1.0f / (fabsf(d.x) > 1e-20f ? d.x : copysignf(1e-20f, d.x));
-  float const idy = 1.0f / (fabsf(d.y) > 1e-20f ? d.y : copysignf(1e-20f, d.y));
-  float const idz = 1.0f / (fabsf(d.z) > 1e-20f ? d.z : copysignf(1e-20f, d.z));
-  uint32_t const oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
-  uint32_t const octinv = oct ^ 7u;
-  wt_ray wt{};
-  if (ISECT == 1) wt = wt_setup(d);
+// Per-ray traversal state of the 8-wide walk. step() performs one iteration
+// (visit the next node of the current group, pushing the group if siblings
+// remain, then test the triangles its leaf slots hit, then pop if the group is
+// exhausted) and returns false once the ray is finished. The per-thread loop
+// (traverse) and the persistent kernel (which refills finished lanes with new
+// rays) both drive it, so they visit the same nodes in the same order.
+template <int ISECT, bool ANY>
+struct walker {
+  f3 o, d;
+  float tmin, tmax;
+  float idx, idy, idz;  // box-test reciprocals, zero components nudged (no 0 * inf)
+  uint32_t octinv;
+  wt_ray wt;
+  float tbest;
+  int32_t best;
+  float bu, bv;
+  uint32_t bleaf;
+  uint2 group;
+  int sp;
+  bool occluded;
 
-  float tbest = tmax;
-  int32_t best = -1;
-  float bu = 0.f, bv = 0.f;
-  uint32_t bleaf = 0;
-  bool occluded = false;
+  __device__ __forceinline__ void init(f3 o_, f3 d_, float tmin_, float tmax_) {
+    o = o_;
+    d = d_;
+    tmin = tmin_;
+    tmax = tmax_;
+    idx = 1.0f / (fabsf(d.x) > 1e-20f ? d.x : copysignf(1e-20f, d.x));
+    idy = 1.0f / (fabsf(d.y) > 1e-20f ? d.y : copysignf(1e-20f, d.y));
+    idz = 1.0f / (fabsf(d.z) > 1e-20f ? d.z : copysignf(1e-20f, d.z));
+    uint32_t const oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+    octinv = oct ^ 7u;
+    if (ISECT == 1) wt = wt_setup(d);
+    tbest = tmax;
+    best = -1;
+    bu = bv = 0.f;
+    bleaf = 0;
+    occluded = false;
+    sp = 0;
+    group = make_uint2(0u, 0x80000000u);  // root: bit of slot 7 ^ octinv, imask 0 -> node 0
+    tg = make_uint2(0u, 0u);
+  }
 
-  uint2 stack[MYRT_STACK_MAX];
-  int sp = 0;
-  uint2 group = make_uint2(0u, 0x80000000u);  // root: bit of slot 7 ^ octinv, imask 0 -> node 0
-
-  while (true) {
-    uint2 tgroup = make_uint2(0u, 0u);
-    if (group.y & 0xff000000u) {
+  // Visits the next node of the current group: pushes the group if siblings
+  // remain, replaces it by the node's hit internal children and returns the
+  // hit leaf triangles in tgroup. False on a stack overflow (recorded in err).
+  template <bool STATS>
+  __device__ __forceinline__ bool visit(uint4 const* __restrict__ nodes, uint2* stack, uint32_t* err,
+      uint32_t& n_nodes, uint2& tgroup) {
+    {
       uint32_t const pos = 31u - __clz(group.y & 0xff000000u);
       group.y &= ~(1u << pos);
       uint32_t const slot = (pos - 24u) ^ octinv;
@@ -176,7 +201,7 @@ __device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4
       if (group.y & 0xff000000u) {
         if (sp >= MYRT_STACK_MAX) {
           atomicOr(err, ERR_STACK_OVERFLOW);
-          break;
+          return false;
         }
         stack[sp++] = group;
       }
@@ -224,64 +249,117 @@ __device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4
       }
       group = make_uint2(w1.x, hit_internal | imask);
       tgroup = make_uint2(w1.y, hit_tris);
+    }
+    return true;
+  }
+
+  // Tests leaf triangle `leaf`. False when an any-hit query is answered.
+  template <bool STATS>
+  __device__ __forceinline__ bool test(float4 const* __restrict__ tris, uint32_t leaf, uint32_t& n_tris) {
+    float4 const* tp = tris + 3 * size_t(leaf);
+    float4 const p0 = __ldg(tp + 0);
+    float4 const p1 = __ldg(tp + 1);
+    float4 const p2 = __ldg(tp + 2);
+    if (STATS) ++n_tris;
+    float t, u, v;
+    bool hit;
+    if (ISECT == 0)
+      hit = isect_reference(o, d, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, t, u, v) &&
+          t >= tmin;
+    else
+      hit = isect_watertight(wt, o, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, tmin, t, u, v);
+    if (!hit) return true;
+    int32_t const prim = __float_as_int(p0.w);
+    if (ANY) {
+      if (t < tmax) {
+        occluded = true;
+        return false;
+      }
+    } else if (t < tbest || (t == tbest && best >= 0 && prim < best)) {
+      tbest = t;
+      best = prim;
+      bu = u;
+      bv = v;
+      bleaf = leaf;
+    }
+    return true;
+  }
+
+  // One iteration: visit a node, test all the triangles it hit, pop if the
+  // current group is exhausted.
+  template <bool STATS>
+  __device__ __forceinline__ bool step(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris, uint2* stack,
+      uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris) {
+    uint2 tgroup = make_uint2(0u, 0u);
+    if (group.y & 0xff000000u) {
+      if (!visit<STATS>(nodes, stack, err, n_nodes, tgroup)) return false;
     } else {
       group.y = 0;
     }
-
     while (tgroup.y) {
       uint32_t const b = __ffs(tgroup.y) - 1u;
       tgroup.y &= tgroup.y - 1u;
-      float4 const* tp = tris + 3 * size_t(tgroup.x + b);
-      float4 const p0 = __ldg(tp + 0);
-      float4 const p1 = __ldg(tp + 1);
-      float4 const p2 = __ldg(tp + 2);
-      if (STATS) ++n_tris;
-      float t, u, v;
-      bool hit;
-      if (ISECT == 0)
-        hit = isect_reference(o, d, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, t, u, v) &&
-            t >= tmin;
-      else
-        hit = isect_watertight(wt, o, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, tmin, t, u, v);
-      if (!hit) continue;
-      int32_t const prim = __float_as_int(p0.w);
-      if (ANY) {
-        if (t < tmax) {
-          occluded = true;
-          break;
-        }
-      } else if (t < tbest || (t == tbest && best >= 0 && prim < best)) {
-        tbest = t;
-        best = prim;
-        bu = u;
-        bv = v;
-        bleaf = tgroup.x + b;
-      }
+      if (!test<STATS>(tris, tgroup.x + b, n_tris)) return false;
     }
-    if (ANY && occluded) break;
     if (!(group.y & 0xff000000u)) {
-      if (sp == 0) break;
+      if (sp == 0) return false;
       group = stack[--sp];
     }
+    return true;
   }
 
-  if (ANY) return occluded;
-  h.prim = best;
-  h.t = best >= 0 ? tbest : tmax;
-  h.u = best >= 0 ? bu : 0.f;
-  h.v = best >= 0 ? bv : 0.f;
-  h.leaf = bleaf;
-  return best >= 0;
+  // One unit of work per iteration: one triangle, one node or one pop, in the
+  // same order as step(), so lanes of a warp stay busy with similar amounts of
+  // work. Uses the member tg for triangles carried between iterations.
+  uint2 tg;
+  template <bool STATS>
+  __device__ __forceinline__ bool step_unit(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris,
+      uint2* stack, uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris) {
+    if (tg.y) {
+      uint32_t const b = __ffs(tg.y) - 1u;
+      tg.y &= tg.y - 1u;
+      return test<STATS>(tris, tg.x + b, n_tris);
+    }
+    if (group.y & 0xff000000u) return visit<STATS>(nodes, stack, err, n_nodes, tg);
+    if (sp == 0) return false;
+    group = stack[--sp];
+    return true;
+  }
+
+  __device__ __forceinline__ void result(hit_rec& h) const {
+    h.prim = best;
+    h.t = best >= 0 ? tbest : tmax;
+    h.u = best >= 0 ? bu : 0.f;
+    h.v = best >= 0 ? bv : 0.f;
+    h.leaf = bleaf;
+  }
+};
+
+// Walks the tree for one ray. Closest hit (ANY = false): fills h and returns
+// whether a triangle was hit. Any hit (ANY = true): returns true at the first
+// triangle with tmin <= t < tmax. n_nodes / n_tris count fetched nodes and
+// tested triangles when STATS.
+template <int ISECT, bool ANY, bool STATS, bool UNIT = false>
+__device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris, f3 o, f3 d,
+    float tmin, float tmax, hit_rec& h, uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris) {
+  uint2 stack[MYRT_STACK_MAX];
+  walker<ISECT, ANY> w;
+  w.init(o, d, tmin, tmax);
+  if (UNIT) {
+    while (w.template step_unit<STATS>(nodes, tris, stack, err, n_nodes, n_tris)) {
+    }
+  } else {
+    while (w.template step<STATS>(nodes, tris, stack, err, n_nodes, n_tris)) {
+    }
+  }
+  if (ANY) return w.occluded;
+  w.result(h);
+  return h.prim >= 0;
 }
 
 template <int ISECT, bool ANY, bool STATS>
-__device__ __forceinline__ void trace_one(trace_args const& a, uint32_t i) {
-  float4 const r0 = __ldg(a.rays + 2 * size_t(i));
-  float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
-  hit_rec h;
-  uint32_t n_nodes = 0, n_tris = 0;
-  bool const r = traverse<ISECT, ANY, STATS>(a.nodes, a.tris, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w, r1.w,
-      h, a.err, n_nodes, n_tris);
+__device__ __forceinline__ void store_result(trace_args const& a, uint32_t i, bool r, hit_rec const& h,
+    uint32_t n_nodes, uint32_t n_tris) {
   if (ANY) {
     a.occluded[i] = r ? 1 : 0;
   } else {
@@ -293,11 +371,63 @@ __device__ __forceinline__ void trace_one(trace_args const& a, uint32_t i) {
   }
 }
 
-template <int ISECT, bool ANY, bool STATS>
-__global__ void __launch_bounds__(128) k_trace(trace_args a) {
+// One thread per ray. MINB = resident 128-thread blocks per SM the compiler
+// must allow (8 leaves it 64 registers; more blocks cap the register count).
+template <int ISECT, bool ANY, bool STATS, int MINB = 8, bool UNIT = false>
+__global__ void __launch_bounds__(128, MINB) k_trace(trace_args a) {
   uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n) return;
-  trace_one<ISECT, ANY, STATS>(a, i);
+  float4 const r0 = __ldg(a.rays + 2 * size_t(i));
+  float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
+  hit_rec h;
+  uint32_t n_nodes = 0, n_tris = 0;
+  bool const r = traverse<ISECT, ANY, STATS, UNIT>(a.nodes, a.tris, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w,
+      r1.w, h, a.err, n_nodes, n_tris);
+  store_result<ISECT, ANY, STATS>(a, i, r, h, n_nodes, n_tris);
+}
+
+// Persistent variant: a fixed grid of warps; whenever at least `refill` lanes
+// of a warp have finished their ray, those lanes take the next rays from a
+// global counter (one atomic per warp), so warps stay full instead of waiting
+// for their slowest ray (Aila and Laine, HPG 2009: persistent threads with
+// dynamic fetch). *next must be 0 at launch.
+template <int ISECT, bool ANY, bool STATS>
+__global__ void __launch_bounds__(128) k_trace_persistent(trace_args a, uint32_t* __restrict__ next, uint32_t refill) {
+  uint2 stack[MYRT_STACK_MAX];
+  walker<ISECT, ANY> w;
+  uint32_t const lane = threadIdx.x & 31u;
+  uint32_t ray = 0;
+  uint32_t n_nodes = 0, n_tris = 0;
+  bool active = false;
+  bool pool_left = true;  // warp-uniform
+  while (true) {
+    uint32_t const idle = __ballot_sync(0xffffffffu, !active);
+    if (pool_left && __popc(idle) >= int(idle == 0xffffffffu ? 1u : refill)) {
+      uint32_t const leader = __ffs(idle) - 1u;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(next, uint32_t(__popc(idle)));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (base + uint32_t(__popc(idle)) >= a.n) pool_left = false;
+      if (!active) {
+        uint32_t const mine = base + __popc(idle & ((1u << lane) - 1u));
+        if (mine < a.n) {
+          float4 const r0 = __ldg(a.rays + 2 * size_t(mine));
+          float4 const r1 = __ldg(a.rays + 2 * size_t(mine) + 1);
+          w.init(f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w, r1.w);
+          ray = mine;
+          n_nodes = n_tris = 0;
+          active = true;
+        }
+      }
+    }
+    if (!__any_sync(0xffffffffu, active)) break;
+    if (active && !w.template step<STATS>(a.nodes, a.tris, stack, a.err, n_nodes, n_tris)) {
+      hit_rec h;
+      if (!ANY) w.result(h);
+      store_result<ISECT, ANY, STATS>(a, ray, ANY ? w.occluded : h.prim >= 0, h, n_nodes, n_tris);
+      active = false;
+    }
+  }
 }
 
 }  // namespace myrt_b200

@@ -152,3 +152,55 @@ def test_errors_are_reported(ctx):
         ctx.upload_scene(np.array([0, 1, 7], np.uint32), np.zeros((3, 3), np.float32))  # index out of range
     with pytest.raises(mb.MyrtError):
         ctx.trace_closest(np.zeros((4, 8), np.float32), intersector=7)
+
+
+@pytest.mark.parametrize("refill", [1, 8, 32])
+def test_persistent_traversal_bit_exact(ctx, hf128, refill):
+    """The persistent kernel (lanes refilled with new rays) visits the same nodes
+    per ray as the one-thread-per-ray kernel: same hits, same counters."""
+    import torch
+
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = np.concatenate([pinhole_rays(256, 256), _rand_rays(100_000, seed=21)])
+    ora, cn, ct = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays)
+    try:
+        ctx.set_tuning(trace_persistent=1, refill=refill, blocks_per_sm=0)
+        assert np.array_equal(ctx.trace_closest(rays), ora)
+        occ = ctx.trace_any(rays)
+        assert np.array_equal(occ.astype(bool), ora["prim"] >= 0)
+        d_rays = torch.from_numpy(rays).cuda()
+        d_hits = torch.empty((rays.shape[0], 4), dtype=torch.float32, device="cuda")
+        d_n = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        d_t = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.trace_closest_stats_device(d_rays, d_hits, d_n, d_t)
+        ctx.sync()
+        assert np.array_equal(d_hits.cpu().numpy().view(mb.HIT_DTYPE).ravel(), ora)
+        assert np.array_equal(d_n.cpu().numpy().astype(np.uint32), cn)
+        assert np.array_equal(d_t.cpu().numpy().astype(np.uint32), ct)
+    finally:
+        ctx.set_tuning(trace_persistent=0)
+
+
+def test_unit_step_traversal_bit_exact(ctx, hf128):
+    """One node / triangle / pop per iteration walks the same order: same hits and counters."""
+    import torch
+
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = np.concatenate([pinhole_rays(256, 256), _rand_rays(100_000, seed=22)])
+    ora, cn, ct = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays)
+    try:
+        ctx.set_tuning(trace_unit_steps=1)
+        assert np.array_equal(ctx.trace_closest(rays), ora)
+        assert np.array_equal(ctx.trace_any(rays).astype(bool), ora["prim"] >= 0)
+        d_rays = torch.from_numpy(rays).cuda()
+        d_hits = torch.empty((rays.shape[0], 4), dtype=torch.float32, device="cuda")
+        d_n = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        d_t = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.trace_closest_stats_device(d_rays, d_hits, d_n, d_t)
+        ctx.sync()
+        assert np.array_equal(d_n.cpu().numpy().astype(np.uint32), cn)
+        assert np.array_equal(d_t.cpu().numpy().astype(np.uint32), ct)
+    finally:
+        ctx.set_tuning()
