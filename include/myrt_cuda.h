@@ -193,6 +193,72 @@ int myrt_trace_any_device(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, uint8
 int myrt_trace_closest_stats_device(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, myrt_hit* hits,
     uint32_t* nodes, uint32_t* tris, int intersector, void* stream);
 
+/* ---- SDF drawables ------------------------------------------------------------ */
+
+/* Flat SDF program instructions. The reference compiles an instruction tree
+ * (src/pathtracer/sdf.hpp:399-633) into GLSL (sdf.cpp:122-407); this core
+ * evaluates the same tree as a post-order program: modifier instructions move
+ * the position of the next primitive (innermost first), primitives push a
+ * distance and a material, operators pop two and push one. param_offset indexes
+ * the float parameter buffer, laid out per type as the reference's sdf_data
+ * (float = 1 block, int = 1 block holding the value, vec3 = 3 blocks). */
+typedef enum myrt_sdf_op {
+  MYRT_SDF_SPHERE = 1,        /* radius, material */
+  MYRT_SDF_BOX = 2,           /* size.xyz, material */
+  MYRT_SDF_TORUS = 3,         /* radius_large, radius_small, material */
+  MYRT_SDF_CAPSULE = 4,       /* vertical capsule: height, radius, material */
+  MYRT_SDF_MENGER = 5,        /* material */
+  MYRT_SDF_UNION = 16,
+  MYRT_SDF_SUBTRACTION = 17,
+  MYRT_SDF_INTERSECTION = 18,
+  MYRT_SDF_SMOOTH_UNION = 19, /* factor */
+  MYRT_SDF_TRANSLATE = 32,    /* offset.xyz */
+  MYRT_SDF_MIRROR = 33        /* axis */
+} myrt_sdf_op;
+
+typedef struct myrt_sdf_instr {
+  int32_t op;
+  int32_t param_offset;
+} myrt_sdf_instr;
+
+typedef struct myrt_sdf_program {
+  int32_t first; /* first instruction */
+  int32_t count;
+} myrt_sdf_program;
+
+/* scene::drawable_sdf_t (src/pathtracer/scene.hpp:105-110): 144 bytes. */
+typedef struct myrt_sdf_drawable {
+  float transformation[16];         /* column-major */
+  float inverse_transformation[16]; /* column-major */
+  int32_t sdf_index;                /* program index */
+  int32_t pad[3];
+} myrt_sdf_drawable;
+
+typedef struct myrt_sdf_view {
+  const myrt_sdf_instr* instrs;
+  size_t instr_count;
+  const myrt_sdf_program* programs;
+  size_t program_count;
+  const float* params;
+  size_t param_count;
+  const myrt_sdf_drawable* drawables;
+  size_t drawable_count;
+} myrt_sdf_view;
+
+/* Replaces the SDF half of scene::prepare (sdf data + drawable uploads,
+ * src/pathtracer/scene.cpp:345-351, 399-401) and the GLSL assembly of
+ * sdf_glsl_assembler (sdf.cpp:378-407). Programs are validated (opcodes,
+ * parameter ranges, stack depth <= 24, one result). drawable_count == 0
+ * removes all SDF drawables. Restarts accumulation. */
+int myrt_sdf_upload(myrt_ctx* ctx, const myrt_sdf_view* sdf);
+/* SDF part of nearest_hit / any_hit (src/pt/pt_trace.comp:321-326, 342-352)
+ * over all SDF drawables for n host rays (tmax = max distance), with
+ * raymarch.glsl's marching (steps, eps). rng_states (may be NULL: all 0) start
+ * each ray's random stream, which picks materials at operator blends. out: 8
+ * floats per ray: hit (0/1), t, normal xyz, u, v, material (int bits). */
+int myrt_trace_sdf(myrt_ctx* ctx, const myrt_ray* rays, uint32_t n, int32_t steps, float eps, int any_hit,
+    const uint32_t* rng_states, float* out);
+
 /* ---- wavefront rendering ---------------------------------------------------- */
 
 /* The matrices sequential_pathtracer uploads to pt_generate.comp (column-major):
@@ -216,6 +282,8 @@ typedef struct myrt_render_params {
   uint32_t frames;     /* frames (one sample per pixel each) to accumulate in this call */
   int32_t shading;     /* myrt_shading */
   uint32_t flags;      /* reserved, 0 */
+  int32_t sdf_marching_steps;  /* set_sdf_marching_steps (reference default 400) */
+  float sdf_marching_epsilon;  /* set_sdf_marching_epsilon (reference default 1e-5) */
 } myrt_render_params;
 
 /* Renders `frames` frames, each the reference's generate -> {trace, color,

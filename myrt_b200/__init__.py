@@ -137,6 +137,27 @@ class Context:
         self._check(self._L.myrt_scene_upload(self._h, C.byref(view)), "myrt_scene_upload")
         return self.bvh_info()
 
+    def upload_sdf(self, instrs, programs, params, drawables):
+        """SDF programs + drawables (myrt_sdf_upload). drawables: float32 [N, 36]
+        (myrt_b200.sdf.sdf_drawables); an empty array removes all SDF drawables."""
+        ins = np.ascontiguousarray(instrs, np.int32).reshape(-1, 2)
+        prs = np.ascontiguousarray(programs, np.int32).reshape(-1, 2)
+        par = np.ascontiguousarray(params, np.float32).ravel()
+        dr = np.ascontiguousarray(drawables, np.float32).reshape(-1, 36)
+        view = _abi.myrt_sdf_view(ins.ctypes.data, ins.shape[0], prs.ctypes.data, prs.shape[0], par.ctypes.data,
+                                  par.size, dr.ctypes.data, dr.shape[0])
+        self._check(self._L.myrt_sdf_upload(self._h, C.byref(view)), "myrt_sdf_upload")
+
+    def trace_sdf(self, rays, steps: int, eps: float, any_hit: bool = False, rng_states=None) -> dict:
+        """SDF closest / any hit for host rays (myrt_trace_sdf)."""
+        r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        out = np.empty((r.shape[0], 8), np.float32)
+        rs = None if rng_states is None else np.ascontiguousarray(rng_states, np.uint32)
+        self._check(self._L.myrt_trace_sdf(self._h, r.ctypes.data, r.shape[0], steps, eps, int(any_hit),
+                                           _ptr(rs), out.ctypes.data), "myrt_trace_sdf")
+        return dict(hit=out[:, 0].astype(np.int32), t=out[:, 1].copy(), normal=out[:, 2:5].copy(),
+                    uv=out[:, 5:7].copy(), material=out[:, 7].copy().view(np.int32))
+
     def bvh_info(self) -> dict:
         info = _abi.myrt_bvh_info()
         self._check(self._L.myrt_scene_bvh_info(self._h, C.byref(info)), "myrt_scene_bvh_info")
@@ -180,22 +201,26 @@ class Context:
 
     # -- wavefront rendering (sequential_pathtracer::run) --
     def render(self, inverse_view, inverse_projection, width: int, height: int, num_bounces: int = 10,
-               frames: int = 1, shading: int = _abi.SHADE_REFERENCE):
+               frames: int = 1, shading: int = _abi.SHADE_REFERENCE, sdf_marching_steps: int = 400,
+               sdf_marching_epsilon: float = 1e-5):
         cam = _abi.myrt_camera()
         cam.inverse_view[:] = np.asarray(inverse_view, np.float32).ravel().tolist()
         cam.inverse_projection[:] = np.asarray(inverse_projection, np.float32).ravel().tolist()
-        p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0)
+        p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0, sdf_marching_steps,
+                                    sdf_marching_epsilon)
         self._check(self._L.myrt_render(self._h, C.byref(cam), C.byref(p)), "myrt_render")
 
     def render_noalloc(self, inverse_view, inverse_projection, width: int, height: int, accum, display,
                        sample_index: int = 0, num_bounces: int = 10, frames: int = 1,
-                       shading: int = _abi.SHADE_REFERENCE, stream: int | None = None):
+                       shading: int = _abi.SHADE_REFERENCE, stream: int | None = None,
+                       sdf_marching_steps: int = 400, sdf_marching_epsilon: float = 1e-5):
         """myrt_render_noalloc: renders into caller-owned device images (torch
         tensors, float32 [H, W, 4]) with no device allocation by the library."""
         cam = _abi.myrt_camera()
         cam.inverse_view[:] = np.asarray(inverse_view, np.float32).ravel().tolist()
         cam.inverse_projection[:] = np.asarray(inverse_projection, np.float32).ravel().tolist()
-        p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0)
+        p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0, sdf_marching_steps,
+                                    sdf_marching_epsilon)
         self._check(self._L.myrt_render_noalloc(self._h, C.byref(cam), C.byref(p), sample_index, _ptr(accum),
                                                 _ptr(display), stream), "myrt_render_noalloc")
 

@@ -59,7 +59,14 @@ class myrt_camera(C.Structure):
 
 class myrt_render_params(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("num_bounces", C.c_int32), ("frames", C.c_uint32),
-                ("shading", C.c_int32), ("flags", C.c_uint32)]
+                ("shading", C.c_int32), ("flags", C.c_uint32), ("sdf_marching_steps", C.c_int32),
+                ("sdf_marching_epsilon", C.c_float)]
+
+
+class myrt_sdf_view(C.Structure):
+    _fields_ = [("instrs", C.c_void_p), ("instr_count", C.c_size_t), ("programs", C.c_void_p),
+                ("program_count", C.c_size_t), ("params", C.c_void_p), ("param_count", C.c_size_t),
+                ("drawables", C.c_void_p), ("drawable_count", C.c_size_t)]
 
 
 class myrt_tuning(C.Structure):
@@ -88,6 +95,8 @@ SIGNATURES = {
     "myrt_get_tuning": (I, [P, C.POINTER(myrt_tuning)]),
     "myrt_scene_upload": (I, [P, C.POINTER(myrt_scene_view)]),
     "myrt_scene_bvh_info": (I, [P, C.POINTER(myrt_bvh_info)]),
+    "myrt_sdf_upload": (I, [P, C.POINTER(myrt_sdf_view)]),
+    "myrt_trace_sdf": (I, [P, P, U32, C.c_int32, C.c_float, I, P, P]),
     "myrt_trace_closest": (I, [P, P, U32, P, I]),
     "myrt_trace_closest_device": (I, [P, P, U32, P, I, P]),
     "myrt_trace_any": (I, [P, P, U32, P, I]),

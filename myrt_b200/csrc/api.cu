@@ -283,6 +283,10 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->aux_stream) cudaStreamSynchronize(ctx->aux_stream);
   free_scene(ctx->scene);
+  cudaFree(ctx->sdf.instrs);
+  cudaFree(ctx->sdf.programs);
+  cudaFree(ctx->sdf.params);
+  cudaFree(ctx->sdf.drawables);
   free_render(ctx->render);
   for (auto& p : ctx->stage) cudaFree(p);
   cudaFree(ctx->d_err);
@@ -419,6 +423,88 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
   s.valid = true;
   ctx->render.sample_counter = 0;  // prepare() reported a change -> invalidate_counter
   return MYRT_OK;
+}
+
+int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
+  if (!ctx || !v) return MYRT_ERR_INVALID_ARGUMENT;
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc) return rc;
+  cudaStreamSynchronize(ctx->stream);
+  device_sdf& D = ctx->sdf;
+  cudaFree(D.instrs);
+  cudaFree(D.programs);
+  cudaFree(D.params);
+  cudaFree(D.drawables);
+  D = device_sdf{};
+  ctx->render.sample_counter = 0;
+  if (v->drawable_count == 0) return MYRT_OK;
+  if (!v->instrs || !v->programs || !v->drawables || (v->param_count && !v->params))
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "null SDF array");
+  // validate every program as the device evaluates it
+  for (size_t p = 0; p < v->program_count; ++p) {
+    myrt_sdf_program const pr = v->programs[p];
+    if (pr.first < 0 || pr.count <= 0 || size_t(pr.first) + size_t(pr.count) > v->instr_count)
+      return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "SDF program outside the instruction array");
+    int depth = 0, max_depth = 0;
+    bool pending_mod = false;
+    for (int k = 0; k < pr.count; ++k) {
+      myrt_sdf_instr const in = v->instrs[pr.first + k];
+      int blocks = 0;
+      switch (in.op) {
+        case MYRT_SDF_SPHERE: blocks = 2; break;
+        case MYRT_SDF_BOX: blocks = 4; break;
+        case MYRT_SDF_TORUS: case MYRT_SDF_CAPSULE: blocks = 3; break;
+        case MYRT_SDF_MENGER: blocks = 1; break;
+        case MYRT_SDF_UNION: case MYRT_SDF_SUBTRACTION: case MYRT_SDF_INTERSECTION: blocks = 0; break;
+        case MYRT_SDF_SMOOTH_UNION: blocks = 1; break;
+        case MYRT_SDF_TRANSLATE: blocks = 3; break;
+        case MYRT_SDF_MIRROR: blocks = 1; break;
+        default: return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "unknown SDF opcode");
+      }
+      if (blocks && (in.param_offset < 0 || size_t(in.param_offset) + size_t(blocks) > v->param_count))
+        return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "SDF parameter outside the parameter buffer");
+      if (in.op == MYRT_SDF_MIRROR) {
+        float const ax = v->params[in.param_offset];
+        if (!(ax == 0.f || ax == 1.f || ax == 2.f)) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "mirror axis");
+      }
+      if (in.op >= MYRT_SDF_TRANSLATE) {
+        pending_mod = true;
+      } else if (in.op >= MYRT_SDF_UNION) {
+        if (depth < 2 || pending_mod) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "SDF operator without two operands");
+        --depth;
+      } else {
+        pending_mod = false;
+        max_depth = std::max(max_depth, ++depth);
+      }
+    }
+    if (depth != 1 || pending_mod) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "SDF program leaves no single result");
+    if (max_depth > 24) return set_error(ctx, MYRT_ERR_UNSUPPORTED, "SDF program stack deeper than 24");
+  }
+  std::vector<float> dr(v->drawable_count * 36);
+  for (size_t d = 0; d < v->drawable_count; ++d) {
+    myrt_sdf_drawable const& s = v->drawables[d];
+    if (s.sdf_index < 0 || size_t(s.sdf_index) >= v->program_count)
+      return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "SDF drawable references a missing program");
+    std::memcpy(&dr[36 * d], &s, sizeof(myrt_sdf_drawable));
+  }
+  rc = upload(ctx, reinterpret_cast<myrt_sdf_instr**>(&D.instrs), v->instrs, v->instr_count, "SDF instructions");
+  if (!rc)
+    rc = upload(ctx, reinterpret_cast<myrt_sdf_program**>(&D.programs), v->programs, v->program_count, "SDF programs");
+  if (!rc && v->param_count) rc = upload(ctx, &D.params, v->params, v->param_count, "SDF parameters");
+  if (!rc) rc = upload(ctx, &D.drawables, dr.data(), dr.size(), "SDF drawables");
+  if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "SDF upload");
+  if (rc) return rc;
+  D.n_drawables = int(v->drawable_count);
+  D.n_programs = int(v->program_count);
+  return MYRT_OK;
+}
+
+int myrt_trace_sdf(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, int32_t steps, float eps, int any_hit,
+    uint32_t const* rng_states, float* out) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!rays || !out) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "null ray or output pointer");
+  if (steps < 0 || !(eps > 0.f)) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "steps >= 0 and eps > 0 required");
+  return trace_sdf_rays(ctx, rays, n, steps, eps, any_hit, rng_states, out);
 }
 
 int myrt_scene_bvh_info(myrt_ctx* ctx, myrt_bvh_info* info) {

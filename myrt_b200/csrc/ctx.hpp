@@ -28,6 +28,16 @@ struct device_scene {
   bool valid = false;
 };
 
+// SDF drawables (uploaded separately; scene::prepare's sdf buffers).
+struct device_sdf {
+  int2* instrs = nullptr;
+  int2* programs = nullptr;
+  float* params = nullptr;
+  float* drawables = nullptr;  // 36 floats each
+  int n_drawables = 0;
+  int n_programs = 0;
+};
+
 // Wavefront render state (sequential_pathtracer's buffers and counters).
 struct render_state {
   uint32_t width = 0, height = 0;
@@ -53,6 +63,7 @@ struct myrt_ctx {
   std::string last_error;
   uint32_t* d_err = nullptr;          // device error word (atomicOr of ERR_* bits)
   myrt_b200::device_scene scene;
+  myrt_b200::device_sdf sdf;
   myrt_b200::render_state render;
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
   myrt_tuning tuning{0u, 1u, 0u, 0u};
@@ -69,6 +80,8 @@ int set_error(myrt_ctx* ctx, int code, std::string msg);
 int check_cuda(myrt_ctx* ctx, cudaError_t e, char const* what);
 void free_render(render_state& r);
 int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p);
+int trace_sdf_rays(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, int steps, float eps, int any_hit,
+    uint32_t const* rng_states, float* out);
 int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p,
     uint32_t sample_index, float4* accum, float4* display, cudaStream_t st);
 }  // namespace myrt_b200

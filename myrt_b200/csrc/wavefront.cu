@@ -32,6 +32,7 @@
 #include "../../include/myrt_cuda.h"
 #include "ctx.hpp"
 #include "refshade.cuh"
+#include "sdf.cuh"
 #include "trace.cuh"
 
 namespace myrt_b200 {
@@ -53,7 +54,13 @@ struct scene_dev {
   int n_mats;
   float const* mat_data;
   uint32_t* err;
+  sdfk::sdf_dev sdf;  // n_drawables == 0: no SDF drawables
 };
+
+sdfk::sdf_dev make_sdf_dev(myrt_ctx const* ctx, int steps, float eps) {
+  device_sdf const& D = ctx->sdf;
+  return sdfk::sdf_dev{D.instrs, D.programs, D.params, D.drawables, D.n_drawables, steps, eps};
+}
 
 struct camera_dev {
   float vp[16];  // inverse_view * inverse_projection (column major), computed on the host
@@ -160,6 +167,20 @@ __global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, float const*
     }
     material = __ldg(s.tri_material + prim);
   }
+  // SDF drawables after the meshes (pt_trace.comp:342-352): a closer march hit
+  // replaces the mesh hit and its attributes.
+  for (int dsdf = 0; dsdf < s.sdf.n_drawables; ++dsdf) {
+    sdfk::sdf_hit const sh =
+        sdfk::march(s.sdf, dsdf, ro, rd, hits ? ht : __int_as_float(0x7f800000), false, &r);
+    if (sh.hits && sh.t < ht) {
+      hits = true;
+      ht = sh.t;
+      position = sh.position;
+      normal = sh.normal;
+      uv = v2{sh.u, sh.v};
+      material = sh.material;
+    }
+  }
 #pragma unroll
   for (int l = 0; l < 2; ++l) {
     float const tl = intersect_sphere(ro, rd, v3{c_lights[l].px, c_lights[l].py, c_lights[l].pz}, c_lights[l].r);
@@ -190,8 +211,11 @@ __global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, float const*
     } else if (rs::dot(dir_l, lnorm) > 0.f) {
       v3 const so = position + lnorm * 0.01f;
       hit_rec hs;
-      bool const occluded = traverse<0, true, false>(s.nodes, s.tris, f3{so.x, so.y, so.z},
+      bool occluded = traverse<0, true, false>(s.nodes, s.tris, f3{so.x, so.y, so.z},
           f3{dir_l.x, dir_l.y, dir_l.z}, 0.f, dist_l, hs, s.err, cn, ct);
+      // any_hit's SDF loop (pt_trace.comp:319-327)
+      for (int dsdf = 0; !occluded && dsdf < s.sdf.n_drawables; ++dsdf)
+        occluded = sdfk::march(s.sdf, dsdf, so, dir_l, dist_l, true, &r).hits;
       if (!occluded) {
         v3 const col{L.cx, L.cy, L.cz};
         light_strength = rs::length(col);
@@ -500,7 +524,8 @@ int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_p
   cd.eye[1] = cam->inverse_view[13];
   cd.eye[2] = cam->inverse_view[14];
   scene_dev sd{S.nodes, S.tris, S.tri_normals, S.tri_uvs, S.tri_material,
-      reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err};
+      reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err,
+      make_sdf_dev(ctx, p->sdf_marching_steps, p->sdf_marching_epsilon)};
   color_args ca{reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, R.accum, R.display, W,
       0, 0};
   size_t const n = size_t(W) * H;
@@ -624,7 +649,8 @@ int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_
   cd.eye[1] = cam->inverse_view[13];
   cd.eye[2] = cam->inverse_view[14];
   scene_dev sd{S.nodes, S.tris, S.tri_normals, S.tri_uvs, S.tri_material,
-      reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err};
+      reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err,
+      make_sdf_dev(ctx, p->sdf_marching_steps, p->sdf_marching_epsilon)};
   color_args ca{reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, accum, display, W,
       sample_index, 0};
   size_t const n = size_t(W) * H;
@@ -653,6 +679,75 @@ int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_
     if (rc) return rc;
   }
   return MYRT_OK;
+}
+
+// ---- SDF ray queries ------------------------------------------------------------
+namespace {
+// The SDF loops of nearest_hit / any_hit for one ray per thread. out: 8 floats
+// per ray (hit, t, normal xyz, u, v, material bits).
+__global__ void __launch_bounds__(128) k_trace_sdf(sdfk::sdf_dev s, float4 const* __restrict__ rays, uint32_t n,
+    int any_hit, uint32_t const* __restrict__ rng_states, float4* __restrict__ out) {
+  uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 const r0 = rays[2 * size_t(i)], r1 = rays[2 * size_t(i) + 1];
+  v3 const ro = xyz(r0), rd = xyz(r1);
+  float const maxd = r1.w;
+  rs::rng_t rng;
+  rng.state = rng_states ? rng_states[i] : 0u;
+  rng.prime = 0;
+  rng.tex = nullptr;
+  bool hit = false;
+  float t = maxd;
+  v3 nrm{0.f, 0.f, 0.f};
+  float u = 0.f, v = 0.f;
+  int mat = -1;
+  if (any_hit) {
+    for (int d = 0; !hit && d < s.n_drawables; ++d) hit = sdfk::march(s, d, ro, rd, maxd, true, &rng).hits;
+  } else {
+    for (int d = 0; d < s.n_drawables; ++d) {
+      sdfk::sdf_hit const h = sdfk::march(s, d, ro, rd, hit ? t : maxd, false, &rng);
+      if (h.hits && h.t < t) {
+        hit = true;
+        t = h.t;
+        nrm = h.normal;
+        u = h.u;
+        v = h.v;
+        mat = h.material;
+      }
+    }
+  }
+  out[2 * size_t(i)] = make_float4(hit ? 1.f : 0.f, t, nrm.x, nrm.y);
+  out[2 * size_t(i) + 1] = make_float4(nrm.z, u, v, __int_as_float(hit ? mat : -1));
+}
+}  // namespace
+
+int trace_sdf_rays(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, int steps, float eps, int any_hit,
+    uint32_t const* rng_states, float* out) {
+  if (n == 0) return MYRT_OK;
+  void* d_rays = nullptr;
+  void* d_out = nullptr;
+  void* d_rng = nullptr;
+  int rc = check_cuda(ctx, cudaMalloc(&d_rays, size_t(n) * 32), "SDF query buffers");
+  if (!rc) rc = check_cuda(ctx, cudaMalloc(&d_out, size_t(n) * 32), "SDF query buffers");
+  if (!rc && rng_states) rc = check_cuda(ctx, cudaMalloc(&d_rng, size_t(n) * 4), "SDF query buffers");
+  if (!rc)
+    rc = check_cuda(ctx, cudaMemcpyAsync(d_rays, rays, size_t(n) * 32, cudaMemcpyHostToDevice, ctx->stream), "upload");
+  if (!rc && rng_states)
+    rc = check_cuda(ctx, cudaMemcpyAsync(d_rng, rng_states, size_t(n) * 4, cudaMemcpyHostToDevice, ctx->stream),
+        "upload");
+  if (!rc) {
+    k_trace_sdf<<<(n + 127) / 128, 128, 0, ctx->stream>>>(make_sdf_dev(ctx, steps, eps),
+        static_cast<float4 const*>(d_rays), n, any_hit, static_cast<uint32_t const*>(d_rng),
+        static_cast<float4*>(d_out));
+    rc = check_cuda(ctx, cudaGetLastError(), "SDF query launch");
+  }
+  if (!rc)
+    rc = check_cuda(ctx, cudaMemcpyAsync(out, d_out, size_t(n) * 32, cudaMemcpyDeviceToHost, ctx->stream), "download");
+  if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "SDF query");
+  cudaFree(d_rays);
+  cudaFree(d_out);
+  cudaFree(d_rng);
+  return rc;
 }
 
 }  // namespace myrt_b200

@@ -41,7 +41,7 @@ GLSL_FILES = ["random.glsl", "intersect.glsl", "ggx.glsl", "color.glsl", "pbr.gl
 
 _FLOAT_LIT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][-+]?\d+)?|\d+[eE][-+]?\d+)(?![\w.])")
 _PARAM_REF = re.compile(r"\b(?:inout|out)\s+([A-Za-z_]\w*)\s+([A-Za-z_]\w*)")
-_GLOBAL_VAR = re.compile(r"^(int|bool|float|uint|random_state_t|material_state_t)(\s+\w+\s*(?:=[^;]*)?;)", re.M)
+_GLOBAL_VAR = re.compile(r"^(int|bool|float|uint|vec3|random_state_t|material_state_t)(\s+\w+\s*(?:=[^;]*)?;)", re.M)
 
 
 # GLSL evaluates function arguments left to right (GLSL 4.60, 6.1.1); C++ leaves
@@ -65,6 +65,53 @@ ORDER_FIXES = {
 }
 
 
+# SDF instruction types of src/pathtracer/sdf.hpp:399-633 whose GLSL snippets
+# compile (smooth_subtraction / smooth_intersection use `h` before declaring it
+# and compile in no language). Each snippet becomes one C++ function with the
+# signature the code generator gives it (sdf.cpp:135-149): prim
+# (in_position, inout_material, params...), op (in_distance0/1, in_material0/1,
+# inout_material, params...), mod (in_position, out_multiplier, params...).
+SDF_TYPES = ["sphere", "translate", "hard_union", "hard_subtraction", "hard_intersection", "smooth_union", "box",
+             "torus", "menger_fractal", "vertical_capsule", "mirror_axis"]
+_SDF_PARAM_CPP = {"float": "float", "int": "int", "uint": "uint", "vec3": "vec3"}
+
+
+def extract_sdf_snippets(src: str) -> str:
+    out = []
+    for name in SDF_TYPES:
+        m = re.search(r"struct %s : (prim|op|mod) \{(.*?)\n  \};" % name, src, re.S)
+        assert m, f"sdf.hpp: struct {name} not found"
+        cat, body = m.group(1), m.group(2)
+        g = re.search(r'constexpr static auto glsl = R"\((.*?)\)";', body, re.S)
+        if g:
+            glsl = g.group(1)
+            head = re.search(r"basic_type\{\s*instruction_type::category::\w+,\s*glsl\s*,\s*\{([^}]*)\}", body, re.S)
+        else:
+            head = re.search(r'basic_type\{\s*instruction_type::category::\w+,\s*(?:R"\((.*?)\)"|"((?:[^"\\]|\\.)*)")'
+                             r'\s*,\s*\{([^}]*)\}', body, re.S)
+            glsl = head.group(1) if head.group(1) is not None else head.group(2)
+        assert head, f"sdf.hpp: basic_type of {name} not found"
+        ptypes = re.findall(r"(\w+)_param::type", head.group(head.lastindex))
+        params = "".join(f", {_SDF_PARAM_CPP[t]} in_param{i}" for i, t in enumerate(ptypes))
+        glsl = glsl.replace("mix_material", "_mxm").replace("load_material", "_ldm")
+        if cat == "prim":
+            sig = f"float sdf_{name}(vec3 in_position, _MT& inout_material{params})"
+        elif cat == "op":
+            sig = (f"float sdf_{name}(float in_distance0, float in_distance1, _MT in_material0, _MT in_material1, "
+                   f"_MT& inout_material{params})")
+        else:
+            sig = f"vec3 sdf_{name}(vec3 in_position, float& out_multiplier{params})"
+        out.append(f"// sdf.hpp: struct {name} ({cat})\n{sig} {{\n{glsl}\n}}\n")
+    return glsl_to_cpp("\n".join(out), globals_thread_local=False)  # snippet bodies hold locals only
+
+
+def raymarch_to_cpp(src: str) -> str:
+    # GLSL lets a float be swizzled (`x.x`); C++ does not. raymarch.glsl:107.
+    src, n = re.subn(r"map\(p \+ 0\.0005 \* e / len, dum, true\)\.x", "map(p + 0.0005 * e / len, dum, true)", src)
+    assert n == 1, "raymarch.glsl: normal estimate changed"
+    return glsl_to_cpp(src)
+
+
 def fix_evaluation_order(name: str, src: str) -> str:
     for pat, rep, count in ORDER_FIXES.get(name, []):
         src, n = re.subn(pat, rep, src)
@@ -72,11 +119,13 @@ def fix_evaluation_order(name: str, src: str) -> str:
     return src
 
 
-def glsl_to_cpp(src: str) -> str:
+def glsl_to_cpp(src: str, globals_thread_local: bool = True) -> str:
     src = re.sub(r"\bconst\s+in\s+", "const ", src)
+    src = re.sub(r"(?<=[(,])\s*in\s+(?=[A-Za-z_]\w*\s+[A-Za-z_]\w*\s*[,)])", " ", src)  # plain `in` parameters
     src = _PARAM_REF.sub(r"\1& \2", src)
     src = _FLOAT_LIT.sub(r"\1f", src)
-    src = _GLOBAL_VAR.sub(r"thread_local \1\2", src)
+    if globals_thread_local:
+        src = _GLOBAL_VAR.sub(r"thread_local \1\2", src)
     return src
 
 
@@ -111,6 +160,9 @@ def write_sources() -> None:
     (OUT / "glsl/material_new.glsl").write_text(material_codegen((REF_ROOT / "src/pt/material_new.glsl").read_text()))
     trace = (REF_ROOT / "src/pt/pt_trace.comp").read_text()
     (OUT / "glsl/pt_trace_visitor.glsl").write_text(extract_trace_visitor(trace))
+    (OUT / "glsl/raymarch.glsl").write_text(raymarch_to_cpp((REF_ROOT / "src/pt/raymarch.glsl").read_text()))
+    (OUT / "glsl/sdf_snippets.inc").write_text(
+        extract_sdf_snippets((REF_ROOT / "src/pathtracer/sdf.hpp").read_text()))
 
 
 def compile_ref() -> Path:

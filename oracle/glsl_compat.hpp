@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <type_traits>
 
 namespace glsl {
 
@@ -29,9 +30,12 @@ template <int I0, int I1, int I2, int N> struct swz3 {
   float d[N];
   operator vec3() const;
 };
+// Readable and writable two-component swizzle (p.xy = p.yx in the Menger fold).
 template <int I0, int I1, int N> struct swz2 {
   float d[N];
   operator vec2() const;
+  swz2& operator=(vec2 const& v);
+  template <int J0, int J1> swz2& operator=(swz2<J0, J1, N> const& o);
 };
 
 struct vec2 {
@@ -41,7 +45,7 @@ struct vec2 {
     float d[2];
   };
   vec2() : x(0), y(0) {}
-  template <typename S> explicit vec2(S s) : x(float(s)), y(float(s)) {}
+  template <typename S> requires std::is_arithmetic_v<S> explicit vec2(S s) : x(float(s)), y(float(s)) {}
   template <typename A, typename B> vec2(A a, B b) : x(float(a)), y(float(b)) {}
   float& operator[](int i) { return d[i]; }
   float operator[](int i) const { return d[i]; }
@@ -53,10 +57,16 @@ struct vec3 {
     struct { float r, g, b; };
     swz3<0, 1, 2, 3> xyz;
     swz3<0, 1, 2, 3> rgb;
+    swz2<0, 1, 3> xy;
+    swz2<1, 0, 3> yx;
+    swz2<0, 2, 3> xz;
+    swz2<2, 0, 3> zx;
+    swz2<1, 2, 3> yz;
+    swz2<2, 1, 3> zy;
     float d[3];
   };
   vec3() : x(0), y(0), z(0) {}
-  template <typename S> explicit vec3(S s) : x(float(s)), y(float(s)), z(float(s)) {}
+  template <typename S> requires std::is_arithmetic_v<S> explicit vec3(S s) : x(float(s)), y(float(s)), z(float(s)) {}
   template <typename A, typename B, typename C> vec3(A a, B b, C c) : x(float(a)), y(float(b)), z(float(c)) {}
   vec3(vec3 const& o) : x(o.x), y(o.y), z(o.z) {}
   vec3& operator=(vec3 const& o) { x = o.x; y = o.y; z = o.z; return *this; }
@@ -78,7 +88,7 @@ struct vec4 {
     float d[4];
   };
   vec4() : x(0), y(0), z(0), w(0) {}
-  template <typename S> explicit vec4(S s) : x(float(s)), y(float(s)), z(float(s)), w(float(s)) {}
+  template <typename S> requires std::is_arithmetic_v<S> explicit vec4(S s) : x(float(s)), y(float(s)), z(float(s)), w(float(s)) {}
   template <typename A, typename B, typename C, typename D>
   vec4(A a, B b, C c, D e) : x(float(a)), y(float(b)), z(float(c)), w(float(e)) {}
   template <typename S> vec4(vec3 const& v, S s) : x(v.x), y(v.y), z(v.z), w(float(s)) {}
@@ -93,6 +103,18 @@ template <int I0, int I1, int I2, int N> swz3<I0, I1, I2, N>::operator vec3() co
   return vec3(d[I0], d[I1], d[I2]);
 }
 template <int I0, int I1, int N> swz2<I0, I1, N>::operator vec2() const { return vec2(d[I0], d[I1]); }
+template <int I0, int I1, int N> swz2<I0, I1, N>& swz2<I0, I1, N>::operator=(vec2 const& v) {
+  float const a = v.x, b = v.y;
+  d[I0] = a;
+  d[I1] = b;
+  return *this;
+}
+template <int I0, int I1, int N>
+template <int J0, int J1>
+swz2<I0, I1, N>& swz2<I0, I1, N>::operator=(swz2<J0, J1, N> const& o) {
+  vec2 const v = o.operator vec2();
+  return *this = v;
+}
 
 struct ivec2 {
   int x = 0, y = 0;
@@ -119,6 +141,7 @@ inline vec2 operator*(vec2 a, float s) { return vec2(a.x * s, a.y * s); }
 inline vec2 operator*(float s, vec2 a) { return vec2(s * a.x, s * a.y); }
 inline vec2 operator*(vec2 a, vec2 b) { return vec2(a.x * b.x, a.y * b.y); }
 inline vec2 operator/(vec2 a, vec2 b) { return vec2(a.x / b.x, a.y / b.y); }
+inline vec2 operator/(vec2 a, float s) { return vec2(a.x / s, a.y / s); }
 
 // ---- vec3 ----
 inline vec3 operator+(vec3 const& a, vec3 const& b) { return vec3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -175,6 +198,10 @@ inline bvec3 isinf(vec3 const& v) { return {isinf(v.x), isinf(v.y), isinf(v.z)};
 inline bvec4 isnan(vec4 const& v) { return {isnan(v.x), isnan(v.y), isnan(v.z), isnan(v.w)}; }
 inline bvec4 isinf(vec4 const& v) { return {isinf(v.x), isinf(v.y), isinf(v.z), isinf(v.w)}; }
 
+inline vec3 max(vec3 const& a, float s) { return vec3(max(a.x, s), max(a.y, s), max(a.z, s)); }
+inline vec3 min(vec3 const& a, float s) { return vec3(min(a.x, s), min(a.y, s), min(a.z, s)); }
+inline float length(vec2 const& v) { return sqrt(v.x * v.x + v.y * v.y); }
+inline vec3& operator*=(vec3& a, double s) { return a *= float(s); }
 inline float dot(vec3 const& a, vec3 const& b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
 inline vec3 cross(vec3 const& a, vec3 const& b) {
   return vec3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
@@ -200,6 +227,24 @@ struct mat3 {
 inline vec3 operator*(mat3 const& m, vec3 const& v) {
   return vec3((m.c[0].x * v.x + m.c[1].x * v.y) + m.c[2].x * v.z, (m.c[0].y * v.x + m.c[1].y * v.y) + m.c[2].y * v.z,
       (m.c[0].z * v.x + m.c[1].z * v.y) + m.c[2].z * v.z);
+}
+
+struct mat4 {
+  vec4 c[4];
+  vec4& operator[](int i) { return c[i]; }
+  vec4 const& operator[](int i) const { return c[i]; }
+};
+inline vec4 operator*(mat4 const& m, vec4 const& v) {
+  vec4 r;
+  for (int k = 0; k < 4; ++k)
+    r[k] = ((m.c[0][k] * v.x + m.c[1][k] * v.y) + m.c[2][k] * v.z) + m.c[3][k] * v.w;
+  return r;
+}
+inline mat4 transpose(mat4 const& m) {
+  mat4 t;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) t.c[i][j] = m.c[j][i];
+  return t;
 }
 
 // ---- packing ----

@@ -326,6 +326,187 @@ inline v3 mat_bounce(material_ctx& mc, rng_t& rng, v2 rnd, v3 tv, v3 n) {
   return pbr_resample(rng, mc.ps, rnd, mc.mat, tv, mc.incoming ? n : -n, mc.ior1, mc.ior2);
 }
 
+// ---- SDF drawables (raymarch.glsl, sdf.hpp:399-633, sdf.cpp:122-407) -------------
+// Flat post-order programs: modifier instructions move the position of the next
+// primitive (innermost first); primitives push (distance, material); operators
+// pop two and push one. Opcodes as include/myrt_cuda.h.
+struct sdf_scene {
+  std::int32_t const* instrs = nullptr;    // (op, param offset) pairs
+  std::int32_t const* programs = nullptr;  // (first, count) pairs
+  float const* params = nullptr;
+  float const* drawables = nullptr;        // 36 floats: mat4, inverse mat4, sdf_index bits, pad
+  int n_drawables = 0;
+  int steps = 0;
+  float eps = 0.f;
+};
+inline v3 abs3(v3 a) { return {std::fabs(a.x), std::fabs(a.y), std::fabs(a.z)}; }
+inline v3 max3s(v3 a, float s) { return {gmax(a.x, s), gmax(a.y, s), gmax(a.z, s)}; }
+inline float len2(float x, float y) { return std::sqrt(x * x + y * y); }
+struct sdf_ctx {
+  sdf_scene const* s;
+  rng_t* rng;
+  bool load = false;  // g_do_load_materials
+  int prog = 0;       // sdf_index_current
+};
+inline int sdf_ldm(sdf_ctx const& c, int index) { return c.load ? index : -1; }
+inline int sdf_mxm(sdf_ctx& c, int a, int b, float t) {
+  if (!c.load) return -1;
+  return random_next(*c.rng) < t ? b : a;
+}
+// sdf.hpp: menger_fractal
+inline float sd_menger(v3 p) {
+  for (int n = 0; n < 4; n++) {
+    p = abs3(p);
+    if (p.x < p.y) std::swap(p.x, p.y);
+    if (p.x < p.z) std::swap(p.x, p.z);
+    if (p.y < p.z) std::swap(p.y, p.z);
+    p.z -= 1.f / 3.f;
+    p.z = -std::fabs(p.z);
+    p.z += 1.f / 3.f;
+    p = p * 3.f;
+    p.x -= 2.f;
+    p.y -= 2.f;
+  }
+  v3 const d = abs3(p) - v3{1.f, 1.f, 1.f};
+  float dis = gmin(gmax(d.x, gmax(d.y, d.z)), 0.f) + length(max3s(d, 0.f));
+  dis *= std::pow(3.f, float(-4));
+  return dis;
+}
+inline float sdf_map(sdf_ctx& c, v3 p, int& mat) {
+  sdf_scene const& s = *c.s;
+  auto G = [&](int i) { return s.params[i]; };
+  std::int32_t const first = s.programs[2 * c.prog], count = s.programs[2 * c.prog + 1];
+  float dist[64];
+  int mats[64];
+  int sp = 0;
+  v3 pos = p;
+  float mul = 1.f;
+  for (int k = 0; k < count; ++k) {
+    int const op = s.instrs[2 * (first + k)], o = s.instrs[2 * (first + k) + 1];
+    int m = mat;
+    float d = 0.f;
+    switch (op) {
+      case 32: pos = pos - v3{G(o), G(o + 1), G(o + 2)}; continue;
+      case 33: {
+        int const ax = int(G(o));
+        float* q = &pos.x;
+        q[ax] = std::fabs(q[ax]);
+        continue;
+      }
+      case 1: m = sdf_ldm(c, int(G(o + 1))); d = length(pos) - G(o); break;
+      case 2: {
+        m = sdf_ldm(c, int(G(o + 3)));
+        v3 const q = abs3(pos) - v3{G(o), G(o + 1), G(o + 2)};
+        d = length(max3s(q, 0.f)) + gmin(gmax(q.x, gmax(q.y, q.z)), 0.f);
+        break;
+      }
+      case 3: m = sdf_ldm(c, int(G(o + 2))); d = len2(len2(pos.x, pos.z) - G(o), pos.y) - G(o + 1); break;
+      case 4: {
+        m = sdf_ldm(c, int(G(o + 2)));
+        v3 q = pos;
+        q.y -= gclamp(q.y, 0.f, G(o));
+        d = length(q) - G(o + 1);
+        break;
+      }
+      case 5: m = sdf_ldm(c, int(G(o))); d = sd_menger(pos); break;
+      default: {
+        float const d1 = dist[sp - 1], d0 = dist[sp - 2];
+        int const m1 = mats[sp - 1], m0 = mats[sp - 2];
+        sp -= 2;
+        if (op == 16 || op == 17 || op == 18) {
+          float const r = op == 16 ? gmin(d0, d1) : (op == 17 ? gmax(-d0, d1) : gmax(d0, d1));
+          m = sdf_mxm(c, m0, m1, float(r == d1));
+          d = r;
+        } else {  // 19: smooth union
+          float const k = G(o);
+          float const h = gclamp(0.5f + 0.5f * (d1 - d0) / k, 0.f, 1.f);
+          m = sdf_mxm(c, m0, m1, 1.f - h);
+          d = mixf(d1, d0, h) - k * h * (1.f - h);
+        }
+        break;
+      }
+    }
+    dist[sp] = d;
+    mats[sp] = m;
+    ++sp;
+    pos = p;
+  }
+  mat = mats[sp - 1];
+  return mul * dist[sp - 1];
+}
+inline v4 mat4_vec(float const* m, v4 v) {
+  float const in[4] = {v.x, v.y, v.z, v.w};
+  float o[4];
+  for (int r = 0; r < 4; ++r)
+    o[r] = ((m[0 * 4 + r] * in[0] + m[1 * 4 + r] * in[1]) + m[2 * 4 + r] * in[2]) + m[3 * 4 + r] * in[3];
+  return {o[0], o[1], o[2], o[3]};
+}
+struct sdf_hit {
+  bool hits = false;
+  float t = 0.f;
+  v3 position{0, 0, 0}, normal{0, 0, 0};
+  v2 uv{0, 0};
+  int material = -1;
+};
+// raymarch.glsl:116-171 for drawable `cur`
+inline sdf_hit march_sdf(sdf_scene const& s, rng_t& rng, int cur, v3 oro, v3 ord, float tmax, bool hits_only) {
+  sdf_ctx c{&s, &rng, false, 0};
+  float const* dr = s.drawables + 36 * cur;
+  float const* inv = dr + 16;
+  std::int32_t idx;
+  std::memcpy(&idx, dr + 32, 4);
+  c.prog = idx;
+  v4 const ro4 = mat4_vec(inv, v4{oro.x, oro.y, oro.z, 1.f});
+  v4 const rd4 = mat4_vec(inv, v4{ord.x, ord.y, ord.z, 0.f});
+  v3 const ro{ro4.x, ro4.y, ro4.z}, rd{rd4.x, rd4.y, rd4.z};
+  float const len = length(rd);
+  float res = -1.f;
+  float t = 10.f * s.eps;
+  int si = 0;
+  for (int i = 0; i < s.steps && t / len < tmax; i++) {
+    int mdum = -1;
+    float const m = sdf_map(c, ro + rd * t / len, mdum);
+    if (si == 0) si = int(signf(m));
+    float const h = m;
+    if (std::fabs(h) < s.eps) {
+      res = t;
+      break;
+    }
+    t += float(si) * h;
+  }
+  sdf_hit hit;
+  if (res < 0.f) return hit;
+  hit.hits = true;
+  if (hits_only) return hit;
+  hit.t = res / len;
+  hit.position = oro + res / len * ord;
+  v3 const poas = ro + res * rd;
+  // nor(): tetrahedral normal, then the material with draws enabled
+  v3 n{0.f, 0.f, 0.f};
+  for (int i = 0; i < 4; i++) {
+    v3 const e = 0.5773f * (2.f * v3{float(((i + 3) >> 1) & 1), float((i >> 1) & 1), float(i & 1)} - v3{1.f, 1.f, 1.f});
+    int mdum = -1;
+    n = n + e * sdf_map(c, poas + 0.0005f * e / len, mdum) * len;
+  }
+  v3 const gn = normalize(n);
+  c.load = true;
+  int mat = -1;
+  sdf_map(c, poas, mat);
+  // normalize((transpose(inverse) * vec4(nor, 0)).xyz): row r of the transpose = column r of inverse
+  float const* m = inv;
+  v3 const tn{((m[0] * gn.x + m[1] * gn.y) + m[2] * gn.z) + m[3] * 0.f,
+      ((m[4] * gn.x + m[5] * gn.y) + m[6] * gn.z) + m[7] * 0.f,
+      ((m[8] * gn.x + m[9] * gn.y) + m[10] * gn.z) + m[11] * 0.f};
+  hit.normal = normalize(tn);
+  // sample_texture(poas, normal, 0.5): triplanar weights pow(abs(n), k)
+  float const wx = std::pow(std::fabs(hit.normal.x), 0.5f), wy = std::pow(std::fabs(hit.normal.y), 0.5f),
+              wz = std::pow(std::fabs(hit.normal.z), 0.5f);
+  float const sw = (wx + wy) + wz;
+  hit.uv = {((poas.y * wx + poas.z * wy) + poas.x * wz) / sw, ((poas.z * wx + poas.x * wy) + poas.y * wz) / sw};
+  hit.material = mat;
+  return hit;
+}
+
 // ---- pass state (pt_*.comp structs) -------------------------------------------
 struct gen_t {  // generate_output_t, 80 bytes
   v3 origin;
@@ -439,6 +620,7 @@ struct frame_ctx {
   std::vector<v4>* display; // output_image
   std::uint32_t sample_index;
   int nthreads;
+  sdf_scene const* sdf;     // n_drawables == 0: no SDF drawables
 };
 
 // pt_generate.comp:50-84
@@ -515,7 +697,7 @@ void pass_trace(frame_ctx& f, pass_rng const& pr, std::vector<gen_t> const& gen,
       float const* P = sc.tris9 + 9 * tri;
       v3 const p0{P[0], P[1], P[2]}, p1{P[3], P[4], P[5]}, p2{P[6], P[7], P[8]};
       float const w = (1.f - bx) - by;
-      v3 const position = (bx * p1 + by * p2) + w * p0;
+      v3 position = (bx * p1 + by * p2) + w * p0;
       v3 normal;
       if (sc.normals9) {
         float const* N = sc.normals9 + 9 * tri;
@@ -528,6 +710,20 @@ void pass_trace(frame_ctx& f, pass_rng const& pr, std::vector<gen_t> const& gen,
       if (sc.uvs6) {
         float const* U = sc.uvs6 + 6 * tri;
         uv = {(bx * U[2] + by * U[4]) + w * U[0], (bx * U[3] + by * U[5]) + w * U[1]};
+      }
+      int material = sc.tri_material[tri];
+      // SDF drawables after the meshes (pt_trace.comp:342-352)
+      for (int d = 0; f.sdf && d < f.sdf->n_drawables; ++d) {
+        sdf_hit const sh = march_sdf(*f.sdf, r, d, base.origin, base.direction,
+            hits ? ht : std::numeric_limits<float>::infinity(), false);
+        if (sh.hits && sh.t < ht) {
+          hits = true;
+          ht = sh.t;
+          position = sh.position;
+          normal = sh.normal;
+          uv = sh.uv;
+          material = sh.material;
+        }
       }
       for (int l = 0; l < 2; ++l) {
         float const t_light = intersect_sphere(base.origin, base.direction, kLights[l].position, kLights[l].radius);
@@ -545,7 +741,7 @@ void pass_trace(frame_ctx& f, pass_rng const& pr, std::vector<gen_t> const& gen,
         res.point = position;
         res.normal = normal;
         res.uv = uv;
-        res.material_index = sc.tri_material[tri];
+        res.material_index = material;
         if (inf3(res.normal) || nan3(res.normal)) res.intersects = 0;
         v3 const path = p_on_light - position;
         v3 const dir_l = normalize(path);
@@ -582,6 +778,15 @@ void pass_trace(frame_ctx& f, pass_rng const& pr, std::vector<gen_t> const& gen,
       su.data(), sv.data(), f.nthreads);
   for (std::size_t id = 0; id < n; ++id) {
     if (!wants_shadow[id] || sp[id] >= 0) continue;
+    // any_hit's SDF loop (pt_trace.comp:319-327); hits-only marches draw no randoms
+    bool sdf_occluded = false;
+    if (f.sdf) {
+      float const* q = &shadow[8 * id];
+      rng_t unused;
+      for (int d = 0; !sdf_occluded && d < f.sdf->n_drawables; ++d)
+        sdf_occluded = march_sdf(*f.sdf, unused, d, {q[0], q[1], q[2]}, {q[4], q[5], q[6]}, q[7], true).hits;
+    }
+    if (sdf_occluded) continue;
     trace_t& res = out[id];
     v3 const col = kLights[light_index[id]].color;
     float const strength = length(col);
@@ -729,7 +934,17 @@ void orc_render_reference(std::size_t n_tris, float const* tris9, float const* n
     std::int32_t const* tri_material, std::int32_t const* mat_refs, std::size_t n_mats, float const* mat_data,
     void const* nodes, std::uint32_t const* bvh_idx, int W, int H, int bounces, int frames,
     std::uint32_t sample_index0, float const* inv_view, float const* inv_proj, std::int32_t const* seeds,
-    float const* tex, float* accum, float* display, int nthreads) {
+    float const* tex, float* accum, float* display, std::int32_t const* sdf_instrs, std::int32_t const* sdf_programs,
+    float const* sdf_params, float const* sdf_drawables, int n_sdf_drawables, int sdf_steps, float sdf_eps,
+    int nthreads) {
+  sdf_scene sdf;
+  sdf.instrs = sdf_instrs;
+  sdf.programs = sdf_programs;
+  sdf.params = sdf_params;
+  sdf.drawables = sdf_drawables;
+  sdf.n_drawables = n_sdf_drawables;
+  sdf.steps = sdf_steps;
+  sdf.eps = sdf_eps;
   scene_t sc{n_tris, tris9, normals9, uvs6, tri_material, mat_refs, n_mats, mat_data, nodes, bvh_idx, {}, {}};
   sc.seq.resize(3 * n_tris);
   for (std::size_t i = 0; i < sc.seq.size(); ++i) sc.seq[i] = std::uint32_t(i);
@@ -748,7 +963,7 @@ void orc_render_reference(std::size_t n_tris, float const* tris9, float const* n
       r.tex.assign(t, t + 1024);
       return r;
     };
-    frame_ctx f{&sc, W, H, inv_view, inv_proj, &acc, &disp, sample_index0 + std::uint32_t(fr), nthreads};
+    frame_ctx f{&sc, W, H, inv_view, inv_proj, &acc, &disp, sample_index0 + std::uint32_t(fr), nthreads, &sdf};
     std::vector<gen_t> gen;
     std::vector<trace_t> tr;
     pass_generate(f, pr(0), gen);
@@ -766,6 +981,70 @@ void orc_render_reference(std::size_t n_tris, float const* tris9, float const* n
 }
 
 // Known-answer access to the restated shading functions (for the pins).
+// map() of program `prog` at n points; with load_materials the material draws
+// consume the random stream started from rng_states[i] (prime index 0).
+void orc_sdf_map(std::int32_t const* instrs, std::int32_t const* programs, float const* params, int prog,
+    float const* pts, std::size_t n, int load_materials, std::uint32_t const* rng_states, float* out_d, int* out_mat) {
+  sdf_scene s;
+  s.instrs = instrs;
+  s.programs = programs;
+  s.params = params;
+  for (std::size_t i = 0; i < n; ++i) {
+    rng_t r;
+    r.state = rng_states ? rng_states[i] : 0u;
+    r.prime = 0;
+    sdf_ctx c{&s, &r, load_materials != 0, prog};
+    int m = -1;
+    out_d[i] = sdf_map(c, {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]}, m);
+    out_mat[i] = m;
+  }
+}
+
+// SDF part of nearest_hit (pt_trace.comp:342-352) / any_hit (:321-326) over all
+// drawables; same arguments and outputs as ref_sdf_trace in oracle/_ref.
+void orc_sdf_trace(std::int32_t const* instrs, std::int32_t const* programs, float const* params,
+    float const* drawables, int n_drawables, float const* rays, std::size_t n, int steps, float eps, int any_hit,
+    std::uint32_t const* rng_states, int* out_hit, float* out_t, float* out_n, float* out_uv, int* out_mat,
+    int nthreads) {
+  sdf_scene s;
+  s.instrs = instrs;
+  s.programs = programs;
+  s.params = params;
+  s.drawables = drawables;
+  s.n_drawables = n_drawables;
+  s.steps = steps;
+  s.eps = eps;
+  par(n, nthreads, [&](std::size_t b, std::size_t e) {
+    for (std::size_t i = b; i < e; ++i) {
+      float const* q = rays + 8 * i;
+      v3 const ro{q[0], q[1], q[2]}, rd{q[4], q[5], q[6]};
+      float const maxd = q[7];
+      rng_t r;
+      r.state = rng_states ? rng_states[i] : 0u;
+      r.prime = 0;
+      sdf_hit hit;
+      hit.t = maxd;
+      if (any_hit) {
+        for (int d = 0; d < n_drawables; ++d)
+          if (march_sdf(s, r, d, ro, rd, maxd, true).hits) {
+            hit.hits = true;
+            break;
+          }
+      } else {
+        for (int d = 0; d < n_drawables; ++d) {
+          sdf_hit const h = march_sdf(s, r, d, ro, rd, hit.hits ? hit.t : maxd, false);
+          if (h.hits && h.t < hit.t) hit = h;
+        }
+      }
+      out_hit[i] = hit.hits ? 1 : 0;
+      out_t[i] = hit.hits ? hit.t : maxd;
+      out_n[3 * i] = hit.normal.x, out_n[3 * i + 1] = hit.normal.y, out_n[3 * i + 2] = hit.normal.z;
+      out_uv[2 * i] = hit.uv.x, out_uv[2 * i + 1] = hit.uv.y;
+      out_mat[i] = hit.hits ? hit.material : -1;
+    }
+  });
+}
+
 void orc_random_stream(float const* tex, int tex_size, int px, int py, int seed, int n, float* out,
     std::uint32_t* state_after_init) {
   rng_t r;

@@ -42,7 +42,7 @@ def oracle() -> C.CDLL:
             "orc_brute_closest": (None, [P, SZ, P, SZ, I, P, P, P, P, I]),
             "orc_host_rng": (None, [C.c_uint32, I, I, P, P]),
             "orc_render_reference": (None, [SZ, P, P, P, P, P, SZ, P, P, P, I, I, I, I, C.c_uint32, P, P, P, P, P,
-                                            P, I]),
+                                            P, P, P, P, P, I, I, C.c_float, I]),
             "orc_random_stream": (None, [P, I, I, I, I, I, P, P]),
             "orc_wang_hash": (C.c_uint32, [C.c_uint32]),
             "orc_transform_local_to_world": (None, [P, P, P]),
@@ -50,6 +50,8 @@ def oracle() -> C.CDLL:
             "orc_intersect_sphere": (C.c_float, [P, P, P, C.c_float]),
             "orc_material_bounce_eval": (None, [P, P, P, P, P, P, P, P, P]),
             "orc_material_eval": (None, [P, I, C.c_float, P, P, P, P, P]),
+            "orc_sdf_map": (None, [P, P, P, I, P, SZ, I, P, P, P]),
+            "orc_sdf_trace": (None, [P, P, P, P, I, P, SZ, I, C.c_float, I, P, P, P, P, P, P, I]),
         }
         for k, (r, a) in sig.items():
             f = getattr(h, k)
@@ -84,6 +86,8 @@ def ref() -> C.CDLL:
             "ref_glsl_pack_unorm4x8": (C.c_uint32, [P]),
             "ref_glsl_material_bounce_eval": (None, [P, P, P, P, P, P, P, P, P]),
             "ref_glsl_material_eval": (None, [P, I, C.c_float, P, P, P, P, P]),
+            "ref_sdf_map": (None, [P, P, P, I, P, SZ, I, P, P, P]),
+            "ref_sdf_trace": (None, [P, P, P, P, I, P, SZ, I, C.c_float, I, P, P, P, P, P, P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(h, k)
@@ -290,8 +294,56 @@ def render_reference(scene: dict, width: int, height: int, bounces: int, frames:
     ip = np.ascontiguousarray(inv_proj, np.float32).ravel()
     nrm_p = nrm.ctypes.data if nrm is not None else None
     uv_p = uvs.ctypes.data if uvs is not None else None
+    sdf = scene.get("sdf")  # optional: dict(lib=SdfLibrary, drawables=[N,36], steps=, eps=)
+    if sdf is not None:
+        s_ins, s_prs, s_par = _sdf_arrays(sdf["lib"])
+        s_dr = np.ascontiguousarray(sdf["drawables"], np.float32).reshape(-1, 36)
+        sdf_args = [s_ins.ctypes.data, s_prs.ctypes.data, s_par.ctypes.data, s_dr.ctypes.data, s_dr.shape[0],
+                    int(sdf["steps"]), float(sdf["eps"])]
+    else:
+        sdf_args = [None, None, None, None, 0, 0, 0.0]
     L.orc_render_reference(tris9.shape[0], tris9.ctypes.data, nrm_p, uv_p, mat.ctypes.data, refs.ctypes.data,
                            refs.shape[0], mdata.ctypes.data, nodes.ctypes.data, bi.ctypes.data, width, height, bounces,
                            frames, sample_index0, iv.ctypes.data, ip.ctypes.data, seeds.ctypes.data, tex.ctypes.data,
-                           accum.ctypes.data, display.ctypes.data, nthreads())
+                           accum.ctypes.data, display.ctypes.data, *sdf_args, nthreads())
     return accum, display
+
+
+# ---- SDF ----------------------------------------------------------------------
+def _sdf_arrays(lib):
+    return (np.ascontiguousarray(lib.instrs, np.int32), np.ascontiguousarray(lib.programs, np.int32),
+            np.ascontiguousarray(lib.params, np.float32))
+
+
+def sdf_map(lib, prog: int, pts, load_materials=False, rng_states=None, use_ref=False):
+    ins, prs, par = _sdf_arrays(lib)
+    p = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+    n = p.shape[0]
+    d = np.zeros(n, np.float32)
+    m = np.zeros(n, np.int32)
+    rs = None if rng_states is None else np.ascontiguousarray(rng_states, np.uint32)
+    fn = ref().ref_sdf_map if use_ref else oracle().orc_sdf_map
+    fn(ins.ctypes.data, prs.ctypes.data, par.ctypes.data, prog, p.ctypes.data, n, int(load_materials),
+       None if rs is None else rs.ctypes.data, d.ctypes.data, m.ctypes.data)
+    return d, m
+
+
+def sdf_trace(lib, drawables, rays, steps, eps, any_hit=False, rng_states=None, use_ref=False):
+    ins, prs, par = _sdf_arrays(lib)
+    dr = np.ascontiguousarray(drawables, np.float32).reshape(-1, 36)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = r.shape[0]
+    hit = np.zeros(n, np.int32)
+    t = np.zeros(n, np.float32)
+    nn = np.zeros((n, 3), np.float32)
+    uv = np.zeros((n, 2), np.float32)
+    mat = np.zeros(n, np.int32)
+    rs = None if rng_states is None else np.ascontiguousarray(rng_states, np.uint32)
+    args = [ins.ctypes.data, prs.ctypes.data, par.ctypes.data, dr.ctypes.data, dr.shape[0], r.ctypes.data, n, steps,
+            float(eps), int(any_hit), None if rs is None else rs.ctypes.data, hit.ctypes.data, t.ctypes.data,
+            nn.ctypes.data, uv.ctypes.data, mat.ctypes.data]
+    if use_ref:
+        ref().ref_sdf_trace(*args)
+    else:
+        oracle().orc_sdf_trace(*args, nthreads())
+    return dict(hit=hit, t=t, normal=nn, uv=uv, material=mat)

@@ -87,6 +87,98 @@ vec4 const* points = nullptr;
 #define MYRT_BVH_VISIT_PRIMITIVE visit_triangle
 #include "bvh.impl.glsl"
 #include "pt_trace_visitor.glsl"
+
+// ---- SDF: raymarch.glsl and the instruction snippets of sdf.hpp ---------------
+// Records of pt_trace.comp:49-66.
+struct drawable_sdf_t {
+  mat4 transformation;
+  mat4 inverse_transformation;
+  int sdf_index;
+  int pad[3];
+};
+struct hit_t {
+  vec3 position;
+  float t;
+  vec3 normal;
+  vec2 uv;
+  bool hits;
+  int material_index;
+  int hits_light;
+};
+drawable_sdf_t const* sdf_drawables = nullptr;
+float const* sdf_buffer = nullptr;
+int sdf_marching_steps = 0;
+#define MYRT_INJECT_SDF_MAP_CODE_HERE float map(vec3 p, _MT& _mt);
+#include "raymarch.glsl"
+#include "sdf_snippets.inc"
+
+// The map() the reference's code generator would emit for a tree
+// (sdf.cpp:122-345, map dispatch sdf.hpp:202 / sdf.cpp:400-407), written as an
+// interpreter over this project's flat post-order program: modifier
+// instructions transform the position of the next primitive (innermost
+// first), primitives push (distance, material), operators pop two and push one;
+// every node starts from the caller's material (`_MT _mt<node> = _mt`), the
+// result is the last node's, scaled by the product of the modifiers'
+// multipliers. Parameters are read from sdf_buffer exactly as the generated
+// loaders do (float: the block, int: int(block), vec3: three blocks).
+struct sdf_instr_ref {
+  int op;
+  int param;
+};
+struct sdf_program_ref {
+  int first;
+  int count;
+};
+sdf_instr_ref const* sdf_instrs = nullptr;
+sdf_program_ref const* sdf_programs = nullptr;
+
+float map(vec3 p, _MT& _mt) {
+  sdf_program_ref const pr = sdf_programs[sdf_index_current];
+  float dist[64];
+  _MT mats[64];
+  int sp = 0;
+  vec3 pos = p;
+  float mul = 1.f;
+  for (int k = 0; k < pr.count; ++k) {
+    sdf_instr_ref const in = sdf_instrs[pr.first + k];
+    int const o = in.param;
+    _MT m = _mt;
+    switch (in.op) {
+      case 32: {
+        float jm = 1.f;
+        pos = sdf_translate(pos, jm, vec3(_G(o), _G(o + 1), _G(o + 2)));
+        mul = mul * jm;
+        continue;
+      }
+      case 33: {
+        float jm = 1.f;
+        pos = sdf_mirror_axis(pos, jm, int(_G(o)));
+        mul = mul * jm;
+        continue;
+      }
+      case 1: dist[sp] = sdf_sphere(pos, m, _G(o), int(_G(o + 1))); break;
+      case 2: dist[sp] = sdf_box(pos, m, vec3(_G(o), _G(o + 1), _G(o + 2)), int(_G(o + 3))); break;
+      case 3: dist[sp] = sdf_torus(pos, m, _G(o), _G(o + 1), int(_G(o + 2))); break;
+      case 4: dist[sp] = sdf_vertical_capsule(pos, m, _G(o), _G(o + 1), int(_G(o + 2))); break;
+      case 5: dist[sp] = sdf_menger_fractal(pos, m, int(_G(o))); break;
+      default: {
+        float const b = dist[sp - 1], a = dist[sp - 2];
+        _MT const mb = mats[sp - 1], ma = mats[sp - 2];
+        sp -= 2;
+        if (in.op == 16) dist[sp] = sdf_hard_union(a, b, ma, mb, m);
+        else if (in.op == 17) dist[sp] = sdf_hard_subtraction(a, b, ma, mb, m);
+        else if (in.op == 18) dist[sp] = sdf_hard_intersection(a, b, ma, mb, m);
+        else dist[sp] = sdf_smooth_union(a, b, ma, mb, m, _G(o));
+        break;
+      }
+    }
+    mats[sp] = m;
+    ++sp;
+    pos = p;
+  }
+  _mt = mats[sp - 1];
+  return mul * dist[sp - 1];
+}
 }  // namespace glsl
 
 using namespace glsl;
@@ -230,6 +322,79 @@ void ref_glsl_traverse(void const* nodes, std::uint32_t const* node_indices, std
     if (b < e) pool.emplace_back(work, b, e);
   }
   for (auto& th : pool) th.join();
+}
+
+// SDF program tables: instrs (op, param) pairs, programs (first, count) pairs,
+// params the sdf_data floats, drawables 36 floats each (two column-major
+// mat4, then sdf_index as an int bit pattern and 3 pad words).
+static void bind_sdf(int const* instrs, int const* programs, float const* params, float const* drawables) {
+  sdf_instrs = reinterpret_cast<sdf_instr_ref const*>(instrs);
+  sdf_programs = reinterpret_cast<sdf_program_ref const*>(programs);
+  sdf_buffer = params;
+  sdf_drawables = reinterpret_cast<drawable_sdf_t const*>(drawables);
+}
+
+// map() of program `prog` at n points (xyz each); with load_materials the
+// material draws consume the random stream started from rng_states[i].
+void ref_sdf_map(int const* instrs, int const* programs, float const* params, int prog, float const* pts, size_t n,
+    int load_materials, std::uint32_t const* rng_states, float* out_d, int* out_mat) {
+  static_assert(sizeof(drawable_sdf_t) == 144, "drawable_sdf_t layout");
+  bind_sdf(instrs, programs, params, nullptr);
+  for (size_t i = 0; i < n; ++i) {
+    sdf_index_current = prog;
+    g_do_load_materials = load_materials != 0;
+    random_state.rng_state = rng_states ? rng_states[i] : 0u;
+    random_state.current_prime = 0;
+    _MT m;
+    m.index = -1;
+    out_d[i] = map(vec3(pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]), m);
+    out_mat[i] = m.index;
+  }
+}
+
+// The SDF part of nearest_hit (pt_trace.comp:342-352) or of any_hit (:321-326)
+// over all drawables, for n rays (8 floats: o, tmin, d, tmax; tmax is the
+// max_distance). Each ray's random stream starts at rng_states[i] (it feeds
+// the material choice of smooth/hard operators). Outputs: hits, t, normal
+// (3), uv (2), material.
+void ref_sdf_trace(int const* instrs, int const* programs, float const* params, float const* drawables,
+    int n_drawables, float const* rays, size_t n, int steps, float eps, int any_hit,
+    std::uint32_t const* rng_states, int* out_hit, float* out_t, float* out_n, float* out_uv, int* out_mat) {
+  bind_sdf(instrs, programs, params, drawables);
+  sdf_marching_steps = steps;
+  for (size_t i = 0; i < n; ++i) {
+    float const* q = rays + 8 * i;
+    vec3 const ro(q[0], q[1], q[2]), rd(q[4], q[5], q[6]);
+    float const max_distance = q[7];
+    random_state.rng_state = rng_states ? rng_states[i] : 0u;
+    random_state.current_prime = 0;
+    hit_t hit;
+    hit.hits = false;
+    hit.t = max_distance;
+    hit.material_index = -1;
+    hit.normal = vec3(0.f);
+    hit.uv = vec2(0.f, 0.f);
+    if (any_hit) {
+      for (int d = 0; d < n_drawables; ++d) {
+        sdf_current = d;
+        if (march_sdf(ro, rd, max_distance, true, steps, eps).hits) {
+          hit.hits = true;
+          break;
+        }
+      }
+    } else {
+      for (int d = 0; d < n_drawables; ++d) {
+        sdf_current = d;
+        hit_t h = march_sdf(ro, rd, hit.hits ? hit.t : max_distance, false, steps, eps);
+        if (h.hits && h.t < hit.t) hit = h;
+      }
+    }
+    out_hit[i] = hit.hits ? 1 : 0;
+    out_t[i] = hit.hits ? hit.t : max_distance;
+    out_n[3 * i] = hit.normal.x, out_n[3 * i + 1] = hit.normal.y, out_n[3 * i + 2] = hit.normal.z;
+    out_uv[2 * i] = hit.uv.x, out_uv[2 * i + 1] = hit.uv.y;
+    out_mat[i] = hit.hits ? hit.material_index : -1;
+  }
 }
 
 }  // extern "C"

@@ -194,6 +194,41 @@ def main() -> int:
                mat_pdf=pdf, mat_lobe=lobe, mat_resample=resample, mat_ltd=ltd, mat_nee_refl=nee_refl,
                mat_nee_pdf=nee_pdf)
     np.savez_compressed(OUT / "glsl_kat.npz", **kat)
+
+    # -- SDF: the reference's raymarch.glsl + sdf.hpp snippets (compiled in _ref) --
+    from myrt_b200 import sdf as S
+
+    lib = S.SdfLibrary()
+    lib.add(S.random_sdf_field(48, seed=5))
+    lib.add(S.smooth_union(S.mirror_axis(S.translate(S.sphere(0.3, 1), (0.4, 0.0, 0.0)), 0),
+                           S.union(S.box((0.2, 0.3, 0.1), 2),
+                                   S.subtraction(S.torus(0.5, 0.1, 3), S.vertical_capsule(0.5, 0.15, 4))), 0.2))
+    lib.add(S.intersection(S.menger_fractal(5), S.box((0.9, 0.9, 0.9), 6)))
+    pts = rng.uniform(-1.2, 1.2, (2048, 3)).astype(np.float32)
+    states = rng.integers(1, 2**32, 2048, dtype=np.uint64).astype(np.uint32)
+    sk = dict(instrs=lib.instrs, programs=lib.programs, params=lib.params, pts=pts, states=states)
+    for prog in range(3):
+        for load in (0, 1):
+            d, m = po.sdf_map(lib, prog, pts, bool(load), states, use_ref=True)
+            sk[f"map{prog}_{load}_d"], sk[f"map{prog}_{load}_m"] = d, m
+    shift = np.array([[1, 0, 0, 0.3], [0, 1, 0, -0.1], [0, 0, 1, 0.2], [0, 0, 0, 1.0]])
+    scale = np.diag([0.8, 1.2, 1.0, 1.0])
+    dr = S.sdf_drawables([np.eye(4), shift @ scale, np.eye(4)], [1, 0, 2])
+    rays = np.zeros((1536, 8), np.float32)
+    rays[:, 0:3] = rng.uniform(-2, 2, (1536, 3))
+    dd = rng.normal(size=(1536, 3))
+    rays[:, 4:7] = dd / np.linalg.norm(dd, axis=1, keepdims=True)
+    rays[:, 7] = np.inf
+    aim = rng.uniform(-0.3, 0.3, (512, 3)) + np.array([0.0, 0.0, 1.0])
+    rays[::3, 0:3] = np.array([0.0, 0.0, -3.0])
+    rays[::3, 4:7] = aim / np.linalg.norm(aim, axis=1, keepdims=True)
+    rays[1::7, 7] = 2.5
+    sk.update(drawables=dr, rays=rays)
+    for anyh in (0, 1):
+        res = po.sdf_trace(lib, dr, rays, 256, 1e-4, bool(anyh), states[:1536], use_ref=True)
+        for k, v in res.items():
+            sk[f"trace{anyh}_{k}"] = v
+    np.savez_compressed(OUT / "sdf_kat.npz", **sk)
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
     return 0

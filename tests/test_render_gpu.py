@@ -94,3 +94,32 @@ def test_reference_render_full_scene(ctx):
     acc, _ = ctx.read_accumulation(W, H)
     ref, _ = po.render_reference(s, W, H, bounces=10, frames=2, inv_view=iv, inv_proj=ip, seed=77)
     _compare(acc, ref)
+
+
+def test_reference_render_mesh_and_sdf(ctx):
+    """Meshes plus SDF drawables (a 64-primitive smooth-union field and a
+    translated Menger sponge) in one frame: the trace pass takes the nearer of
+    the mesh hit and the sphere-traced SDF hits, and shadow rays test both."""
+    from myrt_b200 import sdf as S
+
+    s = icosphere_field(n_spheres=12, subdiv=2, floor_cells=4, seed=6)
+    lib = S.SdfLibrary()
+    lib.add(S.random_sdf_field(64, k=0.1, seed=2, extent=0.6))
+    lib.add(S.intersection(S.menger_fractal(3), S.box((0.9, 0.9, 0.9), 2)))
+    up = np.array([[1, 0, 0, 0.0], [0, 1, 0, 0.2], [0, 0, 1, 0.5], [0, 0, 0, 1]])
+    side = np.array([[0.4, 0, 0, 1.3], [0, 0.4, 0, -0.6], [0, 0, 0.4, -0.4], [0, 0, 0, 1]])
+    dr = S.sdf_drawables([up, side], [0, 1])
+    ctx.upload_scene(**s)
+    ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)
+    W, H = 64, 48
+    iv, ip = look_at((0, 1, -4.5), (0, -0.3, 0), vfov_deg=50, aspect=W / H)
+    ctx.set_seed(31)
+    ctx.render(iv, ip, W, H, num_bounces=4, frames=2, sdf_marching_steps=200, sdf_marching_epsilon=1e-4)
+    acc, _ = ctx.read_accumulation(W, H)
+    scene = dict(s, sdf=dict(lib=lib, drawables=dr, steps=200, eps=1e-4))
+    ref, _ = po.render_reference(scene, W, H, bounces=4, frames=2, inv_view=iv, inv_proj=ip, seed=31)
+    ctx.upload_sdf(np.zeros((0, 2)), np.zeros((0, 2)), np.zeros(0), np.zeros((0, 36)))
+    _compare(acc, ref)
+    # the SDF drawables are visible: the render differs from the meshes-only one
+    ref0, _ = po.render_reference(s, W, H, bounces=4, frames=2, inv_view=iv, inv_proj=ip, seed=31)
+    assert np.abs(ref0[..., :3] - ref[..., :3]).max(-1).mean() > 1e-2

@@ -1,0 +1,109 @@
+"""SDF drawables: the oracle restatement against the reference's own
+raymarch.glsl + sdf.hpp snippets (golden vectors from oracle/_ref), and the
+device implementation against the oracle.
+
+Device bar: hit flags, t, normals and materials bit-exact (the evaluator is
+compiled without FMA contraction and uses only +, *, /, sqrt, min/max, abs);
+uv within 1e-5 (triplanar weights use pow, CUDA's powf vs the host libm).
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from myrt_b200 import sdf as S
+
+
+class _Lib:  # the fixture's arrays in SdfLibrary's shape
+    def __init__(self, k):
+        self.instrs, self.programs, self.params = k["instrs"], k["programs"], k["params"]
+
+
+def test_sdf_map_matches_reference(golden):
+    k = golden("sdf_kat.npz")
+    lib = _Lib(k)
+    pts, states = k["pts"], k["states"]
+    for prog in range(3):
+        for load in (0, 1):
+            d, m = po.sdf_map(lib, prog, pts, bool(load), states)
+            assert np.array_equal(d, k[f"map{prog}_{load}_d"])
+            if load:
+                assert np.array_equal(m, k[f"map{prog}_{load}_m"])
+
+
+@pytest.mark.parametrize("anyh", [0, 1])
+def test_sdf_trace_matches_reference(golden, anyh):
+    k = golden("sdf_kat.npz")
+    lib = _Lib(k)
+    res = po.sdf_trace(lib, k["drawables"], k["rays"], 256, 1e-4, bool(anyh), k["states"][:1536])
+    for key, v in res.items():
+        assert np.array_equal(v, k[f"trace{anyh}_{key}"]), key
+    assert res["hit"].sum() > 100
+
+
+def test_builder_program_shape():
+    lib = S.SdfLibrary()
+    i = lib.add(S.smooth_union(S.translate(S.sphere(0.5, 3), (1, 2, 3)), S.box((1, 1, 1), 2), 0.25))
+    assert i == 0
+    assert lib.instrs.tolist() == [[S.TRANSLATE, 0], [S.SPHERE, 3], [S.BOX, 5], [S.SMOOTH_UNION, 9]]
+    assert lib.params.tolist() == [1, 2, 3, 0.5, 3, 1, 1, 1, 2, 0.25]
+    assert lib.programs.tolist() == [[0, 4]]
+
+
+@pytest.mark.gpu
+def test_sdf_trace_gpu_matches_oracle(ctx, golden):
+    k = golden("sdf_kat.npz")
+    lib = _Lib(k)
+    dr, rays, states = k["drawables"], k["rays"], k["states"][:1536]
+    ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)
+    for anyh in (False, True):
+        got = ctx.trace_sdf(rays, 256, 1e-4, any_hit=anyh, rng_states=states)
+        ora = po.sdf_trace(lib, dr, rays, 256, 1e-4, anyh, states)
+        assert np.array_equal(got["hit"], ora["hit"])
+        assert np.array_equal(got["t"], ora["t"])
+        if not anyh:
+            assert np.array_equal(got["normal"], ora["normal"])
+            assert np.array_equal(got["material"], ora["material"])
+            np.testing.assert_allclose(got["uv"], ora["uv"], rtol=1e-5, atol=1e-6)
+    ctx.upload_sdf(np.zeros((0, 2)), np.zeros((0, 2)), np.zeros(0), np.zeros((0, 36)))
+
+
+@pytest.mark.gpu
+def test_sdf_field_256_prims_gpu(ctx):
+    """The hybrid configuration's SDF: 256 spheres/boxes/tori under smooth union k = 0.1."""
+    lib = S.SdfLibrary()
+    lib.add(S.random_sdf_field(256, k=0.1, seed=9))
+    dr = S.sdf_drawables([np.eye(4)], [0])
+    rng = np.random.default_rng(4)
+    rays = np.zeros((8192, 8), np.float32)
+    rays[:, 0:3] = np.array([0.0, 0.3, -3.5])
+    aim = rng.uniform(-0.35, 0.35, (8192, 3)) + np.array([0.0, 0.0, 1.0])
+    rays[:, 4:7] = aim / np.linalg.norm(aim, axis=1, keepdims=True)
+    rays[:, 7] = np.inf
+    states = rng.integers(1, 2**32, 8192, dtype=np.uint64).astype(np.uint32)
+    ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)
+    got = ctx.trace_sdf(rays, 256, 1e-4, rng_states=states)
+    ora = po.sdf_trace(lib, dr, rays, 256, 1e-4, False, states)
+    assert got["hit"].sum() > 1000
+    assert np.array_equal(got["hit"], ora["hit"])
+    assert np.array_equal(got["t"], ora["t"])
+    assert np.array_equal(got["material"], ora["material"])
+    ctx.upload_sdf(np.zeros((0, 2)), np.zeros((0, 2)), np.zeros(0), np.zeros((0, 36)))
+
+
+@pytest.mark.gpu
+def test_sdf_upload_rejects_bad_programs(ctx):
+    import myrt_b200 as mb
+
+    dr = S.sdf_drawables([np.eye(4)], [0])
+    bad = [
+        (np.array([[S.UNION, 0]]), np.array([[0, 1]]), np.zeros(1)),           # operator without operands
+        (np.array([[S.SPHERE, 0]]), np.array([[0, 1]]), np.zeros(1)),          # parameter outside the buffer
+        (np.array([[99, 0]]), np.array([[0, 1]]), np.zeros(4)),                # unknown opcode
+        (np.array([[S.SPHERE, 0], [S.SPHERE, 0]]), np.array([[0, 2]]), np.zeros(2)),  # two results
+        (np.array([[S.TRANSLATE, 0]]), np.array([[0, 1]]), np.zeros(3)),       # modifier without primitive
+    ]
+    for ins, prs, par in bad:
+        with pytest.raises(mb.MyrtError):
+            ctx.upload_sdf(ins, prs, par, dr)
+    with pytest.raises(mb.MyrtError):  # drawable references a missing program
+        ctx.upload_sdf(np.array([[S.SPHERE, 0]]), np.array([[0, 1]]), np.zeros(2), S.sdf_drawables([np.eye(4)], [3]))
