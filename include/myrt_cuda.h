@@ -146,6 +146,9 @@ typedef struct myrt_tuning {
   uint32_t trace_min_blocks; /* one-thread-per-ray: register cap as blocks per SM: 0 or 8 (64 regs), 10, 12 */
   uint32_t trace_unit_steps; /* one-thread-per-ray: 0 = a node and all its triangles per iteration,
                                 1 = one node, triangle or pop per iteration */
+  uint32_t wave_paths;       /* physical / guided wavefront: paths in flight per wave (0 = 4 Mi) */
+  uint32_t pt_blocks_per_sm; /* physical / guided: resident 128-thread blocks per SM of the
+                                grid-stride extend / shade / shadow kernels (0 = 8) */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */
@@ -273,7 +276,17 @@ typedef enum myrt_shading {
   /* The reference's passes and shading: 2 hard-coded sphere lights with NEE,
    * the PBR material's bounce/evaluate, Russian roulette on the path pdf, sky
    * gradient (src/pt/pt_trace.comp, pt_color.comp). */
-  MYRT_SHADE_REFERENCE = 0
+  MYRT_SHADE_REFERENCE = 0,
+  /* Physically based: GGX + Lambert BSDF over the same PBR record, next-event
+   * estimation to the area lights (myrt_set_area_lights) with power-heuristic
+   * MIS, Russian roulette on the throughput, constant environment radiance.
+   * `frames` is the number of samples per pixel of the call. Results depend
+   * only on (pixel, sample index, seed): wave size and batching do not change
+   * them. */
+  MYRT_SHADE_PHYSICAL = 1,
+  /* MYRT_SHADE_PHYSICAL with a learned proposal mixed into BSDF sampling by
+   * one-sample MIS (myrt_guide_*). */
+  MYRT_SHADE_GUIDED = 2
 } myrt_shading;
 
 typedef struct myrt_render_params {
@@ -284,7 +297,30 @@ typedef struct myrt_render_params {
   uint32_t flags;      /* reserved, 0 */
   int32_t sdf_marching_steps;  /* set_sdf_marching_steps (reference default 400) */
   float sdf_marching_epsilon;  /* set_sdf_marching_epsilon (reference default 1e-5) */
+  /* physical and guided modes (ignored by MYRT_SHADE_REFERENCE) */
+  int32_t max_depth;      /* surface vertices with NEE and a continuation ray (0: 8) */
+  int32_t rr_start;       /* Russian roulette from this vertex index on */
+  uint32_t seed;          /* key of the counter-based random stream */
+  uint32_t accum_fp64;    /* 1: accumulate in FP64 (converged-oracle renders) */
+  float env_radiance[3];  /* radiance of rays that leave the scene */
+  uint32_t wave_paths;    /* paths in flight per wave (0: the context's tuning) */
 } myrt_render_params;
+
+/* Parallelogram area light corner + a*edge_u + b*edge_v, a, b in [0, 1],
+ * emitting `emission` (radiance) on the side of cross(edge_u, edge_v). Used by
+ * the physical and guided modes; lights are not occluders for shadow rays.
+ * Config "one 0.2 x 0.2 area light, emission 20" is one such record. */
+typedef struct myrt_area_light {
+  float corner[3];
+  float edge_u[3];
+  float edge_v[3];
+  float emission[3];
+} myrt_area_light;
+
+/* Replaces the area lights (n <= 64; n = 0 removes them). Restarts
+ * accumulation. NEE picks a light with probability proportional to
+ * luminance(emission) * area. */
+int myrt_set_area_lights(myrt_ctx* ctx, const myrt_area_light* lights, uint32_t n);
 
 /* Renders `frames` frames, each the reference's generate -> {trace, color,
  * filter} x num_bounces -> trace, color sequence, accumulating into the
@@ -299,6 +335,19 @@ int myrt_render(myrt_ctx* ctx, const myrt_camera* camera, const myrt_render_para
  * the display image (output_image: clamp(sum / count, 0, 4)), W*H*4 floats
  * each, row-major from pixel (0, 0); either pointer may be NULL. */
 int myrt_read_accumulation(myrt_ctx* ctx, float* rgba_sum, float* rgba_display);
+/* Rays traced by the physical / guided wavefront since the context was
+ * created (cumulative; take differences around a call). */
+typedef struct myrt_render_stats {
+  uint64_t paths;           /* camera rays */
+  uint64_t extension_rays;  /* closest-hit queries, camera rays included */
+  uint64_t shadow_rays;     /* any-hit queries */
+  uint64_t reserved;
+} myrt_render_stats;
+int myrt_get_render_stats(myrt_ctx* ctx, myrt_render_stats* out);
+
+/* The FP64 accumulation (rgb sum, sample count) of a physical / guided render
+ * made with accum_fp64 = 1, W*H*4 doubles. */
+int myrt_read_accumulation_f64(myrt_ctx* ctx, double* rgba_sum);
 /* Device pointers of the two images (valid until the next resolution change). */
 int myrt_render_buffers(myrt_ctx* ctx, void** accum, void** display);
 /* sequential_pathtracer::invalidate_counter / sample_count / the m_rng seed. */

@@ -95,8 +95,10 @@ class Context:
             raise MyrtError(rc, f"{what}: {buf.value.decode(errors='replace')}")
 
     def set_tuning(self, trace_persistent: int = 0, refill: int = 1, blocks_per_sm: int = 0,
-                   trace_min_blocks: int = 0, trace_unit_steps: int = 0):
-        t = _abi.myrt_tuning(trace_persistent, refill, blocks_per_sm, trace_min_blocks, trace_unit_steps)
+                   trace_min_blocks: int = 0, trace_unit_steps: int = 0, wave_paths: int = 0,
+                   pt_blocks_per_sm: int = 0):
+        t = _abi.myrt_tuning(trace_persistent, refill, blocks_per_sm, trace_min_blocks, trace_unit_steps,
+                             wave_paths, pt_blocks_per_sm)
         self._check(self._L.myrt_set_tuning(self._h, C.byref(t)), "myrt_set_tuning")
 
     def get_tuning(self) -> dict:
@@ -209,6 +211,43 @@ class Context:
         p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0, sdf_marching_steps,
                                     sdf_marching_epsilon)
         self._check(self._L.myrt_render(self._h, C.byref(cam), C.byref(p)), "myrt_render")
+
+    def set_area_lights(self, lights):
+        """myrt_set_area_lights: lights [n, 12] float32 rows (corner, edge_u,
+        edge_v, emission)."""
+        L = np.ascontiguousarray(lights, np.float32).reshape(-1, 12)
+        arr = (_abi.myrt_area_light * max(1, L.shape[0]))()
+        C.memmove(arr, L.ctypes.data, L.nbytes)
+        self._check(self._L.myrt_set_area_lights(self._h, arr, L.shape[0]), "myrt_set_area_lights")
+
+    def render_physical(self, inverse_view, inverse_projection, width: int, height: int, spp: int = 1,
+                        max_depth: int = 8, rr_start: int = 3, seed: int = 0, env=(0.0, 0.0, 0.0),
+                        fp64: bool = False, guided: bool = False, wave_paths: int = 0,
+                        sdf_marching_steps: int = 256, sdf_marching_epsilon: float = 1e-4):
+        """Physical (or guided) shading: `spp` samples per pixel accumulated
+        into the context's images."""
+        cam = _abi.myrt_camera()
+        cam.inverse_view[:] = np.asarray(inverse_view, np.float32).ravel().tolist()
+        cam.inverse_projection[:] = np.asarray(inverse_projection, np.float32).ravel().tolist()
+        p = _abi.myrt_render_params()
+        p.width, p.height, p.num_bounces, p.frames = width, height, 0, spp
+        p.shading = _abi.SHADE_GUIDED if guided else _abi.SHADE_PHYSICAL
+        p.sdf_marching_steps, p.sdf_marching_epsilon = sdf_marching_steps, sdf_marching_epsilon
+        p.max_depth, p.rr_start, p.seed, p.accum_fp64 = max_depth, rr_start, seed, int(fp64)
+        p.env_radiance[:] = [float(x) for x in env]
+        p.wave_paths = wave_paths
+        self._check(self._L.myrt_render(self._h, C.byref(cam), C.byref(p)), "myrt_render")
+
+    def render_stats(self) -> dict:
+        """Cumulative camera / extension / shadow ray counts of the physical wavefront."""
+        st = _abi.myrt_render_stats()
+        self._check(self._L.myrt_get_render_stats(self._h, C.byref(st)), "myrt_get_render_stats")
+        return dict(paths=st.paths, extension_rays=st.extension_rays, shadow_rays=st.shadow_rays)
+
+    def read_accumulation_f64(self, width: int, height: int):
+        acc = np.empty((height, width, 4), np.float64)
+        self._check(self._L.myrt_read_accumulation_f64(self._h, acc.ctypes.data), "myrt_read_accumulation_f64")
+        return acc
 
     def render_noalloc(self, inverse_view, inverse_projection, width: int, height: int, accum, display,
                        sample_index: int = 0, num_bounces: int = 10, frames: int = 1,

@@ -60,7 +60,19 @@ class myrt_camera(C.Structure):
 class myrt_render_params(C.Structure):
     _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("num_bounces", C.c_int32), ("frames", C.c_uint32),
                 ("shading", C.c_int32), ("flags", C.c_uint32), ("sdf_marching_steps", C.c_int32),
-                ("sdf_marching_epsilon", C.c_float)]
+                ("sdf_marching_epsilon", C.c_float), ("max_depth", C.c_int32), ("rr_start", C.c_int32),
+                ("seed", C.c_uint32), ("accum_fp64", C.c_uint32), ("env_radiance", C.c_float * 3),
+                ("wave_paths", C.c_uint32)]
+
+
+class myrt_render_stats(C.Structure):
+    _fields_ = [("paths", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("reserved", C.c_uint64)]
+
+
+class myrt_area_light(C.Structure):
+    _fields_ = [("corner", C.c_float * 3), ("edge_u", C.c_float * 3), ("edge_v", C.c_float * 3),
+                ("emission", C.c_float * 3)]
 
 
 class myrt_sdf_view(C.Structure):
@@ -71,10 +83,13 @@ class myrt_sdf_view(C.Structure):
 
 class myrt_tuning(C.Structure):
     _fields_ = [("trace_persistent", C.c_uint32), ("refill", C.c_uint32), ("blocks_per_sm", C.c_uint32),
-                ("trace_min_blocks", C.c_uint32), ("trace_unit_steps", C.c_uint32)]
+                ("trace_min_blocks", C.c_uint32), ("trace_unit_steps", C.c_uint32), ("wave_paths", C.c_uint32),
+                ("pt_blocks_per_sm", C.c_uint32)]
 
 
 SHADE_REFERENCE = 0
+SHADE_PHYSICAL = 1
+SHADE_GUIDED = 2
 
 P = C.c_void_p
 SZ = C.c_size_t
@@ -104,6 +119,9 @@ SIGNATURES = {
     "myrt_trace_closest_stats_device": (I, [P, P, U32, P, P, P, I, P]),
     "myrt_render": (I, [P, C.POINTER(myrt_camera), C.POINTER(myrt_render_params)]),
     "myrt_read_accumulation": (I, [P, P, P]),
+    "myrt_read_accumulation_f64": (I, [P, P]),
+    "myrt_set_area_lights": (I, [P, P, U32]),
+    "myrt_get_render_stats": (I, [P, C.POINTER(myrt_render_stats)]),
     "myrt_render_buffers": (I, [P, C.POINTER(P), C.POINTER(P)]),
     "myrt_reset_accumulation": (I, [P]),
     "myrt_sample_count": (I, [P, C.POINTER(C.c_uint32)]),

@@ -288,6 +288,7 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   cudaFree(ctx->sdf.params);
   cudaFree(ctx->sdf.drawables);
   free_render(ctx->render);
+  free_physical(ctx->physical);
   for (auto& p : ctx->stage) cudaFree(p);
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_next);
@@ -306,7 +307,8 @@ int myrt_get_last_error(myrt_ctx* ctx, char* buf, size_t size) {
 int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
   if (!ctx || !t) return MYRT_ERR_INVALID_ARGUMENT;
   if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
-      t->trace_unit_steps > 1)
+      t->trace_unit_steps > 1 || (t->wave_paths != 0 && (t->wave_paths < 1024 || t->wave_paths > (1u << 28))) ||
+      t->pt_blocks_per_sm > 16)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;
@@ -570,16 +572,49 @@ int myrt_render(myrt_ctx* ctx, myrt_camera const* camera, myrt_render_params con
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "image size must be 1 .. 2^30 pixels");
   if (p->num_bounces < 0 || p->num_bounces > 1024)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "num_bounces must be in [0, 1024]");
-  if (p->shading != MYRT_SHADE_REFERENCE) return set_error(ctx, MYRT_ERR_UNSUPPORTED, "unknown shading mode");
+  if (p->shading != MYRT_SHADE_REFERENCE && p->shading != MYRT_SHADE_PHYSICAL && p->shading != MYRT_SHADE_GUIDED)
+    return set_error(ctx, MYRT_ERR_UNSUPPORTED, "unknown shading mode");
+  bool const physical = p->shading != MYRT_SHADE_REFERENCE;
+  if (physical && (p->max_depth < 0 || p->max_depth > 64 || p->rr_start < 0 || p->accum_fp64 > 1))
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "max_depth must be in [0, 64], rr_start >= 0, accum_fp64 0 or 1");
+  if (physical && p->frames > (1u << 24))
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "at most 2^24 samples per pixel per call");
   if (p->frames == 0) return MYRT_OK;
-  // set_view_matrix / set_projection_matrix: a changed camera restarts accumulation
+  // set_view_matrix / set_projection_matrix: a changed camera restarts accumulation;
+  // so does a change of shading mode or accumulation precision
   render_state& R = ctx->render;
   if (!R.have_camera || std::memcmp(R.last_camera, camera, sizeof(R.last_camera)) != 0) {
     std::memcpy(R.last_camera, camera, sizeof(R.last_camera));
     R.have_camera = true;
     R.sample_counter = 0;
   }
-  return render_reference_frames(ctx, camera, p);
+  uint32_t const fp64 = physical ? p->accum_fp64 : 0u;
+  if (R.mode != p->shading || R.fp64 != fp64) {
+    R.mode = p->shading;
+    R.fp64 = fp64;
+    R.sample_counter = 0;
+  }
+  return physical ? render_physical_frames(ctx, camera, p) : render_reference_frames(ctx, camera, p);
+}
+
+int myrt_set_area_lights(myrt_ctx* ctx, myrt_area_light const* lights, uint32_t n) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  return set_area_lights(ctx, lights, n);
+}
+
+int myrt_get_render_stats(myrt_ctx* ctx, myrt_render_stats* out) {
+  if (!ctx || !out) return MYRT_ERR_INVALID_ARGUMENT;
+  return get_render_stats(ctx, out);
+}
+
+int myrt_read_accumulation_f64(myrt_ctx* ctx, double* rgba_sum) {
+  if (!ctx || !rgba_sum) return MYRT_ERR_INVALID_ARGUMENT;
+  render_state const& R = ctx->render;
+  if (!R.accum64 || !R.fp64) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "no FP64 accumulation in progress");
+  size_t const bytes = size_t(R.width) * R.height * 32;
+  int rc = check_cuda(ctx, cudaMemcpyAsync(rgba_sum, R.accum64, bytes, cudaMemcpyDeviceToHost, ctx->stream), "read");
+  if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "read");
+  return rc;
 }
 
 int myrt_render_noalloc(myrt_ctx* ctx, myrt_camera const* camera, myrt_render_params const* p, uint32_t sample_index,

@@ -52,6 +52,22 @@ struct render_state {
   uint32_t sample_counter = 0;          // frames accumulated since the last reset
   float last_camera[32] = {};
   bool have_camera = false;
+  int mode = -1;                        // myrt_shading of the accumulation in progress
+  uint32_t fp64 = 0;                    // physical modes: accumulation in accum64
+  double4* accum64 = nullptr;           // physical modes, accum_fp64: rgb sum, count
+};
+
+// Physical / guided wavefront state: ray queues sized for one wave of paths.
+struct physical_state {
+  size_t capacity = 0;                  // paths per wave the buffers hold
+  float4* queue[2] = {nullptr, nullptr};  // 3 float4 per ray: (o, path), (d, prev pdf), (throughput, -)
+  float4* hits = nullptr;               // 3 float4 per queue slot: (p, kind), (ns, t), (ng, -)
+  float4* shadow = nullptr;             // 3 float4 per shadow ray: (o, path), (d, tmax), (contribution, -)
+  float4* radiance = nullptr;           // per path: rgb
+  uint32_t* counts = nullptr;           // [0..1] ray queues, [2] shadow queue
+  unsigned long long* stats = nullptr;  // paths, extension rays, shadow rays (cumulative)
+  void* lights = nullptr;               // ps::area_light[n_lights]
+  int n_lights = 0;
 };
 
 }  // namespace myrt_b200
@@ -65,8 +81,9 @@ struct myrt_ctx {
   myrt_b200::device_scene scene;
   myrt_b200::device_sdf sdf;
   myrt_b200::render_state render;
+  myrt_b200::physical_state physical;
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
-  myrt_tuning tuning{0u, 1u, 0u, 0u};
+  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u};
   int sm_count = 0;
   uint32_t* d_next = nullptr;    // ring of ray counters for the persistent traversal
   uint32_t next_slot = 0;
@@ -79,6 +96,11 @@ namespace myrt_b200 {
 int set_error(myrt_ctx* ctx, int code, std::string msg);
 int check_cuda(myrt_ctx* ctx, cudaError_t e, char const* what);
 void free_render(render_state& r);
+void free_physical(physical_state& p);
+int ensure_images(myrt_ctx* ctx, uint32_t W, uint32_t H);
+int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p);
+int set_area_lights(myrt_ctx* ctx, myrt_area_light const* lights, uint32_t n);
+int get_render_stats(myrt_ctx* ctx, myrt_render_stats* out);
 int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p);
 int trace_sdf_rays(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, int steps, float eps, int any_hit,
     uint32_t const* rng_states, float* out);

@@ -421,32 +421,21 @@ __global__ void __launch_bounds__(kBlock) k_scatter(float4 const* __restrict__ g
 
 // ---- host side ----------------------------------------------------------------------
 int ensure_render_buffers(myrt_ctx* ctx, uint32_t W, uint32_t H) {
+  int rc = ensure_images(ctx, W, H);
   render_state& R = ctx->render;
-  if (R.width == W && R.height == H && R.accum) return MYRT_OK;
-  free_render(R);
+  if (rc || R.gen[0]) return rc;
   size_t const n = size_t(W) * H;
   size_t const nb = (n + kBlock - 1) / kBlock;
-  int rc = MYRT_OK;
   auto alloc = [&](void** p, size_t bytes, char const* what) {
     if (!rc) rc = check_cuda(ctx, cudaMalloc(p, bytes), what);
   };
   alloc(reinterpret_cast<void**>(&R.gen[0]), n * 80, "ray state");
   alloc(reinterpret_cast<void**>(&R.gen[1]), n * 80, "ray state");
   alloc(reinterpret_cast<void**>(&R.trace), n * 64, "trace state");
-  alloc(reinterpret_cast<void**>(&R.accum), n * 16, "accumulation image");
-  alloc(reinterpret_cast<void**>(&R.display), n * 16, "display image");
   alloc(reinterpret_cast<void**>(&R.counts), 2 * sizeof(uint32_t), "ray counts");
   alloc(reinterpret_cast<void**>(&R.block_sums), std::max<size_t>(nb, 1) * sizeof(uint32_t), "block sums");
-  if (!rc) rc = check_cuda(ctx, cudaMemsetAsync(R.accum, 0, n * 16, ctx->stream), "clear");
-  if (!rc) rc = check_cuda(ctx, cudaMemsetAsync(R.display, 0, n * 16, ctx->stream), "clear");
-  if (rc) {
-    free_render(R);
-    return rc;
-  }
-  R.width = W;
-  R.height = H;
-  R.sample_counter = 0;  // invalidate_texture -> invalidate_counter
-  return MYRT_OK;
+  if (rc) free_render(R);
+  return rc;
 }
 
 void mat_mul4(float const* a, float const* b, float* out) {
@@ -462,14 +451,36 @@ void mat_mul4(float const* a, float const* b, float* out) {
 void free_render(render_state& R) {
   for (void* p : {static_cast<void*>(R.gen[0]), static_cast<void*>(R.gen[1]), static_cast<void*>(R.trace),
            static_cast<void*>(R.accum), static_cast<void*>(R.display), static_cast<void*>(R.counts),
-           static_cast<void*>(R.block_sums), static_cast<void*>(R.pass_tex)})
+           static_cast<void*>(R.block_sums), static_cast<void*>(R.pass_tex), static_cast<void*>(R.accum64)})
     cudaFree(p);
   R.gen[0] = R.gen[1] = nullptr;
   R.trace = R.accum = R.display = nullptr;
   R.counts = R.block_sums = nullptr;
   R.pass_tex = nullptr;
+  R.accum64 = nullptr;
   R.pass_tex_capacity = 0;
   R.width = R.height = 0;
+}
+
+// The accumulation and display images of a W x H render (both modes). A new
+// size releases every render buffer and restarts accumulation.
+int ensure_images(myrt_ctx* ctx, uint32_t W, uint32_t H) {
+  render_state& R = ctx->render;
+  if (R.width == W && R.height == H && R.accum) return MYRT_OK;
+  free_render(R);
+  size_t const n = size_t(W) * H;
+  int rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&R.accum), n * 16), "accumulation image");
+  if (!rc) rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&R.display), n * 16), "display image");
+  if (!rc) rc = check_cuda(ctx, cudaMemsetAsync(R.accum, 0, n * 16, ctx->stream), "clear");
+  if (!rc) rc = check_cuda(ctx, cudaMemsetAsync(R.display, 0, n * 16, ctx->stream), "clear");
+  if (rc) {
+    free_render(R);
+    return rc;
+  }
+  R.width = W;
+  R.height = H;
+  R.sample_counter = 0;  // invalidate_texture -> invalidate_counter
+  return MYRT_OK;
 }
 
 // Host random stream of sequential_pathtracer.cpp:282-498 for `frames` frames:

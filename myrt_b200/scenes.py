@@ -171,3 +171,23 @@ def icosphere_camera_rays(width: int = 512, height: int = 512, spp: int = 1, see
         out.append(pinhole_rays(width, height, eye=(0.0, 1.0, -4.5), target=(0.0, -0.3, 0.0), vfov_deg=50.0,
                                 jitter=jit))
     return np.concatenate(out, 0)
+
+
+def area_light(center, size, emission) -> np.ndarray:
+    """Square light of side `size` centred at `center`, facing -y (down):
+    one [12] row (corner, edge_u, edge_v, emission) for set_area_lights."""
+    c = np.asarray(center, np.float32)
+    h = np.float32(size) / 2
+    row = np.zeros(12, np.float32)
+    row[0:3] = c - np.array([h, 0, h], np.float32)
+    row[3:6] = [size, 0, 0]
+    row[6:9] = [0, 0, size]
+    row[9:12] = np.broadcast_to(np.asarray(emission, np.float32), 3)
+    return row
+
+
+def icosphere_field_lit(n_spheres: int = 512, subdiv: int = 3, floor_cells: int = 16, seed: int = 2):
+    """The icosphere field plus its one 0.2 x 0.2 ceiling light of emission 20
+    at y = 1.6 (above every sphere), facing down: (scene, lights[1, 12])."""
+    s = icosphere_field(n_spheres=n_spheres, subdiv=subdiv, floor_cells=floor_cells, seed=seed)
+    return s, area_light((0.0, 1.6, 0.0), 0.2, 20.0)[None, :]

@@ -392,9 +392,23 @@ void orc_refbvh_indices(void* h, std::uint32_t* out) {
 
 // bvh.impl.glsl:8-72 with the pt_trace.comp visitor. nodes: 48-byte records.
 // canonical = 0: first visited wins ties (the reference); 1: smaller prim wins.
+void orc_refbvh_query(void const* nodes_v, std::uint32_t const* bvh_idx, std::uint32_t const* indices,
+    float const* points_xyzw, float const* rays, std::size_t n, int any_hit, int canonical, int isect,
+    std::int32_t* prim, float* t_out, float* u_out, float* v_out, int nthreads);
+
 void orc_refbvh_traverse(void const* nodes_v, std::uint32_t const* bvh_idx, std::uint32_t const* indices,
     float const* points_xyzw, float const* rays, std::size_t n, int any_hit, int canonical, std::int32_t* prim,
     float* t_out, float* u_out, float* v_out, int nthreads) {
+  orc_refbvh_query(nodes_v, bvh_idx, indices, points_xyzw, rays, n, any_hit, canonical, -1, prim, t_out, u_out, v_out,
+      nthreads);
+}
+
+// isect -1: the reference's traversal as written (Moller-Trumbore, no tmin
+// test); 0 / 1: Moller-Trumbore / watertight with the device kernels'
+// acceptance rule (t >= tmin, t < tmax).
+void orc_refbvh_query(void const* nodes_v, std::uint32_t const* bvh_idx, std::uint32_t const* indices,
+    float const* points_xyzw, float const* rays, std::size_t n, int any_hit, int canonical, int isect,
+    std::int32_t* prim, float* t_out, float* u_out, float* v_out, int nthreads) {
   auto const* nodes = static_cast<ref_node const*>(nodes_v);
   auto pt = [points_xyzw](std::uint32_t i) {
     return v3{points_xyzw[4 * i], points_xyzw[4 * i + 1], points_xyzw[4 * i + 2]};
@@ -403,6 +417,7 @@ void orc_refbvh_traverse(void const* nodes_v, std::uint32_t const* bvh_idx, std:
     for (std::size_t r = b; r < e; ++r) {
       ray8 const ray = load_ray(rays + 8 * r);
       v3 const ro = ray.o, rd = ray.d;
+      wt_ray const wt = wt_setup(rd);
       v3 const inv{1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z};
       float maxt = ray.tmax;
       float best_t = ray.tmax, bu = 0, bv = 0;
@@ -431,8 +446,10 @@ void orc_refbvh_traverse(void const* nodes_v, std::uint32_t const* bvh_idx, std:
           for (std::uint32_t tri = current.first; tri <= current.second; ++tri) {
             std::uint32_t const pi = bvh_idx[tri];
             float t, u, v;
-            bool h = isect_reference(ro, rd, pt(indices[3 * pi]), pt(indices[3 * pi + 1]), pt(indices[3 * pi + 2]),
-                t, u, v);
+            bool h = isect < 0 ? isect_reference(ro, rd, pt(indices[3 * pi]), pt(indices[3 * pi + 1]),
+                                     pt(indices[3 * pi + 2]), t, u, v)
+                               : test_tri(isect, wt, ray, pt(indices[3 * pi]), pt(indices[3 * pi + 1]),
+                                     pt(indices[3 * pi + 2]), t, u, v);
             h = h && t < maxt && (canonical ? canonical_better(t, std::int32_t(pi), best_t, best) : best_t > t);
             if (h) {
               best_t = t;

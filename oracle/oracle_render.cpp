@@ -11,7 +11,7 @@
 //   material_new.glsl:14-49 and the dispatch material_registry::generate_code
 //   emits (material.hpp:39-65) for the single PBR type
 //   pt_generate.comp:50-84       pass_generate
-//   pt_trace.comp:134-226, :331-386 (meshes; no SDF drawables)  pass_trace
+//   pt_trace.comp:134-226, :311-386 (meshes, then SDF drawables)  pass_trace
 //   pt_color.comp:77-202         pass_color (no cubemap: sky gradient)
 //   pt_ray_filter.comp:49-64     pass_filter, as a STABLE compaction (slot order
 //                                = serial order; the reference's atomicAdd order
@@ -1097,4 +1097,416 @@ void orc_material_eval(float const* mat7, int lobe, float resample, float const*
   *out_pdf = pdf;
 }
 
+}  // extern "C"
+
+// ==== physical shading mode ======================================================
+extern "C" void orc_refbvh_query(void const* nodes_v, std::uint32_t const* bvh_idx, std::uint32_t const* indices,
+    float const* points_xyzw, float const* rays, std::size_t n, int any_hit, int canonical, int isect,
+    std::int32_t* prim, float* t_out, float* u_out, float* v_out, int nthreads);
+
+// Path-at-a-time restatement of the physical mode (GGX + Lambert over the PBR
+// record, NEE with the power heuristic to parallelogram lights, Russian
+// roulette on the throughput, counter-based random numbers). The method is
+// this project's own (the reference has no such mode); this is its checker.
+// Only +, -, *, /, sqrt and comparisons: with -ffp-contract=off it reproduces
+// the device kernels bit for bit.
+namespace {
+
+struct ph_u4 {
+  std::uint32_t x, y, z, w;
+};
+// pcg4d (Jarzynski and Olano, JCGT 9(3) 2020)
+ph_u4 ph_pcg4d(std::uint32_t a, std::uint32_t b, std::uint32_t c, std::uint32_t d) {
+  ph_u4 v{a * 1664525u + 1013904223u, b * 1664525u + 1013904223u, c * 1664525u + 1013904223u,
+      d * 1664525u + 1013904223u};
+  v.x += v.y * v.w;
+  v.y += v.z * v.x;
+  v.z += v.x * v.y;
+  v.w += v.y * v.z;
+  v.x ^= v.x >> 16;
+  v.y ^= v.y >> 16;
+  v.z ^= v.z >> 16;
+  v.w ^= v.w >> 16;
+  v.x += v.y * v.w;
+  v.y += v.z * v.x;
+  v.z += v.x * v.y;
+  v.w += v.y * v.z;
+  return v;
+}
+inline float ph_u01(std::uint32_t x) { return float(x >> 8) * (1.0f / 16777216.0f); }
+struct ph_r4 {
+  float a, b, c, d;
+};
+inline ph_r4 ph_rand4(std::uint32_t pix, std::uint32_t sample, std::uint32_t seed, std::uint32_t stream) {
+  ph_u4 const h = ph_pcg4d(pix, sample, seed, stream);
+  return {ph_u01(h.x), ph_u01(h.y), ph_u01(h.z), ph_u01(h.w)};
+}
+
+// sin / cos of 2 pi u: nearest quadrant, Taylor series on [-pi/4, pi/4]
+void ph_sincos_turns(float u, float& s, float& c) {
+  float const x = u * 4.0f;
+  float const k = std::nearbyint(x);
+  float const a = (x - k) * 1.57079632679489662f;
+  float const a2 = a * a;
+  float const sp = a * (1.0f + a2 * (-1.0f / 6.0f + a2 * (1.0f / 120.0f + a2 * (-1.0f / 5040.0f + a2 * (1.0f / 362880.0f)))));
+  float const cp = 1.0f + a2 * (-0.5f + a2 * (1.0f / 24.0f + a2 * (-1.0f / 720.0f + a2 * (1.0f / 40320.0f +
+                                                                                        a2 * (-1.0f / 3628800.0f)))));
+  int const q = int(k) & 3;
+  s = q == 0 ? sp : (q == 1 ? cp : (q == 2 ? -sp : -cp));
+  c = q == 0 ? cp : (q == 1 ? -sp : (q == 2 ? -cp : sp));
+}
+
+inline float ph_lum(v3 c) { return (0.2126f * c.x + 0.7152f * c.y) + 0.0722f * c.z; }
+inline float ph_max3(v3 c) { return std::fmax(c.x, std::fmax(c.y, c.z)); }
+inline bool ph_finite(v3 c) { return std::isfinite(c.x) && std::isfinite(c.y) && std::isfinite(c.z); }
+constexpr float kPhPi = 3.14159265358979324f;
+constexpr float kPhInvPi = 0.318309886183790672f;
+
+struct ph_mat {
+  v3 diffuse, f0;
+  float alpha, p_spec;
+};
+ph_mat ph_load(float const* data, int off) {
+  std::uint32_t bits;
+  std::memcpy(&bits, data + off, 4);
+  v3 const alb{float(bits & 0xffu) / 255.0f, float((bits >> 8) & 0xffu) / 255.0f, float((bits >> 16) & 0xffu) / 255.0f};
+  float const ior = data[off + 1], rough = data[off + 2], metal = data[off + 3];
+  float const r = (ior - 1.0f) / (ior + 1.0f);
+  float const f0d = r * r;
+  ph_mat m;
+  m.f0 = v3{f0d, f0d, f0d} * (1.0f - metal) + alb * metal;
+  m.diffuse = alb * ((1.0f - metal) * (1.0f - f0d));
+  m.alpha = std::fmax(rough * rough, 1e-3f);
+  float const ws = ph_lum(m.f0), wd = ph_lum(m.diffuse);
+  m.p_spec = wd > 0.0f ? std::fmin(std::fmax(ws / (ws + wd), 0.25f), 0.9f) : 1.0f;
+  return m;
+}
+inline float ph_lambda(float c, float a2) {
+  float const c2 = c * c;
+  return (std::sqrt(1.0f + a2 * ((1.0f - c2) / c2)) - 1.0f) * 0.5f;
+}
+struct ph_eval {
+  v3 f{0, 0, 0};
+  float pdf = 0, cos_i = 0;
+};
+ph_eval ph_bsdf(ph_mat const& m, v3 ns, v3 ng, v3 wo, v3 wi) {
+  ph_eval r;
+  float const ci = dot(ns, wi), co = dot(ns, wo);
+  if (!(ci > 0.0f) || !(dot(ng, wi) > 0.0f) || !(co > 0.0f)) return r;
+  v3 const h = normalize(wo + wi);
+  float const ch = dot(ns, h), coh = dot(wo, h);
+  float const a2 = m.alpha * m.alpha;
+  float const tt = ch * ch * (a2 - 1.0f) + 1.0f;
+  float const D = a2 / ((kPhPi * tt) * tt);
+  float const lo = ph_lambda(co, a2), li = ph_lambda(ci, a2);
+  float const G1 = 1.0f / (1.0f + lo);
+  float const G2 = 1.0f / ((1.0f + lo) + li);
+  float const om = 1.0f - std::fmax(coh, 0.0f);
+  float const om2 = om * om;
+  float const w5 = om2 * om2 * om;
+  v3 const F = m.f0 + (v3{1.0f, 1.0f, 1.0f} - m.f0) * w5;
+  float const spec = (D * G2) / ((4.0f * co) * ci);
+  r.f = m.diffuse * kPhInvPi + F * spec;
+  float const ps = coh > 0.0f ? (G1 * D) / (4.0f * co) : 0.0f;
+  r.pdf = m.p_spec * ps + (1.0f - m.p_spec) * (ci * kPhInvPi);
+  r.cos_i = ci;
+  return r;
+}
+void ph_onb(v3 n, v3& t, v3& b) {
+  float const sign = n.z >= 0.0f ? 1.0f : -1.0f;
+  float const a = -1.0f / (sign + n.z);
+  float const bb = n.x * n.y * a;
+  t = {1.0f + sign * n.x * n.x * a, sign * bb, -sign * n.x};
+  b = {bb, sign + n.y * n.y * a, -n.y};
+}
+bool ph_sample(ph_mat const& m, v3 ns, v3 wo, float ul, float u1, float u2, v3& wi) {
+  v3 t, b;
+  ph_onb(ns, t, b);
+  float s, c;
+  if (ul < m.p_spec) {  // GGX visible normals (Heitz, JCGT 7(4) 2018)
+    v3 const wl{dot(wo, t), dot(wo, b), dot(wo, ns)};
+    v3 const vh = normalize(v3{m.alpha * wl.x, m.alpha * wl.y, wl.z});
+    float const lensq = vh.x * vh.x + vh.y * vh.y;
+    v3 T1{1.0f, 0.0f, 0.0f};
+    if (lensq > 0.0f) {
+      float const il = 1.0f / std::sqrt(lensq);
+      T1 = v3{-vh.y * il, vh.x * il, 0.0f};
+    }
+    v3 const T2 = cross(vh, T1);
+    float const r = std::sqrt(u1);
+    ph_sincos_turns(u2, s, c);
+    float const t1 = r * c;
+    float const sh = 0.5f * (1.0f + vh.z);
+    float const t2 = (1.0f - sh) * std::sqrt(1.0f - t1 * t1) + sh * (r * s);
+    float const nz = std::sqrt(std::fmax(0.0f, (1.0f - t1 * t1) - t2 * t2));
+    v3 const nh = (T1 * t1 + T2 * t2) + vh * nz;
+    v3 const ne = normalize(v3{m.alpha * nh.x, m.alpha * nh.y, std::fmax(1e-6f, nh.z)});
+    v3 const h = (t * ne.x + b * ne.y) + ns * ne.z;
+    wi = h * (2.0f * dot(wo, h)) - wo;
+  } else {  // cosine-weighted hemisphere
+    float const r = std::sqrt(u1);
+    ph_sincos_turns(u2, s, c);
+    float const z = std::sqrt(std::fmax(0.0f, 1.0f - u1));
+    wi = (t * (r * c) + b * (r * s)) + ns * z;
+  }
+  return dot(wi, ns) > 0.0f;
+}
+
+// 24 floats per light: corner, eu, ev, emission, normal, area, du, prob, dv, cdf
+struct ph_light {
+  v3 c, eu, ev, e, n;
+  float area;
+  v3 du;
+  float prob;
+  v3 dv;
+  float cdf;
+};
+bool ph_light_hit(ph_light const& L, v3 o, v3 d, float tmax, float& t) {
+  float const den = dot(d, L.n);
+  if (!(std::fabs(den) > 1e-12f)) return false;
+  float const tt = dot(L.c - o, L.n) / den;
+  if (!(tt > 0.0f) || !(tt < tmax)) return false;
+  v3 const p = (o + d * tt) - L.c;
+  float const a = dot(p, L.du), b = dot(p, L.dv);
+  if (!(a >= 0.0f && a <= 1.0f && b >= 0.0f && b <= 1.0f)) return false;
+  t = tt;
+  return true;
+}
+inline float ph_power(float a, float b) {
+  float const a2 = a * a;
+  return a2 / (a2 + b * b);
+}
+
+// one watertight query on the restated reference BVH (canonical closest hit)
+inline void extern_refbvh_query(scene_t const& sc, float const* ray, int any_hit, std::int32_t& prim, float& t,
+    float& u, float& v) {
+  orc_refbvh_query(sc.nodes, sc.bvh_idx, sc.seq.data(), sc.pts4.data(), ray, 1, any_hit, 1, 1, &prim, &t, &u, &v, 1);
+}
+
+struct ph_scene {
+  scene_t* sc;
+  sdf_scene const* sdf;
+  std::vector<ph_light> lights;
+  v3 env;
+};
+
+struct ph_hit {
+  int kind = -1;  // material >= 0, -1 miss, -2 - l light
+  float t = 0;
+  v3 pos{0, 0, 0}, ns{0, 0, 0}, ng{0, 0, 0};
+};
+
+ph_hit ph_closest(ph_scene const& S, v3 o, v3 d, std::uint32_t sdf_state) {
+  scene_t const& sc = *S.sc;
+  float const inf = std::numeric_limits<float>::infinity();
+  float const ray[8] = {o.x, o.y, o.z, 0.f, d.x, d.y, d.z, inf};
+  std::int32_t prim;
+  float t, u, v;
+  extern_refbvh_query(sc, ray, 0, prim, t, u, v);
+  ph_hit h;
+  h.t = prim >= 0 ? t : inf;
+  if (prim >= 0) {
+    float const* P = sc.tris9 + 9 * std::size_t(prim);
+    v3 const p0{P[0], P[1], P[2]}, p1{P[3], P[4], P[5]}, p2{P[6], P[7], P[8]};
+    float const w = (1.f - u) - v;
+    h.pos = (u * p1 + v * p2) + w * p0;
+    h.ng = normalize(cross(p1 - p0, p2 - p0));
+    if (sc.normals9) {
+      float const* N = sc.normals9 + 9 * std::size_t(prim);
+      h.ns = normalize((u * v3{N[3], N[4], N[5]} + v * v3{N[6], N[7], N[8]}) + w * v3{N[0], N[1], N[2]});
+    } else {
+      h.ns = h.ng;
+    }
+    h.kind = sc.tri_material[prim];
+  }
+  if (S.sdf && S.sdf->n_drawables > 0) {
+    rng_t r;
+    r.state = sdf_state;
+    r.prime = 0;
+    for (int k = 0; k < S.sdf->n_drawables; ++k) {
+      sdf_hit const sh = march_sdf(*S.sdf, r, k, o, d, h.t, false);
+      if (sh.hits && sh.t < h.t) {
+        h.t = sh.t;
+        h.pos = sh.position;
+        h.ns = h.ng = sh.normal;
+        h.kind = sh.material;
+      }
+    }
+  }
+  for (std::size_t l = 0; l < S.lights.size(); ++l) {
+    float tl;
+    if (ph_light_hit(S.lights[l], o, d, h.t, tl)) {
+      h.t = tl;
+      h.kind = -2 - int(l);
+    }
+  }
+  return h;
+}
+
+bool ph_occluded(ph_scene const& S, v3 o, v3 d, float tmax, std::uint32_t sdf_state) {
+  float const ray[8] = {o.x, o.y, o.z, 0.f, d.x, d.y, d.z, tmax};
+  std::int32_t prim;
+  float t, u, v;
+  extern_refbvh_query(*S.sc, ray, 1, prim, t, u, v);
+  if (prim >= 0) return true;
+  if (S.sdf && S.sdf->n_drawables > 0) {
+    rng_t r;
+    r.state = sdf_state;
+    r.prime = 0;
+    for (int k = 0; k < S.sdf->n_drawables; ++k)
+      if (march_sdf(*S.sdf, r, k, o, d, tmax, true).hits) return true;
+  }
+  return false;
+}
+
+struct ph_params {
+  int W, H, max_depth, rr_start;
+  std::uint32_t seed, sample;
+  float vp[16];
+  v3 eye;
+};
+
+v3 ph_path(ph_scene const& S, ph_params const& P, std::uint32_t pix) {
+  std::uint32_t const x = pix % std::uint32_t(P.W), y = pix / std::uint32_t(P.W);
+  ph_r4 const rc = ph_rand4(pix, P.sample, P.seed, 0xffffu);
+  float const nx = ((rc.a + float(x)) / float(P.W)) * 2.f - 1.f;
+  float const ny = ((rc.b + float(y)) / float(P.H)) * 2.f - 1.f;
+  float h[3];
+  for (int k = 0; k < 3; ++k) h[k] = ((P.vp[0 * 4 + k] * nx + P.vp[1 * 4 + k] * ny) + P.vp[2 * 4 + k]) + P.vp[3 * 4 + k];
+  v3 o = P.eye, d = normalize(v3{h[0], h[1], h[2]});
+  v3 T{1.f, 1.f, 1.f}, L{0.f, 0.f, 0.f};
+  float prev_pdf = 0.f;
+  scene_t const& sc = *S.sc;
+  for (int v = 0;; ++v) {
+    std::uint32_t const sdf_state = ph_pcg4d(pix, P.sample, P.seed, 4u * std::uint32_t(v) + 2u).x;
+    ph_hit const hit = ph_closest(S, o, d, sdf_state);
+    if (hit.kind == -1) {
+      L = L + T * S.env;
+      break;
+    }
+    if (hit.kind <= -2) {
+      ph_light const& lt = S.lights[std::size_t(-2 - hit.kind)];
+      float const cl = -dot(d, lt.n);
+      if (cl > 0.f) {
+        float w = 1.f;
+        if (v > 0 && prev_pdf > 0.f) w = ph_power(prev_pdf, (lt.prob * (hit.t * hit.t)) / (lt.area * cl));
+        L = L + (T * lt.e) * w;
+      }
+      break;
+    }
+    if (v >= P.max_depth) break;
+    if (std::size_t(hit.kind) >= sc.n_mats || sc.mat_refs[2 * hit.kind] != 0) break;
+    ph_mat const m = ph_load(sc.mat_data, sc.mat_refs[2 * hit.kind + 1]);
+    v3 ns = hit.ns, ng = hit.ng;
+    v3 const wo = -d;
+    float const gdo = dot(ng, wo);
+    if (gdo < 0.f) ng = -ng;
+    if (dot(ns, ng) < 0.f) ns = -ns;
+    if (!(dot(ns, wo) > 0.f)) ns = ng;
+    if (gdo == 0.f) break;
+    ph_r4 const r0 = ph_rand4(pix, P.sample, P.seed, 4u * std::uint32_t(v));
+    ph_r4 const r1 = ph_rand4(pix, P.sample, P.seed, 4u * std::uint32_t(v) + 1u);
+    v3 const org = hit.pos + ng * 1e-4f;
+    if (!S.lights.empty()) {
+      std::size_t l = 0;
+      while (l + 1 < S.lights.size() && r1.a >= S.lights[l].cdf) ++l;
+      ph_light const& lt = S.lights[l];
+      v3 const yy = (lt.c + lt.eu * r1.b) + lt.ev * r1.c;
+      v3 const dv = yy - hit.pos;
+      float const dist2 = dot(dv, dv);
+      float const dist = std::sqrt(dist2);
+      v3 const wi = dv * (1.f / dist);
+      float const cl = -dot(wi, lt.n);
+      if (cl > 0.f && dist > 0.f) {
+        ph_eval const bv = ph_bsdf(m, ns, ng, wo, wi);
+        if (bv.pdf > 0.f) {
+          float const pl = (lt.prob * dist2) / (lt.area * cl);
+          float const w = ph_power(pl, bv.pdf);
+          v3 const c = ((T * bv.f) * lt.e) * ((bv.cos_i * w) / pl);
+          if (ph_max3(c) > 0.f && !ph_occluded(S, org, wi, dist * 0.999f, sdf_state)) L = L + c;
+        }
+      }
+    }
+    v3 wi;
+    if (!ph_sample(m, ns, wo, r0.a, r0.b, r0.c, wi)) break;
+    ph_eval const bv = ph_bsdf(m, ns, ng, wo, wi);
+    if (!(bv.pdf > 0.f && bv.cos_i > 0.f)) break;
+    v3 Tn = T * (bv.f * (bv.cos_i / bv.pdf));
+    if (!(ph_finite(Tn) && ph_max3(Tn) > 0.f)) break;
+    if (v >= P.rr_start) {
+      float const q = std::fmin(ph_max3(Tn), 0.95f);
+      if (r0.d >= q) break;
+      Tn = Tn / q;
+    }
+    o = org;
+    d = wi;
+    prev_pdf = bv.pdf;
+    T = Tn;
+  }
+  return L;
+}
+
+}  // namespace
+
+extern "C" {
+// Physical-mode render of samples [sample0, sample0 + spp) into accum (W*H*4;
+// float, or double when fp64). lights: 24 floats each (ph_light layout,
+// precomputed by the caller). sdf_*: as orc_render_reference (n = 0: none).
+void orc_render_physical(std::size_t n_tris, float const* tris9, float const* normals9, std::int32_t const* tri_material,
+    std::int32_t const* mat_refs, std::size_t n_mats, float const* mat_data, void const* nodes,
+    std::uint32_t const* bvh_idx, float const* lights24, int n_lights, float const* env, int W, int H, int spp,
+    std::uint32_t sample0, int max_depth, int rr_start, std::uint32_t seed, float const* vp16, float const* eye,
+    std::int32_t const* sdf_instrs, std::int32_t const* sdf_programs, float const* sdf_params,
+    float const* sdf_drawables, int n_sdf_drawables, int sdf_steps, float sdf_eps, int fp64, void* accum,
+    int nthreads) {
+  sdf_scene sdf;
+  sdf.instrs = sdf_instrs;
+  sdf.programs = sdf_programs;
+  sdf.params = sdf_params;
+  sdf.drawables = sdf_drawables;
+  sdf.n_drawables = n_sdf_drawables;
+  sdf.steps = sdf_steps;
+  sdf.eps = sdf_eps;
+  scene_t sc{n_tris, tris9, normals9, nullptr, tri_material, mat_refs, n_mats, mat_data, nodes, bvh_idx, {}, {}};
+  sc.seq.resize(3 * n_tris);
+  for (std::size_t i = 0; i < sc.seq.size(); ++i) sc.seq[i] = std::uint32_t(i);
+  sc.pts4.resize(4 * 3 * n_tris);
+  for (std::size_t i = 0; i < 3 * n_tris; ++i)
+    for (int k = 0; k < 3; ++k) sc.pts4[4 * i + k] = tris9[3 * i + k];
+  ph_scene S{&sc, &sdf, {}, {env[0], env[1], env[2]}};
+  for (int l = 0; l < n_lights; ++l) {
+    float const* q = lights24 + 24 * l;
+    S.lights.push_back({{q[0], q[1], q[2]}, {q[3], q[4], q[5]}, {q[6], q[7], q[8]}, {q[9], q[10], q[11]},
+        {q[12], q[13], q[14]}, q[15], {q[16], q[17], q[18]}, q[19], {q[20], q[21], q[22]}, q[23]});
+  }
+  std::size_t const WH = std::size_t(W) * H;
+  par(WH, nthreads, [&](std::size_t b, std::size_t e) {
+    for (std::size_t pix = b; pix < e; ++pix) {
+      for (int s = 0; s < spp; ++s) {
+        ph_params P{W, H, max_depth, rr_start, seed, sample0 + std::uint32_t(s), {}, eye ? v3{eye[0], eye[1], eye[2]}
+                                                                                      : v3{0, 0, 0}};
+        std::memcpy(P.vp, vp16, sizeof(P.vp));
+        v3 const L = ph_path(S, P, std::uint32_t(pix));
+        bool const ok = ph_finite(L);
+        if (fp64) {
+          double* a = static_cast<double*>(accum) + 4 * pix;
+          if (ok) {
+            a[0] = a[0] + double(L.x);
+            a[1] = a[1] + double(L.y);
+            a[2] = a[2] + double(L.z);
+          }
+          a[3] = a[3] + 1.0;
+        } else {
+          float* a = static_cast<float*>(accum) + 4 * pix;
+          if (ok) {
+            a[0] = a[0] + L.x;
+            a[1] = a[1] + L.y;
+            a[2] = a[2] + L.z;
+          }
+          a[3] = a[3] + 1.f;
+        }
+      }
+    }
+  });
+}
 }  // extern "C"

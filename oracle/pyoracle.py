@@ -52,6 +52,9 @@ def oracle() -> C.CDLL:
             "orc_material_eval": (None, [P, I, C.c_float, P, P, P, P, P]),
             "orc_sdf_map": (None, [P, P, P, I, P, SZ, I, P, P, P]),
             "orc_sdf_trace": (None, [P, P, P, P, I, P, SZ, I, C.c_float, I, P, P, P, P, P, P, I]),
+            "orc_render_physical": (None, [SZ, P, P, P, P, SZ, P, P, P, P, I, P, I, I, I, C.c_uint32, I, I,
+                                           C.c_uint32, P, P, P, P, P, P, I, I, C.c_float, I, P, I]),
+            "orc_refbvh_query": (None, [P, P, P, P, P, SZ, I, I, I, P, P, P, P, I]),
         }
         for k, (r, a) in sig.items():
             f = getattr(h, k)
@@ -347,3 +350,90 @@ def sdf_trace(lib, drawables, rays, steps, eps, any_hit=False, rng_states=None, 
     else:
         oracle().orc_sdf_trace(*args, nthreads())
     return dict(hit=hit, t=t, normal=nn, uv=uv, material=mat)
+
+
+# ---- physical mode --------------------------------------------------------------
+def physical_lights(lights) -> np.ndarray:
+    """24 floats per light (corner, edge_u, edge_v, emission, normal, area, du,
+    prob, dv, cdf), computed in double and rounded like the device upload.
+    lights: [n, 12] float32 (corner, edge_u, edge_v, emission)."""
+    L = np.asarray(lights, np.float32).reshape(-1, 12).astype(np.float64)
+    out = np.zeros((L.shape[0], 24), np.float32)
+    power = []
+    for i, q in enumerate(L):
+        u, w = q[3:6], q[6:9]
+
+        def cross(x, y):
+            return np.array([x[1] * y[2] - x[2] * y[1], x[2] * y[0] - x[0] * y[2], x[0] * y[1] - x[1] * y[0]])
+
+        c = cross(u, w)
+        area = np.sqrt((c[0] * c[0] + c[1] * c[1]) + c[2] * c[2])
+        nn = c / area
+        a1, b1 = cross(w, nn), cross(nn, u)
+        sa = (a1[0] * u[0] + a1[1] * u[1]) + a1[2] * u[2]
+        sb = (b1[0] * w[0] + b1[1] * w[1]) + b1[2] * w[2]
+        out[i, 0:12] = q[0:12]
+        out[i, 12:15] = nn
+        out[i, 15] = area
+        out[i, 16:19] = a1 / sa
+        out[i, 20:23] = b1 / sb
+        e = q[9:12]
+        power.append(((0.2126 * e[0] + 0.7152 * e[1]) + 0.0722 * e[2]) * area)
+    total = 0.0
+    for pw in power:
+        total = total + pw
+    run = 0.0
+    for i, pw in enumerate(power):
+        p = pw / total if total > 0 else 1.0 / len(power)
+        run = run + p
+        out[i, 19] = p
+        out[i, 23] = 1.0 if i + 1 == len(power) else run
+    return out
+
+
+def mat_mul4(a, b) -> np.ndarray:
+    """Column-major 4x4 product in float32 with the device's summation order."""
+    a = np.asarray(a, np.float32).ravel()
+    b = np.asarray(b, np.float32).ravel()
+    out = np.zeros(16, np.float32)
+    for c in range(4):
+        for r in range(4):
+            out[c * 4 + r] = ((a[0 * 4 + r] * b[c * 4 + 0] + a[1 * 4 + r] * b[c * 4 + 1]) + a[2 * 4 + r] * b[c * 4 + 2]) \
+                + a[3 * 4 + r] * b[c * 4 + 3]
+    return out
+
+
+def render_physical(scene: dict, width: int, height: int, spp: int, inv_view, inv_proj, lights, env=(0, 0, 0),
+                    max_depth: int = 8, rr_start: int = 3, seed: int = 0, sample0: int = 0, fp64: bool = False,
+                    accum=None):
+    """Physical-mode render on the CPU, path at a time (the device's method,
+    restated). Returns the accumulation (rgb sum, count), float32 or float64."""
+    L = oracle()
+    tris9 = bake_world_triangles(scene["indices"], scene["vertices"], scene.get("drawables"))
+    nrm, _, mat = bake_world_attributes(scene["indices"], scene.get("normals"), None, scene.get("drawables"),
+                                        len(scene["vertices"]))
+    idx = np.arange(tris9.shape[0] * 3, dtype=np.uint32)
+    nodes, bi = refbvh_build(idx, tris9.reshape(-1, 3))
+    refs = np.ascontiguousarray(scene.get("materials", np.zeros((1, 2), np.int32)), np.int32).reshape(-1, 2)
+    mdata = np.ascontiguousarray(scene.get("material_data", np.zeros(7, np.float32)), np.float32).ravel()
+    lt = physical_lights(lights) if lights is not None and len(lights) else np.zeros((0, 24), np.float32)
+    env = np.ascontiguousarray(env, np.float32)
+    vp = mat_mul4(inv_view, inv_proj)
+    eye = np.ascontiguousarray(np.asarray(inv_view, np.float32).ravel()[12:15])
+    dt = np.float64 if fp64 else np.float32
+    if accum is None:
+        accum = np.zeros((height, width, 4), dt)
+    sdf = scene.get("sdf")
+    if sdf is not None:
+        s_ins, s_prs, s_par = _sdf_arrays(sdf["lib"])
+        s_dr = np.ascontiguousarray(sdf["drawables"], np.float32).reshape(-1, 36)
+        sdf_args = [s_ins.ctypes.data, s_prs.ctypes.data, s_par.ctypes.data, s_dr.ctypes.data, s_dr.shape[0],
+                    int(sdf["steps"]), float(sdf["eps"])]
+    else:
+        sdf_args = [None, None, None, None, 0, 0, 0.0]
+    nrm_p = nrm.ctypes.data if nrm is not None else None
+    L.orc_render_physical(tris9.shape[0], tris9.ctypes.data, nrm_p, mat.ctypes.data, refs.ctypes.data, refs.shape[0],
+                          mdata.ctypes.data, nodes.ctypes.data, bi.ctypes.data, lt.ctypes.data, lt.shape[0],
+                          env.ctypes.data, width, height, spp, sample0, max_depth, rr_start, seed, vp.ctypes.data,
+                          eye.ctypes.data, *sdf_args, int(fp64), accum.ctypes.data, nthreads())
+    return accum
