@@ -345,6 +345,56 @@ typedef struct myrt_render_stats {
 } myrt_render_stats;
 int myrt_get_render_stats(myrt_ctx* ctx, myrt_render_stats* out);
 
+/* ---- learned path guiding (MYRT_SHADE_GUIDED) ----------------------------------
+ * A 4-layer, 64-wide MLP (BF16 weights, FP32 accumulation on the tensor
+ * cores) maps the shading point's frequency-encoded position, shading normal
+ * and view direction to a mixture of 8 von Mises-Fisher lobes. The shade pass
+ * samples it with probability `fraction` (one-sample MIS with the BSDF); after
+ * every wave the network trains on that wave's radiance samples with Adam. No
+ * counterpart in the reference. */
+typedef struct myrt_guide_params {
+  float fraction;         /* probability of sampling the guide (0.5) */
+  float learning_rate;    /* Adam step size (1e-2) */
+  uint32_t train_steps;   /* Adam steps after each wave (16) */
+  uint32_t batch;         /* samples per step, multiple of 128 (16384) */
+  uint32_t train;         /* 0: inference only, the network stays as it is */
+  uint32_t warmup_waves;  /* waves sampled from the BSDF alone while the network learns (1) */
+  uint32_t seed;          /* initialisation seed; a change re-initialises the network */
+  float weight_clamp;     /* training weights are clamped to this multiple of their mean (10; 0: off) */
+  uint32_t target;        /* 0: learn L_i * f * cos (product), 1: learn L_i (incident radiance) */
+  uint32_t reserved;
+} myrt_guide_params;
+int myrt_guide_configure(myrt_ctx* ctx, const myrt_guide_params* params);
+int myrt_guide_get_config(myrt_ctx* ctx, myrt_guide_params* params);
+/* Re-initialises weights and Adam state (a scene upload does this too). */
+int myrt_guide_reset(myrt_ctx* ctx);
+/* FP32 master parameters: weights [4][64 out][64 in], then biases [4][64]
+ * (16640 floats). Setting them also refreshes the BF16 copy. */
+#define MYRT_GUIDE_PARAM_COUNT 16640
+int myrt_guide_get_params(myrt_ctx* ctx, float* params);
+int myrt_guide_set_params(myrt_ctx* ctx, const float* params);
+/* Mixture for n host points (12 floats each: position, 1, shading normal, 0,
+ * view direction, 0), positions normalised by the uploaded scene's bounds.
+ * lobes: 64 floats per point: 8 x (mu xyz, kappa), then 8 x (weight,
+ * kappa / (2 pi (1 - exp(-2 kappa))), cumulative weight, 1 for lobe 0). */
+int myrt_guide_eval(myrt_ctx* ctx, const float* points, uint32_t n, float* lobes);
+/* Gradient of sum_i -w_i log q(d_i | x_i) w.r.t. the parameters for n host
+ * samples (16 floats each: position, w, shading normal, 0, view direction, 0,
+ * d, 0), computed by the training kernel; loss (may be NULL) gets the sum. */
+int myrt_guide_gradients(myrt_ctx* ctx, const float* samples, uint32_t n, float* grads, float* loss);
+/* `steps` Adam steps on host samples (layout as above), batch = min(n, batch). */
+int myrt_guide_train(myrt_ctx* ctx, const float* samples, uint32_t n, uint32_t steps, float* loss_per_step);
+typedef struct myrt_guide_stats {
+  uint64_t adam_steps;
+  uint64_t waves;
+  uint64_t waves_trained;
+  uint32_t last_samples;  /* training samples the last wave produced */
+  float last_loss;        /* loss sum of the last wave's steps */
+  float last_weight_sum;
+  uint32_t pad;
+} myrt_guide_stats;
+int myrt_guide_get_stats(myrt_ctx* ctx, myrt_guide_stats* out);
+
 /* The FP64 accumulation (rgb sum, sample count) of a physical / guided render
  * made with accum_fp64 = 1, W*H*4 doubles. */
 int myrt_read_accumulation_f64(myrt_ctx* ctx, double* rgba_sum);

@@ -244,6 +244,65 @@ class Context:
         self._check(self._L.myrt_get_render_stats(self._h, C.byref(st)), "myrt_get_render_stats")
         return dict(paths=st.paths, extension_rays=st.extension_rays, shadow_rays=st.shadow_rays)
 
+    # ---- learned path guiding ----
+    def guide_configure(self, **kw):
+        """myrt_guide_configure; keys: fraction, learning_rate, train_steps,
+        batch, train, warmup_waves, seed (unset keys keep their values)."""
+        p = _abi.myrt_guide_params()
+        self._check(self._L.myrt_guide_get_config(self._h, C.byref(p)), "myrt_guide_get_config")
+        for k, v in kw.items():
+            if not hasattr(p, k):
+                raise KeyError(k)
+            setattr(p, k, v)
+        self._check(self._L.myrt_guide_configure(self._h, C.byref(p)), "myrt_guide_configure")
+
+    def guide_config(self) -> dict:
+        p = _abi.myrt_guide_params()
+        self._check(self._L.myrt_guide_get_config(self._h, C.byref(p)), "myrt_guide_get_config")
+        return {f: getattr(p, f) for f, _ in _abi.myrt_guide_params._fields_}
+
+    def guide_reset(self):
+        self._check(self._L.myrt_guide_reset(self._h), "myrt_guide_reset")
+
+    def guide_params(self) -> np.ndarray:
+        out = np.empty(_abi.GUIDE_PARAM_COUNT, np.float32)
+        self._check(self._L.myrt_guide_get_params(self._h, out.ctypes.data), "myrt_guide_get_params")
+        return out
+
+    def guide_set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32).ravel()
+        assert p.size == _abi.GUIDE_PARAM_COUNT
+        self._check(self._L.myrt_guide_set_params(self._h, p.ctypes.data), "myrt_guide_set_params")
+
+    def guide_eval(self, points) -> np.ndarray:
+        """points [n, 12] (position, 1, normal, 0, view, 0) -> lobes [n, 64]."""
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 12)
+        out = np.empty((pts.shape[0], 64), np.float32)
+        self._check(self._L.myrt_guide_eval(self._h, pts.ctypes.data, pts.shape[0], out.ctypes.data),
+                    "myrt_guide_eval")
+        return out
+
+    def guide_gradients(self, samples):
+        """samples [n, 16] (position, w, normal, 0, view, 0, direction, 0) -> (grads, loss)."""
+        smp = np.ascontiguousarray(samples, np.float32).reshape(-1, 16)
+        g = np.empty(_abi.GUIDE_PARAM_COUNT, np.float32)
+        loss = C.c_float()
+        self._check(self._L.myrt_guide_gradients(self._h, smp.ctypes.data, smp.shape[0], g.ctypes.data,
+                                                 C.byref(loss)), "myrt_guide_gradients")
+        return g, loss.value
+
+    def guide_train(self, samples, steps: int) -> np.ndarray:
+        smp = np.ascontiguousarray(samples, np.float32).reshape(-1, 16)
+        loss = np.zeros(max(steps, 1), np.float32)
+        self._check(self._L.myrt_guide_train(self._h, smp.ctypes.data, smp.shape[0], steps, loss.ctypes.data),
+                    "myrt_guide_train")
+        return loss[:steps]
+
+    def guide_stats(self) -> dict:
+        st = _abi.myrt_guide_stats()
+        self._check(self._L.myrt_guide_get_stats(self._h, C.byref(st)), "myrt_guide_get_stats")
+        return {f: getattr(st, f) for f, _ in _abi.myrt_guide_stats._fields_ if f != "pad"}
+
     def read_accumulation_f64(self, width: int, height: int):
         acc = np.empty((height, width, 4), np.float64)
         self._check(self._L.myrt_read_accumulation_f64(self._h, acc.ctypes.data), "myrt_read_accumulation_f64")

@@ -70,6 +70,21 @@ class myrt_render_stats(C.Structure):
                 ("reserved", C.c_uint64)]
 
 
+class myrt_guide_params(C.Structure):
+    _fields_ = [("fraction", C.c_float), ("learning_rate", C.c_float), ("train_steps", C.c_uint32),
+                ("batch", C.c_uint32), ("train", C.c_uint32), ("warmup_waves", C.c_uint32), ("seed", C.c_uint32),
+                ("weight_clamp", C.c_float), ("target", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class myrt_guide_stats(C.Structure):
+    _fields_ = [("adam_steps", C.c_uint64), ("waves", C.c_uint64), ("waves_trained", C.c_uint64),
+                ("last_samples", C.c_uint32), ("last_loss", C.c_float), ("last_weight_sum", C.c_float),
+                ("pad", C.c_uint32)]
+
+
+GUIDE_PARAM_COUNT = 16640
+
+
 class myrt_area_light(C.Structure):
     _fields_ = [("corner", C.c_float * 3), ("edge_u", C.c_float * 3), ("edge_v", C.c_float * 3),
                 ("emission", C.c_float * 3)]
@@ -122,6 +137,15 @@ SIGNATURES = {
     "myrt_read_accumulation_f64": (I, [P, P]),
     "myrt_set_area_lights": (I, [P, P, U32]),
     "myrt_get_render_stats": (I, [P, C.POINTER(myrt_render_stats)]),
+    "myrt_guide_configure": (I, [P, C.POINTER(myrt_guide_params)]),
+    "myrt_guide_get_config": (I, [P, C.POINTER(myrt_guide_params)]),
+    "myrt_guide_reset": (I, [P]),
+    "myrt_guide_get_params": (I, [P, P]),
+    "myrt_guide_set_params": (I, [P, P]),
+    "myrt_guide_eval": (I, [P, P, U32, P]),
+    "myrt_guide_gradients": (I, [P, P, U32, P, P]),
+    "myrt_guide_train": (I, [P, P, U32, U32, P]),
+    "myrt_guide_get_stats": (I, [P, C.POINTER(myrt_guide_stats)]),
     "myrt_render_buffers": (I, [P, C.POINTER(P), C.POINTER(P)]),
     "myrt_reset_accumulation": (I, [P]),
     "myrt_sample_count": (I, [P, C.POINTER(C.c_uint32)]),

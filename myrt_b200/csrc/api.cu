@@ -289,6 +289,8 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   cudaFree(ctx->sdf.drawables);
   free_render(ctx->render);
   free_physical(ctx->physical);
+  free_guide(ctx->guide);
+  ctx->guide = nullptr;
   for (auto& p : ctx->stage) cudaFree(p);
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_next);
@@ -397,6 +399,17 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
 
   device_scene& s = ctx->scene;
   s.stats = tree.stats;
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (size_t i = 0; i < pos.size() / 3; ++i)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], pos[3 * i + k]);
+      hi[k] = std::max(hi[k], pos[3 * i + k]);
+    }
+  for (int k = 0; k < 3; ++k) {
+    s.bounds[k] = lo[k];
+    s.bounds[3 + k] = hi[k];
+  }
+  ctx->guide_generation++;  // a new scene invalidates what the guide learned
   s.n_nodes = tree.nodes.size();
   s.n_tris = tree.triangles.size();
   s.n_prims = n_prims;
@@ -600,6 +613,48 @@ int myrt_render(myrt_ctx* ctx, myrt_camera const* camera, myrt_render_params con
 int myrt_set_area_lights(myrt_ctx* ctx, myrt_area_light const* lights, uint32_t n) {
   if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
   return set_area_lights(ctx, lights, n);
+}
+
+int myrt_guide_configure(myrt_ctx* ctx, myrt_guide_params const* p) {
+  if (!ctx || !p) return MYRT_ERR_INVALID_ARGUMENT;
+  return guide_configure(ctx, p);
+}
+int myrt_guide_get_config(myrt_ctx* ctx, myrt_guide_params* p) {
+  if (!ctx || !p) return MYRT_ERR_INVALID_ARGUMENT;
+  return guide_get_config(ctx, p);
+}
+int myrt_guide_reset(myrt_ctx* ctx) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  return guide_reset(ctx);
+}
+int myrt_guide_get_params(myrt_ctx* ctx, float* params) {
+  if (!ctx || !params) return MYRT_ERR_INVALID_ARGUMENT;
+  return guide_params_io(ctx, params, nullptr);
+}
+int myrt_guide_set_params(myrt_ctx* ctx, float const* params) {
+  if (!ctx || !params) return MYRT_ERR_INVALID_ARGUMENT;
+  return guide_params_io(ctx, nullptr, params);
+}
+int myrt_guide_eval(myrt_ctx* ctx, float const* points, uint32_t n, float* lobes) {
+  if (!ctx || (n && (!points || !lobes))) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!ctx->scene.valid) return set_error(ctx, MYRT_ERR_NO_SCENE, "no scene uploaded (positions use its bounds)");
+  return guide_eval(ctx, points, n, lobes);
+}
+int myrt_guide_gradients(myrt_ctx* ctx, float const* samples, uint32_t n, float* grads, float* loss) {
+  if (!ctx || !grads || (n && !samples)) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!ctx->scene.valid) return set_error(ctx, MYRT_ERR_NO_SCENE, "no scene uploaded (positions use its bounds)");
+  if (n > (1u << 24)) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "at most 2^24 samples");
+  return guide_gradients(ctx, samples, n, grads, loss);
+}
+int myrt_guide_train(myrt_ctx* ctx, float const* samples, uint32_t n, uint32_t steps, float* loss_per_step) {
+  if (!ctx || (n && !samples)) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!ctx->scene.valid) return set_error(ctx, MYRT_ERR_NO_SCENE, "no scene uploaded (positions use its bounds)");
+  if (n > (1u << 24) || steps > 65536) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "too many samples or steps");
+  return guide_train_samples(ctx, samples, n, steps, loss_per_step);
+}
+int myrt_guide_get_stats(myrt_ctx* ctx, myrt_guide_stats* out) {
+  if (!ctx || !out) return MYRT_ERR_INVALID_ARGUMENT;
+  return guide_stats(ctx, out);
 }
 
 int myrt_get_render_stats(myrt_ctx* ctx, myrt_render_stats* out) {

@@ -12,6 +12,8 @@
 
 namespace myrt_b200 {
 
+struct guide_state;
+
 // Device-resident scene: BVH, pre-gathered triangles and the shading buffers.
 struct device_scene {
   uint4* nodes = nullptr;      // 5 uint4 per wide node
@@ -25,6 +27,7 @@ struct device_scene {
   float* material_data = nullptr;
   size_t n_nodes = 0, n_tris = 0, n_prims = 0, n_materials = 0, n_material_data = 0;
   bvh8_stats stats{};
+  float bounds[6] = {0, 0, 0, 0, 0, 0};  // world AABB of the triangles (min xyz, max xyz)
   bool valid = false;
 };
 
@@ -82,6 +85,8 @@ struct myrt_ctx {
   myrt_b200::device_sdf sdf;
   myrt_b200::render_state render;
   myrt_b200::physical_state physical;
+  myrt_b200::guide_state* guide = nullptr;  // learned proposal (guide.cu), created on first use
+  uint64_t guide_generation = 0;            // bumped by scene uploads
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
   myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u};
   int sm_count = 0;
@@ -101,6 +106,15 @@ int ensure_images(myrt_ctx* ctx, uint32_t W, uint32_t H);
 int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p);
 int set_area_lights(myrt_ctx* ctx, myrt_area_light const* lights, uint32_t n);
 int get_render_stats(myrt_ctx* ctx, myrt_render_stats* out);
+void free_guide(guide_state* g);
+int guide_configure(myrt_ctx* ctx, myrt_guide_params const* p);
+int guide_reset(myrt_ctx* ctx);
+int guide_params_io(myrt_ctx* ctx, float* out, float const* in);
+int guide_eval(myrt_ctx* ctx, float const* points, uint32_t n, float* lobes);
+int guide_gradients(myrt_ctx* ctx, float const* samples, uint32_t n, float* grads, float* loss);
+int guide_train_samples(myrt_ctx* ctx, float const* samples, uint32_t n, uint32_t steps, float* loss_per_step);
+int guide_stats(myrt_ctx* ctx, myrt_guide_stats* out);
+int guide_get_config(myrt_ctx* ctx, myrt_guide_params* p);
 int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p);
 int trace_sdf_rays(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, int steps, float eps, int any_hit,
     uint32_t const* rng_states, float* out);

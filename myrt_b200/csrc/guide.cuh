@@ -93,6 +93,7 @@ __device__ __forceinline__ float4* guide_record_at(guide_dev const& g, uint32_t 
 
 // Declared in guide.cu (host side).
 int guide_prepare(myrt_ctx* ctx, size_t paths, myrt_render_params const* p, guide_dev& g);
+void guide_begin_wave(myrt_ctx* ctx, guide_dev& g);
 int guide_infer(myrt_ctx* ctx, guide_dev const& g, uint32_t WH, uint32_t sample_base, float4 const* queue,
     float4 const* hits, uint32_t const* count, cudaStream_t st);
 int guide_train(myrt_ctx* ctx, guide_dev const& g, uint32_t paths, int max_depth, float4 const* radiance,

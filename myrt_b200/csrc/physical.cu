@@ -570,15 +570,18 @@ int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_pa
     uint32_t const rows = std::min(rows_per_wave, spp - s0);
     uint32_t const n = uint32_t(rows * WH);
     fr.sample_base = R.sample_counter + s0;
+    if (p->shading == MYRT_SHADE_GUIDED) guide_begin_wave(ctx, gd);
     k_pt_camera<<<grid, kPtBlock, 0, st>>>(fr, n, P.queue[0], P.radiance, P.counts + 0);
     int cur = 0;
     for (int v = 0; v <= fr.max_depth; ++v) {
       bool const last = v == fr.max_depth;
       k_pt_extend<<<grid, kPtBlock, 0, st>>>(sc, fr, v, P.queue[cur], P.counts + cur, P.hits, P.counts + (1 - cur),
           P.counts + 2, P.stats);
+      guide_dev gv = gd;
+      if (last) gv.n_lobes = 0;
       shade_io io{P.queue[cur], P.hits, P.counts + cur, P.queue[1 - cur], P.counts + (1 - cur), P.shadow,
-          P.counts + 2, P.radiance, gd};
-      if (gd.n_lobes > 0 && !last) {
+          P.counts + 2, P.radiance, gv};
+      if (gv.n_lobes > 0) {
         rc = guide_infer(ctx, gd, fr.WH, fr.sample_base, P.queue[cur], P.hits, P.counts + cur, st);
         if (rc) return rc;
       }

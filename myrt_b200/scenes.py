@@ -191,3 +191,80 @@ def icosphere_field_lit(n_spheres: int = 512, subdiv: int = 3, floor_cells: int 
     at y = 1.6 (above every sphere), facing down: (scene, lights[1, 12])."""
     s = icosphere_field(n_spheres=n_spheres, subdiv=subdiv, floor_cells=floor_cells, seed=seed)
     return s, area_light((0.0, 1.6, 0.0), 0.2, 20.0)[None, :]
+
+
+def _grid(nu: int, nv: int, origin, eu, ev, height=None, up=None):
+    """nu x nv quads spanning origin + [0,1] eu + [0,1] ev (2 triangles each,
+    wound so that cross(eu, ev) is the front side), optionally displaced by
+    height[(nv+1), (nu+1)] along `up`. Returns (indices, vertices)."""
+    u = np.linspace(0.0, 1.0, nu + 1)
+    v = np.linspace(0.0, 1.0, nv + 1)
+    uu, vv = np.meshgrid(u, v)
+    pts = (np.asarray(origin, np.float64)[None, None] + uu[..., None] * np.asarray(eu, np.float64) +
+           vv[..., None] * np.asarray(ev, np.float64))
+    if height is not None:
+        pts = pts + height[..., None] * np.asarray(up, np.float64)
+    pts = pts.reshape(-1, 3).astype(np.float32)
+    i = np.arange(nv)[:, None] * (nu + 1) + np.arange(nu)[None, :]
+    a, b, c, d = i, i + 1, i + nu + 2, i + nu + 1
+    idx = np.stack([a, b, c, a, c, d], -1).reshape(-1).astype(np.uint32)
+    return idx, pts
+
+
+def guiding_box(slab_cells: int = 708, wall_cells: int = 8, seed: int = 7, plate: float = 0.5,
+                plate_y: float = 0.75, gap: float = 0.2, light_x: float = 0.0):
+    """Indirect-dominated scene: the closed box [-1,1]^3 (walls facing
+    inwards), two displaced occluder slabs of 2 * slab_cells^2 triangles each
+    (height U[0, 0.05]; default 1,002,528 each) and a 0.05 x 0.05 ceiling light
+    (emission 400) at (light_x, 0.995, 0) hidden behind a plate x plate
+    occluder at y = plate_y (default 0.5 x 0.5 at y = 0.75): the light lands on
+    the plate and the upper walls, the plate throws it onto the ceiling, and
+    the room is lit mostly by that bright ceiling. Slab 1 (y = 0.3) leaves a
+    slot of width `gap` at x = +1, slab 2 (y = -0.3) one at x = -1, so light
+    reaches the middle and bottom levels only through those slots. Returns
+    (scene, lights[1, 12])."""
+    rng = np.random.default_rng(seed)
+    parts = []  # (indices, vertices, material)
+    n = wall_cells
+    walls = [  # origin, eu, ev with cross(eu, ev) pointing into the box
+        ((-1, -1, -1), (2, 0, 0), (0, 0, 2)),   # floor, +y
+        ((-1, 1, -1), (0, 0, 2), (2, 0, 0)),    # ceiling, -y
+        ((-1, -1, -1), (0, 2, 0), (2, 0, 0)),   # back z = -1, +z
+        ((-1, -1, 1), (2, 0, 0), (0, 2, 0)),    # front z = +1, -z
+        ((-1, -1, -1), (0, 0, 2), (0, 2, 0)),   # x = -1, +x
+        ((1, -1, -1), (0, 2, 0), (0, 0, 2)),    # x = +1, -x
+    ]
+    for k, (o, eu, ev) in enumerate(walls):
+        idx, pts = _grid(n, n, o, eu, ev)
+        parts.append((idx, pts, 0 if k != 4 else 1))
+    for (x0, x1, y) in ((-1.0, 1.0 - gap, 0.3), (-1.0 + gap, 1.0, -0.3)):
+        h = rng.uniform(0.0, 0.05, (slab_cells + 1, slab_cells + 1))
+        idx, pts = _grid(slab_cells, slab_cells, (x0, y, -1.0), (0, 0, 2.0), (x1 - x0, 0, 0), h, (0, 1, 0))
+        parts.append((idx, pts, 2))
+    # the occluder plate under the light (a thin double-sided sheet)
+    idx, pts = _grid(1, 1, (light_x - plate / 2, plate_y, -plate / 2), (0, 0, plate), (plate, 0, 0))
+    parts.append((idx, pts, 0))
+    from ._abi import myrt_drawable
+
+    indices, vertices = [], []
+    drawables = (myrt_drawable * len(parts))()
+    eye = np.eye(4, dtype=np.float32).ravel().tolist()
+    ioff = voff = 0
+    for k, (idx, pts, mat) in enumerate(parts):
+        indices.append(idx)
+        vertices.append(pts)
+        d = drawables[k]
+        d.transformation[:] = eye
+        d.inverse_transformation[:] = eye
+        d.indices_base_index, d.points_base_index, d.index_count = ioff, voff, idx.size
+        d.material_index = mat
+        ioff += idx.size
+        voff += pts.shape[0]
+    mat_data = np.concatenate([pbr_material([0.75, 0.75, 0.75], ior=1.5, roughness=0.9),
+                               pbr_material([0.75, 0.3, 0.25], ior=1.5, roughness=0.7),
+                               pbr_material([0.6, 0.65, 0.7], ior=1.5, roughness=0.4)])
+    materials = np.array([[0, 0], [0, 7], [0, 14]], np.int32)
+    scene = dict(indices=np.concatenate(indices), vertices=np.concatenate(vertices), drawables=drawables,
+                 materials=materials, material_data=mat_data)
+    light = area_light((light_x, 0.995, 0.0), 0.05, 400.0)[None, :]
+    return scene, light
