@@ -345,6 +345,55 @@ typedef struct myrt_render_stats {
 } myrt_render_stats;
 int myrt_get_render_stats(myrt_ctx* ctx, myrt_render_stats* out);
 
+/* ---- batches: many views of many scenes in one CUDA graph ---------------------
+ * A batch renders jobs (scene, camera, resolution, spp, seed) of the physical
+ * mode over several scenes at once: waves pack whole sample rows of many jobs,
+ * the whole frame (every wave of every job) is captured once as a CUDA graph
+ * and each myrt_batch_render replays it. A job's image equals, bit for bit,
+ * the same job rendered alone with myrt_render (MYRT_SHADE_PHYSICAL). No
+ * counterpart in the reference (one view per sequential_pathtracer). */
+typedef struct myrt_batch_job {
+  uint32_t scene;          /* index into the batch's scene contexts */
+  uint32_t width, height;
+  uint32_t spp;            /* samples per pixel per myrt_batch_render */
+  uint32_t seed;
+  int32_t max_depth;       /* 0: 8 */
+  int32_t rr_start;
+  uint32_t accum_fp64;
+  float env_radiance[3];
+  int32_t sdf_marching_steps;
+  float sdf_marching_epsilon;
+  uint32_t pad;
+  myrt_camera camera;
+} myrt_batch_job;
+typedef struct myrt_batch_info {
+  uint32_t waves;           /* waves per frame */
+  uint32_t max_wave_paths;  /* largest wave */
+  uint64_t paths_per_frame;
+  uint32_t graph_nodes;     /* nodes of the captured frame graph */
+  uint32_t wave_paths;      /* tuning in force (0: the first scene context's) */
+  uint32_t blocks_per_sm;
+  uint32_t pad;
+} myrt_batch_info;
+typedef struct myrt_batch myrt_batch;
+/* scenes: contexts holding the uploaded scenes (and their lights / SDF
+ * drawables), all on one device; they must outlive the batch, and the batch
+ * renders on scenes[0]'s stream. The batch owns its queues and images. */
+int myrt_batch_create(myrt_ctx* const* scenes, uint32_t n_scenes, const myrt_batch_job* jobs, uint32_t n_jobs,
+    myrt_batch** out);
+/* Wave size (paths in flight) and resident blocks per SM of the grid-stride
+ * kernels; 0 = the first scene context's tuning. Re-captures on next render. */
+int myrt_batch_set_tuning(myrt_batch* batch, uint32_t wave_paths, uint32_t blocks_per_sm);
+/* One graph launch: every job accumulates its spp samples. Asynchronous. */
+int myrt_batch_render(myrt_batch* batch);
+/* Job `job`'s accumulation (rgb sum, count): W*H*4 floats, and for FP64 jobs
+ * W*H*4 doubles (either pointer may be NULL; an FP64 job's float image is
+ * its display image sum / count). */
+int myrt_batch_read(myrt_batch* batch, uint32_t job, float* rgba, double* rgba64);
+int myrt_batch_reset(myrt_batch* batch);
+int myrt_batch_get_info(myrt_batch* batch, myrt_batch_info* info);
+int myrt_batch_destroy(myrt_batch* batch);
+
 /* ---- learned path guiding (MYRT_SHADE_GUIDED) ----------------------------------
  * A 4-layer, 64-wide MLP (BF16 weights, FP32 accumulation on the tensor
  * cores) maps the shading point's frequency-encoded position, shading normal

@@ -340,3 +340,74 @@ class Context:
 
     def set_seed(self, seed: int):
         self._check(self._L.myrt_set_seed(self._h, seed), "myrt_set_seed")
+
+
+class Batch:
+    """myrt_batch: physical-mode jobs over several scene contexts, rendered as
+    one CUDA graph per frame. jobs: dicts with keys scene, width, height, spp,
+    inverse_view, inverse_projection and optionally seed, max_depth, rr_start,
+    fp64, env, sdf_marching_steps, sdf_marching_epsilon. The contexts must
+    outlive the batch."""
+
+    def __init__(self, contexts, jobs):
+        self._L = _abi.lib()
+        self._ctxs = list(contexts)
+        self._jobs = [dict(j) for j in jobs]
+        arr = (_abi.myrt_batch_job * len(jobs))()
+        for k, j in enumerate(jobs):
+            b = arr[k]
+            b.scene, b.width, b.height, b.spp = j["scene"], j["width"], j["height"], j["spp"]
+            b.seed, b.max_depth, b.rr_start = j.get("seed", 0), j.get("max_depth", 8), j.get("rr_start", 3)
+            b.accum_fp64 = int(j.get("fp64", False))
+            b.env_radiance[:] = [float(x) for x in j.get("env", (0.0, 0.0, 0.0))]
+            b.sdf_marching_steps = j.get("sdf_marching_steps", 256)
+            b.sdf_marching_epsilon = j.get("sdf_marching_epsilon", 1e-4)
+            b.camera.inverse_view[:] = np.asarray(j["inverse_view"], np.float32).ravel().tolist()
+            b.camera.inverse_projection[:] = np.asarray(j["inverse_projection"], np.float32).ravel().tolist()
+        handles = (C.c_void_p * len(self._ctxs))(*[c._h.value for c in self._ctxs])
+        self._h = C.c_void_p()
+        rc = self._L.myrt_batch_create(handles, len(self._ctxs), arr, len(jobs), C.byref(self._h))
+        self._ctxs[0]._check(rc, "myrt_batch_create")
+
+    def _check(self, rc, what):
+        self._ctxs[0]._check(rc, what)
+
+    def close(self):
+        if self._h:
+            self._L.myrt_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return self._ctxs[0].stream
+
+    def set_tuning(self, wave_paths: int = 0, blocks_per_sm: int = 0):
+        self._check(self._L.myrt_batch_set_tuning(self._h, wave_paths, blocks_per_sm), "myrt_batch_set_tuning")
+
+    def render(self):
+        self._check(self._L.myrt_batch_render(self._h), "myrt_batch_render")
+
+    def reset(self):
+        self._check(self._L.myrt_batch_reset(self._h), "myrt_batch_reset")
+
+    def read(self, job: int):
+        """Accumulation (rgb sum, count) float32 [H, W, 4]; FP64 jobs: float64."""
+        j = self._jobs[job]
+        if j.get("fp64", False):
+            out = np.empty((j["height"], j["width"], 4), np.float64)
+            self._check(self._L.myrt_batch_read(self._h, job, None, out.ctypes.data), "myrt_batch_read")
+        else:
+            out = np.empty((j["height"], j["width"], 4), np.float32)
+            self._check(self._L.myrt_batch_read(self._h, job, out.ctypes.data, None), "myrt_batch_read")
+        return out
+
+    def info(self) -> dict:
+        i = _abi.myrt_batch_info()
+        self._check(self._L.myrt_batch_get_info(self._h, C.byref(i)), "myrt_batch_get_info")
+        return {f: getattr(i, f) for f, _ in _abi.myrt_batch_info._fields_ if f != "pad"}

@@ -85,6 +85,19 @@ class myrt_guide_stats(C.Structure):
 GUIDE_PARAM_COUNT = 16640
 
 
+class myrt_batch_job(C.Structure):
+    _fields_ = [("scene", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+                ("seed", C.c_uint32), ("max_depth", C.c_int32), ("rr_start", C.c_int32), ("accum_fp64", C.c_uint32),
+                ("env_radiance", C.c_float * 3), ("sdf_marching_steps", C.c_int32),
+                ("sdf_marching_epsilon", C.c_float), ("pad", C.c_uint32), ("camera", myrt_camera)]
+
+
+class myrt_batch_info(C.Structure):
+    _fields_ = [("waves", C.c_uint32), ("max_wave_paths", C.c_uint32), ("paths_per_frame", C.c_uint64),
+                ("graph_nodes", C.c_uint32), ("wave_paths", C.c_uint32), ("blocks_per_sm", C.c_uint32),
+                ("pad", C.c_uint32)]
+
+
 class myrt_area_light(C.Structure):
     _fields_ = [("corner", C.c_float * 3), ("edge_u", C.c_float * 3), ("edge_v", C.c_float * 3),
                 ("emission", C.c_float * 3)]
@@ -137,6 +150,13 @@ SIGNATURES = {
     "myrt_read_accumulation_f64": (I, [P, P]),
     "myrt_set_area_lights": (I, [P, P, U32]),
     "myrt_get_render_stats": (I, [P, C.POINTER(myrt_render_stats)]),
+    "myrt_batch_create": (I, [P, U32, P, U32, C.POINTER(P)]),
+    "myrt_batch_set_tuning": (I, [P, U32, U32]),
+    "myrt_batch_render": (I, [P]),
+    "myrt_batch_read": (I, [P, U32, P, P]),
+    "myrt_batch_reset": (I, [P]),
+    "myrt_batch_get_info": (I, [P, C.POINTER(myrt_batch_info)]),
+    "myrt_batch_destroy": (I, [P]),
     "myrt_guide_configure": (I, [P, C.POINTER(myrt_guide_params)]),
     "myrt_guide_get_config": (I, [P, C.POINTER(myrt_guide_params)]),
     "myrt_guide_reset": (I, [P]),

@@ -71,6 +71,8 @@ struct physical_state {
   unsigned long long* stats = nullptr;  // paths, extension rays, shadow rays (cumulative)
   void* lights = nullptr;               // ps::area_light[n_lights]
   int n_lights = 0;
+  void* tables = nullptr;               // scene + per-wave job tables of the last call
+  size_t tables_cap = 0;
 };
 
 }  // namespace myrt_b200

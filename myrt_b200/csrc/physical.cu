@@ -1,25 +1,32 @@
-// Physical and guided wavefront path tracing.
+// Physical and guided wavefront path tracing, for one view or a batch of
+// views of many scenes.
 //
-// One call renders `spp` samples per pixel in waves of k full-image sample
-// rows (k * W * H paths). Per wave:
+// Work is organised in waves. A wave holds whole sample rows (all W*H pixels
+// of one sample index) of one or more jobs (job = scene + camera +
+// resolution + spp + seed); the wave's job table gives each job its rows,
+// first sample index and first path slot. Per wave:
 //
 //   k_pt_camera                 camera rays (box-filtered pixel jitter)
 //   for vertex v = 0 .. max_depth:
 //     k_pt_extend               closest hit: 8-wide BVH (watertight), SDF
 //                               drawables (sphere tracing), area lights
-//     [guided: k_guide_features + the MLP forward (guide.cu)]
+//     [guided: k_guide_gather + k_guide_forward (guide.cu)]
 //     k_pt_shade                emission with MIS, NEE toward one light,
 //                               BSDF (or guide) sampling, Russian roulette;
 //                               survivors and shadow rays are appended to
 //                               the next queues with warp-aggregated atomics
 //     k_pt_shadow               any-hit for the NEE rays, adds unoccluded
 //                               contributions
-//   k_pt_resolve                per pixel, the wave's samples in sample order
-//                               into the FP32 or FP64 accumulation
+//   k_pt_resolve (per job)      the job's rows, in sample order, into its
+//                               FP32 or FP64 accumulation
 //
 // Queue order never reaches the result: each path's random numbers are keyed
 // by (pixel, sample, seed) and each path's radiance is summed in event order
-// in its own slot, so the image equals a path-at-a-time render bit for bit.
+// in its own slot; rows reach the accumulation in sample order. A job
+// therefore renders the same image bit for bit alone or inside any batch,
+// with any wave size. A batch's whole frame (all waves) is captured once as
+// a CUDA graph; each replay first copies the per-wave job tables (sample
+// bases, overwrite flags) from pinned host memory.
 // Compiled with -fmad=false (build.py) like the other shading unit.
 #include <cuda_runtime.h>
 
@@ -50,6 +57,7 @@ constexpr float kOffset = 1e-4f;  // ray origin offset along the geometric norma
 constexpr int kMaxLights = 64;
 constexpr float kInf = __builtin_huge_valf();
 
+// One scene: geometry, materials, lights, SDF drawables.
 struct pt_scene {
   uint4 const* nodes;
   float4 const* tris;
@@ -60,21 +68,52 @@ struct pt_scene {
   float const* mat_data;
   ps::area_light const* lights;
   int n_lights;
-  sdfk::sdf_dev sdf;
-  uint32_t* err;
-  float env[3];
+  sdfk::sdf_dev sdf;  // steps / eps come from the job
 };
 
-struct pt_frame {
-  uint32_t W, H, WH;
-  uint32_t sample_base;  // sample index of the wave's first row
+// One job within one wave.
+struct pt_job {
+  uint32_t W, H, WH, scene;
   uint32_t seed;
   int max_depth, rr_start;
-  float vp[16];
+  uint32_t fp64;
+  float vp[16];  // inverse_view * inverse_projection
   float eye[3];
+  float env[3];
+  int sdf_steps;
+  float sdf_eps;
+  uint32_t sample_base;  // sample index of the job's first row in this wave
+  uint32_t rows;         // rows in this wave (0: none)
+  uint32_t path_offset;  // slot of the job's first path in this wave
+  uint32_t overwrite;    // 1: the resolve starts a new accumulation
+  float4* accum;
+  double4* accum64;
+  float4* display;
+};
+
+struct pt_wave {
+  pt_scene const* scenes;
+  pt_job const* jobs;
+  int n_jobs;
+  uint32_t n_paths;
+  uint32_t* err;
 };
 
 __device__ __forceinline__ v3 xyz(float4 a) { return {a.x, a.y, a.z}; }
+
+__device__ __forceinline__ int find_job(pt_wave const& w, uint32_t g) {
+  int j = 0;
+  for (int k = 1; k < w.n_jobs; ++k)
+    if (g >= w.jobs[k].path_offset && w.jobs[k].rows > 0) j = k;
+  return j;
+}
+
+__device__ __forceinline__ sdfk::sdf_dev job_sdf(pt_scene const& s, pt_job const& J) {
+  sdfk::sdf_dev d = s.sdf;
+  d.steps = J.sdf_steps;
+  d.eps = J.sdf_eps;
+  return d;
+}
 
 // Appends one entry per lane with `emit` set; all 32 lanes must call it.
 __device__ __forceinline__ uint32_t warp_append(bool emit, uint32_t* count) {
@@ -87,31 +126,41 @@ __device__ __forceinline__ uint32_t warp_append(bool emit, uint32_t* count) {
 }
 
 // ---- camera ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPtBlock) k_pt_camera(pt_frame f, uint32_t n, float4* __restrict__ q,
+__global__ void __launch_bounds__(kPtBlock) k_pt_camera(pt_wave w, float4* __restrict__ q,
     float4* __restrict__ radiance, uint32_t* __restrict__ count) {
   uint32_t const stride = gridDim.x * blockDim.x;
-  if (blockIdx.x == 0 && threadIdx.x == 0) *count = n;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    uint32_t const pix = i % f.WH, sample = f.sample_base + i / f.WH;
-    uint32_t const x = pix % f.W, y = pix / f.W;
-    ps::rnd4 const r = ps::rand4(pix, sample, f.seed, 0xffffu);
-    float const nx = ((r.a + float(x)) / float(f.W)) * 2.f - 1.f;
-    float const ny = ((r.b + float(y)) / float(f.H)) * 2.f - 1.f;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *count = w.n_paths;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.n_paths; i += stride) {
+    int const j = find_job(w, i);
+    pt_job const& J = w.jobs[j];
+    uint32_t const p = i - J.path_offset;
+    uint32_t const pix = p % J.WH, sample = J.sample_base + p / J.WH;
+    uint32_t const x = pix % J.W, y = pix / J.W;
+    ps::rnd4 const r = ps::rand4(pix, sample, J.seed, 0xffffu);
+    float const nx = ((r.a + float(x)) / float(J.W)) * 2.f - 1.f;
+    float const ny = ((r.b + float(y)) / float(J.H)) * 2.f - 1.f;
     float h[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) h[k] = ((f.vp[0 * 4 + k] * nx + f.vp[1 * 4 + k] * ny) + f.vp[2 * 4 + k]) + f.vp[3 * 4 + k];
+    for (int k = 0; k < 3; ++k) h[k] = ((J.vp[0 * 4 + k] * nx + J.vp[1 * 4 + k] * ny) + J.vp[2 * 4 + k]) + J.vp[3 * 4 + k];
     v3 const d = rs::normalize(v3{h[0], h[1], h[2]});
-    q[3 * size_t(i)] = make_float4(f.eye[0], f.eye[1], f.eye[2], __uint_as_float(i));
+    q[3 * size_t(i)] = make_float4(J.eye[0], J.eye[1], J.eye[2], __uint_as_float(i));
     q[3 * size_t(i) + 1] = make_float4(d.x, d.y, d.z, 0.f);
-    q[3 * size_t(i) + 2] = make_float4(1.f, 1.f, 1.f, 0.f);
+    q[3 * size_t(i) + 2] = make_float4(1.f, 1.f, 1.f, __int_as_float(j));
     radiance[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
 }
 
-__device__ __forceinline__ rs::rng_t sdf_stream(pt_frame const& f, uint32_t path, int v) {
-  uint32_t const pix = path % f.WH, sample = f.sample_base + path / f.WH;
+__device__ __forceinline__ void path_key(pt_job const& J, uint32_t path, uint32_t& pix, uint32_t& sample) {
+  uint32_t const p = path - J.path_offset;
+  pix = p % J.WH;
+  sample = J.sample_base + p / J.WH;
+}
+
+__device__ __forceinline__ rs::rng_t sdf_stream(pt_job const& J, uint32_t path, int v) {
+  uint32_t pix, sample;
+  path_key(J, path, pix, sample);
   rs::rng_t r;
-  r.state = ps::pcg4d(pix, sample, f.seed, 4u * uint32_t(v) + 2u).x;
+  r.state = ps::pcg4d(pix, sample, J.seed, 4u * uint32_t(v) + 2u).x;
   r.prime = 0;
   r.tex = nullptr;
   return r;
@@ -120,7 +169,8 @@ __device__ __forceinline__ rs::rng_t sdf_stream(pt_frame const& f, uint32_t path
 // ---- extend: closest hit over meshes, SDF drawables and lights ---------------------------
 // hits[3i] = (position, kind): kind >= 0 material index, -1 miss, -2 - l light l;
 // hits[3i+1] = (shading normal, t); hits[3i+2] = (geometric normal, 0).
-__global__ void __launch_bounds__(kPtBlock, 8) k_pt_extend(pt_scene s, pt_frame f, int v, float4 const* __restrict__ q,
+template <bool SDF>
+__global__ void __launch_bounds__(kPtBlock, 8) k_pt_extend(pt_wave w, int v, float4 const* __restrict__ q,
     uint32_t const* __restrict__ count, float4* __restrict__ hits, uint32_t* __restrict__ clear_a,
     uint32_t* __restrict__ clear_b, unsigned long long* __restrict__ stats) {
   uint32_t const n = *count;
@@ -133,33 +183,37 @@ __global__ void __launch_bounds__(kPtBlock, 8) k_pt_extend(pt_scene s, pt_frame 
   uint32_t const stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     float4 const q0 = q[3 * size_t(i)], q1 = q[3 * size_t(i) + 1];
+    int const j = __float_as_int(q[3 * size_t(i) + 2].w);
+    pt_job const& J = w.jobs[j];
+    pt_scene const& s = w.scenes[J.scene];
     v3 const o = xyz(q0), d = xyz(q1);
     hit_rec h;
     uint32_t cn = 0, ct = 0;
     bool const hit =
-        traverse<1, false, false>(s.nodes, s.tris, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, 0.f, kInf, h, s.err, cn, ct);
+        traverse<1, false, false>(s.nodes, s.tris, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, 0.f, kInf, h, w.err, cn, ct);
     float t = hit ? h.t : kInf;
     int kind = -1;
     v3 pos{0.f, 0.f, 0.f}, ns{0.f, 0.f, 0.f}, ng{0.f, 0.f, 0.f};
     if (hit) {
       float4 const* tp = s.tris + 3 * size_t(h.leaf);
       v3 const p0 = xyz(__ldg(tp)), p1 = xyz(__ldg(tp + 1)), p2 = xyz(__ldg(tp + 2));
-      float const w = (1.f - h.u) - h.v;
-      pos = (h.u * p1 + h.v * p2) + w * p0;
+      float const wb = (1.f - h.u) - h.v;
+      pos = (h.u * p1 + h.v * p2) + wb * p0;
       ng = rs::normalize(rs::cross(p1 - p0, p2 - p0));
       uint32_t const prim = uint32_t(h.prim);
       if (s.tri_normals) {
         float4 const* np = s.tri_normals + 3 * size_t(prim);
-        ns = rs::normalize((h.u * xyz(__ldg(np + 1)) + h.v * xyz(__ldg(np + 2))) + w * xyz(__ldg(np)));
+        ns = rs::normalize((h.u * xyz(__ldg(np + 1)) + h.v * xyz(__ldg(np + 2))) + wb * xyz(__ldg(np)));
       } else {
         ns = ng;
       }
       kind = __ldg(s.tri_material + prim);
     }
-    if (s.sdf.n_drawables > 0) {
-      rs::rng_t rng = sdf_stream(f, __float_as_uint(q0.w), v);
-      for (int k = 0; k < s.sdf.n_drawables; ++k) {
-        sdfk::sdf_hit const sh = sdfk::march(s.sdf, k, o, d, t, false, &rng);
+    if (SDF && s.sdf.n_drawables > 0) {
+      sdfk::sdf_dev const sd = job_sdf(s, J);
+      rs::rng_t rng = sdf_stream(J, __float_as_uint(q0.w), v);
+      for (int k = 0; k < sd.n_drawables; ++k) {
+        sdfk::sdf_hit const sh = sdfk::march(sd, k, o, d, t, false, &rng);
         if (sh.hits && sh.t < t) {
           t = sh.t;
           pos = sh.position;
@@ -194,7 +248,7 @@ struct shade_io {
   guide_dev guide;  // guide.n_lobes == 0: plain BSDF sampling
 };
 
-__global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_scene s, pt_frame f, int v, shade_io io) {
+__global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_wave w, int v, shade_io io) {
   uint32_t const n = *io.count;
   uint32_t const stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {  // warp-uniform trip count
@@ -206,6 +260,9 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_scene s, pt_frame f, i
       float4 const q0 = io.q[3 * size_t(i)], q1 = io.q[3 * size_t(i) + 1], q2 = io.q[3 * size_t(i) + 2];
       float4 const h0 = io.hits[3 * size_t(i)], h1 = io.hits[3 * size_t(i) + 1], h2 = io.hits[3 * size_t(i) + 2];
       uint32_t const path = __float_as_uint(q0.w);
+      int const j = __float_as_int(q2.w);
+      pt_job const& J = w.jobs[j];
+      pt_scene const& s = w.scenes[J.scene];
       v3 const d = xyz(q1), T = xyz(q2);
       float const prev_pdf = q1.w;
       int const kind = __float_as_int(h0.w);
@@ -214,28 +271,28 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_scene s, pt_frame f, i
       bool touched = false;
       if (io.guide.records && v > 0) guide_record_at(io.guide, path, v - 1)[5] = L0;
       if (kind == -1) {
-        v3 const env{s.env[0], s.env[1], s.env[2]};
+        v3 const env{J.env[0], J.env[1], J.env[2]};
         L = L + T * env;
         touched = true;
       } else if (kind <= -2) {
         ps::area_light const& lt = s.lights[-2 - kind];
         float const cos_l = -rs::dot(d, ps::lv(lt.normal));
         if (cos_l > 0.f) {
-          float w = 1.f;
+          float wm = 1.f;
           if (v > 0 && prev_pdf > 0.f) {
             float const t = h1.w;
             float const pl = (lt.prob * (t * t)) / (lt.area * cos_l);
-            w = ps::power_heuristic(prev_pdf, pl);
+            wm = ps::power_heuristic(prev_pdf, pl);
           }
-          L = L + (T * ps::lv(lt.emission)) * w;
+          L = L + (T * ps::lv(lt.emission)) * wm;
           touched = true;
         }
-      } else if (v < f.max_depth) {
+      } else if (v < J.max_depth) {
         bool ok = kind < s.n_mats;
         int2 mref{0, 0};
         if (ok) mref = __ldg(s.mat_refs + kind);
         if (!ok || mref.x != 0) {
-          atomicOr(s.err, ERR_BAD_MATERIAL);
+          atomicOr(w.err, ERR_BAD_MATERIAL);
           ok = false;
         }
         v3 const pos = xyz(h0);
@@ -247,9 +304,10 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_scene s, pt_frame f, i
         if (!(rs::dot(ns, wo) > 0.f)) ns = ng;
         if (ok && gdo != 0.f) {
           ps::material const m = ps::load_material(s.mat_data, mref.y);
-          uint32_t const pix = path % f.WH, sample = f.sample_base + path / f.WH;
-          ps::rnd4 const r0 = ps::rand4(pix, sample, f.seed, 4u * uint32_t(v));
-          ps::rnd4 const r1 = ps::rand4(pix, sample, f.seed, 4u * uint32_t(v) + 1u);
+          uint32_t pix, sample;
+          path_key(J, path, pix, sample);
+          ps::rnd4 const r0 = ps::rand4(pix, sample, J.seed, 4u * uint32_t(v));
+          ps::rnd4 const r1 = ps::rand4(pix, sample, J.seed, 4u * uint32_t(v) + 1u);
           v3 const org = pos + ng * kOffset;
           guide_lobes gl;
           bool const guided = io.guide.n_lobes > 0 && guide_load(io.guide, i, gl) && io.guide.fraction > 0.f;
@@ -269,13 +327,13 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_scene s, pt_frame f, i
               float const pb = guided ? guide_mix_pdf(io.guide, gl, wi, bv.pdf) : bv.pdf;
               if (bv.pdf > 0.f) {
                 float const pl = (lt.prob * dist2) / (lt.area * cos_l);
-                float const w = ps::power_heuristic(pl, pb);
-                v3 const c = ((T * bv.f) * ps::lv(lt.emission)) * ((bv.cos_i * w) / pl);
+                float const wm = ps::power_heuristic(pl, pb);
+                v3 const c = ((T * bv.f) * ps::lv(lt.emission)) * ((bv.cos_i * wm) / pl);
                 if (ps::max3(c) > 0.f) {
                   emit_shadow = true;
                   sq0 = make_float4(org.x, org.y, org.z, __uint_as_float(path));
                   sq1 = make_float4(wi.x, wi.y, wi.z, dist * 0.999f);
-                  sq2 = make_float4(c.x, c.y, c.z, 0.f);
+                  sq2 = make_float4(c.x, c.y, c.z, __int_as_float(j));
                 }
               }
             }
@@ -284,7 +342,7 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_scene s, pt_frame f, i
           v3 wi;
           bool sampled;
           if (guided && r1.d < io.guide.fraction) {
-            ps::rnd4 const r3 = ps::rand4(pix, sample, f.seed, 4u * uint32_t(v) + 3u);
+            ps::rnd4 const r3 = ps::rand4(pix, sample, J.seed, 4u * uint32_t(v) + 3u);
             sampled = guide_sample(gl, r3.a, r3.b, r3.c, wi) && rs::dot(wi, ng) > 0.f;
           } else {
             sampled = ps::bsdf_sample(m, ns, wo, r0.a, r0.b, r0.c, wi);
@@ -295,7 +353,7 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_scene s, pt_frame f, i
             if (pdf > 0.f && bv.cos_i > 0.f) {
               v3 Tn = T * (bv.f * (bv.cos_i / pdf));
               bool alive = ps::finite3(Tn) && ps::max3(Tn) > 0.f;
-              if (alive && v >= f.rr_start) {
+              if (alive && v >= J.rr_start) {
                 float const qq = fminf(ps::max3(Tn), 0.95f);
                 if (r0.d >= qq) alive = false;
                 else Tn = Tn / qq;
@@ -304,7 +362,7 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_scene s, pt_frame f, i
                 emit_next = true;
                 nq0 = make_float4(org.x, org.y, org.z, __uint_as_float(path));
                 nq1 = make_float4(wi.x, wi.y, wi.z, pdf);
-                nq2 = make_float4(Tn.x, Tn.y, Tn.z, 0.f);
+                nq2 = make_float4(Tn.x, Tn.y, Tn.z, __int_as_float(j));
                 if (io.guide.records) {
                   float4* rec = guide_record_at(io.guide, path, v);
                   rec[0] = make_float4(pos.x, pos.y, pos.z, pdf);
@@ -336,23 +394,26 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_scene s, pt_frame f, i
 }
 
 // ---- shadow ------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kPtBlock, 8) k_pt_shadow(pt_scene s, pt_frame f, int v,
-    float4 const* __restrict__ sq, uint32_t const* __restrict__ count, float4* __restrict__ radiance,
-    unsigned long long* __restrict__ stats) {
+template <bool SDF>
+__global__ void __launch_bounds__(kPtBlock, 8) k_pt_shadow(pt_wave w, int v, float4 const* __restrict__ sq,
+    uint32_t const* __restrict__ count, float4* __restrict__ radiance, unsigned long long* __restrict__ stats) {
   uint32_t const n = *count;
   if (blockIdx.x == 0 && threadIdx.x == 0) stats[2] += n;
   uint32_t const stride = gridDim.x * blockDim.x;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     float4 const s0 = sq[3 * size_t(i)], s1 = sq[3 * size_t(i) + 1], s2 = sq[3 * size_t(i) + 2];
+    pt_job const& J = w.jobs[__float_as_int(s2.w)];
+    pt_scene const& s = w.scenes[J.scene];
     v3 const o = xyz(s0), d = xyz(s1);
     uint32_t const path = __float_as_uint(s0.w);
     hit_rec h;
     uint32_t cn = 0, ct = 0;
-    bool occ = traverse<1, true, false>(s.nodes, s.tris, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, 0.f, s1.w, h, s.err,
+    bool occ = traverse<1, true, false>(s.nodes, s.tris, f3{o.x, o.y, o.z}, f3{d.x, d.y, d.z}, 0.f, s1.w, h, w.err,
         cn, ct);
-    if (!occ && s.sdf.n_drawables > 0) {
-      rs::rng_t rng = sdf_stream(f, path, v);
-      for (int k = 0; !occ && k < s.sdf.n_drawables; ++k) occ = sdfk::march(s.sdf, k, o, d, s1.w, true, &rng).hits;
+    if (SDF && !occ && s.sdf.n_drawables > 0) {
+      sdfk::sdf_dev const sd = job_sdf(s, J);
+      rs::rng_t rng = sdf_stream(J, path, v);
+      for (int k = 0; !occ && k < sd.n_drawables; ++k) occ = sdfk::march(sd, k, o, d, s1.w, true, &rng).hits;
     }
     if (!occ) {
       float4 const L = radiance[path];
@@ -362,40 +423,39 @@ __global__ void __launch_bounds__(kPtBlock, 8) k_pt_shadow(pt_scene s, pt_frame 
 }
 
 // ---- resolve ------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_pt_resolve(uint32_t WH, uint32_t rows, float4 const* __restrict__ radiance,
-    int overwrite, float4* __restrict__ accum, float4* __restrict__ display) {
+__global__ void __launch_bounds__(256) k_pt_resolve(pt_job const* __restrict__ jobs, int j,
+    float4 const* __restrict__ radiance) {
+  pt_job const& J = jobs[j];
   uint32_t const pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix >= WH) return;
-  float4 a = overwrite ? make_float4(0.f, 0.f, 0.f, 0.f) : accum[pix];
-  for (uint32_t j = 0; j < rows; ++j) {
-    float4 const l = radiance[size_t(j) * WH + pix];
-    if (isfinite(l.x) && isfinite(l.y) && isfinite(l.z)) {
-      a.x = a.x + l.x;
-      a.y = a.y + l.y;
-      a.z = a.z + l.z;
+  if (pix >= J.WH || J.rows == 0) return;
+  float4 const* src = radiance + J.path_offset;
+  if (J.fp64) {
+    double4 a = J.overwrite ? make_double4(0., 0., 0., 0.) : J.accum64[pix];
+    for (uint32_t r = 0; r < J.rows; ++r) {
+      float4 const l = src[size_t(r) * J.WH + pix];
+      if (isfinite(l.x) && isfinite(l.y) && isfinite(l.z)) {
+        a.x = a.x + double(l.x);
+        a.y = a.y + double(l.y);
+        a.z = a.z + double(l.z);
+      }
+      a.w = a.w + 1.0;
     }
-    a.w = a.w + 1.f;
-  }
-  accum[pix] = a;
-  display[pix] = make_float4(a.x / a.w, a.y / a.w, a.z / a.w, 1.f);
-}
-
-__global__ void __launch_bounds__(256) k_pt_resolve64(uint32_t WH, uint32_t rows, float4 const* __restrict__ radiance,
-    int overwrite, double4* __restrict__ accum, float4* __restrict__ display) {
-  uint32_t const pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix >= WH) return;
-  double4 a = overwrite ? make_double4(0., 0., 0., 0.) : accum[pix];
-  for (uint32_t j = 0; j < rows; ++j) {
-    float4 const l = radiance[size_t(j) * WH + pix];
-    if (isfinite(l.x) && isfinite(l.y) && isfinite(l.z)) {
-      a.x = a.x + double(l.x);
-      a.y = a.y + double(l.y);
-      a.z = a.z + double(l.z);
+    J.accum64[pix] = a;
+    J.display[pix] = make_float4(float(a.x / a.w), float(a.y / a.w), float(a.z / a.w), 1.f);
+  } else {
+    float4 a = J.overwrite ? make_float4(0.f, 0.f, 0.f, 0.f) : J.accum[pix];
+    for (uint32_t r = 0; r < J.rows; ++r) {
+      float4 const l = src[size_t(r) * J.WH + pix];
+      if (isfinite(l.x) && isfinite(l.y) && isfinite(l.z)) {
+        a.x = a.x + l.x;
+        a.y = a.y + l.y;
+        a.z = a.z + l.z;
+      }
+      a.w = a.w + 1.f;
     }
-    a.w = a.w + 1.0;
+    J.accum[pix] = a;
+    J.display[pix] = make_float4(a.x / a.w, a.y / a.w, a.z / a.w, 1.f);
   }
-  accum[pix] = a;
-  display[pix] = make_float4(float(a.x / a.w), float(a.y / a.w), float(a.z / a.w), 1.f);
 }
 
 void mat_mul4(float const* a, float const* b, float* out) {
@@ -405,8 +465,7 @@ void mat_mul4(float const* a, float const* b, float* out) {
           a[3 * 4 + r] * b[c * 4 + 3];
 }
 
-int ensure_queues(myrt_ctx* ctx, size_t paths) {
-  physical_state& P = ctx->physical;
+int ensure_queues(myrt_ctx* ctx, physical_state& P, size_t paths) {
   if (P.capacity >= paths && P.queue[0]) return MYRT_OK;
   for (void* p : {static_cast<void*>(P.queue[0]), static_cast<void*>(P.queue[1]), static_cast<void*>(P.hits),
            static_cast<void*>(P.shadow), static_cast<void*>(P.radiance), static_cast<void*>(P.counts)})
@@ -433,12 +492,148 @@ int ensure_queues(myrt_ctx* ctx, size_t paths) {
   return MYRT_OK;
 }
 
+pt_scene scene_of(myrt_ctx const* ctx) {
+  device_scene const& S = ctx->scene;
+  physical_state const& P = ctx->physical;
+  return pt_scene{S.nodes, S.tris, S.tri_normals, S.tri_material, reinterpret_cast<int2 const*>(S.materials),
+      int(S.n_materials), S.material_data, static_cast<ps::area_light const*>(P.lights), P.n_lights,
+      sdfk::sdf_dev{ctx->sdf.instrs, ctx->sdf.programs, ctx->sdf.params, ctx->sdf.drawables, ctx->sdf.n_drawables,
+          0, 0.f}};
+}
+
+// A job's static description (camera, resolution, spp, ...); the wave planner
+// fills sample_base / rows / path_offset / overwrite.
+pt_job make_job(uint32_t scene, uint32_t W, uint32_t H, uint32_t seed, int max_depth, int rr_start, uint32_t fp64,
+    myrt_camera const& cam, float const* env, int sdf_steps, float sdf_eps) {
+  pt_job J{};
+  J.W = W;
+  J.H = H;
+  J.WH = W * H;
+  J.scene = scene;
+  J.seed = seed;
+  J.max_depth = max_depth > 0 ? max_depth : 8;
+  J.rr_start = rr_start;
+  J.fp64 = fp64;
+  mat_mul4(cam.inverse_view, cam.inverse_projection, J.vp);
+  J.eye[0] = cam.inverse_view[12];
+  J.eye[1] = cam.inverse_view[13];
+  J.eye[2] = cam.inverse_view[14];
+  for (int k = 0; k < 3; ++k) J.env[k] = env[k];
+  J.sdf_steps = sdf_steps;
+  J.sdf_eps = sdf_eps;
+  return J;
+}
+
+struct wave_plan {
+  std::vector<pt_job> jobs;  // per job: rows / sample offset / path offset of this wave
+  uint32_t n_paths = 0;
+  int max_depth = 0;
+};
+
+// Packs each job's spp rows into waves of at most `target` paths (a job whose
+// single row exceeds the target gets a wave of its own row by row). Rows keep
+// their sample order within every job. sample_base holds the row index
+// relative to the call's first sample.
+std::vector<wave_plan> plan_waves(std::vector<pt_job> const& jobs, std::vector<uint32_t> const& spp, size_t target) {
+  std::vector<wave_plan> out;
+  std::vector<uint32_t> done(jobs.size(), 0);
+  for (;;) {
+    wave_plan w;
+    w.jobs = jobs;
+    size_t used = 0;
+    bool any = false;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+      pt_job& J = w.jobs[j];
+      J.rows = 0;
+      J.path_offset = uint32_t(used);
+      J.sample_base = done[j];
+      uint32_t const left = spp[j] - done[j];
+      if (left == 0) continue;
+      size_t const room = target > used ? (target - used) / J.WH : 0;
+      uint32_t rows = uint32_t(std::min<size_t>(left, room));
+      if (rows == 0 && used == 0) rows = 1;  // one row always fits an empty wave
+      if (rows == 0) continue;
+      J.rows = rows;
+      done[j] += rows;
+      used += size_t(rows) * J.WH;
+      w.max_depth = std::max(w.max_depth, J.max_depth);
+      any = true;
+    }
+    if (!any) break;
+    w.n_paths = uint32_t(used);
+    out.push_back(std::move(w));
+  }
+  return out;
+}
+
+// Launches every wave of a plan. `d_jobs` holds the plan's job tables
+// (plan.size() * n_jobs pt_job, already on the device or copied first in
+// the same stream). gd: guiding (single views only) or null.
+int launch_plan(myrt_ctx* ctx, physical_state& P, cudaStream_t st, pt_scene const* d_scenes, pt_job const* d_jobs,
+    std::vector<wave_plan> const& plan, int n_lights_max, bool any_sdf, guide_dev* gd) {
+  uint32_t const bps = ctx->tuning.pt_blocks_per_sm ? ctx->tuning.pt_blocks_per_sm : 8u;
+  uint32_t const grid = uint32_t(std::max(ctx->sm_count, 1)) * bps;
+  size_t const nj = plan.empty() ? 0 : plan[0].jobs.size();
+  for (size_t wi = 0; wi < plan.size(); ++wi) {
+    wave_plan const& wp = plan[wi];
+    pt_wave w{d_scenes, d_jobs + wi * nj, int(nj), wp.n_paths, ctx->d_err};
+    if (gd) guide_begin_wave(ctx, *gd);
+    k_pt_camera<<<grid, kPtBlock, 0, st>>>(w, P.queue[0], P.radiance, P.counts + 0);
+    int cur = 0;
+    for (int v = 0; v <= wp.max_depth; ++v) {
+      bool const last = v == wp.max_depth;
+      if (any_sdf)
+        k_pt_extend<true><<<grid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
+            P.counts + (1 - cur), P.counts + 2, P.stats);
+      else
+        k_pt_extend<false><<<grid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
+            P.counts + (1 - cur), P.counts + 2, P.stats);
+      guide_dev gv = gd ? *gd : guide_dev{};
+      if (last) gv.n_lobes = 0;
+      if (gv.n_lobes > 0) {
+        int rc = guide_infer(ctx, gv, 0, 0, P.queue[cur], P.hits, P.counts + cur, st);
+        if (rc) return rc;
+      }
+      shade_io io{P.queue[cur], P.hits, P.counts + cur, P.queue[1 - cur], P.counts + (1 - cur), P.shadow,
+          P.counts + 2, P.radiance, gv};
+      k_pt_shade<<<grid, kPtBlock, 0, st>>>(w, v, io);
+      if (!last && n_lights_max > 0) {
+        if (any_sdf) k_pt_shadow<true><<<grid, kPtBlock, 0, st>>>(w, v, P.shadow, P.counts + 2, P.radiance, P.stats);
+        else k_pt_shadow<false><<<grid, kPtBlock, 0, st>>>(w, v, P.shadow, P.counts + 2, P.radiance, P.stats);
+      }
+      cur = 1 - cur;
+    }
+    for (size_t j = 0; j < nj; ++j) {
+      if (wp.jobs[j].rows == 0) continue;
+      uint32_t const rb = (wp.jobs[j].WH + 255) / 256;
+      k_pt_resolve<<<rb, 256, 0, st>>>(d_jobs + wi * nj, int(j), P.radiance);
+    }
+    if (gd && gd->records) {
+      int rc = guide_train(ctx, *gd, wp.n_paths, wp.max_depth, P.radiance, st);
+      if (rc) return rc;
+    }
+    int rc = check_cuda(ctx, cudaGetLastError(), "physical wavefront launch");
+    if (rc) return rc;
+  }
+  return MYRT_OK;
+}
+
+int grow_bytes(myrt_ctx* ctx, void** p, size_t& cap, size_t bytes, char const* what) {
+  if (cap >= bytes && *p) return MYRT_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  cap = 0;
+  int rc = check_cuda(ctx, cudaMalloc(p, bytes), what);
+  if (!rc) cap = bytes;
+  return rc;
+}
+
 }  // namespace
 
 void free_physical(physical_state& P) {
   for (void* p : {static_cast<void*>(P.queue[0]), static_cast<void*>(P.queue[1]), static_cast<void*>(P.hits),
            static_cast<void*>(P.shadow), static_cast<void*>(P.radiance), static_cast<void*>(P.counts), P.lights,
-           static_cast<void*>(P.stats)})
+           static_cast<void*>(P.stats), P.tables})
     cudaFree(p);
   P = physical_state{};
 }
@@ -529,7 +724,6 @@ int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_pa
   if (rc) return rc;
   render_state& R = ctx->render;
   physical_state& P = ctx->physical;
-  device_scene const& S = ctx->scene;
   size_t const WH = size_t(W) * H;
   uint32_t const spp = p->frames;
   if (p->accum_fp64 && !R.accum64) {
@@ -537,74 +731,283 @@ int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_pa
     if (rc) return rc;
   }
   size_t const target = p->wave_paths ? p->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : (4u << 20));
-  uint32_t const rows_per_wave = uint32_t(std::max<size_t>(1, std::min<size_t>(spp, target / WH)));
-  rc = ensure_queues(ctx, size_t(rows_per_wave) * WH);
+  pt_job J = make_job(0, W, H, p->seed, p->max_depth, p->rr_start, p->accum_fp64, *cam, p->env_radiance,
+      p->sdf_marching_steps, p->sdf_marching_epsilon);
+  J.accum = R.accum;
+  J.accum64 = R.accum64;
+  J.display = R.display;
+  std::vector<wave_plan> plan = plan_waves({J}, {spp}, target);
+  size_t max_paths = 0;
+  for (auto& w : plan) {
+    max_paths = std::max<size_t>(max_paths, w.n_paths);
+    pt_job& jj = w.jobs[0];
+    jj.overwrite = (R.sample_counter == 0 && jj.sample_base == 0) ? 1u : 0u;
+    jj.sample_base += R.sample_counter;
+  }
+  rc = ensure_queues(ctx, P, max_paths);
   if (rc) return rc;
   guide_dev gd{};
-  if (p->shading == MYRT_SHADE_GUIDED) {
-    rc = guide_prepare(ctx, size_t(rows_per_wave) * WH, p, gd);
+  bool const guided = p->shading == MYRT_SHADE_GUIDED;
+  if (guided) {
+    rc = guide_prepare(ctx, max_paths, p, gd);
     if (rc) return rc;
   }
-
-  pt_scene sc{S.nodes, S.tris, S.tri_normals, S.tri_material, reinterpret_cast<int2 const*>(S.materials),
-      int(S.n_materials), S.material_data, static_cast<ps::area_light const*>(P.lights), P.n_lights,
-      sdfk::sdf_dev{ctx->sdf.instrs, ctx->sdf.programs, ctx->sdf.params, ctx->sdf.drawables, ctx->sdf.n_drawables,
-          p->sdf_marching_steps, p->sdf_marching_epsilon},
-      ctx->d_err, {p->env_radiance[0], p->env_radiance[1], p->env_radiance[2]}};
-  pt_frame fr{};
-  fr.W = W;
-  fr.H = H;
-  fr.WH = uint32_t(WH);
-  fr.seed = p->seed;
-  fr.max_depth = p->max_depth > 0 ? p->max_depth : 8;
-  fr.rr_start = p->rr_start;
-  mat_mul4(cam->inverse_view, cam->inverse_projection, fr.vp);
-  fr.eye[0] = cam->inverse_view[12];
-  fr.eye[1] = cam->inverse_view[13];
-  fr.eye[2] = cam->inverse_view[14];
-
+  // scene table (1) + job tables (one per wave)
+  pt_scene const sc = scene_of(ctx);
+  size_t const bytes = sizeof(pt_scene) + plan.size() * sizeof(pt_job);
+  rc = grow_bytes(ctx, &P.tables, P.tables_cap, bytes, "wave tables");
+  if (rc) return rc;
+  std::vector<unsigned char> host(bytes);
+  std::memcpy(host.data(), &sc, sizeof(pt_scene));
+  for (size_t i = 0; i < plan.size(); ++i)
+    std::memcpy(host.data() + sizeof(pt_scene) + i * sizeof(pt_job), &plan[i].jobs[0], sizeof(pt_job));
   cudaStream_t const st = ctx->stream;
-  uint32_t const bps = ctx->tuning.pt_blocks_per_sm ? ctx->tuning.pt_blocks_per_sm : 8u;
-  uint32_t const grid = uint32_t(std::max(ctx->sm_count, 1)) * bps;
-  for (uint32_t s0 = 0; s0 < spp; s0 += rows_per_wave) {
-    uint32_t const rows = std::min(rows_per_wave, spp - s0);
-    uint32_t const n = uint32_t(rows * WH);
-    fr.sample_base = R.sample_counter + s0;
-    if (p->shading == MYRT_SHADE_GUIDED) guide_begin_wave(ctx, gd);
-    k_pt_camera<<<grid, kPtBlock, 0, st>>>(fr, n, P.queue[0], P.radiance, P.counts + 0);
-    int cur = 0;
-    for (int v = 0; v <= fr.max_depth; ++v) {
-      bool const last = v == fr.max_depth;
-      k_pt_extend<<<grid, kPtBlock, 0, st>>>(sc, fr, v, P.queue[cur], P.counts + cur, P.hits, P.counts + (1 - cur),
-          P.counts + 2, P.stats);
-      guide_dev gv = gd;
-      if (last) gv.n_lobes = 0;
-      shade_io io{P.queue[cur], P.hits, P.counts + cur, P.queue[1 - cur], P.counts + (1 - cur), P.shadow,
-          P.counts + 2, P.radiance, gv};
-      if (gv.n_lobes > 0) {
-        rc = guide_infer(ctx, gd, fr.WH, fr.sample_base, P.queue[cur], P.hits, P.counts + cur, st);
-        if (rc) return rc;
-      }
-      k_pt_shade<<<grid, kPtBlock, 0, st>>>(sc, fr, v, io);
-      if (!last && P.n_lights > 0)
-        k_pt_shadow<<<grid, kPtBlock, 0, st>>>(sc, fr, v, P.shadow, P.counts + 2, P.radiance, P.stats);
-      cur = 1 - cur;
-    }
-    int const overwrite = (R.sample_counter == 0 && s0 == 0) ? 1 : 0;
-    uint32_t const rb = uint32_t((WH + 255) / 256);
-    if (p->accum_fp64)
-      k_pt_resolve64<<<rb, 256, 0, st>>>(fr.WH, rows, P.radiance, overwrite, R.accum64, R.display);
-    else
-      k_pt_resolve<<<rb, 256, 0, st>>>(fr.WH, rows, P.radiance, overwrite, R.accum, R.display);
-    if (gd.records) {
-      rc = guide_train(ctx, gd, n, fr.max_depth, P.radiance, st);
-      if (rc) return rc;
-    }
-    rc = check_cuda(ctx, cudaGetLastError(), "physical wavefront launch");
-    if (rc) return rc;
-  }
+  rc = check_cuda(ctx, cudaMemcpyAsync(P.tables, host.data(), bytes, cudaMemcpyHostToDevice, st), "wave tables");
+  if (rc) return rc;
+  auto* base = static_cast<unsigned char*>(P.tables);
+  rc = launch_plan(ctx, P, st, reinterpret_cast<pt_scene const*>(base),
+      reinterpret_cast<pt_job const*>(base + sizeof(pt_scene)), plan, P.n_lights, ctx->sdf.n_drawables > 0,
+      guided ? &gd : nullptr);
+  if (rc) return rc;
   R.sample_counter += spp;
   return MYRT_OK;
 }
 
 }  // namespace myrt_b200
+
+// ==== batches: many jobs over many scenes, one CUDA graph per frame ===========================
+using namespace myrt_b200;
+
+struct myrt_batch {
+  myrt_ctx* ctx = nullptr;  // scenes[0]: stream, tuning, error word
+  std::vector<myrt_ctx*> scenes;
+  std::vector<myrt_batch_job> jobs;
+  std::vector<pt_job> base_jobs;  // static job descriptions with image pointers
+  std::vector<wave_plan> plan;
+  physical_state queues;          // the batch's own queues
+  void* d_scenes = nullptr;
+  void* d_jobs = nullptr;
+  size_t d_jobs_cap = 0;
+  pt_job* h_jobs = nullptr;       // pinned: per-wave job tables refreshed by each replay
+  std::vector<void*> images;
+  std::vector<uint32_t> samples;  // accumulated samples per job
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint32_t wave_paths = 0, blocks_per_sm = 0;
+  int n_lights_max = 0;
+  bool any_sdf = false;
+};
+
+namespace {
+
+void drop_graph(myrt_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+// (Re)plans the waves for the current wave size and captures the frame graph.
+int build_graph(myrt_batch* b) {
+  myrt_ctx* ctx = b->ctx;
+  drop_graph(b);
+  size_t const target = b->wave_paths ? b->wave_paths : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : (4u << 20));
+  std::vector<uint32_t> spp;
+  for (auto const& j : b->jobs) spp.push_back(j.spp);
+  b->plan = plan_waves(b->base_jobs, spp, target);
+  size_t max_paths = 0;
+  for (auto const& w : b->plan) max_paths = std::max<size_t>(max_paths, w.n_paths);
+  int rc = ensure_queues(ctx, b->queues, max_paths);
+  if (rc) return rc;
+  size_t const nj = b->jobs.size();
+  size_t const bytes = b->plan.size() * nj * sizeof(pt_job);
+  if (b->d_jobs_cap < bytes) {
+    cudaFree(b->d_jobs);
+    cudaFreeHost(b->h_jobs);
+    b->d_jobs = nullptr;
+    b->h_jobs = nullptr;
+    b->d_jobs_cap = 0;
+    rc = check_cuda(ctx, cudaMalloc(&b->d_jobs, bytes), "batch job tables");
+    if (!rc) rc = check_cuda(ctx, cudaMallocHost(reinterpret_cast<void**>(&b->h_jobs), bytes), "batch job tables");
+    if (rc) return rc;
+    b->d_jobs_cap = bytes;
+  }
+  for (size_t w = 0; w < b->plan.size(); ++w)
+    std::memcpy(b->h_jobs + w * nj, b->plan[w].jobs.data(), nj * sizeof(pt_job));
+  cudaStream_t const st = ctx->stream;
+  rc = check_cuda(ctx, cudaStreamSynchronize(st), "batch graph");
+  if (rc) return rc;
+  myrt_tuning const saved = ctx->tuning;
+  if (b->blocks_per_sm) ctx->tuning.pt_blocks_per_sm = b->blocks_per_sm;
+  rc = check_cuda(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "graph capture");
+  if (!rc) {
+    cudaMemcpyAsync(b->d_jobs, b->h_jobs, bytes, cudaMemcpyHostToDevice, st);
+    int lrc = launch_plan(ctx, b->queues, st, static_cast<pt_scene const*>(b->d_scenes),
+        static_cast<pt_job const*>(b->d_jobs), b->plan, b->n_lights_max, b->any_sdf, nullptr);
+    cudaError_t const e = cudaStreamEndCapture(st, &b->graph);
+    rc = lrc ? lrc : check_cuda(ctx, e, "graph capture");
+  }
+  ctx->tuning = saved;
+  if (!rc) rc = check_cuda(ctx, cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiate");
+  if (rc) drop_graph(b);
+  return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int myrt_batch_create(myrt_ctx* const* scenes, uint32_t n_scenes, myrt_batch_job const* jobs, uint32_t n_jobs,
+    myrt_batch** out) {
+  if (!scenes || !jobs || !out || n_scenes == 0 || n_jobs == 0 || n_jobs > 4096) return MYRT_ERR_INVALID_ARGUMENT;
+  myrt_ctx* ctx = scenes[0];
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  for (uint32_t i = 0; i < n_scenes; ++i) {
+    if (!scenes[i] || scenes[i]->device != ctx->device)
+      return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "batch scenes must be contexts on one device");
+    if (!scenes[i]->scene.valid) return set_error(ctx, MYRT_ERR_NO_SCENE, "a batch scene has no uploaded scene");
+  }
+  for (uint32_t j = 0; j < n_jobs; ++j) {
+    myrt_batch_job const& J = jobs[j];
+    if (J.scene >= n_scenes || J.width == 0 || J.height == 0 || uint64_t(J.width) * J.height > (1u << 26) ||
+        J.spp == 0 || J.spp > 65536 || J.max_depth < 0 || J.max_depth > 64 || J.rr_start < 0 || J.accum_fp64 > 1)
+      return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "batch job out of range");
+  }
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc) return rc;
+  auto* b = new myrt_batch();
+  b->ctx = ctx;
+  b->scenes.assign(scenes, scenes + n_scenes);
+  b->jobs.assign(jobs, jobs + n_jobs);
+  std::vector<pt_scene> sc;
+  for (auto* s : b->scenes) {
+    sc.push_back(scene_of(s));
+    b->n_lights_max = std::max(b->n_lights_max, s->physical.n_lights);
+    b->any_sdf = b->any_sdf || s->sdf.n_drawables > 0;
+  }
+  rc = check_cuda(ctx, cudaMalloc(&b->d_scenes, sc.size() * sizeof(pt_scene)), "batch scene table");
+  if (!rc)
+    rc = check_cuda(ctx, cudaMemcpy(b->d_scenes, sc.data(), sc.size() * sizeof(pt_scene), cudaMemcpyHostToDevice),
+        "batch scene table");
+  for (uint32_t j = 0; !rc && j < n_jobs; ++j) {
+    myrt_batch_job const& bj = jobs[j];
+    size_t const WH = size_t(bj.width) * bj.height;
+    void *acc = nullptr, *disp = nullptr;
+    rc = check_cuda(ctx, cudaMalloc(&acc, WH * (bj.accum_fp64 ? 32 : 16)), "batch images");
+    if (!rc) rc = check_cuda(ctx, cudaMalloc(&disp, WH * 16), "batch images");
+    b->images.push_back(acc);
+    b->images.push_back(disp);
+    if (rc) break;
+    pt_job J = make_job(bj.scene, bj.width, bj.height, bj.seed, bj.max_depth, bj.rr_start, bj.accum_fp64, bj.camera,
+        bj.env_radiance, bj.sdf_marching_steps, bj.sdf_marching_epsilon);
+    if (bj.accum_fp64) J.accum64 = static_cast<double4*>(acc);
+    else J.accum = static_cast<float4*>(acc);
+    J.display = static_cast<float4*>(disp);
+    b->base_jobs.push_back(J);
+  }
+  b->samples.assign(n_jobs, 0);
+  if (rc) {
+    myrt_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return MYRT_OK;
+}
+
+int myrt_batch_set_tuning(myrt_batch* b, uint32_t wave_paths, uint32_t blocks_per_sm) {
+  if (!b) return MYRT_ERR_INVALID_ARGUMENT;
+  if ((wave_paths != 0 && wave_paths < 1024) || blocks_per_sm > 16)
+    return set_error(b->ctx, MYRT_ERR_INVALID_ARGUMENT, "batch tuning out of range");
+  b->wave_paths = wave_paths;
+  b->blocks_per_sm = blocks_per_sm;
+  drop_graph(b);
+  return MYRT_OK;
+}
+
+int myrt_batch_render(myrt_batch* b) {
+  if (!b) return MYRT_ERR_INVALID_ARGUMENT;
+  myrt_ctx* ctx = b->ctx;
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (!rc && !b->exec) rc = build_graph(b);
+  if (rc) return rc;
+  // the previous replay must have consumed the pinned tables before they change
+  rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "batch render");
+  if (rc) return rc;
+  size_t const nj = b->jobs.size();
+  for (size_t w = 0; w < b->plan.size(); ++w)
+    for (size_t j = 0; j < nj; ++j) {
+      pt_job& J = b->h_jobs[w * nj + j];
+      uint32_t const row = b->plan[w].jobs[j].sample_base;  // row index within the frame
+      J.sample_base = b->samples[j] + row;
+      J.overwrite = (b->samples[j] == 0 && row == 0) ? 1u : 0u;
+    }
+  rc = check_cuda(ctx, cudaGraphLaunch(b->exec, ctx->stream), "batch graph launch");
+  if (rc) return rc;
+  for (size_t j = 0; j < nj; ++j) b->samples[j] += b->jobs[j].spp;
+  return MYRT_OK;
+}
+
+int myrt_batch_read(myrt_batch* b, uint32_t job, float* rgba, double* rgba64) {
+  if (!b || job >= b->jobs.size()) return MYRT_ERR_INVALID_ARGUMENT;
+  myrt_ctx* ctx = b->ctx;
+  myrt_batch_job const& bj = b->jobs[job];
+  size_t const WH = size_t(bj.width) * bj.height;
+  if (b->samples[job] == 0) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "nothing rendered yet");
+  int rc = MYRT_OK;
+  if (rgba64) {
+    if (!bj.accum_fp64) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "job has no FP64 accumulation");
+    rc = check_cuda(ctx, cudaMemcpyAsync(rgba64, b->images[2 * job], WH * 32, cudaMemcpyDeviceToHost, ctx->stream),
+        "read");
+  }
+  if (!rc && rgba) {
+    void const* src = bj.accum_fp64 ? b->images[2 * job + 1] : b->images[2 * job];
+    rc = check_cuda(ctx, cudaMemcpyAsync(rgba, src, WH * 16, cudaMemcpyDeviceToHost, ctx->stream), "read");
+  }
+  if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "read");
+  return rc;
+}
+
+int myrt_batch_reset(myrt_batch* b) {
+  if (!b) return MYRT_ERR_INVALID_ARGUMENT;
+  std::fill(b->samples.begin(), b->samples.end(), 0u);
+  return MYRT_OK;
+}
+
+int myrt_batch_get_info(myrt_batch* b, myrt_batch_info* info) {
+  if (!b || !info) return MYRT_ERR_INVALID_ARGUMENT;
+  int rc = MYRT_OK;
+  if (!b->exec) rc = build_graph(b);
+  if (rc) return rc;
+  std::memset(info, 0, sizeof(*info));
+  info->waves = uint32_t(b->plan.size());
+  uint64_t total = 0;
+  uint32_t mx = 0;
+  for (auto const& w : b->plan) {
+    total += w.n_paths;
+    mx = std::max(mx, w.n_paths);
+  }
+  info->paths_per_frame = total;
+  info->max_wave_paths = mx;
+  size_t nodes = 0;
+  if (b->graph) cudaGraphGetNodes(b->graph, nullptr, &nodes);
+  info->graph_nodes = uint32_t(nodes);
+  info->wave_paths = b->wave_paths;
+  info->blocks_per_sm = b->blocks_per_sm;
+  return MYRT_OK;
+}
+
+int myrt_batch_destroy(myrt_batch* b) {
+  if (!b) return MYRT_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  drop_graph(b);
+  free_physical(b->queues);
+  cudaFree(b->d_scenes);
+  cudaFree(b->d_jobs);
+  cudaFreeHost(b->h_jobs);
+  for (void* p : b->images) cudaFree(p);
+  delete b;
+  return MYRT_OK;
+}
+
+}  // extern "C"
