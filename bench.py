@@ -52,6 +52,10 @@ def parse_args():
     p.add_argument("--res", type=int, default=512)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=None)
+    p.add_argument("--workload", choices=["closest", "guiding"], default="closest",
+                   help="closest: closest-hit Mrays/s (with a reduced guided-vs-plain leg); guiding: the full "
+                        "time-to-equal-relRMSE run (1024x1024, FP64 4096-spp oracle)")
+    p.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain leg of the closest workload")
     return p.parse_args()
 
 
@@ -258,6 +262,99 @@ def cpu_reference_rate(scene, rays_np: np.ndarray, target_seconds: float = 10.0)
     return n / dt / 1e6, cores, kind, desc, dt
 
 
+# ---------------------------------------------------------------- guiding --
+GUIDE_CFG = dict(fraction=0.5, train=1, warmup_waves=1, train_steps=16, batch=16384, learning_rate=1e-2,
+                 weight_clamp=10.0, target=0, seed=3)
+GUIDE_SCENE = ("guiding box: closed [-1,1]^3 box, two displaced occluder slabs of 1,002,528 tris (height U[0,0.05]) "
+               "with 0.2-wide slots, 0.05x0.05 ceiling light (emission 400) behind a 0.5x0.5 occluder plate; "
+               "camera (0,0,-0.95) looking +z, 90 deg vfov")
+REL_EPS = 1e-2
+
+
+def rel_rmse(img, ref, eps: float = REL_EPS) -> float:
+    """relRMSE over all pixels and RGB channels: sqrt(mean(((img - ref) / (ref + eps))^2))."""
+    return float(np.sqrt(np.mean(((img - ref) / (ref + eps)) ** 2)))
+
+
+def equal_error_time(series, target):
+    """Time at which a (seconds, error) series, ordered by time, first reaches
+    `target`, interpolated linearly in log(time)-log(error); None if never."""
+    prev = None
+    for t, e in series:
+        if e <= target:
+            if prev is None:
+                return float(t)
+            t0, e0 = prev
+            f = np.log(e0 / target) / np.log(e0 / e)
+            return float(np.exp(np.log(t0) + f * np.log(t / t0)))
+        prev = (t, e)
+    return None
+
+
+def guiding_run(device_index: int, res: int, oracle_spp: int, budget_spp: int, slab_cells: int = 708) -> dict:
+    """Guided vs plain path tracing on the indirect-dominated guiding box, both
+    against an FP64 oracle. Plain: BSDF sampling + NEE with MIS, Russian
+    roulette from vertex 3 (its most efficient setting). Guided: the same
+    with the vMF-mixture guide, trained online from a fresh network in every
+    run (training time included), one-sample MIS (fraction 0.5). Each time is
+    the wall clock of one myrt_render call plus the image read-back."""
+    import myrt_b200 as mb
+    from myrt_b200.camera import look_at
+    from myrt_b200.scenes import guiding_box
+
+    ctx = mb.Context(device_index)
+    scene, lights = guiding_box(slab_cells=slab_cells)
+    info = ctx.upload_scene(**scene)
+    ctx.set_area_lights(lights)
+    iv, ip = look_at((0.0, 0.0, -0.95), (0.0, 0.0, 0.5), vfov_deg=90, aspect=1.0)
+    W = H = res
+
+    def render(spp, seed, guided, rr, fp64=False):
+        ctx.reset_accumulation()
+        ctx.sync()
+        t0 = time.perf_counter()
+        ctx.render_physical(iv, ip, W, H, spp=spp, max_depth=12, rr_start=rr, seed=seed, fp64=fp64, guided=guided)
+        acc = ctx.read_accumulation_f64(W, H) if fp64 else ctx.read_accumulation(W, H)[0]
+        dt = time.perf_counter() - t0
+        return acc[..., :3] / acc[..., 3:4], dt
+
+    lum = np.array([0.2126, 0.7152, 0.0722])
+    # oracle: a trained guide used for inference only, no roulette, FP64 accumulation (unbiased like every
+    # estimator here; guided sampling keeps its noise well below the errors measured against it)
+    ctx.guide_configure(**GUIDE_CFG)
+    ctx.guide_reset()
+    render(256, 77, True, 12)
+    ctx.guide_configure(**{**GUIDE_CFG, "train": 0})
+    ref, t_ref = render(oracle_spp, 999, True, 12, fp64=True)
+    ctx.guide_configure(**GUIDE_CFG)
+    render(4, 5, False, 3)  # warm: buffers at their final sizes
+    img, t_plain = render(budget_spp, 1, False, 3)
+    plain = {"spp": budget_spp, "seconds": t_plain, "rel_rmse": rel_rmse(img, ref),
+             "mse_lum": float(np.mean(((img - ref) @ lum) ** 2)), "rr_start": 3}
+    guided = []
+    for spp in (budget_spp // 8, budget_spp // 4, budget_spp // 2, budget_spp):
+        ctx.guide_reset()
+        img, dt = render(spp, 1, True, 3)
+        guided.append({"spp": spp, "seconds": dt, "rel_rmse": rel_rmse(img, ref),
+                       "mse_lum": float(np.mean(((img - ref) @ lum) ** 2)), "rr_start": 3})
+    t_eq = equal_error_time([(g["seconds"], g["rel_rmse"]) for g in guided], plain["rel_rmse"])
+    t_eq_mse = equal_error_time([(g["seconds"], g["mse_lum"]) for g in guided], plain["mse_lum"])
+    ctx.close()
+    return {
+        "scene": GUIDE_SCENE, "triangles": int(info["triangles"]), "res": res, "max_depth": 12,
+        "oracle": {"spp": oracle_spp, "seconds": round(t_ref, 2),
+                   "method": "guided (trained network, inference only), no roulette, FP64 accumulation"},
+        "plain": plain, "guided": guided,
+        "wave_paths": "default (4 Mi paths) for both; while the guide trains, guided waves grow 1, 2, 4, ... spp "
+                      "up to that size and the guide takes 16 Adam steps after each wave",
+        "guided_seconds_to_plain_rel_rmse": t_eq,
+        "speedup_rel_rmse": (t_plain / t_eq) if t_eq else None,
+        "speedup_mse_lum": (t_plain / t_eq_mse) if t_eq_mse else None,
+        "rel_rmse": f"sqrt(mean(((img - oracle) / (oracle + {REL_EPS}))^2)) over pixels and RGB",
+        "timing": "wall clock of myrt_render + image read-back; guided includes its online training",
+    }
+
+
 # ------------------------------------------------------------------- arms --
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
@@ -429,6 +526,12 @@ def run_ours(args):
         v, cores, kind, sample, dt = cpu_reference_rate(scene, rays_np)
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
                                 "seconds": round(dt, 2)}
+    if rank == 0 and world == 1 and not args.no_guiding:
+        del rays, hits
+        torch.cuda.empty_cache()
+        line["guiding"] = guiding_run(local, res=512, oracle_spp=4096, budget_spp=256)
+        line["guiding"]["note"] = ("reduced guided-vs-plain leg (512x512); the full configuration runs with "
+                                   "--workload guiding")
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -438,10 +541,42 @@ def run_ours(args):
     return 0
 
 
+def run_guiding_workload(args):
+    """Time to equal relRMSE, guided vs plain path tracing, at the full
+    configuration: 1024x1024, depth 12, FP64 4096-spp oracle, plain budget
+    256 spp. Rank 0 only (one GPU); other ranks exit without work."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import torch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    with ClockSampler(local) as clocks:
+        g = guiding_run(local, res=1024, oracle_spp=4096, budget_spp=256)
+    t_eq = g["guided_seconds_to_plain_rel_rmse"]
+    value = g["speedup_rel_rmse"]
+    line = {"metric": "time-to-equal-relRMSE speedup, guided vs plain PT", "value": value, "unit": "x",
+            "n_gpus": 1, "steps": len(g["guided"]) + 1, "warmup": 1,
+            "ms_per_step": (t_eq * 1e3) if t_eq else None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (guide MLP bf16, fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": "learned path guiding, " + GUIDE_SCENE, "res": 1024, "max_depth": 12,
+                       "oracle_spp": 4096, "plain_budget_spp": 256, "triangles": g["triangles"],
+                       "l2": "scene and per-wave path state exceed L2"},
+            "guiding": g,
+            "e2e": {"value": value, "unit": "x", "h2d_bytes_per_step": 128,
+                    "d2h_bytes_per_step": 1024 * 1024 * 16,
+                    "api": "myrt_render + myrt_read_accumulation (times include the image read-back)"},
+            "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "guiding":
+        return run_guiding_workload(args)
     return run_ours(args)
 
 

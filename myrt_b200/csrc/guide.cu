@@ -13,8 +13,10 @@
 //   k_guide_train    forward + backward of 128-sample tiles on tcgen05: the
 //                    data gradient dH = dZ W (W read MN-major) and the weight
 //                    gradient dW += dZ^T H (both operands MN-major), dW kept
-//                    in TMEM across a CTA's tiles
-//   k_guide_adam     Adam on the FP32 master parameters, BF16 copy for the MLP
+//                    in TMEM across a CTA's tiles, then stored as this CTA's
+//                    partial gradient (no global atomics)
+//   k_guide_adam     sum of the CTAs' partial gradients, Adam on the FP32
+//                    master parameters, BF16 copy for the MLP
 //
 // Loss (per sample): -w log q(wi | x); its gradient is the KL-divergence
 // gradient between the normalised target w * q_sample and q (Mueller et al.,
@@ -54,6 +56,8 @@ struct guide_state {
   float* adam_m = nullptr;
   float* adam_v = nullptr;
   float* grads = nullptr;
+  float* partials = nullptr;     // [kMaxParts][kParams] per-CTA gradients of one training launch
+  uint32_t max_parts = 0;
   uint16_t* w_bf16 = nullptr;
   float* sums = nullptr;         // [0] loss sum, [1] weight sum
   uint32_t* counters = nullptr;  // [0] training samples collected
@@ -323,32 +327,47 @@ __global__ void __launch_bounds__(256) k_guide_collect(float4 const* __restrict_
     uint32_t n_paths, int max_depth, float tag, int radiance_only, float4 const* __restrict__ radiance,
     float4* __restrict__ samples, uint32_t capacity, uint32_t* __restrict__ count, float* __restrict__ sums) {
   size_t const total = size_t(n_paths) * size_t(max_depth);
+  uint32_t const lane = threadIdx.x & 31u;
   float wsum = 0.f;
-  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < total; i += size_t(gridDim.x) * blockDim.x) {
-    uint32_t const path = uint32_t(i % n_paths);
-    size_t const v = i / n_paths;
-    float4 const* r = records + (v * stride + path) * kRecordWords;
-    float4 const r2 = r[2];
-    if (r2.w != tag) continue;
-    float4 const r0 = r[0], r1 = r[1], r3 = r[3], r4 = r[4], r5 = r[5];
-    float4 const Lf = radiance[path];
-    float const li_r = r4.x > 0.f ? (Lf.x - r5.x) / r4.x : 0.f;
-    float const li_g = r4.y > 0.f ? (Lf.y - r5.y) / r4.y : 0.f;
-    float const li_b = r4.z > 0.f ? (Lf.z - r5.z) / r4.z : 0.f;
-    float const li = (0.2126f * li_r + 0.7152f * li_g) + 0.0722f * li_b;
-    float const w = (radiance_only ? li : li * r1.w) / r0.w;
-    if (!(w > 0.f) || !isfinite(w)) continue;
-    uint32_t const slot = atomicAdd(count, 1u);
-    if (slot >= capacity) continue;
-    wsum += w;
-    float4* s = samples + size_t(slot) * 4;
-    s[0] = make_float4(r0.x, r0.y, r0.z, w);
-    s[1] = make_float4(r1.x, r1.y, r1.z, 0.f);
-    s[2] = make_float4(r2.x, r2.y, r2.z, 0.f);
-    s[3] = make_float4(r3.x, r3.y, r3.z, 0.f);
+  // warp-uniform trip count; one atomic per warp and iteration reserves the slots
+  for (size_t base = blockIdx.x * size_t(blockDim.x); base < total; base += size_t(gridDim.x) * blockDim.x) {
+    size_t const i = base + threadIdx.x;
+    bool keep = false;
+    float w = 0.f;
+    float4 r0, r1, r2, r3;
+    if (i < total) {
+      uint32_t const path = uint32_t(i % n_paths);
+      size_t const v = i / n_paths;
+      float4 const* r = records + (v * stride + path) * kRecordWords;
+      r2 = r[2];
+      if (r2.w == tag) {
+        r0 = r[0], r1 = r[1], r3 = r[3];
+        float4 const r4 = r[4], r5 = r[5];
+        float4 const Lf = radiance[path];
+        float const li_r = r4.x > 0.f ? (Lf.x - r5.x) / r4.x : 0.f;
+        float const li_g = r4.y > 0.f ? (Lf.y - r5.y) / r4.y : 0.f;
+        float const li_b = r4.z > 0.f ? (Lf.z - r5.z) / r4.z : 0.f;
+        float const li = (0.2126f * li_r + 0.7152f * li_g) + 0.0722f * li_b;
+        w = (radiance_only ? li : li * r1.w) / r0.w;
+        keep = w > 0.f && isfinite(w);
+      }
+    }
+    uint32_t const m = __ballot_sync(0xffffffffu, keep);
+    uint32_t slot0 = 0;
+    if (lane == 0 && m) slot0 = atomicAdd(count, uint32_t(__popc(m)));
+    slot0 = __shfl_sync(0xffffffffu, slot0, 0);
+    uint32_t const slot = slot0 + uint32_t(__popc(m & ((1u << lane) - 1u)));
+    if (keep && slot < capacity) {
+      wsum += w;
+      float4* s = samples + size_t(slot) * 4;
+      s[0] = make_float4(r0.x, r0.y, r0.z, w);
+      s[1] = make_float4(r1.x, r1.y, r1.z, 0.f);
+      s[2] = make_float4(r2.x, r2.y, r2.z, 0.f);
+      s[3] = make_float4(r3.x, r3.y, r3.z, 0.f);
+    }
   }
   for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(0xffffffffu, wsum, o);
-  if ((threadIdx.x & 31) == 0 && wsum > 0.f) atomicAdd(sums + 1, wsum);
+  if (lane == 0 && wsum > 0.f) atomicAdd(sums + 1, wsum);
 }
 
 // ---- k_guide_train -----------------------------------------------------------------------------
@@ -369,7 +388,7 @@ struct train_args {
   uint32_t step;          // which block of the sample buffer this step uses
   float const* sums;      // [1] = weight sum of the collected samples (null: no normalisation)
   float clamp;            // normalised weights above this are clamped (0: off)
-  float* grads;           // kParams, accumulated with atomics
+  float* partials;        // [gridDim.x][kParams]: each CTA stores its gradient sum
   float* loss;            // loss sum (atomic)
 };
 
@@ -561,24 +580,27 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(train_args a) {
     if (tid == 0) atomicOr(a.m.err, ERR_GUIDE_TIMEOUT);
     tc::mbar_wait_bounded(bar, phase ^ 1u, kPollLimit);
   }
-  // flush: weight gradients from TMEM (rows 0..63 live in warps 0 and 1), bias sums
+  // flush: this CTA's partial gradient, every entry written (zeros when it had
+  // no tile): weight rows from TMEM (rows 0..63 live in warps 0 and 1), bias sums
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  if (!failed && tiles_done > 0 && warp < 2) {
+  bool const have = !failed && tiles_done > 0;
+  float* part = a.partials + size_t(blockIdx.x) * kParams;
+  if (warp < 2) {
     uint32_t const out = tid;  // row of dW = output index
     for (int l = 0; l < kLayers; ++l) {
       float g[64];
-      acc_row(tmem, 64u + 64u * uint32_t(l), nullptr, g);
-      float* dst = a.grads + (size_t(l) * 64 + out) * 64;
+      if (have) acc_row(tmem, 64u + 64u * uint32_t(l), nullptr, g);
+      else
 #pragma unroll
-      for (int j = 0; j < 64; ++j)
-        if (g[j] != 0.f) atomicAdd(dst + j, g[j]);
+        for (int j = 0; j < 64; ++j) g[j] = 0.f;
+      float4* dst = reinterpret_cast<float4*>(part + (size_t(l) * 64 + out) * 64);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) dst[j] = make_float4(g[4 * j], g[4 * j + 1], g[4 * j + 2], g[4 * j + 3]);
     }
   }
-  if (!failed && tiles_done > 0)
-    for (uint32_t i = tid; i < kLayers * 64; i += blockDim.x)
-      if (dbias[i] != 0.f) atomicAdd(a.grads + kLayers * 64 * 64 + i, dbias[i]);
+  for (uint32_t i = tid; i < kLayers * 64; i += blockDim.x) part[kLayers * 64 * 64 + i] = have ? dbias[i] : 0.f;
   for (int o = 16; o > 0; o >>= 1) loss_acc += __shfl_xor_sync(0xffffffffu, loss_acc, o);
   if ((tid & 31) == 0 && loss_acc != 0.f && a.loss) atomicAdd(a.loss, loss_acc);
   tc::fence_before_sync();
@@ -589,24 +611,48 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(train_args a) {
   }
 }
 
-// ---- Adam + BF16 copy -----------------------------------------------------------------------
+// ---- gradient reduction, Adam + BF16 copy -------------------------------------------------------
+// A block sums 32 parameters over the n_parts partial gradients: its 8 warps
+// take every 8th part (a warp reads 128 contiguous bytes per part), then warp
+// 0 adds the 8 sums in a fixed order, so the result does not depend on timing.
+constexpr uint32_t kRedParams = 32;
+__device__ __forceinline__ float reduce_parts(float const* __restrict__ parts, uint32_t n_parts, float* red) {
+  uint32_t const lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t const i = blockIdx.x * kRedParams + lane;
+  float acc = 0.f;
+  if (i < uint32_t(kParams))
+    for (uint32_t q = warp; q < n_parts; q += 8u) acc += parts[size_t(q) * kParams + i];
+  red[warp * 32u + lane] = acc;
+  __syncthreads();
+  float gi = 0.f;
+  if (warp == 0)
+#pragma unroll
+    for (int w = 0; w < 8; ++w) gi += red[w * 32 + lane];
+  return gi;
+}
+
+__global__ void __launch_bounds__(256) k_guide_reduce(float const* __restrict__ parts, uint32_t n_parts,
+    float* __restrict__ g) {
+  __shared__ float red[256];
+  float const gi = reduce_parts(parts, n_parts, red);
+  uint32_t const i = blockIdx.x * kRedParams + threadIdx.x;
+  if (threadIdx.x < 32 && i < uint32_t(kParams)) g[i] = gi;
+}
+
 __global__ void __launch_bounds__(256) k_guide_adam(float* __restrict__ p, float* __restrict__ m, float* __restrict__ v,
-    float* __restrict__ g, uint16_t* __restrict__ wbf, float lr, float b1, float b2, float eps, float c1, float c2,
-    uint32_t const* __restrict__ count) {
-  uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= uint32_t(kParams)) return;
-  if (count && *count == 0) {  // nothing collected: no step
-    g[i] = 0.f;
-    return;
-  }
-  float const gi = g[i];
+    float const* __restrict__ parts, uint32_t n_parts, uint16_t* __restrict__ wbf, float lr, float b1, float b2,
+    float eps, float c1, float c2, uint32_t const* __restrict__ count) {
+  __shared__ float red[256];
+  if (count && *count == 0) return;  // nothing collected: no step
+  float const gi = reduce_parts(parts, n_parts, red);
+  uint32_t const i = blockIdx.x * kRedParams + threadIdx.x;
+  if (threadIdx.x >= 32 || i >= uint32_t(kParams)) return;
   float const mi = b1 * m[i] + (1.f - b1) * gi;
   float const vi = b2 * v[i] + (1.f - b2) * gi * gi;
   m[i] = mi;
   v[i] = vi;
   float const pi = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
   p[i] = pi;
-  g[i] = 0.f;
   if (i < uint32_t(kLayers * 64 * 64)) wbf[i] = uint16_t(tc::pack_bf16(pi, 0.f) & 0xffffu);
 }
 
@@ -665,6 +711,8 @@ int ensure_guide(myrt_ctx* ctx) {
     alloc(reinterpret_cast<void**>(&g.adam_m), kParams * 4);
     alloc(reinterpret_cast<void**>(&g.adam_v), kParams * 4);
     alloc(reinterpret_cast<void**>(&g.grads), kParams * 4);
+    g.max_parts = uint32_t(std::max(ctx->sm_count, 1));
+    alloc(reinterpret_cast<void**>(&g.partials), size_t(g.max_parts) * kParams * 4);
     alloc(reinterpret_cast<void**>(&g.w_bf16), kLayers * 4096 * 2);
     alloc(reinterpret_cast<void**>(&g.sums), 4 * 4);
     alloc(reinterpret_cast<void**>(&g.counters), 4 * 4);
@@ -712,19 +760,25 @@ int launch_forward(myrt_ctx* ctx, mlp_args const& a, float4 const* points, uint3
   return check_cuda(ctx, cudaGetLastError(), "guide forward launch");
 }
 
-int launch_train(myrt_ctx* ctx, train_args const& ta, uint32_t max_rows, cudaStream_t st) {
+// Launches one training pass; *parts = CTAs launched (partial gradients written).
+int launch_train(myrt_ctx* ctx, train_args ta, uint32_t max_rows, cudaStream_t st, uint32_t* parts) {
+  guide_state& g = *ctx->guide;
   uint32_t const tiles = (max_rows + 127) / 128;
-  uint32_t const grid = std::max(1u, std::min(tiles, uint32_t(std::max(ctx->sm_count, 1))));
+  uint32_t const grid = std::max(1u, std::min(tiles, g.max_parts));
+  ta.partials = g.partials;
   k_guide_train<<<grid, 128, kTrSmem, st>>>(ta);
+  *parts = grid;
   return check_cuda(ctx, cudaGetLastError(), "guide train launch");
 }
 
-int adam_step(myrt_ctx* ctx, guide_state& g, uint32_t const* count, cudaStream_t st) {
+constexpr uint32_t kRedBlocks = (uint32_t(kParams) + kRedParams - 1) / kRedParams;
+
+int adam_step(myrt_ctx* ctx, guide_state& g, uint32_t parts, uint32_t const* count, cudaStream_t st) {
   g.adam_t++;
   float const b1 = 0.9f, b2 = 0.99f;
   float const c1 = float(1.0 - std::pow(double(b1), double(g.adam_t)));
   float const c2 = float(1.0 - std::pow(double(b2), double(g.adam_t)));
-  k_guide_adam<<<(kParams + 255) / 256, 256, 0, st>>>(g.params, g.adam_m, g.adam_v, g.grads, g.w_bf16,
+  k_guide_adam<<<kRedBlocks, 256, 0, st>>>(g.params, g.adam_m, g.adam_v, g.partials, parts, g.w_bf16,
       g.prm.learning_rate, b1, b2, 1e-8f, c1, c2, count);
   g.steps++;
   return check_cuda(ctx, cudaGetLastError(), "guide adam launch");
@@ -735,7 +789,8 @@ int adam_step(myrt_ctx* ctx, guide_state& g, uint32_t const* count, cudaStream_t
 void free_guide(guide_state* g) {
   if (!g) return;
   for (void* p : {static_cast<void*>(g->params), static_cast<void*>(g->adam_m), static_cast<void*>(g->adam_v),
-           static_cast<void*>(g->grads), static_cast<void*>(g->w_bf16), static_cast<void*>(g->sums),
+           static_cast<void*>(g->grads), static_cast<void*>(g->partials), static_cast<void*>(g->w_bf16),
+           static_cast<void*>(g->sums),
            static_cast<void*>(g->counters), static_cast<void*>(g->points), static_cast<void*>(g->lobes),
            static_cast<void*>(g->records), static_cast<void*>(g->samples)})
     cudaFree(p);
@@ -772,6 +827,14 @@ int guide_prepare(myrt_ctx* ctx, size_t paths, myrt_render_params const* p, guid
   gd.paths = uint32_t(paths);
   gd.lobes = g.lobes;
   gd.records = g.prm.train ? g.records : nullptr;
+  return MYRT_OK;
+}
+
+int guide_schedule(myrt_ctx* ctx, uint64_t* waves_trained, bool* training) {
+  int rc = ensure_guide(ctx);
+  if (rc) return rc;
+  *waves_trained = ctx->guide->waves_trained;
+  *training = ctx->guide->prm.train != 0;
   return MYRT_OK;
 }
 
@@ -817,12 +880,12 @@ int guide_train(myrt_ctx* ctx, guide_dev const& gd, uint32_t paths, int max_dept
   ta.batch = g.prm.batch;
   ta.sums = g.sums;
   ta.clamp = g.prm.weight_clamp;
-  ta.grads = g.grads;
   ta.loss = g.sums;
   for (uint32_t s = 0; !rc && s < g.prm.train_steps; ++s) {
     ta.step = uint32_t(g.steps);
-    rc = launch_train(ctx, ta, g.prm.batch, st);
-    if (!rc) rc = adam_step(ctx, g, g.counters, st);
+    uint32_t parts = 0;
+    rc = launch_train(ctx, ta, g.prm.batch, st, &parts);
+    if (!rc) rc = adam_step(ctx, g, parts, g.counters, st);
   }
   g.waves_trained++;
   return rc;
@@ -911,9 +974,13 @@ int guide_gradients(myrt_ctx* ctx, float const* samples, uint32_t n, float* grad
     ta.batch = n;
     ta.step = 0;
     ta.sums = nullptr;
-    ta.grads = g.grads;
     ta.loss = static_cast<float*>(d_loss);
-    rc = launch_train(ctx, ta, n, st);
+    uint32_t parts = 0;
+    rc = launch_train(ctx, ta, n, st, &parts);
+    if (!rc) {
+      k_guide_reduce<<<kRedBlocks, 256, 0, st>>>(g.partials, parts, g.grads);
+      rc = check_cuda(ctx, cudaGetLastError(), "guide reduce launch");
+    }
   }
   if (!rc) rc = check_cuda(ctx, cudaMemcpyAsync(grads, g.grads, kParams * 4, cudaMemcpyDeviceToHost, st), "read");
   if (!rc && loss) rc = check_cuda(ctx, cudaMemcpyAsync(loss, d_loss, 4, cudaMemcpyDeviceToHost, st), "read");
@@ -946,10 +1013,10 @@ int guide_train_samples(myrt_ctx* ctx, float const* samples, uint32_t n, uint32_
     ta.batch = batch;
     ta.step = s;
     ta.sums = nullptr;
-    ta.grads = g.grads;
     ta.loss = static_cast<float*>(d_loss) + s;
-    rc = launch_train(ctx, ta, batch, st);
-    if (!rc) rc = adam_step(ctx, g, nullptr, st);
+    uint32_t parts = 0;
+    rc = launch_train(ctx, ta, batch, st, &parts);
+    if (!rc) rc = adam_step(ctx, g, parts, nullptr, st);
   }
   if (!rc && loss_per_step && steps)
     rc = check_cuda(ctx, cudaMemcpyAsync(loss_per_step, d_loss, size_t(steps) * 4, cudaMemcpyDeviceToHost, st), "read");

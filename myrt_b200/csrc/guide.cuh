@@ -93,6 +93,9 @@ __device__ __forceinline__ float4* guide_record_at(guide_dev const& g, uint32_t 
 
 // Declared in guide.cu (host side).
 int guide_prepare(myrt_ctx* ctx, size_t paths, myrt_render_params const* p, guide_dev& g);
+// Training state for wave planning: waves trained so far (0 for a new network
+// or a new scene) and whether this render trains.
+int guide_schedule(myrt_ctx* ctx, uint64_t* waves_trained, bool* training);
 void guide_begin_wave(myrt_ctx* ctx, guide_dev& g);
 int guide_infer(myrt_ctx* ctx, guide_dev const& g, uint32_t WH, uint32_t sample_base, float4 const* queue,
     float4 const* hits, uint32_t const* count, cudaStream_t st);

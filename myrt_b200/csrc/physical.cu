@@ -146,7 +146,7 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_camera(pt_wave w, float4* __res
     q[3 * size_t(i)] = make_float4(J.eye[0], J.eye[1], J.eye[2], __uint_as_float(i));
     q[3 * size_t(i) + 1] = make_float4(d.x, d.y, d.z, 0.f);
     q[3 * size_t(i) + 2] = make_float4(1.f, 1.f, 1.f, __int_as_float(j));
-    radiance[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    radiance[i] = make_float4(0.f, 0.f, 0.f, 1.f);  // w: roulette throughput of guided waves
   }
 }
 
@@ -310,7 +310,8 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_wave w, int v, shade_i
           ps::rnd4 const r1 = ps::rand4(pix, sample, J.seed, 4u * uint32_t(v) + 1u);
           v3 const org = pos + ng * kOffset;
           guide_lobes gl;
-          bool const guided = io.guide.n_lobes > 0 && guide_load(io.guide, i, gl) && io.guide.fraction > 0.f;
+          bool const gwave = io.guide.n_lobes > 0;
+          bool const guided = gwave && guide_load(io.guide, i, gl) && io.guide.fraction > 0.f;
           // next-event estimation
           if (s.n_lights > 0) {
             int l = 0;
@@ -353,11 +354,24 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_wave w, int v, shade_i
             if (pdf > 0.f && bv.cos_i > 0.f) {
               v3 Tn = T * (bv.f * (bv.cos_i / pdf));
               bool alive = ps::finite3(Tn) && ps::max3(Tn) > 0.f;
-              if (alive && v >= J.rr_start) {
-                float const qq = fminf(ps::max3(Tn), 0.95f);
-                if (r0.d >= qq) alive = false;
-                else Tn = Tn / qq;
+              // Guided waves: roulette on the throughput the path would carry
+              // under BSDF sampling (radiance.w), not on Tn. A guided direction
+              // has a large pdf exactly where the incident radiance is large,
+              // so a small Tn there does not mean a small contribution.
+              float tb = 0.f;
+              if (gwave) {
+                float const fb = bv.pdf > 0.f ? ps::max3(bv.f * (bv.cos_i / bv.pdf)) : 1.f;
+                tb = L0.w * fb;
               }
+              if (alive && v >= J.rr_start) {
+                float const qq = fminf(gwave ? tb : ps::max3(Tn), 0.95f);
+                if (r0.d >= qq) alive = false;
+                else {
+                  Tn = Tn / qq;
+                  tb = tb / qq;
+                }
+              }
+              if (alive && gwave) io.radiance[path].w = tb;
               if (alive) {
                 emit_next = true;
                 nq0 = make_float4(org.x, org.y, org.z, __uint_as_float(path));
@@ -376,7 +390,7 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_wave w, int v, shade_i
           }
         }
       }
-      if (touched) io.radiance[path] = make_float4(L.x, L.y, L.z, 0.f);
+      if (touched) io.radiance[path] = make_float4(L.x, L.y, L.z, L0.w);
     }
     uint32_t const slot = warp_append(emit_next, io.count_out);
     if (emit_next) {
@@ -417,7 +431,7 @@ __global__ void __launch_bounds__(kPtBlock, 8) k_pt_shadow(pt_wave w, int v, flo
     }
     if (!occ) {
       float4 const L = radiance[path];
-      radiance[path] = make_float4(L.x + s2.x, L.y + s2.y, L.z + s2.z, 0.f);
+      radiance[path] = make_float4(L.x + s2.x, L.y + s2.y, L.z + s2.z, L.w);
     }
   }
 }
@@ -561,6 +575,29 @@ std::vector<wave_plan> plan_waves(std::vector<pt_job> const& jobs, std::vector<u
     }
     if (!any) break;
     w.n_paths = uint32_t(used);
+    out.push_back(std::move(w));
+  }
+  return out;
+}
+
+// Waves of one job whose row counts double from 2^first_wave up to what
+// `target` paths hold: a guide that is still learning trains after small
+// early waves, and later waves run at full size.
+std::vector<wave_plan> plan_waves_growing(pt_job const& J, uint32_t spp, size_t target, uint64_t first_wave) {
+  std::vector<wave_plan> out;
+  uint32_t const cap = uint32_t(std::max<size_t>(1, std::min<size_t>(target / J.WH, 1u << 30)));
+  uint32_t done = 0;
+  for (uint64_t k = first_wave; done < spp; ++k) {
+    uint32_t const grow = k >= 30 ? cap : std::min<uint32_t>(cap, 1u << k);
+    uint32_t const rows = std::min(spp - done, grow);
+    wave_plan w;
+    w.jobs = {J};
+    w.jobs[0].rows = rows;
+    w.jobs[0].path_offset = 0;
+    w.jobs[0].sample_base = done;
+    w.n_paths = rows * J.WH;
+    w.max_depth = J.max_depth;
+    done += rows;
     out.push_back(std::move(w));
   }
   return out;
@@ -736,7 +773,16 @@ int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_pa
   J.accum = R.accum;
   J.accum64 = R.accum64;
   J.display = R.display;
-  std::vector<wave_plan> plan = plan_waves({J}, {spp}, target);
+  bool const guided = p->shading == MYRT_SHADE_GUIDED;
+  std::vector<wave_plan> plan;
+  uint64_t trained = 0;
+  bool training = false;
+  if (guided) {
+    rc = guide_schedule(ctx, &trained, &training);
+    if (rc) return rc;
+  }
+  if (guided && training) plan = plan_waves_growing(J, spp, target, trained);
+  else plan = plan_waves({J}, {spp}, target);
   size_t max_paths = 0;
   for (auto& w : plan) {
     max_paths = std::max<size_t>(max_paths, w.n_paths);
@@ -747,7 +793,6 @@ int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_pa
   rc = ensure_queues(ctx, P, max_paths);
   if (rc) return rc;
   guide_dev gd{};
-  bool const guided = p->shading == MYRT_SHADE_GUIDED;
   if (guided) {
     rc = guide_prepare(ctx, max_paths, p, gd);
     if (rc) return rc;

@@ -213,11 +213,12 @@ def _rel_rmse(img, ref):
 def test_guided_rendering_beats_bsdf_sampling(ctx):
     """The slot box at 128^2 (light reaches the lower levels only through two
     0.2-wide slots): guided rendering with the default settings (fraction 0.5,
-    16 Adam steps after each wave of 16 spp, training weights clamped at 10x
-    their mean) against plain BSDF sampling at the same 1024 spp, both against
-    an FP64 plain render of 16384 spp, two render seeds each. Guided stays
-    unbiased (image means within 3 %) and its relRMSE is lower than plain's
-    (measured: 0.121 against 0.126)."""
+    waves growing 1, 2, 4, 8, 16 spp while the guide trains, 16 Adam steps
+    after each wave, training weights clamped at 10x their mean, roulette on
+    the BSDF-sampling throughput) against plain BSDF sampling at the same 1024
+    spp, both against an FP64 plain render of 16384 spp, two render seeds
+    each. Guided stays unbiased (image means within 3 %) and its relRMSE is
+    well below plain's (measured: 0.058 and 0.059 against 0.128 and 0.130)."""
     _small_box(ctx)
     W = H = 128
     iv, ip = look_at((0.0, 0.0, -0.95), (0.0, 0.0, 0.5), vfov_deg=90, aspect=1.0)
@@ -245,4 +246,4 @@ def test_guided_rendering_beats_bsdf_sampling(ctx):
         e_plain.append(_rel_rmse(plain, ref))
         e_guided.append(_rel_rmse(guided, ref))
     print("relRMSE plain", e_plain, "guided", e_guided)
-    assert np.mean(e_guided) < np.mean(e_plain)
+    assert np.mean(e_guided) < 0.6 * np.mean(e_plain)
