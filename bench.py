@@ -12,10 +12,11 @@ Workload (one step = one closest-hit launch over one ray batch):
 Multi-GPU: one process per GPU, each tracing its own batch (weak scaling, no
 collective on the data path); time = max over ranks of the device time.
 
-Arms: default = this framework (CUDA, sm_100a). `--impl reference` = the
-reference's CPU path (its BVH build + its GLSL traversal and intersector
-compiled as C++, oracle/_ref) on the host cores, on a bounded sample of the
-same rays.
+Arms: default = this framework (CUDA, sm_100a); each step sorts the batch's
+visiting order by origin and direction cell (CUB radix sort of ray indices),
+then traces. `--impl reference` = the reference's CPU path (its BVH build +
+its GLSL traversal and intersector compiled as C++, oracle/_ref) on the host
+cores, on a bounded sample of the same rays.
 """
 from __future__ import annotations
 
@@ -514,12 +515,14 @@ def run_ours(args):
                      "traffic_source": "ncu dram__bytes_read+write per ray of a 3.49M-ray capture, scaled by rays",
                      "bytes_per_ray": alg_bytes / n, "nodes_per_ray": nodes_total / n, "tris_per_ray": tris_total / n,
                      "note": "algorithmic bytes = 80 B/node + 48 B/triangle + 48 B ray+hit; the 37 MB BVH is "
-                             "L2-resident, so most node bytes are served by L2"},
+                             "L2-resident, so most node bytes are served by L2. Duration = the whole step: ray "
+                             "keys + radix sort of the visiting order + traversal (k_trace)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * RAY_BYTES,
                 "d2h_bytes_per_step": n * HIT_BYTES, "steps": e2e_steps,
                 "api": "myrt_trace_closest (host pinned buffers, chunked copy/compute overlap)"},
         "clocks": clocks.summary(),
-        "gpu_launches": args.steps,
+        "gpu_launches": 2 * args.steps,
+        "gpu_launches_note": "per step: k_ray_keys + k_trace (ours) and the CUB radix sort of the visiting order",
         "gpu_launches_e2e": e2e_steps * chunks,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

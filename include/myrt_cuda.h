@@ -149,6 +149,12 @@ typedef struct myrt_tuning {
   uint32_t wave_paths;       /* physical / guided wavefront: paths in flight per wave (0 = 4 Mi) */
   uint32_t pt_blocks_per_sm; /* physical / guided: resident 128-thread blocks per SM of the
                                 grid-stride extend / shade / shadow kernels (0 = 8) */
+  uint32_t trace_smem_stack; /* one-thread-per-ray: 1 = traversal stack in shared memory
+                                (tree depth + 1 entries per ray), 0 = per-thread local memory */
+  uint32_t trace_order;      /* visiting order of closest / any-hit batches: 0 = device-memory queries
+                                of at least 1 Mi rays sorted by origin and direction cell, host-memory
+                                queries in input order; 1 = input order; 2 = always sorted.
+                                Results never depend on it. */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */

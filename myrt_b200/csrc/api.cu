@@ -10,9 +10,12 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "../../include/myrt_cuda.h"
 #include "bvh8.hpp"
 #include "ctx.hpp"
+#include "rayorder.cuh"
 #include "trace.cuh"
 
 namespace myrt_b200 {
@@ -100,8 +103,87 @@ int launch_persistent(myrt_ctx* ctx, trace_args const& a, cudaStream_t s) {
   return MYRT_OK;
 }
 
-int launch_trace(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s) {
+constexpr uint32_t kOrderMin = 1u << 20;  // batches from this size on are sorted (trace_order 0)
+
+void free_order(myrt_ctx::order_scratch& o) {
+  for (int k = 0; k < 2; ++k) {
+    cudaFree(o.keys[k]);
+    cudaFree(o.vals[k]);
+    o.keys[k] = o.vals[k] = nullptr;
+  }
+  cudaFree(o.temp);
+  o.temp = nullptr;
+  o.cap = o.temp_bytes = 0;
+}
+
+// Sorts the batch's ray indices by origin / direction cell (rayorder.cuh) into
+// the lane's scratch and points a.perm at the order. The scratch of a lane is
+// reused by later queries on any stream: each use waits for the previous one.
+int order_rays(myrt_ctx* ctx, trace_args& a, int lane, cudaStream_t s) {
+  auto& o = ctx->order[lane];
+  if (!o.done) {
+    int rc = check_cuda(ctx, cudaEventCreateWithFlags(&o.done, cudaEventDisableTiming), "ray order event");
+    if (rc) return rc;
+  }
+  int rc = check_cuda(ctx, cudaStreamWaitEvent(s, o.done, 0), "ray order wait");
+  if (rc) return rc;
+  size_t need = 0;
+  rc = check_cuda(ctx, cub::DeviceRadixSort::SortPairs(nullptr, need, o.keys[0], o.keys[1], o.vals[0], o.vals[1],
+                           int(a.n), 0, kOrderKeyBits, s), "ray order size");
+  if (rc) return rc;
+  if (o.cap < a.n || o.temp_bytes < need) {
+    rc = check_cuda(ctx, cudaStreamSynchronize(s), "ray order realloc");
+    if (rc) return rc;
+    free_order(o);
+    size_t const cap = std::max<size_t>(a.n, o.cap);
+    for (int k = 0; k < 2 && !rc; ++k) {
+      rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&o.keys[k]), cap * 4), "ray order keys");
+      if (!rc) rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&o.vals[k]), cap * 4), "ray order indices");
+    }
+    if (!rc) rc = check_cuda(ctx, cudaMalloc(&o.temp, need), "ray order temporary");
+    if (rc) {
+      free_order(o);
+      return rc;
+    }
+    o.cap = cap;
+    o.temp_bytes = need;
+  }
+  float const* b = ctx->scene.bounds;
+  float3 lo, sc;
+  float* plo = &lo.x;
+  float* psc = &sc.x;
+  for (int k = 0; k < 3; ++k) {
+    float const ext = b[3 + k] - b[k];
+    plo[k] = b[k] - 1e-3f * ext;
+    psc[k] = ext > 0.f ? 16.f / (ext * 1.002f) : 0.f;
+  }
+  k_ray_keys<<<(a.n + 255) / 256, 256, 0, s>>>(a.rays, a.n, lo, sc, o.keys[0], o.vals[0]);
+  rc = check_cuda(ctx, cudaGetLastError(), "ray key launch");
+  if (rc) return rc;
+  size_t tb = o.temp_bytes;
+  rc = check_cuda(ctx, cub::DeviceRadixSort::SortPairs(o.temp, tb, o.keys[0], o.keys[1], o.vals[0], o.vals[1],
+                           int(a.n), 0, kOrderKeyBits, s), "ray order sort");
+  if (rc) return rc;
+  a.perm = o.vals[1];
+  return MYRT_OK;
+}
+
+int launch_trace_kernels(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s);
+
+// lane: the ray-order scratch to use (0 = the context's stream, 1 = its
+// second lane).
+int launch_trace(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s, int lane = 0) {
   if (a.n == 0) return MYRT_OK;
+  uint32_t const mode = ctx->tuning.trace_order;
+  bool const sorted = mode == 2 || (mode == 0 && a.n >= kOrderMin);
+  if (!sorted) return launch_trace_kernels(ctx, a, intersector, any, stats, s);
+  int rc = order_rays(ctx, a, lane, s);
+  if (!rc) rc = launch_trace_kernels(ctx, a, intersector, any, stats, s);
+  if (!rc) rc = check_cuda(ctx, cudaEventRecord(ctx->order[lane].done, s), "ray order record");
+  return rc;
+}
+
+int launch_trace_kernels(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s) {
   dim3 const block(128);
   dim3 const grid((a.n + 127) / 128);
   if (ctx->tuning.trace_persistent) {
@@ -115,6 +197,26 @@ int launch_trace(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool st
       else if (stats) rc = launch_persistent<1, false, true>(ctx, a, s);
       else rc = launch_persistent<1, false, false>(ctx, a, s);
     }
+    if (rc) return rc;
+    return check_cuda(ctx, cudaGetLastError(), "trace launch");
+  }
+  if (ctx->tuning.trace_smem_stack && !ctx->tuning.trace_unit_steps) {
+    a.stack_cap = std::max(1, std::min(ctx->scene.stats.wide_depth + 1, MYRT_STACK_MAX));
+    size_t const smem = size_t(a.stack_cap) * 128 * sizeof(uint2);
+    auto go_smem = [&](auto kern) -> int {
+      int rc = check_cuda(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)),
+          "trace shared stack");
+      if (rc) return rc;
+      kern<<<grid, block, smem, s>>>(a);
+      return MYRT_OK;
+    };
+    int rc;
+    if (intersector == MYRT_ISECT_REFERENCE)
+      rc = stats ? go_smem(k_trace_smem<0, false, true>) : any ? go_smem(k_trace_smem<0, true, false>)
+                                                               : go_smem(k_trace_smem<0, false, false>);
+    else
+      rc = stats ? go_smem(k_trace_smem<1, false, true>) : any ? go_smem(k_trace_smem<1, true, false>)
+                                                               : go_smem(k_trace_smem<1, false, false>);
     if (rc) return rc;
     return check_cuda(ctx, cudaGetLastError(), "trace launch");
   }
@@ -181,7 +283,10 @@ int host_query(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, void* out, size_
     a.n = cn;
     if (any) a.occluded = reinterpret_cast<uint8_t*>(d_out);
     else a.hits = reinterpret_cast<float4*>(d_out);
-    rc = launch_trace(ctx, a, intersector, any, false, s);
+    // chunks stream through the copy engines, which bound this path: they are
+    // traced in input order unless sorting is forced (trace_order 2)
+    rc = ctx->tuning.trace_order == 2 ? launch_trace(ctx, a, intersector, any, false, s, int(k & 1))
+                                      : launch_trace_kernels(ctx, a, intersector, any, false, s);
     if (rc) return rc;
     rc = check_cuda(ctx,
         cudaMemcpyAsync(static_cast<char*>(out) + size_t(c0) * out_stride, d_out, size_t(cn) * out_stride,
@@ -292,6 +397,10 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   free_guide(ctx->guide);
   ctx->guide = nullptr;
   for (auto& p : ctx->stage) cudaFree(p);
+  for (auto& o : ctx->order) {
+    free_order(o);
+    if (o.done) cudaEventDestroy(o.done);
+  }
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_next);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -310,7 +419,7 @@ int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
   if (!ctx || !t) return MYRT_ERR_INVALID_ARGUMENT;
   if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
       t->trace_unit_steps > 1 || (t->wave_paths != 0 && (t->wave_paths < 1024 || t->wave_paths > (1u << 28))) ||
-      t->pt_blocks_per_sm > 16)
+      t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;

@@ -90,13 +90,22 @@ struct myrt_ctx {
   myrt_b200::guide_state* guide = nullptr;  // learned proposal (guide.cu), created on first use
   uint64_t guide_generation = 0;            // bumped by scene uploads
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
-  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u};
+  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
   int sm_count = 0;
   uint32_t* d_next = nullptr;    // ring of ray counters for the persistent traversal
   uint32_t next_slot = 0;
   // staging buffers of the host-memory entry points (two chunk slots)
   void* stage[2] = {nullptr, nullptr};
   size_t stage_bytes = 0;
+  // ray-order scratch per stream lane (keys and indices, double-buffered, and
+  // the radix sort's temporary storage); `done` orders reuse across streams
+  struct order_scratch {
+    uint32_t* keys[2] = {nullptr, nullptr};
+    uint32_t* vals[2] = {nullptr, nullptr};
+    void* temp = nullptr;
+    size_t cap = 0, temp_bytes = 0;
+    cudaEvent_t done = nullptr;
+  } order[2];
 };
 
 namespace myrt_b200 {

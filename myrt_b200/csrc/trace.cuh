@@ -130,6 +130,8 @@ struct trace_args {
   uint32_t* stat_nodes;
   uint32_t* stat_tris;
   uint32_t* err;
+  int stack_cap;       // k_trace_smem: stack entries per thread
+  uint32_t const* perm;  // visiting order (thread t takes ray perm[t]); null = input order
 };
 
 // Byte (s & 3) of w as an exact float: one byte permute places it in the low
@@ -137,6 +139,38 @@ struct trace_args {
 // the 48 plane conversions per node off the quarter-rate conversion pipe.
 __device__ __forceinline__ float q8(uint32_t w, int s) {
   return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | uint32_t(s & 3))) - 8388608.0f;
+}
+
+// Two lanes of packed FP32 (sm_100 add/fma .f32x2): each lane rounds exactly
+// like the scalar __fadd_rn / fmaf, two planes per instruction.
+__device__ __forceinline__ uint64_t pack2(uint32_t lo, uint32_t hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(lo), "r"(hi));
+  return r;
+}
+__device__ __forceinline__ uint64_t pack2f(float lo, float hi) { return pack2(__float_as_uint(lo), __float_as_uint(hi)); }
+__device__ __forceinline__ void unpack2(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+// Planes of slots s and s + 1 (s even) of word w, scaled: (q - 0) * sc + of per lane.
+__device__ __forceinline__ void plane2(uint32_t w, int s, uint64_t sc2, uint64_t of2, float& t0, float& t1) {
+  uint64_t q = pack2(__byte_perm(w, 0x4B000000u, 0x7440u | uint32_t(s & 3)),
+      __byte_perm(w, 0x4B000000u, 0x7440u | uint32_t((s + 1) & 3)));
+  uint64_t const m23 = 0xCB000000CB000000ull;  // (-2^23, -2^23)
+  asm("add.rn.f32x2 %0, %0, %1;" : "+l"(q) : "l"(m23));
+  uint64_t t;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(t) : "l"(q), "l"(sc2), "l"(of2));
+  unpack2(t, t0, t1);
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
 }
 
 struct hit_rec {
@@ -151,7 +185,10 @@ struct hit_rec {
 // exhausted) and returns false once the ray is finished. The per-thread loop
 // (traverse) and the persistent kernel (which refills finished lanes with new
 // rays) both drive it, so they visit the same nodes in the same order.
-template <int ISECT, bool ANY>
+// SS: distance between consecutive stack entries of one ray (1 for a
+// per-thread array; the block size for a shared-memory stack laid out
+// [entry][thread], which keeps every push and pop free of bank conflicts).
+template <int ISECT, bool ANY, int SS = 1>
 struct walker {
   f3 o, d;
   float tmin, tmax;
@@ -164,9 +201,11 @@ struct walker {
   uint32_t bleaf;
   uint2 group;
   int sp;
+  int cap;  // stack entries available
   bool occluded;
 
-  __device__ __forceinline__ void init(f3 o_, f3 d_, float tmin_, float tmax_) {
+  __device__ __forceinline__ void init(f3 o_, f3 d_, float tmin_, float tmax_, int cap_ = MYRT_STACK_MAX) {
+    cap = cap_;
     o = o_;
     d = d_;
     tmin = tmin_;
@@ -199,11 +238,11 @@ struct walker {
       uint32_t const slot = (pos - 24u) ^ octinv;
       uint32_t const node_idx = group.x + __popc(group.y & 0xffu & ((1u << slot) - 1u));
       if (group.y & 0xff000000u) {
-        if (sp >= MYRT_STACK_MAX) {
+        if (sp >= cap) {
           atomicOr(err, ERR_STACK_OVERFLOW);
           return false;
         }
-        stack[sp++] = group;
+        stack[SS * sp++] = group;
       }
       uint4 const* np = nodes + 5 * size_t(node_idx);
       uint4 const w0 = __ldg(np + 0);
@@ -227,23 +266,33 @@ struct walker {
       uint32_t const nz0 = idz >= 0.f ? w3.x : w4.z, nz1 = idz >= 0.f ? w3.y : w4.w;
       uint32_t const fz0 = idz >= 0.f ? w4.z : w3.x, fz1 = idz >= 0.f ? w4.w : w3.y;
       uint32_t hit_internal = 0, hit_tris = 0;
+      uint64_t const sx2 = pack2f(sx, sx), sy2 = pack2f(sy, sy), sz2 = pack2f(sz, sz);
+      uint64_t const ox2 = pack2f(ox, ox), oy2 = pack2f(oy, oy), oz2 = pack2f(oz, oz);
 #pragma unroll
-      for (int s = 0; s < 8; ++s) {
+      for (int s = 0; s < 8; s += 2) {
         uint32_t const nxw = s < 4 ? nx0 : nx1, fxw = s < 4 ? fx0 : fx1;
         uint32_t const nyw = s < 4 ? ny0 : ny1, fyw = s < 4 ? fy0 : fy1;
         uint32_t const nzw = s < 4 ? nz0 : nz1, fzw = s < 4 ? fz0 : fz1;
-        float const tnx = fmaf(q8(nxw, s), sx, ox), tfx = fmaf(q8(fxw, s), sx, ox);
-        float const tny = fmaf(q8(nyw, s), sy, oy), tfy = fmaf(q8(fyw, s), sy, oy);
-        float const tnz = fmaf(q8(nzw, s), sz, oz), tfz = fmaf(q8(fzw, s), sz, oz);
-        float const tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin));
-        float const tf = fminf(fminf(tfx, tfy), fminf(tfz, tbest));
-        uint32_t const meta = ((s < 4 ? w1.z : w1.w) >> (8 * (s & 3))) & 0xffu;
-        if (meta != 0u && tn <= tf * 1.00000024f) {
-          if (imask & (1u << s)) {
-            hit_internal |= 1u << ((s ^ octinv) + 24u);
-          } else {
-            uint32_t const cnt = meta >> 5, off = meta & 31u;
-            hit_tris |= ((1u << cnt) - 1u) << off;
+        float tnx[2], tfx[2], tny[2], tfy[2], tnz[2], tfz[2];
+        plane2(nxw, s, sx2, ox2, tnx[0], tnx[1]);
+        plane2(fxw, s, sx2, ox2, tfx[0], tfx[1]);
+        plane2(nyw, s, sy2, oy2, tny[0], tny[1]);
+        plane2(fyw, s, sy2, oy2, tfy[0], tfy[1]);
+        plane2(nzw, s, sz2, oz2, tnz[0], tnz[1]);
+        plane2(fzw, s, sz2, oz2, tfz[0], tfz[1]);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          int const c = s + h;
+          float const tn = max3f(tnx[h], tny[h], fmaxf(tnz[h], tmin));
+          float const tf = min3f(tfx[h], tfy[h], fminf(tfz[h], tbest));
+          uint32_t const meta = ((c < 4 ? w1.z : w1.w) >> (8 * (c & 3))) & 0xffu;
+          if (meta != 0u && tn <= tf * 1.00000024f) {
+            if (imask & (1u << c)) {
+              hit_internal |= 1u << ((c ^ octinv) + 24u);
+            } else {
+              uint32_t const cnt = meta >> 5, off = meta & 31u;
+              hit_tris |= ((1u << cnt) - 1u) << off;
+            }
           }
         }
       }
@@ -303,7 +352,7 @@ struct walker {
     }
     if (!(group.y & 0xff000000u)) {
       if (sp == 0) return false;
-      group = stack[--sp];
+      group = stack[SS * --sp];
     }
     return true;
   }
@@ -322,7 +371,7 @@ struct walker {
     }
     if (group.y & 0xff000000u) return visit<STATS>(nodes, stack, err, n_nodes, tg);
     if (sp == 0) return false;
-    group = stack[--sp];
+    group = stack[SS * --sp];
     return true;
   }
 
@@ -371,12 +420,35 @@ __device__ __forceinline__ void store_result(trace_args const& a, uint32_t i, bo
   }
 }
 
+// One thread per ray, traversal stack in shared memory ([entry][thread],
+// a.stack_cap entries per thread; dynamic shared memory of
+// a.stack_cap * 128 * 8 bytes).
+template <int ISECT, bool ANY, bool STATS>
+__global__ void __launch_bounds__(128, 8) k_trace_smem(trace_args a) {
+  extern __shared__ uint2 sstack[];
+  uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  uint32_t const i = a.perm ? __ldg(a.perm + t) : t;
+  float4 const r0 = __ldg(a.rays + 2 * size_t(i));
+  float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
+  walker<ISECT, ANY, 128> w;
+  w.init(f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w, r1.w, a.stack_cap);
+  uint32_t n_nodes = 0, n_tris = 0;
+  uint2* stack = sstack + threadIdx.x;
+  while (w.template step<STATS>(a.nodes, a.tris, stack, a.err, n_nodes, n_tris)) {
+  }
+  hit_rec h;
+  if (!ANY) w.result(h);
+  store_result<ISECT, ANY, STATS>(a, i, ANY ? w.occluded : h.prim >= 0, h, n_nodes, n_tris);
+}
+
 // One thread per ray. MINB = resident 128-thread blocks per SM the compiler
 // must allow (8 leaves it 64 registers; more blocks cap the register count).
 template <int ISECT, bool ANY, bool STATS, int MINB = 8, bool UNIT = false>
 __global__ void __launch_bounds__(128, MINB) k_trace(trace_args a) {
-  uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n) return;
+  uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  uint32_t const i = a.perm ? __ldg(a.perm + t) : t;
   float4 const r0 = __ldg(a.rays + 2 * size_t(i));
   float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
   hit_rec h;
@@ -411,10 +483,11 @@ __global__ void __launch_bounds__(128) k_trace_persistent(trace_args a, uint32_t
       if (!active) {
         uint32_t const mine = base + __popc(idle & ((1u << lane) - 1u));
         if (mine < a.n) {
-          float4 const r0 = __ldg(a.rays + 2 * size_t(mine));
-          float4 const r1 = __ldg(a.rays + 2 * size_t(mine) + 1);
+          uint32_t const ri = a.perm ? __ldg(a.perm + mine) : mine;
+          float4 const r0 = __ldg(a.rays + 2 * size_t(ri));
+          float4 const r1 = __ldg(a.rays + 2 * size_t(ri) + 1);
           w.init(f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w, r1.w);
-          ray = mine;
+          ray = ri;
           n_nodes = n_tris = 0;
           active = true;
         }

@@ -204,3 +204,59 @@ def test_unit_step_traversal_bit_exact(ctx, hf128):
         assert np.array_equal(d_t.cpu().numpy().astype(np.uint32), ct)
     finally:
         ctx.set_tuning()
+
+
+@pytest.mark.parametrize("isect", [0, 1])
+def test_shared_stack_traversal_bit_exact(ctx, hf128, isect):
+    """The traversal stack in shared memory (tree depth + 1 entries per ray)
+    walks the same order as the per-thread stack: same hits and counters, for
+    closest and any hit, both intersectors."""
+    import torch
+
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = np.concatenate([pinhole_rays(256, 256), _rand_rays(100_000, seed=23)])
+    ora, cn, ct = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays, isect=isect)
+    try:
+        ctx.set_tuning(trace_smem_stack=1)
+        assert np.array_equal(ctx.trace_closest(rays, intersector=isect), ora)
+        assert np.array_equal(ctx.trace_any(rays, intersector=isect).astype(bool), ora["prim"] >= 0)
+        d_rays = torch.from_numpy(rays).cuda()
+        d_hits = torch.empty((rays.shape[0], 4), dtype=torch.float32, device="cuda")
+        d_n = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        d_t = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.trace_closest_stats_device(d_rays, d_hits, d_n, d_t, intersector=isect)
+        ctx.sync()
+        assert np.array_equal(d_n.cpu().numpy().astype(np.uint32), cn)
+        assert np.array_equal(d_t.cpu().numpy().astype(np.uint32), ct)
+    finally:
+        ctx.set_tuning()
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_ray_order_does_not_change_results(ctx, hf128, order):
+    """Sorted visiting order (trace_order 2) and input order (1) give the same
+    hits, occlusion and per-ray counters as the oracle, through the host and
+    the device entry points; rays are a shuffled mix of camera and random rays."""
+    import torch
+
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = np.concatenate([pinhole_rays(256, 256), _rand_rays(150_000, seed=24)])
+    rays = rays[np.random.default_rng(3).permutation(rays.shape[0])]
+    ora, cn, ct = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays)
+    try:
+        ctx.set_tuning(trace_order=order)
+        assert np.array_equal(ctx.trace_closest(rays), ora)
+        assert np.array_equal(ctx.trace_any(rays).astype(bool), ora["prim"] >= 0)
+        d_rays = torch.from_numpy(rays).cuda()
+        d_hits = torch.empty((rays.shape[0], 4), dtype=torch.float32, device="cuda")
+        d_n = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        d_t = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.trace_closest_stats_device(d_rays, d_hits, d_n, d_t)
+        ctx.sync()
+        assert np.array_equal(d_hits.cpu().numpy().view(mb.HIT_DTYPE).ravel(), ora)
+        assert np.array_equal(d_n.cpu().numpy().astype(np.uint32), cn)
+        assert np.array_equal(d_t.cpu().numpy().astype(np.uint32), ct)
+    finally:
+        ctx.set_tuning()
