@@ -53,9 +53,11 @@ def parse_args():
     p.add_argument("--res", type=int, default=512)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=None)
-    p.add_argument("--workload", choices=["closest", "guiding"], default="closest",
+    p.add_argument("--workload", choices=["closest", "guiding", "pt", "batch", "sdf"], default="closest",
                    help="closest: closest-hit Mrays/s (with a reduced guided-vs-plain leg); guiding: the full "
-                        "time-to-equal-relRMSE run (1024x1024, FP64 4096-spp oracle)")
+                        "time-to-equal-relRMSE run (1024x1024, FP64 4096-spp oracle); pt: plain path tracing "
+                        "of the icosphere scene (512x512, 64 spp, depth 8); batch: 16 uneven scenes in one "
+                        "CUDA graph per frame; sdf: SDF + mesh hybrid with guiding (768x768, 128 spp)")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain leg of the closest workload")
     return p.parse_args()
 
@@ -574,12 +576,262 @@ def run_guiding_workload(args):
     return 0
 
 
+# ----------------------------------------------------------- render workloads --
+def _render_line(metric, value, unit, steps, warmup, ms, config, extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": steps, "warmup": warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": config}
+    line.update(extra)
+    return line
+
+
+def _timed_frames(ctx_stream, render, steps):
+    """CUDA-event milliseconds of `steps` calls of render() on the given stream."""
+    import torch
+
+    st = torch.cuda.ExternalStream(ctx_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(steps):
+        render()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_pt_workload(args):
+    """Plain path tracing (physical shading: GGX + Lambert, NEE with MIS, RR
+    after vertex 3) of the icosphere scene with its 0.2 x 0.2 light, 512x512,
+    64 spp per step, depth 8. Reports samples/s and traced Mrays/s, the
+    relRMSE of one step's image against an FP64 1024-spp render, and the
+    same throughput through the host API with the image read back (e2e)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import torch
+
+    import myrt_b200 as mb
+    from myrt_b200.camera import look_at
+    from myrt_b200.scenes import icosphere_field_lit
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = mb.Context(local)
+    scene, lights = icosphere_field_lit()
+    info = ctx.upload_scene(**scene)
+    ctx.set_area_lights(lights)
+    W = H = 512
+    spp = 64
+    iv, ip = look_at((0.0, 1.0, -4.5), (0.0, -0.3, 0.0), vfov_deg=50, aspect=1.0)
+
+    def frame(seed=1, fp64=False, n=spp):
+        ctx.render_physical(iv, ip, W, H, spp=n, max_depth=8, rr_start=3, seed=seed, fp64=fp64)
+
+    ctx.reset_accumulation()
+    frame(fp64=True, n=1024, seed=999)
+    ctx.sync()
+    ref = ctx.read_accumulation_f64(W, H)
+    ref = ref[..., :3] / ref[..., 3:4]
+    ctx.reset_accumulation()
+    frame()
+    acc, _ = ctx.read_accumulation(W, H)
+    err_one = rel_rmse(acc[..., :3] / acc[..., 3:4], ref)
+    for _ in range(args.warmup):
+        frame()
+    s0 = ctx.render_stats()
+    with ClockSampler(local) as clocks:
+        ms = _timed_frames(ctx.stream, frame, args.steps)
+    s1 = ctx.render_stats()
+    rays = (s1["extension_rays"] - s0["extension_rays"]) + (s1["shadow_rays"] - s0["shadow_rays"])
+    samples = W * H * spp * args.steps
+    # end to end: the host API call plus the image read-back, wall clock
+    ctx.reset_accumulation()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        frame()
+        ctx.read_accumulation(W, H)
+    e2e_s = time.perf_counter() - t0
+    ctx.close()
+    line = _render_line(
+        "samples/s plain path tracing", samples / (ms / 1e3), "samples/s", args.steps, args.warmup, ms / args.steps,
+        {"workload": "plain path tracing, icosphere scene (655,872 tris) + 0.2x0.2 light of emission 20; "
+                     "512x512, 64 spp per step, depth 8, RR after 3, NEE + MIS", "triangles": int(info["triangles"]),
+         "res": W, "spp_per_step": spp, "l2": "per-wave path state (4 Mi paths, ~1 GB) exceeds L2"},
+        {"mrays_per_s": rays / (ms / 1e3) / 1e6, "rays_per_sample": rays / samples,
+         "rel_rmse_one_step_vs_fp64_1024spp": err_one,
+         "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128,
+                 "d2h_bytes_per_step": W * H * 16, "api": "myrt_render + myrt_read_accumulation"},
+         "clocks": clocks.summary()})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch_workload(args):
+    """Batched uneven scenes: 16 height-field / icosphere scenes with triangle
+    counts log-uniform in [10k, 2M], one view each (128^2 to 1024^2, 4-64
+    spp), all rendered as one CUDA graph per frame with the launch shape the
+    autotuner picks. One step = one frame of every job. Two jobs are checked
+    against their unbatched renders (bit-identical accumulations)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import torch
+
+    import myrt_b200 as mb
+    from myrt_b200 import autotune
+    from myrt_b200.scenes import uneven_batch
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    scenes, jobs = uneven_batch()
+    ctxs = []
+    t0 = time.perf_counter()
+    for s, lights, _ in scenes:
+        c = mb.Context(local)
+        c.upload_scene(**s)
+        c.set_area_lights(lights)
+        ctxs.append(c)
+    upload_s = time.perf_counter() - t0
+    batch = mb.Batch(ctxs, jobs)
+    tuned = autotune.tune_batch(batch, waves=(1 << 20, 4 << 20, 16 << 20), blocks=(4, 8), reps=1)
+    for _ in range(args.warmup):
+        batch.render()
+    s0 = batch.render_stats()
+    with ClockSampler(local) as clocks:
+        ms = _timed_frames(batch.stream, batch.render, args.steps)
+    s1 = batch.render_stats()
+    rays = (s1["extension_rays"] - s0["extension_rays"]) + (s1["shadow_rays"] - s0["shadow_rays"])
+    samples = sum(j["width"] * j["height"] * j["spp"] for j in jobs) * args.steps
+    info = batch.info()
+    # per-job equality with the unbatched renders (one frame each)
+    batch.reset()
+    batch.render()
+    checked = []
+    for k in (1, 5):
+        j = jobs[k]
+        c = ctxs[j["scene"]]
+        c.reset_accumulation()
+        c.render_physical(j["inverse_view"], j["inverse_projection"], j["width"], j["height"], spp=j["spp"],
+                          max_depth=j["max_depth"], rr_start=j["rr_start"], seed=j["seed"])
+        checked.append({"job": k, "equal": bool(np.array_equal(batch.read(k), c.read_accumulation(j["width"],
+                                                                                              j["height"])[0]))})
+    # end to end: the frame call plus every job's image read-back, wall clock
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        batch.render()
+        for k in range(len(jobs)):
+            batch.read(k)
+    e2e_s = time.perf_counter() - t0
+    batch.close()
+    for c in ctxs:
+        c.close()
+    line = _render_line(
+        "samples/s batched uneven scenes", samples / (ms / 1e3), "samples/s", args.steps, args.warmup,
+        ms / args.steps,
+        {"workload": "16 height-field / icosphere scenes, triangles log-uniform 10k-2M (6.56 M total), one view "
+                     "each at 128^2-1024^2 and 4-64 spp, one CUDA graph per frame", "jobs": len(jobs),
+         "paths_per_frame": int(info["paths_per_frame"]), "triangles": [t for _, _, t in scenes],
+         "upload_s": round(upload_s, 2), "l2": "per-wave path state exceeds L2"},
+        {"mrays_per_s": rays / (ms / 1e3) / 1e6, "rays_per_sample": rays / samples,
+         "autotune": {"wave_paths": tuned["wave_paths"], "blocks_per_sm": tuned["blocks_per_sm"],
+                      "candidates": tuned.get("results")},
+         "graph": {"waves": info["waves"], "graph_nodes": info["graph_nodes"]},
+         "equal_to_unbatched": checked,
+         "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 64 * len(jobs),
+                 "d2h_bytes_per_step": sum(j["width"] * j["height"] * 16 for j in jobs),
+                 "api": "myrt_batch_render + myrt_batch_read per job"},
+         "clocks": clocks.summary()})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_sdf_workload(args):
+    """SDF + mesh hybrid: the icosphere scene with a smooth union (k = 0.1) of
+    256 seeded spheres / boxes / tori sphere-traced with 256 steps and eps
+    1e-4, GGX materials, guiding on; 768x768, 128 spp per step. Reports
+    samples/s, traced Mrays/s and the step image's relRMSE against an FP64
+    render."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import torch
+
+    import myrt_b200 as mb
+    from myrt_b200 import sdf as S
+    from myrt_b200.camera import look_at
+    from myrt_b200.scenes import icosphere_field_lit
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = mb.Context(local)
+    scene, lights = icosphere_field_lit()
+    info = ctx.upload_scene(**scene)
+    lib = S.SdfLibrary()
+    lib.add(S.random_sdf_field(256, k=0.1, seed=9, extent=0.8))
+    dr = S.sdf_drawables([np.array([[1, 0, 0, 0.0], [0, 1, 0, -0.2], [0, 0, 1, 0.3], [0, 0, 0, 1]])], [0])
+    ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)
+    ctx.set_area_lights(lights)
+    W = H = 768
+    spp = 128
+    iv, ip = look_at((0.0, 1.0, -4.5), (0.0, -0.3, 0.0), vfov_deg=50, aspect=1.0)
+    ctx.guide_configure(**GUIDE_CFG)
+    ctx.guide_reset()
+
+    def frame(seed=1, fp64=False, n=spp, guided=True, rr=3):
+        ctx.render_physical(iv, ip, W, H, spp=n, max_depth=8, rr_start=rr, seed=seed, fp64=fp64, guided=guided,
+                            sdf_marching_steps=256, sdf_marching_epsilon=1e-4)
+
+    oracle_spp = 512
+    ctx.reset_accumulation()
+    frame(seed=999, fp64=True, n=oracle_spp, guided=False)
+    ctx.sync()
+    ref = ctx.read_accumulation_f64(W, H)
+    ref = ref[..., :3] / ref[..., 3:4]
+    for _ in range(args.warmup):
+        ctx.reset_accumulation()
+        frame()
+    ctx.guide_reset()
+    ctx.reset_accumulation()
+    s0 = ctx.render_stats()
+    with ClockSampler(local) as clocks:
+        ms = _timed_frames(ctx.stream, frame, args.steps)
+    s1 = ctx.render_stats()
+    acc, _ = ctx.read_accumulation(W, H)
+    err = rel_rmse(acc[..., :3] / acc[..., 3:4], ref)
+    rays = (s1["extension_rays"] - s0["extension_rays"]) + (s1["shadow_rays"] - s0["shadow_rays"])
+    samples = W * H * spp * args.steps
+    ctx.reset_accumulation()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        frame()
+        ctx.read_accumulation(W, H)
+    e2e_s = time.perf_counter() - t0
+    ctx.close()
+    line = _render_line(
+        "samples/s SDF + mesh hybrid (guided)", samples / (ms / 1e3), "samples/s", args.steps, args.warmup,
+        ms / args.steps,
+        {"workload": "icosphere scene (655,872 tris) + 256-primitive SDF smooth union (k 0.1), 256 steps, eps "
+                     "1e-4, guided, 768x768, 128 spp per step, depth 8", "triangles": int(info["triangles"]),
+         "sdf_primitives": 256, "res": W, "spp_per_step": spp},
+        {"mrays_per_s": rays / (ms / 1e3) / 1e6, "rays_per_sample": rays / samples,
+         f"rel_rmse_vs_fp64_{oracle_spp}spp": err, "rel_rmse_spp": spp * args.steps,
+         "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128,
+                 "d2h_bytes_per_step": W * H * 16, "api": "myrt_render + myrt_read_accumulation"},
+         "clocks": clocks.summary()})
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.workload == "guiding":
         return run_guiding_workload(args)
+    if args.workload == "pt":
+        return run_pt_workload(args)
+    if args.workload == "batch":
+        return run_batch_workload(args)
+    if args.workload == "sdf":
+        return run_sdf_workload(args)
     return run_ours(args)
 
 

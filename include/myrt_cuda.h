@@ -398,6 +398,9 @@ int myrt_batch_render(myrt_batch* batch);
 int myrt_batch_read(myrt_batch* batch, uint32_t job, float* rgba, double* rgba64);
 int myrt_batch_reset(myrt_batch* batch);
 int myrt_batch_get_info(myrt_batch* batch, myrt_batch_info* info);
+/* Cumulative camera / extension / shadow ray counts of the batch's frames
+ * (the batch's own wavefront; the scene contexts' counters are not touched). */
+int myrt_batch_get_stats(myrt_batch* batch, myrt_render_stats* out);
 int myrt_batch_destroy(myrt_batch* batch);
 
 /* ---- learned path guiding (MYRT_SHADE_GUIDED) ----------------------------------

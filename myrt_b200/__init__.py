@@ -407,6 +407,11 @@ class Batch:
             self._check(self._L.myrt_batch_read(self._h, job, out.ctypes.data, None), "myrt_batch_read")
         return out
 
+    def render_stats(self) -> dict:
+        st = _abi.myrt_render_stats()
+        self._check(self._L.myrt_batch_get_stats(self._h, C.byref(st)), "myrt_batch_get_stats")
+        return dict(paths=st.paths, extension_rays=st.extension_rays, shadow_rays=st.shadow_rays)
+
     def info(self) -> dict:
         i = _abi.myrt_batch_info()
         self._check(self._L.myrt_batch_get_info(self._h, C.byref(i)), "myrt_batch_get_info")

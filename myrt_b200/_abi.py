@@ -157,6 +157,7 @@ SIGNATURES = {
     "myrt_batch_read": (I, [P, U32, P, P]),
     "myrt_batch_reset": (I, [P]),
     "myrt_batch_get_info": (I, [P, C.POINTER(myrt_batch_info)]),
+    "myrt_batch_get_stats": (I, [P, C.POINTER(myrt_render_stats)]),
     "myrt_batch_destroy": (I, [P]),
     "myrt_guide_configure": (I, [P, C.POINTER(myrt_guide_params)]),
     "myrt_guide_get_config": (I, [P, C.POINTER(myrt_guide_params)]),

@@ -1018,6 +1018,23 @@ int myrt_batch_reset(myrt_batch* b) {
   return MYRT_OK;
 }
 
+int myrt_batch_get_stats(myrt_batch* b, myrt_render_stats* out) {
+  if (!b || !out) return MYRT_ERR_INVALID_ARGUMENT;
+  myrt_ctx* ctx = b->ctx;
+  unsigned long long s[4] = {0, 0, 0, 0};
+  if (b->queues.stats) {
+    int rc = check_cuda(ctx, cudaMemcpyAsync(s, b->queues.stats, sizeof(s), cudaMemcpyDeviceToHost, ctx->stream),
+        "read batch statistics");
+    if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "read batch statistics");
+    if (rc) return rc;
+  }
+  out->paths = s[0];
+  out->extension_rays = s[1];
+  out->shadow_rays = s[2];
+  out->reserved = 0;
+  return MYRT_OK;
+}
+
 int myrt_batch_get_info(myrt_batch* b, myrt_batch_info* info) {
   if (!b || !info) return MYRT_ERR_INVALID_ARGUMENT;
   int rc = MYRT_OK;

@@ -268,3 +268,43 @@ def guiding_box(slab_cells: int = 708, wall_cells: int = 8, seed: int = 7, plate
                  materials=materials, material_data=mat_data)
     light = area_light((light_x, 0.995, 0.0), 0.05, 400.0)[None, :]
     return scene, light
+
+
+def heightfield_scene(n: int, seed: int = 1, albedo=(0.7, 0.6, 0.5), roughness: float = 0.4):
+    """The n x n height field (2 n^2 triangles) with one PBR material and a
+    0.5 x 0.5 area light (emission 12) at y = 1.5: (scene, lights[1, 12])."""
+    idx, pts = heightfield(n, seed=seed)
+    s = dict(indices=idx, vertices=pts, materials=np.array([[0, 0]], np.int32),
+             material_data=pbr_material(list(albedo), ior=1.5, roughness=roughness))
+    return s, area_light((0.0, 1.5, 0.0), 0.5, 12.0)[None, :]
+
+
+def uneven_batch(n_scenes: int = 16, seed: int = 11, tri_range=(1e4, 2e6)):
+    """Batched uneven scenes: n_scenes height-field / icosphere scenes with
+    triangle counts log-uniform in tri_range, one view each at a resolution
+    from {128, 256, 512, 1024}^2 and 4-64 spp. Returns (scenes, jobs):
+    scenes = [(scene, lights, triangles)], jobs = Batch job dicts (without the
+    camera matrices' numpy conversion; keys as myrt_b200.Batch expects)."""
+    from .camera import look_at
+
+    rng = np.random.default_rng(seed)
+    scenes, jobs = [], []
+    for k in range(n_scenes):
+        tris = float(np.exp(rng.uniform(np.log(tri_range[0]), np.log(tri_range[1]))))
+        res = int(rng.choice([128, 256, 512, 1024]))
+        spp = int(rng.integers(4, 65))
+        if k % 2 == 0:
+            n = max(2, int(round(np.sqrt(tris / 2))))
+            s, lights = heightfield_scene(n, seed=100 + k)
+            count = 2 * n * n
+            eye, tgt, vfov = (0.0, 1.5, -2.5), (0.0, 0.0, 0.0), 60.0
+        else:
+            spheres = max(1, int(round((tris - 512) / 1280)))
+            s, lights = icosphere_field_lit(n_spheres=spheres, seed=200 + k)
+            count = 1280 * spheres + 512
+            eye, tgt, vfov = (0.0, 1.0, -4.5), (0.0, -0.3, 0.0), 50.0
+        iv, ip = look_at(eye, tgt, vfov_deg=vfov, aspect=1.0)
+        scenes.append((s, lights, count))
+        jobs.append(dict(scene=k, width=res, height=res, spp=spp, seed=1000 + k, max_depth=8, rr_start=3,
+                         inverse_view=iv, inverse_projection=ip))
+    return scenes, jobs

@@ -108,6 +108,8 @@ def test_batch_equals_unbatched():
     info = batch.info()
     assert info["waves"] > 3 and info["graph_nodes"] > 20
     assert info["paths_per_frame"] == sum(j["width"] * j["height"] * j["spp"] for j in jobs)
+    st = batch.render_stats()
+    assert st["paths"] == 2 * info["paths_per_frame"] and st["extension_rays"] >= st["paths"]
     got = [batch.read(k) for k in range(len(jobs))]
     for k, j in enumerate(jobs):
         ref = _unbatched(ctxs, j, 2)
