@@ -49,8 +49,10 @@ def parse_args():
     p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--spp", type=int, default=64)
-    p.add_argument("--res", type=int, default=512)
+    p.add_argument("--spp", type=int, default=None, help="samples per pixel (default: the workload's own)")
+    p.add_argument("--res", type=int, default=None, help="image side (default: the workload's own)")
+    p.add_argument("--oracle-spp", type=int, default=None, help="spp of the FP64 oracle (default: the workload's)")
+    p.add_argument("--budget-spp", type=int, default=None, help="guiding: plain spp budget (default 256)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=None)
     p.add_argument("--workload", choices=["closest", "guiding", "pt", "batch", "sdf"], default="closest",
@@ -59,7 +61,11 @@ def parse_args():
                         "of the icosphere scene (512x512, 64 spp, depth 8); batch: 16 uneven scenes in one "
                         "CUDA graph per frame; sdf: SDF + mesh hybrid with guiding (768x768, 128 spp)")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain leg of the closest workload")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.workload == "closest":
+        a.res = a.res or 512
+        a.spp = a.spp or 64
+    return a
 
 
 # ---------------------------------------------------------------- workload --
@@ -456,6 +462,8 @@ def run_ours(args):
     if dist:
         dist.barrier()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.set_phase_timing(True)  # CUDA events around the ordering phase and the traversal kernel
+    ctx.phase_times()
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
         start.record(stream)
@@ -464,6 +472,8 @@ def run_ours(args):
         end.record(stream)
         torch.cuda.synchronize()
     ctx.sync()
+    phases = ctx.phase_times()
+    ctx.set_phase_timing(False)
     ms = start.elapsed_time(end)
     if dist:
         t = torch.tensor([ms], device=device)
@@ -497,7 +507,9 @@ def run_ours(args):
 
     peaks, peak_kind = measured_peaks()
     hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
-    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    trace_ms = phases["traverse_ms"] / max(1, phases["queries"])  # k_trace's mean launch duration
+    achieved = alg_bytes / (trace_ms / 1e3) / 1e9
+    achieved_step = alg_bytes / (ms_per_step / 1e3) / 1e9
     dram_per_ray = profiled_dram_bytes_per_ray()
     traffic = dram_per_ray * n if dram_per_ray else None
     line = {
@@ -516,9 +528,13 @@ def run_ours(args):
                      "peak_source": f"hbm_gbs of {peak_kind}", "traffic": traffic,
                      "traffic_source": "ncu dram__bytes_read+write per ray of a 3.49M-ray capture, scaled by rays",
                      "bytes_per_ray": alg_bytes / n, "nodes_per_ray": nodes_total / n, "tris_per_ray": tris_total / n,
+                     "kernel": "k_trace (closest hit, reference intersector)", "kernel_ms": trace_ms,
+                     "order_ms": phases["order_ms"] / max(1, phases["queries"]),
+                     "frac_whole_step": achieved_step / hbm,
                      "note": "algorithmic bytes = 80 B/node + 48 B/triangle + 48 B ray+hit; the 37 MB BVH is "
-                             "L2-resident, so most node bytes are served by L2. Duration = the whole step: ray "
-                             "keys + radix sort of the visiting order + traversal (k_trace)"},
+                             "L2-resident, so most node bytes are served by L2. achieved = those bytes over "
+                             "k_trace's CUDA-event duration; frac_whole_step also counts the ordering phase "
+                             "(ray keys + radix sort of the visiting order)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * RAY_BYTES,
                 "d2h_bytes_per_step": n * HIT_BYTES, "steps": e2e_steps,
                 "api": "myrt_trace_closest (host pinned buffers, chunked copy/compute overlap)"},
@@ -534,7 +550,8 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_guiding:
         del rays, hits
         torch.cuda.empty_cache()
-        line["guiding"] = guiding_run(local, res=512, oracle_spp=4096, budget_spp=256)
+        line["guiding"] = guiding_run(local, res=512, oracle_spp=args.oracle_spp or 4096,
+                                      budget_spp=args.budget_spp or 256)
         line["guiding"]["note"] = ("reduced guided-vs-plain leg (512x512); the full configuration runs with "
                                    "--workload guiding")
     if rank == 0:
@@ -557,19 +574,21 @@ def run_guiding_workload(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     with ClockSampler(local) as clocks:
-        g = guiding_run(local, res=1024, oracle_spp=4096, budget_spp=256)
+        g = guiding_run(local, res=args.res or 1024, oracle_spp=args.oracle_spp or 4096,
+                        budget_spp=args.budget_spp or 256)
     t_eq = g["guided_seconds_to_plain_rel_rmse"]
     value = g["speedup_rel_rmse"]
     line = {"metric": "time-to-equal-relRMSE speedup, guided vs plain PT", "value": value, "unit": "x",
             "n_gpus": 1, "steps": len(g["guided"]) + 1, "warmup": 1,
             "ms_per_step": (t_eq * 1e3) if t_eq else None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 (guide MLP bf16, fp32 accumulate)", "data": "synthetic",
-            "config": {"workload": "learned path guiding, " + GUIDE_SCENE, "res": 1024, "max_depth": 12,
-                       "oracle_spp": 4096, "plain_budget_spp": 256, "triangles": g["triangles"],
+            "config": {"workload": "learned path guiding, " + GUIDE_SCENE, "res": g["res"], "max_depth": 12,
+                       "oracle_spp": g["oracle"]["spp"], "plain_budget_spp": g["plain"]["spp"],
+                       "triangles": g["triangles"],
                        "l2": "scene and per-wave path state exceed L2"},
             "guiding": g,
             "e2e": {"value": value, "unit": "x", "h2d_bytes_per_step": 128,
-                    "d2h_bytes_per_step": 1024 * 1024 * 16,
+                    "d2h_bytes_per_step": g["res"] * g["res"] * 16,
                     "api": "myrt_render + myrt_read_accumulation (times include the image read-back)"},
             "clocks": clocks.summary()}
     print(json.dumps(line), flush=True)
@@ -620,15 +639,16 @@ def run_pt_workload(args):
     scene, lights = icosphere_field_lit()
     info = ctx.upload_scene(**scene)
     ctx.set_area_lights(lights)
-    W = H = 512
-    spp = 64
+    W = H = args.res or 512
+    spp = args.spp or 64
     iv, ip = look_at((0.0, 1.0, -4.5), (0.0, -0.3, 0.0), vfov_deg=50, aspect=1.0)
 
     def frame(seed=1, fp64=False, n=spp):
         ctx.render_physical(iv, ip, W, H, spp=n, max_depth=8, rr_start=3, seed=seed, fp64=fp64)
 
     ctx.reset_accumulation()
-    frame(fp64=True, n=1024, seed=999)
+    oracle_spp = args.oracle_spp or 1024
+    frame(fp64=True, n=oracle_spp, seed=999)
     ctx.sync()
     ref = ctx.read_accumulation_f64(W, H)
     ref = ref[..., :3] / ref[..., 3:4]
@@ -658,7 +678,7 @@ def run_pt_workload(args):
                      "512x512, 64 spp per step, depth 8, RR after 3, NEE + MIS", "triangles": int(info["triangles"]),
          "res": W, "spp_per_step": spp, "l2": "per-wave path state (4 Mi paths, ~1 GB) exceeds L2"},
         {"mrays_per_s": rays / (ms / 1e3) / 1e6, "rays_per_sample": rays / samples,
-         "rel_rmse_one_step_vs_fp64_1024spp": err_one,
+         f"rel_rmse_one_step_vs_fp64_{oracle_spp}spp": err_one,
          "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128,
                  "d2h_bytes_per_step": W * H * 16, "api": "myrt_render + myrt_read_accumulation"},
          "clocks": clocks.summary()})
@@ -769,8 +789,8 @@ def run_sdf_workload(args):
     dr = S.sdf_drawables([np.array([[1, 0, 0, 0.0], [0, 1, 0, -0.2], [0, 0, 1, 0.3], [0, 0, 0, 1]])], [0])
     ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)
     ctx.set_area_lights(lights)
-    W = H = 768
-    spp = 128
+    W = H = args.res or 768
+    spp = args.spp or 128
     iv, ip = look_at((0.0, 1.0, -4.5), (0.0, -0.3, 0.0), vfov_deg=50, aspect=1.0)
     ctx.guide_configure(**GUIDE_CFG)
     ctx.guide_reset()
@@ -779,7 +799,7 @@ def run_sdf_workload(args):
         ctx.render_physical(iv, ip, W, H, spp=n, max_depth=8, rr_start=rr, seed=seed, fp64=fp64, guided=guided,
                             sdf_marching_steps=256, sdf_marching_epsilon=1e-4)
 
-    oracle_spp = 512
+    oracle_spp = args.oracle_spp or 512
     ctx.reset_accumulation()
     frame(seed=999, fp64=True, n=oracle_spp, guided=False)
     ctx.sync()

@@ -172,6 +172,14 @@ int myrt_get_stream(myrt_ctx* ctx, void** stream);
 int myrt_set_tuning(myrt_ctx* ctx, const myrt_tuning* tuning);
 int myrt_get_tuning(myrt_ctx* ctx, myrt_tuning* tuning);
 
+/* Device-time accounting of the closest / any-hit queries (no counterpart in
+ * the reference): while enabled, each query records CUDA events around its
+ * ordering phase (ray keys + radix sort) and its traversal kernel.
+ * myrt_get_phase_times waits for the recorded queries, returns the summed
+ * milliseconds and the number of queries since the last call, and clears them. */
+int myrt_set_phase_timing(myrt_ctx* ctx, int enable);
+int myrt_get_phase_times(myrt_ctx* ctx, double* order_ms, double* traverse_ms, uint64_t* queries);
+
 /* ---- scene ---------------------------------------------------------------- */
 
 /* Replaces scene::prepare's buffer uploads (src/pathtracer/scene.cpp:330-409)

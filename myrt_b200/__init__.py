@@ -101,6 +101,18 @@ class Context:
                              wave_paths, pt_blocks_per_sm, trace_smem_stack, trace_order)
         self._check(self._L.myrt_set_tuning(self._h, C.byref(t)), "myrt_set_tuning")
 
+    def set_phase_timing(self, enable: bool = True):
+        """Device-time accounting of the ray queries (ordering, traversal)."""
+        self._check(self._L.myrt_set_phase_timing(self._h, int(enable)), "myrt_set_phase_timing")
+
+    def phase_times(self) -> dict:
+        """Summed device milliseconds of the queries since the last call: order_ms
+        (ray keys + radix sort), traverse_ms (traversal kernel), queries."""
+        o, t, q = C.c_double(), C.c_double(), C.c_uint64()
+        self._check(self._L.myrt_get_phase_times(self._h, C.byref(o), C.byref(t), C.byref(q)),
+                    "myrt_get_phase_times")
+        return dict(order_ms=o.value, traverse_ms=t.value, queries=q.value)
+
     def get_tuning(self) -> dict:
         t = _abi.myrt_tuning()
         self._check(self._L.myrt_get_tuning(self._h, C.byref(t)), "myrt_get_tuning")

@@ -158,6 +158,8 @@ SIGNATURES = {
     "myrt_batch_reset": (I, [P]),
     "myrt_batch_get_info": (I, [P, C.POINTER(myrt_batch_info)]),
     "myrt_batch_get_stats": (I, [P, C.POINTER(myrt_render_stats)]),
+    "myrt_set_phase_timing": (I, [P, C.c_int]),
+    "myrt_get_phase_times": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "myrt_batch_destroy": (I, [P]),
     "myrt_guide_configure": (I, [P, C.POINTER(myrt_guide_params)]),
     "myrt_guide_get_config": (I, [P, C.POINTER(myrt_guide_params)]),

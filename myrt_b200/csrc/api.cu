@@ -176,10 +176,27 @@ int launch_trace(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool st
   if (a.n == 0) return MYRT_OK;
   uint32_t const mode = ctx->tuning.trace_order;
   bool const sorted = mode == 2 || (mode == 0 && a.n >= kOrderMin);
-  if (!sorted) return launch_trace_kernels(ctx, a, intersector, any, stats, s);
-  int rc = order_rays(ctx, a, lane, s);
+  std::array<cudaEvent_t, 3> ev{};
+  if (ctx->time_phases) {
+    if (ctx->phase_pool.empty()) {
+      for (auto& e : ev) {
+        int rc = check_cuda(ctx, cudaEventCreate(&e), "phase timing event");
+        if (rc) return rc;
+      }
+    } else {
+      ev = ctx->phase_pool.back();
+      ctx->phase_pool.pop_back();
+    }
+    cudaEventRecord(ev[0], s);
+  }
+  int rc = sorted ? order_rays(ctx, a, lane, s) : MYRT_OK;
+  if (ctx->time_phases) cudaEventRecord(ev[1], s);
   if (!rc) rc = launch_trace_kernels(ctx, a, intersector, any, stats, s);
-  if (!rc) rc = check_cuda(ctx, cudaEventRecord(ctx->order[lane].done, s), "ray order record");
+  if (ctx->time_phases) {
+    cudaEventRecord(ev[2], s);
+    ctx->phase_pending.push_back(ev);
+  }
+  if (!rc && sorted) rc = check_cuda(ctx, cudaEventRecord(ctx->order[lane].done, s), "ray order record");
   return rc;
 }
 
@@ -401,6 +418,9 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
     free_order(o);
     if (o.done) cudaEventDestroy(o.done);
   }
+  for (auto* list : {&ctx->phase_pending, &ctx->phase_pool})
+    for (auto& ev : *list)
+      for (auto e : ev) cudaEventDestroy(e);
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_next);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -423,6 +443,32 @@ int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;
+}
+
+int myrt_set_phase_timing(myrt_ctx* ctx, int enable) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  ctx->time_phases = enable != 0;
+  return MYRT_OK;
+}
+
+int myrt_get_phase_times(myrt_ctx* ctx, double* order_ms, double* traverse_ms, uint64_t* queries) {
+  if (!ctx || !order_ms || !traverse_ms || !queries) return MYRT_ERR_INVALID_ARGUMENT;
+  double o = 0.0, t = 0.0;
+  int rc = MYRT_OK;
+  for (auto& ev : ctx->phase_pending) {
+    if (!rc) rc = check_cuda(ctx, cudaEventSynchronize(ev[2]), "phase timing");
+    float a = 0.f, b = 0.f;
+    if (!rc) rc = check_cuda(ctx, cudaEventElapsedTime(&a, ev[0], ev[1]), "phase timing");
+    if (!rc) rc = check_cuda(ctx, cudaEventElapsedTime(&b, ev[1], ev[2]), "phase timing");
+    o += a;
+    t += b;
+  }
+  *queries = ctx->phase_pending.size();
+  for (auto& ev : ctx->phase_pending) ctx->phase_pool.push_back(ev);
+  ctx->phase_pending.clear();
+  *order_ms = o;
+  *traverse_ms = t;
+  return rc;
 }
 
 int myrt_get_tuning(myrt_ctx* ctx, myrt_tuning* t) {

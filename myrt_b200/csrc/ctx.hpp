@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <array>
+
 #include <cstdint>
 #include <random>
 #include <string>
@@ -106,6 +108,9 @@ struct myrt_ctx {
     size_t cap = 0, temp_bytes = 0;
     cudaEvent_t done = nullptr;
   } order[2];
+  // phase timing of the ray queries: (before ordering, before traversal, after)
+  bool time_phases = false;
+  std::vector<std::array<cudaEvent_t, 3>> phase_pending, phase_pool;
 };
 
 namespace myrt_b200 {

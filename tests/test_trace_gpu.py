@@ -260,3 +260,24 @@ def test_ray_order_does_not_change_results(ctx, hf128, order):
         assert np.array_equal(d_t.cpu().numpy().astype(np.uint32), ct)
     finally:
         ctx.set_tuning()
+
+
+def test_phase_timing(ctx, hf128):
+    """Per-query device times of the ordering phase and the traversal kernel."""
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = pinhole_rays(1024, 1024)  # 1 Mi rays: sorted by default
+    ctx.set_phase_timing(True)
+    try:
+        ctx.phase_times()
+        ctx.trace_closest(rays)  # host path: input order
+        import torch
+
+        d_rays = torch.from_numpy(rays).cuda()
+        d_hits = torch.empty((rays.shape[0], 4), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.trace_closest_device(d_rays, d_hits)
+        t = ctx.phase_times()
+        assert t["queries"] == 2 and t["traverse_ms"] > 0 and t["order_ms"] > 0
+        assert ctx.phase_times()["queries"] == 0
+    finally:
+        ctx.set_phase_timing(False)
