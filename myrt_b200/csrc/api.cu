@@ -171,11 +171,13 @@ int order_rays(myrt_ctx* ctx, trace_args& a, int lane, cudaStream_t s) {
 int launch_trace_kernels(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s);
 
 // lane: the ray-order scratch to use (0 = the context's stream, 1 = its
-// second lane).
-int launch_trace(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s, int lane = 0) {
+// second lane). host_chunk: a chunk of a host-memory query, sorted only when
+// trace_order forces it.
+int launch_trace(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s, int lane = 0,
+    bool host_chunk = false) {
   if (a.n == 0) return MYRT_OK;
   uint32_t const mode = ctx->tuning.trace_order;
-  bool const sorted = mode == 2 || (mode == 0 && a.n >= kOrderMin);
+  bool const sorted = mode == 2 || (mode == 0 && !host_chunk && a.n >= kOrderMin);
   std::array<cudaEvent_t, 3> ev{};
   if (ctx->time_phases) {
     if (ctx->phase_pool.empty()) {
@@ -302,8 +304,7 @@ int host_query(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, void* out, size_
     else a.hits = reinterpret_cast<float4*>(d_out);
     // chunks stream through the copy engines, which bound this path: they are
     // traced in input order unless sorting is forced (trace_order 2)
-    rc = ctx->tuning.trace_order == 2 ? launch_trace(ctx, a, intersector, any, false, s, int(k & 1))
-                                      : launch_trace_kernels(ctx, a, intersector, any, false, s);
+    rc = launch_trace(ctx, a, intersector, any, false, s, int(k & 1), true);
     if (rc) return rc;
     rc = check_cuda(ctx,
         cudaMemcpyAsync(static_cast<char*>(out) + size_t(c0) * out_stride, d_out, size_t(cn) * out_stride,
