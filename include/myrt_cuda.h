@@ -151,6 +151,9 @@ typedef struct myrt_tuning {
                                 grid-stride extend / shade / shadow kernels (0 = 8) */
   uint32_t trace_smem_stack; /* one-thread-per-ray: 1 = traversal stack in shared memory
                                 (tree depth + 1 entries per ray), 0 = per-thread local memory */
+  uint32_t bvh_builder;      /* myrt_scene_upload: 0 = host binned SAH + SAH-optimal 8-wide collapse,
+                                1 = device linear BVH (Morton order, radix tree, 8-wide collapse on the
+                                GPU): milliseconds for millions of triangles, slower traversal */
   uint32_t trace_order;      /* visiting order of closest / any-hit batches: 0 = device-memory queries
                                 of at least 1 Mi rays sorted by origin and direction cell, host-memory
                                 queries in input order; 1 = input order; 2 = always sorted.
@@ -183,10 +186,15 @@ int myrt_get_phase_times(myrt_ctx* ctx, double* order_ms, double* traverse_ms, u
 /* ---- scene ---------------------------------------------------------------- */
 
 /* Replaces scene::prepare's buffer uploads (src/pathtracer/scene.cpp:330-409)
- * and the per-geometry bvh build (scene.cpp:43-71): builds the 8-wide BVH on
- * the host over all drawables (baked to world space) and uploads it. */
+ * and the per-geometry bvh build (scene.cpp:43-71): builds the 8-wide BVH over
+ * all drawables (baked to world space) on the host, or on the device when
+ * myrt_tuning.bvh_builder = 1, and keeps it in device memory. */
 int myrt_scene_upload(myrt_ctx* ctx, const myrt_scene_view* scene);
 int myrt_scene_bvh_info(myrt_ctx* ctx, myrt_bvh_info* info);
+/* Copies the scene's device tree to host memory: nodes (80 bytes each) and
+ * leaf-ordered triangles (48 bytes each), as counted by myrt_scene_bvh_info;
+ * either pointer may be null. Same layout as myrt_bvh8_copy. */
+int myrt_scene_copy_bvh(myrt_ctx* ctx, void* nodes, void* triangles);
 
 /* ---- ray queries ---------------------------------------------------------- */
 

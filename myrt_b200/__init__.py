@@ -96,10 +96,19 @@ class Context:
 
     def set_tuning(self, trace_persistent: int = 0, refill: int = 1, blocks_per_sm: int = 0,
                    trace_min_blocks: int = 0, trace_unit_steps: int = 0, wave_paths: int = 0,
-                   pt_blocks_per_sm: int = 0, trace_smem_stack: int = 0, trace_order: int = 0):
+                   pt_blocks_per_sm: int = 0, trace_smem_stack: int = 0, trace_order: int = 0,
+                   bvh_builder: int = 0):
         t = _abi.myrt_tuning(trace_persistent, refill, blocks_per_sm, trace_min_blocks, trace_unit_steps,
-                             wave_paths, pt_blocks_per_sm, trace_smem_stack, trace_order)
+                             wave_paths, pt_blocks_per_sm, trace_smem_stack, bvh_builder, trace_order)
         self._check(self._L.myrt_set_tuning(self._h, C.byref(t)), "myrt_set_tuning")
+
+    def scene_bvh(self):
+        """The scene's device tree: (nodes uint32 [N, 20], triangles float32 [T, 12])."""
+        info = self.bvh_info()
+        nodes = np.empty((int(info["wide_nodes"]), 20), np.uint32)
+        tris = np.empty((int(info["triangles"]), 12), np.float32)
+        self._check(self._L.myrt_scene_copy_bvh(self._h, nodes.ctypes.data, tris.ctypes.data), "myrt_scene_copy_bvh")
+        return nodes, tris
 
     def set_phase_timing(self, enable: bool = True):
         """Device-time accounting of the ray queries (ordering, traversal)."""

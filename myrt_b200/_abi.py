@@ -113,7 +113,7 @@ class myrt_tuning(C.Structure):
     _fields_ = [("trace_persistent", C.c_uint32), ("refill", C.c_uint32), ("blocks_per_sm", C.c_uint32),
                 ("trace_min_blocks", C.c_uint32), ("trace_unit_steps", C.c_uint32), ("wave_paths", C.c_uint32),
                 ("pt_blocks_per_sm", C.c_uint32), ("trace_smem_stack", C.c_uint32),
-                ("trace_order", C.c_uint32)]
+                ("bvh_builder", C.c_uint32), ("trace_order", C.c_uint32)]
 
 
 SHADE_REFERENCE = 0
@@ -158,6 +158,7 @@ SIGNATURES = {
     "myrt_batch_reset": (I, [P]),
     "myrt_batch_get_info": (I, [P, C.POINTER(myrt_batch_info)]),
     "myrt_batch_get_stats": (I, [P, C.POINTER(myrt_render_stats)]),
+    "myrt_scene_copy_bvh": (I, [P, P, P]),
     "myrt_set_phase_timing": (I, [P, C.c_int]),
     "myrt_get_phase_times": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "myrt_batch_destroy": (I, [P]),

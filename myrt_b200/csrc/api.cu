@@ -14,8 +14,10 @@
 
 #include "../../include/myrt_cuda.h"
 #include "bvh8.hpp"
+#include "bvh8_device.hpp"
 #include "ctx.hpp"
 #include "rayorder.cuh"
+#include "sdf_skip.hpp"
 #include "trace.cuh"
 
 namespace myrt_b200 {
@@ -440,7 +442,7 @@ int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
   if (!ctx || !t) return MYRT_ERR_INVALID_ARGUMENT;
   if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
       t->trace_unit_steps > 1 || (t->wave_paths != 0 && (t->wave_paths < 1024 || t->wave_paths > (1u << 28))) ||
-      t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2)
+      t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2 || t->bvh_builder > 1)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;
@@ -544,17 +546,45 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
     }
   }
 
+  bool const on_device = ctx->tuning.bvh_builder == 1;
   bvh8 tree;
-  try {
-    tree = build_bvh8(pos.data(), n_prims, nullptr, bvh8_build_options{});
-  } catch (std::exception const& e) {
-    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, std::string("bvh build: ") + e.what());
+  device_bvh8 dtree;
+  if (on_device) {
+    float* d_pos = nullptr;
+    rc = upload(ctx, &d_pos, pos.data(), pos.size(), "triangle upload");
+    if (rc) return rc;
+    char const* what = nullptr;
+    int const e = build_bvh8_device(d_pos, n_prims, ctx->stream, dtree, &what);
+    cudaFree(d_pos);
+    if (e) return check_cuda(ctx, cudaError_t(e > 0 ? e : cudaErrorInvalidValue), what ? what : "device BVH build");
+    if (dtree.wide_depth > MYRT_STACK_MAX) {
+      cudaFree(dtree.nodes);
+      cudaFree(dtree.tris);
+      return set_error(ctx, MYRT_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
+    }
+  } else {
+    try {
+      tree = build_bvh8(pos.data(), n_prims, nullptr, bvh8_build_options{});
+    } catch (std::exception const& e) {
+      return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, std::string("bvh build: ") + e.what());
+    }
+    if (tree.stats.wide_depth > MYRT_STACK_MAX)
+      return set_error(ctx, MYRT_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
   }
-  if (tree.stats.wide_depth > MYRT_STACK_MAX)
-    return set_error(ctx, MYRT_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
 
   device_scene& s = ctx->scene;
-  s.stats = tree.stats;
+  if (on_device) {
+    s.stats = bvh8_stats{};
+    s.stats.binary_nodes = dtree.binary_nodes;
+    s.stats.wide_nodes = dtree.n_nodes;
+    s.stats.leaf_slots = dtree.leaf_slots;
+    s.stats.triangles = dtree.n_tris;
+    s.stats.wide_depth = dtree.wide_depth;
+    s.stats.max_leaf_size = 4;
+    s.stats.build_seconds = dtree.seconds;
+  } else {
+    s.stats = tree.stats;
+  }
   float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (size_t i = 0; i < pos.size() / 3; ++i)
     for (int k = 0; k < 3; ++k) {
@@ -566,13 +596,20 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
     s.bounds[3 + k] = hi[k];
   }
   ctx->guide_generation++;  // a new scene invalidates what the guide learned
-  s.n_nodes = tree.nodes.size();
-  s.n_tris = tree.triangles.size();
   s.n_prims = n_prims;
-  rc = upload(ctx, reinterpret_cast<bvh8_node**>(&s.nodes), tree.nodes.data(), tree.nodes.size(), "node upload");
-  if (!rc)
-    rc = upload(ctx, reinterpret_cast<bvh8_triangle**>(&s.tris), tree.triangles.data(), tree.triangles.size(),
-        "triangle upload");
+  if (on_device) {
+    s.n_nodes = dtree.n_nodes;
+    s.n_tris = dtree.n_tris;
+    s.nodes = reinterpret_cast<uint4*>(dtree.nodes);
+    s.tris = dtree.tris;
+  } else {
+    s.n_nodes = tree.nodes.size();
+    s.n_tris = tree.triangles.size();
+    rc = upload(ctx, reinterpret_cast<bvh8_node**>(&s.nodes), tree.nodes.data(), tree.nodes.size(), "node upload");
+    if (!rc)
+      rc = upload(ctx, reinterpret_cast<bvh8_triangle**>(&s.tris), tree.triangles.data(), tree.triangles.size(),
+          "triangle upload");
+  }
   if (!rc && !nrm.empty()) rc = upload(ctx, &s.tri_normals, nrm.data(), nrm.size(), "normal upload");
   if (!rc && !uvs.empty()) rc = upload(ctx, &s.tri_uvs, uvs.data(), uvs.size(), "uv upload");
   if (!rc) rc = upload(ctx, &s.tri_material, mat.data(), mat.size(), "material index upload");
@@ -596,6 +633,7 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
   return MYRT_OK;
 }
 
+
 int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
   if (!ctx || !v) return MYRT_ERR_INVALID_ARGUMENT;
   int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -606,6 +644,8 @@ int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
   cudaFree(D.programs);
   cudaFree(D.params);
   cudaFree(D.drawables);
+  cudaFree(D.skip_sphere);
+  cudaFree(D.skip_next);
   D = device_sdf{};
   ctx->render.sample_counter = 0;
   if (v->drawable_count == 0) return MYRT_OK;
@@ -651,6 +691,9 @@ int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
     if (depth != 1 || pending_mod) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "SDF program leaves no single result");
     if (max_depth > 24) return set_error(ctx, MYRT_ERR_UNSUPPORTED, "SDF program stack deeper than 24");
   }
+  std::vector<float4> skip_sphere;
+  std::vector<int2> skip_next;
+  sdf_skip_tables(v, skip_sphere, skip_next);
   std::vector<float> dr(v->drawable_count * 36);
   for (size_t d = 0; d < v->drawable_count; ++d) {
     myrt_sdf_drawable const& s = v->drawables[d];
@@ -663,6 +706,10 @@ int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
     rc = upload(ctx, reinterpret_cast<myrt_sdf_program**>(&D.programs), v->programs, v->program_count, "SDF programs");
   if (!rc && v->param_count) rc = upload(ctx, &D.params, v->params, v->param_count, "SDF parameters");
   if (!rc) rc = upload(ctx, &D.drawables, dr.data(), dr.size(), "SDF drawables");
+  if (!rc && !skip_next.empty()) {
+    rc = upload(ctx, &D.skip_sphere, skip_sphere.data(), skip_sphere.size(), "SDF skip spheres");
+    if (!rc) rc = upload(ctx, &D.skip_next, skip_next.data(), skip_next.size(), "SDF skip groups");
+  }
   if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "SDF upload");
   if (rc) return rc;
   D.n_drawables = int(v->drawable_count);
@@ -676,6 +723,20 @@ int myrt_trace_sdf(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, int32_t step
   if (!rays || !out) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "null ray or output pointer");
   if (steps < 0 || !(eps > 0.f)) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "steps >= 0 and eps > 0 required");
   return trace_sdf_rays(ctx, rays, n, steps, eps, any_hit, rng_states, out);
+}
+
+int myrt_scene_copy_bvh(myrt_ctx* ctx, void* nodes, void* triangles) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  if (!ctx->scene.valid) return set_error(ctx, MYRT_ERR_NO_SCENE, "no scene uploaded");
+  int rc = MYRT_OK;
+  if (nodes)
+    rc = check_cuda(ctx, cudaMemcpyAsync(nodes, ctx->scene.nodes, ctx->scene.n_nodes * sizeof(bvh8_node),
+                             cudaMemcpyDeviceToHost, ctx->stream), "node read-back");
+  if (!rc && triangles)
+    rc = check_cuda(ctx, cudaMemcpyAsync(triangles, ctx->scene.tris, ctx->scene.n_tris * sizeof(bvh8_triangle),
+                             cudaMemcpyDeviceToHost, ctx->stream), "triangle read-back");
+  if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "BVH read-back");
+  return rc;
 }
 
 int myrt_scene_bvh_info(myrt_ctx* ctx, myrt_bvh_info* info) {

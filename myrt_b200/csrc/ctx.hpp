@@ -39,6 +39,11 @@ struct device_sdf {
   int2* programs = nullptr;
   float* params = nullptr;
   float* drawables = nullptr;  // 36 floats each
+  // per instruction: bounding sphere (centre, radius) of the group "modifiers,
+  // primitive, union / smooth union" that starts there, and (index after the
+  // group's operator, k bits); next 0 = not a skippable group start
+  float4* skip_sphere = nullptr;
+  int2* skip_next = nullptr;
   int n_drawables = 0;
   int n_programs = 0;
 };
@@ -92,7 +97,7 @@ struct myrt_ctx {
   myrt_b200::guide_state* guide = nullptr;  // learned proposal (guide.cu), created on first use
   uint64_t guide_generation = 0;            // bumped by scene uploads
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
-  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
   int sm_count = 0;
   uint32_t* d_next = nullptr;    // ring of ray counters for the persistent traversal
   uint32_t next_slot = 0;

@@ -49,6 +49,8 @@ struct sdf_dev {
   int n_drawables;
   int steps;
   float eps;
+  float4 const* skip_sphere;  // per instruction, or null (see map)
+  int2 const* skip_next;
 };
 
 __device__ __forceinline__ v3 abs3(v3 a) { return {fabsf(a.x), fabsf(a.y), fabsf(a.z)}; }
@@ -91,6 +93,16 @@ __device__ __forceinline__ float sd_menger(v3 p) {
 }
 
 // map(p) of program `prog`; load = g_do_load_materials (material draws from rng).
+//
+// Exact skipping (load == false only): a group "translations, primitive,
+// union or smooth union (k)" combines the running value d0 with the
+// primitive's distance d1. Its result is d0 itself, bit for bit, whenever
+// d1 >= d0 + k: then (d1 - d0) / k rounds to at least 1, h clamps to 1,
+// mix(d1, d0, 1) = d0 and k h (1 - h) = 0 (for a union, min(d0, d1) = d0).
+// The primitive's distance is at least |p - c| - R for its bounding sphere
+// (c, R), so the group is skipped when |p - c| >= d0 + k + R + margin, the
+// margin covering the rounding of both sides. Material loads (load == true)
+// evaluate every group: their operators draw from the random stream.
 __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load, rs::rng_t* rng, int& mat) {
   int2 const pr = __ldg(s.programs + prog);
   float dist[kStack];
@@ -98,8 +110,22 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
   int sp = 0;
   v3 pos = p;
   float const* G = s.params;
+  bool const skipping = !load && s.skip_next != nullptr;
+  float const margin = 1e-4f + 1e-6f * ((fabsf(p.x) + fabsf(p.y)) + fabsf(p.z));
 #pragma unroll 1
   for (int k = 0; k < pr.y; ++k) {
+    if (skipping) {
+      int2 const nx = __ldg(s.skip_next + pr.x + k);
+      if (nx.x > 0) {
+        float4 const b = __ldg(s.skip_sphere + pr.x + k);
+        float const thr = ((dist[sp - 1] + __int_as_float(nx.y)) + b.w) + margin;
+        float const qx = p.x - b.x, qy = p.y - b.y, qz = p.z - b.z;
+        if (thr <= 0.f || (qx * qx + qy * qy) + qz * qz >= thr * thr) {
+          k = nx.x - pr.x - 1;  // continue after the group's operator
+          continue;
+        }
+      }
+    }
     int2 const in = __ldg(s.instrs + pr.x + k);
     int const o = in.y;
     int m = mat;

@@ -59,7 +59,8 @@ struct scene_dev {
 
 sdfk::sdf_dev make_sdf_dev(myrt_ctx const* ctx, int steps, float eps) {
   device_sdf const& D = ctx->sdf;
-  return sdfk::sdf_dev{D.instrs, D.programs, D.params, D.drawables, D.n_drawables, steps, eps};
+  return sdfk::sdf_dev{D.instrs, D.programs, D.params, D.drawables, D.n_drawables, steps, eps, D.skip_sphere,
+      D.skip_next};
 }
 
 struct camera_dev {

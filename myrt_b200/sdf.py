@@ -134,9 +134,12 @@ def sdf_drawables(transforms, sdf_indices) -> np.ndarray:
     return out
 
 
-def random_sdf_field(n_prims: int = 256, k: float = 0.1, seed: int = 3, extent: float = 1.0) -> Node:
+def random_sdf_field(n_prims: int = 256, k: float = 0.1, seed: int = 3, extent: float = 1.0,
+                     chain: bool = False) -> Node:
     """Smooth union of n seeded spheres, boxes and tori (the SDF + mesh hybrid
-    configuration: 256 primitives, k = 0.1)."""
+    configuration: 256 primitives, k = 0.1). chain=False folds them as a
+    balanced tree, chain=True left to right (((p0 u p1) u p2) u ...), which
+    lets the evaluator skip every primitive far from the point exactly."""
     rng = np.random.default_rng(seed)
     nodes = []
     for i in range(n_prims):
@@ -150,6 +153,11 @@ def random_sdf_field(n_prims: int = 256, k: float = 0.1, seed: int = 3, extent: 
         else:
             p = torus(float(rng.uniform(0.05, 0.12)), float(rng.uniform(0.01, 0.04)), mat)
         nodes.append(translate(p, c))
+    if chain:
+        acc = nodes[0]
+        for nd in nodes[1:]:
+            acc = smooth_union(acc, nd, k)
+        return acc
     # balanced tree: depth log2(n), stack depth stays small
     while len(nodes) > 1:
         nxt = [smooth_union(nodes[i], nodes[i + 1], k) for i in range(0, len(nodes) - 1, 2)]

@@ -1,0 +1,127 @@
+"""Device BVH build (linear BVH + 8-wide collapse on the GPU, tuning
+bvh_builder = 1): every triangle exactly once and inside every quantised slot
+box on its path from the root (the condition for conservative culling; a
+child's own quantised boxes, rounded outwards on its own grid, may reach past
+its parent's), and ray answers bit-identical to the host-built
+tree's (closest-hit ties go to the smaller prim id, so answers do not depend on
+the tree); per-ray node / triangle counters equal the oracle's walk of the same
+device-built tree."""
+import numpy as np
+import pytest
+
+import myrt_b200 as mb
+import pyoracle as po
+from myrt_b200.scenes import heightfield, icosphere_camera_rays, icosphere_field, pinhole_rays
+
+pytestmark = pytest.mark.gpu
+
+
+def _slot_boxes(node):
+    """float64 [8, 2, 3] slot boxes (lo, hi) of one node (uint32 [20])."""
+    p = node[0:3].view(np.float32).astype(np.float64)
+    e = node[3].tobytes()
+    scale = np.array([2.0 ** (int(e[a]) - 127) for a in range(3)])
+    q = node[8:20].tobytes()
+    qlo = np.frombuffer(q[0:24], np.uint8).reshape(3, 8).astype(np.float64)
+    qhi = np.frombuffer(q[24:48], np.uint8).reshape(3, 8).astype(np.float64)
+    lo = p[:, None] + qlo * scale[:, None]
+    hi = p[:, None] + qhi * scale[:, None]
+    return np.stack([lo.T, hi.T], 1)
+
+
+def _check_tree(nodes, tris, n_prims):
+    prims = tris[:, 3].view(np.uint32)
+    assert np.array_equal(np.sort(prims), np.arange(n_prims, dtype=np.uint32))
+    seen = np.zeros(len(nodes), bool)
+    stack = [(0, (np.full(3, -np.inf), np.full(3, np.inf)))]
+    while stack:
+        ni, outer = stack.pop()
+        assert not seen[ni]
+        seen[ni] = True
+        nd = nodes[ni]
+        imask = int(nd[3] >> 24)
+        child_base, tri_base = int(nd[4]), int(nd[5])
+        meta = nd[6:8].tobytes()
+        boxes = _slot_boxes(nd)
+        rank = 0
+        for s in range(8):
+            m = meta[s]
+            if m == 0:
+                continue
+            lo, hi = np.maximum(boxes[s][0], outer[0]), np.minimum(boxes[s][1], outer[1])
+            if imask & (1 << s):
+                stack.append((child_base + rank, (lo, hi)))
+                rank += 1
+            else:
+                off, cnt = m & 31, m >> 5
+                assert 1 <= cnt <= 4
+                v = tris[tri_base + off: tri_base + off + cnt][:, [0, 1, 2, 4, 5, 6, 8, 9, 10]].reshape(-1, 3)
+                assert np.all(v.astype(np.float64) >= lo) and np.all(v.astype(np.float64) <= hi)
+    assert seen.all()
+
+
+def _rand_rays(n, seed, lo=-1.3, hi=1.3):
+    rng = np.random.default_rng(seed)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = rng.uniform(lo, hi, (n, 3))
+    d = rng.normal(size=(n, 3))
+    r[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    r[:, 7] = np.inf
+    r[::11, 7] = rng.uniform(0.05, 1.0, r[::11].shape[0])
+    return r
+
+
+@pytest.mark.parametrize("n", [1, 3, 5, 40, 128])
+def test_device_build_heightfield(ctx, n):
+    idx, pts = heightfield(n, seed=3) if n > 3 else (np.arange(3 * n, dtype=np.uint32),
+                                                     np.random.default_rng(n).uniform(-1, 1, (3 * n, 3)).astype(
+                                                         np.float32))
+    tris9 = pts[idx.reshape(-1, 3)].reshape(-1, 9)
+    hn, ht, _ = mb.build_bvh8(tris9)
+    rays = np.concatenate([pinhole_rays(96, 96), _rand_rays(20_000, seed=n)])
+    host, _, _ = po.bvh8_traverse(hn, ht, rays)
+    try:
+        ctx.set_tuning(bvh_builder=1)
+        info = ctx.upload_scene(idx, pts)
+        nodes, tris = ctx.scene_bvh()
+        assert info["triangles"] == tris9.shape[0] and info["wide_depth"] >= 1
+        _check_tree(nodes, tris, tris9.shape[0])
+        dev_walk, cn, ct = po.bvh8_traverse(nodes, tris, rays)
+        assert np.array_equal(dev_walk, host)
+        got = ctx.trace_closest(rays)
+        assert np.array_equal(got, host)
+        assert np.array_equal(ctx.trace_any(rays).astype(bool), host["prim"] >= 0)
+        import torch
+
+        d_rays = torch.from_numpy(rays).cuda()
+        d_hits = torch.empty((rays.shape[0], 4), dtype=torch.float32, device="cuda")
+        d_n = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        d_t = torch.empty(rays.shape[0], dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.trace_closest_stats_device(d_rays, d_hits, d_n, d_t)
+        ctx.sync()
+        assert np.array_equal(d_n.cpu().numpy().astype(np.uint32), cn)
+        assert np.array_equal(d_t.cpu().numpy().astype(np.uint32), ct)
+    finally:
+        ctx.set_tuning()
+
+
+def test_device_build_instanced_spheres(ctx):
+    """The 655,872-triangle instanced scene: device-built tree, same answers as
+    the host-built tree on camera and random rays."""
+    s = icosphere_field()
+    try:
+        ctx.set_tuning(bvh_builder=1)
+        info = ctx.upload_scene(**s)
+        assert info["triangles"] == 655_872
+        nodes, tris = ctx.scene_bvh()
+        prims = np.sort(tris[:, 3].view(np.uint32))
+        assert np.array_equal(prims, np.arange(655_872, dtype=np.uint32))
+        tris9 = po.bake_world_triangles(s["indices"], s["vertices"], s["drawables"])
+        rays = np.concatenate([icosphere_camera_rays(256, 256), _rand_rays(60_000, seed=5, lo=-1.1, hi=1.1)])
+        hn, ht, _ = mb.build_bvh8(tris9)
+        host, _, _ = po.bvh8_traverse(hn, ht, rays)
+        assert np.array_equal(ctx.trace_closest(rays), host)
+        assert np.array_equal(ctx.trace_any(rays).astype(bool), host["prim"] >= 0)
+    finally:
+        ctx.set_tuning()

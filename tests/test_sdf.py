@@ -107,3 +107,52 @@ def test_sdf_upload_rejects_bad_programs(ctx):
             ctx.upload_sdf(ins, prs, par, dr)
     with pytest.raises(mb.MyrtError):  # drawable references a missing program
         ctx.upload_sdf(np.array([[S.SPHERE, 0]]), np.array([[0, 1]]), np.zeros(2), S.sdf_drawables([np.eye(4)], [3]))
+
+
+@pytest.mark.gpu
+def test_sdf_exact_skipping_matches_oracle(ctx):
+    """Left-to-right unions and smooth unions of translated spheres, boxes, tori
+    and capsules: the device skips groups far from the point (bounding-sphere
+    test); hits, t, normals and materials stay bit-identical to the oracle,
+    which evaluates every primitive."""
+    rng = np.random.default_rng(12)
+    prims = []
+    for i in range(96):
+        kind = i % 4
+        mat = int(rng.integers(0, 4))
+        if kind == 0:
+            p = S.sphere(float(rng.uniform(0.03, 0.12)), mat)
+        elif kind == 1:
+            p = S.box(tuple(rng.uniform(0.02, 0.1, 3)), mat)
+        elif kind == 2:
+            p = S.torus(float(rng.uniform(0.05, 0.12)), float(rng.uniform(0.01, 0.04)), mat)
+        else:
+            p = S.vertical_capsule(float(rng.uniform(0.0, 0.2)), float(rng.uniform(0.02, 0.05)), mat)
+        prims.append(S.translate(p, rng.uniform(-0.8, 0.8, 3)))
+    acc = prims[0]
+    for i, nd in enumerate(prims[1:]):
+        acc = S.union(acc, nd) if i % 3 == 0 else S.smooth_union(acc, nd, 0.1)
+    lib = S.SdfLibrary()
+    lib.add(acc)
+    lib.add(S.random_sdf_field(128, k=0.1, seed=4, chain=True))
+    dr = S.sdf_drawables([np.eye(4), np.array([[1, 0, 0, 0.3], [0, 1, 0, 0], [0, 0, 1, 0.2], [0, 0, 0, 1]])], [0, 1])
+    n = 6144
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, 0:3] = np.array([0.0, 0.2, -3.0])
+    aim = rng.uniform(-0.3, 0.3, (n, 3)) + np.array([0.0, 0.0, 1.0])
+    rays[:, 4:7] = aim / np.linalg.norm(aim, axis=1, keepdims=True)
+    rays[:, 7] = np.inf
+    states = rng.integers(1, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)
+    try:
+        for anyh in (False, True):
+            got = ctx.trace_sdf(rays, 256, 1e-4, any_hit=anyh, rng_states=states)
+            ora = po.sdf_trace(lib, dr, rays, 256, 1e-4, anyh, states)
+            assert got["hit"].sum() > 500
+            assert np.array_equal(got["hit"], ora["hit"])
+            assert np.array_equal(got["t"], ora["t"])
+            if not anyh:
+                assert np.array_equal(got["normal"], ora["normal"])
+                assert np.array_equal(got["material"], ora["material"])
+    finally:
+        ctx.upload_sdf(np.zeros((0, 2)), np.zeros((0, 2)), np.zeros(0), np.zeros((0, 36)))
