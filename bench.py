@@ -555,8 +555,14 @@ def run_ours(args):
         ctx.trace_closest_device(rays, hits, stream=s)
     end.record(stream)
     torch.cuda.synchronize()
+    t_set = []
+    for _ in range(3):  # instance update: re-bake on the device + device rebuild
+        t0 = time.perf_counter()
+        ctx.set_transforms(scene["drawables"])
+        t_set.append(time.perf_counter() - t0)
     line["bvh_device_build"] = {
         "build_s": round(float(dinfo["build_seconds"]), 4), "host_build_s": round(float(info["build_seconds"]), 3),
+        "set_transforms_s": round(min(t_set), 4),
         "wide_nodes": int(dinfo["wide_nodes"]), "wide_depth": int(dinfo["wide_depth"]),
         "mrays_per_s": n * 3 / (start.elapsed_time(end) / 1e3) / 1e6,
         "note": "the same query step on a tree built by the device builder (bvh_builder 1) instead of the host "

@@ -191,6 +191,13 @@ int myrt_get_phase_times(myrt_ctx* ctx, double* order_ms, double* traverse_ms, u
  * myrt_tuning.bvh_builder = 1, and keeps it in device memory. */
 int myrt_scene_upload(myrt_ctx* ctx, const myrt_scene_view* scene);
 int myrt_scene_bvh_info(myrt_ctx* ctx, myrt_bvh_info* info);
+/* Moves instances (scene.cpp:336-344 rebuilds the reference's TLAS on the host
+ * whenever an instance changes): new transformation, inverse_transformation
+ * and material_index for every drawable of the uploaded scene (same count and
+ * index ranges as uploaded). Re-bakes the world triangles and normals on the
+ * device from the object-space geometry kept since the upload and rebuilds the
+ * tree with the device builder; restarts accumulation. */
+int myrt_scene_set_transforms(myrt_ctx* ctx, const myrt_drawable* drawables, size_t count);
 /* Copies the scene's device tree to host memory: nodes (80 bytes each) and
  * leaf-ordered triangles (48 bytes each), as counted by myrt_scene_bvh_info;
  * either pointer may be null. Same layout as myrt_bvh8_copy. */

@@ -102,6 +102,14 @@ class Context:
                              wave_paths, pt_blocks_per_sm, trace_smem_stack, bvh_builder, trace_order)
         self._check(self._L.myrt_set_tuning(self._h, C.byref(t)), "myrt_set_tuning")
 
+    def set_transforms(self, drawables):
+        """myrt_scene_set_transforms: new transforms / material indices for the
+        uploaded drawables (a ctypes array of myrt_drawable); re-bake and rebuild
+        on the device. Returns bvh_info()."""
+        self._check(self._L.myrt_scene_set_transforms(self._h, C.cast(drawables, C.c_void_p), len(drawables)),
+                    "myrt_scene_set_transforms")
+        return self.bvh_info()
+
     def scene_bvh(self):
         """The scene's device tree: (nodes uint32 [N, 20], triangles float32 [T, 12])."""
         info = self.bvh_info()

@@ -159,6 +159,7 @@ SIGNATURES = {
     "myrt_batch_get_info": (I, [P, C.POINTER(myrt_batch_info)]),
     "myrt_batch_get_stats": (I, [P, C.POINTER(myrt_render_stats)]),
     "myrt_scene_copy_bvh": (I, [P, P, P]),
+    "myrt_scene_set_transforms": (I, [P, P, C.c_size_t]),
     "myrt_set_phase_timing": (I, [P, C.c_int]),
     "myrt_get_phase_times": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "myrt_batch_destroy": (I, [P]),

@@ -36,6 +36,9 @@ int check_cuda(myrt_ctx* ctx, cudaError_t e, char const* what) {
 namespace {
 
 void free_scene(device_scene& s) {
+  cudaFree(s.raw_vertices);
+  cudaFree(s.raw_normals);
+  cudaFree(s.prim_src);
   cudaFree(s.nodes);
   cudaFree(s.tris);
   cudaFree(s.tri_normals);
@@ -514,11 +517,13 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
   if (n_prims >= (size_t(1) << 31)) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "too many triangles");
 
   std::vector<float> pos(9 * n_prims);
+  std::vector<uint4> src(n_prims);
   std::vector<float4> nrm(v->normals ? 3 * n_prims : 0);
   std::vector<float2> uvs(v->uvs ? 3 * n_prims : 0);
   std::vector<int32_t> mat(n_prims);
   size_t p = 0;
-  for (auto const& d : drawables) {
+  for (size_t di = 0; di < drawables.size(); ++di) {
+    myrt_drawable const& d = drawables[di];
     bool const ident = is_identity(d.transformation);
     // normal matrix = mat3(transpose(inverse_transformation)) (pt_trace.comp:372)
     float nm[9];
@@ -526,9 +531,11 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
       for (int c = 0; c < 3; ++c) nm[c * 3 + r] = d.inverse_transformation[r * 4 + c];
     for (uint32_t t = 0; t < d.index_count / 3; ++t, ++p) {
       mat[p] = d.material_index;
+      src[p].w = uint32_t(di);
       for (int k = 0; k < 3; ++k) {
         size_t const vi = size_t(d.points_base_index) + v->indices[d.indices_base_index + 3 * t + k];
         if (vi >= v->vertex_count) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "vertex index out of range");
+        (&src[p].x)[k] = uint32_t(vi);
         float const* src = v->vertices + 4 * vi;
         float* dst = &pos[9 * p + 3 * k];
         if (ident) std::memcpy(dst, src, 12);
@@ -611,6 +618,14 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
           "triangle upload");
   }
   if (!rc && !nrm.empty()) rc = upload(ctx, &s.tri_normals, nrm.data(), nrm.size(), "normal upload");
+  // object-space geometry for transform updates
+  if (!rc)
+    rc = upload(ctx, &s.raw_vertices, reinterpret_cast<float4 const*>(v->vertices), v->vertex_count, "vertex upload");
+  if (!rc && v->normals)
+    rc = upload(ctx, &s.raw_normals, reinterpret_cast<float4 const*>(v->normals), v->vertex_count, "normal upload");
+  if (!rc) rc = upload(ctx, &s.prim_src, src.data(), src.size(), "prim source upload");
+  s.n_vertices = v->vertex_count;
+  s.drawables = drawables;
   if (!rc && !uvs.empty()) rc = upload(ctx, &s.tri_uvs, uvs.data(), uvs.size(), "uv upload");
   if (!rc) rc = upload(ctx, &s.tri_material, mat.data(), mat.size(), "material index upload");
   if (!rc && v->material_count) {

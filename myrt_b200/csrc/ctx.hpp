@@ -31,6 +31,13 @@ struct device_scene {
   bvh8_stats stats{};
   float bounds[6] = {0, 0, 0, 0, 0, 0};  // world AABB of the triangles (min xyz, max xyz)
   bool valid = false;
+  // object-space geometry kept for myrt_scene_set_transforms: vertices and
+  // normals as uploaded, per prim its three vertex indices and its drawable
+  float4* raw_vertices = nullptr;
+  float4* raw_normals = nullptr;
+  uint4* prim_src = nullptr;
+  size_t n_vertices = 0;
+  std::vector<myrt_drawable> drawables;
 };
 
 // SDF drawables (uploaded separately; scene::prepare's sdf buffers).

@@ -125,3 +125,56 @@ def test_device_build_instanced_spheres(ctx):
         assert np.array_equal(ctx.trace_any(rays).astype(bool), host["prim"] >= 0)
     finally:
         ctx.set_tuning()
+
+
+def _moved(drawables, seed):
+    """New transforms (rotation about y, scale, translation) and material
+    indices for every drawable of an instanced scene."""
+    from myrt_b200._abi import myrt_drawable
+
+    rng = np.random.default_rng(seed)
+    out = (myrt_drawable * len(drawables))()
+    for k, d in enumerate(drawables):
+        m = np.array(d.transformation[:], np.float64).reshape(4, 4).T
+        a = rng.uniform(0, 2 * np.pi)
+        rot = np.array([[np.cos(a), 0, np.sin(a), 0], [0, 1, 0, 0], [-np.sin(a), 0, np.cos(a), 0], [0, 0, 0, 1]])
+        mv = np.eye(4)
+        mv[:3, 3] = rng.uniform(-0.3, 0.3, 3)
+        m2 = mv @ m @ rot if k % 3 else m  # every third drawable keeps its transform
+        out[k] = d
+        out[k].transformation[:] = m2.T.astype(np.float32).ravel().tolist()
+        out[k].inverse_transformation[:] = np.linalg.inv(m2).T.astype(np.float32).ravel().tolist()
+        out[k].material_index = (d.material_index + k) % 7
+    return out
+
+
+def test_set_transforms_equals_reupload(ctx):
+    """Moving the instances on the device (re-bake + device rebuild) answers
+    rays and renders images exactly like uploading the moved scene again."""
+    from myrt_b200.camera import look_at
+    from myrt_b200.scenes import icosphere_field_lit
+
+    s, lights = icosphere_field_lit(n_spheres=48, subdiv=2, floor_cells=4, seed=8)
+    moved = _moved(s["drawables"], seed=3)
+    rays = np.concatenate([icosphere_camera_rays(160, 120), _rand_rays(30_000, seed=6, lo=-1.2, hi=1.2)])
+    iv, ip = look_at((0, 1, -4.5), (0, -0.3, 0), vfov_deg=50, aspect=4 / 3)
+    ctx.upload_scene(**s)
+    ctx.set_area_lights(lights)
+    info = ctx.set_transforms(moved)
+    assert info["triangles"] == sum(d.index_count for d in moved) // 3
+    got = ctx.trace_closest(rays)
+    got_any = ctx.trace_any(rays)
+    ctx.render_physical(iv, ip, 64, 48, spp=4, max_depth=5, seed=2)
+    img, _ = ctx.read_accumulation(64, 48)
+    ctx.upload_scene(**dict(s, drawables=moved))
+    ref = ctx.trace_closest(rays)
+    assert np.array_equal(got, ref)
+    assert np.array_equal(got_any, ctx.trace_any(rays))
+    ctx.render_physical(iv, ip, 64, 48, spp=4, max_depth=5, seed=2)
+    ref_img, _ = ctx.read_accumulation(64, 48)
+    assert np.array_equal(img, ref_img)
+    # geometry changes are refused
+    bad = _moved(s["drawables"], seed=4)
+    bad[0].index_count -= 3
+    with pytest.raises(mb.MyrtError):
+        ctx.set_transforms(bad)
