@@ -510,6 +510,36 @@ int myrt_render_noalloc(myrt_ctx* ctx, const myrt_camera* camera, const myrt_ren
  * stopped at a limit since the last call (the error word is then cleared). */
 int myrt_sync(myrt_ctx* ctx);
 
+/* ---- post-processing (src/pathtracer/post_process.cpp, src/pt/pp_*.comp) ----
+ * One pass over device images (float RGBA, row-major). Every pass rounds its
+ * output to half precision, as the reference's RGBA16F targets do; texture
+ * reads follow the reference sampler (bilinear, mirrored repeat). Bloom, blur2d
+ * and the per-frame chain of main.cpp:840-875 are sequences of these passes
+ * (myrt_b200/post.py). */
+typedef enum myrt_pp_op {
+  MYRT_PP_DENOISE = 0, /* pp_denoise.comp (denoise): p[0] exponent (spatial sigma), p[1] strength (range sigma) */
+  MYRT_PP_BLUR = 1,    /* pp_blur.comp (blur): i[0] direction (0 = x, 1 = y), p[0] step */
+  MYRT_PP_CUTOFF = 2,  /* pp_cutoff.comp (cutoff): p[0..3] value, i[0] leave_above */
+  MYRT_PP_ADD = 3,     /* pp_add.comp (add): p[0] factor; the overlay image is sampled */
+  MYRT_PP_TONEMAP = 4, /* pp_tonemap.comp / pp_tonemap_filmic.cl: filmic curve; i[0] = 1 sets alpha to 1 */
+  MYRT_PP_FXAA = 5,    /* pp_fxaa.comp (fxaa) */
+  MYRT_PP_SCALE = 6    /* linear_scale (post_process.cpp:112-127): bilinear resample to the output size */
+} myrt_pp_op;
+typedef struct myrt_pp_pass {
+  int32_t op; /* myrt_pp_op */
+  int32_t i[3];
+  float p[4];
+} myrt_pp_pass;
+typedef struct myrt_image {
+  float* rgba; /* device memory, width * height * 4 floats */
+  uint32_t width, height;
+} myrt_image;
+/* Runs one pass on `stream` (null: the context's stream). The output must
+ * have the input's size except for MYRT_PP_SCALE; `overlay` is used by
+ * MYRT_PP_ADD only. Input and output must not overlap. */
+int myrt_post_pass(myrt_ctx* ctx, const myrt_pp_pass* pass, const myrt_image* input, const myrt_image* overlay,
+    const myrt_image* output, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -65,6 +65,17 @@ class myrt_render_params(C.Structure):
                 ("wave_paths", C.c_uint32)]
 
 
+class myrt_pp_pass(C.Structure):
+    _fields_ = [("op", C.c_int32), ("i", C.c_int32 * 3), ("p", C.c_float * 4)]
+
+
+class myrt_image(C.Structure):
+    _fields_ = [("rgba", C.c_void_p), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
+PP_DENOISE, PP_BLUR, PP_CUTOFF, PP_ADD, PP_TONEMAP, PP_FXAA, PP_SCALE = range(7)
+
+
 class myrt_render_stats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("extension_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("reserved", C.c_uint64)]
@@ -160,6 +171,8 @@ SIGNATURES = {
     "myrt_batch_get_stats": (I, [P, C.POINTER(myrt_render_stats)]),
     "myrt_scene_copy_bvh": (I, [P, P, P]),
     "myrt_scene_set_transforms": (I, [P, P, C.c_size_t]),
+    "myrt_post_pass": (I, [P, C.POINTER(myrt_pp_pass), C.POINTER(myrt_image), C.POINTER(myrt_image),
+                           C.POINTER(myrt_image), P]),
     "myrt_set_phase_timing": (I, [P, C.c_int]),
     "myrt_get_phase_times": (I, [P, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
     "myrt_batch_destroy": (I, [P]),

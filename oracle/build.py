@@ -11,7 +11,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
-SRCS = [HERE / "oracle.cpp", HERE / "oracle_render.cpp"]
+SRCS = [HERE / "oracle.cpp", HERE / "oracle_render.cpp", HERE / "oracle_post.cpp"]
 FLAGS = ["-std=c++20", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fwrapv", "-fno-fast-math", "-pthread"]
 
 

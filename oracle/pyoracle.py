@@ -32,6 +32,8 @@ def oracle() -> C.CDLL:
         h = C.CDLL(str(ORACLE_LIB))
         sig = {
             "orc_isect_reference": (I, [P, P, P, P, P]),
+            "oracle_post_pass": (I, [I, P, P, P, I, I, P, I, I, P, I, I]),
+            "oracle_half_rn": (C.c_float, [C.c_float]),
             "orc_refbvh_build": (P, [P, SZ, P]),
             "orc_refbvh_free": (None, [P]),
             "orc_refbvh_node_count": (SZ, [P]),
@@ -437,3 +439,21 @@ def render_physical(scene: dict, width: int, height: int, spp: int, inv_view, in
                           env.ctypes.data, width, height, spp, sample0, max_depth, rr_start, seed, vp.ctypes.data,
                           eye.ctypes.data, *sdf_args, int(fp64), accum.ctypes.data, nthreads())
     return accum
+
+
+def post_pass(op: int, img: np.ndarray, i=(0, 0, 0), p=(0.0, 0.0, 0.0, 0.0), overlay: np.ndarray | None = None,
+              out_size: tuple[int, int] | None = None) -> np.ndarray:
+    """One post-processing pass on a float32 [H, W, 4] image (oracle_post.cpp)."""
+    L = oracle()
+    a = np.ascontiguousarray(img, np.float32)
+    h, w = a.shape[:2]
+    oh, ow = out_size if out_size else (h, w)
+    ov = np.ascontiguousarray(overlay if overlay is not None else a, np.float32)
+    out = np.empty((oh, ow, 4), np.float32)
+    ip = np.asarray(i, np.int32)
+    fp = np.asarray(p, np.float32)
+    rc = L.oracle_post_pass(int(op), ip.ctypes.data, fp.ctypes.data, a.ctypes.data, w, h, ov.ctypes.data,
+                            ov.shape[1], ov.shape[0], out.ctypes.data, ow, oh)
+    if rc:
+        raise ValueError(f"unknown post pass {op}")
+    return out
