@@ -55,11 +55,12 @@ def parse_args():
     p.add_argument("--budget-spp", type=int, default=None, help="guiding: plain spp budget (default 256)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=None)
-    p.add_argument("--workload", choices=["closest", "guiding", "pt", "batch", "sdf"], default="closest",
+    p.add_argument("--workload", choices=["closest", "guiding", "pt", "batch", "sdf", "post"], default="closest",
                    help="closest: closest-hit Mrays/s (with a reduced guided-vs-plain leg); guiding: the full "
                         "time-to-equal-relRMSE run (1024x1024, FP64 4096-spp oracle); pt: plain path tracing "
                         "of the icosphere scene (512x512, 64 spp, depth 8); batch: 16 uneven scenes in one "
-                        "CUDA graph per frame; sdf: SDF + mesh hybrid with guiding (768x768, 128 spp)")
+                        "CUDA graph per frame; sdf: SDF + mesh hybrid with guiding (768x768, 128 spp); post: the "
+                        "per-frame post-processing chain (bloom, tonemap, FXAA) and denoise on 2048x2048")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain leg of the closest workload")
     a = p.parse_args()
     if a.workload == "closest":
@@ -866,6 +867,87 @@ def run_sdf_workload(args):
     return 0
 
 
+def run_post_workload(args):
+    """Post-processing of a 2048x2048 HDR image: one step = main.cpp's frame
+    chain (scale 1, bloom = cutoff x2, scale 1/2, blur x, blur y, scale 2,
+    add; filmic tonemap; FXAA) plus one denoise pass. Reports Mpixels/s of the
+    input and the HBM roofline over the passes' image bytes (every pass reads
+    its input and writes its output once; taps beyond the first are served by
+    L1/L2)."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import torch
+
+    import myrt_b200 as mb
+    from myrt_b200 import post
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = mb.Context(local)
+    n = args.res or 2048
+    g = torch.Generator(device="cuda").manual_seed(3)
+    img = (torch.rand((n, n, 4), generator=g, device="cuda") * 2.0).half().float()
+    counted = {"bytes": 0}
+
+    def px(t):
+        return t.shape[0] * t.shape[1]
+
+    def step(count=False):
+        r = post.frame(ctx, img, super_sampling=1.0)
+        d = post.denoise(ctx, r)
+        if count:
+            h = n * n
+            q = px(post.scale(ctx, img, 0.5))
+            # scale, cutoff, cutoff (full), scale down, blur x2 (quarter), scale up, add (+ overlay), tonemap, fxaa,
+            # denoise: input + output bytes of each pass, 16 B per pixel
+            counted["bytes"] = 16 * (2 * h + 2 * h + 2 * h + (h + q) + 2 * q + 2 * q + (q + h) + (2 * h + h) + 2 * h +
+                                     2 * h + 2 * h)
+        return d
+
+    step(count=True)
+    for _ in range(args.warmup):
+        step()
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record(st)
+        for _ in range(args.steps):
+            step()
+        e1.record(st)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    # end to end: host image in, post-processed image out
+    h_in = img.cpu().pin_memory()
+    h_out = torch.empty((n, n, 4), dtype=torch.float32, pin_memory=True)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        x = h_in.to("cuda", non_blocking=True)
+        r = post.denoise(ctx, post.frame(ctx, x, super_sampling=1.0))
+        h_out.copy_(r, non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    ctx.close()
+    peaks, peak_kind = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    achieved = counted["bytes"] / (ms / 1e3) / 1e9
+    line = _render_line(
+        "Mpixels/s post-processing", n * n / (ms / 1e3) / 1e6, "Mpixels/s", args.steps, args.warmup, ms,
+        {"workload": f"{n}x{n} RGBA16F-range image: frame chain (bloom, filmic tonemap, FXAA) + denoise",
+         "passes": 11, "l2": f"{n * n * 16 / 1e6:.0f} MB per full-size image; the chain's images exceed L2"},
+        {"roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                      "peak_source": f"hbm_gbs of {peak_kind}", "traffic": None,
+                      "note": "algorithmic bytes = input + output image of every pass (16 B per pixel); denoise's "
+                              "81 taps and the blur's 62 bilinear taps per pixel are compute on cached data"},
+         "e2e": {"value": n * n / e2e_s / 1e6, "unit": "Mpixels/s", "h2d_bytes_per_step": n * n * 16,
+                 "d2h_bytes_per_step": n * n * 16, "api": "myrt_post_pass chain on torch's stream"},
+         "gpu_launches": 11,
+         "clocks": clocks.summary()})
+    line["dtype"] = "f32 (stored at f16 precision)"
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -878,6 +960,8 @@ def main():
         return run_batch_workload(args)
     if args.workload == "sdf":
         return run_sdf_workload(args)
+    if args.workload == "post":
+        return run_post_workload(args)
     return run_ours(args)
 
 

@@ -147,6 +147,34 @@ def material_codegen(src: str, type_name: str = "material") -> str:
     return f"thread_local {type_name} {type_name}_instance_;\n" + glsl_to_cpp(src)
 
 
+PP_SHADERS = ["pp_denoise", "pp_blur", "pp_cutoff", "pp_add", "pp_tonemap", "pp_fxaa"]
+
+
+def pp_to_cpp(name: str, src: str) -> str:
+    """A post-processing compute shader as C++ for ref_harness_post.cpp: the
+    #version line and the work-group layout go, `layout(...) uniform` /
+    `uniform` / `writeonly` qualifiers go (the harness sets the globals), main
+    becomes pp_main, swizzles become accessor calls (.rgb(), .xyz(), .xy();
+    .a reads .w), and pp_tonemap's one swizzle assignment is spelled out."""
+    src = re.sub(r"^#version.*$", "", src, flags=re.M)
+    src, n = re.subn(r"^layout\(local_size_x[^)]*\)\s*in\s*;", "", src, flags=re.M)
+    assert n == 1, f"{name}: work-group layout not found"
+    src = re.sub(r"layout\([^)]*\)\s*uniform\s+", "", src)
+    src = re.sub(r"\buniform\s+", "", src)
+    src = re.sub(r"\bwriteonly\s+", "", src)
+    src, n = re.subn(r"\bvoid\s+main\s*\(\s*\)", "void pp_main()", src)
+    assert n == 1, f"{name}: main not found"
+    if name == "pp_tonemap":
+        src, n = re.subn(r"color\.rgb\s*=\s*tonemap\(color\.rgb\);",
+                         "{ vec3 _t = tonemap(color.rgb()); color.x = _t.x; color.y = _t.y; color.z = _t.z; }", src)
+        assert n == 1, "pp_tonemap: swizzle assignment changed"
+    src = re.sub(r"\.rgb\b(?!\()", ".rgb()", src)
+    src = re.sub(r"\.xyz\b(?!\()", ".xyz()", src)
+    src = re.sub(r"\.xy\b(?!\()", ".xy()", src)
+    src = re.sub(r"\.a\b", ".w", src)
+    return glsl_to_cpp(src, globals_thread_local=False)
+
+
 def write_sources() -> None:
     (OUT / "src").mkdir(parents=True, exist_ok=True)
     (OUT / "glsl").mkdir(parents=True, exist_ok=True)
@@ -163,6 +191,8 @@ def write_sources() -> None:
     (OUT / "glsl/raymarch.glsl").write_text(raymarch_to_cpp((REF_ROOT / "src/pt/raymarch.glsl").read_text()))
     (OUT / "glsl/sdf_snippets.inc").write_text(
         extract_sdf_snippets((REF_ROOT / "src/pathtracer/sdf.hpp").read_text()))
+    for name in PP_SHADERS:
+        (OUT / "glsl" / f"{name}.inc").write_text(pp_to_cpp(name, (REF_ROOT / "src/pt" / f"{name}.comp").read_text()))
 
 
 def compile_ref() -> Path:
@@ -172,7 +202,7 @@ def compile_ref() -> Path:
     incs = ["-I", str(HERE / "shim"), "-I", str(REF_ROOT / "src/pathtracer"), "-I", str(REF_ROOT / "src"), "-I",
             str(OUT / "glsl"), "-I", str(HERE)]
     srcs = [str(OUT / "src/bvh.cpp"), str(REF_ROOT / "src/thread_pool.cpp"), str(HERE / "ref_harness_bvh.cpp"),
-            str(HERE / "ref_harness_glsl.cpp")]
+            str(HERE / "ref_harness_glsl.cpp"), str(HERE / "ref_harness_post.cpp")]
     cmd = ["g++", *flags, *incs, *srcs, "-o", str(lib)]
     subprocess.run(cmd, check=True)
     return lib

@@ -93,6 +93,7 @@ def ref() -> C.CDLL:
             "ref_glsl_material_eval": (None, [P, I, C.c_float, P, P, P, P, P]),
             "ref_sdf_map": (None, [P, P, P, I, P, SZ, I, P, P, P]),
             "ref_sdf_trace": (None, [P, P, P, P, I, P, SZ, I, C.c_float, I, P, P, P, P, P, P]),
+            "ref_post_pass": (I, [I, P, P, P, I, I, P, I, I, P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(h, k)
@@ -456,4 +457,21 @@ def post_pass(op: int, img: np.ndarray, i=(0, 0, 0), p=(0.0, 0.0, 0.0, 0.0), ove
                             ov.shape[1], ov.shape[0], out.ctypes.data, ow, oh)
     if rc:
         raise ValueError(f"unknown post pass {op}")
+    return out
+
+
+def ref_post_pass(op: int, img: np.ndarray, i=(0, 0, 0), p=(0.0, 0.0, 0.0, 0.0),
+                  overlay: np.ndarray | None = None) -> np.ndarray:
+    """The reference's own pp_*.comp shader (compiled in oracle/_ref) on a
+    float32 [H, W, 4] image."""
+    a = np.ascontiguousarray(img, np.float32)
+    h, w = a.shape[:2]
+    ov = np.ascontiguousarray(overlay if overlay is not None else a, np.float32)
+    out = np.zeros((h, w, 4), np.float32)
+    ip = np.asarray(i, np.int32)
+    fp = np.asarray(p, np.float32)
+    rc = ref().ref_post_pass(int(op), ip.ctypes.data, fp.ctypes.data, a.ctypes.data, w, h, ov.ctypes.data,
+                             ov.shape[1], ov.shape[0], out.ctypes.data)
+    if rc:
+        raise ValueError(f"no reference shader for post pass {op}")
     return out

@@ -229,10 +229,45 @@ def main() -> int:
         for k, v in res.items():
             sk[f"trace{anyh}_{k}"] = v
     np.savez_compressed(OUT / "sdf_kat.npz", **sk)
+    make_post_kat()
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
     return 0
 
 
+POST_CASES = [  # (name, op, i, p): the reference's post-processing shaders
+    ("denoise", 0, (0, 0, 0), (10.0, 0.05, 0.0, 0.0)),
+    ("denoise_wide", 0, (0, 0, 0), (2.0, 0.3, 0.0, 0.0)),
+    ("blur_x", 1, (0, 0, 0), (1.25, 0.0, 0.0, 0.0)),
+    ("blur_y", 1, (1, 0, 0), (2.5, 0.0, 0.0, 0.0)),
+    ("cutoff_above", 2, (1, 0, 0), (1.0, 1.0, 1.0, 1.0)),
+    ("cutoff_below", 2, (0, 0, 0), (0.5, 0.7, 0.9, 1.1)),
+    ("add", 3, (0, 0, 0), (0.3, 0.0, 0.0, 0.0)),
+    ("tonemap", 4, (0, 0, 0), (0.0, 0.0, 0.0, 0.0)),
+    ("fxaa", 5, (0, 0, 0), (0.0, 0.0, 0.0, 0.0)),
+]
+
+
+def make_post_kat() -> None:
+    """post_kat.npz: the reference's pp_*.comp shaders (compiled in oracle/_ref
+    with the GL-sampling shim of oracle/ref_harness_post.cpp) on seeded
+    RGBA16F images of odd sizes."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    rng = np.random.default_rng(31)
+    img = rng.uniform(0.0, 1.6, (37, 53, 4)).astype(np.float16).astype(np.float32)
+    ldr = rng.uniform(0.0, 1.0, (37, 53, 4)).astype(np.float16).astype(np.float32)
+    ov = rng.uniform(0.0, 2.0, (19, 27, 4)).astype(np.float16).astype(np.float32)
+    kat = dict(img=img, ldr=ldr, overlay=ov)
+    for name, op, i, p in POST_CASES:
+        src = ldr if op == 0 else img
+        kat[name] = po.ref_post_pass(op, src, i=i, p=p, overlay=ov if op == 3 else None)
+    np.savez_compressed(OUT / "post_kat.npz", **kat)
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 1 and sys.argv[1] == "post":
+        make_post_kat()
+        sys.exit(0)
     sys.exit(main())

@@ -33,6 +33,25 @@ def test_half_rounding_matches_numpy():
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
 
 
+POST_CASES = [("denoise", DENOISE, (0, 0, 0), (10.0, 0.05, 0.0, 0.0)),
+              ("denoise_wide", DENOISE, (0, 0, 0), (2.0, 0.3, 0.0, 0.0)),
+              ("blur_x", BLUR, (0, 0, 0), (1.25, 0.0, 0.0, 0.0)), ("blur_y", BLUR, (1, 0, 0), (2.5, 0.0, 0.0, 0.0)),
+              ("cutoff_above", CUTOFF, (1, 0, 0), (1.0, 1.0, 1.0, 1.0)),
+              ("cutoff_below", CUTOFF, (0, 0, 0), (0.5, 0.7, 0.9, 1.1)), ("add", ADD, (0, 0, 0), (0.3, 0.0, 0.0, 0.0)),
+              ("tonemap", TONEMAP, (0, 0, 0), (0.0, 0.0, 0.0, 0.0)), ("fxaa", FXAA, (0, 0, 0), (0.0, 0.0, 0.0, 0.0))]
+
+
+@pytest.mark.parametrize("name,op,i,p", POST_CASES)
+def test_oracle_matches_reference_shaders(golden, name, op, i, p):
+    """The restatement against the reference's own pp_*.comp shaders, compiled
+    as C++ (golden vectors from oracle/_ref; tests/golden/make_golden.py post):
+    bit-exact, the host libm on both sides."""
+    k = golden("post_kat.npz")
+    src = k["ldr"] if op == DENOISE else k["img"]
+    got = po.post_pass(op, src, i=i, p=p, overlay=k["overlay"] if op == ADD else None)
+    assert np.array_equal(got.view(np.uint32), k[name].view(np.uint32))
+
+
 def test_oracle_pass_properties():
     a = np.full((9, 13, 4), 0.5, np.float32)
     # the 31 blur weights sum to 1 within float rounding
