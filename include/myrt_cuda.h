@@ -333,7 +333,29 @@ typedef struct myrt_render_params {
   uint32_t accum_fp64;    /* 1: accumulate in FP64 (converged-oracle renders) */
   float env_radiance[3];  /* radiance of rays that leave the scene */
   uint32_t wave_paths;    /* paths in flight per wave (0: the context's tuning) */
+  /* reference mode: depth of field (pt_generate.comp:35-48, bokeh.glsl;
+   * sequential_pathtracer set_dof_enabled / set_lens_size / set_focus /
+   * set_bokeh_mask) */
+  int32_t dof_active;
+  float lens_size[2];
+  float focus;
+  int32_t bokeh_texture;  /* texture slot + 1 of the bokeh mask (0: none, value 1 everywhere) */
 } myrt_render_params;
+
+/* Textures for the reference shading mode (the bindless albedo textures of
+ * material_new.glsl:29-31 and the bokeh mask): slot < 256; rgba = width *
+ * height * 4 floats (host memory), sampled as GL samples them at level 0
+ * (GL_LINEAR; wrap 0 = GL_REPEAT, the reference's default, 1 = clamp to
+ * edge, 2 = mirrored repeat). A PBR material's texture field (floats 5 and 6
+ * of its 7) holds the handle as bits: (slot + 1, 0); (0, 0) = none. A null
+ * rgba or zero size empties the slot. */
+int myrt_texture_upload(myrt_ctx* ctx, uint32_t slot, const float* rgba, uint32_t width, uint32_t height,
+    uint32_t wrap);
+/* The environment cube map of pt_color.comp:190-199 (set_cubemap): 6 faces
+ * (+x, -x, +y, -y, +z, -z), size * size * 4 floats each, stored at half
+ * precision (the reference's RGB16F); size <= 10 (or 0) uses the sky
+ * gradient, as the reference does for small or missing maps. */
+int myrt_cubemap_upload(myrt_ctx* ctx, const float* faces_rgba, uint32_t size);
 
 /* Parallelogram area light corner + a*edge_u + b*edge_v, a, b in [0, 1],
  * emitting `emission` (radiance) on the side of cross(edge_u, edge_v). Used by

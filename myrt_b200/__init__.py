@@ -233,13 +233,35 @@ class Context:
     # -- wavefront rendering (sequential_pathtracer::run) --
     def render(self, inverse_view, inverse_projection, width: int, height: int, num_bounces: int = 10,
                frames: int = 1, shading: int = _abi.SHADE_REFERENCE, sdf_marching_steps: int = 400,
-               sdf_marching_epsilon: float = 1e-5):
+               sdf_marching_epsilon: float = 1e-5, dof: bool = False, lens_size=(0.2, 0.2), focus: float = 1.0,
+               bokeh_slot: int = -1):
         cam = _abi.myrt_camera()
         cam.inverse_view[:] = np.asarray(inverse_view, np.float32).ravel().tolist()
         cam.inverse_projection[:] = np.asarray(inverse_projection, np.float32).ravel().tolist()
         p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0, sdf_marching_steps,
                                     sdf_marching_epsilon)
+        p.dof_active = int(dof)
+        p.lens_size[:] = [float(lens_size[0]), float(lens_size[1])]
+        p.focus = float(focus)
+        p.bokeh_texture = bokeh_slot + 1 if bokeh_slot >= 0 else 0
         self._check(self._L.myrt_render(self._h, C.byref(cam), C.byref(p)), "myrt_render")
+
+    def upload_texture(self, slot: int, rgba, wrap: int = 0):
+        """myrt_texture_upload: rgba float32 [H, W, 4] (None empties the slot)."""
+        if rgba is None:
+            self._check(self._L.myrt_texture_upload(self._h, slot, None, 0, 0, wrap), "myrt_texture_upload")
+            return
+        a = np.ascontiguousarray(rgba, np.float32)
+        self._check(self._L.myrt_texture_upload(self._h, slot, a.ctypes.data, a.shape[1], a.shape[0], wrap),
+                    "myrt_texture_upload")
+
+    def upload_cubemap(self, faces):
+        """myrt_cubemap_upload: faces float32 [6, S, S, 4] (+x, -x, +y, -y, +z, -z); None removes it."""
+        if faces is None:
+            self._check(self._L.myrt_cubemap_upload(self._h, None, 0), "myrt_cubemap_upload")
+            return
+        a = np.ascontiguousarray(faces, np.float32)
+        self._check(self._L.myrt_cubemap_upload(self._h, a.ctypes.data, a.shape[1]), "myrt_cubemap_upload")
 
     def set_area_lights(self, lights):
         """myrt_set_area_lights: lights [n, 12] float32 rows (corner, edge_u,

@@ -62,7 +62,8 @@ class myrt_render_params(C.Structure):
                 ("shading", C.c_int32), ("flags", C.c_uint32), ("sdf_marching_steps", C.c_int32),
                 ("sdf_marching_epsilon", C.c_float), ("max_depth", C.c_int32), ("rr_start", C.c_int32),
                 ("seed", C.c_uint32), ("accum_fp64", C.c_uint32), ("env_radiance", C.c_float * 3),
-                ("wave_paths", C.c_uint32)]
+                ("wave_paths", C.c_uint32), ("dof_active", C.c_int32), ("lens_size", C.c_float * 2),
+                ("focus", C.c_float), ("bokeh_texture", C.c_int32)]
 
 
 class myrt_pp_pass(C.Structure):
@@ -170,6 +171,8 @@ SIGNATURES = {
     "myrt_batch_get_info": (I, [P, C.POINTER(myrt_batch_info)]),
     "myrt_batch_get_stats": (I, [P, C.POINTER(myrt_render_stats)]),
     "myrt_scene_copy_bvh": (I, [P, P, P]),
+    "myrt_texture_upload": (I, [P, U32, P, U32, U32, U32]),
+    "myrt_cubemap_upload": (I, [P, P, U32]),
     "myrt_scene_set_transforms": (I, [P, P, C.c_size_t]),
     "myrt_post_pass": (I, [P, C.POINTER(myrt_pp_pass), C.POINTER(myrt_image), C.POINTER(myrt_image),
                            C.POINTER(myrt_image), P]),

@@ -416,6 +416,7 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   cudaFree(ctx->sdf.params);
   cudaFree(ctx->sdf.drawables);
   free_render(ctx->render);
+  free_textures(ctx);
   free_physical(ctx->physical);
   free_guide(ctx->guide);
   ctx->guide = nullptr;

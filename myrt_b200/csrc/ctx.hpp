@@ -120,6 +120,16 @@ struct myrt_ctx {
     size_t cap = 0, temp_bytes = 0;
     cudaEvent_t done = nullptr;
   } order[2];
+  // reference-mode textures (slots) and environment cube map; d_textures
+  // mirrors `textures` as {float4*, w, h, wrap} records for the kernels
+  struct texture_slot {
+    float4* data = nullptr;
+    int w = 0, h = 0, wrap = 0;
+  };
+  std::vector<texture_slot> textures;
+  texture_slot* d_textures = nullptr;
+  float4* cubemap = nullptr;
+  int cubemap_size = 0;
   // phase timing of the ray queries: (before ordering, before traversal, after)
   bool time_phases = false;
   std::vector<std::array<cudaEvent_t, 3>> phase_pending, phase_pool;
@@ -129,6 +139,7 @@ namespace myrt_b200 {
 int set_error(myrt_ctx* ctx, int code, std::string msg);
 int check_cuda(myrt_ctx* ctx, cudaError_t e, char const* what);
 void free_render(render_state& r);
+void free_textures(myrt_ctx* ctx);
 void free_physical(physical_state& p);
 int ensure_images(myrt_ctx* ctx, uint32_t W, uint32_t H);
 int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p);

@@ -109,6 +109,13 @@ __device__ __forceinline__ float random_next(rng_t& r) {
   r.prime = r.prime == 5 ? 0 : r.prime + 1;
   return random_value(r, r.prime);
 }
+// random.glsl:77-85
+__device__ __forceinline__ v2 random_uniform_circle(rng_t& r, float radius) {
+  float const a = random_next(r) * 2.f * 3.1415926535897f;
+  float const b = random_next(r);
+  float const s = sqrtf(b) * radius;
+  return {s * sinf(a), s * cosf(a)};
+}
 
 // ---- ggx.glsl / pbr.glsl / transform.glsl ----------------------------------------
 constexpr float kPi = 3.1415926535897f;
@@ -167,6 +174,68 @@ struct matinfo {
   v3 color;
   float ior, roughness, metallic, transmission;
 };
+
+// ---- textures (the GL sampling of the reference's textures, level 0) ----------------
+// wrap: 0 GL_REPEAT, 1 GL_CLAMP_TO_EDGE, 2 GL_MIRRORED_REPEAT. GL_LINEAR:
+// texel coordinates u = s W - 1/2, weights from the fractional parts, summed
+// as ((w00 t00 + w10 t10) + w01 t01) + w11 t11.
+struct tex2d {
+  float4 const* p;
+  int w, h, wrap;
+};
+struct cubemap_dev {
+  float4 const* p;  // faces +x, -x, +y, -y, +z, -z, size * size texels each
+  int size;
+};
+__device__ __forceinline__ int wrap_texel(int i, int size, int mode) {
+  if (mode == 1) return i < 0 ? 0 : (i >= size ? size - 1 : i);
+  if (mode == 2) {
+    int m = i % (2 * size);
+    if (m < 0) m += 2 * size;
+    int const a = m - size;
+    return (size - 1) - (a >= 0 ? a : -(1 + a));
+  }
+  int m = i % size;
+  return m < 0 ? m + size : m;
+}
+__device__ __forceinline__ float4 bilinear_at(float4 const* p, int w, int h, int mode, float s, float t) {
+  float const u = s * float(w) - 0.5f, v = t * float(h) - 0.5f;
+  float const fu = floorf(u), fv = floorf(v);
+  float const a = u - fu, b = v - fv;
+  int const i0 = int(fu), j0 = int(fv);
+  int const x0 = wrap_texel(i0, w, mode), x1 = wrap_texel(i0 + 1, w, mode);
+  int const y0 = wrap_texel(j0, h, mode), y1 = wrap_texel(j0 + 1, h, mode);
+  float const w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
+  float4 const t00 = __ldg(p + size_t(y0) * w + x0), t10 = __ldg(p + size_t(y0) * w + x1);
+  float4 const t01 = __ldg(p + size_t(y1) * w + x0), t11 = __ldg(p + size_t(y1) * w + x1);
+  float4 r;
+  r.x = ((w00 * t00.x + w10 * t10.x) + w01 * t01.x) + w11 * t11.x;
+  r.y = ((w00 * t00.y + w10 * t10.y) + w01 * t01.y) + w11 * t11.y;
+  r.z = ((w00 * t00.z + w10 * t10.z) + w01 * t01.z) + w11 * t11.z;
+  r.w = ((w00 * t00.w + w10 * t10.w) + w01 * t01.w) + w11 * t11.w;
+  return r;
+}
+__device__ __forceinline__ float4 tex_sample(tex2d const& t, float s, float tt) {
+  return bilinear_at(t.p, t.w, t.h, t.wrap, s, tt);
+}
+// textureLod(samplerCube, dir, 0): the face of the major axis (GL 4.6 table
+// 8.19, ties to x, then y), s = (sc / |ma| + 1) / 2, t = (tc / |ma| + 1) / 2,
+// bilinear on that face with clamp to edge.
+__device__ __forceinline__ v3 cube_sample(cubemap_dev const& c, v3 d) {
+  float const ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  int face;
+  float sc, tc, ma;
+  if (ax >= ay && ax >= az) {
+    face = d.x >= 0.f ? 0 : 1, ma = ax, sc = d.x >= 0.f ? -d.z : d.z, tc = -d.y;
+  } else if (ay >= az) {
+    face = d.y >= 0.f ? 2 : 3, ma = ay, sc = d.x, tc = d.y >= 0.f ? d.z : -d.z;
+  } else {
+    face = d.z >= 0.f ? 4 : 5, ma = az, sc = d.z >= 0.f ? d.x : -d.x, tc = -d.y;
+  }
+  float const s = (sc / ma + 1.f) / 2.f, t = (tc / ma + 1.f) / 2.f;
+  float4 const r = bilinear_at(c.p + size_t(face) * c.size * c.size, c.size, c.size, 1, s, t);
+  return {r.x, r.y, r.z};
+}
 struct pbr_state_t {
   int state;
   bool after_sample;
@@ -258,6 +327,7 @@ struct material_ctx {
   int type;
   matinfo mat;
   pbr_state_t ps;
+  uint32_t tex_x, tex_y;  // albedo_texture handle: (slot + 1, 0), (0, 0) = none
 };
 __device__ __forceinline__ void mat_open(material_ctx& mc, int type, float const* data, int offset) {
   mc.type = type;
@@ -270,11 +340,22 @@ __device__ __forceinline__ void mat_open(material_ctx& mc, int type, float const
   mc.mat.roughness = __ldg(d + 2);
   mc.mat.metallic = __ldg(d + 3);
   mc.mat.transmission = __ldg(d + 4);
+  mc.tex_x = __float_as_uint(__ldg(d + 5));
+  mc.tex_y = __float_as_uint(__ldg(d + 6));
 }
-__device__ __forceinline__ void mat_evaluate(material_ctx& mc, v3 n, v3 tl, v3 tv, v3& refl, float& pdf) {
+// material_new.glsl:27-41. With an albedo texture the colour becomes
+// pow(texture(albedo, (u, 1 - v)), 2.2) (the context's texture slot tex_x - 1;
+// handles outside the table read no texture).
+__device__ __forceinline__ void mat_evaluate(material_ctx& mc, v3 n, v3 tl, v3 tv, v3& refl, float& pdf,
+    v2 uv = v2{0.f, 0.f}, tex2d const* textures = nullptr, int n_textures = 0) {
   refl = {0.f, 0.f, 0.f};
   pdf = 1.f;
   if (mc.type != 0) return;
+  if ((mc.tex_x != 0u || mc.tex_y != 0u) && mc.tex_y == 0u && mc.tex_x <= uint32_t(n_textures) && textures &&
+      textures[mc.tex_x - 1u].p) {
+    float4 const c = tex_sample(textures[mc.tex_x - 1u], uv.x, 1.f - uv.y);
+    mc.mat.color = {powf(c.x, 2.2f), powf(c.y, 2.2f), powf(c.z, 2.2f)};
+  }
   bool const incoming = dot(n, -tv) < 0.f;
   float const i1 = incoming ? 1.f : mc.mat.ior;
   float const i2 = incoming ? mc.mat.ior : 1.f;

@@ -66,6 +66,9 @@ sdfk::sdf_dev make_sdf_dev(myrt_ctx const* ctx, int steps, float eps) {
 struct camera_dev {
   float vp[16];  // inverse_view * inverse_projection (column major), computed on the host
   float eye[3];
+  int dof;       // pt_generate.comp dof_active
+  float lens[2], focus;
+  rs::tex2d bokeh;  // bokeh_shape; p = null (or width < 10) = no mask
 };
 
 struct light_t {
@@ -109,12 +112,39 @@ __global__ void __launch_bounds__(kBlock) k_generate(uint32_t W, uint32_t H, flo
 #pragma unroll
   for (int k = 0; k < 3; ++k)
     h[k] = ((cam.vp[0 * 4 + k] * nx + cam.vp[1 * 4 + k] * ny) + cam.vp[2 * 4 + k] * 1.f) + cam.vp[3 * 4 + k] * 1.f;
-  v3 const dir = rs::normalize(v3{h[0], h[1], h[2]});
+  v3 dir = rs::normalize(v3{h[0], h[1], h[2]});
+  v3 origin{cam.eye[0], cam.eye[1], cam.eye[2]};
+  v3 tint{1.f, 1.f, 1.f};
+  if (cam.dof) {
+    // bokeh.glsl:15-34 bokeh_get: the value is read at the previous offset,
+    // then a new offset is drawn (the returned offset was never sampled)
+    v2 offset = rs::random_uniform_circle(r, 0.49f);
+    v3 value{1.f, 1.f, 1.f};
+    float amount = 1.f;
+    if (cam.bokeh.p && cam.bokeh.w >= 10) {
+      int tries = 8;
+      while ((tries == 8 || amount < 1e-5f) && tries-- > 0) {
+        float4 const m = rs::tex_sample(cam.bokeh, 0.5f + offset.x, 0.5f + offset.y);
+        value = {m.x, m.y, m.z};
+        offset = rs::random_uniform_circle(r, 0.49f);
+        amount = rs::gmax(rs::gmax(value.x, value.y), value.z);
+      }
+    }
+    // pt_generate.comp:35-48 apply_bokeh
+    if (!(amount < 1e-5f)) {
+      v3 const center = origin + cam.focus * dir;
+      v3 const alt = rs::transform_local_to_world(
+          rs::normalize(v3{(offset.x * cam.lens[0]) / 2.f, (offset.y * cam.lens[1]) / 2.f, cam.focus}), dir);
+      tint = value;
+      origin = center - cam.focus * alt;
+      dir = alt;
+    }
+  }
   float const rv = rs::random_next(r);
   float4* g = gen + 5 * size_t(id);
-  g[0] = make_float4(cam.eye[0], cam.eye[1], cam.eye[2], rv);
+  g[0] = make_float4(origin.x, origin.y, origin.z, rv);
   g[1] = make_float4(dir.x, dir.y, dir.z, float(x));
-  g[2] = make_float4(1.f, 1.f, 1.f, float(y));
+  g[2] = make_float4(tint.x, tint.y, tint.z, float(y));
   g[3] = make_float4(0.f, 0.f, 0.f, 0.f);
   g[4] = make_float4(1.f, 1.f, 0.f, 0.f);
 }
@@ -247,6 +277,9 @@ struct color_args {
   uint32_t W;
   uint32_t sample_index;
   int force;
+  rs::tex2d const* textures;  // albedo textures by slot (material handle = slot + 1)
+  int n_textures;
+  rs::cubemap_dev cube;       // size <= 10: the sky gradient (pt_color.comp:190-199)
 };
 
 __device__ __forceinline__ bool naninf4(float4 v) {
@@ -307,7 +340,8 @@ __global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, float const
         v3 const generated = rs::mat_bounce(mc, r, v2{m0, m1}, -dir, normal);
         v3 mrefl;
         float mpdf;
-        rs::mat_evaluate(mc, normal, generated, -dir, mrefl, mpdf);
+        v2 const uv{t2.x, t2.y};
+        rs::mat_evaluate(mc, normal, generated, -dir, mrefl, mpdf, uv, a.textures, a.n_textures);
         float const rnd = rs::random_next(r);
         bool done = false;
         if (rnd > pdf0 * 1.f) {
@@ -330,7 +364,7 @@ __global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, float const
           if (t3.w > 0.f) {
             v3 lrefl{1.f, 1.f, 1.f};
             float lpdf = 1.f;
-            rs::mat_evaluate(mc, normal, xyz(t3), -dir, lrefl, lpdf);
+            rs::mat_evaluate(mc, normal, xyz(t3), -dir, lrefl, lpdf, uv, a.textures, a.n_textures);
             if (!rs::inf3(lrefl)) {
               v3 const lc = rs::unpack_rgb(__float_as_uint(t2.w));
               v3 const c = lc * t3.w * rs::clamp3(lrefl, 0.f, 1.f);
@@ -352,9 +386,14 @@ __global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, float const
       }
     } else {
       v3 const dir = xyz(g1);
-      float const t = (dir.y + 1.f) / 2.f;
-      v3 const sky = rs::mix3(v3{0.3f, 0.4f, 0.5f}, v3{1.f, 0.98f, 0.96f}, t);
-      v3 const env = rs::clamp3(refl0 * sky / pdf0, 0.f, 16.f);
+      v3 env;
+      if (a.cube.p && a.cube.size > 10) {
+        env = rs::clamp3(refl0 * rs::cube_sample(a.cube, dir) / pdf0, 0.f, 16.f);
+      } else {
+        float const t = (dir.y + 1.f) / 2.f;
+        v3 const sky = rs::mix3(v3{0.3f, 0.4f, 0.5f}, v3{1.f, 0.98f, 0.96f}, t);
+        env = rs::clamp3(refl0 * sky / pdf0, 0.f, 16.f);
+      }
       accumulate(a, make_float4(g3.x + env.x, g3.y + env.y, g3.z + env.z, g3.w), px, py);
     }
   }
@@ -535,11 +574,20 @@ int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_p
   cd.eye[0] = cam->inverse_view[12];
   cd.eye[1] = cam->inverse_view[13];
   cd.eye[2] = cam->inverse_view[14];
+  cd.dof = p->dof_active ? 1 : 0;
+  cd.lens[0] = p->lens_size[0];
+  cd.lens[1] = p->lens_size[1];
+  cd.focus = p->focus;
+  if (p->bokeh_texture > 0 && size_t(p->bokeh_texture) <= ctx->textures.size()) {
+    auto const& t = ctx->textures[size_t(p->bokeh_texture) - 1];
+    cd.bokeh = rs::tex2d{t.data, t.w, t.h, t.wrap};
+  }
   scene_dev sd{S.nodes, S.tris, S.tri_normals, S.tri_uvs, S.tri_material,
       reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err,
       make_sdf_dev(ctx, p->sdf_marching_steps, p->sdf_marching_epsilon)};
   color_args ca{reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, R.accum, R.display, W,
-      0, 0};
+      0, 0, reinterpret_cast<rs::tex2d const*>(ctx->d_textures), int(ctx->textures.size()),
+      rs::cubemap_dev{ctx->cubemap, ctx->cubemap_size}};
   size_t const n = size_t(W) * H;
   uint32_t const nb = uint32_t((n + kBlock - 1) / kBlock);
   cudaStream_t const st = ctx->stream;
@@ -763,3 +811,108 @@ int trace_sdf_rays(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, int steps, f
 }
 
 }  // namespace myrt_b200
+
+// ---- reference-mode textures and cube map ------------------------------------------------
+namespace myrt_b200 {
+namespace {
+float host_half_rn(float f) {
+  uint32_t x;
+  std::memcpy(&x, &f, 4);
+  uint32_t const sign = x & 0x80000000u, ax = x & 0x7fffffffu;
+  if (ax >= 0x7f800000u) return f;
+  uint32_t r;
+  if (ax >= 0x477ff000u) {
+    r = 0x7f800000u;
+  } else if (ax < 0x38800000u) {
+    float a;
+    std::memcpy(&a, &ax, 4);
+    float const q = std::nearbyint(a * 16777216.f) * (1.f / 16777216.f);
+    std::memcpy(&r, &q, 4);
+  } else {
+    r = (ax + 0x0fffu + ((ax >> 13) & 1u)) & ~0x1fffu;
+  }
+  r |= sign;
+  float out;
+  std::memcpy(&out, &r, 4);
+  return out;
+}
+
+int sync_texture_table(myrt_ctx* ctx) {
+  cudaFree(ctx->d_textures);
+  ctx->d_textures = nullptr;
+  if (ctx->textures.empty()) return MYRT_OK;
+  size_t const bytes = ctx->textures.size() * sizeof(myrt_ctx::texture_slot);
+  int rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->d_textures), bytes), "texture table");
+  if (!rc)
+    rc = check_cuda(ctx, cudaMemcpyAsync(ctx->d_textures, ctx->textures.data(), bytes, cudaMemcpyHostToDevice,
+                             ctx->stream), "texture table");
+  if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "texture table");
+  return rc;
+}
+}  // namespace
+
+void free_textures(myrt_ctx* ctx) {
+  for (auto& t : ctx->textures) cudaFree(t.data);
+  ctx->textures.clear();
+  cudaFree(ctx->d_textures);
+  ctx->d_textures = nullptr;
+  cudaFree(ctx->cubemap);
+  ctx->cubemap = nullptr;
+  ctx->cubemap_size = 0;
+}
+
+}  // namespace myrt_b200
+
+using namespace myrt_b200;
+
+extern "C" int myrt_texture_upload(myrt_ctx* ctx, uint32_t slot, float const* rgba, uint32_t width, uint32_t height,
+    uint32_t wrap) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  if (slot >= 256 || wrap > 2 || width > 16384 || height > 16384)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "texture slot < 256, wrap 0..2, sides <= 16384");
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc) return rc;
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->textures.size() <= slot) ctx->textures.resize(size_t(slot) + 1);
+  auto& t = ctx->textures[slot];
+  cudaFree(t.data);
+  t = myrt_ctx::texture_slot{};
+  if (rgba && width && height) {
+    size_t const bytes = size_t(width) * height * 16;
+    rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&t.data), bytes), "texture");
+    if (!rc) rc = check_cuda(ctx, cudaMemcpy(t.data, rgba, bytes, cudaMemcpyHostToDevice), "texture upload");
+    if (rc) {
+      cudaFree(t.data);
+      t = myrt_ctx::texture_slot{};
+      return rc;
+    }
+    t.w = int(width), t.h = int(height), t.wrap = int(wrap);
+  }
+  ctx->render.sample_counter = 0;
+  return sync_texture_table(ctx);
+}
+
+extern "C" int myrt_cubemap_upload(myrt_ctx* ctx, float const* faces, uint32_t size) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  if (size > 16384) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "cube map faces <= 16384 texels a side");
+  int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc) return rc;
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->cubemap);
+  ctx->cubemap = nullptr;
+  ctx->cubemap_size = 0;
+  ctx->render.sample_counter = 0;
+  if (!faces || size == 0) return MYRT_OK;
+  size_t const n = size_t(6) * size * size * 4;
+  std::vector<float> h(n);
+  for (size_t i = 0; i < n; ++i) h[i] = host_half_rn(faces[i]);  // RGB16F storage
+  rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&ctx->cubemap), n * 4), "cube map");
+  if (!rc) rc = check_cuda(ctx, cudaMemcpy(ctx->cubemap, h.data(), n * 4, cudaMemcpyHostToDevice), "cube map upload");
+  if (rc) {
+    cudaFree(ctx->cubemap);
+    ctx->cubemap = nullptr;
+    return rc;
+  }
+  ctx->cubemap_size = int(size);
+  return MYRT_OK;
+}

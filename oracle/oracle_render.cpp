@@ -283,6 +283,57 @@ inline void pbr_eval(pbr_state_t& ps, matinfo m, v3 tv, v3 tl, v3 n, float i1, f
   r.refl = r.refl * ps.resample;
 }
 
+// Textures of the reference mode, sampled as GL samples them at level 0
+// (GL_LINEAR, wrap 0 repeat / 1 clamp to edge / 2 mirrored repeat; weights
+// summed ((w00 t00 + w10 t10) + w01 t01) + w11 t11), and the cube map
+// (GL 4.6 table 8.19 face selection, ties to x then y, clamp to edge).
+struct tex_view {
+  float const* p = nullptr;  // rgba
+  int w = 0, h = 0, wrap = 0;
+};
+inline int wrap_texel(int i, int size, int mode) {
+  if (mode == 1) return i < 0 ? 0 : (i >= size ? size - 1 : i);
+  if (mode == 2) {
+    int m = i % (2 * size);
+    if (m < 0) m += 2 * size;
+    int const a = m - size;
+    return (size - 1) - (a >= 0 ? a : -(1 + a));
+  }
+  int m = i % size;
+  return m < 0 ? m + size : m;
+}
+inline v4 bilinear_at(float const* p, int w, int h, int mode, float s, float t) {
+  float const u = s * float(w) - 0.5f, v = t * float(h) - 0.5f;
+  float const fu = std::floor(u), fv = std::floor(v);
+  float const a = u - fu, b = v - fv;
+  int const i0 = int(fu), j0 = int(fv);
+  int const x0 = wrap_texel(i0, w, mode), x1 = wrap_texel(i0 + 1, w, mode);
+  int const y0 = wrap_texel(j0, h, mode), y1 = wrap_texel(j0 + 1, h, mode);
+  float const w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
+  float const* t00 = p + 4 * (std::size_t(y0) * w + x0);
+  float const* t10 = p + 4 * (std::size_t(y0) * w + x1);
+  float const* t01 = p + 4 * (std::size_t(y1) * w + x0);
+  float const* t11 = p + 4 * (std::size_t(y1) * w + x1);
+  float r[4];
+  for (int c = 0; c < 4; ++c) r[c] = ((w00 * t00[c] + w10 * t10[c]) + w01 * t01[c]) + w11 * t11[c];
+  return {r[0], r[1], r[2], r[3]};
+}
+inline v3 cube_sample(float const* faces, int size, v3 d) {
+  float const ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+  int face;
+  float sc, tc, ma;
+  if (ax >= ay && ax >= az) {
+    face = d.x >= 0.f ? 0 : 1, ma = ax, sc = d.x >= 0.f ? -d.z : d.z, tc = -d.y;
+  } else if (ay >= az) {
+    face = d.y >= 0.f ? 2 : 3, ma = ay, sc = d.x, tc = d.y >= 0.f ? d.z : -d.z;
+  } else {
+    face = d.z >= 0.f ? 4 : 5, ma = az, sc = d.z >= 0.f ? d.x : -d.x, tc = -d.y;
+  }
+  float const s = (sc / ma + 1.f) / 2.f, t = (tc / ma + 1.f) / 2.f;
+  v4 const r = bilinear_at(faces + std::size_t(face) * size * size * 4, size, size, 1, s, t);
+  return {r.x, r.y, r.z};
+}
+
 // material_new.glsl + generated dispatch (type 0 = PBR, 7 floats)
 struct material_ctx {
   int type = -1;
@@ -290,6 +341,7 @@ struct material_ctx {
   bool incoming = false;
   float ior1 = 1.f, ior2 = 1.f;
   pbr_state_t ps;
+  std::uint32_t tex_x = 0, tex_y = 0;  // albedo_texture handle (slot + 1, 0)
 };
 inline std::uint32_t fbits(float f) {
   std::uint32_t u;
@@ -305,11 +357,21 @@ inline void mat_open(material_ctx& mc, int type, float const* data, int offset) 
   mc.mat.roughness = d[2];
   mc.mat.metallic = d[3];
   mc.mat.transmission = d[4];
+  mc.tex_x = fbits(d[5]);
+  mc.tex_y = fbits(d[6]);
 }
-inline void mat_evaluate(material_ctx& mc, v3 n, v3 tl, v3 tv, v3& refl, float& pdf) {
+// material_new.glsl:27-41: pow(texture(albedo, (u, 1 - v)), 2.2) replaces the colour
+inline void mat_evaluate(material_ctx& mc, v3 n, v3 tl, v3 tv, v3& refl, float& pdf, v2 uv = v2{0.f, 0.f},
+    tex_view const* textures = nullptr, int n_textures = 0) {
   refl = {0.f, 0.f, 0.f};
   pdf = 1.f;
   if (mc.type != 0) return;
+  if ((mc.tex_x != 0u || mc.tex_y != 0u) && mc.tex_y == 0u && mc.tex_x <= std::uint32_t(n_textures) && textures &&
+      textures[mc.tex_x - 1u].p) {
+    tex_view const& t = textures[mc.tex_x - 1u];
+    v4 const c = bilinear_at(t.p, t.w, t.h, t.wrap, uv.x, 1.f - uv.y);
+    mc.mat.color = {std::pow(c.x, 2.2f), std::pow(c.y, 2.2f), std::pow(c.z, 2.2f), std::pow(c.w, 2.2f)};
+  }
   mc.incoming = dot(n, -tv) < 0.f;
   mc.ior1 = mc.incoming ? 1.f : mc.mat.ior;
   mc.ior2 = mc.incoming ? mc.mat.ior : 1.f;
@@ -621,6 +683,15 @@ struct frame_ctx {
   std::uint32_t sample_index;
   int nthreads;
   sdf_scene const* sdf;     // n_drawables == 0: no SDF drawables
+  // reference-mode extras: albedo textures by slot, cube map, depth of field
+  tex_view const* textures = nullptr;
+  int n_textures = 0;
+  float const* cubemap = nullptr;
+  int cubemap_size = 0;
+  int dof = 0;
+  float lens[2] = {0.f, 0.f};
+  float focus = 0.f;
+  tex_view bokeh{};
 };
 
 // pt_generate.comp:50-84
@@ -640,8 +711,32 @@ void pass_generate(frame_ctx& f, pass_rng const& pr, std::vector<gen_t>& gen) {
       gen_t g{};
       g.direction = normalize(v3{hom.x, hom.y, hom.z});
       g.origin = v3{f.inv_view[12], f.inv_view[13], f.inv_view[14]};
+      v3 tint{1.f, 1.f, 1.f};
+      if (f.dof) {
+        // bokeh.glsl:15-34 (bokeh_get) and pt_generate.comp:35-48 (apply_bokeh)
+        v2 offset = random_uniform_circle(r, 0.49f);
+        v3 value{1.f, 1.f, 1.f};
+        float amount = 1.f;
+        if (f.bokeh.p && f.bokeh.w >= 10) {
+          int tries = 8;
+          while ((tries == 8 || amount < 1e-5f) && tries-- > 0) {
+            v4 const m = bilinear_at(f.bokeh.p, f.bokeh.w, f.bokeh.h, f.bokeh.wrap, 0.5f + offset.x, 0.5f + offset.y);
+            value = {m.x, m.y, m.z};
+            offset = random_uniform_circle(r, 0.49f);
+            amount = gmax(gmax(value.x, value.y), value.z);
+          }
+        }
+        if (!(amount < 1e-5f)) {
+          v3 const center = g.origin + f.focus * g.direction;
+          v3 const alt = transform_local_to_world(
+              normalize(v3{(offset.x * f.lens[0]) / 2.f, (offset.y * f.lens[1]) / 2.f, f.focus}), g.direction);
+          tint = value;
+          g.origin = center - f.focus * alt;
+          g.direction = alt;
+        }
+      }
       g.random_value = random_next(r);
-      g.reflectance = {1.f, 1.f, 1.f};
+      g.reflectance = tint;
       g.color = {0.f, 0.f, 0.f, 0.f};
       g.pixel_x = float(x);
       g.pixel_y = float(y);
@@ -843,7 +938,7 @@ void pass_color(frame_ctx& f, pass_rng const& pr, std::vector<gen_t>& gen, std::
         v3 const generated = mat_bounce(mc, r, v2{r0, r1}, -g.direction, trace.normal);
         v3 mrefl;
         float mpdf;
-        mat_evaluate(mc, trace.normal, generated, -g.direction, mrefl, mpdf);
+        mat_evaluate(mc, trace.normal, generated, -g.direction, mrefl, mpdf, trace.uv, f.textures, f.n_textures);
         {
           float const p = g.pdf * 1.f;
           float const rnd = random_next(r);
@@ -868,7 +963,8 @@ void pass_color(frame_ctx& f, pass_rng const& pr, std::vector<gen_t>& gen, std::
         if (trace.light_strength > 0.f) {
           v3 lrefl{1.f, 1.f, 1.f};
           float lpdf = 1.f;
-          mat_evaluate(mc, trace.normal, trace.light_direction, -g.direction, lrefl, lpdf);
+          mat_evaluate(mc, trace.normal, trace.light_direction, -g.direction, lrefl, lpdf, trace.uv, f.textures,
+              f.n_textures);
           if (!inf3(lrefl)) {
             v4 const lc = unpack_unorm4x8(trace.light_color);
             v3 const c = v3{lc.x, lc.y, lc.z} * trace.light_strength * clamp3(lrefl, 0.f, 1.f);
@@ -884,9 +980,14 @@ void pass_color(frame_ctx& f, pass_rng const& pr, std::vector<gen_t>& gen, std::
         g.random_value = random_value(r, int(std::uint32_t(f2i(-1953631673.f * g.random_value)) + 357883444u * uid));
         gen[id] = g;
       } else {
-        float const t = (g.direction.y + 1.f) / 2.f;
-        v3 const sky = mix3(v3{0.3f, 0.4f, 0.5f}, v3{1.f, 0.98f, 0.96f}, t);
-        v3 const env = clamp3(g.reflectance * sky / g.pdf, 0.f, 16.f);
+        v3 env;
+        if (f.cubemap && f.cubemap_size > 10) {  // pt_color.comp:190-199
+          env = clamp3(g.reflectance * cube_sample(f.cubemap, f.cubemap_size, g.direction) / g.pdf, 0.f, 16.f);
+        } else {
+          float const t = (g.direction.y + 1.f) / 2.f;
+          v3 const sky = mix3(v3{0.3f, 0.4f, 0.5f}, v3{1.f, 0.98f, 0.96f}, t);
+          env = clamp3(g.reflectance * sky / g.pdf, 0.f, 16.f);
+        }
         acc(v4{g.color.x + env.x, g.color.y + env.y, g.color.z + env.z, g.color.w});
       }
     }
@@ -936,7 +1037,11 @@ void orc_render_reference(std::size_t n_tris, float const* tris9, float const* n
     std::uint32_t sample_index0, float const* inv_view, float const* inv_proj, std::int32_t const* seeds,
     float const* tex, float* accum, float* display, std::int32_t const* sdf_instrs, std::int32_t const* sdf_programs,
     float const* sdf_params, float const* sdf_drawables, int n_sdf_drawables, int sdf_steps, float sdf_eps,
-    int nthreads) {
+    int nthreads, int n_textures, float const* const* tex_data, int const* tex_dims, float const* cubemap,
+    int cubemap_size, int dof, float lens_x, float lens_y, float focus, int bokeh_texture) {
+  std::vector<tex_view> texv(std::size_t(std::max(n_textures, 0)));
+  for (int k = 0; k < n_textures; ++k)
+    texv[std::size_t(k)] = tex_view{tex_data[k], tex_dims[3 * k], tex_dims[3 * k + 1], tex_dims[3 * k + 2]};
   sdf_scene sdf;
   sdf.instrs = sdf_instrs;
   sdf.programs = sdf_programs;
@@ -964,6 +1069,15 @@ void orc_render_reference(std::size_t n_tris, float const* tris9, float const* n
       return r;
     };
     frame_ctx f{&sc, W, H, inv_view, inv_proj, &acc, &disp, sample_index0 + std::uint32_t(fr), nthreads, &sdf};
+    f.textures = texv.empty() ? nullptr : texv.data();
+    f.n_textures = n_textures;
+    f.cubemap = cubemap;
+    f.cubemap_size = cubemap_size;
+    f.dof = dof;
+    f.lens[0] = lens_x;
+    f.lens[1] = lens_y;
+    f.focus = focus;
+    if (bokeh_texture > 0 && bokeh_texture <= n_textures) f.bokeh = texv[std::size_t(bokeh_texture - 1)];
     std::vector<gen_t> gen;
     std::vector<trace_t> tr;
     pass_generate(f, pr(0), gen);

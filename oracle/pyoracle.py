@@ -44,7 +44,8 @@ def oracle() -> C.CDLL:
             "orc_brute_closest": (None, [P, SZ, P, SZ, I, P, P, P, P, I]),
             "orc_host_rng": (None, [C.c_uint32, I, I, P, P]),
             "orc_render_reference": (None, [SZ, P, P, P, P, P, SZ, P, P, P, I, I, I, I, C.c_uint32, P, P, P, P, P,
-                                            P, P, P, P, P, I, I, C.c_float, I]),
+                                            P, P, P, P, P, I, I, C.c_float, I, I, P, P, P, I, I, C.c_float,
+                                            C.c_float, C.c_float, I]),
             "orc_random_stream": (None, [P, I, I, I, I, I, P, P]),
             "orc_wang_hash": (C.c_uint32, [C.c_uint32]),
             "orc_transform_local_to_world": (None, [P, P, P]),
@@ -280,9 +281,13 @@ def host_rng(seed: int, frames: int, bounces: int):
 
 
 def render_reference(scene: dict, width: int, height: int, bounces: int, frames: int, inv_view, inv_proj,
-                     seed: int = 5489, accum=None, display=None, sample_index0: int = 0):
+                     seed: int = 5489, accum=None, display=None, sample_index0: int = 0, textures=None,
+                     cubemap=None, dof: bool = False, lens_size=(0.2, 0.2), focus: float = 1.0,
+                     bokeh_slot: int = -1):
     """Reference-shading render on the CPU (restated passes). scene: dict with
-    indices, vertices, normals, uvs, drawables, materials, material_data."""
+    indices, vertices, normals, uvs, drawables, materials, material_data.
+    textures: list of (rgba [H, W, 4], wrap) or None per slot; cubemap:
+    [6, S, S, 4] (stored at half precision, as the device stores it)."""
     L = oracle()
     tris9 = bake_world_triangles(scene["indices"], scene["vertices"], scene.get("drawables"))
     nrm, uvs, mat = bake_world_attributes(scene["indices"], scene.get("normals"), scene.get("uvs"),
@@ -308,10 +313,21 @@ def render_reference(scene: dict, width: int, height: int, bounces: int, frames:
                     int(sdf["steps"]), float(sdf["eps"])]
     else:
         sdf_args = [None, None, None, None, 0, 0, 0.0]
+    texs = [None if t is None else (np.ascontiguousarray(t[0], np.float32), int(t[1])) for t in (textures or [])]
+    tex_ptrs = (C.c_void_p * max(1, len(texs)))(*[t[0].ctypes.data if t else None for t in texs])
+    tex_dims = np.array([[t[0].shape[1], t[0].shape[0], t[1]] if t else [0, 0, 0] for t in texs] or [[0, 0, 0]],
+                        np.int32)
+    cube = None
+    if cubemap is not None:
+        cube = np.ascontiguousarray(np.asarray(cubemap, np.float32).astype(np.float16).astype(np.float32))
     L.orc_render_reference(tris9.shape[0], tris9.ctypes.data, nrm_p, uv_p, mat.ctypes.data, refs.ctypes.data,
                            refs.shape[0], mdata.ctypes.data, nodes.ctypes.data, bi.ctypes.data, width, height, bounces,
                            frames, sample_index0, iv.ctypes.data, ip.ctypes.data, seeds.ctypes.data, tex.ctypes.data,
-                           accum.ctypes.data, display.ctypes.data, *sdf_args, nthreads())
+                           accum.ctypes.data, display.ctypes.data, *sdf_args, nthreads(), len(texs),
+                           C.cast(tex_ptrs, C.c_void_p), tex_dims.ctypes.data,
+                           cube.ctypes.data if cube is not None else None, cube.shape[1] if cube is not None else 0,
+                           int(dof), float(lens_size[0]), float(lens_size[1]), float(focus),
+                           bokeh_slot + 1 if bokeh_slot >= 0 else 0)
     return accum, display
 
 

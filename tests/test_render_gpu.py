@@ -123,3 +123,87 @@ def test_reference_render_mesh_and_sdf(ctx):
     # the SDF drawables are visible: the render differs from the meshes-only one
     ref0, _ = po.render_reference(s, W, H, bounces=4, frames=2, inv_view=iv, inv_proj=ip, seed=31)
     assert np.abs(ref0[..., :3] - ref[..., :3]).max(-1).mean() > 1e-2
+
+
+def _textured_heightfield():
+    """32 x 32 height field with uvs from xz, two materials: one with an albedo
+    texture (slot 0, a checker in linear [0, 1]), one plain."""
+    from myrt_b200.scenes import pbr_material
+
+    idx, pts = heightfield(32, seed=3)
+    uvs = np.stack([(pts[:, 0] + 1) * 1.5, (pts[:, 2] + 1) * 1.5], 1).astype(np.float32)  # repeats past 1
+    m0 = pbr_material([0.7, 0.5, 0.3], ior=1.5, roughness=0.6)
+    m0[5] = np.array([1], np.uint32).view(np.float32)[0]  # handle (slot 0 + 1, 0)
+    m1 = pbr_material([0.3, 0.6, 0.8], ior=1.5, roughness=0.3, metallic=1.0)
+    mdata = np.concatenate([m0, m1])
+    from myrt_b200._abi import myrt_drawable
+
+    n = idx.size
+    dr = (myrt_drawable * 2)()
+    eye = np.eye(4, dtype=np.float32).ravel().tolist()
+    for k in range(2):
+        dr[k].transformation[:] = eye
+        dr[k].inverse_transformation[:] = eye
+        dr[k].points_base_index = 0
+        dr[k].material_index = k
+    half = (n // 6) * 3
+    dr[0].indices_base_index, dr[0].index_count = 0, half
+    dr[1].indices_base_index, dr[1].index_count = half, n - half
+    scene = dict(indices=idx, vertices=pts, uvs=uvs, drawables=dr, materials=np.array([[0, 0], [0, 7]], np.int32),
+                 material_data=mdata)
+    g = np.indices((8, 8)).sum(0) % 2
+    checker = np.zeros((8, 8, 4), np.float32)
+    checker[..., 0] = np.where(g, 0.9, 0.2)
+    checker[..., 1] = np.where(g, 0.8, 0.3)
+    checker[..., 2] = np.where(g, 0.1, 0.7)
+    checker[..., 3] = 1.0
+    return scene, checker
+
+
+def _bokeh_mask():
+    """16 x 16 ring with a dark centre: draws inside it trigger bokeh_get's retries."""
+    y, x = np.mgrid[0:16, 0:16]
+    r = np.hypot(x - 7.5, y - 7.5) / 8.0
+    v = np.where((r > 0.35) & (r < 0.95), 1.0, 0.0).astype(np.float32)
+    m = np.zeros((16, 16, 4), np.float32)
+    m[..., 0], m[..., 1], m[..., 2], m[..., 3] = v, 0.8 * v, 0.6 * v, 1.0
+    return m
+
+
+def _cubemap(size=16):
+    f = np.zeros((6, size, size, 4), np.float32)
+    s = np.linspace(0, 1, size, dtype=np.float32)
+    for k in range(6):
+        f[k, ..., 0] = 0.2 + 0.1 * k + 0.5 * s[None, :]
+        f[k, ..., 1] = 0.3 + 0.4 * s[:, None]
+        f[k, ..., 2] = 0.9 - 0.1 * k
+        f[k, ..., 3] = 1.0
+    return f
+
+
+def test_reference_render_textures_cubemap_dof(ctx):
+    """Albedo textures (material handle = slot + 1), the environment cube map and
+    depth of field with a bokeh mask, against the oracle's restated passes."""
+    scene, checker = _textured_heightfield()
+    ctx.upload_scene(**scene)
+    ctx.upload_texture(0, checker, wrap=0)
+    ctx.upload_texture(1, _bokeh_mask(), wrap=0)
+    cube = _cubemap()
+    ctx.upload_cubemap(cube)
+    try:
+        W, H = 80, 60
+        iv, ip = look_at((0, 1.2, -2.5), (0, 0, 0), vfov_deg=55, aspect=W / H)
+        ctx.set_seed(777)
+        ctx.render(iv, ip, W, H, num_bounces=4, frames=3, dof=True, lens_size=(0.2, 0.15), focus=2.4, bokeh_slot=1)
+        acc, _ = ctx.read_accumulation(W, H)
+        ref, _ = po.render_reference(scene, W, H, bounces=4, frames=3, inv_view=iv, inv_proj=ip, seed=777,
+                                     textures=[(checker, 0), (_bokeh_mask(), 0)], cubemap=cube, dof=True,
+                                     lens_size=(0.2, 0.15), focus=2.4, bokeh_slot=1)
+        _compare(acc, ref)
+        # without the extras the image changes (the features are in use)
+        ref_plain, _ = po.render_reference(scene, W, H, bounces=4, frames=3, inv_view=iv, inv_proj=ip, seed=777)
+        assert np.abs(ref_plain[..., :3] - ref[..., :3]).mean() > 1e-2
+    finally:
+        ctx.upload_texture(0, None)
+        ctx.upload_texture(1, None)
+        ctx.upload_cubemap(None)
