@@ -562,6 +562,43 @@ typedef struct myrt_image {
 int myrt_post_pass(myrt_ctx* ctx, const myrt_pp_pass* pass, const myrt_image* input, const myrt_image* overlay,
     const myrt_image* output, void* stream);
 
+/* ---- forward (raster preview) renderer (src/pathtracer/forward_renderer.cpp,
+ * src/pt/fwd_generate.comp, src/pt/forward/*) ----
+ * forward_renderer::run on the uploaded scene: a G-buffer pass (world
+ * position, uv, normal + material at RGBA16F), a shadow pass from a fixed
+ * orthographic light (world positions at RGBA32F) and the resolve pass
+ * (9-tap shadow test, the material's diffuse lobe towards the light and the
+ * normal, 8-sample screen-space ambient occlusion, random brightness), into an
+ * RGBA16F result. Rasterisation follows GL's rules: pixel centres at +0.5,
+ * perspective-correct attributes, clipping to -w <= z <= w, a 24-bit depth
+ * buffer with GL_LESS in draw order (triangles of drawable 0 first), no
+ * culling. Rows are GL window rows (row 0 at the bottom). */
+typedef struct myrt_forward_params {
+  uint32_t width, height;
+  float view[16];         /* set_view_matrix, column-major */
+  float projection[16];   /* set_projection_matrix, column-major */
+  uint32_t random_seed;   /* the resolve pass's random_seed uniform (run draws it from its generator) */
+  uint32_t shadow_size;   /* shadow map edge in texels; 0 = 2048 (the reference's) */
+  int32_t custom_shadow;  /* 0: the reference's light camera (forward_renderer.cpp:306-310); 1: the two below */
+  float shadow_view[16];
+  float shadow_projection[16];
+} myrt_forward_params;
+/* Runs the three passes on the context's stream. */
+int myrt_forward_run(myrt_ctx* ctx, const myrt_forward_params* params);
+/* Host copies of the last run (NULL skips one): result RGBA16F as half bits
+ * (height * width * 4), G-buffer layers position / uv / normal + material as
+ * half bits (3 * height * width * 4), shadow map RGBA32F (size * size * 4),
+ * visibility keys (height * width: 24-bit depth << 32 | triangle index; all
+ * ones where nothing was drawn). Waits for the stream. */
+int myrt_forward_read(myrt_ctx* ctx, uint16_t* result, uint16_t* gbuffer, float* shadow_map, uint64_t* visibility);
+/* Device pointers of the same four images (valid until the next run with
+ * another size or context destruction). */
+int myrt_forward_buffers(myrt_ctx* ctx, void** result, void** gbuffer, void** shadow_map, void** visibility);
+/* The light camera the reference uses: view = inverse(rotation(axis (1,0,0),
+ * -45 degrees) * translation(0, 0, 15)), projection = orthographic(-20, 20,
+ * 20, -20, 0.01, 1000), column-major. */
+int myrt_forward_default_shadow(float* view, float* projection);
+
 #ifdef __cplusplus
 }
 #endif

@@ -38,6 +38,15 @@ def bvh_info_dict(info: _abi.myrt_bvh_info) -> dict:
     return {f: getattr(info, f) for f, _ in _abi.myrt_bvh_info._fields_ if f != "pad"}
 
 
+def forward_default_shadow():
+    """The light camera of forward_renderer::pass_shadow as the library builds
+    it: (view, projection), numpy [4, 4] in math layout."""
+    v = np.zeros(16, np.float32)
+    p = np.zeros(16, np.float32)
+    _abi.lib().myrt_forward_default_shadow(v.ctypes.data, p.ctypes.data)
+    return v.reshape(4, 4).T.copy(), p.reshape(4, 4).T.copy()
+
+
 def build_bvh8(positions: np.ndarray):
     """Host-only BVH build. positions: float32 [T, 3, 3] (or [T, 9]).
     Returns (nodes uint32 [N, 20], triangles float32 [M, 12], info dict)."""
@@ -262,6 +271,47 @@ class Context:
             return
         a = np.ascontiguousarray(faces, np.float32)
         self._check(self._L.myrt_cubemap_upload(self._h, a.ctypes.data, a.shape[1]), "myrt_cubemap_upload")
+
+    def forward_render(self, view, projection, width: int, height: int, random_seed: int = 0,
+                       shadow_size: int = 0, shadow_view=None, shadow_projection=None):
+        """myrt_forward_run (forward_renderer::run): view / projection are
+        column-major 4x4 (numpy [4, 4] in math layout is transposed for you
+        when given as a 2-D array); shadow_view / shadow_projection replace the
+        reference's light camera when both are given."""
+        p = _abi.myrt_forward_params()
+        p.width, p.height = width, height
+
+        def colmajor(m):
+            a = np.asarray(m, np.float32)
+            return (a.T if a.ndim == 2 else a).ravel()
+
+        p.view[:] = colmajor(view).tolist()
+        p.projection[:] = colmajor(projection).tolist()
+        p.random_seed = int(random_seed) & 0xFFFFFFFF
+        p.shadow_size = shadow_size
+        if shadow_view is not None and shadow_projection is not None:
+            p.custom_shadow = 1
+            p.shadow_view[:] = colmajor(shadow_view).tolist()
+            p.shadow_projection[:] = colmajor(shadow_projection).tolist()
+        self._check(self._L.myrt_forward_run(self._h, C.byref(p)), "myrt_forward_run")
+
+    def forward_read(self, width: int, height: int, shadow_size: int = 2048) -> dict:
+        """myrt_forward_read: result / gbuffer as float32 (from their half
+        bits), shadow_map float32, visibility uint64."""
+        res = np.empty((height, width, 4), np.uint16)
+        gb = np.empty((3, height, width, 4), np.uint16)
+        sm = np.empty((shadow_size, shadow_size, 4), np.float32)
+        vis = np.empty((height, width), np.uint64)
+        self._check(self._L.myrt_forward_read(self._h, res.ctypes.data, gb.ctypes.data, sm.ctypes.data,
+                                              vis.ctypes.data), "myrt_forward_read")
+        return {"result": res.view(np.float16).astype(np.float32), "gbuffer": gb.view(np.float16).astype(np.float32),
+                "shadow_map": sm, "visibility": vis}
+
+    def forward_buffers(self) -> dict:
+        """Device pointers of the last forward run's images."""
+        ptrs = [C.c_void_p() for _ in range(4)]
+        self._check(self._L.myrt_forward_buffers(self._h, *[C.byref(q) for q in ptrs]), "myrt_forward_buffers")
+        return dict(zip(("result", "gbuffer", "shadow_map", "visibility"), [q.value for q in ptrs]))
 
     def set_area_lights(self, lights):
         """myrt_set_area_lights: lights [n, 12] float32 rows (corner, edge_u,

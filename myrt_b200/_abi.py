@@ -66,6 +66,13 @@ class myrt_render_params(C.Structure):
                 ("focus", C.c_float), ("bokeh_texture", C.c_int32)]
 
 
+class myrt_forward_params(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("view", C.c_float * 16),
+                ("projection", C.c_float * 16), ("random_seed", C.c_uint32), ("shadow_size", C.c_uint32),
+                ("custom_shadow", C.c_int32), ("shadow_view", C.c_float * 16),
+                ("shadow_projection", C.c_float * 16)]
+
+
 class myrt_pp_pass(C.Structure):
     _fields_ = [("op", C.c_int32), ("i", C.c_int32 * 3), ("p", C.c_float * 4)]
 
@@ -173,6 +180,10 @@ SIGNATURES = {
     "myrt_scene_copy_bvh": (I, [P, P, P]),
     "myrt_texture_upload": (I, [P, U32, P, U32, U32, U32]),
     "myrt_cubemap_upload": (I, [P, P, U32]),
+    "myrt_forward_run": (I, [P, C.POINTER(myrt_forward_params)]),
+    "myrt_forward_read": (I, [P, P, P, P, P]),
+    "myrt_forward_buffers": (I, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
+    "myrt_forward_default_shadow": (I, [P, P]),
     "myrt_scene_set_transforms": (I, [P, P, C.c_size_t]),
     "myrt_post_pass": (I, [P, C.POINTER(myrt_pp_pass), C.POINTER(myrt_image), C.POINTER(myrt_image),
                            C.POINTER(myrt_image), P]),

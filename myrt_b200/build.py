@@ -24,7 +24,7 @@ CUDA_FLAGS = ["-O3", "-lineinfo", "-std=c++20", "--expt-relaxed-constexpr", "-Xc
 CXX_FLAGS = ["-O3", "-std=c++20", "-fPIC", "-pthread"]
 # Translation units whose arithmetic must round every + and * separately (the
 # shading restates GLSL expressions operation by operation).
-NO_FMA = {"wavefront.cu", "physical.cu", "postprocess.cu"}
+NO_FMA = {"wavefront.cu", "physical.cu", "postprocess.cu", "raster.cu"}
 
 
 def sources() -> list[Path]:

@@ -39,6 +39,7 @@ void free_scene(device_scene& s) {
   cudaFree(s.raw_vertices);
   cudaFree(s.raw_normals);
   cudaFree(s.prim_src);
+  cudaFree(s.world_pos);
   cudaFree(s.nodes);
   cudaFree(s.tris);
   cudaFree(s.tri_normals);
@@ -417,6 +418,7 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   cudaFree(ctx->sdf.drawables);
   free_render(ctx->render);
   free_textures(ctx);
+  free_forward(ctx);
   free_physical(ctx->physical);
   free_guide(ctx->guide);
   ctx->guide = nullptr;
@@ -563,7 +565,7 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
     if (rc) return rc;
     char const* what = nullptr;
     int const e = build_bvh8_device(d_pos, n_prims, ctx->stream, dtree, &what);
-    cudaFree(d_pos);
+    ctx->scene.world_pos = d_pos;
     if (e) return check_cuda(ctx, cudaError_t(e > 0 ? e : cudaErrorInvalidValue), what ? what : "device BVH build");
     if (dtree.wide_depth > MYRT_STACK_MAX) {
       cudaFree(dtree.nodes);
@@ -619,6 +621,7 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
           "triangle upload");
   }
   if (!rc && !nrm.empty()) rc = upload(ctx, &s.tri_normals, nrm.data(), nrm.size(), "normal upload");
+  if (!rc && !s.world_pos) rc = upload(ctx, &s.world_pos, pos.data(), pos.size(), "world triangle upload");
   // object-space geometry for transform updates
   if (!rc)
     rc = upload(ctx, &s.raw_vertices, reinterpret_cast<float4 const*>(v->vertices), v->vertex_count, "vertex upload");

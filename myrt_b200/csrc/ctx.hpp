@@ -17,6 +17,8 @@ namespace myrt_b200 {
 struct guide_state;
 
 // Device-resident scene: BVH, pre-gathered triangles and the shading buffers.
+struct forward_state;  // raster.cu
+
 struct device_scene {
   uint4* nodes = nullptr;      // 5 uint4 per wide node
   float4* tris = nullptr;      // 3 float4 per triangle reference (leaf order)
@@ -38,6 +40,9 @@ struct device_scene {
   uint4* prim_src = nullptr;
   size_t n_vertices = 0;
   std::vector<myrt_drawable> drawables;
+  // world-space corners per prim (9 floats, prim id = draw order) for the
+  // forward renderer's rasteriser
+  float* world_pos = nullptr;
 };
 
 // SDF drawables (uploaded separately; scene::prepare's sdf buffers).
@@ -130,6 +135,8 @@ struct myrt_ctx {
   texture_slot* d_textures = nullptr;
   float4* cubemap = nullptr;
   int cubemap_size = 0;
+  // forward (raster preview) renderer buffers, created on first use
+  myrt_b200::forward_state* forward = nullptr;
   // phase timing of the ray queries: (before ordering, before traversal, after)
   bool time_phases = false;
   std::vector<std::array<cudaEvent_t, 3>> phase_pending, phase_pool;
@@ -140,6 +147,7 @@ int set_error(myrt_ctx* ctx, int code, std::string msg);
 int check_cuda(myrt_ctx* ctx, cudaError_t e, char const* what);
 void free_render(render_state& r);
 void free_textures(myrt_ctx* ctx);
+void free_forward(myrt_ctx* ctx);
 void free_physical(physical_state& p);
 int ensure_images(myrt_ctx* ctx, uint32_t W, uint32_t H);
 int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p);

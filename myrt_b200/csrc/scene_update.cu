@@ -161,6 +161,11 @@ int scene_set_transforms(myrt_ctx* ctx, myrt_drawable const* drawables, size_t c
   device_bvh8 dt;
   char const* what = nullptr;
   int const e = build_bvh8_device(d_pos, s.n_prims, st, dt, &what);
+  if (!e) {
+    cudaFree(s.world_pos);  // the re-baked corners become the rasteriser's
+    s.world_pos = d_pos;
+    d_pos = nullptr;
+  }
   cleanup();
   if (e) return check_cuda(ctx, cudaError_t(e > 0 ? e : cudaErrorInvalidValue), what ? what : "device BVH build");
   if (dt.wide_depth > MYRT_STACK_MAX) {

@@ -1624,3 +1624,380 @@ void orc_render_physical(std::size_t n_tris, float const* tris9, float const* no
   });
 }
 }  // extern "C"
+
+// ---- forward (raster preview) renderer ---------------------------------------------------
+// forward_renderer.cpp:13-318 with forward/vert.vert, frag.frag, resolve.frag.
+// Rasterisation as GL defines it (pixel centres at +0.5, perspective-correct
+// attributes, clipping to -w <= z <= w, 24-bit depth, GL_LESS in draw order),
+// written as homogeneous rasterisation (Olano & Greer 1997): per triangle the
+// edge functions of the homogeneous window coordinates (X, Y, w) =
+// ((x + w) W / 2, (y + w) H / 2, w); a pixel centre is covered when the three
+// sign-normalised edge functions are positive (zero: top-left rule);
+// barycentrics are the edge functions over their sum; z_ndc = sum e_i z_i /
+// |det|. Triangles are drawn one after another; a fragment replaces the stored
+// one when its (depth, triangle) key is smaller, which is GL_LESS in draw
+// order. Every product and sum is rounded separately (-ffp-contract=off), in
+// the order the device code writes them.
+extern "C" float oracle_half_rn(float f);
+namespace {
+
+struct fmat {
+  float m[16];
+};
+fmat fmul(fmat const& a, fmat const& b) {
+  fmat c{};
+  for (int col = 0; col < 4; ++col)
+    for (int r = 0; r < 4; ++r) {
+      float s = a.m[r] * b.m[col * 4];
+      for (int k = 1; k < 4; ++k) s = s + a.m[k * 4 + r] * b.m[col * 4 + k];
+      c.m[col * 4 + r] = s;
+    }
+  return c;
+}
+// inverse by cofactors in double, rounded once to float
+fmat finverse(fmat const& a) {
+  double m[16], inv[16];
+  for (int i = 0; i < 16; ++i) m[i] = a.m[i];
+  inv[0] = m[5] * m[10] * m[15] - m[5] * m[11] * m[14] - m[9] * m[6] * m[15] + m[9] * m[7] * m[14] +
+      m[13] * m[6] * m[11] - m[13] * m[7] * m[10];
+  inv[4] = -m[4] * m[10] * m[15] + m[4] * m[11] * m[14] + m[8] * m[6] * m[15] - m[8] * m[7] * m[14] -
+      m[12] * m[6] * m[11] + m[12] * m[7] * m[10];
+  inv[8] = m[4] * m[9] * m[15] - m[4] * m[11] * m[13] - m[8] * m[5] * m[15] + m[8] * m[7] * m[13] +
+      m[12] * m[5] * m[11] - m[12] * m[7] * m[9];
+  inv[12] = -m[4] * m[9] * m[14] + m[4] * m[10] * m[13] + m[8] * m[5] * m[14] - m[8] * m[6] * m[13] -
+      m[12] * m[5] * m[10] + m[12] * m[6] * m[9];
+  inv[1] = -m[1] * m[10] * m[15] + m[1] * m[11] * m[14] + m[9] * m[2] * m[15] - m[9] * m[3] * m[14] -
+      m[13] * m[2] * m[11] + m[13] * m[3] * m[10];
+  inv[5] = m[0] * m[10] * m[15] - m[0] * m[11] * m[14] - m[8] * m[2] * m[15] + m[8] * m[3] * m[14] +
+      m[12] * m[2] * m[11] - m[12] * m[3] * m[10];
+  inv[9] = -m[0] * m[9] * m[15] + m[0] * m[11] * m[13] + m[8] * m[1] * m[15] - m[8] * m[3] * m[13] -
+      m[12] * m[1] * m[11] + m[12] * m[3] * m[9];
+  inv[13] = m[0] * m[9] * m[14] - m[0] * m[10] * m[13] - m[8] * m[1] * m[14] + m[8] * m[2] * m[13] +
+      m[12] * m[1] * m[10] - m[12] * m[2] * m[9];
+  inv[2] = m[1] * m[6] * m[15] - m[1] * m[7] * m[14] - m[5] * m[2] * m[15] + m[5] * m[3] * m[14] +
+      m[13] * m[2] * m[7] - m[13] * m[3] * m[6];
+  inv[6] = -m[0] * m[6] * m[15] + m[0] * m[7] * m[14] + m[4] * m[2] * m[15] - m[4] * m[3] * m[14] -
+      m[12] * m[2] * m[7] + m[12] * m[3] * m[6];
+  inv[10] = m[0] * m[5] * m[15] - m[0] * m[7] * m[13] - m[4] * m[1] * m[15] + m[4] * m[3] * m[13] +
+      m[12] * m[1] * m[7] - m[12] * m[3] * m[5];
+  inv[14] = -m[0] * m[5] * m[14] + m[0] * m[6] * m[13] + m[4] * m[1] * m[14] - m[4] * m[2] * m[13] -
+      m[12] * m[1] * m[6] + m[12] * m[2] * m[5];
+  inv[3] = -m[1] * m[6] * m[11] + m[1] * m[7] * m[10] + m[5] * m[2] * m[11] - m[5] * m[3] * m[10] -
+      m[9] * m[2] * m[7] + m[9] * m[3] * m[6];
+  inv[7] = m[0] * m[6] * m[11] - m[0] * m[7] * m[10] - m[4] * m[2] * m[11] + m[4] * m[3] * m[10] +
+      m[8] * m[2] * m[7] - m[8] * m[3] * m[6];
+  inv[11] = -m[0] * m[5] * m[11] + m[0] * m[7] * m[9] + m[4] * m[1] * m[11] - m[4] * m[3] * m[9] -
+      m[8] * m[1] * m[7] + m[8] * m[3] * m[5];
+  inv[15] = m[0] * m[5] * m[10] - m[0] * m[6] * m[9] - m[4] * m[1] * m[10] + m[4] * m[2] * m[9] +
+      m[8] * m[1] * m[6] - m[8] * m[2] * m[5];
+  double const det = m[0] * inv[0] + m[1] * inv[4] + m[2] * inv[8] + m[3] * inv[12];
+  fmat r{};
+  for (int i = 0; i < 16; ++i) r.m[i] = float(inv[i] / det);
+  return r;
+}
+v4 fmulv(fmat const& a, float x, float y, float z, float w) {
+  v4 r;
+  float* o = &r.x;
+  for (int i = 0; i < 4; ++i) o[i] = ((a.m[i] * x + a.m[4 + i] * y) + a.m[8 + i] * z) + a.m[12 + i] * w;
+  return r;
+}
+
+struct fwd_tri {
+  float e[3][4];  // sign-normalised edge functions (a, b, c) and z_i / |det|
+  std::uint32_t flags = 0;
+  int x0 = 0, y0 = 0, x1 = -1, y1 = -1;
+};
+// vert.vert + the rasteriser's triangle set-up
+bool fwd_setup(float const* p, fmat const& pv, int W, int H, fwd_tri& t) {
+  float const hw = float(W) * 0.5f, hh = float(H) * 0.5f;
+  float X[3], Y[3], Wc[3], Z[3];
+  bool finite = true, front = true;
+  for (int k = 0; k < 3; ++k) {
+    v4 const c = fmulv(pv, p[3 * k], p[3 * k + 1], p[3 * k + 2], 1.f);
+    X[k] = (c.x + c.w) * hw;
+    Y[k] = (c.y + c.w) * hh;
+    Z[k] = c.z;
+    Wc[k] = c.w;
+    finite = finite && std::isfinite(X[k]) && std::isfinite(Y[k]) && std::isfinite(Z[k]) && std::isfinite(Wc[k]);
+    front = front && Wc[k] > 0.f;
+  }
+  float e[3][3];
+  for (int i = 0; i < 3; ++i) {
+    int const j = (i + 1) % 3, k = (i + 2) % 3;
+    e[i][0] = Y[j] * Wc[k] - Wc[j] * Y[k];
+    e[i][1] = Wc[j] * X[k] - X[j] * Wc[k];
+    e[i][2] = X[j] * Y[k] - Y[j] * X[k];
+  }
+  float const det = (e[0][0] * X[0] + e[0][1] * Y[0]) + e[0][2] * Wc[0];
+  if (!finite || det == 0.f || !std::isfinite(det)) return false;
+  float const sg = det > 0.f ? 1.f : -1.f, ad = std::fabs(det);
+  t.flags = 0;
+  for (int i = 0; i < 3; ++i) {
+    float const ea = e[i][0] * sg, eb = e[i][1] * sg, ec = e[i][2] * sg;
+    if (ea > 0.f || (ea == 0.f && eb > 0.f)) t.flags |= 1u << i;
+    t.e[i][0] = ea, t.e[i][1] = eb, t.e[i][2] = ec, t.e[i][3] = Z[i] / ad;
+  }
+  int x0 = 0, y0 = 0, x1 = W - 1, y1 = H - 1;
+  if (front) {
+    float lx = INFINITY, ly = INFINITY, ux = -INFINITY, uy = -INFINITY;
+    for (int k = 0; k < 3; ++k) {
+      float const sx = X[k] / Wc[k], sy = Y[k] / Wc[k];
+      lx = std::fmin(lx, sx), ux = std::fmax(ux, sx), ly = std::fmin(ly, sy), uy = std::fmax(uy, sy);
+    }
+    x0 = int(std::fmax(std::floor(lx) - 1.f, 0.f)), y0 = int(std::fmax(std::floor(ly) - 1.f, 0.f));
+    x1 = int(std::fmin(std::floor(ux) + 1.f, float(W) - 1.f)), y1 = int(std::fmin(std::floor(uy) + 1.f, float(H) - 1.f));
+  }
+  t.x0 = x0, t.y0 = y0, t.x1 = x1, t.y1 = y1;
+  return x1 >= x0 && y1 >= y0;
+}
+bool fwd_covered(fwd_tri const& t, int x, int y, float* e) {
+  float const X = float(x) + 0.5f, Y = float(y) + 0.5f;
+  bool in = true;
+  for (int i = 0; i < 3; ++i) {
+    e[i] = (t.e[i][0] * X + t.e[i][1] * Y) + t.e[i][2];
+    in = in && (e[i] > 0.f || (e[i] == 0.f && ((t.flags >> i) & 1u)));
+  }
+  return in;
+}
+// draws all triangles into keys (W * H, all ones = empty); tris keeps the set-ups
+void fwd_raster(int n, float const* pos, fmat const& pv, int W, int H, std::uint64_t* keys, std::vector<fwd_tri>& tris) {
+  std::fill(keys, keys + std::size_t(W) * H, ~std::uint64_t(0));
+  tris.assign(std::size_t(n), fwd_tri{});
+  for (int t = 0; t < n; ++t) {
+    fwd_tri& tr = tris[std::size_t(t)];
+    if (!fwd_setup(pos + 9 * std::size_t(t), pv, W, H, tr)) continue;
+    for (int y = tr.y0; y <= tr.y1; ++y)
+      for (int x = tr.x0; x <= tr.x1; ++x) {
+        float e[3];
+        if (!fwd_covered(tr, x, y, e)) continue;
+        float const zn = (e[0] * tr.e[0][3] + e[1] * tr.e[1][3]) + e[2] * tr.e[2][3];
+        if (!(zn >= -1.f && zn <= 1.f)) continue;
+        std::uint32_t const d = std::uint32_t(std::nearbyint((zn * 0.5f + 0.5f) * 16777215.f));
+        if (d >= 0xffffffu) continue;
+        std::uint64_t const key = (std::uint64_t(d) << 32) | std::uint32_t(t);
+        std::uint64_t& dst = keys[std::size_t(y) * W + x];
+        if (key < dst) dst = key;
+      }
+  }
+}
+inline float ld(float const* p) { return *p; }
+// frag.frag outputs per pixel: G-buffer layers (half-rounded) or shadow positions
+void fwd_attributes(std::vector<fwd_tri> const& tris, std::uint64_t const* keys, int W, int H, float const* pos,
+    float const* nrm, float const* uvs, std::int32_t const* mat, float* gbuf, float* smap) {
+  std::size_t const plane = std::size_t(W) * H;
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      std::size_t const px = std::size_t(y) * W + x;
+      std::uint64_t const key = keys[px];
+      if (key == ~std::uint64_t(0)) {
+        if (gbuf)
+          for (int l = 0; l < 3; ++l) std::fill(gbuf + 4 * (l * plane + px), gbuf + 4 * (l * plane + px) + 4, 0.f);
+        else
+          std::fill(smap + 4 * px, smap + 4 * px + 4, 0.f);
+        continue;
+      }
+      std::uint32_t const t = std::uint32_t(key & 0xffffffffu);
+      float e[3];
+      fwd_covered(tris[t], x, y, e);
+      float const s = (e[0] + e[1]) + e[2];
+      float const l0 = e[0] / s, l1 = e[1] / s, l2 = e[2] / s;
+      float const* P = pos + 9 * std::size_t(t);
+      v3 const p0{P[0], P[1], P[2]}, p1{P[3], P[4], P[5]}, p2{P[6], P[7], P[8]};
+      v3 const q = (l0 * p0 + l1 * p1) + l2 * p2;
+      if (!gbuf) {
+        float* o = smap + 4 * px;
+        o[0] = q.x, o[1] = q.y, o[2] = q.z, o[3] = 1.f;
+        continue;
+      }
+      v3 n;
+      if (nrm) {
+        float const* N = nrm + 9 * std::size_t(t);  // 3 corners, xyz
+        n = normalize((l0 * v3{N[0], N[1], N[2]} + l1 * v3{N[3], N[4], N[5]}) + l2 * v3{N[6], N[7], N[8]});
+      } else {
+        n = normalize(cross(normalize(p1 - p0), normalize(p2 - p0)));
+      }
+      float u = 0.f, v = 0.f;
+      if (uvs) {
+        float const* U = uvs + 6 * std::size_t(t);
+        u = (l0 * U[0] + l1 * U[2]) + l2 * U[4];
+        v = (l0 * U[1] + l1 * U[3]) + l2 * U[5];
+      }
+      float const vals[3][4] = {{q.x, q.y, q.z, 1.f}, {u, v, 0.f, 0.f}, {n.x, n.y, n.z, float(mat[t])}};
+      for (int l = 0; l < 3; ++l)
+        for (int c = 0; c < 4; ++c) gbuf[4 * (l * plane + px) + c] = oracle_half_rn(vals[l][c]);
+    }
+}
+// uint(f) as NVIDIA GPUs convert it (truncation, saturation, NaN -> 0)
+inline std::uint32_t f2u_sat(float f) {
+  if (!(f > 0.f)) return 0u;
+  if (f >= 4294967296.f) return 0xffffffffu;
+  return std::uint32_t(f);
+}
+inline int f2i_idx(float f) { return (f > -2147483648.f && f < 2147483648.f) ? int(f) : 0; }
+// random.glsl:52-60
+inline void random_init_nt(rng_t& r, int px, int py, int seed) {
+  r.state = std::uint32_t(seed);
+  r.prime = 0;
+  r.tex = nullptr;
+  r.tex_size = 0;
+  int const a = random_int(r, px ^ 0xba77fa);
+  int const b = random_int(r, py ^ 0xcca6df);
+  int const c = random_int(r, seed);
+  int const seed_base = int(std::uint32_t(a) * 69019u + std::uint32_t(b) * 96013u + std::uint32_t(c));
+  int const rem = seed_base % 12352345;
+  random_value(r, int(std::uint32_t(seed_base) + 16756614u * std::uint32_t(rem)));
+}
+
+}  // namespace
+
+extern "C" {
+
+// forward_renderer::run: G-buffer pass, shadow pass, resolve. Outputs (any may
+// be null): vis / svis keys, gbuf (3 layers of H*W*4 half-rounded floats),
+// smap (S*S*4), result (H*W*4 half-rounded).
+void orc_forward_render(int n, float const* pos, float const* nrm, float const* uvs, std::int32_t const* mat,
+    std::int32_t const* refs, int n_refs, float const* mdata, int W, int H, float const* view, float const* proj,
+    std::uint32_t seed, int S, float const* shadow_view, float const* shadow_proj, int n_textures,
+    float const* const* tex_data, int const* tex_dims, std::uint64_t* vis_out, float* gbuf_out,
+    std::uint64_t* svis_out, float* smap_out, float* result) {
+  fmat V, P, SV, SP;
+  std::memcpy(V.m, view, 64);
+  std::memcpy(P.m, proj, 64);
+  std::memcpy(SV.m, shadow_view, 64);
+  std::memcpy(SP.m, shadow_proj, 64);
+  fmat const pv = fmul(P, V), spv = fmul(SP, SV);
+  fmat const inv_view = finverse(V);
+  fmat const inv_vp = fmul(inv_view, finverse(P));
+  fmat const inv_sview = finverse(SV);
+  std::size_t const plane = std::size_t(W) * H, splane = std::size_t(S) * S;
+  std::vector<std::uint64_t> vis(plane), svis(splane);
+  std::vector<float> gbuf(3 * plane * 4), smap(splane * 4);
+  std::vector<fwd_tri> tris;
+  fwd_raster(n, pos, pv, W, H, vis.data(), tris);
+  fwd_attributes(tris, vis.data(), W, H, pos, nrm, uvs, mat, gbuf.data(), nullptr);
+  fwd_raster(n, pos, spv, S, S, svis.data(), tris);
+  fwd_attributes(tris, svis.data(), S, S, pos, nrm, uvs, mat, nullptr, smap.data());
+  if (vis_out) std::copy(vis.begin(), vis.end(), vis_out);
+  if (svis_out) std::copy(svis.begin(), svis.end(), svis_out);
+  if (gbuf_out) std::copy(gbuf.begin(), gbuf.end(), gbuf_out);
+  if (smap_out) std::copy(smap.begin(), smap.end(), smap_out);
+  if (!result) return;
+  std::vector<tex_view> texv(std::size_t(std::max(n_textures, 0)));
+  for (int k = 0; k < n_textures; ++k)
+    texv[std::size_t(k)] = tex_view{tex_data[k], tex_dims[3 * k], tex_dims[3 * k + 1], tex_dims[3 * k + 2]};
+  v3 const cam{inv_view.m[12], inv_view.m[13], inv_view.m[14]};
+  v3 light;
+  {
+    float const lx = ((inv_sview.m[0] * 0.f + inv_sview.m[4] * 0.f) + inv_sview.m[8] * 1.f) + inv_sview.m[12] * 0.f;
+    float const ly = ((inv_sview.m[1] * 0.f + inv_sview.m[5] * 0.f) + inv_sview.m[9] * 1.f) + inv_sview.m[13] * 0.f;
+    float const lz = ((inv_sview.m[2] * 0.f + inv_sview.m[6] * 0.f) + inv_sview.m[10] * 1.f) + inv_sview.m[14] * 0.f;
+    float const len = std::sqrt((lx * lx + ly * ly) + lz * lz);
+    float const inv = 1.f / len;
+    light = {lx * inv, ly * inv, lz * inv};
+  }
+  float const fw = float(W), fh = float(H), fs = float(S);
+  auto g = [&](int layer, std::size_t px) { return gbuf.data() + 4 * (std::size_t(layer) * plane + px); };
+  for (int y = 0; y < H; ++y)
+    for (int x = 0; x < W; ++x) {
+      std::size_t const px = std::size_t(y) * W + x;
+      float const* g0 = g(0, px);
+      float const* g1 = g(1, px);
+      float const* g2 = g(2, px);
+      float* out = result + 4 * px;
+      if (g2[0] == 0.f && g2[1] == 0.f && g2[2] == 0.f) {
+        float const nx = (float(x) / fw) * 2.f - 1.f, ny = (float(y) / fh) * 2.f - 1.f;
+        v4 const h = fmulv(inv_vp, nx, ny, 1.f, 1.f);
+        v3 const d = normalize(v3{h.x, h.y, h.z});
+        v3 const c = mix3(v3{0.3f, 0.4f, 0.5f}, v3{1.0f, 0.98f, 0.96f}, (d.y + 1.f) / 2.f);
+        out[0] = oracle_half_rn(c.x), out[1] = oracle_half_rn(c.y), out[2] = oracle_half_rn(c.z);
+        out[3] = oracle_half_rn(1.f);
+        continue;
+      }
+      v3 const position{g0[0], g0[1], g0[2]};
+      v3 const to_cam = normalize(cam - position);
+      v3 normal = normalize(v3{g2[0], g2[1], g2[2]});
+      normal = faceforward(normal, -to_cam, normal);
+      v2 const uv{g1[0], g1[1]};
+      int const material = f2i_idx(g2[3]);
+      v4 const sp = fmulv(SV, position.x, position.y, position.z, 1.f);
+      v4 const spx = fmulv(SP, sp.x, sp.y, sp.z, sp.w);
+      float const su = ((spx.x / spx.w) + 1.f) / 2.f, sv = ((spx.y / spx.w) + 1.f) / 2.f;
+      rng_t rng;
+      std::uint32_t const sd =
+          ((seed + 9897584u * f2u_sat(position.x)) ^ f2u_sat(position.y)) ^ f2u_sat(position.z);
+      random_init_nt(rng, x, y, int(sd));
+      float avg = 0.f;
+      int const r = 9;
+      for (int i = 0; i < r; ++i) {
+        float const qx = random_next(rng);
+        float const qy = random_next(rng);
+        float const hx = 2.f * qx - 1.f, hy = 2.f * qy - 1.f;
+        float const u = su + (2.5f * hx) / fs, v = sv + (2.5f * hy) / fs;
+        if (u >= 1.f || v >= 1.f || u < 0.f || v < 0.f) {
+          avg += 1.f;
+          continue;
+        }
+        int const tx = int(std::uint32_t(f2i_idx(std::floor(u * fs))) % std::uint32_t(S));
+        int const ty = int(std::uint32_t(f2i_idx(std::floor(v * fs))) % std::uint32_t(S));
+        float const* m = smap.data() + 4 * (std::size_t(ty) * S + tx);
+        v3 const check = position - 100.f * light;
+        float const l1 = length(check - v3{m[0], m[1], m[2]});
+        avg += (l1 - 100.f < 0.01f) ? 1.f : 0.f;
+      }
+      float const shadow = avg / float(r);
+      material_ctx mc;
+      bool const valid = material >= 0 && material < n_refs;
+      if (valid) mat_open(mc, refs[2 * material], mdata, refs[2 * material + 1]);
+      mc.ps.state = 2;  // s_diffuse
+      v3 refl{0.f, 0.f, 0.f};
+      float pdf = 1.f;
+      mat_evaluate(mc, normal, light, to_cam, refl, pdf, uv, texv.data(), n_textures);
+      v3 refgb{0.f, 0.f, 0.f};
+      float refpdf = 1.f;
+      mc.ps.state = 2;
+      mat_evaluate(mc, normal, normal, to_cam, refgb, refpdf, uv, texv.data(), n_textures);
+      float freeness = 0.f;
+      float dist = 0.1f;
+      for (int i = 0; i < 8; ++i) {
+        do {
+          float const qx = random_next(rng);
+          float const qy = random_next(rng);
+          v2 const hs{2.f * qx - 1.f, 2.f * qy - 1.f};
+          v3 const world = normalize(transform_local_to_world(sample_hemisphere(hs), normal));
+          v3 const test = position + world * dist;
+          v4 const hom = fmulv(pv, test.x, test.y, test.z, 1.f);
+          if (hom.w == 0.f) {
+            freeness += 1.f;
+            break;
+          }
+          float const ox = std::fmin(std::fmax((((hom.x / hom.w) + 1.f) / 2.f) * fw, 0.f), fw - 1.f);
+          float const oy = std::fmin(std::fmax((((hom.y / hom.w) + 1.f) / 2.f) * fh, 0.f), fh - 1.f);
+          std::size_t const o = std::size_t(f2i_idx(oy)) * W + std::size_t(f2i_idx(ox));
+          float const* on = g(2, o);
+          if (on[0] == 0.f && on[1] == 0.f && on[2] == 0.f) {
+            freeness += 1.f;
+            break;
+          }
+          float const* op = g(0, o);
+          float const diff = length(cam - v3{op[0], op[1], op[2]}) - length(cam - test);
+          if (diff > 0.f) {
+            freeness += 1.f;
+            break;
+          }
+          freeness += (diff < -0.2f) ? 1.f : 0.f;
+        } while (false);
+        dist /= 2.f;
+      }
+      freeness /= 1.f * 8.f;
+      float const lcol = 3.f;
+      float const ndl = gmax(0.f, dot(normal, light));
+      v3 const direct = (((lcol * refl) / pdf) * shadow) * ndl;
+      v3 c = freeness * (refgb / refpdf + direct);
+      float const k = 0.7f + 0.4f * random_next(rng);
+      c = c * k;
+      out[0] = oracle_half_rn(c.x), out[1] = oracle_half_rn(c.y), out[2] = oracle_half_rn(c.z);
+      out[3] = oracle_half_rn(1.f * 0.f);
+    }
+}
+
+}  // extern "C"

@@ -58,6 +58,8 @@ def oracle() -> C.CDLL:
             "orc_render_physical": (None, [SZ, P, P, P, P, SZ, P, P, P, P, I, P, I, I, I, C.c_uint32, I, I,
                                            C.c_uint32, P, P, P, P, P, P, I, I, C.c_float, I, P, I]),
             "orc_refbvh_query": (None, [P, P, P, P, P, SZ, I, I, I, P, P, P, P, I]),
+            "orc_forward_render": (None, [I, P, P, P, P, P, I, P, I, I, P, P, C.c_uint32, I, P, P, I, P, P, P, P, P,
+                                          P, P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(h, k)
@@ -329,6 +331,44 @@ def render_reference(scene: dict, width: int, height: int, bounces: int, frames:
                            int(dof), float(lens_size[0]), float(lens_size[1]), float(focus),
                            bokeh_slot + 1 if bokeh_slot >= 0 else 0)
     return accum, display
+
+
+# ---- forward (raster preview) renderer -------------------------------------------
+def forward_render(scene: dict, width: int, height: int, view, proj, random_seed: int, shadow_size: int,
+                   shadow_view, shadow_proj, textures=None, result: bool = True) -> dict:
+    """forward_renderer::run on the CPU (restated passes). Matrices are numpy
+    [4, 4] in math layout. Returns visibility / shadow visibility keys (uint64),
+    gbuffer [3, H, W, 4] and result [H, W, 4] (half-rounded float32),
+    shadow_map [S, S, 4]."""
+    L = oracle()
+    tris9 = np.ascontiguousarray(bake_world_triangles(scene["indices"], scene["vertices"], scene.get("drawables")))
+    nrm, uvs, mat = bake_world_attributes(scene["indices"], scene.get("normals"), scene.get("uvs"),
+                                          scene.get("drawables"), len(scene["vertices"]))
+    refs = np.ascontiguousarray(scene.get("materials", np.zeros((1, 2), np.int32)), np.int32).reshape(-1, 2)
+    mdata = np.ascontiguousarray(scene.get("material_data", np.zeros(7, np.float32)), np.float32).ravel()
+
+    def cm(m):
+        return np.ascontiguousarray(np.asarray(m, np.float32).T).ravel()
+
+    v, p, sv, sp = cm(view), cm(proj), cm(shadow_view), cm(shadow_proj)
+    S = shadow_size
+    out = {"visibility": np.empty((height, width), np.uint64), "shadow_visibility": np.empty((S, S), np.uint64),
+           "gbuffer": np.empty((3, height, width, 4), np.float32), "shadow_map": np.empty((S, S, 4), np.float32),
+           "result": np.empty((height, width, 4), np.float32) if result else None}
+    texs = [None if t is None else (np.ascontiguousarray(t[0], np.float32), int(t[1])) for t in (textures or [])]
+    tex_ptrs = (C.c_void_p * max(1, len(texs)))(*[t[0].ctypes.data if t else None for t in texs])
+    tex_dims = np.array([[t[0].shape[1], t[0].shape[0], t[1]] if t else [0, 0, 0] for t in texs] or [[0, 0, 0]],
+                        np.int32)
+    nrm_c = np.ascontiguousarray(nrm, np.float32) if nrm is not None else None
+    uv_c = np.ascontiguousarray(uvs, np.float32) if uvs is not None else None
+    L.orc_forward_render(tris9.shape[0], tris9.ctypes.data, nrm_c.ctypes.data if nrm_c is not None else None,
+                         uv_c.ctypes.data if uv_c is not None else None, mat.ctypes.data, refs.ctypes.data,
+                         refs.shape[0], mdata.ctypes.data, width, height, v.ctypes.data, p.ctypes.data,
+                         int(random_seed) & 0xFFFFFFFF, S, sv.ctypes.data, sp.ctypes.data, len(texs),
+                         C.cast(tex_ptrs, C.c_void_p), tex_dims.ctypes.data, out["visibility"].ctypes.data,
+                         out["gbuffer"].ctypes.data, out["shadow_visibility"].ctypes.data,
+                         out["shadow_map"].ctypes.data, out["result"].ctypes.data if result else None)
+    return out
 
 
 # ---- SDF ----------------------------------------------------------------------
