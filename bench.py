@@ -55,12 +55,13 @@ def parse_args():
     p.add_argument("--budget-spp", type=int, default=None, help="guiding: plain spp budget (default 256)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=None)
-    p.add_argument("--workload", choices=["closest", "guiding", "pt", "batch", "sdf", "post"], default="closest",
+    p.add_argument("--workload", choices=["closest", "guiding", "pt", "batch", "sdf", "post", "forward"], default="closest",
                    help="closest: closest-hit Mrays/s (with a reduced guided-vs-plain leg); guiding: the full "
                         "time-to-equal-relRMSE run (1024x1024, FP64 4096-spp oracle); pt: plain path tracing "
                         "of the icosphere scene (512x512, 64 spp, depth 8); batch: 16 uneven scenes in one "
                         "CUDA graph per frame; sdf: SDF + mesh hybrid with guiding (768x768, 128 spp); post: the "
-                        "per-frame post-processing chain (bloom, tonemap, FXAA) and denoise on 2048x2048")
+                        "per-frame post-processing chain (bloom, tonemap, FXAA) and denoise on 2048x2048; "
+                        "forward: the raster preview renderer (1920x1080, 2048^2 shadow map)")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain leg of the closest workload")
     a = p.parse_args()
     if a.workload == "closest":
@@ -948,6 +949,88 @@ def run_post_workload(args):
     return 0
 
 
+def run_forward_workload(args):
+    """Forward (raster preview) renderer: one step = forward_renderer::run on
+    the 655,872-triangle icosphere scene at 1920x1080 with the reference's
+    2048^2 light camera (G-buffer pass, shadow pass, resolve). Reports
+    Mpixels/s of the output image and the step's compulsory memory traffic
+    over its duration."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import torch
+
+    import myrt_b200 as mb
+    from myrt_b200.camera import view_projection
+    from myrt_b200.scenes import icosphere_field
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = mb.Context(local)
+    scene = icosphere_field()
+    ctx.upload_scene(**scene)
+    n_tris = sum(int(d.index_count) // 3 for d in scene["drawables"])
+    W, H, S = 1920, 1080, 2048
+    view, proj = view_projection((0, 1.0, -4.5), (0, -0.3, 0), vfov_deg=50, aspect=W / H, near=0.05, far=50.0)
+    for k in range(args.warmup):
+        ctx.forward_render(view, proj, W, H, k)
+    ctx.sync()
+    with ClockSampler(local) as clocks:
+        ms = _timed_frames(ctx.stream, lambda: ctx.forward_render(view, proj, W, H, 11), args.steps) / args.steps
+    out = ctx.forward_read(W, H, S)
+    covered = float((out["visibility"] != np.uint64(0xFFFFFFFFFFFFFFFF)).mean())
+    # end to end: matrices in, the RGBA16F result read back to host memory each step
+    res = np.empty((H, W, 4), np.uint16)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        ctx.forward_render(view, proj, W, H, k)
+        ctx._check(ctx._L.myrt_forward_read(ctx._h, res.ctypes.data, None, None, None), "myrt_forward_read")
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    ctx.close()
+    # compulsory bytes: per triangle and pass, corners 36 B read, set-up record 64 B written and read, count 8 B
+    # written and read, sums 8 B written; per image pixel and pass, key cleared and read (16 B) and the G-buffer
+    # (24 B) or shadow position (16 B) written; per triangle once, normals, uvs, material (76 B) read; resolve:
+    # G-buffer read (24 B) and result written (8 B) per pixel
+    px, spx = W * H, S * S
+    nbytes = n_tris * (2 * (36 + 64 + 64 + 8 + 8 + 8) + 76) + px * (16 + 24) + spx * (16 + 16) + px * (24 + 8)
+    peaks, peak_kind = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    achieved = nbytes / (ms / 1e3) / 1e9
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(Path(__file__).resolve().parent / "oracle"))
+        import pyoracle as po
+
+        sv, sp = mb.forward_default_shadow()
+        t0 = time.perf_counter()
+        po.forward_render(scene, W, H, view, proj, 11, S, sv, sp)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": px / cpu_s / 1e6, "unit": "Mpixels/s", "cores": 1, "kind": "port",
+               "sample": "one full frame (1920x1080, 2048^2 shadow map) of the oracle's restated passes, "
+                         "including its world-space bake", "seconds": cpu_s}
+    line = _render_line(
+        "Mpixels/s forward preview", px / (ms / 1e3) / 1e6, "Mpixels/s", args.steps, args.warmup, ms,
+        {"workload": f"forward renderer: icosphere scene {n_tris:,} tris, {W}x{H} + {S}x{S} shadow map",
+         "triangles": n_tris, "res": [W, H], "shadow_size": S, "covered_pixels": covered,
+         "l2": "the step's buffers (set-up records 42 MB, keys 17 + 34 MB, G-buffer 50 MB, shadow map 67 MB) "
+               "exceed L2 together"},
+        {"roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                      "peak_source": f"hbm_gbs of {peak_kind}", "traffic": None,
+                      "note": "whole step: compulsory bytes of every buffer the three passes touch, read or "
+                              "written once, over the step's CUDA-event duration; the pixel kernel's atomics "
+                              "and the resolve's scattered G-buffer taps are not counted"},
+         "e2e": {"value": px / e2e_s / 1e6, "unit": "Mpixels/s", "h2d_bytes_per_step": 2 * 64,
+                 "d2h_bytes_per_step": px * 8, "api": "myrt_forward_run + myrt_forward_read (result only)"},
+         "frames_per_s": 1e3 / ms,
+         "gpu_launches": 9,
+         "gpu_launches_note": "per step: key fill, set-up, pixels, attributes for each pass, then the resolve "
+                              "(ours), plus CUB's scan of the pixel counts per pass",
+         "cpu_baseline": cpu,
+         "clocks": clocks.summary()})
+    line["dtype"] = "f32 (G-buffer and result stored at f16)"
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -962,6 +1045,8 @@ def main():
         return run_sdf_workload(args)
     if args.workload == "post":
         return run_post_workload(args)
+    if args.workload == "forward":
+        return run_forward_workload(args)
     return run_ours(args)
 
 

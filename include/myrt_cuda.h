@@ -503,6 +503,17 @@ int myrt_guide_get_stats(myrt_ctx* ctx, myrt_guide_stats* out);
 int myrt_read_accumulation_f64(myrt_ctx* ctx, double* rgba_sum);
 /* Device pointers of the two images (valid until the next resolution change). */
 int myrt_render_buffers(myrt_ctx* ctx, void** accum, void** display);
+/* Device pointer of the FP64 accumulation (W*H*4 doubles: rgb sum, sample
+ * count) of a render made with accum_fp64 = 1. */
+int myrt_render_buffer_f64(myrt_ctx* ctx, void** accum64);
+/* Starts a new accumulation whose samples are numbered from first_sample: the
+ * next myrt_render overwrites the images, and in the physical and guided modes
+ * (whose results depend only on pixel, sample index and seed) renders sample
+ * indices first_sample, first_sample + 1, ... No counterpart in the reference:
+ * it lets N processes render disjoint slices of one image's samples and sum
+ * their FP64 accumulations (myrt_b200/multigpu.py). In the reference mode the
+ * accumulation restarts at sample 0. */
+int myrt_begin_samples(myrt_ctx* ctx, uint32_t first_sample);
 /* sequential_pathtracer::invalidate_counter / sample_count / the m_rng seed. */
 int myrt_reset_accumulation(myrt_ctx* ctx);
 int myrt_sample_count(myrt_ctx* ctx, uint32_t* count);

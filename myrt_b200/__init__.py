@@ -404,6 +404,17 @@ class Context:
         self._check(self._L.myrt_guide_get_stats(self._h, C.byref(st)), "myrt_guide_get_stats")
         return {f: getattr(st, f) for f, _ in _abi.myrt_guide_stats._fields_ if f != "pad"}
 
+    def begin_samples(self, first_sample: int):
+        """myrt_begin_samples: the next render starts a new accumulation whose
+        (physical / guided) samples are numbered from first_sample."""
+        self._check(self._L.myrt_begin_samples(self._h, int(first_sample)), "myrt_begin_samples")
+
+    def render_buffer_f64(self) -> int:
+        """Device pointer of the FP64 accumulation (myrt_render_buffer_f64)."""
+        p = C.c_void_p()
+        self._check(self._L.myrt_render_buffer_f64(self._h, C.byref(p)), "myrt_render_buffer_f64")
+        return p.value
+
     def read_accumulation_f64(self, width: int, height: int):
         acc = np.empty((height, width, 4), np.float64)
         self._check(self._L.myrt_read_accumulation_f64(self._h, acc.ctypes.data), "myrt_read_accumulation_f64")

@@ -843,7 +843,14 @@ int myrt_render(myrt_ctx* ctx, myrt_camera const* camera, myrt_render_params con
     R.fp64 = fp64;
     R.sample_counter = 0;
   }
-  return physical ? render_physical_frames(ctx, camera, p) : render_reference_frames(ctx, camera, p);
+  if (R.pending_first >= 0) {  // myrt_begin_samples
+    R.sample_counter = physical ? uint32_t(R.pending_first) : 0u;
+    R.restart = true;
+    R.pending_first = -1;
+  }
+  int const rc = physical ? render_physical_frames(ctx, camera, p) : render_reference_frames(ctx, camera, p);
+  R.restart = false;
+  return rc;
 }
 
 int myrt_set_area_lights(myrt_ctx* ctx, myrt_area_light const* lights, uint32_t n) {
@@ -947,6 +954,23 @@ int myrt_render_buffers(myrt_ctx* ctx, void** accum, void** display) {
 int myrt_reset_accumulation(myrt_ctx* ctx) {
   if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
   ctx->render.sample_counter = 0;
+  ctx->render.pending_first = -1;
+  return MYRT_OK;
+}
+
+int myrt_begin_samples(myrt_ctx* ctx, uint32_t first_sample) {
+  if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
+  if (first_sample > (1u << 30))
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "first sample index above 2^30");
+  ctx->render.pending_first = first_sample;
+  return MYRT_OK;
+}
+
+int myrt_render_buffer_f64(myrt_ctx* ctx, void** accum64) {
+  if (!ctx || !accum64) return MYRT_ERR_INVALID_ARGUMENT;
+  render_state const& R = ctx->render;
+  if (!R.accum64 || !R.fp64) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "no FP64 accumulation in progress");
+  *accum64 = R.accum64;
   return MYRT_OK;
 }
 

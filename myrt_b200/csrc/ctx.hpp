@@ -72,6 +72,8 @@ struct render_state {
   float* pass_tex = nullptr;            // frames * passes * 1024 random texture floats
   size_t pass_tex_capacity = 0;         // in floats
   uint32_t sample_counter = 0;          // frames accumulated since the last reset
+  int64_t pending_first = -1;           // myrt_begin_samples: first sample index of the next render
+  bool restart = false;                 // the next physical render overwrites the images
   float last_camera[32] = {};
   bool have_camera = false;
   int mode = -1;                        // myrt_shading of the accumulation in progress

@@ -787,7 +787,7 @@ int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_pa
   for (auto& w : plan) {
     max_paths = std::max<size_t>(max_paths, w.n_paths);
     pt_job& jj = w.jobs[0];
-    jj.overwrite = (R.sample_counter == 0 && jj.sample_base == 0) ? 1u : 0u;
+    jj.overwrite = ((R.sample_counter == 0 || R.restart) && jj.sample_base == 0) ? 1u : 0u;
     jj.sample_base += R.sample_counter;
   }
   rc = ensure_queues(ctx, P, max_paths);

@@ -6,7 +6,7 @@
 // glMultiDrawElementsIndirect draws them in.
 //
 // One raster pass (the G-buffer pass of forward/vert.vert + frag.frag, and the
-// shadow pass with FORWARD_ONLY_POSITION) is four launches:
+// shadow pass with FORWARD_ONLY_POSITION) is five launches:
 //   k_fwd_setup     one thread per triangle: clip-space corners (proj * view *
 //                   world position), the three edge functions of homogeneous
 //                   rasterisation (Olano & Greer, "Triangle scan conversion
@@ -14,20 +14,23 @@
 //                   window coordinates, the depth plane, the pixel bounding
 //                   box (the whole viewport when a corner has w <= 0) and its
 //                   pixel count
-//   CUB inclusive sum of the counts
-//   k_fwd_pixels    one thread per (triangle, bounding-box pixel) pair, found
-//                   by binary search in the sums, so large and small triangles
-//                   share the grid evenly: coverage at the pixel centre with a
-//                   top-left rule on exact ties, clipping to -1 <= z_ndc <= 1,
-//                   24-bit depth, then a 64-bit atomicMin of (depth << 32 |
-//                   triangle) into the pixel. The minimum is what GL_LESS in
-//                   draw order keeps: the nearest depth, the first-drawn
-//                   triangle among equal depths.
+//   k_fwd_small     triangles whose box holds at most 64 pixels (the bulk of
+//                   a fine mesh): 8 lanes per triangle walk its box
+//   CUB inclusive sum of the larger triangles' 8-pixel row segments
+//   k_fwd_pixels    one thread per (large triangle, row segment), found by
+//                   binary search in the sums, so a triangle covering half
+//                   the screen spreads over the whole grid
 //   k_fwd_attributes  per pixel: the kept triangle's perspective-correct
 //                   barycentrics from the same edge functions, the attributes
 //                   vert.vert passes interpolated and written as frag.frag
 //                   writes them (RGBA16F G-buffer layers, or RGBA32F shadow
 //                   positions)
+// (plus the clear of the depth keys). Per pixel, k_fwd_small and k_fwd_pixels
+// test coverage at the centre with a top-left rule on exact ties, clip to
+// -1 <= z_ndc <= 1, quantise depth to 24 bits and do a 64-bit atomicMin of
+// (depth << 32 | triangle) into the pixel. The minimum is what GL_LESS in draw
+// order keeps: the nearest depth, the first-drawn triangle among equal depths;
+// it does not depend on which kernel or thread got there first.
 // Edge functions of a shared edge are exact negations of each other (same
 // products, operands swapped), so shared edges are watertight. This file is
 // compiled with -fmad=false: every + and * rounds separately, which makes the
@@ -52,7 +55,7 @@ namespace myrt_b200 {
 struct forward_state {
   uint32_t W = 0, H = 0, S = 0;
   float4* rec = nullptr;      // 4 per triangle: edge functions + depth plane, box
-  uint64_t* count = nullptr;  // bounding-box pixels per triangle
+  uint64_t* count = nullptr;  // row segments per large triangle (0 for small ones)
   uint64_t* ends = nullptr;   // inclusive sums of count
   size_t tri_cap = 0;
   void* scan_temp = nullptr;
@@ -70,6 +73,8 @@ using rs::v2;
 using rs::v3;
 
 constexpr unsigned long long kEmpty = ~0ull;
+constexpr uint32_t kSmallBox = 64;  // box pixels handled by one 8-lane group
+constexpr uint32_t kSegment = 8;    // pixels per work item of a large triangle
 
 // 4x4 column-major helpers shared by the host-side matrix set-up
 struct mat4 {
@@ -203,6 +208,7 @@ __global__ void k_fwd_setup(setup_args a) {
   float const det = (e[0][0] * X[0] + e[0][1] * Y[0]) + e[0][2] * Wc[0];
   uint64_t cnt = 0;
   float4* r = a.rec + 4 * size_t(t);
+  float4 box = make_float4(0.f, 0.f, 0.f, 0.f);  // bw = 0: nothing to draw
   if (finite && det != 0.f && isfinite(det)) {
     float const sg = det > 0.f ? 1.f : -1.f, ad = fabsf(det);
     uint32_t flags = 0;
@@ -225,11 +231,12 @@ __global__ void k_fwd_setup(setup_args a) {
       x1 = int(fminf(floorf(ux) + 1.f, float(a.W) - 1.f)), y1 = int(fminf(floorf(uy) + 1.f, float(a.H) - 1.f));
     }
     if (x1 >= x0 && y1 >= y0) {
-      uint32_t const bw = uint32_t(x1 - x0 + 1);
-      cnt = uint64_t(bw) * uint64_t(y1 - y0 + 1);
-      r[3] = make_float4(__int_as_float(x0), __int_as_float(y0), __uint_as_float(bw), __uint_as_float(flags));
+      uint32_t const bw = uint32_t(x1 - x0 + 1), bh = uint32_t(y1 - y0 + 1);
+      if (uint64_t(bw) * bh > kSmallBox) cnt = uint64_t(bh) * ((bw + kSegment - 1) / kSegment);
+      box = make_float4(__int_as_float(x0), __int_as_float(y0), __uint_as_float(bw), __uint_as_float(flags | (bh << 4)));
     }
   }
+  r[3] = box;
   a.count[t] = cnt;
 }
 
@@ -249,6 +256,43 @@ __device__ __forceinline__ bool covered(float4 const* r, uint32_t flags, int x, 
   return in;
 }
 
+// one fragment: coverage, clipping, depth, the keyed depth test
+__device__ __forceinline__ void fragment(float4 const (&q)[3], uint32_t flags, uint32_t t, int x, int y, uint32_t W,
+    unsigned long long* __restrict__ vis) {
+  float const X = float(x) + 0.5f, Y = float(y) + 0.5f;
+  float e[3];
+  bool in = true;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    e[i] = (q[i].x * X + q[i].y * Y) + q[i].z;
+    in = in && (e[i] > 0.f || (e[i] == 0.f && ((flags >> i) & 1u)));
+  }
+  if (!in) return;
+  float const zn = (e[0] * q[0].w + e[1] * q[1].w) + e[2] * q[2].w;
+  if (!(zn >= -1.f && zn <= 1.f)) return;
+  uint32_t const d = __float2uint_rn((zn * 0.5f + 0.5f) * 16777215.f);
+  if (d >= 0xffffffu) return;  // cannot pass GL_LESS against the cleared 1.0
+  unsigned long long const key = (static_cast<unsigned long long>(d) << 32) | t;
+  unsigned long long* dst = vis + size_t(y) * W + x;
+  if (key < *reinterpret_cast<volatile unsigned long long*>(dst)) atomicMin(dst, key);
+}
+
+// triangles with at most kSmallBox box pixels: 8 lanes per triangle
+__global__ void __launch_bounds__(256) k_fwd_small(float4 const* __restrict__ rec, uint32_t n, uint32_t W,
+    unsigned long long* __restrict__ vis) {
+  uint32_t const t = blockIdx.x * (blockDim.x / 8) + threadIdx.x / 8, lane = threadIdx.x % 8;
+  if (t >= n) return;
+  float4 const* r = rec + 4 * size_t(t);
+  float4 const box = __ldg(r + 3);
+  uint32_t const bw = __float_as_uint(box.z), fl = __float_as_uint(box.w), bh = fl >> 4;
+  uint32_t const area = bw * bh;
+  if (bw == 0 || area > kSmallBox) return;
+  float4 const q[3] = {__ldg(r), __ldg(r + 1), __ldg(r + 2)};
+  int const x0 = __float_as_int(box.x), y0 = __float_as_int(box.y);
+  for (uint32_t k = lane; k < area; k += 8) fragment(q, fl & 7u, t, x0 + int(k % bw), y0 + int(k / bw), W, vis);
+}
+
+// larger triangles: one thread per row segment of kSegment pixels
 __global__ void __launch_bounds__(256) k_fwd_pixels(float4 const* __restrict__ rec,
     uint64_t const* __restrict__ ends, uint32_t n, uint32_t W, unsigned long long* __restrict__ vis) {
   if (n == 0) return;
@@ -265,17 +309,13 @@ __global__ void __launch_bounds__(256) k_fwd_pixels(float4 const* __restrict__ r
     uint64_t const local = i - (t ? __ldg(ends + t - 1) : 0ull);
     float4 const* r = rec + 4 * size_t(t);
     float4 const box = __ldg(r + 3);
-    uint32_t const bw = __float_as_uint(box.z);
-    int const x = __float_as_int(box.x) + int(local % bw), y = __float_as_int(box.y) + int(local / bw);
-    cover cv;
-    if (!covered(r, __float_as_uint(box.w), x, y, cv)) continue;
-    float const zn = (cv.e[0] * __ldg(&r[0].w) + cv.e[1] * __ldg(&r[1].w)) + cv.e[2] * __ldg(&r[2].w);
-    if (!(zn >= -1.f && zn <= 1.f)) continue;
-    uint32_t const d = __float2uint_rn((zn * 0.5f + 0.5f) * 16777215.f);
-    if (d >= 0xffffffu) continue;  // cannot pass GL_LESS against the cleared 1.0
-    unsigned long long const key = (static_cast<unsigned long long>(d) << 32) | t;
-    unsigned long long* dst = vis + size_t(y) * W + x;
-    if (key < *reinterpret_cast<volatile unsigned long long*>(dst)) atomicMin(dst, key);
+    uint32_t const bw = __float_as_uint(box.z), fl = __float_as_uint(box.w);
+    uint32_t const segs = (bw + kSegment - 1) / kSegment;
+    float4 const q[3] = {__ldg(r), __ldg(r + 1), __ldg(r + 2)};
+    int const y = __float_as_int(box.y) + int(local / segs);
+    uint32_t const s0 = uint32_t(local % segs) * kSegment, s1 = min(s0 + kSegment, bw);
+    int const x0 = __float_as_int(box.x);
+    for (uint32_t k = s0; k < s1; ++k) fragment(q, fl & 7u, t, x0 + int(k), y, W, vis);
   }
 }
 
@@ -540,6 +580,7 @@ int raster_pass(myrt_ctx* ctx, forward_state& f, mat4 const& pv, uint32_t W, uin
     int rc = check_cuda(ctx, cub::DeviceScan::InclusiveSum(f.scan_temp, tb, f.count, f.ends, int(n), st),
         "forward pixel-count scan");
     if (rc) return rc;
+    k_fwd_small<<<(n + 31) / 32, 256, 0, st>>>(f.rec, n, W, keys);
     k_fwd_pixels<<<std::max(1, ctx->sm_count) * 8, 256, 0, st>>>(f.rec, f.ends, n, W, keys);
   }
   attr_args aa{f.rec, keys, W, H, s.world_pos, s.tri_normals, s.tri_uvs, s.tri_material, gbuf, smap};
