@@ -289,7 +289,12 @@ __global__ void __launch_bounds__(256) k_fwd_small(float4 const* __restrict__ re
   if (bw == 0 || area > kSmallBox) return;
   float4 const q[3] = {__ldg(r), __ldg(r + 1), __ldg(r + 2)};
   int const x0 = __float_as_int(box.x), y0 = __float_as_int(box.y);
-  for (uint32_t k = lane; k < area; k += 8) fragment(q, fl & 7u, t, x0 + int(k % bw), y0 + int(k / bw), W, vis);
+  // k / bw as (k * ceil(2^16 / bw)) >> 16: exact while k * bw < 2^16 (k < 64, bw <= 64 here)
+  uint32_t const inv = (65535u + bw) / bw;
+  for (uint32_t k = lane; k < area; k += 8) {
+    uint32_t const ky = (k * inv) >> 16;
+    fragment(q, fl & 7u, t, x0 + int(k - ky * bw), y0 + int(ky), W, vis);
+  }
 }
 
 // larger triangles: one thread per row segment of kSegment pixels

@@ -73,4 +73,7 @@ def render_sharded(ctx, inverse_view, inverse_projection, width: int, height: in
         acc = accumulation_f64(ctx, width, height)
     else:
         acc = torch.zeros((height, width, 4), dtype=torch.float64, device="cuda")
-    return allreduce_accumulation(acc, group)
+    allreduce_accumulation(acc, group)
+    # the next render on this context writes the same buffer from the library's stream
+    torch.cuda.current_stream().synchronize()
+    return acc
