@@ -281,3 +281,41 @@ def test_phase_timing(ctx, hf128):
         assert ctx.phase_times()["queries"] == 0
     finally:
         ctx.set_phase_timing(False)
+
+
+def test_large_sorted_query_matches_input_order(ctx, hf128):
+    """A device query of more than 2 Mi rays (an odd count) in sorted visiting
+    order: hits, occlusion and per-ray counters equal input order and the
+    oracle."""
+    import torch
+
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = np.concatenate([pinhole_rays(1024, 1024), _rand_rays(1_200_001, seed=31)])
+    rays = rays[np.random.default_rng(5).permutation(rays.shape[0])]
+    n = rays.shape[0]
+    assert n >= 2 << 20
+    d_rays = torch.from_numpy(rays).cuda()
+    out = {}
+    try:
+        for order in (1, 0):
+            ctx.set_tuning(trace_order=order)
+            d_hits = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+            d_occ = torch.empty(n, dtype=torch.uint8, device="cuda")
+            d_n = torch.empty(n, dtype=torch.int32, device="cuda")
+            d_t = torch.empty(n, dtype=torch.int32, device="cuda")
+            torch.cuda.synchronize()
+            ctx.trace_closest_device(d_rays, d_hits)
+            ctx.trace_any_device(d_rays, d_occ)
+            ctx.sync()
+            hits = d_hits.cpu().numpy().copy()
+            ctx.trace_closest_stats_device(d_rays, d_hits, d_n, d_t)
+            ctx.sync()
+            out[order] = (hits, d_occ.cpu().numpy(), d_hits.cpu().numpy(), d_n.cpu().numpy(), d_t.cpu().numpy())
+    finally:
+        ctx.set_tuning()
+    for a, b in zip(out[0], out[1]):  # raw bits: a miss's prim -1 reads as NaN in float32
+        assert np.array_equal(np.ascontiguousarray(a).view(np.uint8), np.ascontiguousarray(b).view(np.uint8))
+    sel = np.random.default_rng(6).choice(n, 200_000, replace=False)
+    ora, cn, ct = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays[sel])
+    assert np.array_equal(out[0][0][sel].view(mb.HIT_DTYPE).ravel(), ora)
+    assert np.array_equal(out[0][3][sel].astype(np.uint32), cn)
