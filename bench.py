@@ -983,7 +983,7 @@ def run_forward_workload(args):
     t0 = time.perf_counter()
     for k in range(args.steps):
         ctx.forward_render(view, proj, W, H, k)
-        ctx._check(ctx._L.myrt_forward_read(ctx._h, res.ctypes.data, None, None, None), "myrt_forward_read")
+        ctx.forward_result(W, H, S, out=res)
     e2e_s = (time.perf_counter() - t0) / args.steps
     ctx.close()
     # compulsory bytes: per triangle and pass, corners 36 B read, set-up record 64 B written and read, count 8 B

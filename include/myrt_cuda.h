@@ -503,6 +503,9 @@ int myrt_guide_get_stats(myrt_ctx* ctx, myrt_guide_stats* out);
 int myrt_read_accumulation_f64(myrt_ctx* ctx, double* rgba_sum);
 /* Device pointers of the two images (valid until the next resolution change). */
 int myrt_render_buffers(myrt_ctx* ctx, void** accum, void** display);
+/* Size of the context's render images (0 x 0 before the first render): the
+ * host arrays of myrt_read_accumulation(_f64) hold width * height * 4 values. */
+int myrt_render_size(myrt_ctx* ctx, uint32_t* width, uint32_t* height);
 /* Device pointer of the FP64 accumulation (W*H*4 doubles: rgb sum, sample
  * count) of a render made with accum_fp64 = 1. */
 int myrt_render_buffer_f64(myrt_ctx* ctx, void** accum64);
@@ -598,10 +601,13 @@ typedef struct myrt_forward_params {
 int myrt_forward_run(myrt_ctx* ctx, const myrt_forward_params* params);
 /* Host copies of the last run (NULL skips one): result RGBA16F as half bits
  * (height * width * 4), G-buffer layers position / uv / normal + material as
- * half bits (3 * height * width * 4), shadow map RGBA32F (size * size * 4),
+ * half bits (3 * height * width * 4), shadow map RGBA32F (shadow_size^2 * 4),
  * visibility keys (height * width: 24-bit depth << 32 | triangle index; all
- * ones where nothing was drawn). Waits for the stream. */
-int myrt_forward_read(myrt_ctx* ctx, uint16_t* result, uint16_t* gbuffer, float* shadow_map, uint64_t* visibility);
+ * ones where nothing was drawn). width, height and shadow_size are the sizes
+ * the host arrays were made for and must equal the last run's (shadow_size 0
+ * = 2048), else MYRT_ERR_INVALID_ARGUMENT. Waits for the stream. */
+int myrt_forward_read(myrt_ctx* ctx, uint32_t width, uint32_t height, uint32_t shadow_size, uint16_t* result,
+    uint16_t* gbuffer, float* shadow_map, uint64_t* visibility);
 /* Device pointers of the same four images (valid until the next run with
  * another size or context destruction). */
 int myrt_forward_buffers(myrt_ctx* ctx, void** result, void** gbuffer, void** shadow_map, void** visibility);

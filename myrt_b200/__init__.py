@@ -302,10 +302,18 @@ class Context:
         gb = np.empty((3, height, width, 4), np.uint16)
         sm = np.empty((shadow_size, shadow_size, 4), np.float32)
         vis = np.empty((height, width), np.uint64)
-        self._check(self._L.myrt_forward_read(self._h, res.ctypes.data, gb.ctypes.data, sm.ctypes.data,
-                                              vis.ctypes.data), "myrt_forward_read")
+        self._check(self._L.myrt_forward_read(self._h, width, height, shadow_size, res.ctypes.data, gb.ctypes.data,
+                                              sm.ctypes.data, vis.ctypes.data), "myrt_forward_read")
         return {"result": res.view(np.float16).astype(np.float32), "gbuffer": gb.view(np.float16).astype(np.float32),
                 "shadow_map": sm, "visibility": vis}
+
+    def forward_result(self, width: int, height: int, shadow_size: int = 2048, out=None) -> np.ndarray:
+        """The last forward run's RGBA16F result as half bits (uint16 [H, W, 4]),
+        copied into `out` when given."""
+        res = out if out is not None else np.empty((height, width, 4), np.uint16)
+        self._check(self._L.myrt_forward_read(self._h, width, height, shadow_size, res.ctypes.data, None, None,
+                                              None), "myrt_forward_read")
+        return res
 
     def forward_buffers(self) -> dict:
         """Device pointers of the last forward run's images."""
@@ -415,7 +423,19 @@ class Context:
         self._check(self._L.myrt_render_buffer_f64(self._h, C.byref(p)), "myrt_render_buffer_f64")
         return p.value
 
+    def render_size(self) -> tuple[int, int]:
+        """(width, height) of the context's render images (myrt_render_size)."""
+        w, h = C.c_uint32(), C.c_uint32()
+        self._check(self._L.myrt_render_size(self._h, C.byref(w), C.byref(h)), "myrt_render_size")
+        return w.value, h.value
+
+    def _check_size(self, width: int, height: int):
+        if (width, height) != self.render_size():
+            raise MyrtError(_abi.MYRT_ERR_INVALID_ARGUMENT,
+                            f"images are {self.render_size()}, not {(width, height)}")
+
     def read_accumulation_f64(self, width: int, height: int):
+        self._check_size(width, height)
         acc = np.empty((height, width, 4), np.float64)
         self._check(self._L.myrt_read_accumulation_f64(self._h, acc.ctypes.data), "myrt_read_accumulation_f64")
         return acc
@@ -436,6 +456,7 @@ class Context:
 
     def read_accumulation(self, width: int, height: int):
         """(rgb sum + count, display) images as float32 [H, W, 4]."""
+        self._check_size(width, height)
         acc = np.empty((height, width, 4), np.float32)
         disp = np.empty((height, width, 4), np.float32)
         self._check(self._L.myrt_read_accumulation(self._h, acc.ctypes.data, disp.ctypes.data),

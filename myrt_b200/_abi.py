@@ -182,8 +182,9 @@ SIGNATURES = {
     "myrt_cubemap_upload": (I, [P, P, U32]),
     "myrt_forward_run": (I, [P, C.POINTER(myrt_forward_params)]),
     "myrt_begin_samples": (I, [P, U32]),
+    "myrt_render_size": (I, [P, C.POINTER(U32), C.POINTER(U32)]),
     "myrt_render_buffer_f64": (I, [P, C.POINTER(P)]),
-    "myrt_forward_read": (I, [P, P, P, P, P]),
+    "myrt_forward_read": (I, [P, U32, U32, U32, P, P, P, P]),
     "myrt_forward_buffers": (I, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(P)]),
     "myrt_forward_default_shadow": (I, [P, P]),
     "myrt_scene_set_transforms": (I, [P, P, C.c_size_t]),

@@ -930,6 +930,14 @@ int myrt_render_noalloc(myrt_ctx* ctx, myrt_camera const* camera, myrt_render_pa
       reinterpret_cast<float4*>(display_rgba), stream ? static_cast<cudaStream_t>(stream) : ctx->stream);
 }
 
+int myrt_render_size(myrt_ctx* ctx, uint32_t* width, uint32_t* height) {
+  if (!ctx || !width || !height) return MYRT_ERR_INVALID_ARGUMENT;
+  bool const any = ctx->render.accum != nullptr;
+  *width = any ? ctx->render.width : 0u;
+  *height = any ? ctx->render.height : 0u;
+  return MYRT_OK;
+}
+
 int myrt_read_accumulation(myrt_ctx* ctx, float* rgba_sum, float* rgba_display) {
   if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
   render_state const& R = ctx->render;

@@ -734,11 +734,13 @@ extern "C" int myrt_forward_run(myrt_ctx* ctx, myrt_forward_params const* params
   return myrt_b200::forward_run(ctx, params);
 }
 
-extern "C" int myrt_forward_read(
-    myrt_ctx* ctx, uint16_t* result, uint16_t* gbuffer, float* shadow_map, uint64_t* visibility) {
+extern "C" int myrt_forward_read(myrt_ctx* ctx, uint32_t width, uint32_t height, uint32_t shadow_size,
+    uint16_t* result, uint16_t* gbuffer, float* shadow_map, uint64_t* visibility) {
   if (!ctx) return MYRT_ERR_INVALID_ARGUMENT;
   myrt_b200::forward_state const* f = ctx->forward;
   if (!f || !f->W) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "no forward run yet");
+  if (width != f->W || height != f->H || (shadow_size ? shadow_size : 2048u) != f->S)
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "read sizes differ from the last forward run");
   int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
   size_t const px = size_t(f->W) * f->H, spx = size_t(f->S) * f->S;
   cudaStream_t const st = ctx->stream;

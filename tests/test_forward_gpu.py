@@ -124,3 +124,9 @@ def test_forward_rejects_bad_sizes(ctx):
         ctx.forward_render(view, proj, 0, 16, 1)
     with pytest.raises(MyrtError):
         ctx.forward_render(view, proj, 16, 16, 1, shadow_size=20000)
+    ctx.forward_render(view, proj, 16, 12, 1, shadow_size=64)
+    with pytest.raises(MyrtError):  # host arrays made for another size are refused
+        ctx.forward_read(16, 12, 2048)
+    with pytest.raises(MyrtError):
+        ctx.forward_result(12, 16, 64)
+    assert ctx.forward_result(16, 12, 64).shape == (12, 16, 4)
