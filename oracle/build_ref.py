@@ -20,6 +20,10 @@ What it compiles, from the sources where they lie under the reference tree
     - float literals without a suffix get ``f`` (GLSL literals are float);
     - per-invocation globals become ``thread_local``.
   The rewritten copies go to oracle/_ref/glsl/.
+* The post-processing shaders src/pt/pp_*.comp (ref_harness_post.cpp) and the
+  forward renderer's resolve pass src/pt/forward/resolve.frag
+  (ref_harness_glsl.cpp, see resolve_to_cpp), with the rewrites their
+  converters list.
 
 Output: oracle/_ref/libmyrt_ref.so (git-ignored; it travels with the tree).
 The reference tree is only needed at build time.
@@ -175,6 +179,38 @@ def pp_to_cpp(name: str, src: str) -> str:
     return glsl_to_cpp(src, globals_thread_local=False)
 
 
+def resolve_to_cpp(src: str) -> str:
+    """src/pt/forward/resolve.frag as C++ for ref_harness_glsl.cpp, which
+    includes it inside a namespace of its own after the helper files and the
+    material dispatch: the #version / #extension lines and the #include lines
+    go (the harness included those files already), interface qualifiers go
+    (`layout(...)`, `uniform`, `flat in`, `out` on globals: the harness sets the
+    globals per fragment), the two storage buffers become pointers, main
+    becomes resolve_main, `uint(x)` of a float becomes to_uint(x) (the
+    conversion GLSL leaves undefined for negative values; the harness gives
+    NVIDIA's: truncate, saturate, NaN -> 0), and the one swizzle assignment
+    `color.rgb = ...` is spelled out per component."""
+    src = re.sub(r"^#version.*$", "", src, flags=re.M)
+    src = re.sub(r"^#extension.*$", "", src, flags=re.M)
+    src, n = re.subn(r'^#include\s+"[^"]*"\s*$', "", src, flags=re.M)
+    assert n == 4, f"resolve.frag: expected 4 includes, found {n}"
+    src, n = re.subn(r"layout\([^)]*\)\s*restrict\s+readonly\s+buffer\s+\w+\s*\{\s*(\w+)\s+(\w+)\[\]\s*;\s*\}\s*;",
+                     r"\1 const* \2 = nullptr;", src)
+    assert n == 2, "resolve.frag: storage buffers changed"
+    src = re.sub(r"layout\([^)]*\)\s*", "", src)
+    src = re.sub(r"^\s*flat\s+in\s+", "", src, flags=re.M)
+    src = re.sub(r"^\s*out\s+(?=vec4\s+color\s*;)", "", src, flags=re.M)
+    src = re.sub(r"\buniform\s+", "", src)
+    src, n = re.subn(r"\bvoid\s+main\s*\(\s*\)", "void resolve_main()", src)
+    assert n == 1, "resolve.frag: main not found"
+    src, n = re.subn(r"\buint\((?=position\.)", "to_uint(", src)
+    assert n == 3, f"resolve.frag: expected 3 uint(position.*) conversions, found {n}"
+    src, n = re.subn(r"color\.rgb\s*=\s*background\(ray_direction\);",
+                     "{ vec3 _t = background(ray_direction); color.x = _t.x; color.y = _t.y; color.z = _t.z; }", src)
+    assert n == 1, "resolve.frag: background assignment changed"
+    return glsl_to_cpp(src, globals_thread_local=False)
+
+
 def write_sources() -> None:
     (OUT / "src").mkdir(parents=True, exist_ok=True)
     (OUT / "glsl").mkdir(parents=True, exist_ok=True)
@@ -193,6 +229,8 @@ def write_sources() -> None:
         extract_sdf_snippets((REF_ROOT / "src/pathtracer/sdf.hpp").read_text()))
     for name in PP_SHADERS:
         (OUT / "glsl" / f"{name}.inc").write_text(pp_to_cpp(name, (REF_ROOT / "src/pt" / f"{name}.comp").read_text()))
+    (OUT / "glsl/forward_resolve.inc").write_text(
+        resolve_to_cpp((REF_ROOT / "src/pt/forward/resolve.frag").read_text()))
 
 
 def compile_ref() -> Path:

@@ -85,6 +85,7 @@ struct vec4 {
     struct { float r, g, b, a; };
     swz3<0, 1, 2, 4> xyz;
     swz3<0, 1, 2, 4> rgb;
+    swz2<0, 1, 4> xy;
     float d[4];
   };
   vec4() : x(0), y(0), z(0), w(0) {}
@@ -92,11 +93,13 @@ struct vec4 {
   template <typename A, typename B, typename C, typename D>
   vec4(A a, B b, C c, D e) : x(float(a)), y(float(b)), z(float(c)), w(float(e)) {}
   template <typename S> vec4(vec3 const& v, S s) : x(v.x), y(v.y), z(v.z), w(float(s)) {}
+  template <typename A, typename B> vec4(vec2 const& v, A a, B b) : x(v.x), y(v.y), z(float(a)), w(float(b)) {}
   vec4(vec4 const& o) : x(o.x), y(o.y), z(o.z), w(o.w) {}
   vec4& operator=(vec4 const& o) { x = o.x; y = o.y; z = o.z; w = o.w; return *this; }
   float& operator[](int i) { return d[i]; }
   float operator[](int i) const { return d[i]; }
   vec4& operator+=(vec4 const& o) { x += o.x; y += o.y; z += o.z; w += o.w; return *this; }
+  vec4& operator*=(vec4 const& o) { x *= o.x; y *= o.y; z *= o.z; w *= o.w; return *this; }
 };
 
 template <int I0, int I1, int I2, int N> swz3<I0, I1, I2, N>::operator vec3() const {
@@ -120,6 +123,8 @@ struct ivec2 {
   int x = 0, y = 0;
   ivec2() = default;
   template <typename A, typename B> ivec2(A a, B b) : x(int(a)), y(int(b)) {}
+  explicit ivec2(vec2 const& v) : x(int(v.x)), y(int(v.y)) {}
+  operator vec2() const { return vec2(x, y); }  // GLSL's implicit ivec2 -> vec2
 };
 struct uvec2 {
   uint x = 0, y = 0;
@@ -129,7 +134,9 @@ struct uvec2 {
 };
 inline bool operator!=(uvec2 a, uvec2 b) { return a.x != b.x || a.y != b.y; }
 
+struct bvec2 { bool x, y; };
 struct bvec3 { bool x, y, z; };
+inline bool any(bvec2 b) { return b.x || b.y; }
 struct bvec4 { bool x, y, z, w; };
 inline bool any(bvec3 b) { return b.x || b.y || b.z; }
 inline bool any(bvec4 b) { return b.x || b.y || b.z || b.w; }
@@ -142,6 +149,11 @@ inline vec2 operator*(float s, vec2 a) { return vec2(s * a.x, s * a.y); }
 inline vec2 operator*(vec2 a, vec2 b) { return vec2(a.x * b.x, a.y * b.y); }
 inline vec2 operator/(vec2 a, vec2 b) { return vec2(a.x / b.x, a.y / b.y); }
 inline vec2 operator/(vec2 a, float s) { return vec2(a.x / s, a.y / s); }
+inline vec2 operator+(vec2 a, float s) { return vec2(a.x + s, a.y + s); }
+inline vec2 operator-(vec2 a, float s) { return vec2(a.x - s, a.y - s); }
+inline vec2& operator*=(vec2& a, vec2 b) { a.x *= b.x; a.y *= b.y; return a; }
+inline bvec2 greaterThanEqual(vec2 a, vec2 b) { return {a.x >= b.x, a.y >= b.y}; }
+inline bvec2 lessThan(vec2 a, vec2 b) { return {a.x < b.x, a.y < b.y}; }
 
 // ---- vec3 ----
 inline vec3 operator+(vec3 const& a, vec3 const& b) { return vec3(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -153,6 +165,7 @@ inline vec3 operator*(float s, vec3 const& a) { return vec3(s * a.x, s * a.y, s 
 inline vec3 operator/(vec3 const& a, float s) { return vec3(a.x / s, a.y / s, a.z / s); }
 inline vec3 operator/(float s, vec3 const& a) { return vec3(s / a.x, s / a.y, s / a.z); }
 inline vec3 operator+(vec3 const& a, float s) { return vec3(a.x + s, a.y + s, a.z + s); }
+inline vec3 operator+(float s, vec3 const& a) { return vec3(s + a.x, s + a.y, s + a.z); }
 inline vec3 operator-(vec3 const& a, float s) { return vec3(a.x - s, a.y - s, a.z - s); }
 inline vec3 operator-(vec3 const& a) { return vec3(-a.x, -a.y, -a.z); }
 inline bool operator==(vec3 const& a, vec3 const& b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
@@ -182,6 +195,7 @@ inline bool isnan(float v) { return std::isnan(v); }
 inline bool isinf(float v) { return std::isinf(v); }
 inline float mix(float a, float b, float t) { return a * (1.f - t) + b * t; }
 
+inline vec2 clamp(vec2 v, vec2 lo, vec2 hi) { return vec2(min(max(v.x, lo.x), hi.x), min(max(v.y, lo.y), hi.y)); }
 inline vec3 min(vec3 const& a, vec3 const& b) { return vec3(min(a.x, b.x), min(a.y, b.y), min(a.z, b.z)); }
 inline vec3 max(vec3 const& a, vec3 const& b) { return vec3(max(a.x, b.x), max(a.y, b.y), max(a.z, b.z)); }
 inline vec3 clamp(vec3 const& v, float lo, float hi) {
@@ -238,6 +252,59 @@ inline vec4 operator*(mat4 const& m, vec4 const& v) {
   vec4 r;
   for (int k = 0; k < 4; ++k)
     r[k] = ((m.c[0][k] * v.x + m.c[1][k] * v.y) + m.c[2][k] * v.z) + m.c[3][k] * v.w;
+  return r;
+}
+// products summed left to right over k, no fused multiply-add
+inline mat4 operator*(mat4 const& a, mat4 const& b) {
+  mat4 c;
+  for (int col = 0; col < 4; ++col)
+    for (int r = 0; r < 4; ++r) {
+      float s = a.c[0][r] * b.c[col][0];
+      for (int k = 1; k < 4; ++k) s = s + a.c[k][r] * b.c[col][k];
+      c.c[col][r] = s;
+    }
+  return c;
+}
+// inverse by cofactors in double, rounded once to float (GLSL leaves the method
+// to the implementation)
+inline mat4 inverse(mat4 const& a) {
+  double m[16], inv[16];
+  for (int i = 0; i < 16; ++i) m[i] = a.c[i / 4][i % 4];
+  inv[0] = m[5] * m[10] * m[15] - m[5] * m[11] * m[14] - m[9] * m[6] * m[15] + m[9] * m[7] * m[14] +
+      m[13] * m[6] * m[11] - m[13] * m[7] * m[10];
+  inv[4] = -m[4] * m[10] * m[15] + m[4] * m[11] * m[14] + m[8] * m[6] * m[15] - m[8] * m[7] * m[14] -
+      m[12] * m[6] * m[11] + m[12] * m[7] * m[10];
+  inv[8] = m[4] * m[9] * m[15] - m[4] * m[11] * m[13] - m[8] * m[5] * m[15] + m[8] * m[7] * m[13] +
+      m[12] * m[5] * m[11] - m[12] * m[7] * m[9];
+  inv[12] = -m[4] * m[9] * m[14] + m[4] * m[10] * m[13] + m[8] * m[5] * m[14] - m[8] * m[6] * m[13] -
+      m[12] * m[5] * m[10] + m[12] * m[6] * m[9];
+  inv[1] = -m[1] * m[10] * m[15] + m[1] * m[11] * m[14] + m[9] * m[2] * m[15] - m[9] * m[3] * m[14] -
+      m[13] * m[2] * m[11] + m[13] * m[3] * m[10];
+  inv[5] = m[0] * m[10] * m[15] - m[0] * m[11] * m[14] - m[8] * m[2] * m[15] + m[8] * m[3] * m[14] +
+      m[12] * m[2] * m[11] - m[12] * m[3] * m[10];
+  inv[9] = -m[0] * m[9] * m[15] + m[0] * m[11] * m[13] + m[8] * m[1] * m[15] - m[8] * m[3] * m[13] -
+      m[12] * m[1] * m[11] + m[12] * m[3] * m[9];
+  inv[13] = m[0] * m[9] * m[14] - m[0] * m[10] * m[13] - m[8] * m[1] * m[14] + m[8] * m[2] * m[13] +
+      m[12] * m[1] * m[10] - m[12] * m[2] * m[9];
+  inv[2] = m[1] * m[6] * m[15] - m[1] * m[7] * m[14] - m[5] * m[2] * m[15] + m[5] * m[3] * m[14] +
+      m[13] * m[2] * m[7] - m[13] * m[3] * m[6];
+  inv[6] = -m[0] * m[6] * m[15] + m[0] * m[7] * m[14] + m[4] * m[2] * m[15] - m[4] * m[3] * m[14] -
+      m[12] * m[2] * m[7] + m[12] * m[3] * m[6];
+  inv[10] = m[0] * m[5] * m[15] - m[0] * m[7] * m[13] - m[4] * m[1] * m[15] + m[4] * m[3] * m[13] +
+      m[12] * m[1] * m[7] - m[12] * m[3] * m[5];
+  inv[14] = -m[0] * m[5] * m[14] + m[0] * m[6] * m[13] + m[4] * m[1] * m[14] - m[4] * m[2] * m[13] -
+      m[12] * m[1] * m[6] + m[12] * m[2] * m[5];
+  inv[3] = -m[1] * m[6] * m[11] + m[1] * m[7] * m[10] + m[5] * m[2] * m[11] - m[5] * m[3] * m[10] -
+      m[9] * m[2] * m[7] + m[9] * m[3] * m[6];
+  inv[7] = m[0] * m[6] * m[11] - m[0] * m[7] * m[10] - m[4] * m[2] * m[11] + m[4] * m[3] * m[10] +
+      m[8] * m[2] * m[7] - m[8] * m[3] * m[6];
+  inv[11] = -m[0] * m[5] * m[11] + m[0] * m[7] * m[9] + m[4] * m[1] * m[11] - m[4] * m[3] * m[9] -
+      m[8] * m[1] * m[7] + m[8] * m[3] * m[5];
+  inv[15] = m[0] * m[5] * m[10] - m[0] * m[6] * m[9] - m[4] * m[1] * m[10] + m[4] * m[2] * m[9] +
+      m[8] * m[1] * m[6] - m[8] * m[2] * m[5];
+  double const det = m[0] * inv[0] + m[1] * inv[4] + m[2] * inv[8] + m[3] * inv[12];
+  mat4 r;
+  for (int i = 0; i < 16; ++i) r.c[i / 4][i % 4] = float(inv[i] / det);
   return r;
 }
 inline mat4 transpose(mat4 const& m) {

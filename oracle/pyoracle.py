@@ -97,6 +97,7 @@ def ref() -> C.CDLL:
             "ref_sdf_map": (None, [P, P, P, I, P, SZ, I, P, P, P]),
             "ref_sdf_trace": (None, [P, P, P, P, I, P, SZ, I, C.c_float, I, P, P, P, P, P, P]),
             "ref_post_pass": (I, [I, P, P, P, I, I, P, I, I, P]),
+            "ref_forward_resolve": (None, [I, I, P, P, I, P, P, P, P, C.c_uint32, P, P, P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(h, k)
@@ -368,6 +369,29 @@ def forward_render(scene: dict, width: int, height: int, view, proj, random_seed
                          C.cast(tex_ptrs, C.c_void_p), tex_dims.ctypes.data, out["visibility"].ctypes.data,
                          out["gbuffer"].ctypes.data, out["shadow_visibility"].ctypes.data,
                          out["shadow_map"].ctypes.data, out["result"].ctypes.data if result else None)
+    return out
+
+
+def ref_forward_resolve(gbuffer, shadow_map, view, proj, shadow_view, shadow_proj, random_seed: int, materials,
+                        material_data) -> np.ndarray:
+    """The reference's own forward/resolve.frag (compiled by oracle/build_ref.py)
+    over a G-buffer [3, H, W, 4] and a shadow map [S, S, 4]; returns the colour
+    [H, W, 4] before the RGBA16F store."""
+    L = ref()
+    g = np.ascontiguousarray(gbuffer, np.float32)
+    sm = np.ascontiguousarray(shadow_map, np.float32)
+    H, W = g.shape[1], g.shape[2]
+
+    def cm(m):
+        return np.ascontiguousarray(np.asarray(m, np.float32).T).ravel()
+
+    v, p, sv, sp = cm(view), cm(proj), cm(shadow_view), cm(shadow_proj)
+    refs = np.ascontiguousarray(materials, np.int32).reshape(-1, 2)
+    md = np.ascontiguousarray(material_data, np.float32).ravel()
+    out = np.empty((H, W, 4), np.float32)
+    L.ref_forward_resolve(W, H, g.ctypes.data, sm.ctypes.data, sm.shape[0], v.ctypes.data, p.ctypes.data,
+                          sv.ctypes.data, sp.ctypes.data, int(random_seed) & 0xFFFFFFFF, refs.ctypes.data,
+                          md.ctypes.data, out.ctypes.data)
     return out
 
 

@@ -398,3 +398,118 @@ void ref_sdf_trace(int const* instrs, int const* programs, float const* params, 
 }
 
 }  // extern "C"
+
+// ---- the forward renderer's resolve pass: src/pt/forward/resolve.frag ----------------------
+// build_ref.py rewrites the shader (resolve_to_cpp) into forward_resolve.inc; it runs
+// here once per fragment over host G-buffer and shadow-map images, with the
+// material dispatch material_registry::generate_code emits for the one PBR type
+// (src/material.hpp:39-65) and what a GL fragment invocation provides:
+//   * gl_FragCoord = (x + 0.5, y + 0.5) (pixel centres; only .xy is read);
+//   * cam_pos = inverse(view)[3].xyz, as forward/resolve.vert:17 passes it;
+//   * texelFetch on the G-buffer array returns 0 outside the image;
+//   * texture(shadow_map, uv) samples the nearest texel of level 0 (the
+//     sampler's default GL_NEAREST_MIPMAP_LINEAR minifies here: the shadow taps
+//     jitter by texels from fragment to fragment);
+//   * dFdx / dFdy: the shader computes them but never uses the result, so they
+//     return 0;
+//   * every per-invocation global (pbr_state, after_sample, resample_factor,
+//     the material type) starts at its initial value for each fragment.
+namespace glsl {
+namespace fwd {
+
+uint cmattype = ~0u;
+void open(uint type, uint buf) {
+  cmattype = type;
+  switch (type) {
+    case 0: material_load_mat_(buf); break;
+  }
+}
+void evaluate(vec3 p, vec2 uv, vec3 n, vec3 tl, vec3 tv, vec3& ref, float& pdf) {
+  ref = vec3(0, 0, 0);
+  pdf = 1;
+  if (cmattype == ~0u) return;
+  switch (cmattype) {
+    case 0: material_evaluate_(p, uv, n, tl, tv, ref, pdf); break;
+  }
+}
+
+struct ivec3 {
+  int x, y, z;
+  ivec3(ivec2 v, int c) : x(v.x), y(v.y), z(c) {}
+  ivec3(vec2 v, int c) : x(int(v.x)), y(int(v.y)), z(c) {}
+};
+struct ivec3_size {
+  ivec2 xy;
+  int z;
+};
+struct sampler2DArray {
+  float const* data = nullptr;  // layer-major RGBA floats
+  int w = 0, h = 0, layers = 0;
+};
+inline vec4 texelFetch(sampler2DArray const& s, ivec3 p, int) {
+  if (p.x < 0 || p.y < 0 || p.z < 0 || p.x >= s.w || p.y >= s.h || p.z >= s.layers) return vec4(0.f);
+  float const* q = s.data + 4 * ((size_t(p.z) * s.h + p.y) * s.w + p.x);
+  return vec4(q[0], q[1], q[2], q[3]);
+}
+inline ivec3_size textureSize(sampler2DArray const& s, int) { return {ivec2(s.w, s.h), s.layers}; }
+struct sampler2D {
+  float const* data = nullptr;  // RGBA floats, size x size
+  int size = 0;
+};
+inline ivec2 textureSize(sampler2D const& s, int) { return ivec2(s.size, s.size); }
+inline int nearest_texel(float u, int size) {
+  float const f = std::floor(u * float(size));
+  int const i = (f > -2147483648.f && f < 2147483648.f) ? int(f) : 0;
+  return int(uint(i) % uint(size));  // GL_REPEAT
+}
+inline vec4 texture(sampler2D const& s, vec2 uv) {
+  float const* q = s.data + 4 * (size_t(nearest_texel(uv.y, s.size)) * s.size + nearest_texel(uv.x, s.size));
+  return vec4(q[0], q[1], q[2], q[3]);
+}
+inline vec3 dFdx(vec3 const&) { return vec3(0.f); }
+inline vec3 dFdy(vec3 const&) { return vec3(0.f); }
+inline uint to_uint(float f) {
+  if (!(f > 0.f)) return 0u;
+  if (f >= 4294967296.f) return 0xffffffffu;
+  return uint(f);
+}
+vec4 gl_FragCoord;
+
+#include "forward_resolve.inc"
+
+}  // namespace fwd
+}  // namespace glsl
+
+extern "C" void ref_forward_resolve(int width, int height, float const* gbuf, float const* smap, int shadow_size,
+    float const* view, float const* proj, float const* shadow_view, float const* shadow_proj, std::uint32_t seed,
+    std::int32_t const* refs, float const* mdata, float* out) {
+  namespace f = glsl::fwd;
+  auto m4 = [](float const* p) {
+    glsl::mat4 m;
+    for (int i = 0; i < 16; ++i) m.c[i / 4][i % 4] = p[i];
+    return m;
+  };
+  f::view = m4(view);
+  f::proj = m4(proj);
+  f::shadow_view = m4(shadow_view);
+  f::shadow_proj = m4(shadow_proj);
+  f::random_seed = seed;
+  f::gbuffer = f::sampler2DArray{gbuf, width, height, 3};
+  f::shadow_map = f::sampler2D{smap, shadow_size};
+  f::materials = reinterpret_cast<f::material_reference_t const*>(refs);
+  f::materials_data = mdata;
+  glsl::g_material_data = mdata;
+  f::cam_pos = glsl::inverse(f::view)[3].xyz;
+  for (int y = 0; y < height; ++y)
+    for (int x = 0; x < width; ++x) {
+      f::gl_FragCoord = glsl::vec4(float(x) + 0.5f, float(y) + 0.5f, 0.f, 1.f);
+      glsl::pbr_state = -1;
+      glsl::after_sample = false;
+      glsl::resample_factor = 1.f;
+      f::cmattype = ~0u;
+      f::color = glsl::vec4(0.f);
+      f::resolve_main();
+      float* o = out + 4 * (size_t(y) * width + x);
+      o[0] = f::color.x, o[1] = f::color.y, o[2] = f::color.z, o[3] = f::color.w;
+    }
+}

@@ -2,6 +2,7 @@
 answers and against ray casting, and the library's light camera against the
 restatement of forward_renderer.cpp:306-310. CPU only."""
 import numpy as np
+import pytest
 
 import pyoracle as po
 from myrt_b200 import forward_default_shadow
@@ -139,3 +140,22 @@ def test_oracle_forward_resolve_is_finite_and_lit():
     assert fg.any() and (~fg).any()
     assert (res[..., 3][fg] == 0).all() and (res[..., 3][~fg] == 1).all()
     assert res[fg][:, :3].mean() > 0.01
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("seed,eye", [(7, (0, 1.0, -4.0)), (123456789, (1.5, 0.4, -2.5))])
+def test_resolve_pinned_to_the_reference_shader(seed, eye):
+    """The oracle's resolve pass equals the reference's own resolve.frag
+    (compiled as C++ by oracle/build_ref.py) run on the same G-buffer and
+    shadow map, bit for bit after the RGBA16F store."""
+    s = icosphere_field(n_spheres=8, subdiv=1, floor_cells=2, seed=3)
+    W, H = 48, 36
+    view, proj = view_projection(eye, (0, -0.3, 0), vfov_deg=55, aspect=W / H)
+    sv, sp = forward_default_shadow()
+    out = po.forward_render(s, W, H, view, proj, seed, 256, sv, sp)
+    ref = po.ref_forward_resolve(out["gbuffer"], out["shadow_map"], view, proj, sv, sp, seed, s["materials"],
+                                 s["material_data"])
+    ref16 = ref.astype(np.float16).astype(np.float32)
+    fg = out["visibility"] != EMPTY
+    assert fg.mean() > 0.2
+    assert np.array_equal(out["result"], ref16, equal_nan=True)
