@@ -20,10 +20,11 @@ What it compiles, from the sources where they lie under the reference tree
     - float literals without a suffix get ``f`` (GLSL literals are float);
     - per-invocation globals become ``thread_local``.
   The rewritten copies go to oracle/_ref/glsl/.
-* The post-processing shaders src/pt/pp_*.comp (ref_harness_post.cpp) and the
-  forward renderer's resolve pass src/pt/forward/resolve.frag
-  (ref_harness_glsl.cpp, see resolve_to_cpp), with the rewrites their
-  converters list.
+* The post-processing shaders src/pt/pp_*.comp (ref_harness_post.cpp), the
+  forward renderer's resolve pass src/pt/forward/resolve.frag and the path
+  tracer's generate and color passes src/pt/pt_generate.comp,
+  src/pt/pt_color.comp with src/pt/bokeh.glsl (ref_harness_glsl.cpp, see
+  resolve_to_cpp and pass_to_cpp), with the rewrites their converters list.
 
 Output: oracle/_ref/libmyrt_ref.so (git-ignored; it travels with the tree).
 The reference tree is only needed at build time.
@@ -211,6 +212,49 @@ def resolve_to_cpp(src: str) -> str:
     return glsl_to_cpp(src, globals_thread_local=False)
 
 
+PASS_SHADERS = {"pt_color": 4, "pt_generate": 3}  # shader -> #include lines it has
+
+
+def pass_to_cpp(name: str, src: str) -> str:
+    """A path-tracer pass (pt_generate.comp, pt_color.comp) as C++ for
+    ref_harness_glsl.cpp, which includes it in a namespace of its own after the
+    helper files, the material dispatch and the GL stand-ins (images, samplers,
+    gl_GlobalInvocationID): the #version / #extension lines, the work-group
+    layout, the bindless-sampler default and the #include lines go; a storage
+    buffer holding one array becomes a pointer and one holding scalars becomes
+    those scalars; interface qualifiers (`layout(...)`, `uniform`) go; main
+    becomes pass_main; the unsuffixed literal 2341335623, which GLSL makes an
+    int with that bit pattern (GLSL 4.60, 4.1.3), is written as such; the one
+    array assignment `result.pad = float[2](0,0);` is spelled out; the two
+    random draws in one argument list of pt_color.comp are hoisted in source
+    order (GLSL evaluates arguments left to right, C++ leaves it open)."""
+    src = re.sub(r"^#version.*$", "", src, flags=re.M)
+    src = re.sub(r"^#extension.*$", "", src, flags=re.M)
+    src, n = re.subn(r"^layout\(local_size_x[^)]*\)\s*in\s*;", "", src, flags=re.M)
+    assert n == 1, f"{name}: work-group layout not found"
+    src = re.sub(r"^layout\(bindless_sampler\)\s*uniform\s*;", "", src, flags=re.M)
+    src, n = re.subn(r'^#include\s+"[^"]*"\s*$', "", src, flags=re.M)
+    assert n == PASS_SHADERS[name], f"{name}: expected {PASS_SHADERS[name]} includes, found {n}"
+    src = re.sub(r"layout\([^)]*\)\s*(?:restrict\s+)?(?:readonly\s+|writeonly\s+)?buffer\s+\w+\s*"
+                 r"\{\s*(\w+)\s+(\w+)\[\]\s*;\s*\}\s*;", r"\1* \2 = nullptr;", src)
+    src = re.sub(r"layout\([^)]*\)\s*(?:restrict\s+)?(?:readonly\s+)?buffer\s+\w+\s*\{([^}]*)\}\s*;", r"\1", src)
+    assert "buffer" not in re.sub(r"//.*", "", src), f"{name}: a storage buffer was not rewritten"
+    src = re.sub(r"layout\([^)]*\)\s*", "", src)
+    src = re.sub(r"\buniform\s+", "", src)
+    src, n = re.subn(r"\bvoid\s+main\s*\(\s*\)", "void pass_main()", src)
+    assert n == 1, f"{name}: main not found"
+    src = src.replace("2341335623", "int(2341335623u)")
+    src = src.replace("result.pad = float[2](0,0);", "result.pad[0] = 0; result.pad[1] = 0;")
+    if name == "pt_color":
+        src, n = re.subn(r"vec2 material_randoms = vec2\(random_next\(\), random_next\(\)\);",
+                         "float _r0 = random_next(); float _r1 = random_next(); vec2 material_randoms = vec2(_r0, _r1);",
+                         src)
+        assert n == 1, "pt_color: material_randoms changed"
+    assert not re.search(r"\([^()]*random_\w+\([^()]*\)[^()]*,[^()]*random_\w+\(", src), \
+        f"{name}: another argument list with two random draws"
+    return glsl_to_cpp(src, globals_thread_local=False)
+
+
 def write_sources() -> None:
     (OUT / "src").mkdir(parents=True, exist_ok=True)
     (OUT / "glsl").mkdir(parents=True, exist_ok=True)
@@ -231,6 +275,10 @@ def write_sources() -> None:
         (OUT / "glsl" / f"{name}.inc").write_text(pp_to_cpp(name, (REF_ROOT / "src/pt" / f"{name}.comp").read_text()))
     (OUT / "glsl/forward_resolve.inc").write_text(
         resolve_to_cpp((REF_ROOT / "src/pt/forward/resolve.frag").read_text()))
+    for name in PASS_SHADERS:
+        (OUT / "glsl" / f"{name}.inc").write_text(pass_to_cpp(name, (REF_ROOT / "src/pt" / f"{name}.comp").read_text()))
+    (OUT / "glsl/bokeh.inc").write_text(glsl_to_cpp((REF_ROOT / "src/pt/bokeh.glsl").read_text(),
+                                                    globals_thread_local=False))
 
 
 def compile_ref() -> Path:

@@ -68,6 +68,7 @@ struct vec3 {
   vec3() : x(0), y(0), z(0) {}
   template <typename S> requires std::is_arithmetic_v<S> explicit vec3(S s) : x(float(s)), y(float(s)), z(float(s)) {}
   template <typename A, typename B, typename C> vec3(A a, B b, C c) : x(float(a)), y(float(b)), z(float(c)) {}
+  template <typename S> vec3(vec2 const& v, S s) : x(v.x), y(v.y), z(float(s)) {}
   vec3(vec3 const& o) : x(o.x), y(o.y), z(o.z) {}
   vec3& operator=(vec3 const& o) { x = o.x; y = o.y; z = o.z; return *this; }
   float& operator[](int i) { return d[i]; }
@@ -131,6 +132,8 @@ struct uvec2 {
   uvec2() = default;
   template <typename S> explicit uvec2(S s) : x(uint(s)), y(uint(s)) {}
   template <typename A, typename B> uvec2(A a, B b) : x(uint(a)), y(uint(b)) {}
+  explicit operator vec2() const { return vec2(x, y); }
+  explicit operator ivec2() const { return ivec2(int(x), int(y)); }
 };
 inline bool operator!=(uvec2 a, uvec2 b) { return a.x != b.x || a.y != b.y; }
 

@@ -12,7 +12,7 @@
 //   emits (material.hpp:39-65) for the single PBR type
 //   pt_generate.comp:50-84       pass_generate
 //   pt_trace.comp:134-226, :311-386 (meshes, then SDF drawables)  pass_trace
-//   pt_color.comp:77-202         pass_color (no cubemap: sky gradient)
+//   pt_color.comp:77-202         pass_color (sky gradient, or the cube map)
 //   pt_ray_filter.comp:49-64     pass_filter, as a STABLE compaction (slot order
 //                                = serial order; the reference's atomicAdd order
 //                                is not reproducible)
@@ -1998,6 +1998,56 @@ void orc_forward_render(int n, float const* pos, float const* nrm, float const* 
       out[0] = oracle_half_rn(c.x), out[1] = oracle_half_rn(c.y), out[2] = oracle_half_rn(c.z);
       out[3] = oracle_half_rn(1.f * 0.f);
     }
+}
+
+}  // extern "C"
+
+// ---- single passes on caller buffers (for pinning against the reference's own
+// pt_generate.comp / pt_color.comp compiled as C++) ----------------------------------------
+extern "C" {
+
+// pass_color over n rays: gen (80-byte records) and trace (64-byte records)
+// are updated in place; accum / display are W x H RGBA float images.
+void orc_pass_color(int n, void* gen, void* trace, float* accum, float* display, int width, int height,
+    std::uint32_t sample_index, int force, int seed, float const* random_tex, int tex_size, std::int32_t const* refs,
+    int n_refs, float const* mdata) {
+  scene_t sc{};
+  sc.mat_refs = refs;
+  sc.n_mats = std::size_t(std::max(n_refs, 0));
+  sc.mat_data = mdata;
+  std::size_t const px = std::size_t(width) * std::size_t(height);
+  std::vector<v4> acc(px), disp(px);
+  std::memcpy(acc.data(), accum, px * sizeof(v4));
+  std::memcpy(disp.data(), display, px * sizeof(v4));
+  sdf_scene const no_sdf{};
+  frame_ctx f{&sc, width, height, nullptr, nullptr, &acc, &disp, sample_index, 1, &no_sdf};
+  pass_rng const pr{seed, std::vector<float>(random_tex, random_tex + tex_size)};
+  std::vector<gen_t> g(static_cast<gen_t*>(gen), static_cast<gen_t*>(gen) + n);
+  std::vector<trace_t> t(static_cast<trace_t*>(trace), static_cast<trace_t*>(trace) + n);
+  pass_color(f, pr, g, t, force != 0);
+  std::memcpy(gen, g.data(), std::size_t(n) * sizeof(gen_t));
+  std::memcpy(trace, t.data(), std::size_t(n) * sizeof(trace_t));
+  std::memcpy(accum, acc.data(), px * sizeof(v4));
+  std::memcpy(display, disp.data(), px * sizeof(v4));
+}
+
+// pass_generate over a width x height image into gen (width * height records).
+void orc_pass_generate(int width, int height, float const* inv_view, float const* inv_proj, int seed,
+    float const* random_tex, int tex_size, int dof, float lens_x, float lens_y, float focus, float const* bokeh,
+    int bokeh_w, int bokeh_h, int bokeh_wrap, void* gen) {
+  scene_t sc{};
+  std::vector<v4> acc, disp;
+  sdf_scene const no_sdf{};
+  frame_ctx f{&sc, width, height, inv_view, inv_proj, &acc, &disp, 0u, 1, &no_sdf};
+  f.dof = dof;
+  f.lens[0] = lens_x;
+  f.lens[1] = lens_y;
+  f.focus = focus;
+  if (bokeh) f.bokeh = tex_view{bokeh, bokeh_w, bokeh_h, bokeh_wrap};
+  pass_rng const pr{seed, std::vector<float>(random_tex, random_tex + tex_size)};
+  std::vector<gen_t> g;
+  pass_generate(f, pr, g);
+  std::memcpy(gen, g.data(), g.size() * sizeof(gen_t));
 }
 
 }  // extern "C"

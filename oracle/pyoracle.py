@@ -58,6 +58,8 @@ def oracle() -> C.CDLL:
             "orc_render_physical": (None, [SZ, P, P, P, P, SZ, P, P, P, P, I, P, I, I, I, C.c_uint32, I, I,
                                            C.c_uint32, P, P, P, P, P, P, I, I, C.c_float, I, P, I]),
             "orc_refbvh_query": (None, [P, P, P, P, P, SZ, I, I, I, P, P, P, P, I]),
+            "orc_pass_color": (None, [I, P, P, P, P, I, I, C.c_uint32, I, I, P, I, P, I, P]),
+            "orc_pass_generate": (None, [I, I, P, P, I, P, I, I, C.c_float, C.c_float, C.c_float, P, I, I, I, P]),
             "orc_forward_render": (None, [I, P, P, P, P, P, I, P, I, I, P, P, C.c_uint32, I, P, P, I, P, P, P, P, P,
                                           P, P]),
         }
@@ -98,6 +100,8 @@ def ref() -> C.CDLL:
             "ref_sdf_trace": (None, [P, P, P, P, I, P, SZ, I, C.c_float, I, P, P, P, P, P, P]),
             "ref_post_pass": (I, [I, P, P, P, I, I, P, I, I, P]),
             "ref_forward_resolve": (None, [I, I, P, P, I, P, P, P, P, C.c_uint32, P, P, P]),
+            "ref_pass_color": (None, [I, P, P, P, P, I, I, C.c_uint32, I, I, P, I, P, P]),
+            "ref_pass_generate": (None, [I, I, P, P, I, P, I, I, C.c_float, C.c_float, C.c_float, P, I, I, I, P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(h, k)
@@ -393,6 +397,48 @@ def ref_forward_resolve(gbuffer, shadow_map, view, proj, shadow_view, shadow_pro
                           sv.ctypes.data, sp.ctypes.data, int(random_seed) & 0xFFFFFFFF, refs.ctypes.data,
                           md.ctypes.data, out.ctypes.data)
     return out
+
+
+# ---- single passes of the reference shading mode (pinning) ----------------------
+def pass_generate(width, height, inv_view, inv_proj, seed, random_tex, dof=False, lens=(0.0, 0.0), focus=1.0,
+                  bokeh=None, bokeh_wrap=0, use_ref=False) -> np.ndarray:
+    """pt_generate.comp over the image: the oracle's restatement, or (use_ref)
+    the reference's shader compiled by oracle/build_ref.py. Returns the
+    generate_output_t records as float32 [H * W, 20] (int fields as bits)."""
+    L = ref() if use_ref else oracle()
+    fn = L.ref_pass_generate if use_ref else L.orc_pass_generate
+    iv = np.ascontiguousarray(inv_view, np.float32).ravel()
+    ip = np.ascontiguousarray(inv_proj, np.float32).ravel()
+    tex = np.ascontiguousarray(random_tex, np.float32)
+    bk = np.ascontiguousarray(bokeh, np.float32) if bokeh is not None else None
+    out = np.zeros((width * height, 20), np.float32)
+    fn(width, height, iv.ctypes.data, ip.ctypes.data, int(seed), tex.ctypes.data, tex.size, int(dof),
+       float(lens[0]), float(lens[1]), float(focus), bk.ctypes.data if bk is not None else None,
+       bk.shape[1] if bk is not None else 0, bk.shape[0] if bk is not None else 0, int(bokeh_wrap),
+       out.ctypes.data)
+    return out
+
+
+def pass_color(gen, trace, accum, display, sample_index, force, seed, random_tex, materials, material_data,
+               use_ref=False):
+    """pt_color.comp over the rays of gen / trace (float32 [n, 20] / [n, 16],
+    updated copies are returned with the images)."""
+    L = ref() if use_ref else oracle()
+    g = np.array(gen, np.float32, copy=True, order="C")
+    t = np.array(trace, np.float32, copy=True, order="C")
+    a = np.array(accum, np.float32, copy=True, order="C")
+    d = np.array(display, np.float32, copy=True, order="C")
+    tex = np.ascontiguousarray(random_tex, np.float32)
+    refs = np.ascontiguousarray(materials, np.int32).reshape(-1, 2)
+    md = np.ascontiguousarray(material_data, np.float32).ravel()
+    H, W = a.shape[0], a.shape[1]
+    args = [g.shape[0], g.ctypes.data, t.ctypes.data, a.ctypes.data, d.ctypes.data, W, H, int(sample_index),
+            int(force), int(seed), tex.ctypes.data, tex.size, refs.ctypes.data]
+    if use_ref:
+        L.ref_pass_color(*args, md.ctypes.data)
+    else:
+        L.orc_pass_color(*args, refs.shape[0], md.ctypes.data)
+    return g, t, a, d
 
 
 # ---- SDF ----------------------------------------------------------------------

@@ -415,9 +415,10 @@ void ref_sdf_trace(int const* instrs, int const* programs, float const* params, 
 //   * every per-invocation global (pbr_state, after_sample, resample_factor,
 //     the material type) starts at its initial value for each fragment.
 namespace glsl {
-namespace fwd {
 
-uint cmattype = ~0u;
+// The dispatch material_registry::generate_code emits for the one PBR type
+// (src/material.hpp:39-65): open / evaluate / bounce over the current type.
+thread_local uint cmattype = ~0u;
 void open(uint type, uint buf) {
   cmattype = type;
   switch (type) {
@@ -432,6 +433,21 @@ void evaluate(vec3 p, vec2 uv, vec3 n, vec3 tl, vec3 tv, vec3& ref, float& pdf) 
     case 0: material_evaluate_(p, uv, n, tl, tv, ref, pdf); break;
   }
 }
+vec3 bounce(vec2 rnd, vec3 tv, vec3 n) {
+  switch (cmattype) {
+    case 0: return material_bounce_(rnd, tv, n); break;
+  }
+  return vec3(0);
+}
+// every per-invocation global at its initial value
+void reset_invocation() {
+  pbr_state = -1;
+  after_sample = false;
+  resample_factor = 1.f;
+  cmattype = ~0u;
+}
+
+namespace fwd {
 
 struct ivec3 {
   int x, y, z;
@@ -503,13 +519,153 @@ extern "C" void ref_forward_resolve(int width, int height, float const* gbuf, fl
   for (int y = 0; y < height; ++y)
     for (int x = 0; x < width; ++x) {
       f::gl_FragCoord = glsl::vec4(float(x) + 0.5f, float(y) + 0.5f, 0.f, 1.f);
-      glsl::pbr_state = -1;
-      glsl::after_sample = false;
-      glsl::resample_factor = 1.f;
-      f::cmattype = ~0u;
+      glsl::reset_invocation();
       f::color = glsl::vec4(0.f);
       f::resolve_main();
       float* o = out + 4 * (size_t(y) * width + x);
       o[0] = f::color.x, o[1] = f::color.y, o[2] = f::color.z, o[3] = f::color.w;
     }
 }
+
+// ---- the path tracer's generate and color passes: src/pt/pt_generate.comp, pt_color.comp -----
+// build_ref.py rewrites them (pass_to_cpp) into pt_generate.inc / pt_color.inc;
+// they run here once per invocation over host buffers and images with what a
+// GL compute dispatch provides: gl_GlobalInvocationID; imageLoad / imageStore on
+// RGBA32F images (outside the image: load 0, store dropped); the random texture
+// as a sampler1D; the bokeh mask sampled at level 0 with GL_LINEAR and its wrap
+// mode (weights summed ((w00 t00 + w10 t10) + w01 t01) + w11 t11); no cube map
+// bound (textureSize 0: the sky gradient). pt_generate is dispatched over the
+// image's pixels only: its `pt.x > image_size.x` test would let a column
+// x = width through whose store lands on the next row's first slot (a race
+// between invocations in GL); the images the tests use are multiples of the 8x8
+// work group, where no such invocation exists.
+namespace glsl {
+struct image2D {
+  float* data = nullptr;  // RGBA32F, row-major
+  int w = 0, h = 0;
+};
+inline vec4 imageLoad(image2D const& im, ivec2 p) {
+  if (p.x < 0 || p.y < 0 || p.x >= im.w || p.y >= im.h) return vec4(0.f);
+  float const* q = im.data + 4 * (size_t(p.y) * im.w + p.x);
+  return vec4(q[0], q[1], q[2], q[3]);
+}
+inline void imageStore(image2D& im, ivec2 p, vec4 v) {
+  if (p.x < 0 || p.y < 0 || p.x >= im.w || p.y >= im.h) return;
+  float* q = im.data + 4 * (size_t(p.y) * im.w + p.x);
+  q[0] = v.x, q[1] = v.y, q[2] = v.z, q[3] = v.w;
+}
+struct samplerCube {
+  int size = 0;
+};
+inline ivec2 textureSize(samplerCube const& c, int) { return ivec2(c.size, c.size); }
+inline vec4 textureLod(samplerCube const&, vec3 const&, int) { return vec4(0.f); }
+
+namespace cpass {
+struct gid_t {
+  uint x = 0, y = 0, z = 0;
+};
+gid_t gl_GlobalInvocationID;
+#include "pt_color.inc"
+}  // namespace cpass
+
+namespace gpass {
+struct gid_t {
+  uint x = 0, y = 0, z = 0;
+  uvec2 xy;
+};
+gid_t gl_GlobalInvocationID;
+struct sampler2D {
+  float const* data = nullptr;  // RGBA floats
+  int w = 0, h = 0, wrap = 0;   // wrap 0 repeat, 1 clamp to edge, 2 mirrored repeat
+};
+inline ivec2 textureSize(sampler2D const& s, int) { return ivec2(s.w, s.h); }
+inline int wrap_texel(int i, int size, int mode) {
+  if (mode == 1) return i < 0 ? 0 : (i >= size ? size - 1 : i);
+  if (mode == 2) {
+    int m = i % (2 * size);
+    if (m < 0) m += 2 * size;
+    int const a = m - size;
+    return (size - 1) - (a >= 0 ? a : -(1 + a));
+  }
+  int m = i % size;
+  return m < 0 ? m + size : m;
+}
+inline vec4 textureLod(sampler2D const& s, vec2 uv, int) {
+  float const u = uv.x * float(s.w) - 0.5f, v = uv.y * float(s.h) - 0.5f;
+  float const fu = std::floor(u), fv = std::floor(v);
+  float const a = u - fu, b = v - fv;
+  int const i0 = int(fu), j0 = int(fv);
+  int const x0 = wrap_texel(i0, s.w, s.wrap), x1 = wrap_texel(i0 + 1, s.w, s.wrap);
+  int const y0 = wrap_texel(j0, s.h, s.wrap), y1 = wrap_texel(j0 + 1, s.h, s.wrap);
+  float const w00 = (1.f - a) * (1.f - b), w10 = a * (1.f - b), w01 = (1.f - a) * b, w11 = a * b;
+  float const* t00 = s.data + 4 * (size_t(y0) * s.w + x0);
+  float const* t10 = s.data + 4 * (size_t(y0) * s.w + x1);
+  float const* t01 = s.data + 4 * (size_t(y1) * s.w + x0);
+  float const* t11 = s.data + 4 * (size_t(y1) * s.w + x1);
+  float r[4];
+  for (int c = 0; c < 4; ++c) r[c] = ((w00 * t00[c] + w10 * t10[c]) + w01 * t01[c]) + w11 * t11[c];
+  return vec4(r[0], r[1], r[2], r[3]);
+}
+#include "bokeh.inc"
+#include "pt_generate.inc"
+}  // namespace gpass
+}  // namespace glsl
+
+extern "C" {
+
+// pt_color.comp over n rays: gen (80-byte generate_output_t) and trace (64-byte
+// trace_output_t) are updated in place, accum / display are the debug and
+// output images (W x H RGBA32F).
+void ref_pass_color(int n, void* gen, void* trace, float* accum, float* display, int width, int height,
+    std::uint32_t sample_index, int force_write_color, int random_sample, float const* random_tex, int tex_size,
+    std::int32_t const* refs, float const* mdata) {
+  namespace c = glsl::cpass;
+  c::generate_output = static_cast<c::generate_output_t*>(gen);
+  c::trace_output = static_cast<c::trace_output_t*>(trace);
+  c::num_elements = uint(n);
+  c::materials = reinterpret_cast<c::material_reference_t*>(const_cast<std::int32_t*>(refs));
+  c::materials_data = const_cast<float*>(mdata);
+  glsl::g_material_data = mdata;
+  c::debug_image = glsl::image2D{accum, width, height};
+  c::output_image = glsl::image2D{display, width, height};
+  c::random_texture = glsl::sampler1D{random_tex, tex_size};
+  c::cubemap = glsl::samplerCube{0};
+  c::sample_index = sample_index;
+  c::force_write_color = force_write_color != 0;
+  c::random_sample = random_sample;
+  for (int id = 0; id < n; ++id) {
+    c::gl_GlobalInvocationID = c::gid_t{uint(id), 0u, 0u};
+    glsl::reset_invocation();
+    c::pass_main();
+  }
+}
+
+// pt_generate.comp over a width x height image into gen (width * height records).
+void ref_pass_generate(int width, int height, float const* inv_view, float const* inv_proj, int random_seed,
+    float const* random_tex, int tex_size, int dof, float lens_x, float lens_y, float focus, float const* bokeh,
+    int bokeh_w, int bokeh_h, int bokeh_wrap, void* gen) {
+  namespace g = glsl::gpass;
+  auto m4 = [](float const* p) {
+    glsl::mat4 m;
+    for (int i = 0; i < 16; ++i) m.c[i / 4][i % 4] = p[i];
+    return m;
+  };
+  g::inverse_camera_view = m4(inv_view);
+  g::inverse_camera_projection = m4(inv_proj);
+  g::dof_active = dof != 0;
+  g::image_size = glsl::uvec2(uint(width), uint(height));
+  g::lens_size = glsl::vec2(lens_x, lens_y);
+  g::focus = focus;
+  g::random_seed = random_seed;
+  g::random_texture = glsl::sampler1D{random_tex, tex_size};
+  g::bokeh_shape = g::sampler2D{bokeh, bokeh ? bokeh_w : 0, bokeh ? bokeh_h : 0, bokeh_wrap};
+  g::generate_output = static_cast<g::generate_output_t*>(gen);
+  for (int y = 0; y < height; ++y)
+    for (int x = 0; x < width; ++x) {
+      g::gl_GlobalInvocationID = g::gid_t{uint(x), uint(y), 0u, glsl::uvec2(uint(x), uint(y))};
+      glsl::reset_invocation();
+      g::pass_main();
+    }
+}
+
+}  // extern "C"
