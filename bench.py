@@ -63,6 +63,9 @@ def parse_args():
                         "per-frame post-processing chain (bloom, tonemap, FXAA) and denoise on 2048x2048; "
                         "forward: the raster preview renderer (1920x1080, 2048^2 shadow map)")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain leg of the closest workload")
+    p.add_argument("--sdf-cells", type=int, default=0,
+                   help="sdf: cells along the longest axis of the SDF chain's group-list grid (0 = the library's "
+                        "default, 1 = no grid: every primitive runs at every march step)")
     a = p.parse_args()
     if a.workload == "closest":
         a.res = a.res or 512
@@ -814,6 +817,7 @@ def run_sdf_workload(args):
     lib = S.SdfLibrary()
     lib.add(S.random_sdf_field(256, k=0.1, seed=9, extent=0.8, chain=True))
     dr = S.sdf_drawables([np.array([[1, 0, 0, 0.0], [0, 1, 0, -0.2], [0, 0, 1, 0.3], [0, 0, 0, 1]])], [0])
+    ctx.set_tuning(sdf_cells=args.sdf_cells)
     ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)
     ctx.set_area_lights(lights)
     W = H = args.res or 768
@@ -858,7 +862,7 @@ def run_sdf_workload(args):
         {"workload": "icosphere scene (655,872 tris) + 256-primitive SDF smooth union (k 0.1, folded left to "
                      "right), 256 steps, eps 1e-4, guided, 768x768, 128 spp per step, depth 8",
          "triangles": int(info["triangles"]),
-         "sdf_primitives": 256, "res": W, "spp_per_step": spp},
+         "sdf_primitives": 256, "res": W, "spp_per_step": spp, "sdf_cells": args.sdf_cells},
         {"mrays_per_s": rays / (ms / 1e3) / 1e6, "rays_per_sample": rays / samples,
          f"rel_rmse_vs_fp64_{oracle_spp}spp": err, "rel_rmse_spp": spp * args.steps,
          "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128,

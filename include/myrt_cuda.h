@@ -158,6 +158,10 @@ typedef struct myrt_tuning {
                                 of at least 1 Mi rays sorted by origin and direction cell, host-memory
                                 queries in input order; 1 = input order; 2 = always sorted.
                                 Results never depend on it. */
+  uint32_t sdf_cells;        /* myrt_sdf_upload: cells along the longest axis of the grid of group lists
+                                built for each left-to-right union / smooth-union chain program
+                                (0 = 32, 1 = no grid: every group runs, 2..128). Results never
+                                depend on it. */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */

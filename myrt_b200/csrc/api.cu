@@ -416,6 +416,11 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   cudaFree(ctx->sdf.programs);
   cudaFree(ctx->sdf.params);
   cudaFree(ctx->sdf.drawables);
+  cudaFree(ctx->sdf.skip_sphere);
+  cudaFree(ctx->sdf.skip_next);
+  cudaFree(ctx->sdf.cell_hdr);
+  cudaFree(ctx->sdf.cell_start);
+  cudaFree(ctx->sdf.cell_list);
   free_render(ctx->render);
   free_textures(ctx);
   free_forward(ctx);
@@ -448,7 +453,7 @@ int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
   if (!ctx || !t) return MYRT_ERR_INVALID_ARGUMENT;
   if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
       t->trace_unit_steps > 1 || (t->wave_paths != 0 && (t->wave_paths < 1024 || t->wave_paths > (1u << 28))) ||
-      t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2 || t->bvh_builder > 1)
+      t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2 || t->bvh_builder > 1 || t->sdf_cells > 128)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;
@@ -665,6 +670,9 @@ int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
   cudaFree(D.drawables);
   cudaFree(D.skip_sphere);
   cudaFree(D.skip_next);
+  cudaFree(D.cell_hdr);
+  cudaFree(D.cell_start);
+  cudaFree(D.cell_list);
   D = device_sdf{};
   ctx->render.sample_counter = 0;
   if (v->drawable_count == 0) return MYRT_OK;
@@ -713,6 +721,8 @@ int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
   std::vector<float4> skip_sphere;
   std::vector<int2> skip_next;
   sdf_skip_tables(v, skip_sphere, skip_next);
+  sdf_cells cells;
+  if (ctx->tuning.sdf_cells != 1) sdf_cell_tables(v, ctx->tuning.sdf_cells ? int(ctx->tuning.sdf_cells) : 32, cells);
   std::vector<float> dr(v->drawable_count * 36);
   for (size_t d = 0; d < v->drawable_count; ++d) {
     myrt_sdf_drawable const& s = v->drawables[d];
@@ -728,6 +738,11 @@ int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
   if (!rc && !skip_next.empty()) {
     rc = upload(ctx, &D.skip_sphere, skip_sphere.data(), skip_sphere.size(), "SDF skip spheres");
     if (!rc) rc = upload(ctx, &D.skip_next, skip_next.data(), skip_next.size(), "SDF skip groups");
+  }
+  if (!rc && !cells.list.empty()) {
+    rc = upload(ctx, &D.cell_hdr, cells.hdr.data(), cells.hdr.size(), "SDF cell headers");
+    if (!rc) rc = upload(ctx, &D.cell_start, cells.start.data(), cells.start.size(), "SDF cell starts");
+    if (!rc) rc = upload(ctx, &D.cell_list, cells.list.data(), cells.list.size(), "SDF cell lists");
   }
   if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "SDF upload");
   if (rc) return rc;

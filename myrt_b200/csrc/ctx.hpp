@@ -56,6 +56,11 @@ struct device_sdf {
   // group's operator, k bits); next 0 = not a skippable group start
   float4* skip_sphere = nullptr;
   int2* skip_next = nullptr;
+  // cell lists of left-to-right chain programs (sdf_skip.hpp sdf_cells),
+  // null when no program has them
+  int4* cell_hdr = nullptr;
+  int* cell_start = nullptr;
+  uint32_t* cell_list = nullptr;
   int n_drawables = 0;
   int n_programs = 0;
 };
@@ -111,7 +116,7 @@ struct myrt_ctx {
   myrt_b200::guide_state* guide = nullptr;  // learned proposal (guide.cu), created on first use
   uint64_t guide_generation = 0;            // bumped by scene uploads
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
-  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
   int sm_count = 0;
   uint32_t* d_next = nullptr;    // ring of ray counters for the persistent traversal
   uint32_t next_slot = 0;

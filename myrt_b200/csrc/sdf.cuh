@@ -51,6 +51,14 @@ struct sdf_dev {
   float eps;
   float4 const* skip_sphere;  // per instruction, or null (see map)
   int2 const* skip_next;
+  // cell lists of left-to-right chain programs, or null (see map): 4 int4 per
+  // program ((lo.xyz, 1 / cell) bits; (nx, ny, nz, first cell), nx = 0: none;
+  // (end of the first group, 0, 0, 0); escape sphere (C.xyz, radius) bits, see
+  // march), per cell the first list entry, and the entries (group start |
+  // group end << 16, relative to the program)
+  int4 const* cell_hdr;
+  int const* cell_start;
+  uint32_t const* cell_list;
 };
 
 __device__ __forceinline__ v3 abs3(v3 a) { return {fabsf(a.x), fabsf(a.y), fabsf(a.z)}; }
@@ -103,6 +111,12 @@ __device__ __forceinline__ float sd_menger(v3 p) {
 // (c, R), so the group is skipped when |p - c| >= d0 + k + R + margin, the
 // margin covering the rounding of both sides. Material loads (load == true)
 // evaluate every group: their operators draw from the random stream.
+//
+// Cell lists (load == false, chain programs): when p lies in the program's
+// grid, only the first group and the groups listed for p's cell run, in
+// program order; every group left out returns the running value bit for bit
+// at every point of the cell (sdf_skip.hpp sdf_cell_tables), so the result is
+// the full evaluation's.
 __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load, rs::rng_t* rng, int& mat) {
   int2 const pr = __ldg(s.programs + prog);
   float dist[kStack];
@@ -110,10 +124,33 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
   int sp = 0;
   v3 pos = p;
   float const* G = s.params;
-  bool const skipping = !load && s.skip_next != nullptr;
+  bool skipping = !load && s.skip_next != nullptr;
   float const margin = 1e-4f + 1e-6f * ((fabsf(p.x) + fabsf(p.y)) + fabsf(p.z));
+  int kend = pr.y, li = 0, le = 0;
+  if (!load && s.cell_hdr != nullptr) {
+    int4 const h1 = __ldg(s.cell_hdr + 4 * prog + 1);
+    if (h1.x > 0) {
+      int4 const h0 = __ldg(s.cell_hdr + 4 * prog);
+      float const inv = __int_as_float(h0.w);
+      float const fx = (p.x - __int_as_float(h0.x)) * inv, fy = (p.y - __int_as_float(h0.y)) * inv,
+                  fz = (p.z - __int_as_float(h0.z)) * inv;
+      if (fx >= 0.f && fy >= 0.f && fz >= 0.f && fx < float(h1.x) && fy < float(h1.y) && fz < float(h1.z)) {
+        int const c = h1.w + (int(fz) * h1.y + int(fy)) * h1.x + int(fx);
+        li = __ldg(s.cell_start + c);
+        le = __ldg(s.cell_start + c + 1);
+        kend = __ldg(s.cell_hdr + 4 * prog + 2).x;
+        skipping = false;
+      }
+    }
+  }
 #pragma unroll 1
-  for (int k = 0; k < pr.y; ++k) {
+  for (int k = 0;; ++k) {
+    if (k >= kend) {
+      if (li >= le) break;
+      uint32_t const e = __ldg(s.cell_list + li++);
+      k = int(e & 0xffffu);
+      kend = int(e >> 16);
+    }
     if (skipping) {
       int2 const nx = __ldg(s.skip_next + pr.x + k);
       if (nx.x > 0) {
@@ -211,6 +248,13 @@ __device__ __forceinline__ v3 xform4(float const* m, v3 v, float w) {
 
 // raymarch.glsl:116-171 for drawable `cur`. Returns hits; fills the rest
 // unless hits_only.
+//
+// Early exit (chain programs with an escape sphere): once the march moves
+// forward (si > 0), is outside the sphere (C, r) widened by eps and heads away
+// from C, every later point keeps a value of at least eps (sdf_skip.hpp
+// sdf_cells), so no hit can follow and the march ends as the reference's
+// does without a hit, only sooner (a ray that misses everything otherwise
+// steps until t overflows).
 __device__ __forceinline__ sdf_hit march(
     sdf_dev const& s, int cur, v3 oro, v3 ord, float tmax, bool hits_only, rs::rng_t* rng) {
   sdf_hit hit;
@@ -223,14 +267,24 @@ __device__ __forceinline__ sdf_hit march(
   float res = -1.f;
   float t = 10.f * s.eps;
   int si = 0;
+  float4 esc = make_float4(0.f, 0.f, 0.f, -1.f);
+  if (s.cell_hdr != nullptr && __ldg(s.cell_hdr + 4 * prog + 1).x > 0) {
+    int4 const e = __ldg(s.cell_hdr + 4 * prog + 3);
+    esc = make_float4(__int_as_float(e.x), __int_as_float(e.y), __int_as_float(e.z), __int_as_float(e.w) + s.eps);
+  }
 #pragma unroll 1
   for (int i = 0; i < s.steps && t / len < tmax; i++) {
     int mdum = -1;
-    float const m = map(s, prog, ro + rd * t / len, false, rng, mdum);
+    v3 const q = ro + rd * t / len;
+    float const m = map(s, prog, q, false, rng, mdum);
     if (si == 0) si = int(rs::signf(m));
     if (fabsf(m) < s.eps) {
       res = t;
       break;
+    }
+    if (si > 0 && esc.w > 0.f) {
+      v3 const w{q.x - esc.x, q.y - esc.y, q.z - esc.z};
+      if (rs::dot(w, rd) >= 0.f && rs::dot(w, w) >= esc.w * esc.w) break;
     }
     t += float(si) * m;
   }

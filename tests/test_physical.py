@@ -96,12 +96,15 @@ def test_physical_fp64_and_heightfield(ctx):
 
 
 @pytest.mark.gpu
-def test_physical_mesh_and_sdf(ctx):
+@pytest.mark.parametrize("chain", [False, True])
+def test_physical_mesh_and_sdf(ctx, chain):
+    """Mesh + SDF render bit-identical to the oracle; the chained field runs
+    through the evaluator's cell lists and the march's early exit."""
     from myrt_b200 import sdf as S
 
     s, lights = icosphere_field_lit(n_spheres=12, subdiv=2, floor_cells=4, seed=6)
     lib = S.SdfLibrary()
-    lib.add(S.random_sdf_field(64, k=0.1, seed=2, extent=0.6))
+    lib.add(S.random_sdf_field(64, k=0.1, seed=2, extent=0.6, chain=chain))
     dr = S.sdf_drawables([np.array([[1, 0, 0, 0.0], [0, 1, 0, 0.2], [0, 0, 1, 0.5], [0, 0, 0, 1]])], [0])
     ctx.upload_scene(**s)
     ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)

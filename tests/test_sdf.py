@@ -156,3 +156,49 @@ def test_sdf_exact_skipping_matches_oracle(ctx):
                 assert np.array_equal(got["material"], ora["material"])
     finally:
         ctx.upload_sdf(np.zeros((0, 2)), np.zeros((0, 2)), np.zeros(0), np.zeros((0, 36)))
+
+
+@pytest.mark.gpu
+def test_sdf_cell_lists_and_early_exit_exact(ctx):
+    """Left-to-right chains get per-cell group lists and an escape sphere at
+    upload (tuning sdf_cells). Hits, t, normals and materials are identical
+    with the grid off (1), at the default (0 = 32 cells) and at 8 and 96 cells,
+    for rays that start outside the field, inside its grid, pass it by or
+    leave it, with finite and infinite tmax; the default also equals the
+    oracle on a subset."""
+    rng = np.random.default_rng(21)
+    lib = S.SdfLibrary()
+    lib.add(S.random_sdf_field(256, k=0.1, seed=9, extent=0.8, chain=True))
+    lib.add(S.random_sdf_field(48, k=0.05, seed=3, extent=0.5, chain=True))
+    dr = S.sdf_drawables([np.array([[1, 0, 0, 0.0], [0, 1, 0, -0.2], [0, 0, 1, 0.3], [0, 0, 0, 1]]),
+                          np.array([[0.8, 0, 0, 1.2], [0, 0.8, 0, 0.1], [0, 0, 0.8, -0.4], [0, 0, 0, 1]])], [0, 1])
+    n = 1 << 16
+    rays = np.zeros((n, 8), np.float32)
+    o = rng.uniform(-2.5, 2.5, (n, 3))
+    o[: n // 4] = rng.uniform(-0.8, 0.8, (n // 4, 3))          # inside the grid
+    d = rng.normal(size=(n, 3))
+    aim = -o + rng.uniform(-0.4, 0.4, (n, 3))
+    d[n // 2:] = aim[n // 2:]                                  # aimed at the field
+    rays[:, 0:3] = o
+    rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 7] = np.where(np.arange(n) % 3 == 0, 2.0, np.inf)
+    states = rng.integers(1, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    res = {}
+    try:
+        for cells in (1, 0, 8, 96):
+            ctx.set_tuning(sdf_cells=cells)
+            ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)
+            res[cells] = [ctx.trace_sdf(rays, 256, 1e-4, any_hit=a, rng_states=states) for a in (False, True)]
+    finally:
+        ctx.set_tuning()
+        ctx.upload_sdf(np.zeros((0, 2)), np.zeros((0, 2)), np.zeros(0), np.zeros((0, 36)))
+    full = res[1]
+    assert full[0]["hit"].sum() > 5000 and full[1]["hit"].sum() > 5000
+    for cells in (0, 8, 96):
+        for a in (0, 1):
+            for key, v in full[a].items():
+                assert np.array_equal(res[cells][a][key], v), (cells, a, key)
+    sub = slice(0, n, 16)
+    ora = po.sdf_trace(lib, dr, rays[sub], 256, 1e-4, False, states[sub])
+    for key in ("hit", "t", "normal", "material"):
+        assert np.array_equal(res[0][0][key][sub], ora[key]), key
