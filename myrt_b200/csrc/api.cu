@@ -47,6 +47,10 @@ void free_scene(device_scene& s) {
   cudaFree(s.tri_material);
   cudaFree(s.materials);
   cudaFree(s.material_data);
+  cudaFree(s.spare_nodes);
+  cudaFree(s.spare_tris);
+  cudaFree(s.spare_pos);
+  cudaFree(s.move_stage);
   s = device_scene{};
 }
 
@@ -412,6 +416,7 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->aux_stream) cudaStreamSynchronize(ctx->aux_stream);
   free_scene(ctx->scene);
+  ctx->build_scratch.release();
   cudaFree(ctx->sdf.instrs);
   cudaFree(ctx->sdf.programs);
   cudaFree(ctx->sdf.params);
@@ -569,7 +574,7 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
     rc = upload(ctx, &d_pos, pos.data(), pos.size(), "triangle upload");
     if (rc) return rc;
     char const* what = nullptr;
-    int const e = build_bvh8_device(d_pos, n_prims, ctx->stream, dtree, &what);
+    int const e = build_bvh8_device(d_pos, n_prims, ctx->stream, ctx->build_scratch, nullptr, dtree, &what);
     ctx->scene.world_pos = d_pos;
     if (e) return check_cuda(ctx, cudaError_t(e > 0 ? e : cudaErrorInvalidValue), what ? what : "device BVH build");
     if (dtree.wide_depth > MYRT_STACK_MAX) {
@@ -617,6 +622,8 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
     s.n_tris = dtree.n_tris;
     s.nodes = reinterpret_cast<uint4*>(dtree.nodes);
     s.tris = dtree.tris;
+    s.node_capacity = dtree.node_capacity;
+    s.tri_capacity = dtree.tri_capacity;
   } else {
     s.n_nodes = tree.nodes.size();
     s.n_tris = tree.triangles.size();

@@ -193,10 +193,11 @@ struct collapse_args {
   float const* pos;        // world triangles, 9 floats per prim
   bvh8_node* nodes;
   float4* tris;            // 3 per triangle
-  uint32_t* counters;      // [0] wide nodes, [1] triangles, [2] next queue length, [3] max depth, [4] leaf slots
+  uint32_t* counters;      // [0] wide nodes, [1] triangles, [2] / [5] queue lengths, [3] max depth, [4] leaf slots
   collapse_item const* in;
-  uint32_t n_in;
+  uint32_t const* n_in;    // this level's queue length (device)
   collapse_item* out;
+  uint32_t* n_out;         // the next level's (zeroed before the launch)
   int n;
 };
 
@@ -227,7 +228,7 @@ __device__ __forceinline__ uint8_t biased_exponent(float extent) {
 
 __global__ void k_collapse(collapse_args a) {
   uint32_t const it = blockIdx.x * blockDim.x + threadIdx.x;
-  if (it >= a.n_in) return;
+  if (it >= *a.n_in) return;
   collapse_item const item = a.in[it];
   uint32_t kids[8];
   ibox kb[8];
@@ -312,7 +313,7 @@ __global__ void k_collapse(collapse_args a) {
   }
   uint32_t const child_base = n_int ? atomicAdd(&a.counters[0], n_int) : 0u;
   uint32_t const tri_base = n_tri ? atomicAdd(&a.counters[1], n_tri) : 0u;
-  uint32_t const out_base = n_int ? atomicAdd(&a.counters[2], n_int) : 0u;
+  uint32_t const out_base = n_int ? atomicAdd(a.n_out, n_int) : 0u;
   atomicMax(&a.counters[3], item.depth);
 
   bvh8_node node;
@@ -379,9 +380,20 @@ template <typename T> int dalloc(T** p, size_t count, std::vector<void*>& owned)
   return 0;
 }
 
+// Sub-allocation of the scratch block: 256-byte aligned slices.
+struct carve {
+  size_t total = 0;
+  template <typename T> size_t take(size_t count) {
+    size_t const at = total;
+    total += (std::max<size_t>(count, 1) * sizeof(T) + 255) & ~size_t(255);
+    return at;
+  }
+};
+
 }  // namespace
 
-int build_bvh8_device(float const* d_pos, size_t n_tris, cudaStream_t st, device_bvh8& out, char const** what) {
+int build_bvh8_device(float const* d_pos, size_t n_tris, cudaStream_t st, device_build_scratch& scratch,
+    device_bvh8 const* reuse, device_bvh8& out, char const** what) {
   out = device_bvh8{};
   *what = nullptr;
   if (n_tris == 0) return 0;
@@ -391,64 +403,90 @@ int build_bvh8_device(float const* d_pos, size_t n_tris, cudaStream_t st, device
   }
   auto const t0 = std::chrono::steady_clock::now();
   int const n = int(n_tris);
-  std::vector<void*> tmp;
-  auto fail = [&](int e, char const* w) {
-    for (void* p : tmp) cudaFree(p);
-    *what = w;
-    return e;
-  };
-  ibox* boxes;
-  uint32_t* cb;
-  uint64_t *k0, *k1;
-  uint32_t *v0, *v1;
-  uint2 *child, *range;
-  uint32_t *par_i, *par_l, *arrivals, *counters;
-  ibox* inner;
-  collapse_item *q0, *q1;
   int e = 0;
-  if ((e = dalloc(&boxes, n, tmp)) || (e = dalloc(&cb, 6, tmp)) || (e = dalloc(&k0, n, tmp)) ||
-      (e = dalloc(&k1, n, tmp)) || (e = dalloc(&v0, n, tmp)) || (e = dalloc(&v1, n, tmp)) ||
-      (e = dalloc(&child, n, tmp)) || (e = dalloc(&range, n, tmp)) || (e = dalloc(&par_i, n, tmp)) ||
-      (e = dalloc(&par_l, n, tmp)) || (e = dalloc(&arrivals, n, tmp)) || (e = dalloc(&counters, 8, tmp)) ||
-      (e = dalloc(&inner, n, tmp)) || (e = dalloc(&q0, n, tmp)) || (e = dalloc(&q1, n, tmp)))
-    return fail(e, "device BVH scratch");
+  size_t tb = 0;
+  if ((e = int(cub::DeviceRadixSort::SortPairs(nullptr, tb, static_cast<uint64_t const*>(nullptr),
+           static_cast<uint64_t*>(nullptr), static_cast<uint32_t const*>(nullptr), static_cast<uint32_t*>(nullptr), n,
+           0, 63, st)))) {
+    *what = "device BVH sort size";
+    return e;
+  }
+  carve c;
+  size_t const o_boxes = c.take<ibox>(n), o_cb = c.take<uint32_t>(6), o_k0 = c.take<uint64_t>(n),
+               o_k1 = c.take<uint64_t>(n), o_v0 = c.take<uint32_t>(n), o_v1 = c.take<uint32_t>(n),
+               o_child = c.take<uint2>(n), o_range = c.take<uint2>(n), o_par_i = c.take<uint32_t>(n),
+               o_par_l = c.take<uint32_t>(n), o_arrivals = c.take<uint32_t>(n), o_counters = c.take<uint32_t>(8),
+               o_inner = c.take<ibox>(n), o_q0 = c.take<collapse_item>(n), o_q1 = c.take<collapse_item>(n),
+               o_temp = c.take<char>(tb);
+  if (scratch.bytes < c.total) {
+    scratch.release();
+    if ((e = int(cudaMalloc(&scratch.base, c.total)))) {
+      scratch.base = nullptr;
+      *what = "device BVH scratch";
+      return e;
+    }
+    scratch.bytes = c.total;
+  }
+  char* const B = static_cast<char*>(scratch.base);
+  auto* const boxes = reinterpret_cast<ibox*>(B + o_boxes);
+  auto* const cb = reinterpret_cast<uint32_t*>(B + o_cb);
+  auto* const k0 = reinterpret_cast<uint64_t*>(B + o_k0);
+  auto* const k1 = reinterpret_cast<uint64_t*>(B + o_k1);
+  auto* const v0 = reinterpret_cast<uint32_t*>(B + o_v0);
+  auto* const v1 = reinterpret_cast<uint32_t*>(B + o_v1);
+  auto* const child = reinterpret_cast<uint2*>(B + o_child);
+  auto* const range = reinterpret_cast<uint2*>(B + o_range);
+  auto* const par_i = reinterpret_cast<uint32_t*>(B + o_par_i);
+  auto* const par_l = reinterpret_cast<uint32_t*>(B + o_par_l);
+  auto* const arrivals = reinterpret_cast<uint32_t*>(B + o_arrivals);
+  auto* const counters = reinterpret_cast<uint32_t*>(B + o_counters);
+  auto* const inner = reinterpret_cast<ibox*>(B + o_inner);
+  collapse_item* const q[2] = {reinterpret_cast<collapse_item*>(B + o_q0), reinterpret_cast<collapse_item*>(B + o_q1)};
+  void* const temp = B + o_temp;
   // wide nodes: at most one per 2 triangles (every wide node but the root holds > 4) + 1
   size_t const max_nodes = n_tris / 2 + 2;
   bvh8_node* nodes;
   float4* tris;
-  {
+  bool const reused = reuse && reuse->nodes && reuse->tris && reuse->node_capacity >= max_nodes &&
+                      reuse->tri_capacity >= 3 * n_tris;
+  if (reused) {
+    nodes = reuse->nodes;
+    tris = reuse->tris;
+  } else {
     std::vector<void*> keep;
     if ((e = dalloc(&nodes, max_nodes, keep)) || (e = dalloc(&tris, 3 * n_tris, keep))) {
       for (void* p : keep) cudaFree(p);
-      return fail(e, "device BVH output");
+      *what = "device BVH output";
+      return e;
     }
   }
-  uint32_t const init_cb[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  auto fail = [&](int err, char const* w) {
+    if (!reused) {
+      cudaFree(nodes);
+      cudaFree(tris);
+    }
+    *what = w;
+    return err;
+  };
+  // counters: [0] wide nodes (the root), [2] level-0 queue length (the root item)
+  static uint32_t const init_cb[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  static uint32_t const init_counters[8] = {1u, 0u, 1u, 0u, 0u, 0u, 0u, 0u};
+  collapse_item const root{n >= 2 ? 0u : kLeafBit, 0u, 1u};
   cudaMemcpyAsync(cb, init_cb, sizeof init_cb, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(counters, init_counters, sizeof init_counters, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(q[0], &root, sizeof root, cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(par_i, 0xff, size_t(n) * 4, st);
   cudaMemsetAsync(par_l, 0xff, size_t(n) * 4, st);
   cudaMemsetAsync(arrivals, 0, size_t(n) * 4, st);
   uint32_t const blocks = uint32_t((n + 255) / 256);
   k_prim_boxes<<<blocks, 256, 0, st>>>(d_pos, uint32_t(n), 1e-5f, boxes, cb);
   k_morton<<<blocks, 256, 0, st>>>(boxes, uint32_t(n), cb, k0, v0);
-  size_t tb = 0;
-  cub::DeviceRadixSort::SortPairs(nullptr, tb, k0, k1, v0, v1, n, 0, 63, st);
-  void* temp = nullptr;
-  if ((e = int(cudaMalloc(&temp, tb)))) {
-    cudaFree(nodes);
-    cudaFree(tris);
-    return fail(e, "device BVH sort scratch");
-  }
-  tmp.push_back(temp);
-  cub::DeviceRadixSort::SortPairs(temp, tb, k0, k1, v0, v1, n, 0, 63, st);
+  if ((e = int(cub::DeviceRadixSort::SortPairs(temp, tb, k0, k1, v0, v1, n, 0, 63, st))))
+    return fail(e, "device BVH sort");
   if (n >= 2) {
     k_radix_tree<<<uint32_t((n - 1 + 255) / 256), 256, 0, st>>>(k1, n, child, range, par_i, par_l);
     k_boxes_up<<<blocks, 256, 0, st>>>(boxes, v1, n, child, par_i, par_l, arrivals, inner);
   }
-  collapse_item const root{n >= 2 ? 0u : kLeafBit, 0u, 1u};
-  uint32_t const init_counters[8] = {1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
-  cudaMemcpyAsync(q0, &root, sizeof root, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(counters, init_counters, sizeof init_counters, cudaMemcpyHostToDevice, st);
   collapse_args ca{};
   ca.leaf_boxes = boxes;
   ca.order = v1;
@@ -460,33 +498,35 @@ int build_bvh8_device(float const* d_pos, size_t n_tris, cudaStream_t st, device
   ca.tris = tris;
   ca.counters = counters;
   ca.n = n;
-  uint32_t n_in = 1;
-  collapse_item* qin = q0;
-  collapse_item* qout = q1;
+  // Level l reads queue l & 1 (length in counters[2] or [5]) and appends to
+  // the other. Levels are launched in batches without reading their lengths
+  // back: a level holds at most 8^l items (and at most n), which sizes its
+  // grid; threads past the device-side length return at once. One read-back
+  // per batch finds the end.
   uint32_t hc[8];
-  while (n_in > 0) {
-    cudaMemsetAsync(counters + 2, 0, 4, st);
-    ca.in = qin;
-    ca.n_in = n_in;
-    ca.out = qout;
-    k_collapse<<<(n_in + 127) / 128, 128, 0, st>>>(ca);
-    cudaMemcpyAsync(hc, counters, sizeof hc, cudaMemcpyDeviceToHost, st);
-    if ((e = int(cudaStreamSynchronize(st)))) {
-      cudaFree(nodes);
-      cudaFree(tris);
-      return fail(e, "device BVH collapse");
+  uint32_t bound = 1;
+  for (int level = 0;;) {
+    for (int b = 0; b < 8; ++b, ++level) {
+      int const in = level & 1;
+      uint32_t* const len_out = counters + (in ? 2 : 5);
+      cudaMemsetAsync(len_out, 0, 4, st);
+      ca.in = q[in];
+      ca.n_in = counters + (in ? 5 : 2);
+      ca.out = q[in ^ 1];
+      ca.n_out = len_out;
+      k_collapse<<<(bound + 127) / 128, 128, 0, st>>>(ca);
+      bound = uint32_t(std::min<uint64_t>(uint64_t(bound) * 8u, uint64_t(n)));
     }
-    n_in = hc[2];
-    std::swap(qin, qout);
+    cudaMemcpyAsync(hc, counters, sizeof hc, cudaMemcpyDeviceToHost, st);
+    if ((e = int(cudaStreamSynchronize(st)))) return fail(e, "device BVH collapse");
+    if (hc[(level & 1) ? 5 : 2] == 0) break;  // the next level's queue is empty
+    if (level > 4096) return fail(-1, "device BVH collapse did not finish");
   }
-  if ((e = int(cudaGetLastError()))) {
-    cudaFree(nodes);
-    cudaFree(tris);
-    return fail(e, "device BVH launch");
-  }
-  for (void* p : tmp) cudaFree(p);
+  if ((e = int(cudaGetLastError()))) return fail(e, "device BVH launch");
   out.nodes = nodes;
   out.tris = tris;
+  out.node_capacity = reused ? reuse->node_capacity : max_nodes;
+  out.tri_capacity = reused ? reuse->tri_capacity : 3 * n_tris;
   out.n_nodes = hc[0];
   out.n_tris = hc[1];
   out.wide_depth = int(hc[3]);

@@ -11,6 +11,7 @@
 
 #include "../../include/myrt_cuda.h"
 #include "bvh8.hpp"
+#include "bvh8_device.hpp"
 
 namespace myrt_b200 {
 
@@ -43,6 +44,17 @@ struct device_scene {
   // world-space corners per prim (9 floats, prim id = draw order) for the
   // forward renderer's rasteriser
   float* world_pos = nullptr;
+  // capacities of nodes / tris when the device builder made them (0: host
+  // tree, not reusable), and myrt_scene_set_transforms' second set of tree and
+  // corner buffers: each move builds into the spare set and swaps, so repeated
+  // moves allocate nothing
+  size_t node_capacity = 0, tri_capacity = 0;
+  uint4* spare_nodes = nullptr;
+  float4* spare_tris = nullptr;
+  float* spare_pos = nullptr;
+  size_t spare_node_capacity = 0, spare_tri_capacity = 0;
+  void* move_stage = nullptr;  // drawable transforms + bounds of a move
+  size_t move_stage_bytes = 0;
 };
 
 // SDF drawables (uploaded separately; scene::prepare's sdf buffers).
@@ -110,6 +122,7 @@ struct myrt_ctx {
   std::string last_error;
   uint32_t* d_err = nullptr;          // device error word (atomicOr of ERR_* bits)
   myrt_b200::device_scene scene;
+  myrt_b200::device_build_scratch build_scratch;  // device BVH builder temporaries, kept between builds
   myrt_b200::device_sdf sdf;
   myrt_b200::render_state render;
   myrt_b200::physical_state physical;

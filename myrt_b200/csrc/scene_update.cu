@@ -129,17 +129,30 @@ int scene_set_transforms(myrt_ctx* ctx, myrt_drawable const* drawables, size_t c
     x.material = d.material_index;
   }
   cudaStream_t const st = ctx->stream;
-  drawable_xf* d_xf = nullptr;
-  float* d_pos = nullptr;
-  uint32_t* d_b = nullptr;
+  // staging (transforms, then the bounds words) and the corners: kept in the
+  // scene between moves; the corners come from the spare set when there is one
+  size_t const xf_bytes = (count * sizeof(drawable_xf) + 255) & ~size_t(255);
+  int rc = MYRT_OK;
+  if (s.move_stage_bytes < xf_bytes + 256) {
+    cudaFree(s.move_stage);
+    s.move_stage = nullptr;
+    s.move_stage_bytes = 0;
+    rc = check_cuda(ctx, cudaMalloc(&s.move_stage, xf_bytes + 256), "move staging");
+    if (rc) return rc;
+    s.move_stage_bytes = xf_bytes + 256;
+  }
+  auto* const d_xf = static_cast<drawable_xf*>(s.move_stage);
+  auto* const d_b = reinterpret_cast<uint32_t*>(static_cast<char*>(s.move_stage) + xf_bytes);
+  float* d_pos = s.spare_pos;
+  bool const own_pos = d_pos == nullptr;
+  if (own_pos) rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&d_pos), s.n_prims * 36), "world triangles");
   auto cleanup = [&]() {
-    cudaFree(d_xf);
-    cudaFree(d_pos);
-    cudaFree(d_b);
+    if (own_pos) cudaFree(d_pos);
   };
-  int rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&d_xf), count * sizeof(drawable_xf)), "drawables");
-  if (!rc) rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&d_pos), s.n_prims * 36), "world triangles");
-  if (!rc) rc = check_cuda(ctx, cudaMalloc(reinterpret_cast<void**>(&d_b), 6 * 4), "bounds");
+  // the spare set is the tree before the previous move: work that callers
+  // queued on their own streams may still read it, so wait for the device
+  // before overwriting it (freeing it, as a first move does, waits the same way)
+  if (!rc && !own_pos) rc = check_cuda(ctx, cudaDeviceSynchronize(), "waiting for work on the previous tree");
   if (!rc)
     rc = check_cuda(ctx, cudaMemcpyAsync(d_xf, xf.data(), count * sizeof(drawable_xf), cudaMemcpyHostToDevice, st),
         "drawables");
@@ -158,25 +171,51 @@ int scene_set_transforms(myrt_ctx* ctx, myrt_drawable const* drawables, size_t c
     cleanup();
     return rc;
   }
+  device_bvh8 spare;
+  spare.nodes = reinterpret_cast<bvh8_node*>(s.spare_nodes);
+  spare.tris = s.spare_tris;
+  spare.node_capacity = s.spare_node_capacity;
+  spare.tri_capacity = s.spare_tri_capacity;
   device_bvh8 dt;
   char const* what = nullptr;
-  int const e = build_bvh8_device(d_pos, s.n_prims, st, dt, &what);
-  if (!e) {
-    cudaFree(s.world_pos);  // the re-baked corners become the rasteriser's
-    s.world_pos = d_pos;
-    d_pos = nullptr;
+  int const e = build_bvh8_device(d_pos, s.n_prims, st, ctx->build_scratch, &spare, dt, &what);
+  if (e) {
+    cleanup();
+    return check_cuda(ctx, cudaError_t(e > 0 ? e : cudaErrorInvalidValue), what ? what : "device BVH build");
   }
-  cleanup();
-  if (e) return check_cuda(ctx, cudaError_t(e > 0 ? e : cudaErrorInvalidValue), what ? what : "device BVH build");
+  bool const took_spare = dt.nodes == spare.nodes;
   if (dt.wide_depth > MYRT_STACK_MAX) {
-    cudaFree(dt.nodes);
-    cudaFree(dt.tris);
+    if (!took_spare) {
+      cudaFree(dt.nodes);
+      cudaFree(dt.tris);
+    }
+    cleanup();
     return set_error(ctx, MYRT_ERR_UNSUPPORTED, "BVH deeper than the traversal stack");
   }
-  cudaFree(s.nodes);
-  cudaFree(s.tris);
+  // the re-baked corners become the rasteriser's; the previous corners and
+  // tree become the spare set (a host-built tree has no reusable capacity)
+  s.spare_pos = s.world_pos;
+  s.world_pos = d_pos;
+  if (!took_spare) {
+    cudaFree(s.spare_nodes);
+    cudaFree(s.spare_tris);
+  }
+  if (s.node_capacity > 0) {
+    s.spare_nodes = s.nodes;
+    s.spare_tris = s.tris;
+    s.spare_node_capacity = s.node_capacity;
+    s.spare_tri_capacity = s.tri_capacity;
+  } else {
+    cudaFree(s.nodes);
+    cudaFree(s.tris);
+    s.spare_nodes = nullptr;
+    s.spare_tris = nullptr;
+    s.spare_node_capacity = s.spare_tri_capacity = 0;
+  }
   s.nodes = reinterpret_cast<uint4*>(dt.nodes);
   s.tris = dt.tris;
+  s.node_capacity = dt.node_capacity;
+  s.tri_capacity = dt.tri_capacity;
   s.n_nodes = dt.n_nodes;
   s.n_tris = dt.n_tris;
   s.stats = bvh8_stats{};

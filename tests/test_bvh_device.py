@@ -178,3 +178,45 @@ def test_set_transforms_equals_reupload(ctx):
     bad[0].index_count -= 3
     with pytest.raises(mb.MyrtError):
         ctx.set_transforms(bad)
+
+
+@pytest.mark.parametrize("builder", [0, 1])
+def test_repeated_moves_equal_reupload(ctx, builder):
+    """Moves alternate between two sets of tree and corner buffers (the second
+    move builds into the spare set, the third into the first tree again, ...).
+    After every move in a sequence that returns to earlier poses, ray answers
+    and forward-renderer visibility equal an upload of that pose, for a scene
+    first built on the host (0) and on the device (1)."""
+    from myrt_b200.camera import look_at
+    from myrt_b200.scenes import icosphere_field_lit
+
+    s, _ = icosphere_field_lit(n_spheres=40, subdiv=2, floor_cells=4, seed=9)
+    poses = [_moved(s["drawables"], seed=3), _moved(s["drawables"], seed=5), _moved(s["drawables"], seed=3),
+             s["drawables"], _moved(s["drawables"], seed=7)]
+    rays = np.concatenate([icosphere_camera_rays(96, 72), _rand_rays(20_000, seed=11, lo=-1.2, hi=1.2)])
+    view, proj = look_at((0, 1, -4.5), (0, -0.3, 0), vfov_deg=50, aspect=4 / 3)
+    W, H = 96, 72
+
+    def answers():
+        ctx.forward_render(view, proj, W, H, 1, 256)
+        return ctx.trace_closest(rays), ctx.trace_any(rays), ctx.forward_read(W, H, 256)["visibility"]
+
+    refs = {}
+    try:
+        for i, p in enumerate(poses):
+            key = id(p) if i != 2 else id(poses[0])
+            if key not in refs:
+                ctx.set_tuning(bvh_builder=builder)
+                ctx.upload_scene(**dict(s, drawables=p))
+                refs[key] = answers()
+        ctx.set_tuning(bvh_builder=builder)
+        ctx.upload_scene(**s)
+        for i, p in enumerate(poses):
+            ctx.set_transforms(p)
+            got = answers()
+            ref = refs[id(p) if i != 2 else id(poses[0])]
+            assert np.array_equal(got[0], ref[0]), i
+            assert np.array_equal(got[1], ref[1]), i
+            assert np.array_equal(got[2], ref[2]), i
+    finally:
+        ctx.set_tuning()
