@@ -66,6 +66,8 @@ def parse_args():
     p.add_argument("--sdf-cells", type=int, default=0,
                    help="sdf: cells along the longest axis of the SDF chain's group-list grid (0 = the library's "
                         "default, 1 = no grid: every primitive runs at every march step)")
+    p.add_argument("--sdf-shape", choices=["chain", "tree"], default="chain",
+                   help="sdf: fold the 256 primitives left to right (chain) or as a balanced tree")
     a = p.parse_args()
     if a.workload == "closest":
         a.res = a.res or 512
@@ -815,7 +817,7 @@ def run_sdf_workload(args):
     scene, lights = icosphere_field_lit()
     info = ctx.upload_scene(**scene)
     lib = S.SdfLibrary()
-    lib.add(S.random_sdf_field(256, k=0.1, seed=9, extent=0.8, chain=True))
+    lib.add(S.random_sdf_field(256, k=0.1, seed=9, extent=0.8, chain=args.sdf_shape == "chain"))
     dr = S.sdf_drawables([np.array([[1, 0, 0, 0.0], [0, 1, 0, -0.2], [0, 0, 1, 0.3], [0, 0, 0, 1]])], [0])
     ctx.set_tuning(sdf_cells=args.sdf_cells)
     ctx.upload_sdf(lib.instrs, lib.programs, lib.params, dr)
@@ -859,10 +861,12 @@ def run_sdf_workload(args):
     line = _render_line(
         "samples/s SDF + mesh hybrid (guided)", samples / (ms / 1e3), "samples/s", args.steps, args.warmup,
         ms / args.steps,
-        {"workload": "icosphere scene (655,872 tris) + 256-primitive SDF smooth union (k 0.1, folded left to "
-                     "right), 256 steps, eps 1e-4, guided, 768x768, 128 spp per step, depth 8",
+        {"workload": "icosphere scene (655,872 tris) + 256-primitive SDF smooth union (k 0.1, "
+                     + ("folded left to right" if args.sdf_shape == "chain" else "as a balanced tree")
+                     + "), 256 steps, eps 1e-4, guided, 768x768, 128 spp per step, depth 8",
          "triangles": int(info["triangles"]),
-         "sdf_primitives": 256, "res": W, "spp_per_step": spp, "sdf_cells": args.sdf_cells},
+         "sdf_primitives": 256, "res": W, "spp_per_step": spp, "sdf_cells": args.sdf_cells,
+         "sdf_shape": args.sdf_shape},
         {"mrays_per_s": rays / (ms / 1e3) / 1e6, "rays_per_sample": rays / samples,
          f"rel_rmse_vs_fp64_{oracle_spp}spp": err, "rel_rmse_spp": spp * args.steps,
          "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128,

@@ -51,11 +51,11 @@ struct sdf_dev {
   float eps;
   float4 const* skip_sphere;  // per instruction, or null (see map)
   int2 const* skip_next;
-  // cell lists of left-to-right chain programs, or null (see map): 4 int4 per
-  // program ((lo.xyz, 1 / cell) bits; (nx, ny, nz, first cell), nx = 0: none;
-  // (end of the first group, 0, 0, 0); escape sphere (C.xyz, radius) bits, see
-  // march), per cell the first list entry, and the entries (group start |
-  // group end << 16, relative to the program)
+  // cell lists of union / smooth-union tree programs, or null (see map): 3
+  // int4 per program ((lo.xyz, 1 / cell) bits; (nx, ny, nz, first cell), nx =
+  // 0: none; escape sphere (C.xyz, radius) bits, see march), per cell the
+  // first list entry, and the entries (instruction segment start | end << 16,
+  // relative to the program)
   int4 const* cell_hdr;
   int const* cell_start;
   uint32_t const* cell_list;
@@ -112,11 +112,11 @@ __device__ __forceinline__ float sd_menger(v3 p) {
 // margin covering the rounding of both sides. Material loads (load == true)
 // evaluate every group: their operators draw from the random stream.
 //
-// Cell lists (load == false, chain programs): when p lies in the program's
-// grid, only the first group and the groups listed for p's cell run, in
-// program order; every group left out returns the running value bit for bit
-// at every point of the cell (sdf_skip.hpp sdf_cell_tables), so the result is
-// the full evaluation's.
+// Cell lists (load == false, union / smooth-union trees): when p lies in the
+// program's grid, only the instruction segments listed for p's cell run, in
+// program order; every subtree left out, with its operator, would have left
+// the other operand's value unchanged bit for bit at every point of the cell
+// (sdf_skip.hpp sdf_cell_tables), so the result is the full evaluation's.
 __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load, rs::rng_t* rng, int& mat) {
   int2 const pr = __ldg(s.programs + prog);
   float dist[kStack];
@@ -128,9 +128,9 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
   float const margin = 1e-4f + 1e-6f * ((fabsf(p.x) + fabsf(p.y)) + fabsf(p.z));
   int kend = pr.y, li = 0, le = 0;
   if (!load && s.cell_hdr != nullptr) {
-    int4 const h1 = __ldg(s.cell_hdr + 4 * prog + 1);
+    int4 const h1 = __ldg(s.cell_hdr + 3 * prog + 1);
     if (h1.x > 0) {
-      int4 const h0 = __ldg(s.cell_hdr + 4 * prog);
+      int4 const h0 = __ldg(s.cell_hdr + 3 * prog);
       float const inv = __int_as_float(h0.w);
       float const fx = (p.x - __int_as_float(h0.x)) * inv, fy = (p.y - __int_as_float(h0.y)) * inv,
                   fz = (p.z - __int_as_float(h0.z)) * inv;
@@ -138,7 +138,7 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
         int const c = h1.w + (int(fz) * h1.y + int(fy)) * h1.x + int(fx);
         li = __ldg(s.cell_start + c);
         le = __ldg(s.cell_start + c + 1);
-        kend = __ldg(s.cell_hdr + 4 * prog + 2).x;
+        kend = 0;  // the first segment comes from the list
         skipping = false;
       }
     }
@@ -249,7 +249,7 @@ __device__ __forceinline__ v3 xform4(float const* m, v3 v, float w) {
 // raymarch.glsl:116-171 for drawable `cur`. Returns hits; fills the rest
 // unless hits_only.
 //
-// Early exit (chain programs with an escape sphere): once the march moves
+// Early exit (programs with cell lists and an escape sphere): once the march moves
 // forward (si > 0), is outside the sphere (C, r) widened by eps and heads away
 // from C, every later point keeps a value of at least eps (sdf_skip.hpp
 // sdf_cells), so no hit can follow and the march ends as the reference's
@@ -268,8 +268,8 @@ __device__ __forceinline__ sdf_hit march(
   float t = 10.f * s.eps;
   int si = 0;
   float4 esc = make_float4(0.f, 0.f, 0.f, -1.f);
-  if (s.cell_hdr != nullptr && __ldg(s.cell_hdr + 4 * prog + 1).x > 0) {
-    int4 const e = __ldg(s.cell_hdr + 4 * prog + 3);
+  if (s.cell_hdr != nullptr && __ldg(s.cell_hdr + 3 * prog + 1).x > 0) {
+    int4 const e = __ldg(s.cell_hdr + 3 * prog + 2);
     esc = make_float4(__int_as_float(e.x), __int_as_float(e.y), __int_as_float(e.z), __int_as_float(e.w) + s.eps);
   }
 #pragma unroll 1

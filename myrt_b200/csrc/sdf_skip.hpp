@@ -145,83 +145,114 @@ inline bool sdf_prim_bounds(int op, float const* q, double c[3], double& R, doub
 
 // Per-program cell lists for the evaluator (sdf.cuh map).
 //
-// A program that is a left-to-right chain "T* prim (T* prim op)*" of
-// translations, bounded primitives and union / smooth-union operators keeps a
-// running value d0 that is at most the smallest upper bound |p - c_i| + U_i
-// of the groups before (a smooth union never exceeds the smaller operand). A
-// group i returns d0 bit for bit wherever d_i >= d0 + k_i (see map). Over a
-// cell of a uniform grid laid over the chain's bounding box, group i can be
-// left out when its smallest lower bound is at least the running upper bound
-// plus k_i plus a margin for rounding; the cell keeps the groups that remain,
-// in program order. Points outside the grid evaluate the whole program.
+// Programs that are trees of union / smooth-union operators over translated,
+// bounded primitives (any shape: left or right folds, balanced trees) get a
+// uniform grid over the primitives' bounding boxes. Two facts about an
+// operator op(A, B) with factor k (k = 0 for a union), A the left operand:
+//   * it returns A's value bit for bit where B >= A + k (h clamps to 1), and
+//     B's where A >= B + k (h clamps to 0), up to the sign of a zero result;
+//   * its value lies between min(A, B) - delta and min(A, B): a smooth union
+//     never exceeds its smaller operand and falls below it by at most k / 4;
+//     when one operand is a primitive it stays above min(lower bounds) -
+//     max(delta of the other operand, k) (the blend lowers min(a, b) by
+//     (k - |a - b|)^2 / 4k and never below the primitive minus k).
+// Every node thus has a lower bound (its primitives' |p - c| - R minus its
+// delta) and an upper bound (the smallest |p - c| + U of its primitives) over
+// a cell. Walking the tree from the root, an operator whose right subtree's
+// lower bound is at least the left's upper bound + k + a rounding margin
+// drops the right subtree and itself, and the mirror case drops the left
+// subtree and the operator, for every point of the cell. What remains of the
+// program is stored as instruction segments in program order; the stack then
+// holds the same values as the full evaluation at every step that runs.
+// Points outside the grid evaluate the whole program.
 //
-// Escape sphere: the running value never falls more than k_max below the
-// smallest primitive distance (a smooth union lowers min(d0, d1) by
-// (k - |d1 - d0|)^2 / 4k, which keeps it above the newer operand minus k), so
-// the chain's value is at least |p - C| - rho - k_max with rho bounding every
-// group's |c_i - C| + R_i. A march that is outside the sphere (C, r_esc) and
-// moving away from C never meets a value below eps again (sdf.cuh march).
+// Escape sphere: the root's value is at least |p - C| - rho - delta_root with
+// rho bounding every primitive's |c_i - C| + R_i, so a march that is outside
+// the sphere (C, r_esc) and moving away from C never meets a value below eps
+// again (sdf.cuh march).
 struct sdf_cells {
-  std::vector<int4> hdr;       // 4 per program: (lo.xyz, 1 / cell) bits; (nx, ny, nz, first cell);
-                               // (head end, 0, 0, 0); escape sphere (C.xyz, r_esc) bits
+  std::vector<int4> hdr;       // 3 per program: (lo.xyz, 1 / cell) bits; (nx, ny, nz, first cell);
+                               // escape sphere (C.xyz, r_esc) bits
   std::vector<int> start;      // per program (cells + 1) offsets into list
-  std::vector<uint32_t> list;  // group (start | end << 16), relative to the program's first instruction
+  std::vector<uint32_t> list;  // segment (start | end << 16), relative to the program's first instruction
 };
 
 // cells_long: cells along the grid's longest axis (2..128).
 inline void sdf_cell_tables(myrt_sdf_view const* v, int cells_long, sdf_cells& out) {
   out = sdf_cells{};
-  out.hdr.assign(4 * v->program_count, make_int4(0, 0, 0, 0));
+  out.hdr.assign(3 * v->program_count, make_int4(0, 0, 0, 0));
   float const* G = v->params;
-  struct group {
-    int first, end;
-    double c[3], R, U, k;
+  struct node {
+    int first, end;  // instruction range (end exclusive); an operator's own index is end - 1
+    int a = -1, b = -1;  // operand nodes (operators)
+    double c[3] = {0.0, 0.0, 0.0}, R = 0.0, U = 0.0;  // primitives
+    double k = 0.0, delta = 0.0;
   };
   bool any = false;
   size_t const max_entries = size_t(1) << 26;
   for (size_t p = 0; p < v->program_count; ++p) {
     myrt_sdf_program const pr = v->programs[p];
     if (pr.count >= 65536) continue;
-    std::vector<group> gs;
-    int j = 0;
+    std::vector<node> ns;
+    std::vector<int> st;
+    int n_prims = 0;
     bool ok = true;
-    while (ok && j < pr.count) {
-      group g{};
-      g.first = j;
+    for (int j = 0; ok && j < pr.count;) {
+      myrt_sdf_instr const in = v->instrs[pr.first + j];
+      if (in.op == MYRT_SDF_UNION || in.op == MYRT_SDF_SMOOTH_UNION) {
+        if (st.size() < 2) { ok = false; break; }
+        node n{};
+        n.b = st.back();
+        st.pop_back();
+        n.a = st.back();
+        st.pop_back();
+        n.first = ns[n.a].first;
+        n.end = j + 1;
+        if (in.op == MYRT_SDF_SMOOTH_UNION) {
+          if (!(G[in.param_offset] > 0.f)) { ok = false; break; }
+          n.k = double(G[in.param_offset]);
+        }
+        bool const leaf_a = ns[n.a].a < 0, leaf_b = ns[n.b].a < 0;
+        double const da = ns[n.a].delta, db = ns[n.b].delta;
+        n.delta = (leaf_a || leaf_b) ? std::fmax(std::fmax(da, db), n.k) : std::fmax(da, db) + 0.25 * n.k;
+        if (n.k == 0.0) n.delta = std::fmax(da, db);
+        st.push_back(int(ns.size()));
+        ns.push_back(n);
+        ++j;
+        continue;
+      }
+      node n{};
+      n.first = j;
       while (j < pr.count && v->instrs[pr.first + j].op == MYRT_SDF_TRANSLATE) {
         float const* t = G + v->instrs[pr.first + j].param_offset;
-        for (int a = 0; a < 3; ++a) g.c[a] += double(t[a]);
+        for (int a = 0; a < 3; ++a) n.c[a] += double(t[a]);
         ++j;
       }
       if (j >= pr.count) { ok = false; break; }
       myrt_sdf_instr const prim = v->instrs[pr.first + j];
-      ok = sdf_prim_bounds(prim.op, G + prim.param_offset, g.c, g.R, g.U);
+      ok = sdf_prim_bounds(prim.op, G + prim.param_offset, n.c, n.R, n.U) && std::isfinite(n.R) &&
+           std::isfinite(n.U) && std::isfinite(n.c[0]) && std::isfinite(n.c[1]) && std::isfinite(n.c[2]);
       ++j;
-      if (ok && !gs.empty()) {
-        if (j >= pr.count) { ok = false; break; }
-        myrt_sdf_instr const op = v->instrs[pr.first + j];
-        if (op.op == MYRT_SDF_UNION) g.k = 0.0;
-        else if (op.op == MYRT_SDF_SMOOTH_UNION && G[op.param_offset] > 0.f) g.k = double(G[op.param_offset]);
-        else ok = false;
-        ++j;
-      }
-      g.end = j;
-      ok = ok && std::isfinite(g.R) && std::isfinite(g.U) && std::isfinite(g.c[0]) && std::isfinite(g.c[1]) &&
-           std::isfinite(g.c[2]) && std::isfinite(g.k);
-      if (ok) gs.push_back(g);
+      n.end = j;
+      st.push_back(int(ns.size()));
+      ns.push_back(n);
+      ++n_prims;
     }
-    if (!ok || gs.size() < 8) continue;
-    // grid over the groups' bounding boxes, padded by the largest k
+    if (!ok || st.size() != 1 || n_prims < 8) continue;
+    int const root = st[0];
+    // grid over the primitives' bounding boxes, padded by the largest k
     double lo[3], hi[3], kmax = 0.0, scale = 1.0;
-    for (int a = 0; a < 3; ++a) lo[a] = hi[a] = gs[0].c[a];
-    for (group const& g : gs) {
-      double const r = std::fmax(std::fabs(g.R), std::fabs(g.U));
-      kmax = std::fmax(kmax, g.k);
+    bool first = true;
+    for (node const& n : ns) {
+      kmax = std::fmax(kmax, n.k);
+      if (n.a >= 0) continue;
+      double const r = std::fmax(std::fabs(n.R), std::fabs(n.U));
       for (int a = 0; a < 3; ++a) {
-        lo[a] = std::fmin(lo[a], g.c[a] - r);
-        hi[a] = std::fmax(hi[a], g.c[a] + r);
-        scale = std::fmax(scale, std::fabs(g.c[a]) + r);
+        lo[a] = first ? n.c[a] - r : std::fmin(lo[a], n.c[a] - r);
+        hi[a] = first ? n.c[a] + r : std::fmax(hi[a], n.c[a] + r);
+        scale = std::fmax(scale, std::fabs(n.c[a]) + r);
       }
+      first = false;
     }
     double ext = 0.0;
     for (int a = 0; a < 3; ++a) {
@@ -240,13 +271,26 @@ inline void sdf_cell_tables(myrt_sdf_view const* v, int cells_long, sdf_cells& o
     double const cell = 1.0 / double(inv_f);
     // the device finds a point's cell by rounded float arithmetic: widen each
     // cell; the margin covers the rounding of every distance and of the
-    // running value over all the chain's groups
+    // operators' values over the whole program
     double const widen = 1e-4 * cell + 1e-6 * scale;
-    double const margin = 2e-3 + 4e-6 * double(gs.size()) * scale;
+    double const margin = 2e-3 + 4e-6 * double(n_prims) * scale;
     size_t const first_start = out.start.size();
     size_t const first_entry = out.list.size();
     out.start.reserve(first_start + ncell + 1);
-    std::vector<double> dmin(gs.size()), dmax(gs.size());
+    std::vector<double> lb(ns.size()), ub(ns.size());
+    std::vector<int> todo;
+    uint32_t seg_s = 0, seg_e = 0;
+    bool open = false;
+    auto exec = [&](int s0, int e0) {  // append [s0, e0), merging with the open segment
+      if (open && int(seg_e) == s0) {
+        seg_e = uint32_t(e0);
+        return;
+      }
+      if (open) out.list.push_back(seg_s | (seg_e << 16));
+      seg_s = uint32_t(s0);
+      seg_e = uint32_t(e0);
+      open = true;
+    };
     for (int z = 0; z < dims[2]; ++z)
       for (int y = 0; y < dims[1]; ++y)
         for (int x = 0; x < dims[0]; ++x) {
@@ -257,25 +301,50 @@ inline void sdf_cell_tables(myrt_sdf_view const* v, int cells_long, sdf_cells& o
             bmax[a] = double(lo_f[a]) + (idx[a] + 1) * cell + widen;
           }
           out.start.push_back(int(out.list.size()));
-          double run = 0.0;
-          for (size_t i = 0; i < gs.size(); ++i) {
-            double n2 = 0.0, f2 = 0.0;
-            for (int a = 0; a < 3; ++a) {
-              double const c = gs[i].c[a];
-              double const o = std::fmax(0.0, std::fmax(bmin[a] - c, c - bmax[a]));
-              double const f = std::fmax(std::fabs(c - bmin[a]), std::fabs(c - bmax[a]));
-              n2 += o * o;
-              f2 += f * f;
+          for (size_t i = 0; i < ns.size(); ++i) {  // operands come before their operator
+            node const& n = ns[i];
+            if (n.a < 0) {
+              double n2 = 0.0, f2 = 0.0;
+              for (int a = 0; a < 3; ++a) {
+                double const o = std::fmax(0.0, std::fmax(bmin[a] - n.c[a], n.c[a] - bmax[a]));
+                double const f = std::fmax(std::fabs(n.c[a] - bmin[a]), std::fabs(n.c[a] - bmax[a]));
+                n2 += o * o;
+                f2 += f * f;
+              }
+              lb[i] = std::sqrt(n2) - n.R;
+              ub[i] = std::sqrt(f2) + n.U;
+            } else {
+              lb[i] = std::fmin(lb[n.a] + ns[n.a].delta, lb[n.b] + ns[n.b].delta) - n.delta;
+              ub[i] = std::fmin(ub[n.a], ub[n.b]);
             }
-            double const lb = std::sqrt(n2) - gs[i].R, ub = std::sqrt(f2) + gs[i].U;
-            if (i == 0) {
-              run = ub;
+          }
+          // lb of an operator node is stored as (smallest primitive bound -
+          // its delta); lb + delta recovers the primitives' bound above
+          open = false;
+          todo.assign(1, root);
+          while (!todo.empty()) {  // depth first, left operand first
+            int const i = todo.back();
+            todo.pop_back();
+            if (i < 0) {  // an operator kept with both operands
+              exec(-i - 1, -i);
               continue;
             }
-            if (lb < run + gs[i].k + margin)
-              out.list.push_back(uint32_t(gs[i].first) | (uint32_t(gs[i].end) << 16));
-            run = std::fmin(run, ub);
+            node const& n = ns[i];
+            if (n.a < 0) {
+              exec(n.first, n.end);
+              continue;
+            }
+            if (lb[n.b] >= ub[n.a] + n.k + margin) {
+              todo.push_back(n.a);  // the right operand and the operator drop out
+            } else if (lb[n.a] >= ub[n.b] + n.k + margin) {
+              todo.push_back(n.b);  // the left operand and the operator drop out
+            } else {
+              todo.push_back(-(n.end - 1) - 1);
+              todo.push_back(n.b);
+              todo.push_back(n.a);
+            }
           }
+          if (open) out.list.push_back(seg_s | (seg_e << 16));
         }
     out.start.push_back(int(out.list.size()));
     if (out.list.size() > max_entries) {  // too large: no cells for this program
@@ -283,25 +352,24 @@ inline void sdf_cell_tables(myrt_sdf_view const* v, int cells_long, sdf_cells& o
       out.list.resize(first_entry);
       continue;
     }
-    int lo_bits[3], inv_bits;
-    std::memcpy(lo_bits, lo_f, sizeof lo_bits);
-    std::memcpy(&inv_bits, &inv_f, sizeof inv_bits);
-    out.hdr[4 * p + 0] = make_int4(lo_bits[0], lo_bits[1], lo_bits[2], inv_bits);
-    out.hdr[4 * p + 1] = make_int4(dims[0], dims[1], dims[2], int(first_start));
-    out.hdr[4 * p + 2] = make_int4(gs[0].end, 0, 0, 0);
     // escape sphere about the grid's centre; the radius carries a relative
     // margin for the rounding of values and positions far from the field
     float esc[4];
     double rho = 0.0;
     for (int a = 0; a < 3; ++a) esc[a] = float(0.5 * (lo[a] + hi[a]));
-    for (group const& g : gs) {
-      double const dx = g.c[0] - esc[0], dy = g.c[1] - esc[1], dz = g.c[2] - esc[2];
-      rho = std::fmax(rho, std::sqrt(dx * dx + dy * dy + dz * dz) + g.R);
+    for (node const& n : ns) {
+      if (n.a >= 0) continue;
+      double const dx = n.c[0] - esc[0], dy = n.c[1] - esc[1], dz = n.c[2] - esc[2];
+      rho = std::fmax(rho, std::sqrt(dx * dx + dy * dy + dz * dz) + n.R);
     }
-    esc[3] = float((rho + kmax + margin) * 1.001 + 1e-3);
-    int esc_bits[4];
+    esc[3] = float((rho + ns[root].delta + margin) * 1.001 + 1e-3);
+    int lo_bits[3], inv_bits, esc_bits[4];
+    std::memcpy(lo_bits, lo_f, sizeof lo_bits);
+    std::memcpy(&inv_bits, &inv_f, sizeof inv_bits);
     std::memcpy(esc_bits, esc, sizeof esc_bits);
-    out.hdr[4 * p + 3] = make_int4(esc_bits[0], esc_bits[1], esc_bits[2], esc_bits[3]);
+    out.hdr[3 * p + 0] = make_int4(lo_bits[0], lo_bits[1], lo_bits[2], inv_bits);
+    out.hdr[3 * p + 1] = make_int4(dims[0], dims[1], dims[2], int(first_start));
+    out.hdr[3 * p + 2] = make_int4(esc_bits[0], esc_bits[1], esc_bits[2], esc_bits[3]);
     any = true;
   }
   if (!any) out = sdf_cells{};

@@ -159,8 +159,10 @@ def test_sdf_exact_skipping_matches_oracle(ctx):
 
 
 @pytest.mark.gpu
-def test_sdf_cell_lists_and_early_exit_exact(ctx):
-    """Left-to-right chains get per-cell group lists and an escape sphere at
+@pytest.mark.parametrize("shape", ["chain", "tree", "right_fold"])
+def test_sdf_cell_lists_and_early_exit_exact(ctx, shape):
+    """Union / smooth-union trees (left folds, balanced trees, right folds with
+    unions mixed in) get per-cell instruction segments and an escape sphere at
     upload (tuning sdf_cells). Hits, t, normals and materials are identical
     with the grid off (1), at the default (0 = 32 cells) and at 8 and 96 cells,
     for rays that start outside the field, inside its grid, pass it by or
@@ -168,8 +170,19 @@ def test_sdf_cell_lists_and_early_exit_exact(ctx):
     oracle on a subset."""
     rng = np.random.default_rng(21)
     lib = S.SdfLibrary()
-    lib.add(S.random_sdf_field(256, k=0.1, seed=9, extent=0.8, chain=True))
-    lib.add(S.random_sdf_field(48, k=0.05, seed=3, extent=0.5, chain=True))
+    if shape == "right_fold":
+        r2 = np.random.default_rng(4)
+        for n_prims, k in ((22, 0.08), (16, 0.05)):
+            nodes = [S.translate(S.sphere(float(r2.uniform(0.03, 0.15)), int(r2.integers(0, 4))),
+                                 r2.uniform(-0.7, 0.7, 3)) for _ in range(n_prims)]
+            acc = nodes[-1]
+            for i, nd in enumerate(reversed(nodes[:-1])):
+                acc = S.smooth_union(nd, acc, k) if i % 4 else S.union(nd, acc)
+            lib.add(acc)
+    else:
+        chain = shape == "chain"
+        lib.add(S.random_sdf_field(256, k=0.1, seed=9, extent=0.8, chain=chain))
+        lib.add(S.random_sdf_field(48, k=0.05, seed=3, extent=0.5, chain=chain))
     dr = S.sdf_drawables([np.array([[1, 0, 0, 0.0], [0, 1, 0, -0.2], [0, 0, 1, 0.3], [0, 0, 0, 1]]),
                           np.array([[0.8, 0, 0, 1.2], [0, 0.8, 0, 0.1], [0, 0, 0.8, -0.4], [0, 0, 0, 1]])], [0, 1])
     n = 1 << 16
@@ -193,7 +206,7 @@ def test_sdf_cell_lists_and_early_exit_exact(ctx):
         ctx.set_tuning()
         ctx.upload_sdf(np.zeros((0, 2)), np.zeros((0, 2)), np.zeros(0), np.zeros((0, 36)))
     full = res[1]
-    assert full[0]["hit"].sum() > 5000 and full[1]["hit"].sum() > 5000
+    assert full[0]["hit"].sum() > 2000 and full[1]["hit"].sum() > 2000
     for cells in (0, 8, 96):
         for a in (0, 1):
             for key, v in full[a].items():
