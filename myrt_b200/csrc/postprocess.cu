@@ -43,6 +43,7 @@ __device__ __forceinline__ float4 fetch(img_in const& t, int x, int y) {
   return t.p[size_t(y) * t.w + x];
 }
 __device__ __forceinline__ int mirror_repeat(int i, int size) {
+  if (unsigned(i) < unsigned(size)) return i;  // in range: the mapping below gives i itself
   int m = i % (2 * size);
   if (m < 0) m += 2 * size;
   int const a = m - size;

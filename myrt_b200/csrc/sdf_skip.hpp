@@ -214,8 +214,10 @@ inline void sdf_cell_tables(myrt_sdf_view const* v, int cells_long, sdf_cells& o
         }
         bool const leaf_a = ns[n.a].a < 0, leaf_b = ns[n.b].a < 0;
         double const da = ns[n.a].delta, db = ns[n.b].delta;
-        n.delta = (leaf_a || leaf_b) ? std::fmax(std::fmax(da, db), n.k) : std::fmax(da, db) + 0.25 * n.k;
-        if (n.k == 0.0) n.delta = std::fmax(da, db);
+        // both bounds hold; keep the smaller (two primitives: k / 4; a long
+        // fold saturates at k)
+        n.delta = std::fmax(da, db) + 0.25 * n.k;
+        if (leaf_a || leaf_b) n.delta = std::fmin(n.delta, std::fmax(std::fmax(da, db), n.k));
         st.push_back(int(ns.size()));
         ns.push_back(n);
         ++j;
