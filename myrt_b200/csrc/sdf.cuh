@@ -116,7 +116,9 @@ __device__ __forceinline__ float sd_menger(v3 p) {
 // program's grid, only the instruction segments listed for p's cell run, in
 // program order; every subtree left out, with its operator, would have left
 // the other operand's value unchanged bit for bit at every point of the cell
-// (sdf_skip.hpp sdf_cell_tables), so the result is the full evaluation's.
+// (sdf_skip.hpp sdf_cell_tables), so the result is the full evaluation's. The
+// bounding-sphere test above still applies inside a segment, to groups whose
+// operator runs in the same segment.
 __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load, rs::rng_t* rng, int& mat) {
   int2 const pr = __ldg(s.programs + prog);
   float dist[kStack];
@@ -139,7 +141,6 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
         li = __ldg(s.cell_start + c);
         le = __ldg(s.cell_start + c + 1);
         kend = 0;  // the first segment comes from the list
-        skipping = false;
       }
     }
   }
@@ -153,7 +154,9 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
     }
     if (skipping) {
       int2 const nx = __ldg(s.skip_next + pr.x + k);
-      if (nx.x > 0) {
+      // in a cell segment the group's operator must run in the same segment:
+      // only then is the value below it on the stack its left operand
+      if (nx.x > 0 && nx.x - pr.x <= kend) {
         float4 const b = __ldg(s.skip_sphere + pr.x + k);
         float const thr = ((dist[sp - 1] + __int_as_float(nx.y)) + b.w) + margin;
         float const qx = p.x - b.x, qy = p.y - b.y, qz = p.z - b.z;

@@ -2,7 +2,8 @@
 // tables the library uploads, then evaluates each program and sphere-traces
 // seeded rays twice with the device evaluator's arithmetic restated on the host
 // (sdf.cuh map / march, load == false, every + and * rounded separately):
-// once in full and once through the cell segments and the escape sphere. It
+// once in full and once as the device runs it (cell segments, the per-point
+// bounding-sphere test and the escape sphere). It
 // prints, per program, the grid, the number of points and marches whose
 // results differ in any bit, and the instructions evaluated per march.
 //
@@ -46,6 +47,8 @@ std::vector<myrt_sdf_instr> I;
 std::vector<myrt_sdf_program> P;
 std::vector<float> G;
 sdf_cells C;
+std::vector<float4> skip_sphere;
+std::vector<int2> skip_next;
 long evaluated = 0;
 
 float fbits(int b) {
@@ -60,6 +63,8 @@ float map(int prog, v3 p, bool cells) {
   int sp = 0;
   v3 pos = p;
   int kend = pr.count, li = 0, le = 0;
+  bool const skipping = cells && !skip_next.empty();
+  float const margin = 1e-4f + 1e-6f * ((std::fabs(p.x) + std::fabs(p.y)) + std::fabs(p.z));
   if (cells && !C.hdr.empty() && C.hdr[3 * prog + 1].x > 0) {
     int4 const h0 = C.hdr[3 * prog], h1 = C.hdr[3 * prog + 1];
     float const inv = fbits(h0.w);
@@ -77,6 +82,18 @@ float map(int prog, v3 p, bool cells) {
       uint32_t const e = C.list[li++];
       k = int(e & 0xffffu);
       kend = int(e >> 16);
+    }
+    if (skipping) {  // the per-point bounding-sphere test, as the device runs it
+      int2 const nx = skip_next[pr.first + k];
+      if (nx.x > 0 && nx.x - pr.first <= kend) {
+        float4 const b = skip_sphere[pr.first + k];
+        float const thr = ((dist[sp - 1] + fbits(nx.y)) + b.w) + margin;
+        float const qx = p.x - b.x, qy = p.y - b.y, qz = p.z - b.z;
+        if (thr <= 0.f || (qx * qx + qy * qy) + qz * qz >= thr * thr) {
+          k = nx.x - pr.first - 1;
+          continue;
+        }
+      }
     }
     myrt_sdf_instr const in = I[pr.first + k];
     int const o = in.param_offset;
@@ -168,6 +185,7 @@ int main(int argc, char** argv) {
   v.param_count = G.size();
   int const cells = std::atoi(argv[2]), n_rays = std::atoi(argv[3]);
   sdf_cell_tables(&v, cells, C);
+  sdf_skip_tables(&v, skip_sphere, skip_next);
   std::mt19937 rng(unsigned(std::atoi(argv[4])));
   std::uniform_real_distribution<float> U(-2.5f, 2.5f), J(-0.3f, 0.3f);
   for (int prog = 0; prog < int(P.size()); ++prog) {

@@ -3,9 +3,10 @@
 the device evaluator's float arithmetic (tests/sdf_cells_check.cpp). For left
 folds, balanced trees, right folds with unions, clusters of coincident
 spheres (where smooth unions lower the value the most) and mixed primitives,
-every march point evaluates bit for bit the same through the cell segments as
-in full, and every march (with the escape sphere's early exit) returns the
-same hit and t. Programs outside the supported shape get no grid."""
+every march point evaluates bit for bit the same as the device runs it (cell
+segments and the per-point bounding-sphere test) as in full, and every march
+(with the escape sphere's early exit) returns the same hit and t. Programs
+outside the supported shape get no grid."""
 import shutil
 import subprocess
 from pathlib import Path
@@ -97,5 +98,5 @@ def test_cell_segments_and_early_exit_are_exact(checker, tmp_path, cells):
         assert (grid > 0) == expect_grid, name
         if expect_grid:
             assert cell_i < 0.5 * full_i, (name, cell_i, full_i)
-        else:
-            assert cell_i == full_i, name
+        else:  # no grid: only the per-point bounding-sphere test of the inner groups
+            assert cell_i <= full_i, name
