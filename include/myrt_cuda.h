@@ -158,10 +158,11 @@ typedef struct myrt_tuning {
                                 of at least 1 Mi rays sorted by origin and direction cell, host-memory
                                 queries in input order; 1 = input order; 2 = always sorted.
                                 Results never depend on it. */
-  uint32_t sdf_cells;        /* myrt_sdf_upload: cells along the longest axis of the grid of group lists
-                                built for each left-to-right union / smooth-union chain program
-                                (0 = 32, 1 = no grid: every group runs, 2..128). Results never
-                                depend on it. */
+  uint32_t sdf_cells;        /* myrt_sdf_upload: cells along the longest axis of the grid of
+                                instruction segments built for each program that is a tree of
+                                unions / smooth unions over translated spheres, boxes, tori and
+                                capsules (0 = 32, 1 = no grid and no early exit, 2..128). Results
+                                never depend on it. */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */
@@ -285,7 +286,11 @@ typedef struct myrt_sdf_view {
  * src/pathtracer/scene.cpp:345-351, 399-401) and the GLSL assembly of
  * sdf_glsl_assembler (sdf.cpp:378-407). Programs are validated (opcodes,
  * parameter ranges, stack depth <= 24, one result). drawable_count == 0
- * removes all SDF drawables. Restarts accumulation. */
+ * removes all SDF drawables. Restarts accumulation. Programs that are trees
+ * of unions / smooth unions also get, per cell of a grid (myrt_tuning.
+ * sdf_cells), the instruction segments that can change their value there,
+ * and a sphere outside which a march that moves away ends without a hit;
+ * both leave every result bit-identical. */
 int myrt_sdf_upload(myrt_ctx* ctx, const myrt_sdf_view* sdf);
 /* SDF part of nearest_hit / any_hit (src/pt/pt_trace.comp:321-326, 342-352)
  * over all SDF drawables for n host rays (tmax = max distance), with
