@@ -201,7 +201,10 @@ int myrt_scene_bvh_info(myrt_ctx* ctx, myrt_bvh_info* info);
  * and material_index for every drawable of the uploaded scene (same count and
  * index ranges as uploaded). Re-bakes the world triangles and normals on the
  * device from the object-space geometry kept since the upload and rebuilds the
- * tree with the device builder; restarts accumulation. */
+ * tree with the device builder; restarts accumulation. From the second move
+ * on, the new tree is built into the buffers of the tree before the previous
+ * move (no allocation), after a device-wide synchronisation, so work that
+ * callers queued on their own streams against that older tree has finished. */
 int myrt_scene_set_transforms(myrt_ctx* ctx, const myrt_drawable* drawables, size_t count);
 /* Copies the scene's device tree to host memory: nodes (80 bytes each) and
  * leaf-ordered triangles (48 bytes each), as counted by myrt_scene_bvh_info;
