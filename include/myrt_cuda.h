@@ -161,8 +161,9 @@ typedef struct myrt_tuning {
   uint32_t sdf_cells;        /* myrt_sdf_upload: cells along the longest axis of the grid of
                                 instruction segments built for each program that is a tree of
                                 unions / smooth unions over translated spheres, boxes, tori and
-                                capsules (0 = 32, 1 = no grid and no early exit, 2..128). Results
-                                never depend on it. */
+                                capsules (0 = 32, 1 = no grid and no early exit, 2..128; programs
+                                with thousands of primitives get coarser grids so that the upload
+                                stays near a second). Results never depend on it. */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */

@@ -262,12 +262,16 @@ inline void sdf_cell_tables(myrt_sdf_view const* v, int cells_long, sdf_cells& o
       hi[a] += kmax + 1e-3;
       ext = std::fmax(ext, hi[a] - lo[a]);
     }
-    float const inv_f = float(double(cells_long) / ext);
+    // host work is cells x nodes: coarser grids for very large programs keep
+    // an upload within about 2^26 node bounds (about a second)
+    int n_long = cells_long;
+    while (n_long > 4 && double(n_long) * n_long * n_long * double(ns.size()) > double(1 << 26)) n_long = n_long * 3 / 4;
+    float const inv_f = float(double(n_long) / ext);
     float lo_f[3];
     int dims[3];
     for (int a = 0; a < 3; ++a) {
       lo_f[a] = float(lo[a]);
-      dims[a] = std::max(1, std::min(cells_long, int(std::ceil((hi[a] - double(lo_f[a])) * double(inv_f)))));
+      dims[a] = std::max(1, std::min(n_long, int(std::ceil((hi[a] - double(lo_f[a])) * double(inv_f)))));
     }
     size_t const ncell = size_t(dims[0]) * dims[1] * dims[2];
     double const cell = 1.0 / double(inv_f);

@@ -93,15 +93,20 @@ class SdfLibrary:
         self._params.extend(float(v) for v in values)
         return off
 
-    def _emit(self, n: Node):
-        if n.children:
-            self._emit(n.children[0])
-            self._emit(n.children[1])
+    def _emit(self, root: Node):
+        # post order without recursion (long folds nest thousands deep)
+        todo = [(root, False)]
+        while todo:
+            n, expanded = todo.pop()
+            if n.children and not expanded:
+                todo.append((n, True))
+                todo.append((n.children[1], False))
+                todo.append((n.children[0], False))
+                continue
+            if not n.children:
+                for op, params in n.mods:
+                    self._instrs.append((op, self._param(params)))
             self._instrs.append((n.op, self._param(n.params)))
-            return
-        for op, params in n.mods:
-            self._instrs.append((op, self._param(params)))
-        self._instrs.append((n.op, self._param(n.params)))
 
     def add(self, root: Node) -> int:
         first = len(self._instrs)
