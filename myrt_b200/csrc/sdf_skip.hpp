@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -282,82 +283,113 @@ inline void sdf_cell_tables(myrt_sdf_view const* v, int cells_long, sdf_cells& o
     double const margin = 2e-3 + 4e-6 * double(n_prims) * scale;
     size_t const first_start = out.start.size();
     size_t const first_entry = out.list.size();
-    out.start.reserve(first_start + ncell + 1);
-    std::vector<double> lb(ns.size()), ub(ns.size());
-    std::vector<int> todo;
-    uint32_t seg_s = 0, seg_e = 0;
-    bool open = false;
-    auto exec = [&](int s0, int e0) {  // append [s0, e0), merging with the open segment
-      if (open && int(seg_e) == s0) {
-        seg_e = uint32_t(e0);
-        return;
-      }
-      if (open) out.list.push_back(seg_s | (seg_e << 16));
-      seg_s = uint32_t(s0);
-      seg_e = uint32_t(e0);
-      open = true;
+    // z-slabs of cells on host threads; each keeps its cells' segment counts
+    // and segments, concatenated in cell order afterwards
+    struct slab {
+      std::vector<int> sizes;
+      std::vector<uint32_t> segs;
     };
-    for (int z = 0; z < dims[2]; ++z)
-      for (int y = 0; y < dims[1]; ++y)
-        for (int x = 0; x < dims[0]; ++x) {
-          int const idx[3] = {x, y, z};
-          double bmin[3], bmax[3];
-          for (int a = 0; a < 3; ++a) {
-            bmin[a] = double(lo_f[a]) + idx[a] * cell - widen;
-            bmax[a] = double(lo_f[a]) + (idx[a] + 1) * cell + widen;
-          }
-          out.start.push_back(int(out.list.size()));
-          for (size_t i = 0; i < ns.size(); ++i) {  // operands come before their operator
-            node const& n = ns[i];
-            if (n.a < 0) {
-              double n2 = 0.0, f2 = 0.0;
-              for (int a = 0; a < 3; ++a) {
-                double const o = std::fmax(0.0, std::fmax(bmin[a] - n.c[a], n.c[a] - bmax[a]));
-                double const f = std::fmax(std::fabs(n.c[a] - bmin[a]), std::fabs(n.c[a] - bmax[a]));
-                n2 += o * o;
-                f2 += f * f;
-              }
-              lb[i] = std::sqrt(n2) - n.R;
-              ub[i] = std::sqrt(f2) + n.U;
-            } else {
-              lb[i] = std::fmin(lb[n.a] + ns[n.a].delta, lb[n.b] + ns[n.b].delta) - n.delta;
-              ub[i] = std::fmin(ub[n.a], ub[n.b]);
-            }
-          }
-          // lb of an operator node is stored as (smallest primitive bound -
-          // its delta); lb + delta recovers the primitives' bound above
-          open = false;
-          todo.assign(1, root);
-          while (!todo.empty()) {  // depth first, left operand first
-            int const i = todo.back();
-            todo.pop_back();
-            if (i < 0) {  // an operator kept with both operands
-              exec(-i - 1, -i);
-              continue;
-            }
-            node const& n = ns[i];
-            if (n.a < 0) {
-              exec(n.first, n.end);
-              continue;
-            }
-            if (lb[n.b] >= ub[n.a] + n.k + margin) {
-              todo.push_back(n.a);  // the right operand and the operator drop out
-            } else if (lb[n.a] >= ub[n.b] + n.k + margin) {
-              todo.push_back(n.b);  // the left operand and the operator drop out
-            } else {
-              todo.push_back(-(n.end - 1) - 1);
-              todo.push_back(n.b);
-              todo.push_back(n.a);
-            }
-          }
-          if (open) out.list.push_back(seg_s | (seg_e << 16));
+    int const n_threads = std::max(1, std::min<int>(dims[2], int(std::thread::hardware_concurrency())));
+    std::vector<slab> slabs(n_threads);
+    auto fill = [&](int t) {
+      slab& out_t = slabs[t];
+      std::vector<double> lb(ns.size()), ub(ns.size());
+      std::vector<int> todo;
+      uint32_t seg_s = 0, seg_e = 0;
+      bool open = false;
+      auto exec = [&](int s0, int e0) {  // append [s0, e0), merging with the open segment
+        if (open && int(seg_e) == s0) {
+          seg_e = uint32_t(e0);
+          return;
         }
-    out.start.push_back(int(out.list.size()));
-    if (out.list.size() > max_entries) {  // too large: no cells for this program
-      out.start.resize(first_start);
-      out.list.resize(first_entry);
-      continue;
+        if (open) out_t.segs.push_back(seg_s | (seg_e << 16));
+        seg_s = uint32_t(s0);
+        seg_e = uint32_t(e0);
+        open = true;
+      };
+      int const z0 = int(int64_t(dims[2]) * t / n_threads), z1 = int(int64_t(dims[2]) * (t + 1) / n_threads);
+      for (int z = z0; z < z1; ++z)
+        for (int y = 0; y < dims[1]; ++y)
+          for (int x = 0; x < dims[0]; ++x) {
+            int const idx[3] = {x, y, z};
+            double bmin[3], bmax[3];
+            for (int a = 0; a < 3; ++a) {
+              bmin[a] = double(lo_f[a]) + idx[a] * cell - widen;
+              bmax[a] = double(lo_f[a]) + (idx[a] + 1) * cell + widen;
+            }
+            size_t const before = out_t.segs.size();
+            for (size_t i = 0; i < ns.size(); ++i) {  // operands come before their operator
+              node const& n = ns[i];
+              if (n.a < 0) {
+                double n2 = 0.0, f2 = 0.0;
+                for (int a = 0; a < 3; ++a) {
+                  double const o = std::fmax(0.0, std::fmax(bmin[a] - n.c[a], n.c[a] - bmax[a]));
+                  double const f = std::fmax(std::fabs(n.c[a] - bmin[a]), std::fabs(n.c[a] - bmax[a]));
+                  n2 += o * o;
+                  f2 += f * f;
+                }
+                lb[i] = std::sqrt(n2) - n.R;
+                ub[i] = std::sqrt(f2) + n.U;
+              } else {
+                // lb of an operator node is (its primitives' smallest bound -
+                // its delta); lb + delta recovers the primitives' bound
+                lb[i] = std::fmin(lb[n.a] + ns[n.a].delta, lb[n.b] + ns[n.b].delta) - n.delta;
+                ub[i] = std::fmin(ub[n.a], ub[n.b]);
+              }
+            }
+            open = false;
+            todo.assign(1, root);
+            while (!todo.empty()) {  // depth first, left operand first
+              int const i = todo.back();
+              todo.pop_back();
+              if (i < 0) {  // an operator kept with both operands
+                exec(-i - 1, -i);
+                continue;
+              }
+              node const& n = ns[i];
+              if (n.a < 0) {
+                exec(n.first, n.end);
+                continue;
+              }
+              if (lb[n.b] >= ub[n.a] + n.k + margin) {
+                todo.push_back(n.a);  // the right operand and the operator drop out
+              } else if (lb[n.a] >= ub[n.b] + n.k + margin) {
+                todo.push_back(n.b);  // the left operand and the operator drop out
+              } else {
+                todo.push_back(-(n.end - 1) - 1);
+                todo.push_back(n.b);
+                todo.push_back(n.a);
+              }
+            }
+            if (open) out_t.segs.push_back(seg_s | (seg_e << 16));
+            out_t.sizes.push_back(int(out_t.segs.size() - before));
+          }
+    };
+    {
+      std::vector<std::thread> pool;
+      for (int t = 1; t < n_threads; ++t) pool.emplace_back(fill, t);
+      fill(0);
+      for (std::thread& th : pool) th.join();
     }
+    size_t total = out.list.size();
+    for (slab const& sl : slabs) total += sl.segs.size();
+    if (total > max_entries) continue;  // too large: no cells for this program
+    out.start.reserve(first_start + ncell + 1);
+    out.list.reserve(total);
+    for (slab const& sl : slabs) {
+      for (int n_seg : sl.sizes) {
+        out.start.push_back(int(out.list.size()));
+        out.list.resize(out.list.size() + size_t(n_seg));
+      }
+    }
+    {  // copy the segments behind the offsets just laid out
+      size_t at = first_entry;
+      for (slab const& sl : slabs) {
+        std::copy(sl.segs.begin(), sl.segs.end(), out.list.begin() + ptrdiff_t(at));
+        at += sl.segs.size();
+      }
+    }
+    out.start.push_back(int(out.list.size()));
     // escape sphere about the grid's centre; the radius carries a relative
     // margin for the rounding of values and positions far from the field
     float esc[4];

@@ -25,7 +25,7 @@ def checker(tmp_path_factory):
     if gxx is None:
         pytest.skip("g++ not available")
     exe = tmp_path_factory.mktemp("sdfcells") / "sdf_cells_check"
-    subprocess.run([gxx, "-O2", "-std=c++20", "-ffp-contract=off", "-I", "/usr/local/cuda/include",
+    subprocess.run([gxx, "-O2", "-std=c++20", "-pthread", "-ffp-contract=off", "-I", "/usr/local/cuda/include",
                     "-o", str(exe), str(ROOT / "tests" / "sdf_cells_check.cpp")], check=True)
     return exe
 
