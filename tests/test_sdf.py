@@ -215,3 +215,22 @@ def test_sdf_cell_lists_and_early_exit_exact(ctx, shape):
     ora = po.sdf_trace(lib, dr, rays[sub], 256, 1e-4, False, states[sub])
     for key in ("hit", "t", "normal", "material"):
         assert np.array_equal(res[0][0][key][sub], ora[key]), key
+
+
+def test_sdf_library_emits_deep_folds():
+    """The flat-program emitter walks the tree without recursion: a left fold of
+    3,000 translated spheres serialises in post order (translate, sphere, then
+    translate, sphere, smooth union per further primitive)."""
+    n = 3000
+    acc = S.translate(S.sphere(0.1, 1), (0.0, 0.0, 0.0))
+    for i in range(1, n):
+        acc = S.smooth_union(acc, S.translate(S.sphere(0.1, 1), (0.01 * i, 0.0, 0.0)), 0.05)
+    lib = S.SdfLibrary()
+    assert lib.add(acc) == 0
+    ops = lib.instrs[:, 0]
+    assert lib.programs.tolist() == [[0, 3 * n - 1]]
+    assert ops[:2].tolist() == [S.TRANSLATE, S.SPHERE]
+    assert (ops[2:].reshape(-1, 3) == [S.TRANSLATE, S.SPHERE, S.SMOOTH_UNION]).all()
+    # parameter offsets point at each translation's own x offset
+    offs = lib.instrs[2::3, 1]
+    assert np.allclose(lib.params[offs], 0.01 * np.arange(1, n))
