@@ -426,6 +426,7 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   cudaFree(ctx->sdf.cell_hdr);
   cudaFree(ctx->sdf.cell_start);
   cudaFree(ctx->sdf.cell_list);
+  cudaFree(ctx->sdf.op_count);
   free_render(ctx->render);
   free_textures(ctx);
   free_forward(ctx);
@@ -680,6 +681,7 @@ int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
   cudaFree(D.cell_hdr);
   cudaFree(D.cell_start);
   cudaFree(D.cell_list);
+  cudaFree(D.op_count);
   D = device_sdf{};
   ctx->render.sample_counter = 0;
   if (v->drawable_count == 0) return MYRT_OK;
@@ -729,7 +731,11 @@ int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
   std::vector<int2> skip_next;
   sdf_skip_tables(v, skip_sphere, skip_next);
   sdf_cells cells;
-  if (ctx->tuning.sdf_cells != 1) sdf_cell_tables(v, ctx->tuning.sdf_cells ? int(ctx->tuning.sdf_cells) : 32, cells);
+  std::vector<int> op_count;
+  if (ctx->tuning.sdf_cells != 1) {
+    sdf_cell_tables(v, ctx->tuning.sdf_cells ? int(ctx->tuning.sdf_cells) : 32, cells);
+    if (!skip_next.empty() || !cells.list.empty()) sdf_op_counts(v, op_count);
+  }
   std::vector<float> dr(v->drawable_count * 36);
   for (size_t d = 0; d < v->drawable_count; ++d) {
     myrt_sdf_drawable const& s = v->drawables[d];
@@ -751,6 +757,7 @@ int myrt_sdf_upload(myrt_ctx* ctx, myrt_sdf_view const* v) {
     if (!rc) rc = upload(ctx, &D.cell_start, cells.start.data(), cells.start.size(), "SDF cell starts");
     if (!rc) rc = upload(ctx, &D.cell_list, cells.list.data(), cells.list.size(), "SDF cell lists");
   }
+  if (!rc && !op_count.empty()) rc = upload(ctx, &D.op_count, op_count.data(), op_count.size(), "SDF operator counts");
   if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "SDF upload");
   if (rc) return rc;
   D.n_drawables = int(v->drawable_count);

@@ -73,6 +73,7 @@ struct device_sdf {
   int4* cell_hdr = nullptr;
   int* cell_start = nullptr;
   uint32_t* cell_list = nullptr;
+  int* op_count = nullptr;  // sdf_skip.hpp sdf_op_counts, null when not usable
   int n_drawables = 0;
   int n_programs = 0;
 };

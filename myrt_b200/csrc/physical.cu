@@ -513,7 +513,7 @@ pt_scene scene_of(myrt_ctx const* ctx) {
       int(S.n_materials), S.material_data, static_cast<ps::area_light const*>(P.lights), P.n_lights,
       sdfk::sdf_dev{ctx->sdf.instrs, ctx->sdf.programs, ctx->sdf.params, ctx->sdf.drawables, ctx->sdf.n_drawables,
           0, 0.f, ctx->sdf.skip_sphere, ctx->sdf.skip_next, ctx->sdf.cell_hdr, ctx->sdf.cell_start,
-          ctx->sdf.cell_list}};
+          ctx->sdf.cell_list, ctx->sdf.op_count}};
 }
 
 // A job's static description (camera, resolution, spp, ...); the wave planner

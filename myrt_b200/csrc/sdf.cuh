@@ -59,6 +59,9 @@ struct sdf_dev {
   int4 const* cell_hdr;
   int const* cell_start;
   uint32_t const* cell_list;
+  // per instruction: operators of its program up to and including it, or null
+  // (material loads then evaluate everything)
+  int const* op_count;
 };
 
 __device__ __forceinline__ v3 abs3(v3 a) { return {fabsf(a.x), fabsf(a.y), fabsf(a.z)}; }
@@ -110,7 +113,8 @@ __device__ __forceinline__ float sd_menger(v3 p) {
 // The primitive's distance is at least |p - c| - R for its bounding sphere
 // (c, R), so the group is skipped when |p - c| >= d0 + k + R + margin, the
 // margin covering the rounding of both sides. Material loads (load == true)
-// evaluate every group: their operators draw from the random stream.
+// skip the same way when the per-instruction operator counts are present: the
+// operators left out still draw from the random stream, in program order.
 //
 // Cell lists (load == false, union / smooth-union trees): when p lies in the
 // program's grid, only the instruction segments listed for p's cell run, in
@@ -126,10 +130,16 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
   int sp = 0;
   v3 pos = p;
   float const* G = s.params;
-  bool skipping = !load && s.skip_next != nullptr;
+  // material loads skip too when every left-out operator's draw can still be
+  // made (op_count): a right operand left out never decides the material (t =
+  // 0); a left operand left out decides it only on a draw of exactly 1, after
+  // which the whole program runs again from the saved random state
+  bool const counting = load && s.op_count != nullptr;
+  bool const skipping = (!load || counting) && s.skip_next != nullptr;
   float const margin = 1e-4f + 1e-6f * ((fabsf(p.x) + fabsf(p.y)) + fabsf(p.z));
-  int kend = pr.y, li = 0, le = 0;
-  if (!load && s.cell_hdr != nullptr) {
+  int cell_li = 0, cell_le = 0;
+  bool use_cells = false;
+  if ((!load || counting) && s.cell_hdr != nullptr) {
     int4 const h1 = __ldg(s.cell_hdr + 3 * prog + 1);
     if (h1.x > 0) {
       int4 const h0 = __ldg(s.cell_hdr + 3 * prog);
@@ -138,12 +148,30 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
                   fz = (p.z - __int_as_float(h0.z)) * inv;
       if (fx >= 0.f && fy >= 0.f && fz >= 0.f && fx < float(h1.x) && fy < float(h1.y) && fz < float(h1.z)) {
         int const c = h1.w + (int(fz) * h1.y + int(fy)) * h1.x + int(fx);
-        li = __ldg(s.cell_start + c);
-        le = __ldg(s.cell_start + c + 1);
-        kend = 0;  // the first segment comes from the list
+        cell_li = __ldg(s.cell_start + c);
+        cell_le = __ldg(s.cell_start + c + 1);
+        use_cells = true;
       }
     }
   }
+  rs::rng_t const saved = counting ? *rng : rs::rng_t{};
+  bool redo = false;
+  // the draws of the operators in instructions [a, b) that do not run
+  auto draw_gap = [&](int a, int b) {
+    if (b <= a) return;
+    int const n = __ldg(s.op_count + pr.x + b - 1) - (a > 0 ? __ldg(s.op_count + pr.x + a - 1) : 0);
+#pragma unroll 1
+    for (int i = 0; i < n; ++i)
+      if (rs::random_next(*rng) >= 1.f) redo = true;
+  };
+#pragma unroll 1
+  for (int pass = 0;; ++pass) {
+  bool const fast = pass == 0;
+  int kend = fast && use_cells ? 0 : pr.y;  // cells: the first segment comes from the list
+  int li = fast && use_cells ? cell_li : 0, le = fast && use_cells ? cell_le : 0;
+  int drawn = 0;  // counting: the operators before this instruction have drawn
+  sp = 0;
+  pos = p;
 #pragma unroll 1
   for (int k = 0;; ++k) {
     if (k >= kend) {
@@ -151,8 +179,9 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
       uint32_t const e = __ldg(s.cell_list + li++);
       k = int(e & 0xffffu);
       kend = int(e >> 16);
+      if (counting) draw_gap(drawn, k);
     }
-    if (skipping) {
+    if (skipping && fast) {
       int2 const nx = __ldg(s.skip_next + pr.x + k);
       // in a cell segment the group's operator must run in the same segment:
       // only then is the value below it on the stack its left operand
@@ -161,11 +190,14 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
         float const thr = ((dist[sp - 1] + __int_as_float(nx.y)) + b.w) + margin;
         float const qx = p.x - b.x, qy = p.y - b.y, qz = p.z - b.z;
         if (thr <= 0.f || (qx * qx + qy * qy) + qz * qz >= thr * thr) {
+          if (counting) draw_gap(k, nx.x - pr.x);
+          drawn = nx.x - pr.x;
           k = nx.x - pr.x - 1;  // continue after the group's operator
           continue;
         }
       }
     }
+    drawn = k + 1;
     int2 const in = __ldg(s.instrs + pr.x + k);
     int const o = in.y;
     int m = mat;
@@ -230,6 +262,11 @@ __device__ __forceinline__ float map(sdf_dev const& s, int prog, v3 p, bool load
     mats[sp] = m;
     ++sp;
     pos = p;
+  }
+  if (counting && fast) draw_gap(drawn, pr.y);
+  if (!redo) break;
+  *rng = saved;  // a left-out left operand met a draw of 1: run everything
+  redo = false;
   }
   mat = mats[sp - 1];
   return dist[sp - 1];

@@ -113,6 +113,29 @@ inline void sdf_skip_tables(myrt_sdf_view const* v, std::vector<float4>& sphere,
   }
 }
 
+// Per instruction: the number of operator instructions of its program up to and
+// including it, so that an evaluation that leaves out a range of instructions
+// can still draw the random numbers those operators would have drawn (sdf.cuh
+// map, material loads). Empty when programs share instructions at different
+// offsets.
+inline void sdf_op_counts(myrt_sdf_view const* v, std::vector<int>& out) {
+  out.assign(v->instr_count, -1);
+  for (size_t p = 0; p < v->program_count; ++p) {
+    myrt_sdf_program const pr = v->programs[p];
+    int n = 0;
+    for (int k = 0; k < pr.count; ++k) {
+      int const op = v->instrs[pr.first + k].op;
+      if (op >= MYRT_SDF_UNION && op < MYRT_SDF_TRANSLATE) ++n;
+      int& slot = out[pr.first + k];
+      if (slot >= 0 && slot != n) {
+        out.clear();
+        return;
+      }
+      slot = n;
+    }
+  }
+}
+
 // Distance bounds of a primitive about a centre c (updated in place for the
 // capsule, whose centre is its segment's midpoint):
 //   |p - c| - R  <=  d(p)  <=  |p - c| + U   for every point p.

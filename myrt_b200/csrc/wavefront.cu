@@ -60,7 +60,7 @@ struct scene_dev {
 sdfk::sdf_dev make_sdf_dev(myrt_ctx const* ctx, int steps, float eps) {
   device_sdf const& D = ctx->sdf;
   return sdfk::sdf_dev{D.instrs, D.programs, D.params, D.drawables, D.n_drawables, steps, eps, D.skip_sphere,
-      D.skip_next, D.cell_hdr, D.cell_start, D.cell_list};
+      D.skip_next, D.cell_hdr, D.cell_start, D.cell_list, D.op_count};
 }
 
 struct camera_dev {

@@ -49,7 +49,39 @@ std::vector<float> G;
 sdf_cells C;
 std::vector<float4> skip_sphere;
 std::vector<int2> skip_next;
-long evaluated = 0;
+std::vector<int> op_count;
+long evaluated = 0, redos = 0;
+
+// random.glsl's stream as the device restates it (refshade.cuh)
+struct rng_t {
+  uint32_t state;
+  int prime;
+};
+uint32_t wang(uint32_t a) {
+  a = (a ^ 61u) ^ (a >> 16);
+  a = a + (a << 3);
+  a = a ^ (a >> 4);
+  a = a * 0x27d4eb2du;
+  a = a ^ (a >> 15);
+  return a;
+}
+float random_next(rng_t& r) {
+  r.prime = r.prime == 5 ? 0 : r.prime + 1;
+  r.state += wang(uint32_t(r.prime));
+  r.state ^= (r.state << 13);
+  r.state ^= (r.state >> 17);
+  r.state ^= (r.state << 5);
+  return gclamp(float(r.state) * (1.f / 4294967296.f), 0.f, 1.f);
+}
+// the state before random_next, given the state after it
+rng_t random_prev(rng_t r) {
+  uint32_t x = r.state;
+  x ^= (x << 5) ^ (x << 10) ^ (x << 15) ^ (x << 20) ^ (x << 25) ^ (x << 30);
+  x ^= (x >> 17);
+  x ^= (x << 13) ^ (x << 26);
+  x -= wang(uint32_t(r.prime));
+  return rng_t{x, r.prime == 0 ? 5 : r.prime - 1};
+}
 
 float fbits(int b) {
   float f;
@@ -57,15 +89,17 @@ float fbits(int b) {
   return f;
 }
 
-float map(int prog, v3 p, bool cells) {
+float map(int prog, v3 p, bool cells, bool load = false, rng_t* rng = nullptr, int* mat = nullptr) {
   myrt_sdf_program const pr = P[prog];
   float dist[64];
+  int mats[64];
   int sp = 0;
   v3 pos = p;
   int kend = pr.count, li = 0, le = 0;
-  bool const skipping = cells && !skip_next.empty();
+  bool const counting = cells && load && !op_count.empty();
+  bool const skipping = cells && (!load || counting) && !skip_next.empty();
   float const margin = 1e-4f + 1e-6f * ((std::fabs(p.x) + std::fabs(p.y)) + std::fabs(p.z));
-  if (cells && !C.hdr.empty() && C.hdr[3 * prog + 1].x > 0) {
+  if (cells && (!load || counting) && !C.hdr.empty() && C.hdr[3 * prog + 1].x > 0) {
     int4 const h0 = C.hdr[3 * prog], h1 = C.hdr[3 * prog + 1];
     float const inv = fbits(h0.w);
     float const fx = (p.x - fbits(h0.x)) * inv, fy = (p.y - fbits(h0.y)) * inv, fz = (p.z - fbits(h0.z)) * inv;
@@ -76,41 +110,65 @@ float map(int prog, v3 p, bool cells) {
       kend = 0;
     }
   }
+  rng_t const saved = counting ? *rng : rng_t{};
+  bool redo = false;
+  auto draw_gap = [&](int a, int b) {
+    if (b <= a) return;
+    int const n = op_count[pr.first + b - 1] - (a > 0 ? op_count[pr.first + a - 1] : 0);
+    for (int i = 0; i < n; ++i)
+      if (random_next(*rng) >= 1.f) redo = true;
+  };
+  int const cell_li = li, cell_le = le, cell_kend = kend;
+  for (int pass = 0;; ++pass) {
+  bool const fast = pass == 0;
+  kend = fast ? cell_kend : pr.count;
+  li = fast ? cell_li : 0;
+  le = fast ? cell_le : 0;
+  int drawn = 0;
+  sp = 0;
+  pos = p;
   for (int k = 0;; ++k) {
     if (k >= kend) {
       if (li >= le) break;
       uint32_t const e = C.list[li++];
       k = int(e & 0xffffu);
       kend = int(e >> 16);
+      if (counting) draw_gap(drawn, k);
     }
-    if (skipping) {  // the per-point bounding-sphere test, as the device runs it
+    if (skipping && fast) {  // the per-point bounding-sphere test, as the device runs it
       int2 const nx = skip_next[pr.first + k];
       if (nx.x > 0 && nx.x - pr.first <= kend) {
         float4 const b = skip_sphere[pr.first + k];
         float const thr = ((dist[sp - 1] + fbits(nx.y)) + b.w) + margin;
         float const qx = p.x - b.x, qy = p.y - b.y, qz = p.z - b.z;
         if (thr <= 0.f || (qx * qx + qy * qy) + qz * qz >= thr * thr) {
+          if (counting) draw_gap(k, nx.x - pr.first);
+          drawn = nx.x - pr.first;
           k = nx.x - pr.first - 1;
           continue;
         }
       }
     }
+    drawn = k + 1;
     myrt_sdf_instr const in = I[pr.first + k];
     int const o = in.param_offset;
     float d = 0.f;
+    int m = -1;
     ++evaluated;
     switch (in.op) {
       case MYRT_SDF_TRANSLATE:
         pos = {pos.x - G[o], pos.y - G[o + 1], pos.z - G[o + 2]};
         continue;
-      case MYRT_SDF_SPHERE: d = len3(pos) - G[o]; break;
+      case MYRT_SDF_SPHERE: m = int(G[o + 1]); d = len3(pos) - G[o]; break;
       case MYRT_SDF_BOX: {
+        m = int(G[o + 3]);
         v3 const q{std::fabs(pos.x) - G[o], std::fabs(pos.y) - G[o + 1], std::fabs(pos.z) - G[o + 2]};
         d = len3({gmax(q.x, 0.f), gmax(q.y, 0.f), gmax(q.z, 0.f)}) + gmin(gmax(q.x, gmax(q.y, q.z)), 0.f);
         break;
       }
-      case MYRT_SDF_TORUS: d = len2(len2(pos.x, pos.z) - G[o], pos.y) - G[o + 1]; break;
+      case MYRT_SDF_TORUS: m = int(G[o + 2]); d = len2(len2(pos.x, pos.z) - G[o], pos.y) - G[o + 1]; break;
       case MYRT_SDF_CAPSULE: {
+        m = int(G[o + 2]);
         v3 q = pos;
         q.y -= gclamp(q.y, 0.f, G[o]);
         d = len3(q) - G[o + 1];
@@ -118,25 +176,37 @@ float map(int prog, v3 p, bool cells) {
       }
       case MYRT_SDF_UNION: case MYRT_SDF_SMOOTH_UNION: case MYRT_SDF_SUBTRACTION: case MYRT_SDF_INTERSECTION: {
         float const d1 = dist[sp - 1], d0 = dist[sp - 2];
+        int const m1 = mats[sp - 1], m0 = mats[sp - 2];
         sp -= 2;
+        float t;
         if (in.op == MYRT_SDF_SMOOTH_UNION) {
           float const kk = G[o];
           float const h = gclamp(0.5f + 0.5f * (d1 - d0) / kk, 0.f, 1.f);
+          t = 1.f - h;
           d = mixf(d1, d0, h) - kk * h * (1.f - h);
-        } else if (in.op == MYRT_SDF_UNION) {
-          d = gmin(d0, d1);
-        } else if (in.op == MYRT_SDF_SUBTRACTION) {
-          d = gmax(-d0, d1);
         } else {
-          d = gmax(d0, d1);
+          float const r = in.op == MYRT_SDF_UNION ? gmin(d0, d1)
+                                                  : (in.op == MYRT_SDF_SUBTRACTION ? gmax(-d0, d1) : gmax(d0, d1));
+          t = float(r == d1);
+          d = r;
         }
+        if (load) m = random_next(*rng) < t ? m1 : m0;
         break;
       }
       default: std::fprintf(stderr, "opcode %d not restated here\n", in.op); std::exit(2);
     }
-    dist[sp++] = d;
+    dist[sp] = d;
+    mats[sp] = m;
+    ++sp;
     pos = p;
   }
+  if (counting && fast) draw_gap(drawn, pr.count);
+  if (!redo) break;
+  ++redos;
+  *rng = saved;
+  redo = false;
+  }
+  if (mat) *mat = mats[sp - 1];
   return dist[sp - 1];
 }
 
@@ -186,6 +256,7 @@ int main(int argc, char** argv) {
   int const cells = std::atoi(argv[2]), n_rays = std::atoi(argv[3]);
   sdf_cell_tables(&v, cells, C);
   sdf_skip_tables(&v, skip_sphere, skip_next);
+  sdf_op_counts(&v, op_count);
   std::mt19937 rng(unsigned(std::atoi(argv[4])));
   std::uniform_real_distribution<float> U(-2.5f, 2.5f), J(-0.3f, 0.3f);
   for (int prog = 0; prog < int(P.size()); ++prog) {
@@ -218,8 +289,46 @@ int main(int argc, char** argv) {
         t += std::fabs(fa);
       }
     }
-    std::printf("%d %d %ld %ld %ld %ld %.1f %.1f\n", prog, grid, points, bad_points, hits, bad_marches,
-        double(full_instr) / n_rays, double(cell_instr) / n_rays);
+    // material loads: distance, material and the random state after the call,
+    // at points near the surfaces; then with a draw of exactly 1 planted at
+    // each of the first 64 draw positions in turn
+    long load_points = 0, bad_loads = 0, bad_forced = 0, redo_before = redos;
+    for (int r = 0; r < n_rays / 4; ++r) {
+      v3 o{U(rng), U(rng), U(rng)};
+      v3 d{-o.x + J(rng), -o.y + J(rng), -o.z + J(rng)};
+      float const len = len3(d);
+      float t = 1e-3f, fa = 1.f;
+      v3 q = o;
+      for (int s = 0; s < 64 && t < 6.f; ++s) {  // march to near a surface
+        q = {o.x + d.x * t / len, o.y + d.y * t / len, o.z + d.z * t / len};
+        fa = map(prog, q, false);
+        if (std::fabs(fa) < 1e-3f) break;
+        t += std::fabs(fa);
+      }
+      rng_t const start{uint32_t(rng()), int(rng() % 6)};
+      rng_t ra = start, rb = start;
+      int ma = -7, mb = -7;
+      float const la = map(prog, q, false, true, &ra, &ma), lb = map(prog, q, true, true, &rb, &mb);
+      ++load_points;
+      if (std::memcmp(&la, &lb, 4) != 0 || ma != mb || ra.state != rb.state || ra.prime != rb.prime) ++bad_loads;
+      if (r % 8 == 0) {
+        for (int j = 0; j < 64; ++j) {
+          rng_t one{0xffffffc0u, int(rng() % 6)};  // random_next returns exactly 1 for this state
+          rng_t s0 = one;
+          for (int i = 0; i < j + 1; ++i) s0 = random_prev(s0);  // j draws before it
+          rng_t fa2 = s0, fb2 = s0;
+          int m1 = -7, m2 = -7;
+          float const x1 = map(prog, q, false, true, &fa2, &m1), x2 = map(prog, q, true, true, &fb2, &m2);
+          if (std::memcmp(&x1, &x2, 4) != 0 || m1 != m2 || fa2.state != fb2.state || fa2.prime != fb2.prime)
+            ++bad_forced;
+        }
+      }
+    }
+    std::fprintf(stderr, "prog %d loads %ld bad %ld forced-one bad %ld redos %ld\n", prog, load_points, bad_loads,
+        bad_forced, redos - redo_before);
+    std::printf("%d %d %ld %ld %ld %ld %.1f %.1f %ld %ld %ld %ld\n", prog, grid, points, bad_points, hits, bad_marches,
+        double(full_instr) / n_rays, double(cell_instr) / n_rays, load_points, bad_loads, bad_forced,
+        redos - redo_before);
   }
   return 0;
 }

@@ -4,9 +4,11 @@ the device evaluator's float arithmetic (tests/sdf_cells_check.cpp). For left
 folds, balanced trees, right folds with unions, clusters of coincident
 spheres (where smooth unions lower the value the most) and mixed primitives,
 every march point evaluates bit for bit the same as the device runs it (cell
-segments and the per-point bounding-sphere test) as in full, and every march
-(with the escape sphere's early exit) returns the same hit and t. Programs
-outside the supported shape get no grid."""
+segments and the per-point bounding-sphere test) as in full, every march (with
+the escape sphere's early exit) returns the same hit and t, and every material
+load returns the same distance, material and random state, also when a
+left-out operator draws exactly 1 and the load falls back to the full
+program. Programs outside the supported shape get no grid."""
 import shutil
 import subprocess
 from pathlib import Path
@@ -92,8 +94,13 @@ def test_cell_segments_and_early_exit_are_exact(checker, tmp_path, cells):
     rows = [list(map(float, r.split())) for r in res if r.strip()]
     assert len(rows) == len(progs)
     for (name, _, expect_grid), r in zip(progs, rows):
-        _, grid, points, bad_points, hits, bad_marches, full_i, cell_i = r
+        _, grid, points, bad_points, hits, bad_marches, full_i, cell_i, loads, bad_loads, bad_forced, redos = r
         assert bad_points == 0 and bad_marches == 0, name
+        # material loads: distance, material and final random state; a draw of
+        # exactly 1 planted at each of the first 64 positions makes some calls
+        # fall back to the full evaluation
+        assert loads >= 100 and bad_loads == 0 and bad_forced == 0, name
+        assert redos > 0, name
         assert points > 3_000 and hits > 20, name
         assert (grid > 0) == expect_grid, name
         if expect_grid:
