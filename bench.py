@@ -63,6 +63,7 @@ def parse_args():
                         "per-frame post-processing chain (bloom, tonemap, FXAA) and denoise on 2048x2048; "
                         "forward: the raster preview renderer (1920x1080, 2048^2 shadow map)")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain leg of the closest workload")
+    p.add_argument("--no-c1", action="store_true", help="skip the height-field (32,768 tris, 1024^2 rays) sub-record")
     p.add_argument("--sdf-cells", type=int, default=0,
                    help="sdf: cells along the longest axis of the SDF chain's group-list grid (0 = the library's "
                         "default, 1 = no grid: every primitive runs at every march step)")
@@ -76,95 +77,111 @@ def parse_args():
 
 
 # ---------------------------------------------------------------- workload --
-def camera_rays_torch(res: int, spp: int, seed: int, device):
-    """Jittered pinhole rays of the icosphere scene's camera, float32 [res*res*spp, 8]."""
+RAY_SEED = 1000  # + rank
+
+
+def closest_config(triangles: int, res: int, spp: int, n_gpus: int) -> dict:
+    """The closest-hit workload's config; both arms print exactly this dict."""
+    cam = res * res * spp
+    return {"workload": WORKLOAD, "triangles": triangles, "res": res, "spp": spp, "camera_rays": cam,
+            "bounce_rays": "one per camera ray that hits: cosine-distributed about the face normal",
+            "ray_generation": "counter-based (SplitMix64 of the ray index, seed 1000 + rank): a sample of ray "
+                              "indices regenerates exactly the batch's rays",
+            "intersector": "reference (Moller-Trumbore)",
+            "l2": f"inputs larger than L2: the camera rays alone are {cam * (RAY_BYTES + HIT_BYTES) / 1e6:.0f} MB of "
+                  "rays + hits per step",
+            "parallelism": f"dp{n_gpus} (independent ray batches)"}
+
+
+def make_batch(ctx, tris9, res, spp, seed, device):
+    """The step's ray batch, built on the host and uploaded: res^2 * spp
+    jittered camera rays, traced once on the device to find their hits, then
+    the first diffuse bounce of every camera ray that hits (origin on the hit
+    triangle, direction from the camera ray's index)."""
     import torch
 
-    g = torch.Generator(device=device).manual_seed(seed)
-    eye = torch.tensor([0.0, 1.0, -4.5], dtype=torch.float64, device=device)
-    tgt = torch.tensor([0.0, -0.3, 0.0], dtype=torch.float64, device=device)
-    fwd = (tgt - eye) / torch.linalg.norm(tgt - eye)
-    right = torch.linalg.cross(fwd, torch.tensor([0.0, 1.0, 0.0], dtype=torch.float64, device=device))
-    right = right / torch.linalg.norm(right)
-    up = torch.linalg.cross(right, fwd)
-    tan_half = float(np.tan(np.radians(50.0) / 2))
-    n = res * res * spp
-    pix = torch.arange(res * res, device=device, dtype=torch.float64).repeat(spp)
-    px = (pix % res) + torch.rand(n, generator=g, device=device, dtype=torch.float64)
-    py = torch.div(pix, res, rounding_mode="floor") + torch.rand(n, generator=g, device=device, dtype=torch.float64)
-    sx = (2.0 * px / res - 1.0) * tan_half
-    sy = (1.0 - 2.0 * py / res) * tan_half
-    d = fwd[None] + sx[:, None] * right[None] + sy[:, None] * up[None]
-    d = d / torch.linalg.norm(d, dim=1, keepdim=True)
-    rays = torch.empty((n, 8), dtype=torch.float32, device=device)
-    rays[:, 0:3] = eye.float()
-    rays[:, 3] = 0.0
-    rays[:, 4:7] = d.float()
-    rays[:, 7] = float("inf")
-    return rays
+    from myrt_b200.scenes import diffuse_bounce_rays, jittered_camera_rays
 
-
-def world_triangles(scene) -> np.ndarray:
-    """World-space triangles [T, 9] in prim order (drawables in order)."""
-    idx = scene["indices"].astype(np.int64)
-    v = scene["vertices"].astype(np.float64)
-    out = []
-    for d in scene["drawables"]:
-        m = np.array(d.transformation[:], np.float64).reshape(4, 4).T
-        sel = idx[d.indices_base_index: d.indices_base_index + d.index_count] + d.points_base_index
-        p = v[sel] @ m[:3, :3].T + m[:3, 3]
-        out.append(p.reshape(-1, 9))
-    return np.concatenate(out).astype(np.float32)
-
-
-def bounce_rays_torch(rays, hits, tris9, seed: int):
-    """First diffuse bounce (cosine-weighted about the face normal) of each hit ray."""
-    import torch
-
-    hit = hits[:, 0].view(torch.int32)
-    ok = hit >= 0
-    r = rays[ok]
-    h = hits[ok]
-    prim = hit[ok].long()
-    tri = tris9[prim].view(-1, 3, 3)
-    n = torch.linalg.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0])
-    n = n / torch.linalg.norm(n, dim=1, keepdim=True).clamp_min(1e-30)
-    d = r[:, 4:7]
-    n = torch.where(((n * d).sum(1, keepdim=True) > 0), -n, n)
-    p = r[:, 0:3] + h[:, 1:2] * d
-    g = torch.Generator(device=rays.device).manual_seed(seed)
-    u1 = torch.rand(r.shape[0], generator=g, device=rays.device)
-    u2 = torch.rand(r.shape[0], generator=g, device=rays.device)
-    a = torch.where(n[:, 0:1].abs() > 0.9, torch.tensor([0.0, 1.0, 0.0], device=rays.device),
-                    torch.tensor([1.0, 0.0, 0.0], device=rays.device))
-    t = torch.linalg.cross(n, a)
-    t = t / torch.linalg.norm(t, dim=1, keepdim=True)
-    b = torch.linalg.cross(n, t)
-    rad = u1.sqrt()
-    phi = 2.0 * np.pi * u2
-    local = torch.stack([rad * phi.cos(), rad * phi.sin(), (1.0 - u1).clamp_min(0).sqrt()], 1)
-    wd = local[:, 0:1] * t + local[:, 1:2] * b + local[:, 2:3] * n
-    out = torch.empty((r.shape[0], 8), dtype=torch.float32, device=rays.device)
-    out[:, 0:3] = p + 1e-4 * n
-    out[:, 3] = 0.0
-    out[:, 4:7] = wd / torch.linalg.norm(wd, dim=1, keepdim=True)
-    out[:, 7] = float("inf")
-    return out
-
-
-def make_batch(ctx, scene, res, spp, seed, device):
-    import torch
-
-    prim_rays = camera_rays_torch(res, spp, seed, device)
-    hits = torch.empty((prim_rays.shape[0], 4), dtype=torch.float32, device=device)
+    ncam = res * res * spp
+    chunk = 1 << 22
+    cam = np.empty((ncam, 8), np.float32)
+    for a in range(0, ncam, chunk):
+        cam[a:a + chunk] = jittered_camera_rays(np.arange(a, min(ncam, a + chunk)), res, seed)
+    d_cam = torch.from_numpy(cam).to(device)
+    hits = torch.empty((ncam, 4), dtype=torch.float32, device=device)
     torch.cuda.synchronize()
-    ctx.trace_closest_device(prim_rays, hits, stream=ctx.stream)
+    ctx.trace_closest_device(d_cam, hits, stream=ctx.stream)
     ctx.sync()
-    tris9 = torch.from_numpy(world_triangles(scene)).to(device)
-    sec = bounce_rays_torch(prim_rays, hits, tris9, seed + 1)
+    h = hits.cpu().numpy()
     del hits
-    rays = torch.cat([prim_rays, sec], 0).contiguous()
-    return rays, int(prim_rays.shape[0]), int(sec.shape[0])
+    prim = h[:, 0].view(np.int32)
+    ok = np.nonzero(prim >= 0)[0]
+    bounce = np.empty((ok.size, 8), np.float32)
+    for a in range(0, ok.size, chunk):
+        sel = ok[a:a + chunk]
+        bounce[a:a + sel.size] = diffuse_bounce_rays(cam[sel], prim[sel], h[sel, 1], tris9, sel, seed)
+    rays = torch.cat([d_cam, torch.from_numpy(bounce).to(device)], 0).contiguous()
+    return rays, ncam, int(ok.size)
+
+
+class ReferenceSampler:
+    """The reference's CPU path on samples of the closest-hit workload: camera
+    ray indices drawn uniformly (with replacement) from the batch, those rays
+    regenerated exactly, traced, then the bounce of every hit traced too --
+    the batch's own mix of camera and bounce rays. Tracer: oracle/_ref (the
+    reference's bvh.cpp build + its bvh.impl.glsl / intersect.glsl traversal
+    compiled as C++) on all host threads, else the oracle's restatement."""
+
+    def __init__(self, scene: dict, res: int, spp: int, seed: int):
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import pyoracle as po
+
+        from myrt_b200.scenes import world_triangles
+
+        self.po = po
+        self.res, self.ncam, self.seed = res, res * res * spp, seed
+        self.tris9 = world_triangles(scene)
+        self.idx = np.arange(self.tris9.shape[0] * 3, dtype=np.uint32)
+        self.pts = self.tris9.reshape(-1, 3)
+        self.cores = po.nthreads()
+        self.kind = "reference" if po.ref_available() else "port"
+        t0 = time.perf_counter()
+        if self.kind == "reference":
+            h = po.ref_bvh(self.idx, self.pts, split=False)
+            self.nodes, self.bi = po.ref_bvh_arrays(h)
+            po.ref().ref_bvh_free(h)
+        else:
+            self.nodes, self.bi = po.refbvh_build(self.idx, self.pts)
+        self.build_s = time.perf_counter() - t0
+        self.rng = np.random.default_rng(seed + 17)
+
+    def trace(self, rays):
+        if self.kind == "reference":
+            return self.po.ref_glsl_traverse(self.nodes, self.bi, self.idx, self.pts, rays, threads=self.cores)
+        return self.po.refbvh_traverse(self.nodes, self.bi, self.idx, self.pts, rays, canonical=False)
+
+    def step(self, m: int):
+        """One sample of m camera rays + their bounces. Returns (rays traced,
+        seconds spent tracing)."""
+        from myrt_b200.scenes import diffuse_bounce_rays, jittered_camera_rays
+
+        sel = self.rng.integers(0, self.ncam, m)
+        cam = jittered_camera_rays(sel, self.res, self.seed)
+        t0 = time.perf_counter()
+        h = self.trace(cam)
+        dt = time.perf_counter() - t0
+        ok = h["prim"] >= 0
+        b = diffuse_bounce_rays(cam[ok], h["prim"][ok], h["t"][ok], self.tris9, sel[ok], self.seed)
+        t0 = time.perf_counter()
+        self.trace(b)
+        dt += time.perf_counter() - t0
+        return m + b.shape[0], dt
+
+    def describe(self, m: int) -> str:
+        return (f"{m} camera rays per step drawn uniformly (with replacement) from the batch's "
+                f"{self.ncam} by index, regenerated exactly, plus the bounce ray of each hit; reference BVH "
+                f"(bvh.cpp, dont_split, {self.build_s:.2f} s) over the world triangles + bvh.impl.glsl/"
+                f"intersect.glsl traversal compiled as C++, {self.cores} threads")
 
 
 # ---------------------------------------------------------------- helpers --
@@ -238,44 +255,15 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_reference_rate(scene, rays_np: np.ndarray, target_seconds: float = 10.0):
-    """The reference's CPU path on a bounded sample: oracle/_ref when built
-    (reference BVH build with dont_split + its GLSL traversal compiled as C++),
-    else the oracle's restatement. Returns (Mrays/s, cores, kind, sample)."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyoracle as po
-
-    tris9 = world_triangles(scene)
-    idx = np.arange(tris9.shape[0] * 3, dtype=np.uint32)
-    pts = tris9.reshape(-1, 3)
-    cores = po.nthreads()
-    if po.ref_available():
-        kind = "reference"
-        h = po.ref_bvh(idx, pts, split=False)
-        nodes, bi = po.ref_bvh_arrays(h)
-        po.ref().ref_bvh_free(h)
-
-        def run(r):
-            return po.ref_glsl_traverse(nodes, bi, idx, pts, r, threads=cores)
-    else:
-        kind = "port"
-        nodes, bi = po.refbvh_build(idx, pts)
-
-        def run(r):
-            return po.refbvh_traverse(nodes, bi, idx, pts, r, canonical=False)
-    rng = np.random.default_rng(0)
-    probe = rays_np[rng.choice(rays_np.shape[0], 32768, replace=False)]
-    t0 = time.perf_counter()
-    run(probe)
-    rate = probe.shape[0] / (time.perf_counter() - t0)
-    n = int(min(rays_np.shape[0], max(65536, rate * target_seconds)))
-    sample = rays_np[rng.choice(rays_np.shape[0], n, replace=False)]
-    t0 = time.perf_counter()
-    run(sample)
-    dt = time.perf_counter() - t0
-    desc = (f"{n} rays drawn uniformly from the step's batch; reference BVH (bvh.cpp, dont_split) over the baked "
-            f"world triangles + bvh.impl.glsl/intersect.glsl traversal, {cores} threads")
-    return n / dt / 1e6, cores, kind, desc, dt
+def cpu_reference_rate(sampler: "ReferenceSampler", target_seconds: float = 10.0):
+    """The reference's CPU path on a bounded sample of the closest-hit
+    workload (about target_seconds of tracing). Returns (Mrays/s, seconds,
+    sample description)."""
+    n, dt = sampler.step(1 << 15)
+    rate = n / dt
+    m = int(min(sampler.ncam, max(1 << 16, rate * target_seconds / 1.7)))
+    n, dt = sampler.step(m)
+    return n / dt / 1e6, dt, sampler.describe(m)
 
 
 # ---------------------------------------------------------------- guiding --
@@ -373,54 +361,160 @@ def guiding_run(device_index: int, res: int, oracle_spp: int, budget_spp: int, s
 
 # ------------------------------------------------------------------- arms --
 def run_reference_arm(args):
+    """The reference's CPU closest-hit path on the closest-hit workload: each
+    step a bounded sample of the batch (camera rays by index + their bounces),
+    on all host threads. Loads only the reference's own code (oracle/_ref) or,
+    where it is not built, the oracle's restatement; never the CUDA library."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    from myrt_b200.scenes import icosphere_camera_rays, icosphere_field
+    from myrt_b200 import _abi
+    from myrt_b200.scenes import icosphere_field
 
     scene = icosphere_field()
-    rays = icosphere_camera_rays(args.res, args.res, spp=1)
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import pyoracle as po
-
-    tris9 = world_triangles(scene)
-    idx = np.arange(tris9.shape[0] * 3, dtype=np.uint32)
-    pts = tris9.reshape(-1, 3)
-    cores = po.nthreads()
-    kind = "reference" if po.ref_available() else "port"
-    if kind == "reference":
-        h = po.ref_bvh(idx, pts, split=False)
-        nodes, bi = po.ref_bvh_arrays(h)
-        po.ref().ref_bvh_free(h)
-    else:
-        nodes, bi = po.refbvh_build(idx, pts)
-    per_step = 131072
-    rng = np.random.default_rng(1)
-
-    def step():
-        r = rays[rng.choice(rays.shape[0], per_step, replace=False)]
-        if kind == "reference":
-            po.ref_glsl_traverse(nodes, bi, idx, pts, r, threads=cores)
-        else:
-            po.refbvh_traverse(nodes, bi, idx, pts, r, canonical=False)
-
+    sampler = ReferenceSampler(scene, args.res, args.spp, RAY_SEED + rank)
+    m = 1 << 21
     for _ in range(args.warmup):
-        step()
-    t0 = time.perf_counter()
+        sampler.step(m)
+    total_rays, total_s = 0, 0.0
     for _ in range(args.steps):
-        step()
-    dt = time.perf_counter() - t0
-    value = per_step * args.steps / dt / 1e6
-    sample = (f"{per_step} camera rays per step drawn from the 512x512 view; reference BVH (bvh.cpp, dont_split) "
-              f"+ its GLSL traversal compiled as C++, {cores} threads")
+        n, dt = sampler.step(m)
+        total_rays += n
+        total_s += dt
+    assert _abi._lib is None, "the reference arm must not load the CUDA library"
+    value = total_rays / total_s / 1e6
+    triangles = int(sampler.tris9.shape[0])
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_s / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "triangles": int(tris9.shape[0]), "rays_per_step": per_step},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": closest_config(triangles, args.res, args.spp, args.gpus),
+            "rays_per_step": total_rays / args.steps,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": sampler.cores, "kind": sampler.kind,
+                             "sample": sampler.describe(m)},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "timing": "host wall clock of the tracing calls only (ray generation and bounce set-up excluded)"}
     print(json.dumps(line), flush=True)
     return 0
+
+
+C1_WORKLOAD = ("height field 128x128 cells on [-1,1]^2 in xz (32,768 tris, y ~ U[0,0.1], seed 1); 1024x1024 pinhole "
+               "rays through pixel centres from (0,2,-3) at the origin, 60 deg vfov, 1 ray per pixel")
+
+
+def c1_run(local: int, args) -> dict:
+    """Config 1, the closest-hit configuration the metric is quoted on: the
+    128 x 128 height field and 1,048,576 pinhole rays. The rays and hits fit in
+    L2, so L2 is flushed (a 256 MB write) before every timed launch and each
+    launch is timed alone with CUDA events on the context's stream. Both
+    visiting orders are tried in warm-up and the faster is kept (results never
+    depend on it). CPU baseline: the reference's own build with spatial splits
+    (bvh.cpp, split_aabbs) and its GLSL traversal, on all host threads."""
+    import torch
+
+    import myrt_b200 as mb
+    from myrt_b200.scenes import heightfield, pinhole_rays
+
+    idx, pts = heightfield(128, amp=0.1, seed=1)
+    rays_np = pinhole_rays(1024, 1024)
+    n = rays_np.shape[0]
+    ctx = mb.Context(local)
+    info = ctx.upload_scene(idx, pts)
+    device = torch.device("cuda", local)
+    rays = torch.from_numpy(rays_np).to(device)
+    hits = torch.empty((n, 4), dtype=torch.float32, device=device)
+    s = ctx.stream
+    stream = torch.cuda.ExternalStream(s, device=device)
+    cn = torch.empty(n, dtype=torch.int32, device=device)
+    ct = torch.empty(n, dtype=torch.int32, device=device)
+    torch.cuda.synchronize()
+    ctx.trace_closest_stats_device(rays, hits, cn, ct, stream=s)
+    ctx.sync()
+    nodes_total, tris_total = int(cn.sum(dtype=torch.int64)), int(ct.sum(dtype=torch.int64))
+    del cn, ct
+    alg_bytes = NODE_BYTES * nodes_total + TRI_BYTES * tris_total + (RAY_BYTES + HIT_BYTES) * n
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=device)  # 256 MB, twice L2
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(order: int, steps: int):
+        ctx.set_tuning(trace_order=order)
+        total = 0.0
+        for k in range(steps):
+            flush.fill_(float(k))
+            torch.cuda.synchronize()
+            e0.record(stream)
+            ctx.trace_closest_device(rays, hits, stream=s)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total += e0.elapsed_time(e1)
+        return total
+
+    orders = {o: timed(o, max(3, args.warmup)) for o in (1, 2)}
+    order = min(orders, key=orders.get)
+    ctx.set_phase_timing(True)
+    ctx.phase_times()
+    with ClockSampler(local) as clocks:
+        ms = timed(order, args.steps)
+    phases = ctx.phase_times()
+    ctx.set_phase_timing(False)
+    ms_per_step = ms / args.steps
+    trace_ms = phases["traverse_ms"] / max(1, phases["queries"])
+    # end to end through the host-buffer entry point (pinned buffers)
+    h_rays = torch.from_numpy(rays_np).pin_memory()
+    h_hits = torch.empty((n, 4), dtype=torch.float32, pin_memory=True)
+    hr, hh = h_rays.numpy(), h_hits.numpy().view(mb.HIT_DTYPE).reshape(-1)
+    ctx.trace_closest(hr, out=hh)
+    e2e_steps = max(3, min(args.steps, 20))
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.trace_closest(hr, out=hh)
+    e2e_s = time.perf_counter() - t0
+    ctx.set_tuning()
+    ctx.close()
+    peaks, peak_kind = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    achieved = alg_bytes / (trace_ms / 1e3) / 1e9
+    out = {"metric": METRIC, "value": n / (ms_per_step / 1e3) / 1e6, "unit": UNIT, "steps": args.steps,
+           "ms_per_step": ms_per_step,
+           "config": {"workload": C1_WORKLOAD, "triangles": int(info["triangles"]), "rays_per_step": n,
+                      "l2": "rays + hits (48 MB) fit in L2: a 256 MB buffer is written before every timed launch",
+                      "visiting_order": {1: "input order", 2: "sorted by origin and direction cell"}[order],
+                      "order_trial_ms": {"input": orders[1], "sorted": orders[2]}},
+           "bvh": {"wide_nodes": int(info["wide_nodes"]), "wide_depth": int(info["wide_depth"]),
+                   "build_s": round(float(info["build_seconds"]), 4)},
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                        "peak_source": f"hbm_gbs of {peak_kind}", "traffic": None,
+                        "bytes_per_ray": alg_bytes / n, "nodes_per_ray": nodes_total / n,
+                        "tris_per_ray": tris_total / n, "kernel": "k_trace (closest hit, reference intersector)",
+                        "kernel_ms": trace_ms, "frac_whole_step": alg_bytes / (ms_per_step / 1e3) / 1e9 / hbm,
+                        "note": "algorithmic bytes = 80 B/node + 48 B/triangle + 48 B ray+hit over k_trace's "
+                                "CUDA-event duration; the 2 MB tree is L2-resident"},
+           "e2e": {"value": n * e2e_steps / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": n * RAY_BYTES,
+                   "d2h_bytes_per_step": n * HIT_BYTES, "steps": e2e_steps,
+                   "api": "myrt_trace_closest (host pinned buffers)"},
+           "clocks": clocks.summary(),
+           "gpu_launches": args.steps * (1 if order == 1 else 2)}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import pyoracle as po
+
+        if po.ref_available():
+            t0 = time.perf_counter()
+            h = po.ref_bvh(idx, pts, split=True)
+            build_s = time.perf_counter() - t0
+            nodes, bi = po.ref_bvh_arrays(h)
+            po.ref().ref_bvh_free(h)
+            times = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                po.ref_glsl_traverse(nodes, bi, idx, pts, rays_np, threads=po.nthreads())
+                times.append(time.perf_counter() - t0)
+            out["cpu_baseline"] = {
+                "value": n / statistics.median(times) / 1e6, "unit": UNIT, "cores": po.nthreads(),
+                "kind": "reference",
+                "sample": f"all {n} rays, median of 3; the reference's own tree with spatial splits (bvh.cpp, "
+                          f"split_aabbs, {nodes.shape[0]} nodes, {bi.size} indices, built in {build_s:.2f} s) "
+                          f"and its bvh.impl.glsl/intersect.glsl traversal compiled as C++"}
+    return out
 
 
 def run_ours(args):
@@ -439,12 +533,13 @@ def run_ours(args):
     device = torch.device("cuda", local)
 
     import myrt_b200 as mb
-    from myrt_b200.scenes import icosphere_field
+    from myrt_b200.scenes import icosphere_field, world_triangles
 
     scene = icosphere_field()
+    tris9 = world_triangles(scene)
     ctx = mb.Context(local)
     info = ctx.upload_scene(**scene)
-    rays, n_primary, n_secondary = make_batch(ctx, scene, args.res, args.spp, seed=1000 + rank, device=device)
+    rays, n_primary, n_secondary = make_batch(ctx, tris9, args.res, args.spp, seed=RAY_SEED + rank, device=device)
     n = rays.shape[0]
     hits = torch.empty((n, 4), dtype=torch.float32, device=device)
     # all launches and events go to the context's own (non-blocking) stream
@@ -523,14 +618,11 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "triangles": int(info["triangles"]), "rays_per_step": n,
-                   "camera_rays": n_primary, "bounce_rays": n_secondary, "res": args.res, "spp": args.spp,
-                   "intersector": "reference (Moller-Trumbore, bit-exact)",
-                   "l2": f"inputs larger than L2: {n * (RAY_BYTES + HIT_BYTES) / 1e6:.0f} MB of rays+hits per step",
-                   "bvh": {"wide_nodes": int(info["wide_nodes"]), "wide_depth": int(info["wide_depth"]),
-                           "node_bytes": int(info["node_bytes"]), "triangle_bytes": int(info["triangle_bytes"]),
-                           "build_s": round(float(info["build_seconds"]), 3)},
-                   "parallelism": f"dp{world} (independent ray batches)"},
+        "config": closest_config(int(info["triangles"]), args.res, args.spp, world),
+        "rays_per_step": n, "camera_rays": n_primary, "bounce_rays": n_secondary,
+        "bvh": {"wide_nodes": int(info["wide_nodes"]), "wide_depth": int(info["wide_depth"]),
+                "node_bytes": int(info["node_bytes"]), "triangle_bytes": int(info["triangle_bytes"]),
+                "build_s": round(float(info["build_seconds"]), 3)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": f"hbm_gbs of {peak_kind}", "traffic": traffic,
                      "traffic_source": "ncu dram__bytes_read+write per ray of a 3.49M-ray capture, scaled by rays",
@@ -576,9 +668,13 @@ def run_ours(args):
                 "SAH builder; build_s = device build time of the 655,872 world triangles"}
     ctx.upload_scene(**scene)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, cores, kind, sample, dt = cpu_reference_rate(scene, rays_np)
-        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
-                                "seconds": round(dt, 2)}
+        sampler = ReferenceSampler(scene, args.res, args.spp, RAY_SEED + rank)
+        v, dt, sample = cpu_reference_rate(sampler)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": sampler.cores, "kind": sampler.kind,
+                                "sample": sample, "seconds": round(dt, 2)}
+    if rank == 0 and world == 1 and not args.no_c1:
+        del h_rays, h_hits, rays_np, hits_np
+        line["c1"] = c1_run(local, args)
     if rank == 0 and world == 1 and not args.no_guiding:
         del rays, hits
         torch.cuda.empty_cache()

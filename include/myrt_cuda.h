@@ -164,6 +164,13 @@ typedef struct myrt_tuning {
                                 capsules (0 = 32, 1 = no grid and no early exit, 2..128; programs
                                 with thousands of primitives get coarser grids so that the upload
                                 stays near a second). Results never depend on it. */
+  uint32_t guide_poll_limit; /* guide tensor-core kernels: polls of each CTA's first mbarrier wait
+                                (0 = 2^22, the bound of every other wait); a wait that runs out sets
+                                the device error word (myrt_sync: MYRT_ERR_DEVICE_ABORT) after the
+                                MMA in flight has retired and TMEM is freed */
+  uint32_t guide_stall_test; /* 1: that first wait watches a barrier nothing arrives at, so it runs
+                                out after guide_poll_limit polls: tests the timeout path without a
+                                fault. 0 in normal use */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */
@@ -546,12 +553,18 @@ int myrt_set_seed(myrt_ctx* ctx, uint32_t seed);
  * count in a; read as well as written when sample_index > 0) and display_rgba,
  * width * height * 4 floats each. The caller tracks sample_index (0 starts a new
  * accumulation); the context's own images and sample counter are not touched.
- * Limits: width * height <= 65536 and frames * (2 * num_bounces + 3) <= 256,
- * else MYRT_ERR_INVALID_ARGUMENT. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture. All calls share the array: calls that overlap on the GPU
- * (other streams, other threads) race and must be serialised by the caller.
- * Asynchronous on `stream` (NULL = the ctx stream). */
+ * Depth of field, the bokeh mask, albedo textures and the cube map apply as in
+ * myrt_render; only MYRT_SHADE_REFERENCE is supported (else
+ * MYRT_ERR_UNSUPPORTED). Limits: width * height <= 65536 and
+ * frames * (2 * num_bounces + 3) <= 256, else MYRT_ERR_INVALID_ARGUMENT. The
+ * first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. All
+ * calls share the array: calls that overlap on the GPU (other streams, other
+ * threads) race and must be serialised by the caller. The call makes the
+ * context's device current while it runs and then restores the caller's.
+ * Asynchronous on `stream` (NULL = the ctx stream); a caller stream first waits
+ * for the work already queued on the context's stream (scene and transform
+ * updates). */
 int myrt_render_noalloc(myrt_ctx* ctx, const myrt_camera* camera, const myrt_render_params* params,
     uint32_t sample_index, float* accum_rgba, float* display_rgba, void* stream);
 

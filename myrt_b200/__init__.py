@@ -1,8 +1,11 @@
 """myrt_b200: B200-native wavefront path-tracing core behind myrt's interfaces.
 
 Python front end over the C ABI (include/myrt_cuda.h). The compute path is the
-in-tree CUDA library libmyrt_b200.so; importing this package without it
-raises (there is no CPU fallback).
+in-tree CUDA library libmyrt_b200.so. It is loaded on first use (a Context,
+a host BVH build, ...), not at import, so the pure-numpy scene generators in
+``myrt_b200.scenes`` can be used by processes that must not map it; every
+call that needs it raises when it has not been built (there is no CPU
+fallback).
 """
 from __future__ import annotations
 
@@ -12,8 +15,6 @@ import numpy as np
 
 from . import _abi
 from ._abi import ISECT_REFERENCE, ISECT_WATERTIGHT, MYRT_ERR_DEVICE_ABORT, MYRT_OK  # noqa: F401
-
-_abi.lib()  # fail loudly at import if the native library is absent
 
 HIT_DTYPE = np.dtype([("prim", np.int32), ("t", np.float32), ("u", np.float32), ("v", np.float32)])
 
@@ -106,9 +107,10 @@ class Context:
     def set_tuning(self, trace_persistent: int = 0, refill: int = 1, blocks_per_sm: int = 0,
                    trace_min_blocks: int = 0, trace_unit_steps: int = 0, wave_paths: int = 0,
                    pt_blocks_per_sm: int = 0, trace_smem_stack: int = 0, trace_order: int = 0,
-                   bvh_builder: int = 0, sdf_cells: int = 0):
+                   bvh_builder: int = 0, sdf_cells: int = 0, guide_poll_limit: int = 0, guide_stall_test: int = 0):
         t = _abi.myrt_tuning(trace_persistent, refill, blocks_per_sm, trace_min_blocks, trace_unit_steps,
-                             wave_paths, pt_blocks_per_sm, trace_smem_stack, bvh_builder, trace_order, sdf_cells)
+                             wave_paths, pt_blocks_per_sm, trace_smem_stack, bvh_builder, trace_order, sdf_cells,
+                             guide_poll_limit, guide_stall_test)
         self._check(self._L.myrt_set_tuning(self._h, C.byref(t)), "myrt_set_tuning")
 
     def set_transforms(self, drawables):
@@ -443,14 +445,20 @@ class Context:
     def render_noalloc(self, inverse_view, inverse_projection, width: int, height: int, accum, display,
                        sample_index: int = 0, num_bounces: int = 10, frames: int = 1,
                        shading: int = _abi.SHADE_REFERENCE, stream: int | None = None,
-                       sdf_marching_steps: int = 400, sdf_marching_epsilon: float = 1e-5):
+                       sdf_marching_steps: int = 400, sdf_marching_epsilon: float = 1e-5, dof: bool = False,
+                       lens_size=(0.2, 0.2), focus: float = 1.0, bokeh_slot: int = -1):
         """myrt_render_noalloc: renders into caller-owned device images (torch
-        tensors, float32 [H, W, 4]) with no device allocation by the library."""
+        tensors, float32 [H, W, 4]) with no device allocation by the library.
+        Camera and shading options as render()."""
         cam = _abi.myrt_camera()
         cam.inverse_view[:] = np.asarray(inverse_view, np.float32).ravel().tolist()
         cam.inverse_projection[:] = np.asarray(inverse_projection, np.float32).ravel().tolist()
         p = _abi.myrt_render_params(width, height, num_bounces, frames, shading, 0, sdf_marching_steps,
                                     sdf_marching_epsilon)
+        p.dof_active = int(dof)
+        p.lens_size[:] = [float(lens_size[0]), float(lens_size[1])]
+        p.focus = float(focus)
+        p.bokeh_texture = bokeh_slot + 1 if bokeh_slot >= 0 else 0
         self._check(self._L.myrt_render_noalloc(self._h, C.byref(cam), C.byref(p), sample_index, _ptr(accum),
                                                 _ptr(display), stream), "myrt_render_noalloc")
 

@@ -396,6 +396,7 @@ int myrt_ctx_create(myrt_device_opts const* opts, myrt_ctx** out) {
   int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
   if (!rc) rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
   if (!rc) rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking), "stream");
+  if (!rc) rc = check_cuda(ctx, cudaEventCreateWithFlags(&ctx->order_event, cudaEventDisableTiming), "event");
   if (!rc) rc = check_cuda(ctx, cudaMalloc(&ctx->d_err, sizeof(uint32_t)), "error word");
   if (!rc) rc = check_cuda(ctx, cudaMemset(ctx->d_err, 0, sizeof(uint32_t)), "error word");
   if (!rc) rc = check_cuda(ctx, cudaMalloc(&ctx->d_next, kCounterRing * sizeof(uint32_t)), "ray counters");
@@ -445,6 +446,7 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   cudaFree(ctx->d_next);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
+  if (ctx->order_event) cudaEventDestroy(ctx->order_event);
   delete ctx;
   return MYRT_OK;
 }
@@ -459,7 +461,8 @@ int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
   if (!ctx || !t) return MYRT_ERR_INVALID_ARGUMENT;
   if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
       t->trace_unit_steps > 1 || (t->wave_paths != 0 && (t->wave_paths < 1024 || t->wave_paths > (1u << 28))) ||
-      t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2 || t->bvh_builder > 1 || t->sdf_cells > 128)
+      t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2 || t->bvh_builder > 1 || t->sdf_cells > 128 ||
+      t->guide_stall_test > 1)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;
@@ -953,7 +956,8 @@ int myrt_render_noalloc(myrt_ctx* ctx, myrt_camera const* camera, myrt_render_pa
   if (p->width == 0 || p->height == 0) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "empty image");
   if (p->num_bounces < 0 || p->num_bounces > 1024)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "num_bounces must be in [0, 1024]");
-  if (p->shading != MYRT_SHADE_REFERENCE) return set_error(ctx, MYRT_ERR_UNSUPPORTED, "unknown shading mode");
+  if (p->shading != MYRT_SHADE_REFERENCE)
+    return set_error(ctx, MYRT_ERR_UNSUPPORTED, "myrt_render_noalloc: only MYRT_SHADE_REFERENCE is supported");
   if (p->frames == 0) return MYRT_OK;
   return render_reference_frames_noalloc(ctx, camera, p, sample_index, reinterpret_cast<float4*>(accum_rgba),
       reinterpret_cast<float4*>(display_rgba), stream ? static_cast<cudaStream_t>(stream) : ctx->stream);

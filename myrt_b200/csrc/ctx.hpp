@@ -120,6 +120,7 @@ struct myrt_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t aux_stream = nullptr;  // second lane for copy/compute overlap
+  cudaEvent_t order_event = nullptr;  // orders a caller's stream after the context's stream
   std::string last_error;
   uint32_t* d_err = nullptr;          // device error word (atomicOr of ERR_* bits)
   myrt_b200::device_scene scene;
@@ -130,7 +131,7 @@ struct myrt_ctx {
   myrt_b200::guide_state* guide = nullptr;  // learned proposal (guide.cu), created on first use
   uint64_t guide_generation = 0;            // bumped by scene uploads
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
-  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
   int sm_count = 0;
   uint32_t* d_next = nullptr;    // ring of ray counters for the persistent traversal
   uint32_t next_slot = 0;

@@ -84,6 +84,9 @@ struct mlp_args {
   float const* bias;   // [4][64]
   float center[3], inv_half[3];
   uint32_t* err;
+  uint32_t poll_limit;  // polls of each CTA's first tensor-core wait (the others use kPollLimit)
+  uint32_t stall;       // 1: that first wait watches a barrier nothing arrives at, so it runs out
+                        // (exercises the timeout path; the MMA in flight is still drained)
 };
 
 // ---- encoding ------------------------------------------------------------------------
@@ -223,9 +226,9 @@ __global__ void __launch_bounds__(256) k_guide_gather(float4 const* __restrict__
 
 // ---- k_guide_forward --------------------------------------------------------------------
 // Shared memory (from a 1024-aligned base): W tiles 4 x 8 KB, H tile 16 KB,
-// biases 1 KB, mbarrier, TMEM address.
-constexpr uint32_t kFwdW = 0, kFwdH = 32768, kFwdBias = 49152, kFwdBar = 50176, kFwdTmem = 50184;
-constexpr uint32_t kFwdSmem = 50192 + 1024;
+// biases 1 KB, mbarrier, TMEM address, the stall-test mbarrier.
+constexpr uint32_t kFwdW = 0, kFwdH = 32768, kFwdBias = 49152, kFwdBar = 50176, kFwdTmem = 50184, kFwdStall = 50192;
+constexpr uint32_t kFwdSmem = 50200 + 1024;
 
 __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
   uint32_t const s = tc::smem_u32(p);
@@ -240,13 +243,17 @@ __global__ void __launch_bounds__(128) k_guide_forward(mlp_args a, float4 const*
   uint8_t* ht = sm + kFwdH;
   float* bias = reinterpret_cast<float*>(sm + kFwdBias);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFwdBar);
+  uint64_t* stall_bar = reinterpret_cast<uint64_t*>(sm + kFwdStall);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kFwdTmem);
   uint32_t const tid = threadIdx.x, warp = tid >> 5;
   if (warp == 0) {
     tc::tmem_alloc(tmem_slot, 64);
     tc::tmem_relinquish();
   }
-  if (tid == 0) tc::mbar_init(bar, 1);
+  if (tid == 0) {
+    tc::mbar_init(bar, 1);
+    tc::mbar_init(stall_bar, 1);
+  }
   load_weights(a, wt, bias);
   tc::fence_proxy_async();
   tc::fence_before_sync();
@@ -256,6 +263,7 @@ __global__ void __launch_bounds__(128) k_guide_forward(mlp_args a, float4 const*
   uint32_t const n = count_ptr ? *count_ptr : n_fixed;
   uint32_t phase = 0;
   bool failed = false;
+  bool first_wait = true;
   constexpr uint32_t kIdF = tc::idesc_bf16_m128_n64(false, false);
   for (uint32_t tile = blockIdx.x; tile * 128u < n && !failed; tile += gridDim.x) {
     uint32_t const row = tile * 128u + tid;
@@ -282,7 +290,9 @@ __global__ void __launch_bounds__(128) k_guide_forward(mlp_args a, float4 const*
               k > 0 ? 1u : 0u);
         tc::mma_commit(bar);
       }
-      bool const ok = tc::mbar_wait_bounded(bar, phase, kPollLimit);
+      bool const ok = tc::mbar_wait_bounded(first_wait && a.stall ? stall_bar : bar, phase,
+          first_wait ? a.poll_limit : kPollLimit);
+      first_wait = false;
       phase ^= 1u;
       if (__syncthreads_or(!ok)) {
         failed = true;
@@ -372,10 +382,10 @@ __global__ void __launch_bounds__(256) k_guide_collect(float4 const* __restrict_
 
 // ---- k_guide_train -----------------------------------------------------------------------------
 // Shared memory: W 4 x 8 KB | H0..H3 4 x 16 KB | dZ 16 KB | zero 16 KB | bias 1 KB |
-// dbias 1 KB | per-row (wi, weight) 2 KB | mbarrier | TMEM address.
+// dbias 1 KB | per-row (wi, weight) 2 KB | mbarrier | TMEM address | stall-test mbarrier.
 constexpr uint32_t kTrW = 0, kTrH = 32768, kTrDZ = 98304, kTrZero = 114688, kTrBias = 131072, kTrDBias = 132096,
-                   kTrRow = 133120, kTrBar = 135168, kTrTmem = 135176;
-constexpr uint32_t kTrSmem = 135184 + 1024;
+                   kTrRow = 133120, kTrBar = 135168, kTrTmem = 135176, kTrStall = 135184;
+constexpr uint32_t kTrSmem = 135192 + 1024;
 constexpr uint32_t kTmemCols = 512;  // accumulator (64) + dW for 4 layers (4 x 64)
 
 struct train_args {
@@ -412,6 +422,7 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(train_args a) {
   float* dbias = reinterpret_cast<float*>(sm + kTrDBias);
   float4* rowd = reinterpret_cast<float4*>(sm + kTrRow);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kTrBar);
+  uint64_t* stall_bar = reinterpret_cast<uint64_t*>(sm + kTrStall);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kTrTmem);
   uint32_t const tid = threadIdx.x, warp = tid >> 5;
   auto H = [&](int l) { return sm + kTrH + uint32_t(l) * 16384u; };
@@ -420,7 +431,10 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(train_args a) {
     tc::tmem_alloc(tmem_slot, kTmemCols);
     tc::tmem_relinquish();
   }
-  if (tid == 0) tc::mbar_init(bar, 1);
+  if (tid == 0) {
+    tc::mbar_init(bar, 1);
+    tc::mbar_init(stall_bar, 1);
+  }
   load_weights(a.m, wt, bias);
   for (uint32_t i = tid; i < 16384 / 16; i += blockDim.x) reinterpret_cast<uint4*>(zt)[i] = make_uint4(0, 0, 0, 0);
   for (uint32_t i = tid; i < kLayers * 64; i += blockDim.x) dbias[i] = 0.f;
@@ -446,6 +460,7 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(train_args a) {
   constexpr uint32_t kIdDW = tc::idesc_bf16_m128_n64(true, true);
   uint32_t phase = 0;
   bool failed = false;
+  bool first_wait = true;
   uint32_t tiles_done = 0;
   float loss_acc = 0.f;
 
@@ -455,7 +470,9 @@ __global__ void __launch_bounds__(128, 1) k_guide_train(train_args a) {
     __syncthreads();
   };
   auto wait_mma = [&]() -> bool {
-    bool const ok = tc::mbar_wait_bounded(bar, phase, kPollLimit);
+    bool const ok = tc::mbar_wait_bounded(first_wait && a.m.stall ? stall_bar : bar, phase,
+        first_wait ? a.m.poll_limit : kPollLimit);
+    first_wait = false;
     phase ^= 1u;
     bool const bad = __syncthreads_or(!ok);
     tc::fence_after_sync();
@@ -749,6 +766,8 @@ mlp_args make_mlp(myrt_ctx* ctx) {
     a.inv_half[k] = h > 0.f ? 1.f / h : 1.f;
   }
   a.err = ctx->d_err;
+  a.poll_limit = ctx->tuning.guide_poll_limit ? ctx->tuning.guide_poll_limit : kPollLimit;
+  a.stall = ctx->tuning.guide_stall_test ? 1u : 0u;
   return a;
 }
 

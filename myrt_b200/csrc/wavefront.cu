@@ -544,12 +544,46 @@ void draw_host_randomness(std::mt19937& rng, int frames, int bounces, std::vecto
   }
 }
 
+// Launch arguments of one reference-shading call: the camera (with depth of
+// field and the bokeh mask), the scene and the colour pass (textures, cube
+// map), shared by myrt_render and myrt_render_noalloc so both run the same
+// frames.
+struct frame_setup {
+  camera_dev cd;
+  scene_dev sd;
+  color_args ca;
+};
+
+frame_setup make_frame_setup(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p, float4* accum,
+    float4* display, uint32_t sample_index) {
+  device_scene const& S = ctx->scene;
+  camera_dev cd{};
+  mat_mul4(cam->inverse_view, cam->inverse_projection, cd.vp);
+  cd.eye[0] = cam->inverse_view[12];
+  cd.eye[1] = cam->inverse_view[13];
+  cd.eye[2] = cam->inverse_view[14];
+  cd.dof = p->dof_active ? 1 : 0;
+  cd.lens[0] = p->lens_size[0];
+  cd.lens[1] = p->lens_size[1];
+  cd.focus = p->focus;
+  if (p->bokeh_texture > 0 && size_t(p->bokeh_texture) <= ctx->textures.size()) {
+    auto const& t = ctx->textures[size_t(p->bokeh_texture) - 1];
+    cd.bokeh = rs::tex2d{t.data, t.w, t.h, t.wrap};
+  }
+  scene_dev sd{S.nodes, S.tris, S.tri_normals, S.tri_uvs, S.tri_material,
+      reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err,
+      make_sdf_dev(ctx, p->sdf_marching_steps, p->sdf_marching_epsilon)};
+  color_args ca{reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, accum, display,
+      p->width, sample_index, 0, reinterpret_cast<rs::tex2d const*>(ctx->d_textures), int(ctx->textures.size()),
+      rs::cubemap_dev{ctx->cubemap, ctx->cubemap_size}};
+  return frame_setup{cd, sd, ca};
+}
+
 int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p) {
   uint32_t const W = p->width, H = p->height;
   int rc = ensure_render_buffers(ctx, W, H);
   if (rc) return rc;
   render_state& R = ctx->render;
-  device_scene const& S = ctx->scene;
   int const B = p->num_bounces;
   int const F = int(p->frames);
   int const passes = 2 * B + 3;
@@ -569,25 +603,10 @@ int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_p
       "pass randomness upload");
   if (rc) return rc;
 
-  camera_dev cd{};
-  mat_mul4(cam->inverse_view, cam->inverse_projection, cd.vp);
-  cd.eye[0] = cam->inverse_view[12];
-  cd.eye[1] = cam->inverse_view[13];
-  cd.eye[2] = cam->inverse_view[14];
-  cd.dof = p->dof_active ? 1 : 0;
-  cd.lens[0] = p->lens_size[0];
-  cd.lens[1] = p->lens_size[1];
-  cd.focus = p->focus;
-  if (p->bokeh_texture > 0 && size_t(p->bokeh_texture) <= ctx->textures.size()) {
-    auto const& t = ctx->textures[size_t(p->bokeh_texture) - 1];
-    cd.bokeh = rs::tex2d{t.data, t.w, t.h, t.wrap};
-  }
-  scene_dev sd{S.nodes, S.tris, S.tri_normals, S.tri_uvs, S.tri_material,
-      reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err,
-      make_sdf_dev(ctx, p->sdf_marching_steps, p->sdf_marching_epsilon)};
-  color_args ca{reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, R.accum, R.display, W,
-      0, 0, reinterpret_cast<rs::tex2d const*>(ctx->d_textures), int(ctx->textures.size()),
-      rs::cubemap_dev{ctx->cubemap, ctx->cubemap_size}};
+  frame_setup const fs = make_frame_setup(ctx, cam, p, R.accum, R.display, R.sample_counter);
+  camera_dev const& cd = fs.cd;
+  scene_dev const& sd = fs.sd;
+  color_args ca = fs.ca;
   size_t const n = size_t(W) * H;
   uint32_t const nb = uint32_t((n + kBlock - 1) / kBlock);
   cudaStream_t const st = ctx->stream;
@@ -642,24 +661,31 @@ constexpr size_t kNaBytes = 2 * kNaGen + kNaTrace + kNaCounts + kNaSums + kNaTex
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
 namespace {
-// Device address of g_noalloc_scratch, resolved once per device with that device
-// current (in host code the symbol is only a host-side stand-in).
+// Device address of g_noalloc_scratch on the context's device, resolved once per
+// device with that device current (in host code the symbol is only a host-side
+// stand-in). The caller has made ctx->device current.
 int noalloc_scratch(myrt_ctx* ctx, unsigned char** out) {
   static std::mutex m;
   static void* addr[64] = {};
   if (ctx->device < 0 || ctx->device >= 64) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "device ordinal >= 64");
   std::lock_guard<std::mutex> lock(m);
   if (!addr[ctx->device]) {
-    int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
-    if (rc) return rc;
     void* p = nullptr;
-    rc = check_cuda(ctx, cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)");
+    int rc = check_cuda(ctx, cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)");
     if (rc) return rc;
     addr[ctx->device] = p;
   }
   *out = static_cast<unsigned char*>(addr[ctx->device]);
   return MYRT_OK;
 }
+
+// Restores the calling thread's current device when a call returns.
+struct device_guard {
+  int prev = -1;
+  ~device_guard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
 }  // namespace
 
 int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p,
@@ -673,8 +699,12 @@ int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_
   if (size_t(F) * size_t(passes) > kNoAllocMaxPasses)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT,
         "myrt_render_noalloc: frames * (2 * num_bounces + 3) exceeds 256 passes");
+  device_guard guard;
+  int rc = check_cuda(ctx, cudaGetDevice(&guard.prev), "cudaGetDevice");
+  if (!rc && guard.prev != ctx->device) rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+  if (rc) return rc;
   unsigned char* base = nullptr;
-  int rc = noalloc_scratch(ctx, &base);
+  rc = noalloc_scratch(ctx, &base);
   if (rc) return rc;
   float4* gen[2] = {reinterpret_cast<float4*>(base), reinterpret_cast<float4*>(base + kNaGen)};
   float4* trace = reinterpret_cast<float4*>(base + 2 * kNaGen);
@@ -682,37 +712,46 @@ int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_
   uint32_t* sums = reinterpret_cast<uint32_t*>(base + 2 * kNaGen + kNaTrace + kNaCounts);
   float* ptex = reinterpret_cast<float*>(base + 2 * kNaGen + kNaTrace + kNaCounts + kNaSums);
 
-  // Host randomness in draw_host_randomness's order, one pass at a time through
-  // a stack buffer (no heap, no device allocation).
+  // Work the context queued on its own stream (scene or transform updates, the
+  // error word's reset) comes first when the caller passes another stream.
+  if (st != ctx->stream) {
+    rc = check_cuda(ctx, cudaEventRecord(ctx->order_event, ctx->stream), "cudaEventRecord");
+    if (!rc) rc = check_cuda(ctx, cudaStreamWaitEvent(st, ctx->order_event, 0), "cudaStreamWaitEvent");
+    if (rc) return rc;
+  }
+
+  // Host randomness in draw_host_randomness's order, staged through a stack
+  // buffer of kNaTexChunk passes (no heap, no device allocation) and uploaded
+  // with one copy per chunk.
+  constexpr int kNaTexChunk = 16;
   int seeds[kNoAllocMaxPasses];
-  float tbuf[kTexSize];
-  for (int f = 0; f < F; ++f) {
-    for (int q = 0; q < passes; ++q) {
+  float tbuf[kNaTexChunk * kTexSize];
+  int const total = F * passes;
+  for (int q0 = 0; q0 < total; q0 += kNaTexChunk) {
+    int const qn = std::min(kNaTexChunk, total - q0);
+    for (int j = 0; j < qn; ++j) {
+      int const q = (q0 + j) % passes;
       std::uniform_int_distribution<> dist;
       std::uniform_real_distribution<float> uni(0.f, 1.f);
       bool const is_color = q >= 1 && ((q - 1) % 2 == 1);
-      int& s = seeds[f * passes + q];
+      int& s = seeds[q0 + j];
       if (!is_color) s = dist(ctx->host_rng);
-      for (int k = 0; k < kTexSize; ++k) tbuf[k] = uni(ctx->host_rng);
+      for (int k = 0; k < kTexSize; ++k) tbuf[size_t(j) * kTexSize + k] = uni(ctx->host_rng);
       if (is_color) s = dist(ctx->host_rng);
-      rc = check_cuda(ctx,
-          cudaMemcpyAsync(ptex + (size_t(f) * passes + q) * kTexSize, tbuf, sizeof(tbuf), cudaMemcpyHostToDevice, st),
-          "pass randomness upload");
-      if (rc) return rc;
     }
+    rc = check_cuda(ctx,
+        cudaMemcpyAsync(ptex + size_t(q0) * kTexSize, tbuf, size_t(qn) * kTexSize * sizeof(float),
+            cudaMemcpyHostToDevice, st),
+        "pass randomness upload");
+    // A copy from pageable memory has read its source when the call returns, so
+    // the buffer can be refilled at once.
+    if (rc) return rc;
   }
 
-  device_scene const& S = ctx->scene;
-  camera_dev cd{};
-  mat_mul4(cam->inverse_view, cam->inverse_projection, cd.vp);
-  cd.eye[0] = cam->inverse_view[12];
-  cd.eye[1] = cam->inverse_view[13];
-  cd.eye[2] = cam->inverse_view[14];
-  scene_dev sd{S.nodes, S.tris, S.tri_normals, S.tri_uvs, S.tri_material,
-      reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, ctx->d_err,
-      make_sdf_dev(ctx, p->sdf_marching_steps, p->sdf_marching_epsilon)};
-  color_args ca{reinterpret_cast<int2 const*>(S.materials), int(S.n_materials), S.material_data, accum, display, W,
-      sample_index, 0};
+  frame_setup const fs = make_frame_setup(ctx, cam, p, accum, display, sample_index);
+  camera_dev const& cd = fs.cd;
+  scene_dev const& sd = fs.sd;
+  color_args ca = fs.ca;
   size_t const n = size_t(W) * H;
   uint32_t const nb = uint32_t((n + kBlock - 1) / kBlock);
   for (int f = 0; f < F; ++f) {

@@ -162,6 +162,102 @@ def icosphere_field(n_spheres: int = 512, subdiv: int = 3, floor_cells: int = 16
                 material_data=mat_data.ravel())
 
 
+_GOLDEN64 = np.uint64(0x9E3779B97F4A7C15)
+
+
+def counter_uniform(index: np.ndarray, stream: int, seed: int = 0) -> np.ndarray:
+    """Uniform float64 numbers in [0, 1), one per entry of `index`, as a pure
+    function of (seed, index, stream): the SplitMix64 output function (Steele,
+    Lea and Flood, OOPSLA 2014) over the counter 8 * index + stream. Any
+    subset of a ray batch can be regenerated exactly from its indices."""
+    with np.errstate(over="ignore"):
+        z = (np.asarray(index, np.uint64) * np.uint64(8) + np.uint64(stream & 7) + np.uint64(seed) * np.uint64(1 << 40)
+             + np.uint64(1)) * _GOLDEN64
+        z ^= z >> np.uint64(30)
+        z *= np.uint64(0xBF58476D1CE4E5B9)
+        z ^= z >> np.uint64(27)
+        z *= np.uint64(0x94D049BB133111EB)
+        z ^= z >> np.uint64(31)
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / (1 << 53))
+
+
+def _unit(v: np.ndarray) -> np.ndarray:
+    return v / np.sqrt(v[..., 0] * v[..., 0] + v[..., 1] * v[..., 1] + v[..., 2] * v[..., 2])[..., None]
+
+
+ICOSPHERE_EYE, ICOSPHERE_TARGET, ICOSPHERE_VFOV = (0.0, 1.0, -4.5), (0.0, -0.3, 0.0), 50.0
+
+
+def jittered_camera_rays(index: np.ndarray, res: int, seed: int = 1000) -> np.ndarray:
+    """Camera rays of a res x res view of the icosphere scene, ray `i` through
+    pixel i mod res^2 (row-major, y down) at a uniformly jittered position
+    inside it (sample i div res^2), float32 [len(index), 8]. Rays depend only on
+    (index, res, seed), so a sample of indices gives exactly the same rays as
+    the full batch."""
+    index = np.asarray(index, np.int64)
+    eye = np.asarray(ICOSPHERE_EYE, np.float64)
+    fwd = _unit(np.asarray(ICOSPHERE_TARGET, np.float64) - eye)
+    right = _unit(np.cross(fwd, np.array([0.0, 1.0, 0.0])))
+    up = np.cross(right, fwd)
+    tan_half = np.tan(np.radians(ICOSPHERE_VFOV) / 2)
+    pix = index % (res * res)
+    px = (pix % res) + counter_uniform(index, 0, seed)
+    py = (pix // res) + counter_uniform(index, 1, seed)
+    sx = (2.0 * px / res - 1.0) * tan_half
+    sy = (1.0 - 2.0 * py / res) * tan_half
+    d = _unit(fwd[None] + sx[:, None] * right[None] + sy[:, None] * up[None])
+    rays = np.empty((index.size, 8), np.float32)
+    rays[:, 0:3] = eye
+    rays[:, 3] = 0.0
+    rays[:, 4:7] = d
+    rays[:, 7] = np.inf
+    return rays
+
+
+def diffuse_bounce_rays(rays: np.ndarray, prim: np.ndarray, t: np.ndarray, tris9: np.ndarray, index: np.ndarray,
+                        seed: int = 1000) -> np.ndarray:
+    """The first diffuse bounce of each hit ray: origin at the hit point moved
+    1e-4 along the face normal turned toward the ray, cosine-distributed
+    direction about that normal (random numbers from the parent ray's index).
+    rays float32 [n, 8], prim int32 [n] (hits only, >= 0), t float32 [n],
+    tris9 float32 [T, 9] world triangles by prim id. Returns float32 [n, 8]."""
+    tri = tris9[prim].astype(np.float64).reshape(-1, 3, 3)
+    n = _unit(np.cross(tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]))
+    d = rays[:, 4:7].astype(np.float64)
+    n = np.where(((n * d).sum(1) > 0)[:, None], -n, n)
+    p = rays[:, 0:3].astype(np.float64) + t.astype(np.float64)[:, None] * d
+    u1 = counter_uniform(index, 2, seed)
+    u2 = counter_uniform(index, 3, seed)
+    a = np.where((np.abs(n[:, 0]) > 0.9)[:, None], np.array([0.0, 1.0, 0.0]), np.array([1.0, 0.0, 0.0]))
+    tt = _unit(np.cross(n, a))
+    b = np.cross(n, tt)
+    r = np.sqrt(u1)
+    phi = 2.0 * np.pi * u2
+    wd = _unit((r * np.cos(phi))[:, None] * tt + (r * np.sin(phi))[:, None] * b
+               + np.sqrt(np.maximum(1.0 - u1, 0.0))[:, None] * n)
+    out = np.empty((prim.size, 8), np.float32)
+    out[:, 0:3] = p + 1e-4 * n
+    out[:, 3] = 0.0
+    out[:, 4:7] = wd
+    out[:, 7] = np.inf
+    return out
+
+
+def world_triangles(scene: dict) -> np.ndarray:
+    """World-space triangles float32 [T, 9] of an upload_scene argument dict,
+    in the library's prim numbering (drawables in order, triangles in index
+    order), each corner transformed in float64 and rounded once."""
+    idx = scene["indices"].astype(np.int64)
+    v = scene["vertices"].astype(np.float64).reshape(-1, 3)
+    out = []
+    for d in scene["drawables"]:
+        m = np.array(d.transformation[:], np.float64).reshape(4, 4).T
+        sel = idx[d.indices_base_index: d.indices_base_index + d.index_count] + d.points_base_index
+        p = v[sel] @ m[:3, :3].T + m[:3, 3]
+        out.append(p.reshape(-1, 9))
+    return np.concatenate(out).astype(np.float32)
+
+
 def icosphere_camera_rays(width: int = 512, height: int = 512, spp: int = 1, seed: int = 5) -> np.ndarray:
     """Camera rays of the icosphere scene; spp > 1 adds sub-pixel jitter."""
     rng = np.random.default_rng(seed)

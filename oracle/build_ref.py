@@ -5,7 +5,8 @@ library it builds; tests/, the smoke check and bench.py's CPU-baseline leg use
 the result as a checker / reference timing.
 
 What it compiles, from the sources where they lie under the reference tree
-(REF_ROOT, default /root/reference):
+(REF_ROOT: MYRT_REFERENCE_ROOT, by default the checkout beside this
+repository, ../reference; here /root/reference):
 
 * src/pathtracer/bvh.cpp and src/thread_pool.cpp with the two shims under
   oracle/shim (rnu vector math, <experimental/generator>). bvh.cpp needs one
@@ -39,7 +40,8 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
-REF_ROOT = Path(os.environ.get("MYRT_REFERENCE_ROOT", "/root/reference"))
+# the reference checkout beside this repository (../reference), or MYRT_REFERENCE_ROOT
+REF_ROOT = Path(os.environ.get("MYRT_REFERENCE_ROOT", HERE.parent.parent / "reference")).resolve()
 
 GLSL_FILES = ["random.glsl", "intersect.glsl", "ggx.glsl", "color.glsl", "pbr.glsl", "transform.glsl", "bvh.glsl",
               "bvh.impl.glsl"]

@@ -44,11 +44,15 @@ def test_golden_closest_hits_on_gpu(ctx, golden):
     ctx.upload_scene(idx, pts)
     hits = ctx.trace_closest(rays)
     same = hits["prim"] == glsl["prim"]
-    assert same.mean() >= 0.999
-    # where ids differ, the reference's first-visited rule resolved an exact tie in t
+    print(f"prim id agreement with the reference's GLSL traversal: {same.mean():.6f} "
+          f"({int((~same).sum())} of {same.size} differ)")
+    # no ray of the golden set ties exactly in t, so the tie rules (first visited in the reference,
+    # smaller prim id here) never come into play: every id agrees
+    assert same.all()
     assert np.array_equal(hits["t"], glsl["t"])
     hit = glsl["prim"] >= 0
-    assert np.array_equal(hits["u"][hit & same], glsl["u"][hit & same])
+    assert np.array_equal(hits["u"][hit], glsl["u"][hit])
+    assert np.array_equal(hits["v"][hit], glsl["v"][hit])
     occ = ctx.trace_any(g["shadow_rays"])
     assert np.array_equal(occ.astype(bool), g["any_short_prim"] >= 0)
 

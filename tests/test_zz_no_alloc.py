@@ -8,8 +8,10 @@ row (a new accumulation, then one more frame on top) and checks each result
 against the allocating entry point myrt_render on the same scene, camera and
 host random stream. Both run the same kernels on the same inputs, so the
 images must agree bit for bit (stricter than the 1e-3 bar of the render
-parity tests). It uses its own context, so it passes alone in a fresh process
-as well as after the other tests.
+parity tests). A second case renders a textured scene with the environment
+cube map and depth of field through a bokeh mask, on a stream the caller
+owns. It uses its own contexts, so it passes alone in a fresh process as well
+as after the other tests.
 """
 import numpy as np
 import pytest
@@ -59,3 +61,43 @@ def test_render_noalloc_matches_render():
         big = torch.zeros((512, 512, 4), dtype=torch.float32, device="cuda")
         with pytest.raises(mb.MyrtError, match="65536"):
             ctx.render_noalloc(iv, ip, 512, 512, big, big, num_bounces=bounces)
+
+
+def test_render_noalloc_textures_cubemap_dof_on_caller_stream():
+    import torch
+    from test_render_gpu import _bokeh_mask, _cubemap, _textured_heightfield
+
+    W, H, bounces = 80, 60, 4
+    scene, checker = _textured_heightfield()
+    iv, ip = look_at((0, 1.2, -2.5), (0, 0, 0), vfov_deg=55, aspect=W / H)
+    opts = dict(num_bounces=bounces, frames=2, dof=True, lens_size=(0.2, 0.15), focus=2.4, bokeh_slot=1)
+    with mb.Context(0) as ctx:
+        ctx.upload_scene(**scene)
+        ctx.upload_texture(0, checker, wrap=0)
+        ctx.upload_texture(1, _bokeh_mask(), wrap=0)
+        ctx.upload_cubemap(_cubemap())
+        ctx.set_seed(4242)
+        ctx.render(iv, ip, W, H, **opts)
+        ref1, disp1 = ctx.read_accumulation(W, H)
+        ctx.render(iv, ip, W, H, **opts)
+        ref2, disp2 = ctx.read_accumulation(W, H)
+
+        ctx.set_seed(4242)
+        stream = torch.cuda.Stream()
+        acc = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+        disp = torch.zeros((H, W, 4), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        ctx.render_noalloc(iv, ip, W, H, acc, disp, sample_index=0, stream=stream.cuda_stream, **opts)
+        stream.synchronize()
+        got1, gdisp1 = acc.cpu().numpy(), disp.cpu().numpy()
+        ctx.render_noalloc(iv, ip, W, H, acc, disp, sample_index=2, stream=stream.cuda_stream, **opts)
+        stream.synchronize()
+        ctx.sync()
+        got2, gdisp2 = acc.cpu().numpy(), disp.cpu().numpy()
+        for got, ref, gd, rd in ((got1, ref1, gdisp1, disp1), (got2, ref2, gdisp2, disp2)):
+            assert np.array_equal(got, ref)
+            assert np.array_equal(gd, rd)
+        assert np.all(got2[..., 3] == 4.0)
+        # only the reference shading runs here, and the refusal says so
+        with pytest.raises(mb.MyrtError, match="only MYRT_SHADE_REFERENCE"):
+            ctx.render_noalloc(iv, ip, W, H, acc, disp, shading=1, num_bounces=bounces)
