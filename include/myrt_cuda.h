@@ -171,6 +171,15 @@ typedef struct myrt_tuning {
   uint32_t guide_stall_test; /* 1: that first wait watches a barrier nothing arrives at, so it runs
                                 out after guide_poll_limit polls: tests the timeout path without a
                                 fault. 0 in normal use */
+  uint32_t instancing;       /* ray queries (myrt_trace_closest / _any and their _device forms):
+                                0 = one tree over the world-space (baked) triangles; 1 = the
+                                reference's two-level walk (src/pt/pt_trace.comp:284-309): a tree
+                                over the drawables' world boxes, each ray moved into the drawable's
+                                object space by inverse_transformation and tested against the
+                                untransformed geometry, so t, u and v equal the reference's bit for
+                                bit. 1 must be set before myrt_scene_upload, which then also builds
+                                one object-space tree per distinct geometry; renders always use the
+                                baked tree. */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */

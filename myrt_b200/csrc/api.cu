@@ -51,6 +51,10 @@ void free_scene(device_scene& s) {
   cudaFree(s.spare_tris);
   cudaFree(s.spare_pos);
   cudaFree(s.move_stage);
+  cudaFree(s.blas_nodes);
+  cudaFree(s.blas_tris);
+  cudaFree(s.tlas_nodes);
+  cudaFree(s.inst_records);
   s = device_scene{};
 }
 
@@ -215,6 +219,19 @@ int launch_trace(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool st
 int launch_trace_kernels(myrt_ctx* ctx, trace_args a, int intersector, bool any, bool stats, cudaStream_t s) {
   dim3 const block(128);
   dim3 const grid((a.n + 127) / 128);
+  if (ctx->tuning.instancing) {
+    a.nodes = ctx->scene.tlas_nodes;
+    if (intersector == MYRT_ISECT_REFERENCE) {
+      if (stats) k_trace_inst<0, false, true><<<grid, block, 0, s>>>(a);
+      else if (any) k_trace_inst<0, true, false><<<grid, block, 0, s>>>(a);
+      else k_trace_inst<0, false, false><<<grid, block, 0, s>>>(a);
+    } else {
+      if (stats) k_trace_inst<1, false, true><<<grid, block, 0, s>>>(a);
+      else if (any) k_trace_inst<1, true, false><<<grid, block, 0, s>>>(a);
+      else k_trace_inst<1, false, false><<<grid, block, 0, s>>>(a);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "instanced trace launch");
+  }
   if (ctx->tuning.trace_persistent) {
     int rc;
     if (intersector == MYRT_ISECT_REFERENCE) {
@@ -279,6 +296,8 @@ int validate_query(myrt_ctx* ctx, void const* rays, void const* out, int interse
   if (!rays || !out) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "null ray or output pointer");
   if (intersector != MYRT_ISECT_REFERENCE && intersector != MYRT_ISECT_WATERTIGHT)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "unknown intersector");
+  if (ctx->tuning.instancing && !ctx->scene.instanced)
+    return set_error(ctx, MYRT_ERR_UNSUPPORTED, "instancing = 1 needs a scene uploaded with instancing = 1");
   return MYRT_OK;
 }
 
@@ -287,6 +306,9 @@ trace_args base_args(myrt_ctx* ctx) {
   a.nodes = ctx->scene.nodes;
   a.tris = ctx->scene.tris;
   a.err = ctx->d_err;
+  a.blas_nodes = ctx->scene.blas_nodes;
+  a.blas_tris = ctx->scene.blas_tris;
+  a.inst = ctx->scene.inst_records;
   return a;
 }
 
@@ -462,7 +484,7 @@ int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
   if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
       t->trace_unit_steps > 1 || (t->wave_paths != 0 && (t->wave_paths < 1024 || t->wave_paths > (1u << 28))) ||
       t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2 || t->bvh_builder > 1 || t->sdf_cells > 128 ||
-      t->guide_stall_test > 1)
+      t->guide_stall_test > 1 || t->instancing > 1)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;
@@ -505,6 +527,68 @@ int myrt_get_stream(myrt_ctx* ctx, void** stream) {
   *stream = ctx->stream;
   return MYRT_OK;
 }
+
+}  // extern "C"
+
+namespace myrt_b200 {
+// Uploads the tree over the drawables' world boxes and its instance records
+// (rebuilt whenever transforms change).
+int upload_top_level(myrt_ctx* ctx, std::vector<myrt_drawable> const& drawables) {
+  device_scene& s = ctx->scene;
+  two_level objects;
+  objects.geometries = s.geometries;
+  objects.drawable_geometry = s.drawable_geometry;
+  objects.prim_base = s.drawable_prim_base;
+  top_level top;
+  try {
+    top = build_top_level(objects, drawables.data(), drawables.size());
+  } catch (std::exception const& e) {
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, std::string("instance tree build: ") + e.what());
+  }
+  if (top.nodes.empty()) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "instancing: no drawable has triangles");
+  if (top.depth + s.blas_depth + kInstanceSave > MYRT_STACK_MAX)
+    return set_error(ctx, MYRT_ERR_UNSUPPORTED, "instance tree + object tree deeper than the traversal stack");
+  cudaFree(s.tlas_nodes);
+  cudaFree(s.inst_records);
+  s.tlas_nodes = nullptr;
+  s.inst_records = nullptr;
+  int rc = upload(ctx, reinterpret_cast<bvh8_node**>(&s.tlas_nodes), top.nodes.data(), top.nodes.size(),
+      "instance tree upload");
+  if (!rc)
+    rc = upload(ctx, reinterpret_cast<instance_record**>(&s.inst_records), top.records.data(), top.records.size(),
+        "instance record upload");
+  s.n_tlas_nodes = top.nodes.size();
+  s.n_inst_records = top.records.size();
+  s.tlas_depth = top.depth;
+  return rc;
+}
+
+// Object-space trees of the distinct geometries, then the instance level.
+int upload_two_level(myrt_ctx* ctx, myrt_scene_view const* v, std::vector<myrt_drawable> const& drawables) {
+  device_scene& s = ctx->scene;
+  two_level objects;
+  std::string err;
+  if (!build_object_trees(v->vertices, v->vertex_count, v->indices, v->index_count, drawables.data(),
+          drawables.size(), objects, err))
+    return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, err);
+  s.geometries = objects.geometries;
+  s.drawable_geometry = objects.drawable_geometry;
+  s.drawable_prim_base = objects.prim_base;
+  s.blas_depth = objects.blas_depth;
+  int rc = upload(ctx, reinterpret_cast<bvh8_node**>(&s.blas_nodes), objects.blas_nodes.data(),
+      objects.blas_nodes.size(), "object tree upload");
+  if (!rc)
+    rc = upload(ctx, reinterpret_cast<bvh8_triangle**>(&s.blas_tris), objects.blas_tris.data(),
+        objects.blas_tris.size(), "object triangle upload");
+  s.n_blas_nodes = objects.blas_nodes.size();
+  s.n_blas_tris = objects.blas_tris.size();
+  if (!rc) rc = upload_top_level(ctx, drawables);
+  if (!rc) s.instanced = true;
+  return rc;
+}
+}  // namespace myrt_b200
+
+extern "C" {
 
 int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
   if (!ctx || !v) return MYRT_ERR_INVALID_ARGUMENT;
@@ -658,6 +742,7 @@ int myrt_scene_upload(myrt_ctx* ctx, myrt_scene_view const* v) {
     else rc = upload(ctx, &s.material_data, v->material_data, v->material_data_count, "material data upload");
     s.n_material_data = v->material_data_count;
   }
+  if (!rc && ctx->tuning.instancing) rc = upload_two_level(ctx, v, drawables);
   if (!rc) rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "scene upload");
   if (rc) {
     free_scene(s);

@@ -12,6 +12,7 @@
 #include "../../include/myrt_cuda.h"
 #include "bvh8.hpp"
 #include "bvh8_device.hpp"
+#include "instances.hpp"
 
 namespace myrt_b200 {
 
@@ -55,6 +56,19 @@ struct device_scene {
   size_t spare_node_capacity = 0, spare_tri_capacity = 0;
   void* move_stage = nullptr;  // drawable transforms + bounds of a move
   size_t move_stage_bytes = 0;
+  // two-level structure for instanced ray queries (tuning.instancing = 1,
+  // instances.hpp): object-space trees of the distinct geometries, the tree over
+  // the drawables' world boxes and its instance records (4 float4 each)
+  uint4* blas_nodes = nullptr;
+  float4* blas_tris = nullptr;
+  uint4* tlas_nodes = nullptr;
+  float4* inst_records = nullptr;
+  size_t n_blas_nodes = 0, n_blas_tris = 0, n_tlas_nodes = 0, n_inst_records = 0;
+  int blas_depth = 0, tlas_depth = 0;
+  std::vector<geometry_tree> geometries;         // per distinct geometry
+  std::vector<uint32_t> drawable_geometry;       // per drawable
+  std::vector<uint32_t> drawable_prim_base;      // per drawable
+  bool instanced = false;
 };
 
 // SDF drawables (uploaded separately; scene::prepare's sdf buffers).
@@ -131,7 +145,7 @@ struct myrt_ctx {
   myrt_b200::guide_state* guide = nullptr;  // learned proposal (guide.cu), created on first use
   uint64_t guide_generation = 0;            // bumped by scene uploads
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
-  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
   int sm_count = 0;
   uint32_t* d_next = nullptr;    // ring of ray counters for the persistent traversal
   uint32_t next_slot = 0;
@@ -189,4 +203,5 @@ int trace_sdf_rays(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, int steps, f
     uint32_t const* rng_states, float* out);
 int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p,
     uint32_t sample_index, float4* accum, float4* display, cudaStream_t st);
+int upload_top_level(myrt_ctx* ctx, std::vector<myrt_drawable> const& drawables);
 }  // namespace myrt_b200

@@ -227,6 +227,10 @@ int scene_set_transforms(myrt_ctx* ctx, myrt_drawable const* drawables, size_t c
   s.stats.max_leaf_size = 4;
   for (int k = 0; k < 6; ++k) s.bounds[k] = ord2f(hb[k]);
   s.drawables.assign(drawables, drawables + count);
+  if (s.instanced) {  // the instance level follows the new transforms (host build, small)
+    int const e = upload_top_level(ctx, s.drawables);
+    if (e) return e;
+  }
   s.stats.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   ctx->render.sample_counter = 0;  // the image restarts, as after prepare() reported a change
   return MYRT_OK;

@@ -132,6 +132,14 @@ struct trace_args {
   uint32_t* err;
   int stack_cap;       // k_trace_smem: stack entries per thread
   uint32_t const* perm;  // visiting order (thread t takes ray perm[t]); null = input order
+  // two-level (instanced) walk, k_trace_inst: `nodes` is the tree over the
+  // instances, whose leaf slots index `inst` (4 float4 per instance record,
+  // instances.hpp); the object-space trees of the geometries live in
+  // blas_nodes / blas_tris
+  const uint4* blas_nodes;
+  const float4* blas_tris;
+  const float4* inst;
+  uint32_t* stat_inst;  // instances entered per ray (STATS)
 };
 
 // Byte (s & 3) of w as an exact float: one byte permute places it in the low
@@ -418,6 +426,167 @@ __device__ __forceinline__ void store_result(trace_args const& a, uint32_t i, bo
     a.stat_nodes[i] = n_nodes;
     a.stat_tris[i] = n_tris;
   }
+}
+
+// Two-level walk for instanced scenes: the reference's bvh_traverse_global
+// with visit_object_aabb (src/pt/pt_trace.comp:98-116, 284-309). The tree over
+// the instances is walked with the world ray; each instance leaf moves the ray
+// into the instance's object space -- (inverse_transformation * vec4(o, 1)).xyz
+// and (inverse_transformation * vec4(d, 0)).xyz, every product and sum rounded
+// separately, left to right, the direction not renormalised -- and walks the
+// geometry's object-space tree on the same stack with the same t scale.
+// Triangles are tested in object space with the object-space ray, so t, u and v
+// equal the reference's bit for bit; ties in t go to the smaller global prim id
+// (the drawable's first prim id + the triangle's index in its geometry).
+// Entering an instance saves the instance level's state on the stack (its node
+// group, the instance leaves still pending and the world ray: 5 entries), so
+// none of it occupies registers during the instance's walk.
+constexpr int kInstanceSave = 5;
+
+template <int ISECT, bool ANY>
+__device__ __forceinline__ void set_walker_ray(walker<ISECT, ANY>& w, f3 o, f3 d) {
+  w.o = o;
+  w.d = d;
+  w.idx = 1.0f / (fabsf(d.x) > 1e-20f ? d.x : copysignf(1e-20f, d.x));
+  w.idy = 1.0f / (fabsf(d.y) > 1e-20f ? d.y : copysignf(1e-20f, d.y));
+  w.idz = 1.0f / (fabsf(d.z) > 1e-20f ? d.z : copysignf(1e-20f, d.z));
+  uint32_t const oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+  w.octinv = oct ^ 7u;
+  if (ISECT == 1) w.wt = wt_setup(d);
+}
+
+// row . (x, y, z, w) summed left to right, each step rounded
+__device__ __forceinline__ float row_dot(float4 r, f3 v, float vw) {
+  return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(r.x, v.x), __fmul_rn(r.y, v.y)), __fmul_rn(r.z, v.z)),
+      __fmul_rn(r.w, vw));
+}
+
+// Walks the two-level structure for one ray: as traverse(), n_inst counts the
+// instances entered.
+template <int ISECT, bool ANY, bool STATS>
+__device__ __forceinline__ bool traverse_two_level(trace_args const& a, f3 o, f3 d, float tmin, float tmax,
+    hit_rec& h, uint32_t& n_nodes, uint32_t& n_tris, uint32_t& n_inst) {
+  uint2 stack[MYRT_STACK_MAX];
+  walker<ISECT, ANY> w;
+  w.init(o, d, tmin, tmax);
+  uint2 pending = make_uint2(0u, 0u);  // instance leaves of the last top-level node
+  bool answered = false;
+  while (!answered) {
+    while (pending.y) {
+      uint32_t const b = __ffs(pending.y) - 1u;
+      pending.y &= pending.y - 1u;
+      int const save = w.sp;
+      if (save + kInstanceSave > w.cap) {
+        atomicOr(a.err, ERR_STACK_OVERFLOW);
+        answered = true;
+        break;
+      }
+      stack[save] = w.group;
+      stack[save + 1] = pending;
+      stack[save + 2] = make_uint2(__float_as_uint(w.o.x), __float_as_uint(w.o.y));
+      stack[save + 3] = make_uint2(__float_as_uint(w.o.z), __float_as_uint(w.d.x));
+      stack[save + 4] = make_uint2(__float_as_uint(w.d.y), __float_as_uint(w.d.z));
+      w.sp = save + kInstanceSave;
+      float4 const* r = a.inst + 4 * size_t(pending.x + b);
+      float4 const r0 = __ldg(r + 0), r1 = __ldg(r + 1), r2 = __ldg(r + 2);
+      int4 const meta = __ldg(reinterpret_cast<int4 const*>(r + 3));
+      if (STATS) ++n_inst;
+      f3 const oo{row_dot(r0, w.o, 1.0f), row_dot(r1, w.o, 1.0f), row_dot(r2, w.o, 1.0f)};
+      f3 const od{row_dot(r0, w.d, 0.0f), row_dot(r1, w.d, 0.0f), row_dot(r2, w.d, 0.0f)};
+      set_walker_ray(w, oo, od);
+      w.group = make_uint2(uint32_t(meta.x), 0x80000000u);  // the geometry's root
+      int32_t const prim_base = meta.y;
+      // the instance's walk, on the stack above the saved state
+      while (true) {
+        uint2 tgroup = make_uint2(0u, 0u);
+        if (w.group.y & 0xff000000u) {
+          if (!w.template visit<STATS>(a.blas_nodes, stack, a.err, n_nodes, tgroup)) {
+            answered = true;
+            break;
+          }
+        } else {
+          w.group.y = 0;
+        }
+        while (tgroup.y) {
+          uint32_t const tb = __ffs(tgroup.y) - 1u;
+          tgroup.y &= tgroup.y - 1u;
+          float4 const* tp = a.blas_tris + 3 * size_t(tgroup.x + tb);
+          float4 const p0 = __ldg(tp + 0);
+          float4 const p1 = __ldg(tp + 1);
+          float4 const p2 = __ldg(tp + 2);
+          if (STATS) ++n_tris;
+          float t, u, v;
+          bool hit;
+          if (ISECT == 0)
+            hit = isect_reference(w.o, w.d, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, t, u,
+                      v) && t >= w.tmin;
+          else
+            hit = isect_watertight(w.wt, w.o, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z},
+                w.tmin, t, u, v);
+          if (!hit) continue;
+          int32_t const prim = prim_base + __float_as_int(p0.w);
+          if (ANY) {
+            if (t < w.tmax) {
+              w.occluded = true;
+              answered = true;
+              break;
+            }
+          } else if (t < w.tbest || (t == w.tbest && w.best >= 0 && prim < w.best)) {
+            w.tbest = t;
+            w.best = prim;
+            w.bu = u;
+            w.bv = v;
+          }
+        }
+        if (answered) break;
+        if (!(w.group.y & 0xff000000u)) {
+          if (w.sp == save + kInstanceSave) break;
+          w.group = stack[--w.sp];
+        }
+      }
+      if (answered) break;
+      uint2 const s2 = stack[save + 2], s3 = stack[save + 3], s4 = stack[save + 4];
+      w.group = stack[save];
+      pending = stack[save + 1];
+      w.sp = save;
+      set_walker_ray(w, f3{__uint_as_float(s2.x), __uint_as_float(s2.y), __uint_as_float(s3.x)},
+          f3{__uint_as_float(s3.y), __uint_as_float(s4.x), __uint_as_float(s4.y)});
+    }
+    if (answered) break;
+    if (w.group.y & 0xff000000u) {
+      if (!w.template visit<STATS>(a.nodes, stack, a.err, n_nodes, pending)) break;
+      if (pending.y) continue;
+    } else {
+      w.group.y = 0;
+    }
+    if (!(w.group.y & 0xff000000u)) {
+      if (w.sp == 0) break;
+      w.group = stack[--w.sp];
+    }
+  }
+  if (ANY) return w.occluded;
+  h.prim = w.best;
+  h.t = w.best >= 0 ? w.tbest : tmax;
+  h.u = w.best >= 0 ? w.bu : 0.f;
+  h.v = w.best >= 0 ? w.bv : 0.f;
+  h.leaf = 0;
+  return h.prim >= 0;
+}
+
+// One thread per ray over the two-level structure.
+template <int ISECT, bool ANY, bool STATS>
+__global__ void __launch_bounds__(128, 8) k_trace_inst(trace_args a) {
+  uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  uint32_t const i = a.perm ? __ldg(a.perm + t) : t;
+  float4 const r0 = __ldg(a.rays + 2 * size_t(i));
+  float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
+  hit_rec h;
+  uint32_t n_nodes = 0, n_tris = 0, n_inst = 0;
+  bool const r = traverse_two_level<ISECT, ANY, STATS>(a, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w, r1.w, h,
+      n_nodes, n_tris, n_inst);
+  store_result<ISECT, ANY, STATS>(a, i, r, h, n_nodes, n_tris);
+  if (STATS && a.stat_inst) a.stat_inst[i] = n_inst;
 }
 
 // One thread per ray, traversal stack in shared memory ([entry][thread],

@@ -258,6 +258,72 @@ def world_triangles(scene: dict) -> np.ndarray:
     return np.concatenate(out).astype(np.float32)
 
 
+def _rotation(axis, angle) -> np.ndarray:
+    a = np.asarray(axis, np.float64)
+    a = a / np.linalg.norm(a)
+    c, s = np.cos(angle), np.sin(angle)
+    K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    return np.eye(3) + s * K + (1 - c) * (K @ K)
+
+
+def unit_box():
+    """Axis-aligned cube [-1, 1]^3 as 12 triangles: (indices uint32, points float32)."""
+    p = np.array([[x, y, z] for z in (-1, 1) for y in (-1, 1) for x in (-1, 1)], np.float32)
+    quads = [(0, 2, 3, 1), (4, 5, 7, 6), (0, 1, 5, 4), (2, 6, 7, 3), (0, 4, 6, 2), (1, 3, 7, 5)]
+    tri = []
+    for a, b, c, d in quads:
+        tri += [a, b, c, a, c, d]
+    return np.array(tri, np.uint32), p
+
+
+def instanced_field(n_spheres: int = 48, n_boxes: int = 24, subdiv: int = 2, floor_cells: int = 8, seed: int = 21):
+    """Instances with general affine transforms: icospheres and boxes under
+    random rotations, non-uniform scales (0.05-0.3 per axis) and translations in
+    [-1, 1]^3, plus a floor grid at y = -1.2 drawn with an identity transform.
+    Each drawable's inverse_transformation is its transformation inverted in
+    float64 and rounded to float32. Returns upload_scene arguments."""
+    from ._abi import myrt_drawable
+
+    rng = np.random.default_rng(seed)
+    si, sp = icosphere(subdiv)
+    bi, bp = unit_box()
+    g = np.linspace(-3.0, 3.0, floor_cells + 1)
+    gx, gz = np.meshgrid(g, g, indexing="xy")
+    fp = np.stack([gx.ravel(), np.full(gx.size, -1.2), gz.ravel()], 1).astype(np.float32)
+    i, j = np.meshgrid(np.arange(floor_cells), np.arange(floor_cells), indexing="xy")
+    v00 = (j * (floor_cells + 1) + i).ravel()
+    fi = np.stack([np.stack([v00, v00 + floor_cells + 1, v00 + 1], 1),
+                   np.stack([v00 + 1, v00 + floor_cells + 1, v00 + floor_cells + 2], 1)], 1).reshape(-1)
+    indices = np.concatenate([si, bi, fi.astype(np.uint32)])
+    vertices = np.concatenate([sp, bp, fp]).astype(np.float32)
+    normals = np.concatenate([sp, bp / np.linalg.norm(bp, axis=1, keepdims=True),
+                              np.tile(np.array([[0.0, 1.0, 0.0]], np.float32), (fp.shape[0], 1))]).astype(np.float32)
+    geo = [(0, 0, si.size), (si.size, sp.shape[0], bi.size), (si.size + bi.size, sp.shape[0] + bp.shape[0], fi.size)]
+    kinds = [0] * n_spheres + [1] * n_boxes
+    drawables = (myrt_drawable * (len(kinds) + 1))()
+    for k, kind in enumerate(kinds):
+        R = _rotation(rng.normal(size=3), rng.uniform(0, 2 * np.pi))
+        S = np.diag(rng.uniform(0.05, 0.3, 3))
+        M = np.eye(4)
+        M[:3, :3] = R @ S
+        M[:3, 3] = rng.uniform(-1.0, 1.0, 3)
+        m32 = M.astype(np.float32)
+        inv = np.linalg.inv(m32.astype(np.float64)).astype(np.float32)
+        d = drawables[k]
+        d.transformation[:] = m32.T.ravel().tolist()  # column-major
+        d.inverse_transformation[:] = inv.T.ravel().tolist()
+        d.indices_base_index, d.points_base_index, d.index_count = geo[kind]
+        d.material_index = 0
+    fl = drawables[len(kinds)]
+    eye = np.eye(4, dtype=np.float32).ravel().tolist()
+    fl.transformation[:] = eye
+    fl.inverse_transformation[:] = eye
+    fl.indices_base_index, fl.points_base_index, fl.index_count = geo[2]
+    mat = np.array([[0, 0]], np.int32)
+    return dict(indices=indices, vertices=vertices, normals=normals, drawables=drawables, materials=mat,
+                material_data=pbr_material([0.6, 0.6, 0.6], roughness=0.8))
+
+
 def icosphere_camera_rays(width: int = 512, height: int = 512, spp: int = 1, seed: int = 5) -> np.ndarray:
     """Camera rays of the icosphere scene; spp > 1 adds sub-pixel jitter."""
     rng = np.random.default_rng(seed)

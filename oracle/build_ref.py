@@ -14,8 +14,10 @@ repository, ../reference; here /root/reference):
   ``generate_triangle_bounds`` at bvh.cpp:136 is an MSVC-ism that g++ rejects,
   so a copy with that token removed is written to oracle/_ref/src/.
 * The shader helper files src/pt/{random,intersect,ggx,color,pbr,transform,
-  bvh,bvh.impl}.glsl and the traversal visitor of src/pt/pt_trace.comp
-  (lines 229-282: traversal_state_t, traversal_init, visit_triangle), compiled
+  bvh,bvh.impl}.glsl and the traversal visitors of src/pt/pt_trace.comp
+  (lines 229-309: traversal_state_t, traversal_init, visit_triangle and the
+  instance visitor visit_object_aabb; the drawable record of lines 34-47),
+  compiled
   as C++ through oracle/glsl_compat.hpp after these mechanical rewrites only:
     - ``out T x`` / ``inout T x`` parameters -> ``T& x``; ``const in`` -> ``const``;
     - float literals without a suffix get ``f`` (GLSL literals are float);
@@ -137,13 +139,22 @@ def glsl_to_cpp(src: str, globals_thread_local: bool = True) -> str:
 
 
 def extract_trace_visitor(src: str) -> str:
-    """pt_trace.comp:229-282 (traversal state, traversal_init, visit_triangle)."""
+    """pt_trace.comp:229-309 (traversal state, traversal_init, visit_triangle and
+    the instance visitor visit_object_aabb), up to any_hit()."""
     start = src.index("struct traversal_state_t")
-    end = src.index("bool visit_object_aabb")
+    end = src.index("bool any_hit(vec3 ray_origin, vec3 ray_direction, float max_distance)\n{")
     seg = src[start:end]
+    assert "bool visit_object_aabb" in seg, "pt_trace.comp: visit_object_aabb moved"
     seg, n = re.subn(r"\}\s*traversal\s*;", "};\nthread_local traversal_state_t traversal;", seg)
     assert n == 1, "pt_trace.comp: traversal_state_t layout changed"
     return glsl_to_cpp(seg)
+
+
+def extract_drawable_geometry(src: str) -> str:
+    """pt_trace.comp:34-47: the per-drawable record (drawable_geometry_t)."""
+    start = src.index("struct drawable_geometry_t")
+    end = src.index("};", start) + 2
+    return glsl_to_cpp(src[start:end])
 
 
 def material_codegen(src: str, type_name: str = "material") -> str:
@@ -270,6 +281,7 @@ def write_sources() -> None:
     (OUT / "glsl/material_new.glsl").write_text(material_codegen((REF_ROOT / "src/pt/material_new.glsl").read_text()))
     trace = (REF_ROOT / "src/pt/pt_trace.comp").read_text()
     (OUT / "glsl/pt_trace_visitor.glsl").write_text(extract_trace_visitor(trace))
+    (OUT / "glsl/pt_trace_geometry.glsl").write_text(extract_drawable_geometry(trace))
     (OUT / "glsl/raymarch.glsl").write_text(raymarch_to_cpp((REF_ROOT / "src/pt/raymarch.glsl").read_text()))
     (OUT / "glsl/sdf_snippets.inc").write_text(
         extract_sdf_snippets((REF_ROOT / "src/pathtracer/sdf.hpp").read_text()))

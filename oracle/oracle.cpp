@@ -17,6 +17,8 @@
 //                         dont_split (no primitive splitting)
 //   orc_refbvh_traverse   src/pt/bvh.impl.glsl:8-72 + pt_trace.comp:259-282
 //                         (first visited wins ties) and a canonical variant
+//   orc_instanced_query   src/pt/pt_trace.comp:284-309 (visit_object_aabb): object-space
+//                         walks of every drawable's geometry tree, canonical ties
 //   orc_bvh8_traverse     the device traversal of the 8-wide tree, instrumented
 //                         (nodes fetched, triangles tested per ray)
 //   orc_brute_closest     all-triangle closest hit, canonical ties
@@ -403,6 +405,100 @@ void orc_refbvh_traverse(void const* nodes_v, std::uint32_t const* bvh_idx, std:
       nthreads);
 }
 
+}  // extern "C"
+
+namespace {
+struct query_hit {
+  bool found;
+  std::int32_t prim;
+  float t, u, v;
+};
+
+// One ray through one reference tree (bvh.impl.glsl:8-72 + the pt_trace.comp
+// visitor). Node child / parent indices and triangle indices are relative to
+// the arrays passed in (the reference's node_base / primitive_base scheme).
+query_hit refbvh_closest(ref_node const* nodes, std::uint32_t const* bvh_idx, std::uint32_t const* indices,
+    float const* points_xyzw, ray8 const& ray, int any_hit, int canonical, int isect) {
+  auto pt = [points_xyzw](std::uint32_t i) {
+    return v3{points_xyzw[4 * i], points_xyzw[4 * i + 1], points_xyzw[4 * i + 2]};
+  };
+  v3 const ro = ray.o, rd = ray.d;
+  wt_ray const wt = wt_setup(rd);
+  v3 const inv{1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z};
+  float maxt = ray.tmax;
+  float best_t = ray.tmax, bu = 0, bv = 0;
+  std::int32_t best = -1;
+  bool found = false;
+  std::uint32_t visited = 0, lr = 0, node_index = 0;
+  float tmp;
+  bool hits_any = slab(nodes[0], ro, inv, maxt, tmp);
+  bool done = false;
+  while (hits_any && !done) {
+    ref_node current = nodes[node_index];
+    while (!(current.type_and_parent & 0x80000000u)) {
+      float tl, tr;
+      ref_node const& fc = nodes[current.first];
+      ref_node const& sc = nodes[current.second];
+      bool const hl = slab(fc, ro, inv, maxt, tl);
+      bool const hr = slab(sc, ro, inv, maxt, tr);
+      if (!hl && !hr) break;
+      bool const use_right = !hl || (hr && tl >= tr);
+      lr = std::uint32_t(use_right) | (lr << 1);
+      visited = std::uint32_t(hl && hr) | (visited << 1);
+      node_index = use_right ? current.second : current.first;
+      current = nodes[node_index];
+    }
+    if (current.type_and_parent & 0x80000000u) {
+      for (std::uint32_t tri = current.first; tri <= current.second; ++tri) {
+        std::uint32_t const pi = bvh_idx[tri];
+        float t, u, v;
+        bool h = isect < 0 ? isect_reference(ro, rd, pt(indices[3 * pi]), pt(indices[3 * pi + 1]),
+                                 pt(indices[3 * pi + 2]), t, u, v)
+                           : test_tri(isect, wt, ray, pt(indices[3 * pi]), pt(indices[3 * pi + 1]),
+                                 pt(indices[3 * pi + 2]), t, u, v);
+        h = h && t < maxt && (canonical ? canonical_better(t, std::int32_t(pi), best_t, best) : best_t > t);
+        if (h) {
+          best_t = t;
+          bu = u;
+          bv = v;
+          best = std::int32_t(pi);
+          found = true;
+          maxt = canonical ? std::nextafter(t, std::numeric_limits<float>::infinity()) : t;
+          if (any_hit) {
+            done = true;
+            break;
+          }
+        }
+      }
+      if (done) break;
+    }
+    while ((visited & 1u) != 1u) {
+      if (visited == 0) {
+        done = true;
+        break;
+      }
+      node_index = nodes[node_index].type_and_parent & 0x7fffffffu;
+      visited >>= 1;
+      lr >>= 1;
+    }
+    if (done) break;
+    std::uint32_t const parent = nodes[node_index].type_and_parent & 0x7fffffffu;
+    node_index = (lr & 1u) ? nodes[parent].first : nodes[parent].second;
+    visited ^= 1u;
+  }
+  return {found, found ? best : -1, found ? best_t : ray.tmax, found ? bu : 0.f, found ? bv : 0.f};
+}
+
+// GLSL's (m * vec4(v, w)).xyz for a column-major mat4: products and sums
+// rounded one by one, left to right.
+inline v3 mat4_apply(float const* m, v3 p, float w) {
+  return {((m[0] * p.x + m[4] * p.y) + m[8] * p.z) + m[12] * w, ((m[1] * p.x + m[5] * p.y) + m[9] * p.z) + m[13] * w,
+      ((m[2] * p.x + m[6] * p.y) + m[10] * p.z) + m[14] * w};
+}
+}  // namespace
+
+extern "C" {
+
 // isect -1: the reference's traversal as written (Moller-Trumbore, no tmin
 // test); 0 / 1: Moller-Trumbore / watertight with the device kernels'
 // acceptance rule (t >= tmin, t < tmax).
@@ -410,80 +506,64 @@ void orc_refbvh_query(void const* nodes_v, std::uint32_t const* bvh_idx, std::ui
     float const* points_xyzw, float const* rays, std::size_t n, int any_hit, int canonical, int isect,
     std::int32_t* prim, float* t_out, float* u_out, float* v_out, int nthreads) {
   auto const* nodes = static_cast<ref_node const*>(nodes_v);
-  auto pt = [points_xyzw](std::uint32_t i) {
-    return v3{points_xyzw[4 * i], points_xyzw[4 * i + 1], points_xyzw[4 * i + 2]};
-  };
+  parallel_for(n, nthreads, [&](std::size_t b, std::size_t e) {
+    for (std::size_t r = b; r < e; ++r) {
+      query_hit const q =
+          refbvh_closest(nodes, bvh_idx, indices, points_xyzw, load_ray(rays + 8 * r), any_hit, canonical, isect);
+      prim[r] = q.prim;
+      t_out[r] = q.t;
+      u_out[r] = q.u;
+      v_out[r] = q.v;
+    }
+  });
+}
+
+// Instanced scenes, src/pt/pt_trace.comp:284-309 (visit_object_aabb) under
+// the two-level walk: for every drawable, the ray moved into object space by
+// inverse_transformation (origin with w = 1, direction with w = 0, not
+// renormalised) walks that drawable's geometry tree (node and index bases
+// bvh_node_base_index / bvh_index_base_index of the drawable record, vertices
+// at points_base_index, indices at indices_base_index, as the reference
+// addresses them). Every drawable is visited (no tree over the instances: a
+// tree only decides which instances are skipped, never the answer). Closest
+// hit keeps the smallest t, ties to the smaller global prim id (drawable's
+// first prim + the triangle's index in its geometry); any hit answers whether
+// some t in [tmin, tmax) exists. drawables: 40 words each (myrt_drawable).
+void orc_instanced_query(void const* nodes_v, std::uint32_t const* bvh_idx, std::uint32_t const* indices,
+    float const* points_xyzw, void const* drawables_v, std::size_t n_drawables, float const* rays, std::size_t n,
+    int any_hit, int isect, std::int32_t* prim, float* t_out, float* u_out, float* v_out, int nthreads) {
+  auto const* nodes = static_cast<ref_node const*>(nodes_v);
+  auto const* dw = static_cast<std::uint32_t const*>(drawables_v);
+  std::vector<std::int32_t> prim_base(n_drawables);
+  std::int64_t acc = 0;
+  for (std::size_t i = 0; i < n_drawables; ++i) {
+    prim_base[i] = std::int32_t(acc);
+    acc += dw[40 * i + 36] / 3;
+  }
   parallel_for(n, nthreads, [&](std::size_t b, std::size_t e) {
     for (std::size_t r = b; r < e; ++r) {
       ray8 const ray = load_ray(rays + 8 * r);
-      v3 const ro = ray.o, rd = ray.d;
-      wt_ray const wt = wt_setup(rd);
-      v3 const inv{1.0f / rd.x, 1.0f / rd.y, 1.0f / rd.z};
-      float maxt = ray.tmax;
-      float best_t = ray.tmax, bu = 0, bv = 0;
-      std::int32_t best = -1;
-      bool found = false;
-      std::uint32_t visited = 0, lr = 0, node_index = 0;
-      float tmp;
-      bool hits_any = slab(nodes[0], ro, inv, maxt, tmp);
-      bool done = false;
-      while (hits_any && !done) {
-        ref_node current = nodes[node_index];
-        while (!(current.type_and_parent & 0x80000000u)) {
-          float tl, tr;
-          ref_node const& fc = nodes[current.first];
-          ref_node const& sc = nodes[current.second];
-          bool const hl = slab(fc, ro, inv, maxt, tl);
-          bool const hr = slab(sc, ro, inv, maxt, tr);
-          if (!hl && !hr) break;
-          bool const use_right = !hl || (hr && tl >= tr);
-          lr = std::uint32_t(use_right) | (lr << 1);
-          visited = std::uint32_t(hl && hr) | (visited << 1);
-          node_index = use_right ? current.second : current.first;
-          current = nodes[node_index];
+      query_hit best{false, -1, ray.tmax, 0.f, 0.f};
+      for (std::size_t i = 0; i < n_drawables; ++i) {
+        std::uint32_t const* d = dw + 40 * i;
+        if (d[36] == 0) continue;
+        float inv[16];
+        std::memcpy(inv, d + 16, 64);
+        ray8 const obj{mat4_apply(inv, ray.o, 1.0f), ray.tmin, mat4_apply(inv, ray.d, 0.0f), ray.tmax};
+        query_hit const q = refbvh_closest(nodes + d[32], bvh_idx + d[33], indices + d[34], points_xyzw + 4 * size_t(d[35]),
+            obj, any_hit, 1, isect);
+        if (!q.found) continue;
+        std::int32_t const gp = prim_base[i] + q.prim;
+        if (any_hit) {
+          best = {true, gp, q.t, q.u, q.v};
+          break;
         }
-        if (current.type_and_parent & 0x80000000u) {
-          for (std::uint32_t tri = current.first; tri <= current.second; ++tri) {
-            std::uint32_t const pi = bvh_idx[tri];
-            float t, u, v;
-            bool h = isect < 0 ? isect_reference(ro, rd, pt(indices[3 * pi]), pt(indices[3 * pi + 1]),
-                                     pt(indices[3 * pi + 2]), t, u, v)
-                               : test_tri(isect, wt, ray, pt(indices[3 * pi]), pt(indices[3 * pi + 1]),
-                                     pt(indices[3 * pi + 2]), t, u, v);
-            h = h && t < maxt && (canonical ? canonical_better(t, std::int32_t(pi), best_t, best) : best_t > t);
-            if (h) {
-              best_t = t;
-              bu = u;
-              bv = v;
-              best = std::int32_t(pi);
-              found = true;
-              maxt = canonical ? std::nextafter(t, std::numeric_limits<float>::infinity()) : t;
-              if (any_hit) {
-                done = true;
-                break;
-              }
-            }
-          }
-          if (done) break;
-        }
-        while ((visited & 1u) != 1u) {
-          if (visited == 0) {
-            done = true;
-            break;
-          }
-          node_index = nodes[node_index].type_and_parent & 0x7fffffffu;
-          visited >>= 1;
-          lr >>= 1;
-        }
-        if (done) break;
-        std::uint32_t const parent = nodes[node_index].type_and_parent & 0x7fffffffu;
-        node_index = (lr & 1u) ? nodes[parent].first : nodes[parent].second;
-        visited ^= 1u;
+        if (!best.found || canonical_better(q.t, gp, best.t, best.prim)) best = {true, gp, q.t, q.u, q.v};
       }
-      prim[r] = found ? best : -1;
-      t_out[r] = found ? best_t : ray.tmax;
-      u_out[r] = found ? bu : 0.f;
-      v_out[r] = found ? bv : 0.f;
+      prim[r] = best.found ? best.prim : -1;
+      t_out[r] = best.found ? best.t : ray.tmax;
+      u_out[r] = best.found ? best.u : 0.f;
+      v_out[r] = best.found ? best.v : 0.f;
     }
   });
 }

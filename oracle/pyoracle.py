@@ -42,6 +42,7 @@ def oracle() -> C.CDLL:
             "orc_refbvh_traverse": (None, [P, P, P, P, P, SZ, I, I, P, P, P, P, I]),
             "orc_bvh8_traverse": (None, [P, P, P, SZ, I, I, P, P, P, P, P, P, P, I]),
             "orc_brute_closest": (None, [P, SZ, P, SZ, I, P, P, P, P, I]),
+            "orc_instanced_query": (None, [P, P, P, P, P, SZ, P, SZ, I, I, P, P, P, P, I]),
             "orc_host_rng": (None, [C.c_uint32, I, I, P, P]),
             "orc_render_reference": (None, [SZ, P, P, P, P, P, SZ, P, P, P, I, I, I, I, C.c_uint32, P, P, P, P, P,
                                             P, P, P, P, P, I, I, C.c_float, I, I, P, P, P, I, I, C.c_float,
@@ -81,6 +82,9 @@ def ref() -> C.CDLL:
         sig = {
             "ref_bvh_build": (P, [P, SZ, P, SZ, I]),
             "ref_bvh_free": (None, [P]),
+            "ref_bvh_aabb": (None, [P, P]),
+            "ref_bvh_build_instances": (P, [P, P, SZ]),
+            "ref_glsl_traverse_instanced": (None, [P, P, P, P, P, P, P, P, SZ, I, P, P, P, P, P, I]),
             "ref_bvh_node_count": (SZ, [P]),
             "ref_bvh_index_count": (SZ, [P]),
             "ref_bvh_nodes": (None, [P, P]),
@@ -223,6 +227,119 @@ def ref_glsl_traverse(nodes, bvh_indices, indices, points, rays, any_hit=False, 
     L.ref_glsl_traverse(nodes.ctypes.data, bvh_indices.ctypes.data, indices.ctypes.data, p4.ctypes.data,
                         r.ctypes.data, r.shape[0], int(any_hit), *[o.ctypes.data for o in out], threads or nthreads())
     return _pack(*out)
+
+
+# ---- instanced scenes: two-level walks (pt_trace.comp:284-309) ---------------
+def _geometries(scene):
+    """Distinct geometries of a scene's drawables, keyed like the reference's
+    push_geometry results: (indices_base, points_base, index_count) -> slot;
+    and per drawable its slot and first global prim id."""
+    keys, slot, base, acc = {}, [], [], 0
+    for d in scene["drawables"]:
+        k = (int(d.indices_base_index), int(d.points_base_index), int(d.index_count))
+        slot.append(keys.setdefault(k, len(keys)))
+        base.append(acc)
+        acc += k[2] // 3
+    return list(keys), np.array(slot, np.int64), np.array(base, np.int64)
+
+
+def _points4(scene):
+    v = np.asarray(scene["vertices"], np.float32)
+    p4 = np.zeros((v.shape[0], 4), np.float32)
+    p4[:, :3] = v[:, :3]
+    return p4
+
+
+def instanced_closest(scene: dict, rays, any_hit=False, isect=0):
+    """The oracle's restatement of the instanced query (orc_instanced_query):
+    per drawable, the ray in object space through the restated reference tree
+    of its geometry; canonical ties on global prim ids. Returns hits (closest)
+    or a bool array (any hit)."""
+    L = oracle()
+    idx = np.ascontiguousarray(scene["indices"], np.uint32)
+    p4 = _points4(scene)
+    geoms, _, _ = _geometries(scene)
+    node_blocks, idx_blocks, bases = [], [], {}
+    nn = ni = 0
+    for (ib, pb, cnt) in geoms:
+        local = np.ascontiguousarray(idx[ib:ib + cnt])
+        pts = np.ascontiguousarray(p4[pb:, :3])
+        nodes, bi = refbvh_build(local, pts)
+        bases[(ib, pb, cnt)] = (nn, ni)
+        node_blocks.append(nodes)
+        idx_blocks.append(bi)
+        nn += nodes.shape[0]
+        ni += bi.size
+    nodes = np.ascontiguousarray(np.concatenate(node_blocks), np.uint32)
+    bi = np.ascontiguousarray(np.concatenate(idx_blocks), np.uint32)
+    dr = _drawables_with_bases(scene, bases)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    out = _hits(r.shape[0])
+    L.orc_instanced_query(nodes.ctypes.data, bi.ctypes.data, idx.ctypes.data, p4.ctypes.data, dr.ctypes.data,
+                          len(scene["drawables"]), r.ctypes.data, r.shape[0], int(any_hit), int(isect),
+                          *[o.ctypes.data for o in out], nthreads())
+    h = _pack(*out)
+    return h["prim"] >= 0 if any_hit else h
+
+
+def _drawables_with_bases(scene, bases) -> np.ndarray:
+    """The drawables as 40-word records with bvh_node_base_index and
+    bvh_index_base_index pointing at their geometry's tree."""
+    import ctypes as _C
+    n = len(scene["drawables"])
+    raw = np.frombuffer(_C.string_at(_C.addressof(scene["drawables"]), 160 * n), np.uint32).reshape(n, 40).copy()
+    for i, d in enumerate(scene["drawables"]):
+        nb, ib = bases[(int(d.indices_base_index), int(d.points_base_index), int(d.index_count))]
+        raw[i, 32], raw[i, 33] = nb, ib
+    return raw
+
+
+def ref_instanced(scene: dict, rays, any_hit=False, threads=None):
+    """The reference's own instanced query (oracle/_ref): geometry trees built
+    by bvh.cpp with split_aabbs (scene::push_geometry), the tree over the
+    drawables' world boxes with dont_split (scene::enqueue / prepare), walked
+    by the compiled bvh.impl.glsl + visit_object_aabb. Returns (drawable,
+    local prim, hits with global prim ids)."""
+    L = ref()
+    idx = np.ascontiguousarray(scene["indices"], np.uint32)
+    p4 = _points4(scene)
+    geoms, slot, base = _geometries(scene)
+    node_blocks, idx_blocks, bases, boxes = [], [], {}, []
+    nn = ni = 0
+    for (ib, pb, cnt) in geoms:
+        local = np.ascontiguousarray(idx[ib:ib + cnt])
+        pts = np.ascontiguousarray(p4[pb:, :3])
+        h = ref_bvh(local, pts, split=True)
+        nodes, bi = ref_bvh_arrays(h)
+        box = np.zeros(6, np.float32)
+        L.ref_bvh_aabb(h, box.ctypes.data)
+        L.ref_bvh_free(h)
+        bases[(ib, pb, cnt)] = (nn, ni)
+        node_blocks.append(nodes)
+        idx_blocks.append(bi)
+        boxes.append(box)
+        nn += nodes.shape[0]
+        ni += bi.size
+    onodes = np.ascontiguousarray(np.concatenate(node_blocks), np.uint32)
+    obi = np.ascontiguousarray(np.concatenate(idx_blocks), np.uint32)
+    dr = _drawables_with_bases(scene, bases)
+    dboxes = np.ascontiguousarray(np.stack([boxes[k] for k in slot]), np.float32)
+    xf = np.ascontiguousarray(dr[:, 0:16].view(np.float32))
+    th = L.ref_bvh_build_instances(dboxes.ctypes.data, xf.ctypes.data, dr.shape[0])
+    gnodes, gbi = ref_bvh_arrays(th)
+    L.ref_bvh_free(th)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = r.shape[0]
+    geom = np.empty(n, np.int32)
+    out = _hits(n)
+    L.ref_glsl_traverse_instanced(gnodes.ctypes.data, gbi.ctypes.data, onodes.ctypes.data, obi.ctypes.data,
+                                  idx.ctypes.data, p4.ctypes.data, dr.ctypes.data, r.ctypes.data, n, int(any_hit),
+                                  geom.ctypes.data, *[o.ctypes.data for o in out], threads or nthreads())
+    h = _pack(*out)
+    local = h["prim"].copy()
+    hit = geom >= 0
+    h["prim"][hit] = (base[geom[hit]] + local[hit]).astype(np.int32)
+    return geom, local, h
 
 
 # ---- scene baking (numpy, independent of the product's C++ bake) -----------

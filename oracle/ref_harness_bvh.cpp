@@ -7,6 +7,12 @@
 //                         (bvh.cpp:136-161, :356-512), split = dont_split or
 //                         split_aabbs exactly as scene::push_geometry uses it
 //                         (scene.cpp:60-62).
+//   ref_bvh_aabb       -> bvh::aabb (bvh.cpp:554-556), the box scene::enqueue
+//                         transforms for the tree over the drawables.
+//   ref_bvh_build_instances -> scene::enqueue's world boxes (scene.cpp:255-271:
+//                         the 8 corners of the geometry's box under the
+//                         drawable's transformation) and scene::prepare's
+//                         bvh(m_drawable_aabbs, dont_split) (scene.cpp:336-340).
 //   ref_pick_closest   -> scene::pick (scene.cpp:273-314) for one drawable with
 //                         an identity transform: the reference generator
 //                         traversal bvh::traverse (bvh.cpp:237-346) feeding
@@ -47,6 +53,36 @@ void* ref_bvh_build(std::uint32_t const* indices, std::size_t n_indices, float c
 }
 
 void ref_bvh_free(void* p) { delete static_cast<ref_bvh_handle*>(p); }
+
+void ref_bvh_aabb(void* p, float* lo_hi) {
+  myrt::aabb_t const b = static_cast<ref_bvh_handle*>(p)->bvh->aabb();
+  for (int k = 0; k < 3; ++k) {
+    lo_hi[k] = b.min[k];
+    lo_hi[3 + k] = b.max[k];
+  }
+}
+
+// boxes: per drawable its geometry's box (min xyz, max xyz); transforms: the
+// drawables' column-major 4x4 transformation. The corner products are summed
+// left to right (the reference multiplies with rnu, which is not vendored).
+void* ref_bvh_build_instances(float const* boxes, float const* transforms, std::size_t n) {
+  auto* h = new ref_bvh_handle;
+  std::vector<myrt::aabb_t> aabbs(n);
+  for (std::size_t d = 0; d < n; ++d) {
+    float const* b = boxes + 6 * d;
+    float const* m = transforms + 16 * d;
+    myrt::aabb_t transformed;
+    for (unsigned i = 0; i < 8; ++i) {
+      float const p[3] = {b[(i & 1) ? 3 : 0], b[(i & 2) ? 4 : 1], b[(i & 4) ? 5 : 2]};
+      rnu::vec3 q;
+      for (int r = 0; r < 3; ++r) q[r] = ((m[r] * p[0] + m[4 + r] * p[1]) + m[8 + r] * p[2]) + m[12 + r] * 1.0f;
+      transformed.enclose(q);
+    }
+    aabbs[d] = transformed;
+  }
+  h->bvh = std::make_unique<myrt::bvh>(std::span<myrt::aabb_t const>(aabbs), myrt::dont_split);
+  return h;
+}
 
 std::size_t ref_bvh_node_count(void* p) { return static_cast<ref_bvh_handle*>(p)->bvh->nodes().size(); }
 

@@ -8,7 +8,8 @@
 //   src/pt/intersect.glsl:3-39      (Moller-Trumbore, ray/sphere)
 //   src/pt/bvh.glsl:31-55           (slab test, node accessors)
 //   src/pt/bvh.impl.glsl:8-72       (stackless bit-trail traversal)
-//   src/pt/pt_trace.comp:229-282    (closest / any-hit triangle visitor)
+//   src/pt/pt_trace.comp:229-309    (closest / any-hit triangle visitor and the
+//                                    instance visitor visit_object_aabb)
 //   src/pt/ggx.glsl, pbr.glsl, color.glsl, transform.glsl
 //   src/pt/material_new.glsl        (after the same text substitution that
 //                                    material_registry::push_type applies,
@@ -80,13 +81,33 @@ bvh_node_t const* bvh_nodes = nullptr;
 uint const* bvh_indices = nullptr;
 uint const* indices = nullptr;
 vec4 const* points = nullptr;
+// pt_trace.comp:34-47, :91-92: drawables and the tree over their world boxes
+#include "pt_trace_geometry.glsl"
+static_assert(sizeof(drawable_geometry_t) == 160, "std430 drawable layout");
+drawable_geometry_t const* geometries = nullptr;
+bvh_node_t const* global_bvh_nodes = nullptr;
+uint const* global_bvh_indices = nullptr;
 
 #define MYRT_BVH_NODES_BUFFER bvh_nodes
 #define MYRT_BVH_INDICES_BUFFER bvh_indices
 #define MYRT_BVH_TRAVERSE bvh_traverse
 #define MYRT_BVH_VISIT_PRIMITIVE visit_triangle
 #include "bvh.impl.glsl"
+#undef MYRT_BVH_VISIT_PRIMITIVE
+#undef MYRT_BVH_TRAVERSE
+#undef MYRT_BVH_INDICES_BUFFER
+#undef MYRT_BVH_NODES_BUFFER
 #include "pt_trace_visitor.glsl"
+// the second instantiation, as pt_trace.comp:108-116
+#define MYRT_BVH_NODES_BUFFER global_bvh_nodes
+#define MYRT_BVH_INDICES_BUFFER global_bvh_indices
+#define MYRT_BVH_TRAVERSE bvh_traverse_global
+#define MYRT_BVH_VISIT_PRIMITIVE visit_object_aabb
+#include "bvh.impl.glsl"
+#undef MYRT_BVH_VISIT_PRIMITIVE
+#undef MYRT_BVH_TRAVERSE
+#undef MYRT_BVH_INDICES_BUFFER
+#undef MYRT_BVH_NODES_BUFFER
 
 // ---- SDF: raymarch.glsl and the instruction snippets of sdf.hpp ---------------
 // Records of pt_trace.comp:49-66.
@@ -309,6 +330,52 @@ void ref_glsl_traverse(void const* nodes, std::uint32_t const* node_indices, std
       t_out[r] = h ? traversal.t : maxt;
       u_out[r] = h ? traversal.barycentric.x : 0.f;
       v_out[r] = h ? traversal.barycentric.y : 0.f;
+    }
+  };
+  if (nthreads <= 1) {
+    work(0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  std::size_t const per = (n + std::size_t(nthreads) - 1) / std::size_t(nthreads);
+  for (int i = 0; i < nthreads; ++i) {
+    std::size_t const b = std::size_t(i) * per, e = std::min(n, b + per);
+    if (b < e) pool.emplace_back(work, b, e);
+  }
+  for (auto& th : pool) th.join();
+}
+
+// The instanced query of nearest_hit / any_hit (pt_trace.comp:311-341, mesh
+// part): bvh_traverse_global over the tree of the drawables' world boxes, whose
+// visitor visit_object_aabb moves the ray into each drawable's object space and
+// walks its geometry tree (node / index bases from the drawable record). Outputs
+// per ray the drawable (hit_geometry), the triangle's index in its geometry
+// (global_hit_index), t and the barycentrics; geometry -1 = miss.
+void ref_glsl_traverse_instanced(void const* global_nodes, std::uint32_t const* global_indices,
+    void const* object_nodes, std::uint32_t const* object_indices, std::uint32_t const* tri_indices,
+    float const* points_xyzw, void const* drawables, float const* rays, std::size_t n, int any_hit,
+    std::int32_t* geometry, std::int32_t* prim, float* t_out, float* u_out, float* v_out, int nthreads) {
+  global_bvh_nodes = static_cast<bvh_node_t const*>(global_nodes);
+  global_bvh_indices = global_indices;
+  bvh_nodes = static_cast<bvh_node_t const*>(object_nodes);
+  bvh_indices = object_indices;
+  indices = tri_indices;
+  points = reinterpret_cast<vec4 const*>(points_xyzw);
+  geometries = static_cast<drawable_geometry_t const*>(drawables);
+  auto work = [=](std::size_t begin, std::size_t end) {
+    for (std::size_t r = begin; r < end; ++r) {
+      float const* q = rays + 8 * r;
+      float const maxt = q[7];
+      traversal_init();
+      traversal.any_hit = any_hit != 0;
+      traversal.t = maxt;
+      traversal.global_t = maxt;
+      bool const h = bvh_traverse_global(0, 0, vec3(q[0], q[1], q[2]), vec3(q[4], q[5], q[6]), maxt);
+      geometry[r] = h ? std::int32_t(traversal.hit_geometry) : -1;
+      prim[r] = h ? std::int32_t(traversal.global_hit_index) : -1;
+      t_out[r] = h ? traversal.global_t : maxt;
+      u_out[r] = h ? traversal.global_barycentric.x : 0.f;
+      v_out[r] = h ? traversal.global_barycentric.y : 0.f;
     }
   };
   if (nthreads <= 1) {

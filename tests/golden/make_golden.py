@@ -1,7 +1,8 @@
 """Generates the golden fixtures in tests/golden/ from the reference's own code.
 
 Run in a container that has the reference tree (it builds oracle/_ref first):
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            (all fixtures)
+    python tests/golden/make_golden.py instanced  (instanced_field.npz only)
 
 Every output comes from code compiled from the reference's sources
 (oracle/_ref/libmyrt_ref.so; see oracle/build_ref.py), never from the oracle
@@ -18,6 +19,14 @@ Fixtures:
                     (scene::pick over bvh::traverse + ray_t::intersect) and from
                     its GLSL traversal (bvh.impl.glsl + pt_trace.comp visitor),
                     closest and any-hit.
+  instanced_field.npz  an instanced scene (48 icospheres and 24 boxes under
+                    random rotations, non-uniform scales and translations, plus
+                    a floor): 6,912 camera rays and 2,048 random rays through the
+                    reference's two-level walk -- geometry trees by bvh.cpp with
+                    split_aabbs (scene::push_geometry), the tree over the
+                    drawables' world boxes with dont_split (scene::prepare),
+                    bvh.impl.glsl with visit_object_aabb (pt_trace.comp:284-309)
+                    -- closest and any-hit (shadow rays with finite tmax).
   glsl_kat.npz      known answers of random.glsl, intersect.glsl,
                     transform.glsl, color.glsl and the PBR material
                     (pbr.glsl / ggx.glsl / material_new.glsl) on seeded inputs.
@@ -230,6 +239,7 @@ def main() -> int:
             sk[f"trace{anyh}_{k}"] = v
     np.savez_compressed(OUT / "sdf_kat.npz", **sk)
     make_post_kat()
+    make_instanced()
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
     return 0
@@ -246,6 +256,37 @@ POST_CASES = [  # (name, op, i, p): the reference's post-processing shaders
     ("tonemap", 4, (0, 0, 0), (0.0, 0.0, 0.0, 0.0)),
     ("fxaa", 5, (0, 0, 0), (0.0, 0.0, 0.0, 0.0)),
 ]
+
+
+def make_instanced() -> None:
+    """instanced_field.npz (see the module docstring)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    from myrt_b200.scenes import instanced_field
+
+    sc = instanced_field()
+    cam = pinhole_rays(96, 72, eye=(0.3, 1.5, -3.5), target=(0.0, -0.2, 0.0), vfov_deg=55)
+    rng = np.random.default_rng(41)
+    n = 2048
+    o = rng.uniform(-2.5, 2.5, (n, 3))
+    tgt = rng.uniform(-1.0, 1.0, (n, 3))
+    d = tgt - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rnd = np.zeros((n, 8), np.float32)
+    rnd[:, 0:3], rnd[:, 4:7], rnd[:, 7] = o, d, np.inf
+    rays = np.concatenate([cam, rnd], 0)
+    geom, local, hits = po.ref_instanced(sc, rays)
+    sh = rays.copy()
+    # just past the first hit (occluded) on even rays, halfway to it on odd rays, 2.0 on misses
+    scale = np.where(np.arange(sh.shape[0]) % 2 == 0, 1.001, 0.5)
+    sh[:, 7] = np.where(hits["prim"] >= 0, hits["t"] * scale, 2.0).astype(np.float32)
+    sgeom, _, shadow = po.ref_instanced(sc, sh, any_hit=True)
+    raw = po._drawables_with_bases(sc, {k: (0, 0) for k in po._geometries(sc)[0]})
+    raw[:, 32:34] = 0
+    np.savez_compressed(OUT / "instanced_field.npz", indices=sc["indices"], vertices=sc["vertices"],
+                        drawables=raw, rays=rays, drawable=geom, local_prim=local, hits=hits, shadow_rays=sh,
+                        shadow_hit=sgeom >= 0)
 
 
 def make_post_kat() -> None:
@@ -269,5 +310,8 @@ def make_post_kat() -> None:
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "post":
         make_post_kat()
+        sys.exit(0)
+    if len(sys.argv) > 1 and sys.argv[1] == "instanced":
+        make_instanced()
         sys.exit(0)
     sys.exit(main())

@@ -247,3 +247,48 @@ def test_guided_rendering_beats_bsdf_sampling(ctx):
         e_guided.append(_rel_rmse(guided, ref))
     print("relRMSE plain", e_plain, "guided", e_guided)
     assert np.mean(e_guided) < 0.6 * np.mean(e_plain)
+
+
+@pytest.mark.gpu
+def test_tensor_core_wait_timeout_reports_and_context_recovers(ctx):
+    """The first mbarrier wait of every CTA of the forward and training kernels
+    is pointed at a barrier nothing arrives at (guide_stall_test) with a limit
+    of 64 polls: each CTA gives up, drains its MMA in flight, frees its TMEM and
+    returns; myrt_sync reports MYRT_ERR_DEVICE_ABORT with the guide timeout bit
+    (1 << 5). With the default tuning the same context then evaluates and trains
+    normally, with results equal to those before the stall."""
+    import myrt_b200 as mb
+
+    rng = np.random.default_rng(12)
+    _small_box(ctx)
+    ctx.guide_reset()
+    _sharpen(ctx, rng)
+    pts = _points(rng, 700)
+    ref = ctx.guide_eval(pts)
+    ctx.sync()
+    n = 512
+    s = np.zeros((n, 16), np.float32)
+    q = _points(rng, n)
+    s[:, 0:3], s[:, 4:7], s[:, 8:11] = q[:, 0:3], q[:, 4:7], q[:, 8:11]
+    s[:, 3] = 1.0
+    s[:, 12:15] = _unit(rng.normal(size=(n, 3)))
+    g_ref, loss_ref = ctx.guide_gradients(s)
+    ctx.sync()
+    try:
+        ctx.set_tuning(guide_poll_limit=64, guide_stall_test=1)
+        ctx.guide_eval(pts)
+        with pytest.raises(mb.MyrtError, match="0x00000020") as e:
+            ctx.sync()
+        assert e.value.code == mb.MYRT_ERR_DEVICE_ABORT
+        ctx.guide_gradients(s)
+        with pytest.raises(mb.MyrtError, match="0x00000020"):
+            ctx.sync()
+    finally:
+        ctx.set_tuning()
+    ctx.sync()  # the error word was cleared by the report
+    assert np.array_equal(ctx.guide_eval(pts), ref)
+    g, loss = ctx.guide_gradients(s)
+    ctx.sync()
+    # per-warp bias sums meet in shared-memory atomics, so the last bits may move
+    np.testing.assert_allclose(g, g_ref, rtol=1e-5, atol=1e-7)
+    assert abs(loss - loss_ref) <= 1e-5 * abs(loss_ref)
