@@ -577,6 +577,26 @@ int myrt_set_seed(myrt_ctx* ctx, uint32_t seed);
 int myrt_render_noalloc(myrt_ctx* ctx, const myrt_camera* camera, const myrt_render_params* params,
     uint32_t sample_index, float* accum_rgba, float* display_rgba, void* stream);
 
+/* The GLSL built-ins as the library computes them in the reference shading
+ * (pt_generate / pt_color / pbr.glsl: sin, cos, atan, pow), the forward
+ * preview's resolve and the post-processing passes (exp, pow). No counterpart
+ * in the reference, whose GL driver supplies its own (GLSL leaves their
+ * precision to the implementation). They are defined in
+ * myrt_b200/csrc/glmath.hpp with IEEE-exact operations only, so a host build of
+ * that header (-ffp-contract=off) gives the same bits; this call evaluates them
+ * on the context's device: out[i] = fn(x[i]) or pow(x[i], y[i]). Host arrays
+ * of n floats (y only for MYRT_GLSL_POW). Accuracy against the exact values:
+ * sin / cos <= 2 ulp for |x| < 1e5, atan <= 2.5 ulp, exp <= 1 ulp,
+ * pow <= 4.5 ulp. Synchronous. */
+typedef enum myrt_glsl_fn {
+  MYRT_GLSL_SIN = 0,
+  MYRT_GLSL_COS = 1,
+  MYRT_GLSL_ATAN = 2,
+  MYRT_GLSL_EXP = 3,
+  MYRT_GLSL_POW = 4
+} myrt_glsl_fn;
+int myrt_glsl_builtins(myrt_ctx* ctx, int fn, const float* x, const float* y, uint32_t n, float* out);
+
 /* Waits for the context's work and returns MYRT_ERR_DEVICE_ABORT if a kernel
  * stopped at a limit since the last call (the error word is then cleared). */
 int myrt_sync(myrt_ctx* ctx);

@@ -242,6 +242,19 @@ class Context:
     def sync(self):
         self._check(self._L.myrt_sync(self._h), "myrt_sync")
 
+    GLSL_FUNCTIONS = {"sin": 0, "cos": 1, "atan": 2, "exp": 3, "pow": 4}
+
+    def glsl_builtin(self, name: str, x, y=None) -> np.ndarray:
+        """myrt_glsl_builtins: the library's GLSL built-in `name` on the device."""
+        xs = np.ascontiguousarray(x, np.float32).ravel()
+        ys = None if y is None else np.ascontiguousarray(np.broadcast_to(np.float32(y) if np.isscalar(y) else y,
+                                                                          xs.shape), np.float32).ravel()
+        out = np.empty_like(xs)
+        self._check(self._L.myrt_glsl_builtins(self._h, self.GLSL_FUNCTIONS[name], xs.ctypes.data,
+                                               None if ys is None else ys.ctypes.data, xs.size, out.ctypes.data),
+                    "myrt_glsl_builtins")
+        return out
+
     # -- wavefront rendering (sequential_pathtracer::run) --
     def render(self, inverse_view, inverse_projection, width: int, height: int, num_bounces: int = 10,
                frames: int = 1, shading: int = _abi.SHADE_REFERENCE, sdf_marching_steps: int = 400,

@@ -210,6 +210,7 @@ SIGNATURES = {
     "myrt_set_seed": (I, [P, C.c_uint32]),
     "myrt_render_noalloc": (I, [P, C.POINTER(myrt_camera), C.POINTER(myrt_render_params), C.c_uint32, P, P, P]),
     "myrt_sync": (I, [P]),
+    "myrt_glsl_builtins": (I, [P, I, P, P, U32, P]),
 }
 
 _lib = None

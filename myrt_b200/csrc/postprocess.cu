@@ -15,9 +15,9 @@
 // ((w00 t00 + w10 t10) + w01 t01) + w11 t11 with w00 = (1 - a)(1 - b),
 // w10 = a (1 - b), w01 = (1 - a) b, w11 = a b. The linear_scale blit samples
 // the source at the destination pixel centres with the same filter and
-// clamp-to-edge wrapping. This unit is compiled without FMA contraction, so a
-// host restatement reproduces every pass except for the exp / pow of
-// denoise and tonemap (CUDA's expf / powf against the host libm).
+// clamp-to-edge wrapping. This unit is compiled without FMA contraction, and
+// the exp / pow of denoise and tonemap are the library's GLSL built-ins
+// (glmath.hpp), so a host restatement reproduces every pass bit for bit.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -25,6 +25,7 @@
 
 #include "../../include/myrt_cuda.h"
 #include "ctx.hpp"
+#include "glmath.hpp"
 
 namespace myrt_b200 {
 namespace {
@@ -85,11 +86,11 @@ struct pass_args {
 // pp_denoise.comp: bilateral filter, 9 x 9 window (MSIZE 10), spatial sigma
 // = exponent, range sigma = strength.
 __device__ __forceinline__ float normpdf(float x, float sigma) {
-  return 0.39894f * expf(((-0.5f * x) * x) / (sigma * sigma)) / sigma;
+  return 0.39894f * myrt_glmath::exp(((-0.5f * x) * x) / (sigma * sigma)) / sigma;
 }
 __device__ __forceinline__ float normpdf3(float3 v, float sigma) {
   float const d = (v.x * v.x + v.y * v.y) + v.z * v.z;
-  return 0.39894f * expf((-0.5f * d) / (sigma * sigma)) / sigma;
+  return 0.39894f * myrt_glmath::exp((-0.5f * d) / (sigma * sigma)) / sigma;
 }
 __global__ void k_pp_denoise(pass_args a) {
   int const x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
@@ -164,7 +165,7 @@ __global__ void k_pp_add(pass_args a) {
 __device__ __forceinline__ float filmic(float x) {
   float const X = fmaxf(0.f, x - 0.004f);
   float const r = (X * (6.2f * X + 0.5f)) / (X * (6.2f * X + 1.7f) + 0.06f);
-  return powf(r, 1.3f);
+  return myrt_glmath::pow(r, 1.3f);
 }
 __global__ void k_pp_tonemap(pass_args a) {
   int const x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;

@@ -6,11 +6,14 @@
 //   (src/material.hpp:39-65) for the single PBR type (7 floats).
 // This translation unit is compiled with -fmad=false so every + and * rounds
 // separately, as the GLSL reads; random draws happen in the left-to-right
-// order GLSL defines for arguments. Transcendentals are CUDA's sinf, cosf,
-// atanf, powf; sqrt and division are IEEE.
+// order GLSL defines for arguments. The transcendentals sin, cos, atan and
+// pow are this library's GLSL built-ins (glmath.hpp), which the CPU oracle
+// evaluates to the same bits; sqrt and division are IEEE.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+
+#include "glmath.hpp"
 
 namespace myrt_b200 {
 namespace rs {
@@ -114,7 +117,7 @@ __device__ __forceinline__ v2 random_uniform_circle(rng_t& r, float radius) {
   float const a = random_next(r) * 2.f * 3.1415926535897f;
   float const b = random_next(r);
   float const s = sqrtf(b) * radius;
-  return {s * sinf(a), s * cosf(a)};
+  return {s * myrt_glmath::sin(a), s * myrt_glmath::cos(a)};
 }
 
 // ---- ggx.glsl / pbr.glsl / transform.glsl ----------------------------------------
@@ -128,12 +131,12 @@ __device__ __forceinline__ float ggx_distribution(v3 n, v3 h, float alpha) {
 __device__ __forceinline__ v2 ggx_importance_sample(v2 rsm, float roughness) {
   float const phi = rsm.y * 2.f * kPi;
   float const rough2 = roughness * roughness;
-  float const theta = atanf(sqrtf(rough2 * rsm.x / (1.f - rsm.x)));
+  float const theta = myrt_glmath::atan(sqrtf(rough2 * rsm.x / (1.f - rsm.x)));
   return {phi, theta};
 }
 __device__ __forceinline__ v3 sample_hemisphere(v2 is) {
-  float const c = cosf(is.y), s = sinf(is.y);
-  return {s * cosf(is.x), s * sinf(is.x), c};
+  float const c = myrt_glmath::cos(is.y), s = myrt_glmath::sin(is.y);
+  return {s * myrt_glmath::cos(is.x), s * myrt_glmath::sin(is.x), c};
 }
 __device__ __forceinline__ v3 transform_local_to_world(v3 v, v3 n) {
   v3 perp{1.f, 0.f, 0.f};
@@ -154,7 +157,7 @@ __device__ __forceinline__ v3 transform_local_to_world(v3 v, v3 n) {
 __device__ __forceinline__ float fresnel(float cos_theta, float ior_in, float ior_out, float metallic) {
   float f0 = fabsf((ior_in - ior_out) / (ior_in + ior_out));
   f0 = mixf(f0 * f0, 1.f, metallic);
-  return f0 + (1.f - f0) * powf(1.f - cos_theta, 5.f);
+  return f0 + (1.f - f0) * myrt_glmath::pow(1.f - cos_theta, 5.f);
 }
 __device__ __forceinline__ v3 nreflect(v3 tv, v3 n, v3 mn) {
   v3 ray = reflect(-tv, mn);
@@ -354,7 +357,7 @@ __device__ __forceinline__ void mat_evaluate(material_ctx& mc, v3 n, v3 tl, v3 t
   if ((mc.tex_x != 0u || mc.tex_y != 0u) && mc.tex_y == 0u && mc.tex_x <= uint32_t(n_textures) && textures &&
       textures[mc.tex_x - 1u].p) {
     float4 const c = tex_sample(textures[mc.tex_x - 1u], uv.x, 1.f - uv.y);
-    mc.mat.color = {powf(c.x, 2.2f), powf(c.y, 2.2f), powf(c.z, 2.2f)};
+    mc.mat.color = {myrt_glmath::pow(c.x, 2.2f), myrt_glmath::pow(c.y, 2.2f), myrt_glmath::pow(c.z, 2.2f)};
   }
   bool const incoming = dot(n, -tv) < 0.f;
   float const i1 = incoming ? 1.f : mc.mat.ior;

@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kBlock) k_generate(uint32_t W, uint32_t H, flo
   float const a = rs::random_next(r) * 2.f * 3.1415926535897f;
   float const b = rs::random_next(r);
   float const s = sqrtf(b) * 0.7071067812f;
-  v2 const off{s * sinf(a), s * cosf(a)};
+  v2 const off{s * myrt_glmath::sin(a), s * myrt_glmath::cos(a)};
   float const nx = ((off.x + float(x)) / float(W)) * 2.f - 1.f;
   float const ny = ((off.y + float(y)) / float(H)) * 2.f - 1.f;
   float h[3];

@@ -15,6 +15,7 @@
 // (post_process.cpp:41-55, OpenGL 4.6 section 8.14.2): bilinear at level 0,
 // GL_MIRRORED_REPEAT, and every pass storing RGBA16F (round to nearest even).
 // Compiled with -ffp-contract=off: every + and * rounds separately.
+#include "oracle_glsl_math.hpp"
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -86,10 +87,10 @@ f4 bilinear(img const& t, float s, float tt, bool mirrored) {
   return add(add(add(mul(w00, t00), mul(w10, t10)), mul(w01, t01)), mul(w11, t11));
 }
 
-float normpdf(float x, float sigma) { return 0.39894f * std::exp(((-0.5f * x) * x) / (sigma * sigma)) / sigma; }
+float normpdf(float x, float sigma) { return 0.39894f * orc_glsl::exp(((-0.5f * x) * x) / (sigma * sigma)) / sigma; }
 float normpdf3(float vx, float vy, float vz, float sigma) {
   float const d = (vx * vx + vy * vy) + vz * vz;
-  return 0.39894f * std::exp((-0.5f * d) / (sigma * sigma)) / sigma;
+  return 0.39894f * orc_glsl::exp((-0.5f * d) / (sigma * sigma)) / sigma;
 }
 float clamp01(float v) { return std::fmin(std::fmax(v, 0.f), 1.f); }
 
@@ -145,7 +146,7 @@ f4 cutoff(img const& in, int x, int y, float const* value, int leave_above) {
 float filmic(float x) {
   float const X = std::fmax(0.f, x - 0.004f);
   float const r = (X * (6.2f * X + 0.5f)) / (X * (6.2f * X + 1.7f) + 0.06f);
-  return std::pow(r, 1.3f);
+  return orc_glsl::pow(r, 1.3f);
 }
 
 float luma(f4 c) { return (c.x * 0.299f + c.y * 0.587f) + c.z * 0.114f; }

@@ -28,6 +28,8 @@
 #include <cstring>
 #include <limits>
 #include <random>
+
+#include "oracle_glsl_math.hpp"
 #include <thread>
 #include <vector>
 
@@ -142,7 +144,7 @@ inline v2 random_uniform_circle(rng_t& r, float radius) {
   float const a = random_next(r) * 2.f * 3.1415926535897f;
   float const b = random_next(r);
   float const s = std::sqrt(b) * radius;
-  return {s * std::sin(a), s * std::cos(a)};
+  return {s * orc_glsl::sin(a), s * orc_glsl::cos(a)};
 }
 
 // ---- ggx.glsl / pbr.glsl / transform.glsl -------------------------------------
@@ -156,12 +158,12 @@ inline float ggx_distribution(v3 n, v3 h, float alpha) {
 inline v2 ggx_importance_sample(v2 rs, float roughness) {
   float const phi = rs.y * 2.f * kPi;
   float const rough2 = roughness * roughness;
-  float const theta = std::atan(std::sqrt(rough2 * rs.x / (1.f - rs.x)));
+  float const theta = orc_glsl::atan(std::sqrt(rough2 * rs.x / (1.f - rs.x)));
   return {phi, theta};
 }
 inline v3 sample_hemisphere(v2 is) {
-  float const c = std::cos(is.y), s = std::sin(is.y);
-  return {s * std::cos(is.x), s * std::sin(is.x), c};
+  float const c = orc_glsl::cos(is.y), s = orc_glsl::sin(is.y);
+  return {s * orc_glsl::cos(is.x), s * orc_glsl::sin(is.x), c};
 }
 inline v3 transform_local_to_world(v3 v, v3 n) {
   v3 perp{1.f, 0.f, 0.f};
@@ -179,7 +181,7 @@ inline v3 transform_local_to_world(v3 v, v3 n) {
 inline float fresnel(float cos_theta, float ior_in, float ior_out, float metallic) {
   float f0 = std::fabs((ior_in - ior_out) / (ior_in + ior_out));
   f0 = mixf(f0 * f0, 1.f, metallic);
-  return f0 + (1.f - f0) * std::pow(1.f - cos_theta, 5.f);
+  return f0 + (1.f - f0) * orc_glsl::pow(1.f - cos_theta, 5.f);
 }
 inline v3 nreflect(v3 tv, v3 n, v3 mn) {
   v3 ray = reflect(-tv, mn);
@@ -370,7 +372,8 @@ inline void mat_evaluate(material_ctx& mc, v3 n, v3 tl, v3 tv, v3& refl, float& 
       textures[mc.tex_x - 1u].p) {
     tex_view const& t = textures[mc.tex_x - 1u];
     v4 const c = bilinear_at(t.p, t.w, t.h, t.wrap, uv.x, 1.f - uv.y);
-    mc.mat.color = {std::pow(c.x, 2.2f), std::pow(c.y, 2.2f), std::pow(c.z, 2.2f), std::pow(c.w, 2.2f)};
+    mc.mat.color = {orc_glsl::pow(c.x, 2.2f), orc_glsl::pow(c.y, 2.2f), orc_glsl::pow(c.z, 2.2f),
+        orc_glsl::pow(c.w, 2.2f)};
   }
   mc.incoming = dot(n, -tv) < 0.f;
   mc.ior1 = mc.incoming ? 1.f : mc.mat.ior;
@@ -1005,7 +1008,30 @@ void pass_filter(std::vector<gen_t>& gen, std::vector<trace_t> const& tr) {
 
 }  // namespace
 
+namespace orc_glsl {
+int mode = 0;
+}
+
 extern "C" {
+
+// GLSL built-ins of the restated passes (oracle_glsl_math.hpp): 0 = host libm
+// (the pins against oracle/_ref), 1 = the library's glmath.hpp definitions.
+void orc_set_glsl_math(int mode) { orc_glsl::mode = mode ? 1 : 0; }
+
+// The library's GLSL built-ins (glmath.hpp) on the host: fn 0 sin, 1 cos,
+// 2 atan, 3 exp, 4 pow(x, y).
+void orc_glsl_eval(int fn, float const* x, float const* y, std::size_t n, float* out) {
+  for (std::size_t i = 0; i < n; ++i) {
+    switch (fn) {
+      case 0: out[i] = myrt_glmath::sin(x[i]); break;
+      case 1: out[i] = myrt_glmath::cos(x[i]); break;
+      case 2: out[i] = myrt_glmath::atan(x[i]); break;
+      case 3: out[i] = myrt_glmath::exp(x[i]); break;
+      default: out[i] = myrt_glmath::pow(x[i], y[i]); break;
+    }
+  }
+}
+
 
 // Per-pass host randomness in the order sequential_pathtracer draws it for
 // `frames` frames of `bounces` bounces from std::mt19937(seed):

@@ -43,6 +43,8 @@ def oracle() -> C.CDLL:
             "orc_bvh8_traverse": (None, [P, P, P, SZ, I, I, P, P, P, P, P, P, P, I]),
             "orc_brute_closest": (None, [P, SZ, P, SZ, I, P, P, P, P, I]),
             "orc_instanced_query": (None, [P, P, P, P, P, SZ, P, SZ, I, I, P, P, P, P, I]),
+            "orc_set_glsl_math": (None, [I]),
+            "orc_glsl_eval": (None, [I, P, P, SZ, P]),
             "orc_host_rng": (None, [C.c_uint32, I, I, P, P]),
             "orc_render_reference": (None, [SZ, P, P, P, P, P, SZ, P, P, P, I, I, I, I, C.c_uint32, P, P, P, P, P,
                                             P, P, P, P, P, I, I, C.c_float, I, I, P, P, P, I, I, C.c_float,
@@ -227,6 +229,37 @@ def ref_glsl_traverse(nodes, bvh_indices, indices, points, rays, any_hit=False, 
     L.ref_glsl_traverse(nodes.ctypes.data, bvh_indices.ctypes.data, indices.ctypes.data, p4.ctypes.data,
                         r.ctypes.data, r.shape[0], int(any_hit), *[o.ctypes.data for o in out], threads or nthreads())
     return _pack(*out)
+
+
+# ---- GLSL built-ins of the restated shader passes ------------------------------
+GLSL_FNS = {"sin": 0, "cos": 1, "atan": 2, "exp": 3, "pow": 4}
+
+
+class glsl_math:
+    """Context manager: the oracle's restated passes use the host libm (0, the
+    default, as the reference compiled in oracle/_ref does) or the library's
+    built-ins (1, myrt_b200/csrc/glmath.hpp, as the device does)."""
+
+    def __init__(self, mode: int):
+        self.mode = mode
+
+    def __enter__(self):
+        oracle().orc_set_glsl_math(self.mode)
+        return self
+
+    def __exit__(self, *exc):
+        oracle().orc_set_glsl_math(0)
+
+
+def glsl_eval(name: str, x, y=None) -> np.ndarray:
+    """The library's built-in `name` evaluated on the host (glmath.hpp)."""
+    xs = np.ascontiguousarray(x, np.float32).ravel()
+    ys = None if y is None else np.ascontiguousarray(np.broadcast_to(np.float32(y) if np.isscalar(y) else y,
+                                                                      xs.shape), np.float32).ravel()
+    out = np.empty_like(xs)
+    oracle().orc_glsl_eval(GLSL_FNS[name], xs.ctypes.data, None if ys is None else ys.ctypes.data, xs.size,
+                           out.ctypes.data)
+    return out
 
 
 # ---- instanced scenes: two-level walks (pt_trace.comp:284-309) ---------------
