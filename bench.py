@@ -64,6 +64,8 @@ def parse_args():
                         "forward: the raster preview renderer (1920x1080, 2048^2 shadow map)")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain leg of the closest workload")
     p.add_argument("--no-c1", action="store_true", help="skip the height-field (32,768 tris, 1024^2 rays) sub-record")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the path-tracing (pt), batch and SDF sub-records of the default closest-hit run")
     p.add_argument("--sdf-cells", type=int, default=0,
                    help="sdf: cells along the longest axis of the SDF chain's group-list grid (0 = the library's "
                         "default, 1 = no grid: every primitive runs at every march step)")
@@ -323,14 +325,10 @@ def guiding_run(device_index: int, res: int, oracle_spp: int, budget_spp: int, s
         return acc[..., :3] / acc[..., 3:4], dt
 
     lum = np.array([0.2126, 0.7152, 0.0722])
-    # oracle: a trained guide used for inference only, no roulette, FP64 accumulation (unbiased like every
-    # estimator here; guided sampling keeps its noise well below the errors measured against it)
+    # oracle: plain BSDF sampling + NEE with MIS (the method under comparison has no part in it), roulette from
+    # vertex 3, FP64 accumulation, oracle_spp samples per pixel
     ctx.guide_configure(**GUIDE_CFG)
-    ctx.guide_reset()
-    render(256, 77, True, 12)
-    ctx.guide_configure(**{**GUIDE_CFG, "train": 0})
-    ref, t_ref = render(oracle_spp, 999, True, 12, fp64=True)
-    ctx.guide_configure(**GUIDE_CFG)
+    ref, t_ref = render(oracle_spp, 999, False, 3, fp64=True)
     render(4, 5, False, 3)  # warm: buffers at their final sizes
     img, t_plain = render(budget_spp, 1, False, 3)
     plain = {"spp": budget_spp, "seconds": t_plain, "rel_rmse": rel_rmse(img, ref),
@@ -347,7 +345,7 @@ def guiding_run(device_index: int, res: int, oracle_spp: int, budget_spp: int, s
     return {
         "scene": GUIDE_SCENE, "triangles": int(info["triangles"]), "res": res, "max_depth": 12,
         "oracle": {"spp": oracle_spp, "seconds": round(t_ref, 2),
-                   "method": "guided (trained network, inference only), no roulette, FP64 accumulation"},
+                   "method": "plain BSDF sampling + NEE with MIS, roulette from vertex 3, FP64 accumulation"},
         "plain": plain, "guided": guided,
         "wave_paths": "default (4 Mi paths) for both; while the guide trains, guided waves grow 1, 2, 4, ... spp "
                       "up to that size and the guide takes 16 Adam steps after each wave",
@@ -702,10 +700,19 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_guiding:
         del rays, hits
         torch.cuda.empty_cache()
-        line["guiding"] = guiding_run(local, res=512, oracle_spp=args.oracle_spp or 4096,
+        line["guiding"] = guiding_run(local, res=1024, oracle_spp=args.oracle_spp or 4096,
                                       budget_spp=args.budget_spp or 256)
-        line["guiding"]["note"] = ("reduced guided-vs-plain leg (512x512); the full configuration runs with "
-                                   "--workload guiding")
+        line["guiding"]["note"] = "the learned-guiding configuration: 1024x1024, depth 12, FP64 4096-spp oracle"
+    if rank == 0 and world == 1 and not args.no_configs:
+        import argparse as _ap
+
+        sub = _ap.Namespace(**vars(args))
+        sub.steps, sub.warmup, sub.res, sub.spp, sub.oracle_spp = min(args.steps, 3), 1, None, None, None
+        for key, fn in (("c2_pt", run_pt_workload), ("c3_batch", run_batch_workload), ("c5_sdf", run_sdf_workload)):
+            t0 = time.perf_counter()
+            rec = fn(sub, emit=False)
+            rec["wall_s"] = round(time.perf_counter() - t0, 1)
+            line[key] = rec
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -771,7 +778,7 @@ def _timed_frames(ctx_stream, render, steps):
     return e0.elapsed_time(e1)
 
 
-def run_pt_workload(args):
+def run_pt_workload(args, emit: bool = True):
     """Plain path tracing (physical shading: GGX + Lambert, NEE with MIS, RR
     after vertex 3) of the icosphere scene with its 0.2 x 0.2 light, 512x512,
     64 spp per step, depth 8. Reports samples/s and traced Mrays/s, the
@@ -834,11 +841,13 @@ def run_pt_workload(args):
          "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128,
                  "d2h_bytes_per_step": W * H * 16, "api": "myrt_render + myrt_read_accumulation"},
          "clocks": clocks.summary()})
+    if not emit:
+        return line
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_batch_workload(args):
+def run_batch_workload(args, emit: bool = True):
     """Batched uneven scenes: 16 height-field / icosphere scenes with triangle
     counts log-uniform in [10k, 2M], one view each (128^2 to 1024^2, 4-64
     spp), all rendered as one CUDA graph per frame with the launch shape the
@@ -912,11 +921,13 @@ def run_batch_workload(args):
                  "d2h_bytes_per_step": sum(j["width"] * j["height"] * 16 for j in jobs),
                  "api": "myrt_batch_render + myrt_batch_read per job"},
          "clocks": clocks.summary()})
+    if not emit:
+        return line
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_sdf_workload(args):
+def run_sdf_workload(args, emit: bool = True):
     """SDF + mesh hybrid: the icosphere scene with a smooth union (k = 0.1) of
     256 seeded spheres / boxes / tori sphere-traced with 256 steps and eps
     1e-4, GGX materials, guiding on; 768x768, 128 spp per step. Reports
@@ -992,6 +1003,8 @@ def run_sdf_workload(args):
          "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128,
                  "d2h_bytes_per_step": W * H * 16, "api": "myrt_render + myrt_read_accumulation"},
          "clocks": clocks.summary()})
+    if not emit:
+        return line
     print(json.dumps(line), flush=True)
     return 0
 

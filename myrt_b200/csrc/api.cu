@@ -268,6 +268,17 @@ int launch_trace_kernels(myrt_ctx* ctx, trace_args a, int intersector, bool any,
   }
   uint32_t const mb = ctx->tuning.trace_min_blocks;
   bool const unit = ctx->tuning.trace_unit_steps != 0;
+  if (ctx->tuning.trace_postpone && !stats && !unit && mb < 10) {
+    a.postpone = ctx->tuning.trace_postpone;
+    if (intersector == MYRT_ISECT_REFERENCE) {
+      if (any) k_trace_postpone<0, true><<<grid, block, 0, s>>>(a);
+      else k_trace_postpone<0, false><<<grid, block, 0, s>>>(a);
+    } else {
+      if (any) k_trace_postpone<1, true><<<grid, block, 0, s>>>(a);
+      else k_trace_postpone<1, false><<<grid, block, 0, s>>>(a);
+    }
+    return check_cuda(ctx, cudaGetLastError(), "trace launch");
+  }
   auto go = [&](auto isect_tag) {
     constexpr int IS = decltype(isect_tag)::value;
     if (unit) {
@@ -484,7 +495,7 @@ int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
   if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
       t->trace_unit_steps > 1 || (t->wave_paths != 0 && (t->wave_paths < 1024 || t->wave_paths > (1u << 28))) ||
       t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2 || t->bvh_builder > 1 || t->sdf_cells > 128 ||
-      t->guide_stall_test > 1 || t->instancing > 1)
+      t->guide_stall_test > 1 || t->instancing > 1 || t->trace_postpone > 32)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;

@@ -140,6 +140,7 @@ struct trace_args {
   const float4* blas_tris;
   const float4* inst;
   uint32_t* stat_inst;  // instances entered per ray (STATS)
+  uint32_t postpone;    // k_trace_postpone: lanes threshold of the postponing heuristic
 };
 
 // Byte (s & 3) of w as an exact float: one byte permute places it in the low
@@ -361,6 +362,50 @@ struct walker {
     if (!(group.y & 0xff000000u)) {
       if (sp == 0) return false;
       group = stack[SS * --sp];
+    }
+    return true;
+  }
+
+  // As step(), but a lane that has both triangles and more nodes in hand
+  // postpones the triangles -- pushes them as a tagged stack entry (tri_base
+  // with bit 31 set) and keeps walking -- while fewer than `lanes` lanes of the
+  // warp have triangles to test, so the warp's lanes stay in the same phase
+  // (the postponing heuristic of Ylitie, Karras and Laine, HPG 2017). A popped
+  // triangle entry is tested at once. Answers do not change: ties are decided
+  // by prim id, not by visiting order.
+  template <bool STATS>
+  __device__ __forceinline__ bool step_postpone(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris,
+      uint2* stack, uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris, uint32_t lanes) {
+    uint2 tgroup = make_uint2(0u, 0u);
+    if (group.y & 0xff000000u) {
+      if (!visit<STATS>(nodes, stack, err, n_nodes, tgroup)) return false;
+    } else {
+      group.y = 0;
+    }
+    uint32_t const tri_lanes = __ballot_sync(__activemask(), tgroup.y != 0u);
+    if (tgroup.y && (group.y & 0xff000000u) && uint32_t(__popc(tri_lanes)) < lanes && sp < cap) {
+      stack[SS * sp++] = make_uint2(tgroup.x | 0x80000000u, tgroup.y);
+      tgroup.y = 0;
+    }
+    while (tgroup.y) {
+      uint32_t const b = __ffs(tgroup.y) - 1u;
+      tgroup.y &= tgroup.y - 1u;
+      if (!test<STATS>(tris, tgroup.x + b, n_tris)) return false;
+    }
+    if (!(group.y & 0xff000000u)) {
+      if (sp == 0) return false;
+      uint2 const e = stack[SS * --sp];
+      if (e.x & 0x80000000u) {
+        group = make_uint2(0u, 0u);
+        uint2 tg = make_uint2(e.x & 0x7fffffffu, e.y);
+        while (tg.y) {
+          uint32_t const b = __ffs(tg.y) - 1u;
+          tg.y &= tg.y - 1u;
+          if (!test<STATS>(tris, tg.x + b, n_tris)) return false;
+        }
+        return sp != 0 || (group.y & 0xff000000u);
+      }
+      group = e;
     }
     return true;
   }
@@ -625,6 +670,25 @@ __global__ void __launch_bounds__(128, MINB) k_trace(trace_args a) {
   bool const r = traverse<ISECT, ANY, STATS, UNIT>(a.nodes, a.tris, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w,
       r1.w, h, a.err, n_nodes, n_tris);
   store_result<ISECT, ANY, STATS>(a, i, r, h, n_nodes, n_tris);
+}
+
+// One thread per ray with postponed triangle tests (walker::step_postpone).
+template <int ISECT, bool ANY>
+__global__ void __launch_bounds__(128, 8) k_trace_postpone(trace_args a) {
+  uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  uint32_t const i = a.perm ? __ldg(a.perm + t) : t;
+  float4 const r0 = __ldg(a.rays + 2 * size_t(i));
+  float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
+  uint2 stack[MYRT_STACK_MAX];
+  walker<ISECT, ANY> w;
+  w.init(f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w, r1.w);
+  uint32_t n_nodes = 0, n_tris = 0;
+  while (w.template step_postpone<false>(a.nodes, a.tris, stack, a.err, n_nodes, n_tris, a.postpone)) {
+  }
+  hit_rec h;
+  if (!ANY) w.result(h);
+  store_result<ISECT, ANY, false>(a, i, ANY ? w.occluded : h.prim >= 0, h, n_nodes, n_tris);
 }
 
 // Persistent variant: a fixed grid of warps; whenever at least `refill` lanes

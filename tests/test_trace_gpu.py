@@ -237,6 +237,31 @@ def test_shared_stack_traversal_bit_exact(ctx, hf128, isect):
         ctx.set_tuning()
 
 
+@pytest.mark.parametrize("isect", [0, 1])
+@pytest.mark.parametrize("lanes", [1, 8, 32])
+def test_postponed_triangles_bit_exact(ctx, hf128, isect, lanes):
+    """Postponing a lane's triangle tests while few lanes of its warp have some
+    (trace_postpone) changes the visiting order only: closest and any hit equal
+    the oracle's, for both intersectors, on the height field and on the
+    instanced icosphere scene."""
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = np.concatenate([pinhole_rays(256, 256), _rand_rays(100_000, seed=29)])
+    ora, _, _ = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays, isect=isect)
+    try:
+        ctx.set_tuning(trace_postpone=lanes, trace_order=1)
+        assert np.array_equal(ctx.trace_closest(rays, intersector=isect), ora)
+        assert np.array_equal(ctx.trace_any(rays, intersector=isect).astype(bool), ora["prim"] >= 0)
+        s = icosphere_field(n_spheres=64, subdiv=3, floor_cells=8, seed=9)
+        ctx.upload_scene(**s)
+        cam = pinhole_rays(192, 160, eye=(0.0, 1.0, -4.5), target=(0.0, -0.3, 0.0), vfov_deg=50)
+        tris9 = po.bake_world_triangles(s["indices"], s["vertices"], s["drawables"])
+        nodes, tris, _ = mb.build_bvh8(tris9)
+        ref, _, _ = po.bvh8_traverse(nodes, tris, cam, isect=isect)
+        assert np.array_equal(ctx.trace_closest(cam, intersector=isect), ref)
+    finally:
+        ctx.set_tuning()
+
+
 @pytest.mark.parametrize("order", [1, 2])
 def test_ray_order_does_not_change_results(ctx, hf128, order):
     """Sorted visiting order (trace_order 2) and input order (1) give the same
