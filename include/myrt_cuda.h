@@ -180,10 +180,11 @@ typedef struct myrt_tuning {
                                 bit. 1 must be set before myrt_scene_upload, which then also builds
                                 one object-space tree per distinct geometry; renders always use the
                                 baked tree. */
-  uint32_t trace_postpone;   /* one-thread-per-ray closest / any hit (baked tree): 0 = test a node's
-                                triangles as soon as it is visited; 1..32 = a lane that has more nodes
-                                to visit postpones its triangles while fewer than this many lanes of
-                                its warp have triangles to test. Results never depend on it. */
+  uint32_t trace_prefetch;   /* one-thread-per-ray closest / any hit: 1 = prefetch the next node into
+                                L1 before testing a node's triangles. Results never depend on it. */
+  uint32_t trace_order_bits; /* sorted visiting order: key bits (0 = 24: 16^3 origin cells and 16^3
+                                direction cells; fewer bits drop the finest ones and the radix
+                                sort's last passes). Results never depend on it. */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */

@@ -140,7 +140,6 @@ struct trace_args {
   const float4* blas_tris;
   const float4* inst;
   uint32_t* stat_inst;  // instances entered per ray (STATS)
-  uint32_t postpone;    // k_trace_postpone: lanes threshold of the postponing heuristic
 };
 
 // Byte (s & 3) of w as an exact float: one byte permute places it in the low
@@ -345,12 +344,23 @@ struct walker {
 
   // One iteration: visit a node, test all the triangles it hit, pop if the
   // current group is exhausted.
-  template <bool STATS>
+  // PREFETCH: when the visited node leaves internal children to walk and leaf
+  // triangles to test, the next node's 80 bytes are prefetched into L1 before
+  // the triangle tests, which then hide their latency.
+  template <bool STATS, bool PREFETCH = false>
   __device__ __forceinline__ bool step(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris, uint2* stack,
       uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris) {
     uint2 tgroup = make_uint2(0u, 0u);
     if (group.y & 0xff000000u) {
       if (!visit<STATS>(nodes, stack, err, n_nodes, tgroup)) return false;
+      if (PREFETCH && tgroup.y && (group.y & 0xff000000u)) {
+        uint32_t const pos = 31u - __clz(group.y & 0xff000000u);
+        uint32_t const slot = (pos - 24u) ^ octinv;
+        char const* np = reinterpret_cast<char const*>(nodes + 5 * size_t(group.x + __popc(group.y & 0xffu &
+                                                                                   ((1u << slot) - 1u))));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(np));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(np + 64));
+      }
     } else {
       group.y = 0;
     }
@@ -362,50 +372,6 @@ struct walker {
     if (!(group.y & 0xff000000u)) {
       if (sp == 0) return false;
       group = stack[SS * --sp];
-    }
-    return true;
-  }
-
-  // As step(), but a lane that has both triangles and more nodes in hand
-  // postpones the triangles -- pushes them as a tagged stack entry (tri_base
-  // with bit 31 set) and keeps walking -- while fewer than `lanes` lanes of the
-  // warp have triangles to test, so the warp's lanes stay in the same phase
-  // (the postponing heuristic of Ylitie, Karras and Laine, HPG 2017). A popped
-  // triangle entry is tested at once. Answers do not change: ties are decided
-  // by prim id, not by visiting order.
-  template <bool STATS>
-  __device__ __forceinline__ bool step_postpone(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris,
-      uint2* stack, uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris, uint32_t lanes) {
-    uint2 tgroup = make_uint2(0u, 0u);
-    if (group.y & 0xff000000u) {
-      if (!visit<STATS>(nodes, stack, err, n_nodes, tgroup)) return false;
-    } else {
-      group.y = 0;
-    }
-    uint32_t const tri_lanes = __ballot_sync(__activemask(), tgroup.y != 0u);
-    if (tgroup.y && (group.y & 0xff000000u) && uint32_t(__popc(tri_lanes)) < lanes && sp < cap) {
-      stack[SS * sp++] = make_uint2(tgroup.x | 0x80000000u, tgroup.y);
-      tgroup.y = 0;
-    }
-    while (tgroup.y) {
-      uint32_t const b = __ffs(tgroup.y) - 1u;
-      tgroup.y &= tgroup.y - 1u;
-      if (!test<STATS>(tris, tgroup.x + b, n_tris)) return false;
-    }
-    if (!(group.y & 0xff000000u)) {
-      if (sp == 0) return false;
-      uint2 const e = stack[SS * --sp];
-      if (e.x & 0x80000000u) {
-        group = make_uint2(0u, 0u);
-        uint2 tg = make_uint2(e.x & 0x7fffffffu, e.y);
-        while (tg.y) {
-          uint32_t const b = __ffs(tg.y) - 1u;
-          tg.y &= tg.y - 1u;
-          if (!test<STATS>(tris, tg.x + b, n_tris)) return false;
-        }
-        return sp != 0 || (group.y & 0xff000000u);
-      }
-      group = e;
     }
     return true;
   }
@@ -441,7 +407,7 @@ struct walker {
 // whether a triangle was hit. Any hit (ANY = true): returns true at the first
 // triangle with tmin <= t < tmax. n_nodes / n_tris count fetched nodes and
 // tested triangles when STATS.
-template <int ISECT, bool ANY, bool STATS, bool UNIT = false>
+template <int ISECT, bool ANY, bool STATS, bool UNIT = false, bool PREFETCH = false>
 __device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris, f3 o, f3 d,
     float tmin, float tmax, hit_rec& h, uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris) {
   uint2 stack[MYRT_STACK_MAX];
@@ -451,7 +417,7 @@ __device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4
     while (w.template step_unit<STATS>(nodes, tris, stack, err, n_nodes, n_tris)) {
     }
   } else {
-    while (w.template step<STATS>(nodes, tris, stack, err, n_nodes, n_tris)) {
+    while (w.template step<STATS, PREFETCH>(nodes, tris, stack, err, n_nodes, n_tris)) {
     }
   }
   if (ANY) return w.occluded;
@@ -658,7 +624,7 @@ __global__ void __launch_bounds__(128, 8) k_trace_smem(trace_args a) {
 
 // One thread per ray. MINB = resident 128-thread blocks per SM the compiler
 // must allow (8 leaves it 64 registers; more blocks cap the register count).
-template <int ISECT, bool ANY, bool STATS, int MINB = 8, bool UNIT = false>
+template <int ISECT, bool ANY, bool STATS, int MINB = 8, bool UNIT = false, bool PREFETCH = false>
 __global__ void __launch_bounds__(128, MINB) k_trace(trace_args a) {
   uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n) return;
@@ -667,28 +633,9 @@ __global__ void __launch_bounds__(128, MINB) k_trace(trace_args a) {
   float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
   hit_rec h;
   uint32_t n_nodes = 0, n_tris = 0;
-  bool const r = traverse<ISECT, ANY, STATS, UNIT>(a.nodes, a.tris, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w,
-      r1.w, h, a.err, n_nodes, n_tris);
+  bool const r = traverse<ISECT, ANY, STATS, UNIT, PREFETCH>(a.nodes, a.tris, f3{r0.x, r0.y, r0.z},
+      f3{r1.x, r1.y, r1.z}, r0.w, r1.w, h, a.err, n_nodes, n_tris);
   store_result<ISECT, ANY, STATS>(a, i, r, h, n_nodes, n_tris);
-}
-
-// One thread per ray with postponed triangle tests (walker::step_postpone).
-template <int ISECT, bool ANY>
-__global__ void __launch_bounds__(128, 8) k_trace_postpone(trace_args a) {
-  uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.n) return;
-  uint32_t const i = a.perm ? __ldg(a.perm + t) : t;
-  float4 const r0 = __ldg(a.rays + 2 * size_t(i));
-  float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
-  uint2 stack[MYRT_STACK_MAX];
-  walker<ISECT, ANY> w;
-  w.init(f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w, r1.w);
-  uint32_t n_nodes = 0, n_tris = 0;
-  while (w.template step_postpone<false>(a.nodes, a.tris, stack, a.err, n_nodes, n_tris, a.postpone)) {
-  }
-  hit_rec h;
-  if (!ANY) w.result(h);
-  store_result<ISECT, ANY, false>(a, i, ANY ? w.occluded : h.prim >= 0, h, n_nodes, n_tris);
 }
 
 // Persistent variant: a fixed grid of warps; whenever at least `refill` lanes

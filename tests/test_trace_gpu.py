@@ -238,17 +238,18 @@ def test_shared_stack_traversal_bit_exact(ctx, hf128, isect):
 
 
 @pytest.mark.parametrize("isect", [0, 1])
-@pytest.mark.parametrize("lanes", [1, 8, 32])
-def test_postponed_triangles_bit_exact(ctx, hf128, isect, lanes):
-    """Postponing a lane's triangle tests while few lanes of its warp have some
-    (trace_postpone) changes the visiting order only: closest and any hit equal
-    the oracle's, for both intersectors, on the height field and on the
-    instanced icosphere scene."""
+@pytest.mark.parametrize("variant", [dict(trace_prefetch=1), dict(trace_prefetch=1, trace_min_blocks=10),
+                                     dict(trace_order=2, trace_order_bits=16)])
+def test_launch_variants_bit_exact(ctx, hf128, isect, variant):
+    """Prefetching the next node, the 10-blocks register cap and a coarser
+    16-bit visiting-order key change how the walk runs, not what it finds:
+    closest and any hit equal the oracle's, for both intersectors, on the
+    height field and on the instanced icosphere scene."""
     ctx.upload_scene(hf128["idx"], hf128["pts"])
     rays = np.concatenate([pinhole_rays(256, 256), _rand_rays(100_000, seed=29)])
     ora, _, _ = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays, isect=isect)
     try:
-        ctx.set_tuning(trace_postpone=lanes, trace_order=1)
+        ctx.set_tuning(**variant)
         assert np.array_equal(ctx.trace_closest(rays, intersector=isect), ora)
         assert np.array_equal(ctx.trace_any(rays, intersector=isect).astype(bool), ora["prim"] >= 0)
         s = icosphere_field(n_spheres=64, subdiv=3, floor_cells=8, seed=9)
