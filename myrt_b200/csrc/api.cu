@@ -222,15 +222,20 @@ int launch_trace_kernels(myrt_ctx* ctx, trace_args a, int intersector, bool any,
   dim3 const grid((a.n + 127) / 128);
   if (ctx->tuning.instancing) {
     a.nodes = ctx->scene.tlas_nodes;
-    if (intersector == MYRT_ISECT_REFERENCE) {
-      if (stats) k_trace_inst<0, false, true><<<grid, block, 0, s>>>(a);
-      else if (any) k_trace_inst<0, true, false><<<grid, block, 0, s>>>(a);
-      else k_trace_inst<0, false, false><<<grid, block, 0, s>>>(a);
-    } else {
-      if (stats) k_trace_inst<1, false, true><<<grid, block, 0, s>>>(a);
-      else if (any) k_trace_inst<1, true, false><<<grid, block, 0, s>>>(a);
-      else k_trace_inst<1, false, false><<<grid, block, 0, s>>>(a);
-    }
+    auto go_inst = [&](auto flat_tag) {
+      constexpr bool FL = decltype(flat_tag)::value;
+      if (intersector == MYRT_ISECT_REFERENCE) {
+        if (stats) k_trace_inst<0, false, true, FL><<<grid, block, 0, s>>>(a);
+        else if (any) k_trace_inst<0, true, false, FL><<<grid, block, 0, s>>>(a);
+        else k_trace_inst<0, false, false, FL><<<grid, block, 0, s>>>(a);
+      } else {
+        if (stats) k_trace_inst<1, false, true, FL><<<grid, block, 0, s>>>(a);
+        else if (any) k_trace_inst<1, true, false, FL><<<grid, block, 0, s>>>(a);
+        else k_trace_inst<1, false, false, FL><<<grid, block, 0, s>>>(a);
+      }
+    };
+    if (ctx->tuning.instancing == 2) go_inst(std::false_type{});
+    else go_inst(std::true_type{});
     return check_cuda(ctx, cudaGetLastError(), "instanced trace launch");
   }
   if (ctx->tuning.trace_persistent) {
@@ -500,7 +505,7 @@ int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
   if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
       t->trace_unit_steps > 1 || (t->wave_paths != 0 && (t->wave_paths < 1024 || t->wave_paths > (1u << 28))) ||
       t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2 || t->bvh_builder > 1 || t->sdf_cells > 128 ||
-      t->guide_stall_test > 1 || t->instancing > 1 || t->trace_prefetch > 1 || t->trace_order_bits > 24 || (t->trace_order_bits != 0 && t->trace_order_bits < 8))
+      t->guide_stall_test > 1 || t->instancing > 2 || t->trace_prefetch > 1 || t->trace_order_bits > 24 || (t->trace_order_bits != 0 && t->trace_order_bits < 8))
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;
@@ -562,7 +567,7 @@ int upload_top_level(myrt_ctx* ctx, std::vector<myrt_drawable> const& drawables)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, std::string("instance tree build: ") + e.what());
   }
   if (top.nodes.empty()) return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "instancing: no drawable has triangles");
-  if (top.depth + s.blas_depth + kInstanceSave > MYRT_STACK_MAX)
+  if (std::max(top.depth + s.blas_depth + kInstanceSave, 2 * top.depth + s.blas_depth + kInstanceRay) > MYRT_STACK_MAX)
     return set_error(ctx, MYRT_ERR_UNSUPPORTED, "instance tree + object tree deeper than the traversal stack");
   cudaFree(s.tlas_nodes);
   cudaFree(s.inst_records);

@@ -584,8 +584,122 @@ __device__ __forceinline__ bool traverse_two_level(trace_args const& a, f3 o, f3
   return h.prim >= 0;
 }
 
-// One thread per ray over the two-level structure.
+// The same walk as one loop whose every iteration visits one node of either
+// level, so lanes of a warp in the instance tree and lanes inside instances
+// run the same node-visit instructions together. The leaves of an instance-tree
+// node become a tagged stack entry (first record | 1 << 31, leaf bits); popping
+// one enters its lowest instance (the rest is pushed back), saving the world
+// ray as three stack entries above which the instance's walk runs; popping
+// back down to them leaves the instance. Stack use: instance depth x 2 +
+// object depth + 3 (checked at upload).
+constexpr int kInstanceRay = 3;
+
 template <int ISECT, bool ANY, bool STATS>
+__device__ __forceinline__ bool traverse_two_level_flat(trace_args const& a, f3 o, f3 d, float tmin, float tmax,
+    hit_rec& h, uint32_t& n_nodes, uint32_t& n_tris, uint32_t& n_inst) {
+  uint2 stack[MYRT_STACK_MAX];
+  walker<ISECT, ANY> w;
+  w.init(o, d, tmin, tmax);
+  int base_sp = -1;  // stack depth at which the current instance's walk ends; -1 = instance level
+  int32_t prim_base = 0;
+  while (true) {
+    if (w.group.y & 0xff000000u) {
+      uint2 tg = make_uint2(0u, 0u);
+      if (!w.template visit<STATS>(base_sp >= 0 ? a.blas_nodes : a.nodes, stack, a.err, n_nodes, tg)) break;
+      if (tg.y) {
+        if (base_sp < 0) {  // instance leaves: visited after the node's children
+          if (w.sp >= w.cap) {
+            atomicOr(a.err, ERR_STACK_OVERFLOW);
+            break;
+          }
+          stack[w.sp++] = make_uint2(tg.x | 0x80000000u, tg.y);
+        } else {
+          bool answered = false;
+          while (tg.y) {
+            uint32_t const tb = __ffs(tg.y) - 1u;
+            tg.y &= tg.y - 1u;
+            float4 const* tp = a.blas_tris + 3 * size_t(tg.x + tb);
+            float4 const p0 = __ldg(tp + 0);
+            float4 const p1 = __ldg(tp + 1);
+            float4 const p2 = __ldg(tp + 2);
+            if (STATS) ++n_tris;
+            float t, u, v;
+            bool hit;
+            if (ISECT == 0)
+              hit = isect_reference(w.o, w.d, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z}, t, u,
+                        v) && t >= w.tmin;
+            else
+              hit = isect_watertight(w.wt, w.o, f3{p0.x, p0.y, p0.z}, f3{p1.x, p1.y, p1.z}, f3{p2.x, p2.y, p2.z},
+                  w.tmin, t, u, v);
+            if (!hit) continue;
+            int32_t const prim = prim_base + __float_as_int(p0.w);
+            if (ANY) {
+              if (t < w.tmax) {
+                w.occluded = true;
+                answered = true;
+                break;
+              }
+            } else if (t < w.tbest || (t == w.tbest && w.best >= 0 && prim < w.best)) {
+              w.tbest = t;
+              w.best = prim;
+              w.bu = u;
+              w.bv = v;
+            }
+          }
+          if (answered) break;
+        }
+      }
+      if (w.group.y & 0xff000000u) continue;
+    }
+    w.group.y = 0;
+    if (base_sp >= 0 && w.sp == base_sp) {  // leave the instance: the world ray comes back
+      uint2 const s0 = stack[w.sp - 3], s1 = stack[w.sp - 2], s2 = stack[w.sp - 1];
+      w.sp -= kInstanceRay;
+      set_walker_ray(w, f3{__uint_as_float(s0.x), __uint_as_float(s0.y), __uint_as_float(s1.x)},
+          f3{__uint_as_float(s1.y), __uint_as_float(s2.x), __uint_as_float(s2.y)});
+      base_sp = -1;
+      continue;
+    }
+    if (w.sp == 0) break;
+    uint2 const e = stack[--w.sp];
+    if (!(e.x & 0x80000000u)) {
+      w.group = e;
+      continue;
+    }
+    // an instance leaf group: enter its lowest instance, keep the rest
+    uint32_t const b = __ffs(e.y) - 1u;
+    uint32_t const rest = e.y & (e.y - 1u);
+    if (rest) stack[w.sp++] = make_uint2(e.x, rest);
+    if (w.sp + kInstanceRay > w.cap) {
+      atomicOr(a.err, ERR_STACK_OVERFLOW);
+      break;
+    }
+    stack[w.sp] = make_uint2(__float_as_uint(w.o.x), __float_as_uint(w.o.y));
+    stack[w.sp + 1] = make_uint2(__float_as_uint(w.o.z), __float_as_uint(w.d.x));
+    stack[w.sp + 2] = make_uint2(__float_as_uint(w.d.y), __float_as_uint(w.d.z));
+    w.sp += kInstanceRay;
+    base_sp = w.sp;
+    float4 const* r = a.inst + 4 * size_t((e.x & 0x7fffffffu) + b);
+    float4 const r0 = __ldg(r + 0), r1 = __ldg(r + 1), r2 = __ldg(r + 2);
+    int4 const meta = __ldg(reinterpret_cast<int4 const*>(r + 3));
+    if (STATS) ++n_inst;
+    f3 const oo{row_dot(r0, w.o, 1.0f), row_dot(r1, w.o, 1.0f), row_dot(r2, w.o, 1.0f)};
+    f3 const od{row_dot(r0, w.d, 0.0f), row_dot(r1, w.d, 0.0f), row_dot(r2, w.d, 0.0f)};
+    set_walker_ray(w, oo, od);
+    w.group = make_uint2(uint32_t(meta.x), 0x80000000u);  // the geometry's root
+    prim_base = meta.y;
+  }
+  if (ANY) return w.occluded;
+  h.prim = w.best;
+  h.t = w.best >= 0 ? w.tbest : tmax;
+  h.u = w.best >= 0 ? w.bu : 0.f;
+  h.v = w.best >= 0 ? w.bv : 0.f;
+  h.leaf = 0;
+  return h.prim >= 0;
+}
+
+// One thread per ray over the two-level structure.
+template <int ISECT, bool ANY, bool STATS, bool FLAT = true>
 __global__ void __launch_bounds__(128, 8) k_trace_inst(trace_args a) {
   uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n) return;
@@ -594,8 +708,10 @@ __global__ void __launch_bounds__(128, 8) k_trace_inst(trace_args a) {
   float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
   hit_rec h;
   uint32_t n_nodes = 0, n_tris = 0, n_inst = 0;
-  bool const r = traverse_two_level<ISECT, ANY, STATS>(a, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w, r1.w, h,
-      n_nodes, n_tris, n_inst);
+  bool const r = FLAT ? traverse_two_level_flat<ISECT, ANY, STATS>(a, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z},
+                             r0.w, r1.w, h, n_nodes, n_tris, n_inst)
+                       : traverse_two_level<ISECT, ANY, STATS>(a, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w,
+                             r1.w, h, n_nodes, n_tris, n_inst);
   store_result<ISECT, ANY, STATS>(a, i, r, h, n_nodes, n_tris);
   if (STATS && a.stat_inst) a.stat_inst[i] = n_inst;
 }
