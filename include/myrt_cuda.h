@@ -143,7 +143,8 @@ typedef struct myrt_tuning {
   uint32_t trace_persistent; /* 0: one thread per ray; 1: persistent warps that refill finished lanes */
   uint32_t refill;           /* persistent: refill once at least this many lanes of a warp are idle (1..32) */
   uint32_t blocks_per_sm;    /* persistent: resident 128-thread blocks per SM (0 = occupancy maximum) */
-  uint32_t trace_min_blocks; /* one-thread-per-ray: register cap as blocks per SM: 0 or 8 (64 regs), 10, 12 */
+  uint32_t trace_min_blocks; /* one-thread-per-ray: register cap as blocks per SM: 8 (64 regs), 10 (48 regs;
+                                0 = 10), 12 */
   uint32_t trace_unit_steps; /* one-thread-per-ray: 0 = a node and all its triangles per iteration,
                                 1 = one node, triangle or pop per iteration */
   uint32_t wave_paths;       /* physical / guided wavefront: paths in flight per wave (0 = 4 Mi) */
@@ -177,14 +178,10 @@ typedef struct myrt_tuning {
                                 over the drawables' world boxes, each ray moved into the drawable's
                                 object space by inverse_transformation and tested against the
                                 untransformed geometry, so t, u and v equal the reference's bit for
-                                bit. 1 must be set before myrt_scene_upload, which then also builds
+                                bit (2 = the same walk as two nested loops, for comparison). 1 must
+                                be set before myrt_scene_upload, which then also builds
                                 one object-space tree per distinct geometry; renders always use the
                                 baked tree. */
-  uint32_t trace_prefetch;   /* one-thread-per-ray closest / any hit: 1 = prefetch the next node into
-                                L1 before testing a node's triangles. Results never depend on it. */
-  uint32_t trace_order_bits; /* sorted visiting order: key bits (0 = 24: 16^3 origin cells and 16^3
-                                direction cells; fewer bits drop the finest ones and the radix
-                                sort's last passes). Results never depend on it. */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */

@@ -25,9 +25,8 @@ __device__ __forceinline__ uint32_t cell4(float x) {  // x in [0, 16) -> 0..15, 
 }
 
 // keys[i], vals[i] = i for rays given as (o, tmin), (d, tmax) float4 pairs.
-// drop: low key bits dropped (the finest direction, then origin, cells), 0 = the full 24-bit key.
 __global__ void __launch_bounds__(256) k_ray_keys(float4 const* __restrict__ rays, uint32_t n, float3 lo,
-    float3 cell_scale, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals, uint32_t drop) {
+    float3 cell_scale, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 const r0 = __ldg(rays + 2 * size_t(i));
@@ -40,7 +39,7 @@ __global__ void __launch_bounds__(256) k_ray_keys(float4 const* __restrict__ ray
   uint32_t const dx = cell4(fmaf(r1.x, s, 8.f)), dy = cell4(fmaf(r1.y, s, 8.f)), dz = cell4(fmaf(r1.z, s, 8.f));
   uint32_t const om = spread4(ox) | (spread4(oy) << 1) | (spread4(oz) << 2);
   uint32_t const dm = spread4(dx) | (spread4(dy) << 1) | (spread4(dz) << 2);
-  keys[i] = ((om << 12) | dm) >> drop;
+  keys[i] = (om << 12) | dm;
   vals[i] = i;
 }
 

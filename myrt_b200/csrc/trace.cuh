@@ -344,23 +344,12 @@ struct walker {
 
   // One iteration: visit a node, test all the triangles it hit, pop if the
   // current group is exhausted.
-  // PREFETCH: when the visited node leaves internal children to walk and leaf
-  // triangles to test, the next node's 80 bytes are prefetched into L1 before
-  // the triangle tests, which then hide their latency.
-  template <bool STATS, bool PREFETCH = false>
+  template <bool STATS>
   __device__ __forceinline__ bool step(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris, uint2* stack,
       uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris) {
     uint2 tgroup = make_uint2(0u, 0u);
     if (group.y & 0xff000000u) {
       if (!visit<STATS>(nodes, stack, err, n_nodes, tgroup)) return false;
-      if (PREFETCH && tgroup.y && (group.y & 0xff000000u)) {
-        uint32_t const pos = 31u - __clz(group.y & 0xff000000u);
-        uint32_t const slot = (pos - 24u) ^ octinv;
-        char const* np = reinterpret_cast<char const*>(nodes + 5 * size_t(group.x + __popc(group.y & 0xffu &
-                                                                                   ((1u << slot) - 1u))));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(np));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(np + 64));
-      }
     } else {
       group.y = 0;
     }
@@ -407,7 +396,7 @@ struct walker {
 // whether a triangle was hit. Any hit (ANY = true): returns true at the first
 // triangle with tmin <= t < tmax. n_nodes / n_tris count fetched nodes and
 // tested triangles when STATS.
-template <int ISECT, bool ANY, bool STATS, bool UNIT = false, bool PREFETCH = false>
+template <int ISECT, bool ANY, bool STATS, bool UNIT = false>
 __device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4 const* __restrict__ tris, f3 o, f3 d,
     float tmin, float tmax, hit_rec& h, uint32_t* err, uint32_t& n_nodes, uint32_t& n_tris) {
   uint2 stack[MYRT_STACK_MAX];
@@ -417,7 +406,7 @@ __device__ __forceinline__ bool traverse(uint4 const* __restrict__ nodes, float4
     while (w.template step_unit<STATS>(nodes, tris, stack, err, n_nodes, n_tris)) {
     }
   } else {
-    while (w.template step<STATS, PREFETCH>(nodes, tris, stack, err, n_nodes, n_tris)) {
+    while (w.template step<STATS>(nodes, tris, stack, err, n_nodes, n_tris)) {
     }
   }
   if (ANY) return w.occluded;
@@ -740,7 +729,7 @@ __global__ void __launch_bounds__(128, 8) k_trace_smem(trace_args a) {
 
 // One thread per ray. MINB = resident 128-thread blocks per SM the compiler
 // must allow (8 leaves it 64 registers; more blocks cap the register count).
-template <int ISECT, bool ANY, bool STATS, int MINB = 8, bool UNIT = false, bool PREFETCH = false>
+template <int ISECT, bool ANY, bool STATS, int MINB = 8, bool UNIT = false>
 __global__ void __launch_bounds__(128, MINB) k_trace(trace_args a) {
   uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n) return;
@@ -749,8 +738,8 @@ __global__ void __launch_bounds__(128, MINB) k_trace(trace_args a) {
   float4 const r1 = __ldg(a.rays + 2 * size_t(i) + 1);
   hit_rec h;
   uint32_t n_nodes = 0, n_tris = 0;
-  bool const r = traverse<ISECT, ANY, STATS, UNIT, PREFETCH>(a.nodes, a.tris, f3{r0.x, r0.y, r0.z},
-      f3{r1.x, r1.y, r1.z}, r0.w, r1.w, h, a.err, n_nodes, n_tris);
+  bool const r = traverse<ISECT, ANY, STATS, UNIT>(a.nodes, a.tris, f3{r0.x, r0.y, r0.z}, f3{r1.x, r1.y, r1.z}, r0.w,
+      r1.w, h, a.err, n_nodes, n_tris);
   store_result<ISECT, ANY, STATS>(a, i, r, h, n_nodes, n_tris);
 }
 

@@ -238,13 +238,13 @@ def test_shared_stack_traversal_bit_exact(ctx, hf128, isect):
 
 
 @pytest.mark.parametrize("isect", [0, 1])
-@pytest.mark.parametrize("variant", [dict(trace_prefetch=1), dict(trace_prefetch=1, trace_min_blocks=10),
-                                     dict(trace_order=2, trace_order_bits=16)])
+@pytest.mark.parametrize("variant", [dict(trace_min_blocks=8), dict(trace_min_blocks=10), dict(trace_min_blocks=12),
+                                     dict(trace_order=2, trace_min_blocks=10)])
 def test_launch_variants_bit_exact(ctx, hf128, isect, variant):
-    """Prefetching the next node, the 10-blocks register cap and a coarser
-    16-bit visiting-order key change how the walk runs, not what it finds:
-    closest and any hit equal the oracle's, for both intersectors, on the
-    height field and on the instanced icosphere scene."""
+    """The register caps (8, 10 and 12 blocks per SM) and the sorted order change
+    how the walk runs, not what it finds: closest and any hit equal the
+    oracle's, for both intersectors, on the height field and on the instanced
+    icosphere scene."""
     ctx.upload_scene(hf128["idx"], hf128["pts"])
     rays = np.concatenate([pinhole_rays(256, 256), _rand_rays(100_000, seed=29)])
     ora, _, _ = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays, isect=isect)
