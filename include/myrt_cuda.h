@@ -182,6 +182,12 @@ typedef struct myrt_tuning {
                                 be set before myrt_scene_upload, which then also builds
                                 one object-space tree per distinct geometry; renders always use the
                                 baked tree. */
+  uint32_t pt_grid;          /* physical / guided extend, shade and shadow kernels: 0 = default (2),
+                                1 = grid-stride loops over pt_blocks_per_sm resident blocks per SM,
+                                2 = one thread per queue entry (the grid covers the wave's paths;
+                                blocks past the queue's count return at once; pt_blocks_per_sm >= 10
+                                then selects a 48-register cap for the mesh traversal kernels).
+                                Results never depend on it. */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */

@@ -98,15 +98,22 @@ __device__ __forceinline__ void encode(mlp_args const& a, float4 p, float4 n, fl
     pn[k] = fminf(fmaxf(pn[k], -1.f), 1.f);
     f[k] = pn[k];
   }
+  // sin / cos of 2^f pi p: one sincospi per axis, then the double-angle
+  // formulas (the features are rounded to BF16 before the first layer, far
+  // above the recurrence's few-ulp drift)
 #pragma unroll
-  for (int fr = 0; fr < 6; ++fr)
+  for (int k = 0; k < 3; ++k) {
+    float s, c;
+    sincospif(pn[k], &s, &c);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      float s, c;
-      sincospif(pn[k] * float(1 << fr), &s, &c);
+    for (int fr = 0; fr < 6; ++fr) {
       f[3 + 6 * fr + 2 * k] = s;
       f[4 + 6 * fr + 2 * k] = c;
+      float const s2 = 2.f * s * c;
+      c = fmaf(-2.f * s, s, 1.f);
+      s = s2;
     }
+  }
   f[39] = n.x, f[40] = n.y, f[41] = n.z;
   f[42] = wo.x, f[43] = wo.y, f[44] = wo.z;
   f[45] = 1.f;
@@ -175,16 +182,17 @@ __device__ __forceinline__ void mixture(float const (&o)[64], lobe_set& L) {
   float sum = 0.f;
 #pragma unroll
   for (int k = 0; k < kGuideLobes; ++k) {
-    L.w[k] = expf(o[5 * k] - mx);
+    L.w[k] = __expf(o[5 * k] - mx);
     sum += L.w[k];
   }
 #pragma unroll
   for (int k = 0; k < kGuideLobes; ++k) {
     L.w[k] = L.w[k] / sum;
     float const x = o[5 * k + 1];
-    float const sp = x > 20.f ? x : log1pf(expf(x));
+    float const ex = __expf(-fabsf(x));  // softplus(x) = max(x, 0) + log(1 + e^-|x|)
+    float const sp = fmaxf(x, 0.f) + log1pf(ex);
     float kap = sp + kKappaMin;
-    float dk = 1.f / (1.f + expf(-x));  // d softplus / dx
+    float dk = x >= 0.f ? __frcp_rn(1.f + ex) : ex * __frcp_rn(1.f + ex);  // d softplus / dx
     if (kap > kKappaMax) {
       kap = kKappaMax;
       dk = 0.f;

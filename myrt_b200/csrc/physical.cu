@@ -169,8 +169,8 @@ __device__ __forceinline__ rs::rng_t sdf_stream(pt_job const& J, uint32_t path, 
 // ---- extend: closest hit over meshes, SDF drawables and lights ---------------------------
 // hits[3i] = (position, kind): kind >= 0 material index, -1 miss, -2 - l light l;
 // hits[3i+1] = (shading normal, t); hits[3i+2] = (geometric normal, 0).
-template <bool SDF>
-__global__ void __launch_bounds__(kPtBlock, 8) k_pt_extend(pt_wave w, int v, float4 const* __restrict__ q,
+template <bool SDF, int MINB = 8>
+__global__ void __launch_bounds__(kPtBlock, MINB) k_pt_extend(pt_wave w, int v, float4 const* __restrict__ q,
     uint32_t const* __restrict__ count, float4* __restrict__ hits, uint32_t* __restrict__ clear_a,
     uint32_t* __restrict__ clear_b, unsigned long long* __restrict__ stats) {
   uint32_t const n = *count;
@@ -408,8 +408,8 @@ __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_wave w, int v, shade_i
 }
 
 // ---- shadow ------------------------------------------------------------------------------
-template <bool SDF>
-__global__ void __launch_bounds__(kPtBlock, 8) k_pt_shadow(pt_wave w, int v, float4 const* __restrict__ sq,
+template <bool SDF, int MINB = 8>
+__global__ void __launch_bounds__(kPtBlock, MINB) k_pt_shadow(pt_wave w, int v, float4 const* __restrict__ sq,
     uint32_t const* __restrict__ count, float4* __restrict__ radiance, unsigned long long* __restrict__ stats) {
   uint32_t const n = *count;
   if (blockIdx.x == 0 && threadIdx.x == 0) stats[2] += n;
@@ -615,16 +615,26 @@ int launch_plan(myrt_ctx* ctx, physical_state& P, cudaStream_t st, pt_scene cons
   for (size_t wi = 0; wi < plan.size(); ++wi) {
     wave_plan const& wp = plan[wi];
     pt_wave w{d_scenes, d_jobs + wi * nj, int(nj), wp.n_paths, ctx->d_err};
+    // extend / shade / shadow: queue entries (at most the wave's paths) per thread
+    bool const per_entry = ctx->tuning.pt_grid != 1;
+    uint32_t const qgrid = per_entry
+        ? std::max<uint32_t>(1u, uint32_t((uint64_t(wp.n_paths) + kPtBlock - 1) / kPtBlock))
+        : grid;
+    // one thread per entry: pt_blocks_per_sm >= 10 selects the traversal kernels' 10-blocks register cap
+    bool const cap10 = per_entry && ctx->tuning.pt_blocks_per_sm >= 10;
     if (gd) guide_begin_wave(ctx, *gd);
     k_pt_camera<<<grid, kPtBlock, 0, st>>>(w, P.queue[0], P.radiance, P.counts + 0);
     int cur = 0;
     for (int v = 0; v <= wp.max_depth; ++v) {
       bool const last = v == wp.max_depth;
       if (any_sdf)
-        k_pt_extend<true><<<grid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
+        k_pt_extend<true><<<qgrid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
+            P.counts + (1 - cur), P.counts + 2, P.stats);
+      else if (cap10)
+        k_pt_extend<false, 10><<<qgrid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
             P.counts + (1 - cur), P.counts + 2, P.stats);
       else
-        k_pt_extend<false><<<grid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
+        k_pt_extend<false><<<qgrid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
             P.counts + (1 - cur), P.counts + 2, P.stats);
       guide_dev gv = gd ? *gd : guide_dev{};
       if (last) gv.n_lobes = 0;
@@ -634,10 +644,11 @@ int launch_plan(myrt_ctx* ctx, physical_state& P, cudaStream_t st, pt_scene cons
       }
       shade_io io{P.queue[cur], P.hits, P.counts + cur, P.queue[1 - cur], P.counts + (1 - cur), P.shadow,
           P.counts + 2, P.radiance, gv};
-      k_pt_shade<<<grid, kPtBlock, 0, st>>>(w, v, io);
+      k_pt_shade<<<qgrid, kPtBlock, 0, st>>>(w, v, io);
       if (!last && n_lights_max > 0) {
-        if (any_sdf) k_pt_shadow<true><<<grid, kPtBlock, 0, st>>>(w, v, P.shadow, P.counts + 2, P.radiance, P.stats);
-        else k_pt_shadow<false><<<grid, kPtBlock, 0, st>>>(w, v, P.shadow, P.counts + 2, P.radiance, P.stats);
+        if (any_sdf) k_pt_shadow<true><<<qgrid, kPtBlock, 0, st>>>(w, v, P.shadow, P.counts + 2, P.radiance, P.stats);
+        else if (cap10) k_pt_shadow<false, 10><<<qgrid, kPtBlock, 0, st>>>(w, v, P.shadow, P.counts + 2, P.radiance, P.stats);
+        else k_pt_shadow<false><<<qgrid, kPtBlock, 0, st>>>(w, v, P.shadow, P.counts + 2, P.radiance, P.stats);
       }
       cur = 1 - cur;
     }
