@@ -233,29 +233,155 @@ __global__ void __launch_bounds__(256) k_guide_gather(float4 const* __restrict__
 }
 
 // ---- k_guide_forward --------------------------------------------------------------------
-// Shared memory (from a 1024-aligned base): W tiles 4 x 8 KB, H tile 16 KB,
-// biases 1 KB, mbarrier, TMEM address, the stall-test mbarrier.
-constexpr uint32_t kFwdW = 0, kFwdH = 32768, kFwdBias = 49152, kFwdBar = 50176, kFwdTmem = 50184, kFwdStall = 50192;
-constexpr uint32_t kFwdSmem = 50200 + 1024;
+// Four warpgroups per CTA, each with its own 128-row tile, H tile, 64 TMEM
+// columns and mbarrier; the four weight tiles are shared. A thread owns one row
+// of its group's tile and keeps at most 32 accumulator columns in registers at a
+// time (encoding, layer epilogues and the mixture head run in 8- or 32-column
+// pieces), so 512 threads fit at 64 registers and two CTAs -- eight tiles in
+// flight, 32 warps -- share an SM, one tile's MMAs overlapping the others'
+// epilogues.
+// Shared memory (from a 1024-aligned base): W tiles 4 x 8 KB, H tiles 4 x 16 KB,
+// biases 1 KB, 4 mbarriers, 4 stall-test mbarriers, TMEM address.
+constexpr uint32_t kFwdGroups = 4;
+constexpr uint32_t kFwdW = 0, kFwdH = 32768, kFwdBias = 98304, kFwdBar = 99328, kFwdStall = 99360, kFwdTmem = 99392;
+constexpr uint32_t kFwdSmem = 99400 + 1024;
 
 __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
   uint32_t const s = tc::smem_u32(p);
   return p + ((1024u - (s & 1023u)) & 1023u);
 }
 
-__global__ void __launch_bounds__(128) k_guide_forward(mlp_args a, float4 const* __restrict__ points,
+// Encoding of one point (as encode()) written to row r of a swizzled tile in
+// eight 16-byte chunks, each stored as soon as its 8 features exist.
+__device__ __forceinline__ void encode_store(mlp_args const& a, float4 p, float4 n, float4 wo, uint8_t* tile,
+    uint32_t r) {
+  float pn[3] = {(p.x - a.center[0]) * a.inv_half[0], (p.y - a.center[1]) * a.inv_half[1],
+      (p.z - a.center[2]) * a.inv_half[2]};
+  float sn[3], cs[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    pn[k] = fminf(fmaxf(pn[k], -1.f), 1.f);
+    sincospif(pn[k], &sn[k], &cs[k]);
+  }
+  float buf[8];
+  auto put = [&](int i, float v) {
+    buf[i & 7] = v;
+    if ((i & 7) == 7) {
+      uint4 q;
+      q.x = tc::pack_bf16(buf[0], buf[1]);
+      q.y = tc::pack_bf16(buf[2], buf[3]);
+      q.z = tc::pack_bf16(buf[4], buf[5]);
+      q.w = tc::pack_bf16(buf[6], buf[7]);
+      *reinterpret_cast<uint4*>(tile + tc::sw128_offset(r, uint32_t(i >> 3))) = q;
+    }
+  };
+  put(0, pn[0]);
+  put(1, pn[1]);
+  put(2, pn[2]);
+#pragma unroll
+  for (int fr = 0; fr < 6; ++fr) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      put(3 + 6 * fr + 2 * k, sn[k]);
+      put(4 + 6 * fr + 2 * k, cs[k]);
+      float const s2 = 2.f * sn[k] * cs[k];
+      cs[k] = fmaf(-2.f * sn[k], sn[k], 1.f);
+      sn[k] = s2;
+    }
+  }
+  put(39, n.x);
+  put(40, n.y);
+  put(41, n.z);
+  put(42, wo.x);
+  put(43, wo.y);
+  put(44, wo.z);
+  put(45, 1.f);
+#pragma unroll
+  for (int k = 46; k < 64; ++k) put(k, 0.f);
+}
+
+// Hidden-layer epilogue of one row: accumulator + bias, ReLU, BF16, back into
+// the group's H tile (the next layer's A operand), 32 columns at a time.
+__device__ __forceinline__ void relu_to_tile(uint32_t tacc, float const* bias, uint8_t* tile, uint32_t r) {
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    float v[32];
+    tc::tmem_ld32(tacc + 32u * h, v);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float x[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) x[j] = fmaxf(v[8 * c + j] + bias[32 * h + 8 * c + j], 0.f);
+      uint4 q;
+      q.x = tc::pack_bf16(x[0], x[1]);
+      q.y = tc::pack_bf16(x[2], x[3]);
+      q.z = tc::pack_bf16(x[4], x[5]);
+      q.w = tc::pack_bf16(x[6], x[7]);
+      *reinterpret_cast<uint4*>(tile + tc::sw128_offset(r, uint32_t(4 * h + c))) = q;
+    }
+  }
+}
+
+// Output layer of one row -> its mixture (as mixture()) written as 16 float4:
+// o[k] = (mu, kappa), o[8 + k] = (w, vmf normaliser, cdf, flag on k = 0). The
+// TMEM loads are warp-wide (every lane runs them); only rows that hold a point
+// (`store`) write.
+__device__ __forceinline__ void head_to_lobes(uint32_t tacc, float const* bias, bool store, float flag, float4* o) {
+  float v[40];
+  {
+    float lo[32], hi[8];
+    tc::tmem_ld32(tacc, lo);
+    tc::tmem_ld8(tacc + 32u, hi);
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = lo[j] + bias[j];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[32 + j] = hi[j] + bias[32 + j];
+  }
+  float mx = v[0];
+#pragma unroll
+  for (int k = 1; k < kGuideLobes; ++k) mx = fmaxf(mx, v[5 * k]);
+  float sum = 0.f;
+#pragma unroll
+  for (int k = 0; k < kGuideLobes; ++k) {
+    v[5 * k] = __expf(v[5 * k] - mx);
+    sum += v[5 * k];
+  }
+  float cdf = 0.f;
+#pragma unroll
+  for (int k = 0; k < kGuideLobes; ++k) {
+    float const w = v[5 * k] / sum;
+    float const x = v[5 * k + 1];
+    float const ex = __expf(-fabsf(x));
+    float const kap = fminf(fmaxf(x, 0.f) + log1pf(ex) + kKappaMin, kKappaMax);
+    float const mx3 = v[5 * k + 2], my = v[5 * k + 3], mz = v[5 * k + 4];
+    float const len = sqrtf(mx3 * mx3 + my * my + mz * mz);
+    float4 mu = make_float4(0.f, 0.f, 1.f, kap);
+    if (len > 1e-6f) mu = make_float4(mx3 / len, my / len, mz / len, kap);
+    cdf += w;
+    if (store) {
+      o[k] = mu;
+      o[kGuideLobes + k] = make_float4(w, vmf_norm(kap), k == kGuideLobes - 1 ? 1.f : cdf, k == 0 ? flag : 0.f);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128 * kFwdGroups, 2) k_guide_forward(mlp_args a, float4 const* __restrict__ points,
     uint32_t const* __restrict__ count_ptr, uint32_t n_fixed, float4* __restrict__ lobes) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = align1024(smem_raw);
   uint8_t* wt = sm + kFwdW;
-  uint8_t* ht = sm + kFwdH;
   float* bias = reinterpret_cast<float*>(sm + kFwdBias);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFwdBar);
-  uint64_t* stall_bar = reinterpret_cast<uint64_t*>(sm + kFwdStall);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + kFwdTmem);
-  uint32_t const tid = threadIdx.x, warp = tid >> 5;
+  uint32_t const warp = threadIdx.x >> 5;
+  uint32_t const g = warp >> 2;                 // warpgroup: its tile, H buffer, TMEM columns, barrier
+  uint32_t const q = warp & 3u;                 // TMEM lane quarter of this warp
+  uint32_t const tid = threadIdx.x & 127u;      // row of the group's tile
+  uint8_t* ht = sm + kFwdH + 16384u * g;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFwdBar) + g;
+  uint64_t* stall_bar = reinterpret_cast<uint64_t*>(sm + kFwdStall) + g;
+  uint32_t const bar_id = 1u + g;
   if (warp == 0) {
-    tc::tmem_alloc(tmem_slot, 64);
+    tc::tmem_alloc(tmem_slot, 64 * kFwdGroups);
     tc::tmem_relinquish();
   }
   if (tid == 0) {
@@ -267,28 +393,27 @@ __global__ void __launch_bounds__(128) k_guide_forward(mlp_args a, float4 const*
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  uint32_t const tmem = *tmem_slot;
+  uint32_t const tmem = *tmem_slot + 64u * g;          // this group's accumulator columns
+  uint32_t const tacc = tmem + ((32u * q) << 16);      // ... at this warp's lanes
   uint32_t const n = count_ptr ? *count_ptr : n_fixed;
   uint32_t phase = 0;
   bool failed = false;
   bool first_wait = true;
   constexpr uint32_t kIdF = tc::idesc_bf16_m128_n64(false, false);
-  for (uint32_t tile = blockIdx.x; tile * 128u < n && !failed; tile += gridDim.x) {
+  for (uint32_t tile = blockIdx.x * kFwdGroups + g; tile * 128u < n && !failed; tile += gridDim.x * kFwdGroups) {
     uint32_t const row = tile * 128u + tid;
     bool const valid = row < n;
-    float f[64];
     float4 p{0.f, 0.f, 0.f, 0.f}, nn{0.f, 0.f, 1.f, 0.f}, wo{0.f, 0.f, 1.f, 0.f};
     if (valid) {
       p = points[3 * size_t(row)];
       nn = points[3 * size_t(row) + 1];
       wo = points[3 * size_t(row) + 2];
     }
-    encode(a, p, nn, wo, f);
-    store_row(ht, tid, f);
+    encode_store(a, p, nn, wo, ht, tid);
     for (int l = 0; l < kLayers; ++l) {
       tc::fence_proxy_async();
       tc::fence_before_sync();
-      __syncthreads();
+      tc::named_bar_sync(bar_id, 128);
       if (tid == 0) {
         tc::fence_after_sync();
         uint32_t const ha = tc::smem_u32(ht), wa = tc::smem_u32(wt + l * 8192);
@@ -302,29 +427,15 @@ __global__ void __launch_bounds__(128) k_guide_forward(mlp_args a, float4 const*
           first_wait ? a.poll_limit : kPollLimit);
       first_wait = false;
       phase ^= 1u;
-      if (__syncthreads_or(!ok)) {
+      if (tc::named_bar_or(bar_id, 128, !ok)) {
         failed = true;
         break;
       }
       tc::fence_after_sync();
-      acc_row(tmem, 0, bias + 64 * l, f);
-      if (l < kLayers - 1) {
-#pragma unroll
-        for (int j = 0; j < 64; ++j) f[j] = fmaxf(f[j], 0.f);
-        store_row(ht, tid, f);
-      } else if (valid) {
-        lobe_set L;
-        mixture(f, L);
-        float4* o = lobes + size_t(row) * 2 * kGuideLobes;
-        float cdf = 0.f;
-#pragma unroll
-        for (int k = 0; k < kGuideLobes; ++k) {
-          cdf += L.w[k];
-          o[k] = make_float4(L.mu[k][0], L.mu[k][1], L.mu[k][2], L.kappa[k]);
-          o[kGuideLobes + k] = make_float4(L.w[k], vmf_norm(L.kappa[k]), k == kGuideLobes - 1 ? 1.f : cdf,
-              k == 0 ? p.w : 0.f);
-        }
-      }
+      if (l < kLayers - 1)
+        relu_to_tile(tacc, bias + 64 * l, ht, tid);
+      else
+        head_to_lobes(tacc, bias + 64 * l, valid, p.w, lobes + size_t(valid ? row : 0u) * 2 * kGuideLobes);
     }
   }
   if (failed) {
@@ -335,7 +446,7 @@ __global__ void __launch_bounds__(128) k_guide_forward(mlp_args a, float4 const*
   __syncthreads();
   if (warp == 0) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(tmem, 64);
+    tc::tmem_dealloc(*tmem_slot, 64 * kFwdGroups);
   }
 }
 
@@ -782,8 +893,9 @@ mlp_args make_mlp(myrt_ctx* ctx) {
 int launch_forward(myrt_ctx* ctx, mlp_args const& a, float4 const* points, uint32_t const* count, uint32_t n_fixed,
     size_t max_rows, float4* lobes, cudaStream_t st) {
   uint32_t const tiles = uint32_t((max_rows + 127) / 128);
-  uint32_t const grid = std::max(1u, std::min(tiles, uint32_t(std::max(ctx->sm_count, 1)) * 4u));
-  k_guide_forward<<<grid, 128, kFwdSmem, st>>>(a, points, count, n_fixed, lobes);
+  uint32_t const ctas = (tiles + kFwdGroups - 1) / kFwdGroups;
+  uint32_t const grid = std::max(1u, std::min(ctas, uint32_t(std::max(ctx->sm_count, 1)) * 2u));
+  k_guide_forward<<<grid, 128 * kFwdGroups, kFwdSmem, st>>>(a, points, count, n_fixed, lobes);
   return check_cuda(ctx, cudaGetLastError(), "guide forward launch");
 }
 
