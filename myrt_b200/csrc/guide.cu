@@ -311,22 +311,25 @@ __device__ __forceinline__ void relu_to_tile(uint32_t tacc, float const* bias, u
     for (int c = 0; c < 4; ++c) {
       float x[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) x[j] = fmaxf(v[8 * c + j] + bias[32 * h + 8 * c + j], 0.f);
-      uint4 q;
-      q.x = tc::pack_bf16(x[0], x[1]);
-      q.y = tc::pack_bf16(x[2], x[3]);
-      q.z = tc::pack_bf16(x[4], x[5]);
-      q.w = tc::pack_bf16(x[6], x[7]);
+      for (int j = 0; j < 8; ++j) x[j] = v[8 * c + j] + bias[32 * h + 8 * c + j];
+      uint4 q;  // ReLU inside the BF16 conversion
+      q.x = tc::pack_bf16_relu(x[0], x[1]);
+      q.y = tc::pack_bf16_relu(x[2], x[3]);
+      q.z = tc::pack_bf16_relu(x[4], x[5]);
+      q.w = tc::pack_bf16_relu(x[6], x[7]);
       *reinterpret_cast<uint4*>(tile + tc::sw128_offset(r, uint32_t(4 * h + c))) = q;
     }
   }
 }
 
-// Output layer of one row -> its mixture (as mixture()) written as 16 float4:
-// o[k] = (mu, kappa), o[8 + k] = (w, vmf normaliser, cdf, flag on k = 0). The
-// TMEM loads are warp-wide (every lane runs them); only rows that hold a point
-// (`store`) write.
-__device__ __forceinline__ void head_to_lobes(uint32_t tacc, float const* bias, bool store, float flag, float4* o) {
+// Output layer of one row -> its mixture (as mixture()) as 16 float4:
+// o[k] = (mu, kappa), o[8 + k] = (w, vmf normaliser, cdf, flag on k = 0).
+// The first eight go to row r of the swizzled staging tile `st` (the group's H
+// tile, free once the last layer's MMA is done), the other eight to the row's
+// own 32 accumulator columns in TMEM (already read); the group copies them out
+// as whole 128-byte segments, one half at a time. TMEM loads and stores are
+// warp-wide.
+__device__ __forceinline__ void head_to_stage(uint32_t tacc, float const* bias, float flag, uint8_t* st, uint32_t r) {
   float v[40];
   {
     float lo[32], hi[8];
@@ -346,22 +349,51 @@ __device__ __forceinline__ void head_to_lobes(uint32_t tacc, float const* bias, 
     v[5 * k] = __expf(v[5 * k] - mx);
     sum += v[5 * k];
   }
+  // fast intrinsics here: the lobes feed sampling and pdfs that always use the
+  // stored values, so only their consistency matters, not their last bits
+  float second[32];
   float cdf = 0.f;
+  float const inv_sum = __frcp_rn(sum);
 #pragma unroll
   for (int k = 0; k < kGuideLobes; ++k) {
-    float const w = v[5 * k] / sum;
+    float const w = v[5 * k] * inv_sum;
     float const x = v[5 * k + 1];
-    float const ex = __expf(-fabsf(x));
-    float const kap = fminf(fmaxf(x, 0.f) + log1pf(ex) + kKappaMin, kKappaMax);
-    float const mx3 = v[5 * k + 2], my = v[5 * k + 3], mz = v[5 * k + 4];
-    float const len = sqrtf(mx3 * mx3 + my * my + mz * mz);
-    float4 mu = make_float4(0.f, 0.f, 1.f, kap);
-    if (len > 1e-6f) mu = make_float4(mx3 / len, my / len, mz / len, kap);
+    float const kap = fminf(fmaxf(x, 0.f) + __logf(1.f + __expf(-fabsf(x))) + kKappaMin, kKappaMax);
     cdf += w;
-    if (store) {
-      o[k] = mu;
-      o[kGuideLobes + k] = make_float4(w, vmf_norm(kap), k == kGuideLobes - 1 ? 1.f : cdf, k == 0 ? flag : 0.f);
-    }
+    float const mx3 = v[5 * k + 2], my = v[5 * k + 3], mz = v[5 * k + 4];
+    float const l2 = mx3 * mx3 + my * my + mz * mz;
+    float const il = rsqrtf(l2);
+    float4 const mu = l2 > 1e-12f ? make_float4(mx3 * il, my * il, mz * il, kap) : make_float4(0.f, 0.f, 1.f, kap);
+    *reinterpret_cast<float4*>(st + tc::sw128_offset(r, uint32_t(k))) = mu;
+    second[4 * k + 0] = w;
+    second[4 * k + 1] = __fdividef(kap, -6.28318530717958648f * (__expf(-2.f * kap) - 1.f));
+    second[4 * k + 2] = k == kGuideLobes - 1 ? 1.f : cdf;
+    second[4 * k + 3] = k == 0 ? flag : 0.f;
+  }
+  tc::tmem_st32(tacc, second);
+}
+
+// The second half back from TMEM into the staging tile.
+__device__ __forceinline__ void second_to_stage(uint32_t tacc, uint8_t* st, uint32_t r) {
+  float v[32];
+  tc::tmem_ld32(tacc, v);
+#pragma unroll
+  for (int k = 0; k < kGuideLobes; ++k)
+    *reinterpret_cast<float4*>(st + tc::sw128_offset(r, uint32_t(k))) =
+        make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+}
+
+// The group's staged 128 x 128-byte tile -> half `half` of the output rows
+// (rows of 256 bytes); each warp store covers four whole 128-byte segments.
+__device__ __forceinline__ void stage_out(uint8_t const* st, uint32_t tid, uint32_t first_row, uint32_t n, int half,
+    float4* lobes) {
+#pragma unroll
+  for (uint32_t i = 0; i < 8; ++i) {
+    uint32_t const idx = tid + 128u * i;
+    uint32_t const r = idx >> 3, c = idx & 7u;
+    if (first_row + r < n)
+      lobes[size_t(first_row + r) * 2 * kGuideLobes + uint32_t(half) * kGuideLobes + c] =
+          *reinterpret_cast<float4 const*>(st + tc::sw128_offset(r, c));
   }
 }
 
@@ -432,10 +464,18 @@ __global__ void __launch_bounds__(128 * kFwdGroups, 2) k_guide_forward(mlp_args 
         break;
       }
       tc::fence_after_sync();
-      if (l < kLayers - 1)
+      if (l < kLayers - 1) {
         relu_to_tile(tacc, bias + 64 * l, ht, tid);
-      else
-        head_to_lobes(tacc, bias + 64 * l, valid, p.w, lobes + size_t(valid ? row : 0u) * 2 * kGuideLobes);
+      } else {
+        head_to_stage(tacc, bias + 64 * l, p.w, ht, tid);
+        tc::named_bar_sync(bar_id, 128);
+        stage_out(ht, tid, tile * 128u, n, 0, lobes);
+        tc::named_bar_sync(bar_id, 128);
+        second_to_stage(tacc, ht, tid);
+        tc::named_bar_sync(bar_id, 128);
+        stage_out(ht, tid, tile * 128u, n, 1, lobes);
+        tc::named_bar_sync(bar_id, 128);  // the tile is rewritten next
+      }
     }
   }
   if (failed) {
