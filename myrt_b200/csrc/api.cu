@@ -319,18 +319,20 @@ trace_args base_args(myrt_ctx* ctx) {
   return a;
 }
 
-// Host-memory query: chunks alternate between two streams so the copy of one
-// chunk overlaps the traversal of the other.
+// Host-memory query: chunks go round four streams, each running its chunks'
+// upload, traversal and download in order, so the host-to-device copy engine
+// always has the next chunk's upload queued while earlier chunks trace and
+// download (with two streams it idled while a stream's download finished).
 int host_query(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, void* out, size_t out_stride, int intersector,
     bool any) {
   size_t const chunk_bytes = size_t(kChunkRays) * (sizeof(myrt_ray) + sizeof(myrt_hit));
   int rc = ensure_stage(ctx, chunk_bytes);
   if (rc) return rc;
-  cudaStream_t lanes[2] = {ctx->stream, ctx->aux_stream};
+  cudaStream_t lanes[4] = {ctx->stream, ctx->aux_stream, ctx->copy_lanes[0], ctx->copy_lanes[1]};
   for (uint32_t c0 = 0, k = 0; c0 < n; c0 += kChunkRays, ++k) {
     uint32_t const cn = std::min(kChunkRays, n - c0);
-    cudaStream_t const s = lanes[k & 1];
-    char* base = static_cast<char*>(ctx->stage[k & 1]);
+    cudaStream_t const s = lanes[k & 3];
+    char* base = static_cast<char*>(ctx->stage[k & 3]);
     auto* d_rays = reinterpret_cast<float4*>(base);
     char* d_out = base + size_t(kChunkRays) * sizeof(myrt_ray);
     rc = check_cuda(ctx, cudaMemcpyAsync(d_rays, rays + c0, size_t(cn) * sizeof(myrt_ray), cudaMemcpyHostToDevice, s),
@@ -343,7 +345,7 @@ int host_query(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, void* out, size_
     else a.hits = reinterpret_cast<float4*>(d_out);
     // chunks stream through the copy engines, which bound this path: they are
     // traced in input order unless sorting is forced (trace_order 2)
-    rc = launch_trace(ctx, a, intersector, any, false, s, int(k & 1), true);
+    rc = launch_trace(ctx, a, intersector, any, false, s, int(k & 3), true);
     if (rc) return rc;
     rc = check_cuda(ctx,
         cudaMemcpyAsync(static_cast<char*>(out) + size_t(c0) * out_stride, d_out, size_t(cn) * out_stride,
@@ -351,7 +353,7 @@ int host_query(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, void* out, size_
         "result download");
     if (rc) return rc;
   }
-  rc = check_cuda(ctx, cudaStreamSynchronize(ctx->aux_stream), "sync");
+  for (int l = 1; l < 4 && !rc; ++l) rc = check_cuda(ctx, cudaStreamSynchronize(lanes[l]), "sync");
   if (rc) return rc;
   return myrt_sync(ctx);
 }
@@ -425,6 +427,8 @@ int myrt_ctx_create(myrt_device_opts const* opts, myrt_ctx** out) {
   int rc = check_cuda(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
   if (!rc) rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking), "stream");
   if (!rc) rc = check_cuda(ctx, cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking), "stream");
+  for (auto& cs : ctx->copy_lanes)
+    if (!rc) rc = check_cuda(ctx, cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
   if (!rc) rc = check_cuda(ctx, cudaEventCreateWithFlags(&ctx->order_event, cudaEventDisableTiming), "event");
   if (!rc) rc = check_cuda(ctx, cudaMalloc(&ctx->d_err, sizeof(uint32_t)), "error word");
   if (!rc) rc = check_cuda(ctx, cudaMemset(ctx->d_err, 0, sizeof(uint32_t)), "error word");
@@ -445,6 +449,8 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->aux_stream) cudaStreamSynchronize(ctx->aux_stream);
+  for (auto cs : ctx->copy_lanes)
+    if (cs) cudaStreamSynchronize(cs);
   free_scene(ctx->scene);
   ctx->build_scratch.release();
   cudaFree(ctx->sdf.instrs);
@@ -475,6 +481,8 @@ int myrt_ctx_destroy(myrt_ctx* ctx) {
   cudaFree(ctx->d_next);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   if (ctx->aux_stream) cudaStreamDestroy(ctx->aux_stream);
+  for (auto cs : ctx->copy_lanes)
+    if (cs) cudaStreamDestroy(cs);
   if (ctx->order_event) cudaEventDestroy(ctx->order_event);
   delete ctx;
   return MYRT_OK;

@@ -134,6 +134,7 @@ struct myrt_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaStream_t aux_stream = nullptr;  // second lane for copy/compute overlap
+  cudaStream_t copy_lanes[2] = {nullptr, nullptr};  // third and fourth lanes of the host-memory queries
   cudaEvent_t order_event = nullptr;  // orders a caller's stream after the context's stream
   std::string last_error;
   uint32_t* d_err = nullptr;          // device error word (atomicOr of ERR_* bits)
@@ -149,8 +150,8 @@ struct myrt_ctx {
   int sm_count = 0;
   uint32_t* d_next = nullptr;    // ring of ray counters for the persistent traversal
   uint32_t next_slot = 0;
-  // staging buffers of the host-memory entry points (two chunk slots)
-  void* stage[2] = {nullptr, nullptr};
+  // staging buffers of the host-memory entry points (one chunk slot per lane)
+  void* stage[4] = {nullptr, nullptr, nullptr, nullptr};
   size_t stage_bytes = 0;
   // ray-order scratch per stream lane (keys and indices, double-buffered, and
   // the radix sort's temporary storage); `done` orders reuse across streams
@@ -160,7 +161,7 @@ struct myrt_ctx {
     void* temp = nullptr;
     size_t cap = 0, temp_bytes = 0;
     cudaEvent_t done = nullptr;
-  } order[2];
+  } order[4];
   // reference-mode textures (slots) and environment cube map; d_textures
   // mirrors `textures` as {float4*, w, h, wrap} records for the kernels
   struct texture_slot {
