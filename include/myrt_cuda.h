@@ -575,7 +575,9 @@ int myrt_set_seed(myrt_ctx* ctx, uint32_t seed);
  * MYRT_ERR_UNSUPPORTED). Limits: width * height <= 65536 and
  * frames * (2 * num_bounces + 3) <= 256, else MYRT_ERR_INVALID_ARGUMENT. The
  * first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture. All
+ * (cudaGetSymbolAddress). The call must not be captured into a CUDA graph: each
+ * call draws fresh pass randomness from the context's host stream and uploads
+ * it with copies from a stack buffer, which a graph would replay frozen. All
  * calls share the array: calls that overlap on the GPU (other streams, other
  * threads) race and must be serialised by the caller. The call makes the
  * context's device current while it runs and then restores the caller's.
