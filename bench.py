@@ -55,17 +55,19 @@ def parse_args():
     p.add_argument("--budget-spp", type=int, default=None, help="guiding: plain spp budget (default 256)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=None)
-    p.add_argument("--workload", choices=["closest", "guiding", "pt", "batch", "sdf", "post", "forward"], default="closest",
+    p.add_argument("--workload", choices=["closest", "guiding", "pt", "render", "batch", "sdf", "post", "forward"],
+                   default="closest",
                    help="closest: closest-hit Mrays/s (with a reduced guided-vs-plain leg); guiding: the full "
                         "time-to-equal-relRMSE run (1024x1024, FP64 4096-spp oracle); pt: plain path tracing "
-                        "of the icosphere scene (512x512, 64 spp, depth 8); batch: 16 uneven scenes in one "
+                        "of the icosphere scene (512x512, 64 spp, depth 8); render: the reference's per-frame "
+                        "render in reference shading (512x512, 8 bounces, 64 frames); batch: 16 uneven scenes in one "
                         "CUDA graph per frame; sdf: SDF + mesh hybrid with guiding (768x768, 128 spp); post: the "
                         "per-frame post-processing chain (bloom, tonemap, FXAA) and denoise on 2048x2048; "
                         "forward: the raster preview renderer (1920x1080, 2048^2 shadow map)")
     p.add_argument("--no-guiding", action="store_true", help="skip the guided-vs-plain leg of the closest workload")
     p.add_argument("--no-c1", action="store_true", help="skip the height-field (32,768 tris, 1024^2 rays) sub-record")
     p.add_argument("--no-configs", action="store_true",
-                   help="skip the path-tracing (pt), batch and SDF sub-records of the default closest-hit run")
+                   help="skip the path-tracing (pt, render), batch and SDF sub-records of the default closest-hit run")
     p.add_argument("--sdf-cells", type=int, default=0,
                    help="sdf: cells along the longest axis of the SDF chain's group-list grid (0 = the library's "
                         "default, 1 = no grid: every primitive runs at every march step)")
@@ -721,7 +723,8 @@ def run_ours(args):
 
         sub = _ap.Namespace(**vars(args))
         sub.steps, sub.warmup, sub.res, sub.spp, sub.oracle_spp = min(args.steps, 3), 1, None, None, None
-        for key, fn in (("c2_pt", run_pt_workload), ("c3_batch", run_batch_workload), ("c5_sdf", run_sdf_workload)):
+        for key, fn in (("c2_pt", run_pt_workload), ("c2_ref", run_render_workload), ("c3_batch", run_batch_workload),
+                        ("c5_sdf", run_sdf_workload)):
             t0 = time.perf_counter()
             rec = fn(sub, emit=False)
             rec["wall_s"] = round(time.perf_counter() - t0, 1)
@@ -853,6 +856,95 @@ def run_pt_workload(args, emit: bool = True):
          f"rel_rmse_one_step_vs_fp64_{oracle_spp}spp": err_one,
          "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128,
                  "d2h_bytes_per_step": W * H * 16, "api": "myrt_render + myrt_read_accumulation"},
+         "clocks": clocks.summary()})
+    if not emit:
+        return line
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_render_workload(args, emit: bool = True):
+    """The reference's own per-frame render (sequential_pathtracer::run:
+    pt_generate, then per bounce pt_trace, pt_color and the ray filter, with
+    the host random textures of every pass) through myrt_render in reference
+    shading, on the icosphere scene with its PBR materials: 512x512, 8
+    bounces, 64 frames of one sample per pixel per step. Checks a small render
+    bit for bit against the oracle's restated passes, and times those passes
+    on the host cores for the CPU baseline."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    import torch
+
+    import myrt_b200 as mb
+    from myrt_b200.camera import look_at
+    from myrt_b200.scenes import icosphere_field
+
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    ctx = mb.Context(local)
+    scene = icosphere_field()
+    info = ctx.upload_scene(**scene)
+    W = H = args.res or 512
+    frames = args.spp or 64
+    B = 8
+    iv, ip = look_at((0.0, 1.0, -4.5), (0.0, -0.3, 0.0), vfov_deg=50, aspect=1.0)
+
+    def step():
+        ctx.render(iv, ip, W, H, num_bounces=B, frames=frames)
+
+    # parity: a small view, two frames, bit for bit against the oracle (library built-ins in both)
+    prepared = po.prepare_reference(scene)
+    pw, ph = 128, 96
+    piv, pip = look_at((0.0, 1.0, -4.5), (0.0, -0.3, 0.0), vfov_deg=50, aspect=pw / ph)
+    ctx.set_seed(77)
+    ctx.render(piv, pip, pw, ph, num_bounces=B, frames=2)
+    acc, _ = ctx.read_accumulation(pw, ph)
+    with po.glsl_math(1):
+        ref, _ = po.render_reference(scene, pw, ph, B, 2, piv, pip, seed=77, prepared=prepared)
+    parity = bool(np.array_equal(acc, ref))
+    ctx.set_seed(5489)
+    ctx.reset_accumulation()
+    for _ in range(args.warmup):
+        step()
+    with ClockSampler(local) as clocks:
+        ms = _timed_frames(ctx.stream, step, args.steps) / args.steps
+    samples = W * H * frames
+    # end to end: the host call (host random textures drawn and uploaded inside it) + the image read back
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+        ctx.read_accumulation(W, H)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    ctx.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        t0 = time.perf_counter()
+        po.render_reference(scene, W, H, B, 1, iv, ip, seed=5489, prepared=prepared)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": W * H / cpu_s, "unit": "samples/s", "cores": po.nthreads(), "kind": "port",
+               "sample": f"one frame ({W}x{H}, 1 sample per pixel, {B} bounces) of the oracle's restated "
+                         "pt_generate / pt_trace / pt_color passes (pinned to the reference's compiled shaders) "
+                         "over the reference's binary tree, all host threads; tree built beforehand",
+               "seconds": round(cpu_s, 2)}
+    passes = 2 * B + 3
+    line = _render_line(
+        "samples/s reference shading", samples / (ms / 1e3), "samples/s", args.steps, args.warmup, ms,
+        {"workload": f"the reference's per-frame render (reference shading): icosphere scene "
+                     f"({int(info['triangles']):,} tris, PBR materials), {W}x{H}, {B} bounces, "
+                     f"{frames} frames of 1 sample per pixel per step",
+         "triangles": int(info["triangles"]), "res": W, "frames_per_step": frames, "bounces": B,
+         "l2": "ray states, trace records and images (~40 MB) fit L2; the tree and triangles (35 MB) too"},
+        {"parity_bit_exact_vs_oracle": parity,
+         "parity_case": f"{pw}x{ph}, 2 frames, {B} bounces, seed 77: accumulation bit-identical to the oracle",
+         "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128 + frames * passes * 4096,
+                 "d2h_bytes_per_step": W * H * 16 * 2, "api": "myrt_render + myrt_read_accumulation"},
+         "gpu_launches": frames * (4 * B + 3),
+         "gpu_launches_note": "per frame: generate, then per bounce trace + color, plus scan + scatter of the "
+                              "surviving rays after every bounce but the last",
+         "cpu_baseline": cpu,
          "clocks": clocks.summary()})
     if not emit:
         return line
@@ -1209,6 +1301,8 @@ def main():
         return run_guiding_workload(args)
     if args.workload == "pt":
         return run_pt_workload(args)
+    if args.workload == "render":
+        return run_render_workload(args)
     if args.workload == "batch":
         return run_batch_workload(args)
     if args.workload == "sdf":

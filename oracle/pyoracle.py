@@ -437,20 +437,29 @@ def host_rng(seed: int, frames: int, bounces: int):
     return seeds, tex
 
 
-def render_reference(scene: dict, width: int, height: int, bounces: int, frames: int, inv_view, inv_proj,
-                     seed: int = 5489, accum=None, display=None, sample_index0: int = 0, textures=None,
-                     cubemap=None, dof: bool = False, lens_size=(0.2, 0.2), focus: float = 1.0,
-                     bokeh_slot: int = -1):
-    """Reference-shading render on the CPU (restated passes). scene: dict with
-    indices, vertices, normals, uvs, drawables, materials, material_data.
-    textures: list of (rgba [H, W, 4], wrap) or None per slot; cubemap:
-    [6, S, S, 4] (stored at half precision, as the device stores it)."""
-    L = oracle()
+def prepare_reference(scene: dict):
+    """World-space triangles and attributes of a scene and the reference's
+    tree over them (bvh.cpp's build restated), as render_reference uses them."""
     tris9 = bake_world_triangles(scene["indices"], scene["vertices"], scene.get("drawables"))
     nrm, uvs, mat = bake_world_attributes(scene["indices"], scene.get("normals"), scene.get("uvs"),
                                           scene.get("drawables"), len(scene["vertices"]))
     idx = np.arange(tris9.shape[0] * 3, dtype=np.uint32)
     nodes, bi = refbvh_build(idx, tris9.reshape(-1, 3))
+    return tris9, nrm, uvs, mat, nodes, bi
+
+
+def render_reference(scene: dict, width: int, height: int, bounces: int, frames: int, inv_view, inv_proj,
+                     seed: int = 5489, accum=None, display=None, sample_index0: int = 0, textures=None,
+                     cubemap=None, dof: bool = False, lens_size=(0.2, 0.2), focus: float = 1.0,
+                     bokeh_slot: int = -1, prepared=None):
+    """Reference-shading render on the CPU (restated passes). scene: dict with
+    indices, vertices, normals, uvs, drawables, materials, material_data.
+    textures: list of (rgba [H, W, 4], wrap) or None per slot; cubemap:
+    [6, S, S, 4] (stored at half precision, as the device stores it).
+    prepared: the result of prepare_reference(scene), to skip the world-space
+    bake and the tree build (scene::prepare's work) on repeated renders."""
+    L = oracle()
+    tris9, nrm, uvs, mat, nodes, bi = prepared if prepared is not None else prepare_reference(scene)
     refs = np.ascontiguousarray(scene.get("materials", np.zeros((1, 2), np.int32)), np.int32).reshape(-1, 2)
     mdata = np.ascontiguousarray(scene.get("material_data", np.zeros(7, np.float32)), np.float32).ravel()
     seeds, tex = host_rng(seed, frames, bounces)

@@ -53,3 +53,19 @@ def test_reference_arm_prints_the_library_arms_config_without_the_cuda_library()
     assert line["config"] == bench.closest_config(655_872, 512, 64, 1)
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_oracle_render_with_a_prepared_scene_equals_a_fresh_one():
+    """The render workload times the oracle's passes with the scene prepared
+    (baked and its tree built) beforehand; the image is the same."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle as po
+    from myrt_b200.camera import look_at
+    from myrt_b200.scenes import icosphere_field
+
+    s = icosphere_field(n_spheres=6, subdiv=1, floor_cells=2, seed=3)
+    iv, ip = look_at((0, 1, -4.5), (0, -0.3, 0), vfov_deg=50, aspect=1.5)
+    a, da = po.render_reference(s, 24, 16, 3, 2, iv, ip, seed=9)
+    b, db = po.render_reference(s, 24, 16, 3, 2, iv, ip, seed=9, prepared=po.prepare_reference(s))
+    assert np.array_equal(a, b) and np.array_equal(da, db)
+    assert a[..., 3].min() == 2
