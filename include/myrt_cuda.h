@@ -188,6 +188,10 @@ typedef struct myrt_tuning {
                                 blocks past the queue's count return at once; pt_blocks_per_sm >= 10
                                 then selects a 48-register cap for the mesh traversal kernels).
                                 Results never depend on it. */
+  uint32_t ref_frames;       /* reference shading (myrt_render): frames of one call whose passes run
+                                together, each in its own region of ray slots (0 = as many as fill
+                                about 4 Mi rays, at most 64; 1 = one frame at a time, as the
+                                reference; 2..64). Results never depend on it. */
 } myrt_tuning;
 
 /* ---- context ------------------------------------------------------------ */

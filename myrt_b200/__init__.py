@@ -108,10 +108,10 @@ class Context:
                    trace_min_blocks: int = 0, trace_unit_steps: int = 0, wave_paths: int = 0,
                    pt_blocks_per_sm: int = 0, trace_smem_stack: int = 0, trace_order: int = 0,
                    bvh_builder: int = 0, sdf_cells: int = 0, guide_poll_limit: int = 0, guide_stall_test: int = 0,
-                   instancing: int = 0, pt_grid: int = 0):
+                   instancing: int = 0, pt_grid: int = 0, ref_frames: int = 0):
         t = _abi.myrt_tuning(trace_persistent, refill, blocks_per_sm, trace_min_blocks, trace_unit_steps,
                              wave_paths, pt_blocks_per_sm, trace_smem_stack, bvh_builder, trace_order, sdf_cells,
-                             guide_poll_limit, guide_stall_test, instancing, pt_grid)
+                             guide_poll_limit, guide_stall_test, instancing, pt_grid, ref_frames)
         self._check(self._L.myrt_set_tuning(self._h, C.byref(t)), "myrt_set_tuning")
 
     def set_transforms(self, drawables):

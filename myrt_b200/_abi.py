@@ -134,7 +134,8 @@ class myrt_tuning(C.Structure):
                 ("pt_blocks_per_sm", C.c_uint32), ("trace_smem_stack", C.c_uint32),
                 ("bvh_builder", C.c_uint32), ("trace_order", C.c_uint32),
                 ("sdf_cells", C.c_uint32), ("guide_poll_limit", C.c_uint32), ("guide_stall_test", C.c_uint32),
-                ("instancing", C.c_uint32), ("pt_grid", C.c_uint32)]
+                ("instancing", C.c_uint32), ("pt_grid", C.c_uint32),
+                ("ref_frames", C.c_uint32)]
 
 
 SHADE_REFERENCE = 0

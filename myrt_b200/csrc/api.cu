@@ -499,7 +499,7 @@ int myrt_set_tuning(myrt_ctx* ctx, myrt_tuning const* t) {
   if (t->trace_persistent > 1 || t->refill < 1 || t->refill > 32 || t->blocks_per_sm > 64 || t->trace_min_blocks > 16 ||
       t->trace_unit_steps > 1 || (t->wave_paths != 0 && (t->wave_paths < 1024 || t->wave_paths > (1u << 28))) ||
       t->pt_blocks_per_sm > 16 || t->trace_smem_stack > 1 || t->trace_order > 2 || t->bvh_builder > 1 || t->sdf_cells > 128 ||
-      t->guide_stall_test > 1 || t->instancing > 2 || t->pt_grid > 2)
+      t->guide_stall_test > 1 || t->instancing > 2 || t->pt_grid > 2 || t->ref_frames > 64)
     return set_error(ctx, MYRT_ERR_INVALID_ARGUMENT, "tuning out of range");
   ctx->tuning = *t;
   return MYRT_OK;

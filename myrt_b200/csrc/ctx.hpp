@@ -102,6 +102,8 @@ struct render_state {
   uint32_t* counts = nullptr;           // [2] active ray counts (ping-pong)
   uint32_t* block_sums = nullptr;       // per-block survivor counts, then offsets
   float* pass_tex = nullptr;            // frames * passes * 1024 random texture floats
+  float4* fcol = nullptr;               // frames in flight: final colour per frame and pixel
+  uint32_t frames_cap = 0;              // frames in flight the ray buffers hold
   size_t pass_tex_capacity = 0;         // in floats
   uint32_t sample_counter = 0;          // frames accumulated since the last reset
   int64_t pending_first = -1;           // myrt_begin_samples: first sample index of the next render
@@ -146,7 +148,7 @@ struct myrt_ctx {
   myrt_b200::guide_state* guide = nullptr;  // learned proposal (guide.cu), created on first use
   uint64_t guide_generation = 0;            // bumped by scene uploads
   std::mt19937 host_rng{5489u};  // sequential_pathtracer::m_rng (default-constructed)
-  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  myrt_tuning tuning{0u, 1u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
   int sm_count = 0;
   uint32_t* d_next = nullptr;    // ring of ray counters for the persistent traversal
   uint32_t next_slot = 0;

@@ -18,6 +18,15 @@
 // std::mt19937 in the reference's order) is generated for all frames of a
 // call up front and copied to the device once.
 //
+// Frames in flight: the reference renders a call's frames one after another,
+// each pass over one image of rays. Here up to kMaxFramesInFlight frames of a
+// call run their passes together (about 4 Mi rays per launch instead of one
+// image's), each in its own region of ray slots with its own ray counts,
+// compaction, pass randomness and slot ids, so every ray sees exactly what it
+// would see alone. A path's final colour is kept per frame and pixel, and
+// k_resolve_frames then accumulates the frames in their order, pixel by pixel:
+// the images equal the sequential ones bit for bit.
+//
 // Compiled with -fmad=false (see build.py): the shading arithmetic rounds every
 // operation as written, like the CPU oracle.
 #include <cuda_runtime.h>
@@ -43,6 +52,25 @@ using rs::v3;
 
 constexpr int kBlock = 256;
 constexpr int kTexSize = 1024;
+constexpr int kMaxFramesInFlight = 64;
+
+// One pass's randomness for every frame in flight: frame f's texture at
+// tex + f * tex_stride, its seed in seed[f].
+struct pass_rand {
+  float const* tex;
+  uint32_t tex_stride;  // floats
+  int seed[kMaxFramesInFlight];
+};
+
+// Frame and slot of this thread when each frame in flight owns `nb`
+// consecutive blocks (its region of ray slots).
+struct frame_slot {
+  uint32_t f, id;
+};
+__device__ __forceinline__ frame_slot frame_of(uint32_t nb) {
+  uint32_t const f = blockIdx.x / nb;
+  return {f, (blockIdx.x - f * nb) * blockDim.x + threadIdx.x};
+}
 
 struct scene_dev {
   uint4 const* nodes;
@@ -93,10 +121,15 @@ __device__ __forceinline__ float intersect_sphere(v3 r0, v3 rd, v3 s0, float sr)
 }
 
 // ---- pt_generate.comp -----------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_generate(uint32_t W, uint32_t H, float const* __restrict__ tex, int seed,
+// gen: the frames' regions of W * H slots; count[f] = W * H.
+__global__ void __launch_bounds__(kBlock) k_generate(uint32_t W, uint32_t H, uint32_t nb, pass_rand pr,
     camera_dev cam, float4* __restrict__ gen, uint32_t* __restrict__ count) {
-  uint32_t const id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id == 0) *count = W * H;
+  frame_slot const fs = frame_of(nb);
+  uint32_t const id = fs.id;
+  float const* const tex = pr.tex + fs.f * pr.tex_stride;
+  int const seed = pr.seed[fs.f];
+  gen += 5 * size_t(fs.f) * W * H;
+  if (id == 0) count[fs.f] = W * H;
   if (id >= W * H) return;
   int const x = int(id % W), y = int(id / W);
   rs::rng_t r;
@@ -150,23 +183,26 @@ __global__ void __launch_bounds__(kBlock) k_generate(uint32_t W, uint32_t H, flo
 }
 
 // ---- pt_trace.comp --------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, float const* __restrict__ tex, int seed,
-    float4 const* __restrict__ gen, float4* __restrict__ trace, uint32_t const* __restrict__ count) {
-  uint32_t const id = blockIdx.x * blockDim.x + threadIdx.x;
-  if (id >= *count) return;
+// One thread per ray of the pass. The steps are ordered so that little state
+// is live across the two tree walks: the closest-hit walk needs only the ray;
+// pt_trace.comp:134-146's random draws (light choice, point on the light) come
+// after it -- the walk draws nothing, and the SDF marches, which do draw, still
+// follow them as in the reference; the trace record is written before the
+// shadow walk, which then only adds the light term. Same operations, same
+// results as the reference's order.
+// gen / trace: the frames' regions of `slots` rays; count[f]: frame f's rays.
+__global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, pass_rand pr, float4 const* __restrict__ gen,
+    float4* __restrict__ trace, uint32_t const* __restrict__ count, uint32_t slots, uint32_t nb) {
+  frame_slot const fs = frame_of(nb);
+  uint32_t const id = fs.id;
+  if (id >= count[fs.f]) return;
+  float const* const tex = pr.tex + fs.f * pr.tex_stride;
+  int const seed = pr.seed[fs.f];
+  gen += 5 * size_t(fs.f) * slots;
+  trace += 4 * size_t(fs.f) * slots;
   float4 const g0 = gen[5 * size_t(id) + 0];
   float4 const g1 = gen[5 * size_t(id) + 1];
-  float4 const g2 = gen[5 * size_t(id) + 2];
   v3 const ro = xyz(g0), rd = xyz(g1);
-  rs::rng_t r;
-  rs::random_init(r, tex, rs::f2i(g1.w), rs::f2i(g2.w), seed);
-  int const li = min(max(rs::f2i(2.f * rs::random_next(r)), 0), 1);
-  float const rx = rs::random_next(r);
-  float const ry = rs::random_next(r);
-  float const rz = rs::random_next(r);
-  float const rq = rs::random_next(r);
-  light_t const L = c_lights[li];
-  v3 const p_on_light = v3{L.px, L.py, L.pz} + rs::normalize(v3{rx, ry, rz}) * L.r * sqrtf(rq);
 
   hit_rec h;
   uint32_t cn = 0, ct = 0;
@@ -198,6 +234,21 @@ __global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, float const*
     }
     material = __ldg(s.tri_material + prim);
   }
+
+  float4 const g2 = gen[5 * size_t(id) + 2];
+  rs::rng_t r;
+  rs::random_init(r, tex, rs::f2i(g1.w), rs::f2i(g2.w), seed);
+  int const li = min(max(rs::f2i(2.f * rs::random_next(r)), 0), 1);
+  float const rx = rs::random_next(r);
+  float const ry = rs::random_next(r);
+  float const rz = rs::random_next(r);
+  float const rq = rs::random_next(r);
+  v3 p_on_light;
+  {
+    light_t const L = c_lights[li];
+    p_on_light = v3{L.px, L.py, L.pz} + rs::normalize(v3{rx, ry, rz}) * L.r * sqrtf(rq);
+  }
+
   // SDF drawables after the meshes (pt_trace.comp:342-352): a closer march hit
   // replaces the mesh hit and its attributes.
   for (int dsdf = 0; dsdf < s.sdf.n_drawables; ++dsdf) {
@@ -225,12 +276,15 @@ __global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, float const*
   uint32_t light_color = 0;
   v3 light_dir{0.f, 0.f, 0.f};
   float light_strength = 0.f;
+  bool shadow = false;
+  v3 so{0.f, 0.f, 0.f}, dir_l{0.f, 0.f, 0.f};
+  float dist_l = 0.f;
   if (hits) {
     intersects = 1;
     if (rs::inf3(normal) || rs::nan3(normal)) intersects = 0;
     v3 const path = p_on_light - position;
-    v3 const dir_l = rs::normalize(path);
-    float const dist_l = rs::length(path);
+    dir_l = rs::normalize(path);
+    dist_l = rs::length(path);
     v3 const lnorm = rs::faceforward(normal, rd, normal);
     if (hits_light >= 0) {
       intersects = 2;
@@ -240,21 +294,8 @@ __global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, float const*
           0.f / light_strength);
       light_dir = dir_l;
     } else if (rs::dot(dir_l, lnorm) > 0.f) {
-      v3 const so = position + lnorm * 0.01f;
-      hit_rec hs;
-      bool occluded = traverse<0, true, false>(s.nodes, s.tris, f3{so.x, so.y, so.z},
-          f3{dir_l.x, dir_l.y, dir_l.z}, 0.f, dist_l, hs, s.err, cn, ct);
-      // any_hit's SDF loop (pt_trace.comp:319-327)
-      for (int dsdf = 0; !occluded && dsdf < s.sdf.n_drawables; ++dsdf)
-        occluded = sdfk::march(s.sdf, dsdf, so, dir_l, dist_l, true, &r).hits;
-      if (!occluded) {
-        v3 const col{L.cx, L.cy, L.cz};
-        light_strength = rs::length(col);
-        light_color = rs::pack_unorm4x8(col.x / light_strength, col.y / light_strength, col.z / light_strength,
-            0.f / light_strength);
-        light_strength = light_strength * (2.f / dist_l);
-        light_dir = dir_l;
-      }
+      so = position + lnorm * 0.01f;
+      shadow = true;
     }
   } else {
     position = {0.f, 0.f, 0.f};
@@ -265,6 +306,21 @@ __global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, float const*
   t[1] = make_float4(normal.x, normal.y, normal.z, __uint_as_float(id));
   t[2] = make_float4(uv.x, uv.y, __int_as_float(material), __uint_as_float(light_color));
   t[3] = make_float4(light_dir.x, light_dir.y, light_dir.z, light_strength);
+  if (!shadow) return;
+  hit_rec hs;
+  bool occluded = traverse<0, true, false>(s.nodes, s.tris, f3{so.x, so.y, so.z}, f3{dir_l.x, dir_l.y, dir_l.z},
+      0.f, dist_l, hs, s.err, cn, ct);
+  // any_hit's SDF loop (pt_trace.comp:319-327)
+  for (int dsdf = 0; !occluded && dsdf < s.sdf.n_drawables; ++dsdf)
+    occluded = sdfk::march(s.sdf, dsdf, so, dir_l, dist_l, true, &r).hits;
+  if (occluded) return;
+  v3 const col{c_lights[li].cx, c_lights[li].cy, c_lights[li].cz};
+  light_strength = rs::length(col);
+  light_color = rs::pack_unorm4x8(col.x / light_strength, col.y / light_strength, col.z / light_strength,
+      0.f / light_strength);
+  light_strength = light_strength * (2.f / dist_l);
+  reinterpret_cast<float*>(t + 2)[3] = __uint_as_float(light_color);
+  t[3] = make_float4(dir_l.x, dir_l.y, dir_l.z, light_strength);
 }
 
 // ---- pt_color.comp ----------------------------------------------------------------
@@ -301,18 +357,30 @@ __device__ __forceinline__ void accumulate(color_args const& a, float4 nc, int p
       rs::gclamp(last.z / last.w, 0.f, 4.f), 1.f);
 }
 
-__global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, float const* __restrict__ tex, int seed,
-    float4* __restrict__ gen, float4* __restrict__ trace, uint32_t const* __restrict__ count,
-    uint32_t* __restrict__ block_sums) {
-  uint32_t const id = blockIdx.x * blockDim.x + threadIdx.x;
+// A path that ends adds its colour to the accumulation (one frame in flight:
+// fcol null) or leaves it in fcol[f * slots + pixel] for k_resolve_frames.
+// block_sums[blockIdx.x]: the block's surviving rays.
+__global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, pass_rand pr, float4* __restrict__ gen,
+    float4* __restrict__ trace, uint32_t const* __restrict__ count, uint32_t* __restrict__ block_sums,
+    float4* __restrict__ fcol, uint32_t slots, uint32_t nb) {
+  frame_slot const fs = frame_of(nb);
+  uint32_t const id = fs.id;
+  float const* const tex = pr.tex + fs.f * pr.tex_stride;
+  int const seed = pr.seed[fs.f];
+  gen += 5 * size_t(fs.f) * slots;
+  trace += 4 * size_t(fs.f) * slots;
   bool keep = false;
-  if (id < *count) {
+  if (id < count[fs.f]) {
     float4* gp = gen + 5 * size_t(id);
     float4* tp = trace + 4 * size_t(id);
     float4 const t0 = tp[0], t1 = tp[1], t2 = tp[2], t3 = tp[3];
     float4 g0 = gp[0], g1 = gp[1], g2 = gp[2], g3 = gp[3], g4 = gp[4];
     int const intersects = __float_as_int(t0.w);
     int const px = rs::f2i(g1.w), py = rs::f2i(g2.w);
+    auto finish = [&](float4 nc) {
+      if (fcol) fcol[size_t(fs.f) * slots + size_t(py) * a.W + size_t(px)] = nc;
+      else accumulate(a, nc, px, py);
+    };
     v3 const refl0 = xyz(g2);
     float const pdf0 = g4.x;
     if (intersects != 0) {
@@ -320,7 +388,7 @@ __global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, float const
         reinterpret_cast<int*>(tp)[3] = 0;
         v3 const lc = rs::unpack_rgb(__float_as_uint(t2.w));
         v3 const c = lc * t3.w * refl0 / pdf0;
-        accumulate(a, make_float4(c.x + g3.x, c.y + g3.y, c.z + g3.z, 1.f + g3.w), px, py);
+        finish(make_float4(c.x + g3.x, c.y + g3.y, c.z + g3.z, 1.f + g3.w));
       } else {
         v3 const normal = xyz(t1);
         rs::rng_t r;
@@ -347,16 +415,16 @@ __global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, float const
         if (rnd > pdf0 * 1.f) {
           reinterpret_cast<int*>(tp)[3] = 0;
           v3 const c = refl0 / pdf0;
-          accumulate(a, make_float4(g3.x + c.x, g3.y + c.y, g3.z + c.z, g3.w), px, py);
+          finish(make_float4(g3.x + c.x, g3.y + c.y, g3.z + c.z, g3.w));
           done = true;
         } else if (a.force || pdf0 < 1e-5f || mpdf < 1e-6f || isnan(mpdf) || isinf(mpdf) || rs::nan3(mrefl) ||
                    rs::inf3(mrefl) || rs::nan3(generated) || rs::inf3(generated)) {
           reinterpret_cast<int*>(tp)[3] = 0;
           if (rs::nan3(mrefl) || rs::inf3(mrefl) || isnan(pdf0) || isinf(pdf0) || pdf0 < 1e-5f) {
-            accumulate(a, g3, px, py);
+            finish(g3);
           } else {
             v3 const c = refl0 / pdf0;
-            accumulate(a, make_float4(g3.x + c.x, g3.y + c.y, g3.z + c.z, g3.w), px, py);
+            finish(make_float4(g3.x + c.x, g3.y + c.y, g3.z + c.z, g3.w));
           }
           done = true;
         }
@@ -394,7 +462,7 @@ __global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, float const
         v3 const sky = rs::mix3(v3{0.3f, 0.4f, 0.5f}, v3{1.f, 0.98f, 0.96f}, t);
         env = rs::clamp3(refl0 * sky / pdf0, 0.f, 16.f);
       }
-      accumulate(a, make_float4(g3.x + env.x, g3.y + env.y, g3.z + env.z, g3.w), px, py);
+      finish(make_float4(g3.x + env.x, g3.y + env.y, g3.z + env.z, g3.w));
     }
   }
   int const c = __syncthreads_count(keep);
@@ -402,9 +470,12 @@ __global__ void __launch_bounds__(kBlock) k_color_pass(color_args a, float const
 }
 
 // ---- pt_ray_filter.comp (stable) ---------------------------------------------------
-// Exclusive scan of the per-block survivor counts (one block), total -> *new_count.
+// Exclusive scan of one frame's per-block survivor counts (block f: frame f's
+// nblocks sums), its total -> new_count[f].
 __global__ void __launch_bounds__(1024) k_scan_blocks(uint32_t* __restrict__ sums, uint32_t nblocks,
     uint32_t* __restrict__ new_count) {
+  sums += size_t(blockIdx.x) * nblocks;
+  new_count += blockIdx.x;
   __shared__ uint32_t warp_tot[32];
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
@@ -440,11 +511,19 @@ __global__ void __launch_bounds__(1024) k_scan_blocks(uint32_t* __restrict__ sum
   if (threadIdx.x == 0) *new_count = carry;
 }
 
+// Survivors of each frame's region, in order, to the front of the same region
+// of gen_out (offsets: the scanned block sums).
 __global__ void __launch_bounds__(kBlock) k_scatter(float4 const* __restrict__ gen_in, float4 const* __restrict__ trace,
-    uint32_t const* __restrict__ count, uint32_t const* __restrict__ offsets, float4* __restrict__ gen_out) {
+    uint32_t const* __restrict__ count, uint32_t const* __restrict__ offsets, float4* __restrict__ gen_out,
+    uint32_t slots, uint32_t nb) {
   __shared__ uint32_t warp_cnt[kBlock / 32];
-  uint32_t const id = blockIdx.x * blockDim.x + threadIdx.x;
-  bool const keep = id < *count && __float_as_int(trace[4 * size_t(id)].w) == 1;
+  frame_slot const fs = frame_of(nb);
+  uint32_t const id = fs.id;
+  size_t const base = size_t(fs.f) * slots;
+  gen_in += 5 * base;
+  gen_out += 5 * base;
+  trace += 4 * base;
+  bool const keep = id < count[fs.f] && __float_as_int(trace[4 * size_t(id)].w) == 1;
   uint32_t const lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   uint32_t const ballot = __ballot_sync(0xffffffffu, keep);
   if (lane == 0) warp_cnt[warp] = __popc(ballot);
@@ -459,23 +538,55 @@ __global__ void __launch_bounds__(kBlock) k_scatter(float4 const* __restrict__ g
   }
 }
 
+// The frames in flight into the accumulation, in frame order, pixel by pixel
+// (frame f restarts it when sample_index + f == 0).
+__global__ void __launch_bounds__(kBlock) k_resolve_frames(color_args a, float4 const* __restrict__ fcol,
+    uint32_t frames, uint32_t W, uint32_t H) {
+  uint32_t const pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= W * H) return;
+  uint32_t const s0 = a.sample_index;
+  for (uint32_t f = 0; f < frames; ++f) {
+    a.sample_index = s0 + f;
+    accumulate(a, fcol[size_t(f) * W * H + pix], int(pix % W), int(pix / W));
+  }
+}
+
 // ---- host side ----------------------------------------------------------------------
-int ensure_render_buffers(myrt_ctx* ctx, uint32_t W, uint32_t H) {
+void free_ray_buffers(render_state& R) {
+  for (void* p : {static_cast<void*>(R.gen[0]), static_cast<void*>(R.gen[1]), static_cast<void*>(R.trace),
+           static_cast<void*>(R.counts), static_cast<void*>(R.block_sums), static_cast<void*>(R.fcol)})
+    cudaFree(p);
+  R.gen[0] = R.gen[1] = nullptr;
+  R.trace = R.fcol = nullptr;
+  R.counts = R.block_sums = nullptr;
+  R.frames_cap = 0;
+}
+
+// Ray buffers for `frames` frames in flight of a W x H render (grown, never shrunk).
+int ensure_render_buffers(myrt_ctx* ctx, uint32_t W, uint32_t H, uint32_t frames) {
   int rc = ensure_images(ctx, W, H);
   render_state& R = ctx->render;
-  if (rc || R.gen[0]) return rc;
-  size_t const n = size_t(W) * H;
-  size_t const nb = (n + kBlock - 1) / kBlock;
+  if (rc || (R.gen[0] && R.frames_cap >= frames)) return rc;
+  rc = check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "ray buffers in use");
+  if (rc) return rc;
+  free_ray_buffers(R);
+  size_t const n = size_t(W) * H * frames;
+  size_t const nb = size_t(frames) * ((size_t(W) * H + kBlock - 1) / kBlock);
   auto alloc = [&](void** p, size_t bytes, char const* what) {
     if (!rc) rc = check_cuda(ctx, cudaMalloc(p, bytes), what);
   };
   alloc(reinterpret_cast<void**>(&R.gen[0]), n * 80, "ray state");
   alloc(reinterpret_cast<void**>(&R.gen[1]), n * 80, "ray state");
   alloc(reinterpret_cast<void**>(&R.trace), n * 64, "trace state");
-  alloc(reinterpret_cast<void**>(&R.counts), 2 * sizeof(uint32_t), "ray counts");
+  alloc(reinterpret_cast<void**>(&R.counts), 2 * kMaxFramesInFlight * sizeof(uint32_t), "ray counts");
   alloc(reinterpret_cast<void**>(&R.block_sums), std::max<size_t>(nb, 1) * sizeof(uint32_t), "block sums");
-  if (rc) free_render(R);
-  return rc;
+  if (frames > 1) alloc(reinterpret_cast<void**>(&R.fcol), n * 16, "frame colours");
+  if (rc) {
+    free_ray_buffers(R);
+    return rc;
+  }
+  R.frames_cap = frames;
+  return MYRT_OK;
 }
 
 void mat_mul4(float const* a, float const* b, float* out) {
@@ -489,13 +600,11 @@ void mat_mul4(float const* a, float const* b, float* out) {
 
 // Releases the device buffers; the camera record and the sample counter stay.
 void free_render(render_state& R) {
-  for (void* p : {static_cast<void*>(R.gen[0]), static_cast<void*>(R.gen[1]), static_cast<void*>(R.trace),
-           static_cast<void*>(R.accum), static_cast<void*>(R.display), static_cast<void*>(R.counts),
-           static_cast<void*>(R.block_sums), static_cast<void*>(R.pass_tex), static_cast<void*>(R.accum64)})
+  free_ray_buffers(R);
+  for (void* p : {static_cast<void*>(R.accum), static_cast<void*>(R.display), static_cast<void*>(R.pass_tex),
+           static_cast<void*>(R.accum64)})
     cudaFree(p);
-  R.gen[0] = R.gen[1] = nullptr;
-  R.trace = R.accum = R.display = nullptr;
-  R.counts = R.block_sums = nullptr;
+  R.accum = R.display = nullptr;
   R.pass_tex = nullptr;
   R.accum64 = nullptr;
   R.pass_tex_capacity = 0;
@@ -581,12 +690,17 @@ frame_setup make_frame_setup(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_
 
 int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_params const* p) {
   uint32_t const W = p->width, H = p->height;
-  int rc = ensure_render_buffers(ctx, W, H);
-  if (rc) return rc;
-  render_state& R = ctx->render;
   int const B = p->num_bounces;
   int const F = int(p->frames);
   int const passes = 2 * B + 3;
+  size_t const n = size_t(W) * H;
+  uint32_t const nb = uint32_t((n + kBlock - 1) / kBlock);
+  // frames in flight: enough to fill about 4 Mi ray slots per launch
+  uint32_t K = ctx->tuning.ref_frames ? ctx->tuning.ref_frames : uint32_t(std::max<size_t>(1, (size_t(1) << 22) / n));
+  K = std::min<uint32_t>({K, uint32_t(kMaxFramesInFlight), uint32_t(std::max(F, 1))});
+  int rc = ensure_render_buffers(ctx, W, H, K);
+  if (rc) return rc;
+  render_state& R = ctx->render;
   std::vector<int> seeds;
   std::vector<float> tex;
   draw_host_randomness(ctx->host_rng, F, B, seeds, tex);
@@ -607,33 +721,42 @@ int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_p
   camera_dev const& cd = fs.cd;
   scene_dev const& sd = fs.sd;
   color_args ca = fs.ca;
-  size_t const n = size_t(W) * H;
-  uint32_t const nb = uint32_t((n + kBlock - 1) / kBlock);
   cudaStream_t const st = ctx->stream;
-  for (int f = 0; f < F; ++f) {
-    auto tex_of = [&](int pass) { return R.pass_tex + (size_t(f) * passes + pass) * kTexSize; };
-    auto seed_of = [&](int pass) { return seeds[size_t(f) * passes + pass]; };
+  uint32_t* const cnt[2] = {R.counts, R.counts + kMaxFramesInFlight};
+  for (int f0 = 0; f0 < F; f0 += int(K)) {
+    uint32_t const k = std::min<uint32_t>(K, uint32_t(F - f0));
+    auto rand_of = [&](int pass) {
+      pass_rand pr{};
+      pr.tex = R.pass_tex + (size_t(f0) * passes + pass) * kTexSize;
+      pr.tex_stride = uint32_t(passes * kTexSize);
+      for (uint32_t j = 0; j < k; ++j) pr.seed[j] = seeds[(size_t(f0) + j) * passes + pass];
+      return pr;
+    };
+    float4* const fcol = k > 1 ? R.fcol : nullptr;
+    uint32_t const grid = k * nb;
     int cur = 0;
     ca.sample_index = R.sample_counter;
-    k_generate<<<nb, kBlock, 0, st>>>(W, H, tex_of(0), seed_of(0), cd, R.gen[cur], R.counts + cur);
+    k_generate<<<grid, kBlock, 0, st>>>(W, H, nb, rand_of(0), cd, R.gen[cur], cnt[cur]);
     int pass = 1;
     for (int i = 0; i <= B; ++i) {
       bool const last = i == B;
-      k_trace_pass<<<nb, kBlock, 0, st>>>(sd, tex_of(pass), seed_of(pass), R.gen[cur], R.trace, R.counts + cur);
+      k_trace_pass<<<grid, kBlock, 0, st>>>(sd, rand_of(pass), R.gen[cur], R.trace, cnt[cur], uint32_t(n), nb);
       ++pass;
       ca.force = last ? 1 : 0;
-      k_color_pass<<<nb, kBlock, 0, st>>>(ca, tex_of(pass), seed_of(pass), R.gen[cur], R.trace, R.counts + cur,
-          R.block_sums);
+      k_color_pass<<<grid, kBlock, 0, st>>>(ca, rand_of(pass), R.gen[cur], R.trace, cnt[cur], R.block_sums, fcol,
+          uint32_t(n), nb);
       ++pass;
       if (!last) {
-        k_scan_blocks<<<1, 1024, 0, st>>>(R.block_sums, nb, R.counts + (1 - cur));
-        k_scatter<<<nb, kBlock, 0, st>>>(R.gen[cur], R.trace, R.counts + cur, R.block_sums, R.gen[1 - cur]);
+        k_scan_blocks<<<k, 1024, 0, st>>>(R.block_sums, nb, cnt[1 - cur]);
+        k_scatter<<<grid, kBlock, 0, st>>>(R.gen[cur], R.trace, cnt[cur], R.block_sums, R.gen[1 - cur],
+            uint32_t(n), nb);
         cur = 1 - cur;
       }
     }
+    if (fcol) k_resolve_frames<<<nb, kBlock, 0, st>>>(ca, fcol, k, W, H);
     rc = check_cuda(ctx, cudaGetLastError(), "wavefront launch");
     if (rc) return rc;
-    ++R.sample_counter;
+    R.sample_counter += k;
   }
   return MYRT_OK;
 }
@@ -754,23 +877,29 @@ int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_
   color_args ca = fs.ca;
   size_t const n = size_t(W) * H;
   uint32_t const nb = uint32_t((n + kBlock - 1) / kBlock);
-  for (int f = 0; f < F; ++f) {
-    auto tex_of = [&](int pass) { return ptex + (size_t(f) * passes + pass) * kTexSize; };
-    auto seed_of = [&](int pass) { return seeds[f * passes + pass]; };
+  for (int f = 0; f < F; ++f) {  // one frame at a time: one region of ray slots
+    auto rand_of = [&](int pass) {
+      pass_rand pr{};
+      pr.tex = ptex + (size_t(f) * passes + pass) * kTexSize;
+      pr.tex_stride = 0;
+      pr.seed[0] = seeds[f * passes + pass];
+      return pr;
+    };
     int cur = 0;
     ca.sample_index = sample_index + uint32_t(f);
-    k_generate<<<nb, kBlock, 0, st>>>(W, H, tex_of(0), seed_of(0), cd, gen[cur], counts + cur);
+    k_generate<<<nb, kBlock, 0, st>>>(W, H, nb, rand_of(0), cd, gen[cur], counts + cur);
     int pass = 1;
     for (int i = 0; i <= B; ++i) {
       bool const last = i == B;
-      k_trace_pass<<<nb, kBlock, 0, st>>>(sd, tex_of(pass), seed_of(pass), gen[cur], trace, counts + cur);
+      k_trace_pass<<<nb, kBlock, 0, st>>>(sd, rand_of(pass), gen[cur], trace, counts + cur, uint32_t(n), nb);
       ++pass;
       ca.force = last ? 1 : 0;
-      k_color_pass<<<nb, kBlock, 0, st>>>(ca, tex_of(pass), seed_of(pass), gen[cur], trace, counts + cur, sums);
+      k_color_pass<<<nb, kBlock, 0, st>>>(ca, rand_of(pass), gen[cur], trace, counts + cur, sums, nullptr,
+          uint32_t(n), nb);
       ++pass;
       if (!last) {
         k_scan_blocks<<<1, 1024, 0, st>>>(sums, nb, counts + (1 - cur));
-        k_scatter<<<nb, kBlock, 0, st>>>(gen[cur], trace, counts + cur, sums, gen[1 - cur]);
+        k_scatter<<<nb, kBlock, 0, st>>>(gen[cur], trace, counts + cur, sums, gen[1 - cur], uint32_t(n), nb);
         cur = 1 - cur;
       }
     }

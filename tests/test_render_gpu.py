@@ -209,3 +209,27 @@ def test_reference_render_textures_cubemap_dof(ctx):
         ctx.upload_texture(0, None)
         ctx.upload_texture(1, None)
         ctx.upload_cubemap(None)
+
+
+@pytest.mark.parametrize("frames_in_flight", [1, 2, 3])
+def test_frames_in_flight_do_not_change_the_images(ctx, frames_in_flight):
+    """Frames of one call rendered together (tuning ref_frames), in batches that
+    leave a remainder, give the images of frames rendered one at a time -- and
+    of the oracle's sequential frames."""
+    s = icosphere_field(n_spheres=16, subdiv=2, floor_cells=4, seed=6)
+    ctx.upload_scene(**s)
+    W, H = 80, 48
+    iv, ip = look_at((0, 1, -4.5), (0, -0.3, 0), vfov_deg=50, aspect=W / H)
+    try:
+        ctx.set_tuning(ref_frames=frames_in_flight)
+        ctx.reset_accumulation()
+        ctx.set_seed(321)
+        ctx.render(iv, ip, W, H, num_bounces=5, frames=5)
+        ctx.render(iv, ip, W, H, num_bounces=5, frames=2)
+        acc, disp = ctx.read_accumulation(W, H)
+    finally:
+        ctx.set_tuning()
+    assert ctx.sample_count() == 7
+    ref, ref_disp = po.render_reference(s, W, H, bounces=5, frames=7, inv_view=iv, inv_proj=ip, seed=321)
+    _compare(acc, ref)
+    assert np.array_equal(disp, ref_disp)
