@@ -157,8 +157,10 @@ typedef struct myrt_tuning {
                                 GPU): milliseconds for millions of triangles, slower traversal */
   uint32_t trace_order;      /* visiting order of closest / any-hit batches: 0 = device-memory queries
                                 of at least 1 Mi rays sorted by origin and direction cell, host-memory
-                                queries in input order; 1 = input order; 2 = always sorted.
-                                Results never depend on it. */
+                                queries in input order; 1 = input order; 2 = always sorted. The
+                                trace passes of reference shading likewise: 0 = the first two passes
+                                sorted once the frames in flight hold 1 Mi rays, 1 = never, 2 = every
+                                pass. Results never depend on it. */
   uint32_t sdf_cells;        /* myrt_sdf_upload: cells along the longest axis of the grid of
                                 instruction segments built for each program that is a tree of
                                 unions / smooth unions over translated spheres, boxes, tori and

@@ -162,15 +162,8 @@ int order_rays(myrt_ctx* ctx, trace_args& a, int lane, cudaStream_t s) {
     o.cap = cap;
     o.temp_bytes = need;
   }
-  float const* b = ctx->scene.bounds;
   float3 lo, sc;
-  float* plo = &lo.x;
-  float* psc = &sc.x;
-  for (int k = 0; k < 3; ++k) {
-    float const ext = b[3 + k] - b[k];
-    plo[k] = b[k] - 1e-3f * ext;
-    psc[k] = ext > 0.f ? 16.f / (ext * 1.002f) : 0.f;
-  }
+  ray_key_grid(ctx->scene.bounds, lo, sc);
   k_ray_keys<<<(a.n + 255) / 256, 256, 0, s>>>(a.rays, a.n, lo, sc, o.keys[0], o.vals[0]);
   rc = check_cuda(ctx, cudaGetLastError(), "ray key launch");
   if (rc) return rc;

@@ -104,6 +104,10 @@ struct render_state {
   float* pass_tex = nullptr;            // frames * passes * 1024 random texture floats
   float4* fcol = nullptr;               // frames in flight: final colour per frame and pixel
   uint32_t frames_cap = 0;              // frames in flight the ray buffers hold
+  uint32_t* okeys[2] = {nullptr, nullptr};  // visiting order of a trace pass: keys, slots
+  uint32_t* ovals[2] = {nullptr, nullptr};
+  void* otemp = nullptr;                // radix sort temporary
+  size_t otemp_bytes = 0;
   size_t pass_tex_capacity = 0;         // in floats
   uint32_t sample_counter = 0;          // frames accumulated since the last reset
   int64_t pending_first = -1;           // myrt_begin_samples: first sample index of the next render

@@ -24,23 +24,38 @@ __device__ __forceinline__ uint32_t cell4(float x) {  // x in [0, 16) -> 0..15, 
   return x >= 15.f ? 15u : (x > 0.f ? uint32_t(x) : 0u);
 }
 
+// The key of a ray with origin o and direction d (any length); lo and
+// cell_scale map the scene box onto [0, 16)^3.
+__device__ __forceinline__ uint32_t ray_key(float4 o, float4 d, float3 lo, float3 cell_scale) {
+  uint32_t const ox = cell4((o.x - lo.x) * cell_scale.x);
+  uint32_t const oy = cell4((o.y - lo.y) * cell_scale.y);
+  uint32_t const oz = cell4((o.z - lo.z) * cell_scale.z);
+  float const l2 = d.x * d.x + d.y * d.y + d.z * d.z;
+  float const s = l2 > 0.f ? 8.f * rsqrtf(l2) : 0.f;  // unit direction in [-1, 1] -> [0, 16)
+  uint32_t const dx = cell4(fmaf(d.x, s, 8.f)), dy = cell4(fmaf(d.y, s, 8.f)), dz = cell4(fmaf(d.z, s, 8.f));
+  uint32_t const om = spread4(ox) | (spread4(oy) << 1) | (spread4(oz) << 2);
+  uint32_t const dm = spread4(dx) | (spread4(dy) << 1) | (spread4(dz) << 2);
+  return (om << 12) | dm;
+}
+
 // keys[i], vals[i] = i for rays given as (o, tmin), (d, tmax) float4 pairs.
-__global__ void __launch_bounds__(256) k_ray_keys(float4 const* __restrict__ rays, uint32_t n, float3 lo,
+static __global__ void __launch_bounds__(256) k_ray_keys(float4 const* __restrict__ rays, uint32_t n, float3 lo,
     float3 cell_scale, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
   uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float4 const r0 = __ldg(rays + 2 * size_t(i));
-  float4 const r1 = __ldg(rays + 2 * size_t(i) + 1);
-  uint32_t const ox = cell4((r0.x - lo.x) * cell_scale.x);
-  uint32_t const oy = cell4((r0.y - lo.y) * cell_scale.y);
-  uint32_t const oz = cell4((r0.z - lo.z) * cell_scale.z);
-  float const l2 = r1.x * r1.x + r1.y * r1.y + r1.z * r1.z;
-  float const s = l2 > 0.f ? 8.f * rsqrtf(l2) : 0.f;  // unit direction in [-1, 1] -> [0, 16)
-  uint32_t const dx = cell4(fmaf(r1.x, s, 8.f)), dy = cell4(fmaf(r1.y, s, 8.f)), dz = cell4(fmaf(r1.z, s, 8.f));
-  uint32_t const om = spread4(ox) | (spread4(oy) << 1) | (spread4(oz) << 2);
-  uint32_t const dm = spread4(dx) | (spread4(dy) << 1) | (spread4(dz) << 2);
-  keys[i] = (om << 12) | dm;
+  keys[i] = ray_key(__ldg(rays + 2 * size_t(i)), __ldg(rays + 2 * size_t(i) + 1), lo, cell_scale);
   vals[i] = i;
+}
+
+// The scene box [b[0..2], b[3..5]] -> lo and cell_scale of ray_key.
+inline void ray_key_grid(float const* b, float3& lo, float3& cell_scale) {
+  float* plo = &lo.x;
+  float* psc = &cell_scale.x;
+  for (int k = 0; k < 3; ++k) {
+    float const ext = b[3 + k] - b[k];
+    plo[k] = b[k] - 1e-3f * ext;
+    psc[k] = ext > 0.f ? 16.f / (ext * 1.002f) : 0.f;
+  }
 }
 
 }  // namespace myrt_b200

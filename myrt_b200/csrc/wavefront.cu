@@ -38,8 +38,11 @@
 #include <random>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "../../include/myrt_cuda.h"
 #include "ctx.hpp"
+#include "rayorder.cuh"
 #include "refshade.cuh"
 #include "sdf.cuh"
 #include "trace.cuh"
@@ -190,10 +193,33 @@ __global__ void __launch_bounds__(kBlock) k_generate(uint32_t W, uint32_t H, uin
 // follow them as in the reference; the trace record is written before the
 // shadow walk, which then only adds the light term. Same operations, same
 // results as the reference's order.
-// gen / trace: the frames' regions of `slots` rays; count[f]: frame f's rays.
-__global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, pass_rand pr, float4 const* __restrict__ gen,
-    float4* __restrict__ trace, uint32_t const* __restrict__ count, uint32_t slots, uint32_t nb) {
+// Visiting order of a trace pass over the frames in flight: for every thread
+// of the pass's grid, the origin / direction cell key of its ray slot
+// (ray_key), or 0xFFFFFF, after every live key, for an empty slot.
+__global__ void __launch_bounds__(kBlock) k_gen_keys(float4 const* __restrict__ gen, uint32_t const* __restrict__ count,
+    uint32_t slots, uint32_t nb, float3 lo, float3 cell_scale, uint32_t* __restrict__ keys,
+    uint32_t* __restrict__ vals) {
   frame_slot const fs = frame_of(nb);
+  uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t key = 0xFFFFFFu;
+  if (fs.id < count[fs.f]) {
+    float4 const* g = gen + 5 * (size_t(fs.f) * slots + fs.id);
+    key = min(ray_key(g[0], g[1], lo, cell_scale), 0xFFFFFEu);
+  }
+  keys[t] = key;
+  vals[t] = t;
+}
+
+// gen / trace: the frames' regions of `slots` rays; count[f]: frame f's rays.
+// perm (may be null): thread t takes the ray slot of thread perm[t] of the grid.
+__global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, pass_rand pr, float4 const* __restrict__ gen,
+    float4* __restrict__ trace, uint32_t const* __restrict__ count, uint32_t slots, uint32_t nb,
+    uint32_t const* __restrict__ perm) {
+  uint32_t thread = blockIdx.x * blockDim.x + threadIdx.x;
+  if (perm) thread = __ldg(perm + thread);
+  frame_slot fs;
+  fs.f = thread / (nb * kBlock);
+  fs.id = thread - fs.f * nb * kBlock;
   uint32_t const id = fs.id;
   if (id >= count[fs.f]) return;
   float const* const tex = pr.tex + fs.f * pr.tex_stride;
@@ -554,11 +580,16 @@ __global__ void __launch_bounds__(kBlock) k_resolve_frames(color_args a, float4 
 // ---- host side ----------------------------------------------------------------------
 void free_ray_buffers(render_state& R) {
   for (void* p : {static_cast<void*>(R.gen[0]), static_cast<void*>(R.gen[1]), static_cast<void*>(R.trace),
-           static_cast<void*>(R.counts), static_cast<void*>(R.block_sums), static_cast<void*>(R.fcol)})
+           static_cast<void*>(R.counts), static_cast<void*>(R.block_sums), static_cast<void*>(R.fcol),
+           static_cast<void*>(R.okeys[0]), static_cast<void*>(R.okeys[1]), static_cast<void*>(R.ovals[0]),
+           static_cast<void*>(R.ovals[1]), R.otemp})
     cudaFree(p);
   R.gen[0] = R.gen[1] = nullptr;
   R.trace = R.fcol = nullptr;
   R.counts = R.block_sums = nullptr;
+  R.okeys[0] = R.okeys[1] = R.ovals[0] = R.ovals[1] = nullptr;
+  R.otemp = nullptr;
+  R.otemp_bytes = 0;
   R.frames_cap = 0;
 }
 
@@ -581,6 +612,16 @@ int ensure_render_buffers(myrt_ctx* ctx, uint32_t W, uint32_t H, uint32_t frames
   alloc(reinterpret_cast<void**>(&R.counts), 2 * kMaxFramesInFlight * sizeof(uint32_t), "ray counts");
   alloc(reinterpret_cast<void**>(&R.block_sums), std::max<size_t>(nb, 1) * sizeof(uint32_t), "block sums");
   if (frames > 1) alloc(reinterpret_cast<void**>(&R.fcol), n * 16, "frame colours");
+  // visiting order of the trace passes: one key and slot per thread of a pass's grid
+  size_t const threads = nb * kBlock;
+  for (int k = 0; k < 2; ++k) {
+    alloc(reinterpret_cast<void**>(&R.okeys[k]), threads * 4, "pass order keys");
+    alloc(reinterpret_cast<void**>(&R.ovals[k]), threads * 4, "pass order slots");
+  }
+  if (!rc)
+    rc = check_cuda(ctx, cub::DeviceRadixSort::SortPairs(nullptr, R.otemp_bytes, R.okeys[0], R.okeys[1], R.ovals[0],
+                             R.ovals[1], int(threads), 0, kOrderKeyBits, ctx->stream), "pass order size");
+  alloc(&R.otemp, std::max<size_t>(R.otemp_bytes, 16), "pass order temporary");
   if (rc) {
     free_ray_buffers(R);
     return rc;
@@ -723,6 +764,12 @@ int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_p
   color_args ca = fs.ca;
   cudaStream_t const st = ctx->stream;
   uint32_t* const cnt[2] = {R.counts, R.counts + kMaxFramesInFlight};
+  // Visiting order of the trace passes (trace_order): sorted by origin / direction cell for the first
+  // two passes, which hold most of the rays, once the frames in flight fill 1 Mi slots (0); never
+  // (1); every pass (2). Results never depend on it.
+  uint32_t const order = ctx->tuning.trace_order;
+  float3 klo, ksc;
+  ray_key_grid(ctx->scene.bounds, klo, ksc);
   for (int f0 = 0; f0 < F; f0 += int(K)) {
     uint32_t const k = std::min<uint32_t>(K, uint32_t(F - f0));
     auto rand_of = [&](int pass) {
@@ -740,7 +787,17 @@ int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_p
     int pass = 1;
     for (int i = 0; i <= B; ++i) {
       bool const last = i == B;
-      k_trace_pass<<<grid, kBlock, 0, st>>>(sd, rand_of(pass), R.gen[cur], R.trace, cnt[cur], uint32_t(n), nb);
+      bool const sorted = order == 2 || (order == 0 && i < 2 && size_t(k) * n >= (size_t(1) << 20));
+      uint32_t const* perm = nullptr;
+      if (sorted) {
+        k_gen_keys<<<grid, kBlock, 0, st>>>(R.gen[cur], cnt[cur], uint32_t(n), nb, klo, ksc, R.okeys[0], R.ovals[0]);
+        size_t tb = R.otemp_bytes;
+        rc = check_cuda(ctx, cub::DeviceRadixSort::SortPairs(R.otemp, tb, R.okeys[0], R.okeys[1], R.ovals[0],
+                                 R.ovals[1], int(size_t(grid) * kBlock), 0, kOrderKeyBits, st), "pass order sort");
+        if (rc) return rc;
+        perm = R.ovals[1];
+      }
+      k_trace_pass<<<grid, kBlock, 0, st>>>(sd, rand_of(pass), R.gen[cur], R.trace, cnt[cur], uint32_t(n), nb, perm);
       ++pass;
       ca.force = last ? 1 : 0;
       k_color_pass<<<grid, kBlock, 0, st>>>(ca, rand_of(pass), R.gen[cur], R.trace, cnt[cur], R.block_sums, fcol,
@@ -891,7 +948,8 @@ int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_
     int pass = 1;
     for (int i = 0; i <= B; ++i) {
       bool const last = i == B;
-      k_trace_pass<<<nb, kBlock, 0, st>>>(sd, rand_of(pass), gen[cur], trace, counts + cur, uint32_t(n), nb);
+      k_trace_pass<<<nb, kBlock, 0, st>>>(sd, rand_of(pass), gen[cur], trace, counts + cur, uint32_t(n), nb,
+          nullptr);
       ++pass;
       ca.force = last ? 1 : 0;
       k_color_pass<<<nb, kBlock, 0, st>>>(ca, rand_of(pass), gen[cur], trace, counts + cur, sums, nullptr,

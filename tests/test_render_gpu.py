@@ -233,3 +233,26 @@ def test_frames_in_flight_do_not_change_the_images(ctx, frames_in_flight):
     ref, ref_disp = po.render_reference(s, W, H, bounces=5, frames=7, inv_view=iv, inv_proj=ip, seed=321)
     _compare(acc, ref)
     assert np.array_equal(disp, ref_disp)
+
+
+def test_sorted_trace_passes_do_not_change_the_images(ctx):
+    """16 frames in flight of 256 x 256 fill 1 Mi ray slots, so the first two
+    trace passes run in the sorted visiting order (trace_order 0); every pass
+    sorted (2) and none (1) give the same bits."""
+    s = icosphere_field(n_spheres=64, subdiv=2, floor_cells=8, seed=8)
+    ctx.upload_scene(**s)
+    W = H = 256
+    iv, ip = look_at((0, 1, -4.5), (0, -0.3, 0), vfov_deg=50, aspect=1.0)
+    out = []
+    try:
+        for order in (1, 0, 2):
+            ctx.set_tuning(trace_order=order)
+            ctx.reset_accumulation()
+            ctx.set_seed(99)
+            ctx.render(iv, ip, W, H, num_bounces=3, frames=16)
+            out.append(ctx.read_accumulation(W, H))
+    finally:
+        ctx.set_tuning()
+    for acc, disp in out[1:]:
+        assert np.array_equal(acc, out[0][0]) and np.array_equal(disp, out[0][1])
+    assert out[0][0][..., 3].min() == 16
