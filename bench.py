@@ -851,7 +851,7 @@ def run_pt_workload(args, emit: bool = True):
         "samples/s plain path tracing", samples / (ms / 1e3), "samples/s", args.steps, args.warmup, ms / args.steps,
         {"workload": "plain path tracing, icosphere scene (655,872 tris) + 0.2x0.2 light of emission 20; "
                      "512x512, 64 spp per step, depth 8, RR after 3, NEE + MIS", "triangles": int(info["triangles"]),
-         "res": W, "spp_per_step": spp, "l2": "per-wave path state (4 Mi paths, ~1 GB) exceeds L2"},
+         "res": W, "spp_per_step": spp, "l2": "per-wave path state (16 Mi paths, ~3.5 GB) exceeds L2"},
         {"mrays_per_s": rays / (ms / 1e3) / 1e6, "rays_per_sample": rays / samples,
          f"rel_rmse_one_step_vs_fp64_{oracle_spp}spp": err_one,
          "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128,

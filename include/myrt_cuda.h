@@ -147,7 +147,8 @@ typedef struct myrt_tuning {
                                 0 = 10), 12 */
   uint32_t trace_unit_steps; /* one-thread-per-ray: 0 = a node and all its triangles per iteration,
                                 1 = one node, triangle or pop per iteration */
-  uint32_t wave_paths;       /* physical / guided wavefront: paths in flight per wave (0 = 4 Mi) */
+  uint32_t wave_paths;       /* physical / guided wavefront: paths in flight per wave (0 = 16 Mi for
+                                physical, 4 Mi for guided renders and batches) */
   uint32_t pt_blocks_per_sm; /* physical / guided: resident 128-thread blocks per SM of the
                                 grid-stride extend / shade / shadow kernels (0 = 8) */
   uint32_t trace_smem_stack; /* one-thread-per-ray: 1 = traversal stack in shared memory
@@ -187,8 +188,9 @@ typedef struct myrt_tuning {
   uint32_t pt_grid;          /* physical / guided extend, shade and shadow kernels: 0 = default (2),
                                 1 = grid-stride loops over pt_blocks_per_sm resident blocks per SM,
                                 2 = one thread per queue entry (the grid covers the wave's paths;
-                                blocks past the queue's count return at once; pt_blocks_per_sm >= 10
-                                then selects a 48-register cap for the mesh traversal kernels).
+                                blocks past the queue's count return at once; the mesh traversal
+                                kernels then run under a 48-register cap unless pt_blocks_per_sm is
+                                1..9, which gives them 64 registers).
                                 Results never depend on it. */
   uint32_t ref_frames;       /* reference shading (myrt_render): frames of one call whose passes run
                                 together, each in its own region of ray slots (0 = as many as fill
