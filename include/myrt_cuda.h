@@ -147,8 +147,8 @@ typedef struct myrt_tuning {
                                 0 = 10), 12 */
   uint32_t trace_unit_steps; /* one-thread-per-ray: 0 = a node and all its triangles per iteration,
                                 1 = one node, triangle or pop per iteration */
-  uint32_t wave_paths;       /* physical / guided wavefront: paths in flight per wave (0 = 16 Mi for
-                                physical, 4 Mi for guided renders and batches) */
+  uint32_t wave_paths;       /* physical / guided wavefront: paths in flight per wave (0 = 16 Mi; 4 Mi
+                                while a guide trains and for batches, whose autotuner picks its own) */
   uint32_t pt_blocks_per_sm; /* physical / guided: resident 128-thread blocks per SM of the
                                 grid-stride extend / shade / shadow kernels (0 = 8) */
   uint32_t trace_smem_stack; /* one-thread-per-ray: 1 = traversal stack in shared memory

@@ -780,23 +780,23 @@ int render_physical_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_pa
     if (rc) return rc;
   }
   bool const guided = p->shading == MYRT_SHADE_GUIDED;
-  // default wave: 16 Mi paths for plain shading (fewer, fuller launches at the late, sparse vertices:
-  // 439 -> 513 M samples/s on a 512x512 64-spp frame against 4 Mi), 4 Mi for guided renders, whose
-  // guide trains after every wave
-  size_t const target = p->wave_paths ? p->wave_paths
-                                      : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : (guided ? 4u << 20 : 16u << 20));
-  pt_job J = make_job(0, W, H, p->seed, p->max_depth, p->rr_start, p->accum_fp64, *cam, p->env_radiance,
-      p->sdf_marching_steps, p->sdf_marching_epsilon);
-  J.accum = R.accum;
-  J.accum64 = R.accum64;
-  J.display = R.display;
-  std::vector<wave_plan> plan;
   uint64_t trained = 0;
   bool training = false;
   if (guided) {
     rc = guide_schedule(ctx, &trained, &training);
     if (rc) return rc;
   }
+  // default wave: 16 Mi paths (fewer, fuller launches at the late, sparse vertices: 439 -> 513 M
+  // samples/s on a 512x512 64-spp frame against 4 Mi), 4 Mi while a guide is training, since it
+  // trains after every wave
+  size_t const target = p->wave_paths ? p->wave_paths
+      : (ctx->tuning.wave_paths ? ctx->tuning.wave_paths : (guided && training ? 4u << 20 : 16u << 20));
+  pt_job J = make_job(0, W, H, p->seed, p->max_depth, p->rr_start, p->accum_fp64, *cam, p->env_radiance,
+      p->sdf_marching_steps, p->sdf_marching_epsilon);
+  J.accum = R.accum;
+  J.accum64 = R.accum64;
+  J.display = R.display;
+  std::vector<wave_plan> plan;
   if (guided && training) plan = plan_waves_growing(J, spp, target, trained);
   else plan = plan_waves({J}, {spp}, target);
   size_t max_paths = 0;
