@@ -362,8 +362,8 @@ def guiding_run(device_index: int, res: int, oracle_spp: int, budget_spp: int, s
         "oracle": {"spp": oracle_spp, "seconds": round(t_ref, 2),
                    "method": "plain BSDF sampling + NEE with MIS, roulette from vertex 3, FP64 accumulation"},
         "plain": plain, "guided": guided,
-        "wave_paths": "default (4 Mi paths) for both; while the guide trains, guided waves grow 1, 2, 4, ... spp "
-                      "up to that size and the guide takes 16 Adam steps after each wave",
+        "wave_paths": "the library's defaults: plain 16 Mi paths per wave; guided, while its guide trains, waves "
+                      "growing 1, 2, 4, ... spp up to 4 Mi paths, the guide taking 16 Adam steps after each wave",
         "guided_seconds_to_plain_rel_rmse": t_eq,
         "speedup_rel_rmse": (t_plain / t_eq) if t_eq else None,
         "speedup_mse_lum": (t_plain / t_eq_mse) if t_eq_mse else None,
