@@ -107,6 +107,7 @@ struct render_state {
   uint32_t* okeys[2] = {nullptr, nullptr};  // visiting order of a trace pass: keys, slots
   uint32_t* ovals[2] = {nullptr, nullptr};
   void* otemp = nullptr;                // radix sort temporary
+  float4* shadow_q = nullptr;           // NEE shadow rays of a trace pass, 2 float4 each
   size_t otemp_bytes = 0;
   size_t pass_tex_capacity = 0;         // in floats
   uint32_t sample_counter = 0;          // frames accumulated since the last reset

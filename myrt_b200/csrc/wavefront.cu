@@ -5,8 +5,12 @@
 //   k_generate     pt_generate.comp:50-84
 //   k_trace_pass   pt_trace.comp:134-226, nearest_hit :331-386 (meshes), any_hit
 //                  :311-329 for the NEE shadow ray; both walk the 8-wide BVH
+//   k_shadow_pass  that any_hit for mesh-only scenes, over the queue of shadow
+//                  rays k_trace_pass leaves, so that every lane walks one
 //   k_color_pass   pt_color.comp:77-202 (sky gradient, no cubemap), plus a
 //                  per-block count of surviving rays for the compaction
+//   k_gen_keys     visiting order of the first two trace passes (ray_key)
+//   k_resolve_frames  the frames in flight into the accumulation, in order
 //   k_scan_blocks + k_scatter
 //                  pt_ray_filter.comp:49-64 as a STABLE compaction: survivors
 //                  keep their relative order, so slot ids (which feed the
@@ -212,9 +216,12 @@ __global__ void __launch_bounds__(kBlock) k_gen_keys(float4 const* __restrict__ 
 
 // gen / trace: the frames' regions of `slots` rays; count[f]: frame f's rays.
 // perm (may be null): thread t takes the ray slot of thread perm[t] of the grid.
+// shadow_q (may be null): without SDF drawables, the NEE shadow rays are
+// appended there (2 float4 each, *shadow_count of them) for k_shadow_pass
+// instead of being walked here.
 __global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, pass_rand pr, float4 const* __restrict__ gen,
     float4* __restrict__ trace, uint32_t const* __restrict__ count, uint32_t slots, uint32_t nb,
-    uint32_t const* __restrict__ perm) {
+    uint32_t const* __restrict__ perm, float4* __restrict__ shadow_q, uint32_t* __restrict__ shadow_count) {
   uint32_t thread = blockIdx.x * blockDim.x + threadIdx.x;
   if (perm) thread = __ldg(perm + thread);
   frame_slot fs;
@@ -333,6 +340,20 @@ __global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, pass_rand pr
   t[2] = make_float4(uv.x, uv.y, __int_as_float(material), __uint_as_float(light_color));
   t[3] = make_float4(light_dir.x, light_dir.y, light_dir.z, light_strength);
   if (!shadow) return;
+  if (shadow_q && s.sdf.n_drawables == 0) {
+    // one atomic per group of converged lanes; entry: (so, dist_l), (dir_l, slot | light << 31)
+    uint32_t const lanes = __activemask();
+    uint32_t const lane = threadIdx.x & 31u;
+    uint32_t const leader = uint32_t(__ffs(lanes)) - 1u;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(shadow_count, uint32_t(__popc(lanes)));
+    base = __shfl_sync(lanes, base, int(leader));
+    uint32_t const e = base + uint32_t(__popc(lanes & ((1u << lane) - 1u)));
+    uint32_t const slot = fs.f * slots + id;
+    shadow_q[2 * size_t(e)] = make_float4(so.x, so.y, so.z, dist_l);
+    shadow_q[2 * size_t(e) + 1] = make_float4(dir_l.x, dir_l.y, dir_l.z, __uint_as_float(slot | (uint32_t(li) << 31)));
+    return;
+  }
   hit_rec hs;
   bool occluded = traverse<0, true, false>(s.nodes, s.tris, f3{so.x, so.y, so.z}, f3{dir_l.x, dir_l.y, dir_l.z},
       0.f, dist_l, hs, s.err, cn, ct);
@@ -347,6 +368,33 @@ __global__ void __launch_bounds__(kBlock) k_trace_pass(scene_dev s, pass_rand pr
   light_strength = light_strength * (2.f / dist_l);
   reinterpret_cast<float*>(t + 2)[3] = __uint_as_float(light_color);
   t[3] = make_float4(dir_l.x, dir_l.y, dir_l.z, light_strength);
+}
+
+// The NEE shadow rays k_trace_pass queued (meshes only): any_hit
+// (pt_trace.comp:311-318) and, when unoccluded, the light term of the ray's
+// trace record, as k_trace_pass computes it in place.
+constexpr int kShadowBlock = 128;
+__global__ void __launch_bounds__(kShadowBlock, 8) k_shadow_pass(scene_dev s, float4 const* __restrict__ q,
+    uint32_t const* __restrict__ count, float4* __restrict__ trace) {
+  uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *count) return;
+  float4 const a = q[2 * size_t(i)], b = q[2 * size_t(i) + 1];
+  uint32_t const w = __float_as_uint(b.w);
+  uint32_t const slot = w & 0x7fffffffu;
+  int const li = int(w >> 31);
+  float const dist_l = a.w;
+  hit_rec hs;
+  uint32_t cn = 0, ct = 0;
+  if (traverse<0, true, false>(s.nodes, s.tris, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.f, dist_l, hs, s.err, cn, ct))
+    return;
+  v3 const col{c_lights[li].cx, c_lights[li].cy, c_lights[li].cz};
+  float light_strength = rs::length(col);
+  uint32_t const light_color = rs::pack_unorm4x8(col.x / light_strength, col.y / light_strength,
+      col.z / light_strength, 0.f / light_strength);
+  light_strength = light_strength * (2.f / dist_l);
+  float4* t = trace + 4 * size_t(slot);
+  reinterpret_cast<float*>(t + 2)[3] = __uint_as_float(light_color);
+  t[3] = make_float4(b.x, b.y, b.z, light_strength);
 }
 
 // ---- pt_color.comp ----------------------------------------------------------------
@@ -582,7 +630,7 @@ void free_ray_buffers(render_state& R) {
   for (void* p : {static_cast<void*>(R.gen[0]), static_cast<void*>(R.gen[1]), static_cast<void*>(R.trace),
            static_cast<void*>(R.counts), static_cast<void*>(R.block_sums), static_cast<void*>(R.fcol),
            static_cast<void*>(R.okeys[0]), static_cast<void*>(R.okeys[1]), static_cast<void*>(R.ovals[0]),
-           static_cast<void*>(R.ovals[1]), R.otemp})
+           static_cast<void*>(R.ovals[1]), R.otemp, static_cast<void*>(R.shadow_q)})
     cudaFree(p);
   R.gen[0] = R.gen[1] = nullptr;
   R.trace = R.fcol = nullptr;
@@ -590,6 +638,7 @@ void free_ray_buffers(render_state& R) {
   R.okeys[0] = R.okeys[1] = R.ovals[0] = R.ovals[1] = nullptr;
   R.otemp = nullptr;
   R.otemp_bytes = 0;
+  R.shadow_q = nullptr;
   R.frames_cap = 0;
 }
 
@@ -609,7 +658,8 @@ int ensure_render_buffers(myrt_ctx* ctx, uint32_t W, uint32_t H, uint32_t frames
   alloc(reinterpret_cast<void**>(&R.gen[0]), n * 80, "ray state");
   alloc(reinterpret_cast<void**>(&R.gen[1]), n * 80, "ray state");
   alloc(reinterpret_cast<void**>(&R.trace), n * 64, "trace state");
-  alloc(reinterpret_cast<void**>(&R.counts), 2 * kMaxFramesInFlight * sizeof(uint32_t), "ray counts");
+  alloc(reinterpret_cast<void**>(&R.counts), (2 * kMaxFramesInFlight + 1) * sizeof(uint32_t), "ray counts");
+  alloc(reinterpret_cast<void**>(&R.shadow_q), n * 32, "shadow rays");
   alloc(reinterpret_cast<void**>(&R.block_sums), std::max<size_t>(nb, 1) * sizeof(uint32_t), "block sums");
   if (frames > 1) alloc(reinterpret_cast<void**>(&R.fcol), n * 16, "frame colours");
   // visiting order of the trace passes: one key and slot per thread of a pass's grid
@@ -768,6 +818,10 @@ int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_p
   // two passes, which hold most of the rays, once the frames in flight fill 1 Mi slots (0); never
   // (1); every pass (2). Results never depend on it.
   uint32_t const order = ctx->tuning.trace_order;
+  // NEE shadow rays of mesh-only scenes walk in their own pass, every lane with a ray (a queue
+  // entry names its slot in 31 bits)
+  bool const split_shadow = sd.sdf.n_drawables == 0 && size_t(K) * n < (size_t(1) << 31);
+  uint32_t* const shadow_count = R.counts + 2 * kMaxFramesInFlight;
   float3 klo, ksc;
   ray_key_grid(ctx->scene.bounds, klo, ksc);
   for (int f0 = 0; f0 < F; f0 += int(K)) {
@@ -797,7 +851,15 @@ int render_reference_frames(myrt_ctx* ctx, myrt_camera const* cam, myrt_render_p
         if (rc) return rc;
         perm = R.ovals[1];
       }
-      k_trace_pass<<<grid, kBlock, 0, st>>>(sd, rand_of(pass), R.gen[cur], R.trace, cnt[cur], uint32_t(n), nb, perm);
+      if (split_shadow) {
+        rc = check_cuda(ctx, cudaMemsetAsync(shadow_count, 0, sizeof(uint32_t), st), "shadow queue reset");
+        if (rc) return rc;
+      }
+      k_trace_pass<<<grid, kBlock, 0, st>>>(sd, rand_of(pass), R.gen[cur], R.trace, cnt[cur], uint32_t(n), nb, perm,
+          split_shadow ? R.shadow_q : nullptr, shadow_count);
+      if (split_shadow)
+        k_shadow_pass<<<uint32_t((size_t(k) * n + kShadowBlock - 1) / kShadowBlock), kShadowBlock, 0, st>>>(sd,
+            R.shadow_q, shadow_count, R.trace);
       ++pass;
       ca.force = last ? 1 : 0;
       k_color_pass<<<grid, kBlock, 0, st>>>(ca, rand_of(pass), R.gen[cur], R.trace, cnt[cur], R.block_sums, fcol,
@@ -949,7 +1011,7 @@ int render_reference_frames_noalloc(myrt_ctx* ctx, myrt_camera const* cam, myrt_
     for (int i = 0; i <= B; ++i) {
       bool const last = i == B;
       k_trace_pass<<<nb, kBlock, 0, st>>>(sd, rand_of(pass), gen[cur], trace, counts + cur, uint32_t(n), nb,
-          nullptr);
+          nullptr, nullptr, nullptr);
       ++pass;
       ca.force = last ? 1 : 0;
       k_color_pass<<<nb, kBlock, 0, st>>>(ca, rand_of(pass), gen[cur], trace, counts + cur, sums, nullptr,
