@@ -930,7 +930,7 @@ def run_render_workload(args, emit: bool = True):
                          "over the reference's binary tree, all host threads; tree built beforehand",
                "seconds": round(cpu_s, 2)}
     passes = 2 * B + 3
-    k_fl = min(64, max(1, (1 << 22) // (W * H)), frames)  # the library's default frames in flight
+    k_fl = min(64, max(1, (1 << 24) // (W * H)), frames)  # the library's default frames in flight
     n_batches = -(-frames // k_fl)
     line = _render_line(
         "samples/s reference shading", samples / (ms / 1e3), "samples/s", args.steps, args.warmup, ms,
@@ -938,16 +938,17 @@ def run_render_workload(args, emit: bool = True):
                      f"({int(info['triangles']):,} tris, PBR materials), {W}x{H}, {B} bounces, "
                      f"{frames} frames of 1 sample per pixel per step",
          "triangles": int(info["triangles"]), "res": W, "frames_per_step": frames, "bounces": B,
-         "l2": "ray states and trace records of the frames in flight (~1 GB) exceed L2"},
+         "l2": "ray states and trace records of the frames in flight (~5 GB) exceed L2"},
         {"parity_bit_exact_vs_oracle": parity,
          "parity_case": f"{pw}x{ph}, 2 frames, {B} bounces, seed 77: accumulation bit-identical to the oracle",
          "e2e": {"value": samples / e2e_s, "unit": "samples/s", "h2d_bytes_per_step": 128 + frames * passes * 4096,
                  "d2h_bytes_per_step": W * H * 16 * 2, "api": "myrt_render + myrt_read_accumulation"},
          "frames_in_flight": k_fl,
-         "gpu_launches": n_batches * (4 * B + 3) + (n_batches if k_fl > 1 else 0),
-         "gpu_launches_note": "per batch of frames in flight: generate, then per bounce trace + color, plus scan + "
-                              "scatter of the surviving rays after every bounce but the last, and the in-order "
-                              "resolve of the batch's frames into the accumulation",
+         "gpu_launches": n_batches * (1 + 3 * (B + 1) + 2 * B + 2) + (n_batches if k_fl > 1 else 0),
+         "gpu_launches_note": "per batch of frames in flight: generate; per bounce trace, shadow and color, plus "
+                              "scan + scatter of the surviving rays after every bounce but the last; the visiting-"
+                              "order keys of the first two trace passes; the in-order resolve of the batch's frames "
+                              "into the accumulation (CUB's radix-sort kernels not counted)",
          "cpu_baseline": cpu,
          "clocks": clocks.summary()})
     if not emit:

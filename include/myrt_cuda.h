@@ -194,7 +194,7 @@ typedef struct myrt_tuning {
                                 Results never depend on it. */
   uint32_t ref_frames;       /* reference shading (myrt_render): frames of one call whose passes run
                                 together, each in its own region of ray slots (0 = as many as fill
-                                about 4 Mi rays, at most 64; 1 = one frame at a time, as the
+                                about 16 Mi rays, at most 64; 1 = one frame at a time, as the
                                 reference; 2..64). Results never depend on it. */
 } myrt_tuning;
 
