@@ -414,6 +414,35 @@ C1_WORKLOAD = ("height field 128x128 cells on [-1,1]^2 in xz (32,768 tris, y ~ U
                "rays through pixel centres from (0,2,-3) at the origin, 60 deg vfov, 1 ray per pixel")
 
 
+def pcie_roofline(d_in, h_in, d_out, h_out, device, e2e_step_s: float, rays: int) -> dict:
+    """The PCIe bound of a host-buffer query step: its ray upload (h_in ->
+    d_in) and hit download (d_out -> h_out) alone, pinned, the two directions
+    on two streams at once, wall clock; frac = that over the step's time."""
+    import torch
+
+    up, down = torch.cuda.Stream(device), torch.cuda.Stream(device)
+
+    def copies():
+        with torch.cuda.stream(up):
+            d_in.copy_(h_in, non_blocking=True)
+        with torch.cuda.stream(down):
+            h_out.copy_(d_out, non_blocking=True)
+
+    copies()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        copies()
+    torch.cuda.synchronize()
+    copy_s = (time.perf_counter() - t0) / 3
+    nbytes = h_in.numel() * h_in.element_size() + h_out.numel() * h_out.element_size()
+    return {"bound": "pcie", "copies_only_ms": copy_s * 1e3, "e2e_ms_per_step": e2e_step_s * 1e3,
+            "frac": copy_s / e2e_step_s, "bound_value": rays / copy_s / 1e6, "copy_gbs": nbytes / copy_s / 1e9,
+            "note": "copies_only_ms: the step's ray upload and hit download alone (pinned, both directions at "
+                    "once, wall clock); bound_value: rays per second at that time; frac = copies alone over "
+                    "the e2e step"}
+
+
 def c1_run(local: int, args) -> dict:
     """Config 1, the closest-hit configuration the metric is quoted on: the
     128 x 128 height field and 1,048,576 pinhole rays. The rays and hits fit in
@@ -481,6 +510,7 @@ def c1_run(local: int, args) -> dict:
     for _ in range(e2e_steps):
         ctx.trace_closest(hr, out=hh)
     e2e_s = time.perf_counter() - t0
+    e2e_pcie = pcie_roofline(rays, h_rays, hits, h_hits, device, e2e_s / e2e_steps, n)
     ctx.set_tuning()
     ctx.close()
     peaks, peak_kind = measured_peaks()
@@ -503,7 +533,7 @@ def c1_run(local: int, args) -> dict:
                                 "CUDA-event duration; the 2 MB tree is L2-resident"},
            "e2e": {"value": n * e2e_steps / e2e_s / 1e6, "unit": UNIT, "h2d_bytes_per_step": n * RAY_BYTES,
                    "d2h_bytes_per_step": n * HIT_BYTES, "steps": e2e_steps,
-                   "api": "myrt_trace_closest (host pinned buffers)"},
+                   "api": "myrt_trace_closest (host pinned buffers)", "roofline": e2e_pcie},
            "clocks": clocks.summary(),
            "gpu_launches": args.steps * (1 if order == 1 else 2)}
     if not args.no_cpu_baseline:
@@ -619,6 +649,7 @@ def run_ours(args):
         e2e_s = float(t.item())
     e2e_value = n * world * e2e_steps / e2e_s / 1e6
     chunks = (n + (1 << 20) - 1) >> 20
+    e2e_pcie = pcie_roofline(rays, h_rays, hits, h_hits, device, e2e_s / e2e_steps, n * world)
 
     peaks, peak_kind = measured_peaks()
     hbm = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
@@ -649,7 +680,8 @@ def run_ours(args):
                              "(ray keys + radix sort of the visiting order)"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * RAY_BYTES,
                 "d2h_bytes_per_step": n * HIT_BYTES, "steps": e2e_steps,
-                "api": "myrt_trace_closest (host pinned buffers, chunked copy/compute overlap)"},
+                "api": "myrt_trace_closest (host pinned buffers, chunked copy/compute overlap)",
+                "roofline": e2e_pcie},
         "clocks": clocks.summary(),
         "gpu_launches": 2 * args.steps,
         "gpu_launches_note": "per step: k_ray_keys + k_trace (ours) and the CUB radix sort of the visiting order",

@@ -316,14 +316,17 @@ trace_args base_args(myrt_ctx* ctx) {
 // upload, traversal and download in order, so the host-to-device copy engine
 // always has the next chunk's upload queued while earlier chunks trace and
 // download (with two streams it idled while a stream's download finished).
+// Chunks are an eighth of the query (at least 64 Ki rays, at most kChunkRays),
+// so that a query of 1 Mi rays pipelines too instead of running as one chunk.
 int host_query(myrt_ctx* ctx, myrt_ray const* rays, uint32_t n, void* out, size_t out_stride, int intersector,
     bool any) {
   size_t const chunk_bytes = size_t(kChunkRays) * (sizeof(myrt_ray) + sizeof(myrt_hit));
   int rc = ensure_stage(ctx, chunk_bytes);
   if (rc) return rc;
+  uint32_t const chunk = std::min<uint32_t>(kChunkRays, std::max<uint32_t>(1u << 16, ((n / 8) + 4095u) & ~4095u));
   cudaStream_t lanes[4] = {ctx->stream, ctx->aux_stream, ctx->copy_lanes[0], ctx->copy_lanes[1]};
-  for (uint32_t c0 = 0, k = 0; c0 < n; c0 += kChunkRays, ++k) {
-    uint32_t const cn = std::min(kChunkRays, n - c0);
+  for (uint32_t c0 = 0, k = 0; c0 < n; c0 += chunk, ++k) {
+    uint32_t const cn = std::min(chunk, n - c0);
     cudaStream_t const s = lanes[k & 3];
     char* base = static_cast<char*>(ctx->stage[k & 3]);
     auto* d_rays = reinterpret_cast<float4*>(base);
