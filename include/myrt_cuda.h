@@ -217,7 +217,9 @@ int myrt_get_tuning(myrt_ctx* ctx, myrt_tuning* tuning);
  * the reference): while enabled, each query records CUDA events around its
  * ordering phase (ray keys + radix sort) and its traversal kernel.
  * myrt_get_phase_times waits for the recorded queries, returns the summed
- * milliseconds and the number of queries since the last call, and clears them. */
+ * milliseconds and the number of traversal launches since the last call, and
+ * clears them: one per device-memory query, one per chunk of a host-memory
+ * query (chunks of an eighth of the query, 64 Ki to 1 Mi rays). */
 int myrt_set_phase_timing(myrt_ctx* ctx, int enable);
 int myrt_get_phase_times(myrt_ctx* ctx, double* order_ms, double* traverse_ms, uint64_t* queries);
 
