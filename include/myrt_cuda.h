@@ -161,7 +161,9 @@ typedef struct myrt_tuning {
                                 queries in input order; 1 = input order; 2 = always sorted. The
                                 trace passes of reference shading likewise: 0 = the first two passes
                                 sorted once the frames in flight hold 1 Mi rays, 1 = never, 2 = every
-                                pass. Results never depend on it. */
+                                pass; and the extension queues of physical / guided waves: 0 = those
+                                of vertices 1 and 2 in waves of at least 1 Mi paths, 1 = never, 2 =
+                                every vertex after the camera's. Results never depend on it. */
   uint32_t sdf_cells;        /* myrt_sdf_upload: cells along the longest axis of the grid of
                                 instruction segments built for each program that is a tree of
                                 unions / smooth unions over translated spheres, boxes, tori and

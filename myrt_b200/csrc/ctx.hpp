@@ -128,6 +128,10 @@ struct physical_state {
   float4* shadow = nullptr;             // 3 float4 per shadow ray: (o, path), (d, tmax), (contribution, -)
   float4* radiance = nullptr;           // per path: rgb
   uint32_t* counts = nullptr;           // [0..1] ray queues, [2] shadow queue
+  uint32_t* okeys[2] = {nullptr, nullptr};  // visiting order of an extension queue: keys, entries
+  uint32_t* ovals[2] = {nullptr, nullptr};
+  void* otemp = nullptr;                // radix sort temporary
+  size_t otemp_bytes = 0;
   unsigned long long* stats = nullptr;  // paths, extension rays, shadow rays (cumulative)
   void* lights = nullptr;               // ps::area_light[n_lights]
   int n_lights = 0;

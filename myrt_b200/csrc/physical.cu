@@ -30,6 +30,8 @@
 // Compiled with -fmad=false (build.py) like the other shading unit.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -42,6 +44,7 @@
 #include "refshade.cuh"
 #include "sdf.cuh"
 #include "trace.cuh"
+#include "rayorder.cuh"
 
 namespace myrt_b200 {
 
@@ -69,6 +72,7 @@ struct pt_scene {
   ps::area_light const* lights;
   int n_lights;
   sdfk::sdf_dev sdf;  // steps / eps come from the job
+  float3 key_lo, key_scale;  // ray_key's grid over the scene box
 };
 
 // One job within one wave.
@@ -167,12 +171,14 @@ __device__ __forceinline__ rs::rng_t sdf_stream(pt_job const& J, uint32_t path, 
 }
 
 // ---- extend: closest hit over meshes, SDF drawables and lights ---------------------------
+// perm (may be null): the visiting order; thread i takes queue entry perm[i],
+// whose hit record is written at that entry's own index.
 // hits[3i] = (position, kind): kind >= 0 material index, -1 miss, -2 - l light l;
 // hits[3i+1] = (shading normal, t); hits[3i+2] = (geometric normal, 0).
 template <bool SDF, int MINB = 8>
 __global__ void __launch_bounds__(kPtBlock, MINB) k_pt_extend(pt_wave w, int v, float4 const* __restrict__ q,
     uint32_t const* __restrict__ count, float4* __restrict__ hits, uint32_t* __restrict__ clear_a,
-    uint32_t* __restrict__ clear_b, unsigned long long* __restrict__ stats) {
+    uint32_t* __restrict__ clear_b, unsigned long long* __restrict__ stats, uint32_t const* __restrict__ perm) {
   uint32_t const n = *count;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     *clear_a = 0;
@@ -181,7 +187,8 @@ __global__ void __launch_bounds__(kPtBlock, MINB) k_pt_extend(pt_wave w, int v, 
     if (v == 0) stats[0] += n;
   }
   uint32_t const stride = gridDim.x * blockDim.x;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  for (uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += stride) {
+    uint32_t const i = perm ? __ldg(perm + i0) : i0;
     float4 const q0 = q[3 * size_t(i)], q1 = q[3 * size_t(i) + 1];
     int const j = __float_as_int(q[3 * size_t(i) + 2].w);
     pt_job const& J = w.jobs[j];
@@ -233,6 +240,22 @@ __global__ void __launch_bounds__(kPtBlock, MINB) k_pt_extend(pt_wave w, int v, 
     hits[3 * size_t(i) + 1] = make_float4(ns.x, ns.y, ns.z, t);
     hits[3 * size_t(i) + 2] = make_float4(ng.x, ng.y, ng.z, 0.f);
   }
+}
+
+// Visiting order of an extension queue: each live entry's origin / direction
+// cell key in its scene's grid (ray_key), 0xFFFFFF (after every live key) for
+// the wave's empty slots.
+__global__ void __launch_bounds__(256) k_pt_keys(pt_wave w, float4 const* __restrict__ q,
+    uint32_t const* __restrict__ count, uint32_t n_max, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  uint32_t const i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_max) return;
+  uint32_t key = 0xFFFFFFu;
+  if (i < *count) {
+    pt_scene const& s = w.scenes[w.jobs[__float_as_int(q[3 * size_t(i) + 2].w)].scene];
+    key = min(ray_key(q[3 * size_t(i)], q[3 * size_t(i) + 1], s.key_lo, s.key_scale), 0xFFFFFEu);
+  }
+  keys[i] = key;
+  vals[i] = i;
 }
 
 // ---- shade ------------------------------------------------------------------------------
@@ -482,10 +505,15 @@ void mat_mul4(float const* a, float const* b, float* out) {
 int ensure_queues(myrt_ctx* ctx, physical_state& P, size_t paths) {
   if (P.capacity >= paths && P.queue[0]) return MYRT_OK;
   for (void* p : {static_cast<void*>(P.queue[0]), static_cast<void*>(P.queue[1]), static_cast<void*>(P.hits),
-           static_cast<void*>(P.shadow), static_cast<void*>(P.radiance), static_cast<void*>(P.counts)})
+           static_cast<void*>(P.shadow), static_cast<void*>(P.radiance), static_cast<void*>(P.counts),
+           static_cast<void*>(P.okeys[0]), static_cast<void*>(P.okeys[1]), static_cast<void*>(P.ovals[0]),
+           static_cast<void*>(P.ovals[1]), P.otemp})
     cudaFree(p);
   P.queue[0] = P.queue[1] = P.hits = P.shadow = P.radiance = nullptr;
   P.counts = nullptr;
+  P.okeys[0] = P.okeys[1] = P.ovals[0] = P.ovals[1] = nullptr;
+  P.otemp = nullptr;
+  P.otemp_bytes = 0;
   P.capacity = 0;
   int rc = MYRT_OK;
   auto alloc = [&](void** p, size_t bytes, char const* what) {
@@ -497,6 +525,14 @@ int ensure_queues(myrt_ctx* ctx, physical_state& P, size_t paths) {
   alloc(reinterpret_cast<void**>(&P.shadow), paths * 48, "shadow queue");
   alloc(reinterpret_cast<void**>(&P.radiance), paths * 16, "path radiance");
   alloc(reinterpret_cast<void**>(&P.counts), 4 * sizeof(uint32_t), "queue counts");
+  for (int k = 0; k < 2; ++k) {  // visiting order of the extension queues
+    alloc(reinterpret_cast<void**>(&P.okeys[k]), paths * 4, "queue order keys");
+    alloc(reinterpret_cast<void**>(&P.ovals[k]), paths * 4, "queue order entries");
+  }
+  if (!rc)
+    rc = check_cuda(ctx, cub::DeviceRadixSort::SortPairs(nullptr, P.otemp_bytes, P.okeys[0], P.okeys[1], P.ovals[0],
+                             P.ovals[1], int(paths), 0, kOrderKeyBits, ctx->stream), "queue order size");
+  alloc(&P.otemp, std::max<size_t>(P.otemp_bytes, 16), "queue order temporary");
   if (!rc && !P.stats) {
     alloc(reinterpret_cast<void**>(&P.stats), 4 * sizeof(unsigned long long), "ray statistics");
     if (!rc) rc = check_cuda(ctx, cudaMemsetAsync(P.stats, 0, 4 * sizeof(unsigned long long), ctx->stream), "clear");
@@ -509,11 +545,14 @@ int ensure_queues(myrt_ctx* ctx, physical_state& P, size_t paths) {
 pt_scene scene_of(myrt_ctx const* ctx) {
   device_scene const& S = ctx->scene;
   physical_state const& P = ctx->physical;
-  return pt_scene{S.nodes, S.tris, S.tri_normals, S.tri_material, reinterpret_cast<int2 const*>(S.materials),
+  pt_scene r{S.nodes, S.tris, S.tri_normals, S.tri_material, reinterpret_cast<int2 const*>(S.materials),
       int(S.n_materials), S.material_data, static_cast<ps::area_light const*>(P.lights), P.n_lights,
       sdfk::sdf_dev{ctx->sdf.instrs, ctx->sdf.programs, ctx->sdf.params, ctx->sdf.drawables, ctx->sdf.n_drawables,
           0, 0.f, ctx->sdf.skip_sphere, ctx->sdf.skip_next, ctx->sdf.cell_hdr, ctx->sdf.cell_start,
-          ctx->sdf.cell_list, ctx->sdf.op_count}};
+          ctx->sdf.cell_list, ctx->sdf.op_count},
+      float3{0.f, 0.f, 0.f}, float3{0.f, 0.f, 0.f}};
+  ray_key_grid(S.bounds, r.key_lo, r.key_scale);
+  return r;
 }
 
 // A job's static description (camera, resolution, spp, ...); the wave planner
@@ -627,15 +666,31 @@ int launch_plan(myrt_ctx* ctx, physical_state& P, cudaStream_t st, pt_scene cons
     int cur = 0;
     for (int v = 0; v <= wp.max_depth; ++v) {
       bool const last = v == wp.max_depth;
+      // visiting order (trace_order): the first bounces' queues (vertices 1 and 2), whose paths have
+      // scattered, sorted by origin / direction cell in waves of at least 1 Mi paths (0); never (1);
+      // every vertex after the camera's (2). Results never depend on it.
+      uint32_t const order = ctx->tuning.trace_order;
+      bool const sorted = per_entry && v >= 1 && wp.n_paths <= P.capacity &&
+          (order == 2 || (order == 0 && v <= 2 && wp.n_paths >= (1u << 20)));
+      uint32_t const* perm = nullptr;
+      if (sorted) {
+        k_pt_keys<<<(wp.n_paths + 255) / 256, 256, 0, st>>>(w, P.queue[cur], P.counts + cur, wp.n_paths, P.okeys[0],
+            P.ovals[0]);
+        size_t tb = P.otemp_bytes;
+        int rc = check_cuda(ctx, cub::DeviceRadixSort::SortPairs(P.otemp, tb, P.okeys[0], P.okeys[1], P.ovals[0],
+                                     P.ovals[1], int(wp.n_paths), 0, kOrderKeyBits, st), "queue order sort");
+        if (rc) return rc;
+        perm = P.ovals[1];
+      }
       if (any_sdf)
         k_pt_extend<true><<<qgrid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
-            P.counts + (1 - cur), P.counts + 2, P.stats);
+            P.counts + (1 - cur), P.counts + 2, P.stats, perm);
       else if (cap10)
         k_pt_extend<false, 10><<<qgrid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
-            P.counts + (1 - cur), P.counts + 2, P.stats);
+            P.counts + (1 - cur), P.counts + 2, P.stats, perm);
       else
         k_pt_extend<false><<<qgrid, kPtBlock, 0, st>>>(w, v, P.queue[cur], P.counts + cur, P.hits,
-            P.counts + (1 - cur), P.counts + 2, P.stats);
+            P.counts + (1 - cur), P.counts + 2, P.stats, perm);
       guide_dev gv = gd ? *gd : guide_dev{};
       if (last) gv.n_lobes = 0;
       if (gv.n_lobes > 0) {
@@ -682,7 +737,8 @@ int grow_bytes(myrt_ctx* ctx, void** p, size_t& cap, size_t bytes, char const* w
 void free_physical(physical_state& P) {
   for (void* p : {static_cast<void*>(P.queue[0]), static_cast<void*>(P.queue[1]), static_cast<void*>(P.hits),
            static_cast<void*>(P.shadow), static_cast<void*>(P.radiance), static_cast<void*>(P.counts), P.lights,
-           static_cast<void*>(P.stats), P.tables})
+           static_cast<void*>(P.stats), P.tables, static_cast<void*>(P.okeys[0]), static_cast<void*>(P.okeys[1]),
+           static_cast<void*>(P.ovals[0]), static_cast<void*>(P.ovals[1]), P.otemp})
     cudaFree(p);
   P = physical_state{};
 }
