@@ -269,14 +269,16 @@ struct shade_io {
   uint32_t* count_shadow;
   float4* radiance;
   guide_dev guide;  // guide.n_lobes == 0: plain BSDF sampling
+  uint32_t const* perm;  // may be null: thread i shades entry perm[i] (the extend kernel's order)
 };
 
 __global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_wave w, int v, shade_io io) {
   uint32_t const n = *io.count;
   uint32_t const stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {  // warp-uniform trip count
-    uint32_t const i = base + threadIdx.x;
-    bool const active = i < n;
+    uint32_t const i0 = base + threadIdx.x;
+    bool const active = i0 < n;
+    uint32_t const i = active && io.perm ? __ldg(io.perm + i0) : i0;
     bool emit_next = false, emit_shadow = false;
     float4 nq0, nq1, nq2, sq0, sq1, sq2;
     if (active) {
@@ -697,8 +699,9 @@ int launch_plan(myrt_ctx* ctx, physical_state& P, cudaStream_t st, pt_scene cons
         int rc = guide_infer(ctx, gv, 0, 0, P.queue[cur], P.hits, P.counts + cur, st);
         if (rc) return rc;
       }
+      // shading in the same order appends the next queue and the shadow rays in that order too
       shade_io io{P.queue[cur], P.hits, P.counts + cur, P.queue[1 - cur], P.counts + (1 - cur), P.shadow,
-          P.counts + 2, P.radiance, gv};
+          P.counts + 2, P.radiance, gv, perm};
       k_pt_shade<<<qgrid, kPtBlock, 0, st>>>(w, v, io);
       if (!last && n_lights_max > 0) {
         if (any_sdf) k_pt_shadow<true><<<qgrid, kPtBlock, 0, st>>>(w, v, P.shadow, P.counts + 2, P.radiance, P.stats);
