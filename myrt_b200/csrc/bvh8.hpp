@@ -3,8 +3,8 @@
 // Stage 1: binned-SAH binary tree (16 bins, split cost 7 / intersection cost 2,
 // as the reference's bvh::compute_split_axis, src/pathtracer/bvh.cpp:43-116),
 // over triangle boxes padded by 1e-5 with the triangle centroid as split key
-// (generate_triangle_bounds, bvh.cpp:136-152). Leaves hold at most
-// `max_leaf` (4) triangles. O(n log n): no spatial splits, so no mid-vector
+// (generate_triangle_bounds, bvh.cpp:136-152), split down to single
+// triangles (`binary_leaf`). O(n log n): no spatial splits, so no mid-vector
 // inserts or whole-tree index fix-ups (the reference's bvh.cpp:460-488 path).
 //
 // Stage 2: collapse into an 8-wide tree with quantised child boxes: one 80-byte
@@ -54,7 +54,10 @@ struct bvh8_triangle {
 static_assert(sizeof(bvh8_triangle) == 48, "bvh8_triangle must be 48 bytes");
 
 struct bvh8_build_options {
-  int max_leaf = 4;        // triangles per leaf of the binary tree (and per wide-node slot)
+  int max_leaf = 4;        // triangles per wide-node leaf slot
+  int binary_leaf = 1;     // triangles per leaf of the binary tree (1..max_leaf); the collapse regroups
+                           // them into slots of up to max_leaf
+  float collapse_prim_cost = 0.8f;  // collapse SAH: cost of a triangle test relative to a node visit
   int bins = 16;           // SAH bins per axis
   float cost_traverse = 7.f;
   float cost_intersect = 2.f;
