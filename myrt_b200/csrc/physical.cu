@@ -272,7 +272,9 @@ struct shade_io {
   uint32_t const* perm;  // may be null: thread i shades entry perm[i] (the extend kernel's order)
 };
 
-__global__ void __launch_bounds__(kPtBlock) k_pt_shade(pt_wave w, int v, shade_io io) {
+// Six resident blocks per SM (80 registers, some spills; 150 unbounded): measured 1.8 % faster per
+// frame on a 512x512 64-spp render.
+__global__ void __launch_bounds__(kPtBlock, 6) k_pt_shade(pt_wave w, int v, shade_io io) {
   uint32_t const n = *io.count;
   uint32_t const stride = gridDim.x * blockDim.x;
   for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {  // warp-uniform trip count
