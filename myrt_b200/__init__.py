@@ -14,7 +14,7 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
-from ._abi import ISECT_REFERENCE, ISECT_WATERTIGHT, MYRT_ERR_DEVICE_ABORT, MYRT_OK  # noqa: F401
+from ._abi import ISECT_REFERENCE, ISECT_WATERTIGHT, MYRT_ERR_DEVICE_ABORT, MYRT_ERR_UNSUPPORTED, MYRT_OK  # noqa: F401
 
 HIT_DTYPE = np.dtype([("prim", np.int32), ("t", np.float32), ("u", np.float32), ("v", np.float32)])
 

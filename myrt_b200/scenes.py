@@ -266,6 +266,21 @@ def _rotation(axis, angle) -> np.ndarray:
     return np.eye(3) + s * K + (1 - c) * (K @ K)
 
 
+def exponential_chain(ratio: float = 1.2, k0: int = -450, k1: int = 480) -> np.ndarray:
+    """A degenerate scene: triangles k = k0 .. k1-1 at x = ratio^k along the x
+    axis, each 0.3 x its distance from the origin in size (those that overflow
+    float32 are dropped). Every SAH split cuts off only a few triangles, so the
+    tree grows about one level per few triangles: with the defaults, deeper
+    than the traversal stack allows (32 wide levels). float32 [T, 9]."""
+    k = np.arange(k0, k1, dtype=np.float64)
+    x = ratio ** k
+    s = 0.3 * x
+    z = np.zeros_like(x)
+    t = np.stack([x, z, z, x + s, z, z, x, s, z], 1)
+    keep = np.isfinite(t).all(1) & (np.abs(t).max(1) < 1e37)
+    return t[keep].astype(np.float32)
+
+
 def unit_box():
     """Axis-aligned cube [-1, 1]^3 as 12 triangles: (indices uint32, points float32)."""
     p = np.array([[x, y, z] for z in (-1, 1) for y in (-1, 1) for x in (-1, 1)], np.float32)

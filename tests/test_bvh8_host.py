@@ -129,3 +129,13 @@ def test_cpu_bvh8_traversal_equals_brute_force(isect):
         assert np.array_equal(b8, bf)
         occ, _, _ = po.bvh8_traverse(nodes, tris, r, isect=isect, any_hit=True)
         assert np.array_equal(occ.astype(bool), bf["prim"] >= 0)
+
+
+def test_exponential_chain_is_deeper_than_the_traversal_stack():
+    """The degenerate chain the GPU tests use to check that an upload of a tree
+    deeper than 32 wide levels is refused really builds one."""
+    from myrt_b200.scenes import exponential_chain
+
+    nodes, tris, info = mb.build_bvh8(exponential_chain())
+    assert info["wide_depth"] > 32
+    assert info["triangles"] == exponential_chain().shape[0]

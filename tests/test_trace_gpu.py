@@ -350,3 +350,19 @@ def test_large_sorted_query_matches_input_order(ctx, hf128):
     ora, cn, ct = po.bvh8_traverse(hf128["nodes"], hf128["tris"], rays[sel])
     assert np.array_equal(out[0][0][sel].view(mb.HIT_DTYPE).ravel(), ora)
     assert np.array_equal(out[0][3][sel].astype(np.uint32), cn)
+
+
+def test_upload_of_a_tree_deeper_than_the_stack_is_refused(ctx, hf128):
+    """myrt_scene_upload refuses a tree deeper than the traversal stack (32
+    wide levels) with MYRT_ERR_UNSUPPORTED instead of letting kernels overflow
+    it; the context then takes a normal scene and answers queries."""
+    from myrt_b200.scenes import exponential_chain
+
+    t9 = exponential_chain()
+    with pytest.raises(mb.MyrtError, match="deeper than the traversal stack") as e:
+        ctx.upload_scene(np.arange(t9.shape[0] * 3, dtype=np.uint32), t9.reshape(-1, 3))
+    assert e.value.code == mb.MYRT_ERR_UNSUPPORTED
+    ctx.upload_scene(hf128["idx"], hf128["pts"])
+    rays = pinhole_rays(64, 64)
+    hits = ctx.trace_closest(rays)
+    assert (hits["prim"] >= 0).any()
