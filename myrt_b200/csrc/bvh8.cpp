@@ -311,27 +311,27 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
     self(self, std::uint32_t(bn[n].left + 1), prims);
   };
 
-  struct item {
-    std::uint32_t bnode;
-    int depth;
+  // Emission, level by level of the wide tree (nodes are numbered in breadth-first order, the
+  // children of a node contiguous): plan every node of a level in parallel (its slots, boxes,
+  // quantised planes, leaf meta, internal children and triangle count), turn the counts into
+  // child and triangle bases by a prefix sum in level order, then write the nodes and their leaf
+  // triangles in parallel. The result equals a sequential breadth-first emission.
+  struct wide_plan {
+    bvh8_node node;
+    std::int32_t slot_kid[8];
+    std::uint32_t kids[8];
+    int n_kids;
+    std::uint32_t n_tris;
+    int n_leaf_slots;
   };
-  std::vector<item> queue;
-  queue.push_back({0, 1});
-  out.nodes.resize(1);
-  out.triangles.reserve(n_tris);
-  int wide_depth = 0;
-  std::size_t leaf_slots = 0;
-  std::vector<slot_t> slots;
-  std::vector<std::uint32_t> prims;
-  for (std::size_t qi = 0; qi < queue.size(); ++qi) {
-    item const it = queue[qi];
-    wide_depth = std::max(wide_depth, it.depth);
+  auto plan = [&](std::uint32_t bnode_index, wide_plan& w, std::vector<slot_t>& slots,
+                  std::vector<std::uint32_t>& prims) {
     slots.clear();
-    if (bn[it.bnode].left < 0) {
-      slots.push_back({it.bnode, false});  // a lone leaf (tiny scenes): one leaf slot
+    if (bn[bnode_index].left < 0) {
+      slots.push_back({bnode_index, false});  // a lone leaf (tiny scenes): one leaf slot
     } else {
-      gather(gather, std::uint32_t(bn[it.bnode].left), D[it.bnode].split8, slots);
-      gather(gather, std::uint32_t(bn[it.bnode].left + 1), 8 - D[it.bnode].split8, slots);
+      gather(gather, std::uint32_t(bn[bnode_index].left), D[bnode_index].split8, slots);
+      gather(gather, std::uint32_t(bn[bnode_index].left + 1), 8 - D[bnode_index].split8, slots);
     }
     int const nk = int(slots.size());
     std::uint32_t kids[8];
@@ -373,18 +373,18 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
         slot_of[bk] = bs;
       }
     }
-    std::int32_t slot_kid[8];
     bool slot_internal[8];
     for (int s = 0; s < 8; ++s) {
-      slot_kid[s] = -1;
+      w.slot_kid[s] = -1;
       slot_internal[s] = false;
     }
     for (int k = 0; k < nk; ++k) {
-      slot_kid[slot_of[k]] = std::int32_t(kids[k]);
+      w.slot_kid[slot_of[k]] = std::int32_t(kids[k]);
       slot_internal[slot_of[k]] = slots[std::size_t(k)].internal;
     }
 
-    bvh8_node node{};
+    bvh8_node& node = w.node;
+    node = bvh8_node{};
     node.px = nbox.lo[0];
     node.py = nbox.lo[1];
     node.pz = nbox.lo[2];
@@ -394,11 +394,11 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
       scale[a] = std::ldexp(1.0, int(node.e[a]) - 127);
     }
     float const p[3] = {node.px, node.py, node.pz};
-    node.child_base = std::uint32_t(out.nodes.size());
-    node.tri_base = std::uint32_t(out.triangles.size());
     std::uint32_t tri_off = 0;
+    w.n_kids = 0;
+    w.n_leaf_slots = 0;
     for (int s = 0; s < 8; ++s) {
-      if (slot_kid[s] < 0) {
+      if (w.slot_kid[s] < 0) {
         for (int a = 0; a < 3; ++a) {
           node.qlo[a][s] = 1;
           node.qhi[a][s] = 0;
@@ -406,7 +406,7 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
         node.meta[s] = 0;
         continue;
       }
-      bnode const& c = bn[std::uint32_t(slot_kid[s])];
+      bnode const& c = bn[std::uint32_t(w.slot_kid[s])];
       for (int a = 0; a < 3; ++a) {
         double const lo = std::floor((double(c.box.lo[a]) - double(p[a])) / scale[a]);
         double const hi = std::ceil((double(c.box.hi[a]) - double(p[a])) / scale[a]);
@@ -416,30 +416,93 @@ bvh8 build_bvh8(float const* positions, std::size_t n_tris, std::uint32_t const*
       if (slot_internal[s]) {
         node.imask |= std::uint8_t(1u << s);
         node.meta[s] = std::uint8_t(0x20u | unsigned(s));
-        out.nodes.emplace_back();
-        queue.push_back({std::uint32_t(slot_kid[s]), it.depth + 1});
+        w.kids[w.n_kids++] = std::uint32_t(w.slot_kid[s]);
+        w.slot_kid[s] = -1;  // only leaf slots keep their binary node for the triangle pass
       } else {
         prims.clear();
-        collect(collect, std::uint32_t(slot_kid[s]), prims);
+        collect(collect, std::uint32_t(w.slot_kid[s]), prims);
         std::uint32_t const cnt = std::uint32_t(prims.size());
         node.meta[s] = std::uint8_t(tri_off | (cnt << 5));
-        for (std::uint32_t prim : prims) {
-          float const* v = positions + 9 * std::size_t(prim);
-          bvh8_triangle t{};
-          std::memcpy(t.v0, v, 12);
-          std::memcpy(t.v1, v + 3, 12);
-          std::memcpy(t.v2, v + 6, 12);
-          t.prim = prim_ids ? prim_ids[prim] : prim;
-          out.triangles.push_back(t);
-        }
         tri_off += cnt;
-        ++leaf_slots;
+        ++w.n_leaf_slots;
       }
     }
-    out.nodes[qi] = node;
+    w.n_tris = tri_off;
+  };
+  // parallel loop over [0, n) in contiguous chunks, fn(begin, end, worker scratch index)
+  unsigned const workers = std::max(1u, opt.threads > 0 ? unsigned(opt.threads) : std::thread::hardware_concurrency());
+  auto parallel_for = [&](std::size_t n, auto&& fn) {
+    std::size_t const parts = std::min<std::size_t>(workers, (n + 1023) / 1024);
+    if (parts <= 1) {
+      fn(std::size_t(0), n, 0u);
+      return;
+    }
+    std::vector<std::thread> pool;
+    std::size_t const step = (n + parts - 1) / parts;
+    for (std::size_t w = 0; w < parts; ++w) {
+      std::size_t const b = w * step, e = std::min(n, b + step);
+      if (b >= e) break;
+      pool.emplace_back([&fn, b, e, w] { fn(b, e, unsigned(w)); });
+    }
+    for (auto& t : pool) t.join();
+  };
+  std::vector<std::vector<slot_t>> slot_scratch(workers);
+  std::vector<std::vector<std::uint32_t>> prim_scratch(workers);
+
+  out.triangles.resize(n_tris);
+  std::vector<std::uint32_t> level{0}, next;  // binary nodes of the current level, in node order
+  std::vector<wide_plan> plans;
+  std::vector<std::uint32_t> child_base, tri_base;
+  std::size_t level_base = 0, tris_done = 0, leaf_slots = 0;
+  int wide_depth = 0;
+  while (!level.empty()) {
+    ++wide_depth;
+    std::size_t const n_level = level.size();
+    plans.resize(n_level);
+    parallel_for(n_level, [&](std::size_t b, std::size_t e, unsigned w) {
+      for (std::size_t i = b; i < e; ++i) plan(level[i], plans[i], slot_scratch[w], prim_scratch[w]);
+    });
+    child_base.resize(n_level);
+    tri_base.resize(n_level);
+    std::size_t next_base = level_base + n_level, kids_total = 0;
+    for (std::size_t i = 0; i < n_level; ++i) {
+      child_base[i] = std::uint32_t(next_base + kids_total);
+      tri_base[i] = std::uint32_t(tris_done);
+      kids_total += std::size_t(plans[i].n_kids);
+      tris_done += plans[i].n_tris;
+      leaf_slots += std::size_t(plans[i].n_leaf_slots);
+    }
+    out.nodes.resize(next_base + kids_total);
+    next.resize(kids_total);
+    parallel_for(n_level, [&](std::size_t b, std::size_t e, unsigned w) {
+      std::vector<std::uint32_t>& pr = prim_scratch[w];
+      for (std::size_t i = b; i < e; ++i) {
+        wide_plan& wp = plans[i];
+        wp.node.child_base = child_base[i];
+        wp.node.tri_base = tri_base[i];
+        out.nodes[level_base + i] = wp.node;
+        for (int k = 0; k < wp.n_kids; ++k) next[child_base[i] - next_base + std::size_t(k)] = wp.kids[k];
+        std::size_t t = tri_base[i];
+        for (int s = 0; s < 8; ++s) {
+          if (wp.slot_kid[s] < 0) continue;
+          pr.clear();
+          collect(collect, std::uint32_t(wp.slot_kid[s]), pr);
+          for (std::uint32_t prim : pr) {
+            float const* v = positions + 9 * std::size_t(prim);
+            bvh8_triangle& tr = out.triangles[t++];
+            tr = bvh8_triangle{};
+            std::memcpy(tr.v0, v, 12);
+            std::memcpy(tr.v1, v + 3, 12);
+            std::memcpy(tr.v2, v + 6, 12);
+            tr.prim = prim_ids ? prim_ids[prim] : prim;
+          }
+        }
+      }
+    });
+    level_base = next_base;
+    level.swap(next);
   }
-  // The queue index equals the wide-node index: children are appended in the
-  // same order as they are queued.
+  if (tris_done != n_tris) throw std::runtime_error("BVH emission lost triangles");
 
   auto const t1 = std::chrono::steady_clock::now();
   out.stats.binary_nodes = nb;

@@ -7,7 +7,8 @@
 // triangles (`binary_leaf`). O(n log n): no spatial splits, so no mid-vector
 // inserts or whole-tree index fix-ups (the reference's bvh.cpp:460-488 path).
 //
-// Stage 2: collapse into an 8-wide tree with quantised child boxes: one 80-byte
+// Stage 2: collapse into an 8-wide tree with quantised child boxes (emitted level
+// by level, each level's nodes planned and written in parallel): one 80-byte
 // node = five 16-byte words (compressed wide BVH in the manner of Ylitie,
 // Karras and Laine, HPG 2017). Children are placed in slots by ray octant so
 // that visiting slot bits from high to low is roughly front to back.
